@@ -1,0 +1,239 @@
+/*
+ * qes_b200.h -- C ABI of the B200 RBM variational-Monte-Carlo library.
+ *
+ * One shared library (libqes_b200.so) exposes the hot path of QES's
+ * neural-quantum-state VMC step for RBM ansaetze: Markov-chain sampling,
+ * local energy, log-derivatives and the stochastic-reconfiguration solve.
+ * Each entry point names the reference callable it replaces (file:line
+ * within makskliczkowski/pyqusolver, Python/QES/...).
+ *
+ * Conventions
+ *  - All array arguments are DEVICE pointers owned by the caller; the library
+ *    never allocates.  Scratch space is passed in (size from *_workspace_bytes).
+ *  - Every call is asynchronous on `stream` (a cudaStream_t, 0 = legacy default)
+ *    and returns a status code; qes_last_error() gives the message.
+ *  - dtype: QES_DTYPE_F32 (real RBM, float32) or QES_DTYPE_C64 (holomorphic
+ *    complex RBM, complex64 interleaved re/im).
+ *  - Spin configurations are bit-packed uint32 words, ceil(ns/32) per
+ *    configuration: bit (i & 31) of word (i >> 5) is 1 for spin up
+ *    (s = +0.5, sigma = +1).  Site order follows the lattice.
+ *  - RBM: log psi(sigma) = sum_i a_i sigma_i + sum_m log cosh(theta_m),
+ *    theta = W^T sigma + b, W row-major (ns x nh).  Flat parameter order is
+ *    [a (ns), b (nh), W (ns*nh)].
+ */
+#ifndef QES_B200_H
+#define QES_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QES_OK 0
+#define QES_ERR_ARG 1             /* bad shape / pointer / option              */
+#define QES_ERR_CUDA 2            /* CUDA runtime error                        */
+#define QES_ERR_WORKSPACE 3       /* workspace too small                       */
+#define QES_ERR_NOT_CONVERGED 4   /* iterative solve hit maxiter               */
+#define QES_ERR_TIMEOUT 5         /* a bounded device wait gave up             */
+#define QES_ERR_SIZE 6            /* size beyond a compiled or static limit    */
+
+#define QES_DTYPE_F32 0
+#define QES_DTYPE_C64 1
+
+#define QES_INIT_RND 0            /* independent random spins                  */
+#define QES_INIT_RND_FIXED 1      /* fixed number of up spins, random order    */
+#define QES_INIT_UP 2
+#define QES_INIT_DOWN 3
+
+#define QES_RULE_LOCAL 0          /* single spin flip                          */
+#define QES_RULE_EXCHANGE 1       /* Sz-conserving neighbour exchange          */
+
+#define QES_MOVE_FLIP1 0          /* flip site i                               */
+#define QES_MOVE_PAIR_ANTI 1      /* flip i and j, active when sigma_i != sigma_j */
+#define QES_MOVE_PAIR_PAR 2       /* flip i and j, active when sigma_i == sigma_j */
+
+/* Last error message of the calling thread (static storage). */
+const char* qes_last_error(void);
+/* Library version: 100*major + minor. */
+int qes_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Initial chain states.
+ * Replaces QES/Solver/MonteCarlo/initialization/states.py:242-297
+ * (_set_state_rand_fixed) and the RND initializer of the same file.
+ * Philox stream: counter (chain, word|pos, 0, 1|2), key = seed.             */
+int qes_init_chains(int kind, int n_up, uint64_t seed, int64_t chain_offset,
+                    int n_chains, int ns, uint32_t* bits_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Per-move ratio tables of the RBM (rebuilt after each parameter update).
+ * For move k with sites (i, j) and kind:  D_k = W_i (FLIP1), W_i - W_j
+ * (PAIR_ANTI), W_i + W_j (PAIR_PAR); Ct = cosh(2 D_km), St = sinh(2 D_km)
+ * stored [m][k] (move_major = 0, local energy) or [k][m] (move_major = 1,
+ * sampler); A[k] = a_i, a_i - a_j or a_i + a_j.
+ * psi(s')/psi(s) = exp(-2 sigma_i A_k) prod_m (C_km - sigma_i tanh(theta_m) S_km).
+ * Replaces the per-proposal ratio of net_rbm.log_psi_delta
+ * (contract: Python/tests/nqs/test_rbm_fast_update.py:47-147).              */
+int qes_rbm_move_tables(int dtype, int ns, int nh, const void* a, const void* W,
+                        int n_moves, const int32_t* move_i, const int32_t* move_j,
+                        const int32_t* move_kind, int move_major, void* Ct,
+                        void* St, void* A, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* RBM forward on a batch of packed configurations: theta = W^T sigma + b,
+ * tanh(theta) and log psi.  Any output pointer may be NULL.
+ * Replaces the RBM apply (general_python net_rbm) as driven by
+ * QES/Solver/MonteCarlo/vmc.py:1113-1164 (_batched_network_apply,
+ * _init_logprobas_jax) and QES/NQS/nqs.py:1257-1280.                        */
+int qes_rbm_forward(int dtype, int ns, int nh, int64_t n_samples,
+                    const uint32_t* bits, const void* a, const void* b,
+                    const void* W, void* theta_out, void* tanh_out,
+                    void* logpsi_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Metropolis sampler (persistent: one warp per chain).
+ * Replaces VMCSampler._static_sample_jax / _run_mcmc_steps_jax
+ * (QES/Solver/MonteCarlo/vmc.py:952-1103, 1186-1283) with the proposals of
+ * QES/Solver/MonteCarlo/updates/spin_jax.py:51-158.
+ * Schedule: therm_steps_total proposals, then num_samples records each
+ * preceded by sweep_steps proposals.  Outputs are sample-major:
+ * record r of chain c is row r*n_chains + c.                               */
+typedef struct {
+    int rule;                  /* QES_RULE_LOCAL / QES_RULE_EXCHANGE           */
+    int ns, nh;
+    int n_chains;
+    int64_t chain_offset;      /* global id of chain 0 (Philox counter)        */
+    int num_samples;
+    int64_t therm_steps_total; /* proposals before the first record            */
+    int sweep_steps;           /* proposals before each record                 */
+    int recompute_every;       /* full theta recompute period (0 -> ns)        */
+    float mu, beta;            /* acceptance: log u < min(beta*mu*Re dlogpsi, 0) */
+    uint64_t seed;
+    int deg;                   /* neighbour-table width (EXCHANGE)             */
+} qes_sampler_config;
+
+int qes_sampler_run(int dtype, const qes_sampler_config* cfg,
+                    const void* a, const void* b, const void* W,
+                    const void* flipCt, const void* flipSt,   /* tables of moves FLIP1 i=0..ns-1 */
+                    const int32_t* nbr_table,                /* [ns*deg], -1 padded           */
+                    const int32_t* nbr_pair,                 /* [ns*deg] pair index or -1     */
+                    const int32_t* pair_i, const int32_t* pair_j, int n_pairs,
+                    const void* pairCt, const void* pairSt,  /* PAIR_ANTI tables of the pairs */
+                    uint32_t* chain_bits, uint64_t* chain_step,
+                    int32_t* proposed, int32_t* accepted,
+                    uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
+                    void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Hamiltonian lowered to moves (off-diagonal) and diagonal terms.
+ * Off-diagonal move k contributes  conj(c_k(s)) psi(s')/psi(s)  with
+ * conj(c_k(s)) = (coef[4k] + i coef[4k+1]) + sigma_i (coef[4k+2] + i coef[4k+3]).
+ * Diagonal: sum zf_h[t] sigma_{zf_site[t]} + sum zz_J[t] sigma_{zz_i[t]} sigma_{zz_j[t]}
+ * (0.5 / 0.25 spin factors and QES signs already folded in).
+ * Replaces QES/Algebra/Hamil/hamil_energy_jax.py:428-576 and the model
+ * term builders (transverse_ising.py:192-300, xxz.py:278-433, j1j2.py:119-295). */
+typedef struct {
+    int n_moves;
+    const int32_t* move_i;
+    const int32_t* move_j;
+    const int32_t* move_kind;
+    const float* move_coef;    /* [4*n_moves] */
+    int n_zfield;
+    const int32_t* zf_site;
+    const float* zf_h;
+    int n_zz;
+    const int32_t* zz_i;
+    const int32_t* zz_j;
+    const float* zz_J;
+} qes_hamiltonian;
+
+/* Local energy E_loc(s) = sum_k conj(c_k) psi(s'_k)/psi(s), complex64 out.
+ * tanh_theta: [n_samples][nh] from qes_rbm_forward; Ct/St/A: move tables of
+ * the same Hamiltonian moves.  Replaces net_utils_jax.apply_callable_batched_jax
+ * (contract: Python/tests/nqs/test_nqs_generic_config_and_learning.py:282-371)
+ * as called by QES/NQS/src/nqs_kernels.py:294-375.                          */
+int qes_local_energy_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples,
+                                     int n_moves, size_t* bytes);
+int qes_local_energy(int dtype, int ns, int nh, int64_t n_samples,
+                     const uint32_t* bits, const void* tanh_theta,
+                     const qes_hamiltonian* ham, const void* Ct, const void* St,
+                     const void* A, void* workspace, size_t workspace_bytes,
+                     void* eloc_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Energy statistics in float64 (compensated): out = [mean_re, mean_im, var, std]
+ * with weights probs (NULL = uniform).  Replaces the mean/std of
+ * QES/NQS/src/tdvp.py:1075-1076 and the estimator statistics.              */
+int qes_loss_stats_workspace_bytes(int64_t n_samples, size_t* bytes);
+int qes_loss_stats(int64_t n_samples, const void* eloc, const float* probs,
+                   double* out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Per-sample log-derivatives O (rows of P = ns + nh + ns*nh, leading dim ldo):
+ * O_a = sigma_i, O_b = tanh theta_m, O_W = sigma_i tanh theta_m.
+ * Replaces compute_gradients_batched / log_derivative_jax
+ * (QES/NQS/src/nqs_kernels.py:212-259, QES/NQS/nqs.py:2134-2188).          */
+int qes_rbm_log_derivatives(int dtype, int ns, int nh, int64_t n_samples,
+                            const uint32_t* bits, const void* tanh_theta,
+                            void* O_out, int64_t ldo, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Stochastic reconfiguration with the RBM's structured O (never materialised):
+ *   (O_c^H O_c / Ns + shift) x = F,  F = O_c^H E_c / Ns,  x <- rhs_prefactor x.
+ * Vectors are float64 (real RBM) or complex128 (complex RBM), length P.
+ * Replaces TDVP.get_tdvp_standard / _solve_prepare_matvec / solve
+ * (QES/NQS/src/tdvp.py:1056-1197,1524-1609) with SciPy-style CG
+ * (||r|| <= max(rtol ||b||, atol); nqs.py:3014 default 'scipy_cg').        */
+typedef struct {
+    double shift;
+    double rtol;
+    double atol;
+    int maxiter;
+    int check_every;           /* host convergence check period (iterations) */
+    double rhs_prefactor;
+} qes_sr_options;
+
+typedef struct {
+    int iterations;
+    int converged;
+    double residual;
+    double rhs_norm;
+    double e_mean_re, e_mean_im;
+} qes_sr_result;
+
+int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
+
+/* F = O_c^H E_c / Ns (force) and the matvec y = (O_c^H O_c / Ns + shift) v. */
+int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples,
+                 const uint32_t* bits, const void* tanh_theta, const void* eloc,
+                 void* force_out, void* workspace, size_t workspace_bytes, void* stream);
+int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples,
+                  const uint32_t* bits, const void* tanh_theta, double shift,
+                  const void* v, void* y_out, void* workspace,
+                  size_t workspace_bytes, void* stream);
+int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples,
+                    const uint32_t* bits, const void* tanh_theta, const void* eloc,
+                    const qes_sr_options* opt, void* x_out, qes_sr_result* result,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* Vector-Jacobian product of log psi for the hand-written backward:
+ * grad = O^H g  (g: complex64 per sample; real part used for a real RBM),
+ * float64/complex128 out, length P.  Replaces jax.vjp of the RBM apply
+ * behind compute_gradients_batched (QES/NQS/src/nqs_kernels.py:212-259).
+ * Workspace: qes_sr_workspace_bytes.                                        */
+int qes_rbm_logpsi_vjp(int dtype, int ns, int nh, int64_t n_samples,
+                       const uint32_t* bits, const void* tanh_theta, const void* g,
+                       void* grad_out, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/* Euler / SGD update in float64: master += lr * x; params = (float) master.
+ * Replaces NQSTrainer._apply_parameter_update (QES/NQS/src/nqs_train.py:1235-1262). */
+int qes_param_update(int dtype, int64_t n_params, double lr, const void* x,
+                     void* master, void* params, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QES_B200_H */

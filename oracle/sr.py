@@ -1,0 +1,113 @@
+"""Stochastic reconfiguration / TDVP solve (oracle side).
+
+TEST INFRASTRUCTURE ONLY (see ``oracle/__init__.py``).
+
+Follows ``TDVP`` (``QES/NQS/src/tdvp.py``) with the normalisation pinned by
+``Python/tests/nqs/test_tdvp_matrix_free_regressions.py:46-151``:
+
+* centring of E_loc and O, promotion to float64/complex128 (``tdvp.py:1056-1085``);
+* force F = O_c^H E_c / Ns (``tdvp.py:1099-1108``);
+* standard SR solves (O_c^H O_c / Ns + shift I) x = F
+  (GRAM form: s = O_c, s_p = O_c^H; MATVEC form v -> O_c^H (O_c v) / Ns);
+* MinSR solves (O_c O_c^H / Ns + shift I) y = E_c / Ns and projects x = O_c^H y
+  (``tdvp.py:1199-1226,1393-1408``);
+* x <- rhs_prefactor * x (default -1), optional global-norm clip
+  (``tdvp.py:882-907,1382-1422``);
+* Euler / SGD update p <- p + lr * x (``nqs_train.py:1235-1262``).
+
+The CG stopping rule is SciPy's (the reference's default ``lin_solver`` is
+``scipy_cg``, ``QES/NQS/nqs.py:3014``): stop when ||r|| <= max(rtol*||b||, atol).
+Centring with non-uniform sample weights is not pinned by the reference
+(its SR module is in the empty submodule); the weighted form here uses the
+weighted means and weights w_s / Ns in every sum.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def prepare(e_loc, O, probs=None):
+    e = np.asarray(e_loc)
+    O = np.asarray(O)
+    dt = np.complex128 if (np.iscomplexobj(e) or np.iscomplexobj(O)) else np.float64
+    e = e.astype(dt)
+    O = O.astype(np.complex128 if np.iscomplexobj(O) else np.float64)
+    ns = e.shape[0]
+    if probs is None:
+        w = np.ones(ns)
+    else:
+        w = np.asarray(probs, dtype=np.float64).reshape(-1)
+    e_m = np.sum(w * e) / ns
+    o_m = (w @ O) / ns
+    return e - e_m, O - o_m[None, :], w, e_m, o_m
+
+
+def force(O_c, e_c, w=None):
+    ns = O_c.shape[0]
+    w = np.ones(ns) if w is None else w
+    return np.conj(O_c).T @ (w * e_c) / ns
+
+
+def s_matrix(O_c, w=None):
+    ns = O_c.shape[0]
+    w = np.ones(ns) if w is None else w
+    return np.conj(O_c).T @ (w[:, None] * O_c) / ns
+
+
+def cg(matvec, b, *, rtol=1e-8, atol=0.0, maxiter=1000, x0=None):
+    """Conjugate gradients in float64/complex128.  Returns (x, iterations, residual_norm, converged)."""
+    b = np.asarray(b)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=b.dtype)
+    r = b - matvec(x) if x0 is not None else b.copy()
+    p = r.copy()
+    rr = np.vdot(r, r).real
+    bnorm = np.linalg.norm(b)
+    thresh = max(rtol * bnorm, atol)
+    if np.sqrt(rr) <= thresh:
+        return x, 0, np.sqrt(rr), True
+    for it in range(1, maxiter + 1):
+        Ap = matvec(p)
+        alpha = rr / np.vdot(p, Ap)
+        x = x + alpha * p
+        r = r - alpha * Ap
+        rr_new = np.vdot(r, r).real
+        if np.sqrt(rr_new) <= thresh:
+            return x, it, np.sqrt(rr_new), True
+        p = r + (rr_new / rr) * p
+        rr = rr_new
+    return x, maxiter, np.sqrt(rr), False
+
+
+def solve_sr(e_loc, O, *, shift=1e-3, probs=None, method="dense", rtol=1e-8,
+             maxiter=1000, rhs_prefactor=-1.0, grad_clip=None, use_minsr=False):
+    """Return (x, info) with x already scaled by rhs_prefactor (and clipped)."""
+    e_c, O_c, w, e_m, o_m = prepare(e_loc, O, probs)
+    ns, npar = O_c.shape
+    info = {"mean": e_m, "o_mean": o_m}
+    if use_minsr:
+        T = (np.sqrt(w)[:, None] * O_c) @ (np.conj(O_c).T * np.sqrt(w)[None, :]) / ns
+        rhs = np.sqrt(w) * e_c / ns
+        y = np.linalg.solve(T + shift * np.eye(ns), rhs)
+        x = np.conj(O_c).T @ (np.sqrt(w) * y)
+        info.update(iterations=0, converged=True)
+    else:
+        F = force(O_c, e_c, w)
+        info["force"] = F
+        if method == "dense":
+            S = s_matrix(O_c, w)
+            x = np.linalg.solve(S + shift * np.eye(npar), F)
+            info.update(iterations=0, converged=True)
+        elif method == "cg":
+            def mv(v):
+                return np.conj(O_c).T @ (w * (O_c @ v)) / ns + shift * v
+            x, it, res, conv = cg(mv, F, rtol=rtol, maxiter=maxiter)
+            info.update(iterations=it, residual=res, converged=conv)
+        else:
+            raise ValueError(method)
+    x = rhs_prefactor * x
+    if grad_clip is not None and grad_clip > 0:
+        nrm = np.linalg.norm(x)
+        if nrm > grad_clip:
+            x = x * (grad_clip / (nrm + 1e-12))
+    return x, info

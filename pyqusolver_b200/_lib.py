@@ -1,0 +1,140 @@
+"""ctypes binding of libqes_b200.so (the C ABI declared in include/qes_b200.h).
+
+Loading never falls back to anything: if the library is missing the import of
+the compute path raises, and every call that returns a nonzero status raises
+``QESError`` with the library's message.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqes_b200.so")
+
+QES_OK = 0
+QES_ERR_ARG = 1
+QES_ERR_CUDA = 2
+QES_ERR_WORKSPACE = 3
+QES_ERR_NOT_CONVERGED = 4
+QES_ERR_TIMEOUT = 5
+QES_ERR_SIZE = 6
+
+DTYPE_F32 = 0
+DTYPE_C64 = 1
+
+INIT_RND, INIT_RND_FIXED, INIT_UP, INIT_DOWN = 0, 1, 2, 3
+RULE_LOCAL, RULE_EXCHANGE = 0, 1
+MOVE_FLIP1, MOVE_PAIR_ANTI, MOVE_PAIR_PAR = 0, 1, 2
+
+_vp = C.c_void_p
+_i32 = C.c_int32
+_i64 = C.c_int64
+_u64 = C.c_uint64
+_sz = C.c_size_t
+
+
+class QESError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"qes status {code}: {msg}")
+        self.code = code
+
+
+class SamplerConfig(C.Structure):
+    _fields_ = [
+        ("rule", C.c_int), ("ns", C.c_int), ("nh", C.c_int), ("n_chains", C.c_int),
+        ("chain_offset", _i64), ("num_samples", C.c_int), ("therm_steps_total", _i64),
+        ("sweep_steps", C.c_int), ("recompute_every", C.c_int), ("mu", C.c_float), ("beta", C.c_float),
+        ("seed", _u64), ("deg", C.c_int),
+    ]
+
+
+class Hamiltonian(C.Structure):
+    _fields_ = [
+        ("n_moves", C.c_int), ("move_i", _vp), ("move_j", _vp), ("move_kind", _vp), ("move_coef", _vp),
+        ("n_zfield", C.c_int), ("zf_site", _vp), ("zf_h", _vp),
+        ("n_zz", C.c_int), ("zz_i", _vp), ("zz_j", _vp), ("zz_J", _vp),
+    ]
+
+
+class SROptions(C.Structure):
+    _fields_ = [
+        ("shift", C.c_double), ("rtol", C.c_double), ("atol", C.c_double), ("maxiter", C.c_int),
+        ("check_every", C.c_int), ("rhs_prefactor", C.c_double),
+    ]
+
+
+class SRResult(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double), ("rhs_norm", C.c_double),
+        ("e_mean_re", C.c_double), ("e_mean_im", C.c_double),
+    ]
+
+
+# name -> argtypes ; every symbol declared in include/qes_b200.h
+SIGNATURES = {
+    "qes_last_error": [],
+    "qes_version": [],
+    "qes_init_chains": [C.c_int, C.c_int, _u64, _i64, C.c_int, C.c_int, _vp, _vp],
+    "qes_rbm_move_tables": [C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp],
+    "qes_rbm_forward": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "qes_sampler_run": [C.c_int, C.POINTER(SamplerConfig), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int,
+                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "qes_local_energy_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.c_int, C.POINTER(_sz)],
+    "qes_local_energy": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.POINTER(Hamiltonian), _vp, _vp, _vp, _vp,
+                         _sz, _vp, _vp],
+    "qes_loss_stats_workspace_bytes": [_i64, C.POINTER(_sz)],
+    "qes_loss_stats": [_i64, _vp, _vp, _vp, _vp, _sz, _vp],
+    "qes_rbm_log_derivatives": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _i64, _vp],
+    "qes_sr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
+    "qes_sr_force": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
+    "qes_sr_matvec": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.c_double, _vp, _vp, _vp, _sz, _vp],
+    "qes_sr_solve_cg": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
+                        C.POINTER(SRResult), _vp, _sz, _vp],
+    "qes_rbm_logpsi_vjp": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
+    "qes_param_update": [C.c_int, _i64, C.c_double, _vp, _vp, _vp, _vp],
+}
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library once; raises OSError when it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: build it with `python -m pyqusolver_b200.build`")
+    lib = C.CDLL(path)
+    for name, argt in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argt
+        fn.restype = C.c_char_p if name == "qes_last_error" else C.c_int
+    _LIB = lib
+    return lib
+
+
+def check(code: int):
+    if code != QES_OK:
+        msg = _LIB.qes_last_error().decode() if _LIB is not None else "?"
+        raise QESError(code, msg)
+    return code
+
+
+def call(name, *args, allow=()):
+    rc = getattr(load(), name)(*args)
+    if rc != QES_OK and rc not in allow:
+        check(rc)
+    return rc
+
+
+def ptr(t):
+    """Device pointer of a torch tensor (None -> NULL)."""
+    return None if t is None else _vp(t.data_ptr())
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return _vp(s.cuda_stream)

@@ -1,0 +1,269 @@
+// Persistent Metropolis sampler: one warp per chain.
+//
+// Chain state: packed spins in shared memory; theta and tanh(theta) of the
+// chain live in registers, lane l owning hidden units m = l + 32 r (r < MPL).
+// A proposal costs one Philox call, O(M/32) complex FMAs per lane against the
+// move's cosh/sinh table row, a per-lane log and one warp sum -- the
+// reference instead re-evaluates the whole network for every exchange
+// proposal (vmc.py:1050-1054).  An accepted move updates theta by the rank-1
+// (flip) or rank-2 (exchange) column of W; theta is recomputed from the spins
+// every `recompute_every` proposals to bound float32 drift.
+//
+// Reference semantics kept (vmc.py:1016-1097, spin_jax.py:51-158):
+//   log_acc = min(beta*mu*Re dlogpsi, 0); accept iff log u < log_acc;
+//   exchange with an invalid slot or equal spins is a no-op with dlogpsi = 0,
+//   accepted (u < 1); proposed += 1 and accepted += keep for every proposal.
+#include "common.cuh"
+
+#define QES_ARG_CHECK(cond, msg) do { if (!(cond)) { qes_set_last_message(msg); return QES_ERR_ARG; } } while (0)
+
+constexpr int SMP_WARPS = 4;        // chains per block
+constexpr int SMP_MAX_WORDS = 64;   // ns <= 2048
+
+template <class T>
+QES_D float log_abs(T v);
+template <>
+QES_D float log_abs<float>(float v) { return logf(fabsf(v)); }
+template <>
+QES_D float log_abs<float2>(float2 v) { return 0.5f * logf(v.x * v.x + v.y * v.y); }
+
+template <class T, int MPL>
+QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ b,
+                      const T* __restrict__ W, T (&th)[MPL], T (&tn)[MPL]) {
+#pragma unroll
+  for (int r = 0; r < MPL; ++r) {
+    const int m = lane + 32 * r;
+    th[r] = (m < nh) ? b[m] : ScalarTraits<T>::zero();
+  }
+  for (int i = 0; i < ns; ++i) {
+    const float sg = ((cfg[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
+    const T* wr = W + (int64_t)i * nh;
+#pragma unroll
+    for (int r = 0; r < MPL; ++r) {
+      const int m = lane + 32 * r;
+      if (m < nh) th[r] = addx(th[r], scal(sg, wr[m]));
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < MPL; ++r) tn[r] = tanhx(th[r]);
+}
+
+template <class T, int MPL>
+QES_D T chain_logpsi(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ a, const T (&th)[MPL]) {
+  T s = ScalarTraits<T>::zero();
+#pragma unroll
+  for (int r = 0; r < MPL; ++r) {
+    const int m = lane + 32 * r;
+    if (m < nh) s = addx(s, log_cosh(th[r]));
+  }
+  for (int i = lane; i < ns; i += 32) {
+    const float sg = ((cfg[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
+    s = addx(s, scal(sg, a[i]));
+  }
+  return warp_sum(s);
+}
+
+template <class T, int MPL, int RULE>
+__global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
+    qes_sampler_config cfg, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ W,
+    const T* __restrict__ flipC, const T* __restrict__ flipS, const int32_t* __restrict__ nbr,
+    const int32_t* __restrict__ nbr_pair, const int32_t* __restrict__ pair_i, const int32_t* __restrict__ pair_j,
+    const T* __restrict__ pairC, const T* __restrict__ pairS, uint32_t* __restrict__ chain_bits,
+    uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed, int32_t* __restrict__ accepted,
+    uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
+  __shared__ uint32_t cfg_sm[SMP_WARPS][SMP_MAX_WORDS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int chain = blockIdx.x * SMP_WARPS + wid;
+  if (chain >= cfg.n_chains) return;            // whole warp leaves together
+  const int ns = cfg.ns, nh = cfg.nh, nw = n_words(ns);
+  uint32_t* cw = cfg_sm[wid];
+  for (int q = lane; q < nw; q += 32) cw[q] = chain_bits[(int64_t)chain * nw + q];
+  __syncwarp();
+
+  const uint32_t k0 = (uint32_t)(cfg.seed & 0xffffffffu), k1 = (uint32_t)(cfg.seed >> 32);
+  const uint32_t cid = (uint32_t)(cfg.chain_offset + chain);
+  uint64_t step = chain_step[chain];
+  int32_t n_prop = proposed[chain], n_acc = accepted[chain];
+  const int recompute = cfg.recompute_every > 0 ? cfg.recompute_every : ns;
+  const float bm = cfg.beta * cfg.mu;
+
+  T th[MPL], tn[MPL];
+  full_theta<T, MPL>(ns, nh, lane, cw, b, W, th, tn);
+  int since = 0;
+
+  const int64_t total = cfg.therm_steps_total + (int64_t)cfg.num_samples * cfg.sweep_steps;
+  int64_t rec = 0;
+  int64_t next_record = cfg.therm_steps_total + cfg.sweep_steps;
+
+  for (int64_t it = 0; it < total; ++it) {
+    const Philox4 r = philox4x32_10(cid, (uint32_t)step, (uint32_t)(step >> 32), QES_STREAM_PROPOSAL, k0, k1);
+    const int i = (int)bounded_u32(r.x, (uint32_t)ns);
+    bool moved;
+    int i0 = i, j0 = -1;        // sites flipped (j0 = -1 for a single flip)
+    const T* Crow;
+    const T* Srow;
+    if (RULE == QES_RULE_LOCAL) {
+      moved = true;
+      Crow = flipC + (int64_t)i * nh;
+      Srow = flipS + (int64_t)i * nh;
+    } else {
+      const int kk = (int)bounded_u32(r.y, (uint32_t)cfg.deg);
+      const int j = nbr[i * cfg.deg + kk];
+      moved = false;
+      Crow = flipC; Srow = flipS;
+      if (j >= 0) {
+        const uint32_t bi = (cw[i >> 5] >> (i & 31)) & 1u;
+        const uint32_t bj = (cw[j >> 5] >> (j & 31)) & 1u;
+        if (bi != bj) {
+          const int p = nbr_pair[i * cfg.deg + kk];
+          moved = true;
+          i0 = pair_i[p]; j0 = pair_j[p];
+          Crow = pairC + (int64_t)p * nh;
+          Srow = pairS + (int64_t)p * nh;
+        }
+      }
+    }
+    float re_delta = 0.f;
+    float g = 0.f;
+    if (moved) {
+      g = ((cw[i0 >> 5] >> (i0 & 31)) & 1u) ? -1.f : 1.f;      // -sigma_i0
+      T prod = ScalarTraits<T>::one();
+      int ex = 0;
+#pragma unroll
+      for (int rr = 0; rr < MPL; ++rr) {
+        const int m = lane + 32 * rr;
+        if (m < nh) prod = mulx(prod, ratio_factor(Crow[m], g, tn[rr], Srow[m]));
+        if ((rr & 7) == 7) renorm(prod, ex);
+      }
+      float la = log_abs<T>(prod) + 0.69314718055994531f * (float)ex;
+      la = warp_sum(la);
+      T av = a[i0];
+      if (j0 >= 0) av = addx(av, scal(-1.f, a[j0]));
+      re_delta = la + 2.f * g * to_re(av);
+    }
+    const float log_acc = fminf(bm * re_delta, 0.f);
+    const bool keep = logf(uniform_open(r.z)) < log_acc;
+    if (keep && moved) {
+      const T* wi = W + (int64_t)i0 * nh;
+      const T* wj = W + (int64_t)(j0 >= 0 ? j0 : i0) * nh;
+#pragma unroll
+      for (int rr = 0; rr < MPL; ++rr) {
+        const int m = lane + 32 * rr;
+        if (m < nh) {
+          T d = wi[m];
+          if (j0 >= 0) d = addx(d, scal(-1.f, wj[m]));
+          th[rr] = addx(th[rr], scal(2.f * g, d));
+          tn[rr] = tanhx(th[rr]);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        cw[i0 >> 5] ^= 1u << (i0 & 31);
+        if (j0 >= 0) cw[j0 >> 5] ^= 1u << (j0 & 31);
+      }
+      __syncwarp();
+    }
+    n_prop += 1;
+    n_acc += keep ? 1 : 0;
+    ++step;
+    if (++since >= recompute) {
+      full_theta<T, MPL>(ns, nh, lane, cw, b, W, th, tn);
+      since = 0;
+    }
+    if (it + 1 == next_record) {
+      const int64_t row = rec * cfg.n_chains + chain;
+      for (int q = lane; q < nw; q += 32) sample_bits[row * nw + q] = cw[q];
+      const T lp = chain_logpsi<T, MPL>(ns, nh, lane, cw, a, th);
+      if (lane == 0 && sample_logpsi) sample_logpsi[row] = lp;
+      ++rec;
+      next_record += cfg.sweep_steps;
+    }
+  }
+  for (int q = lane; q < nw; q += 32) chain_bits[(int64_t)chain * nw + q] = cw[q];
+  const T lp = chain_logpsi<T, MPL>(ns, nh, lane, cw, a, th);
+  if (lane == 0) {
+    chain_step[chain] = step;
+    proposed[chain] = n_prop;
+    accepted[chain] = n_acc;
+    if (last_logpsi) last_logpsi[chain] = lp;
+  }
+}
+
+template <class T, int MPL>
+static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, const void* b, const void* W,
+                              const void* flipC, const void* flipS, const int32_t* nbr, const int32_t* nbr_pair,
+                              const int32_t* pi, const int32_t* pj, const void* pairC, const void* pairS,
+                              uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
+                              uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi, cudaStream_t st) {
+  const unsigned grid = (unsigned)((cfg->n_chains + SMP_WARPS - 1) / SMP_WARPS);
+  if (cfg->rule == QES_RULE_LOCAL)
+    sampler_kernel<T, MPL, QES_RULE_LOCAL><<<grid, 32 * SMP_WARPS, 0, st>>>(
+        *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
+        (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
+        (T*)sample_logpsi, (T*)last_logpsi);
+  else
+    sampler_kernel<T, MPL, QES_RULE_EXCHANGE><<<grid, 32 * SMP_WARPS, 0, st>>>(
+        *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
+        (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
+        (T*)sample_logpsi, (T*)last_logpsi);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+template <class T>
+static int launch_sampler(int mpl_needed, int mpl_max, const qes_sampler_config* cfg, const void* a, const void* b,
+                          const void* W, const void* flipC, const void* flipS, const int32_t* nbr,
+                          const int32_t* nbr_pair, const int32_t* pi, const int32_t* pj, const void* pairC,
+                          const void* pairS, uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed,
+                          int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
+                          cudaStream_t st) {
+#define QES_SMP_CASE(M)                                                                                          \
+  if (mpl_needed <= M && M <= mpl_max)                                                                           \
+    return launch_sampler_mpl<T, M>(cfg, a, b, W, flipC, flipS, nbr, nbr_pair, pi, pj, pairC, pairS, chain_bits, \
+                                    chain_step, proposed, accepted, sample_bits, sample_logpsi, last_logpsi, st);
+  QES_SMP_CASE(1)
+  QES_SMP_CASE(2)
+  QES_SMP_CASE(4)
+  QES_SMP_CASE(8)
+  QES_SMP_CASE(16)
+  if constexpr (!ScalarTraits<T>::is_complex) {
+    QES_SMP_CASE(32)
+    QES_SMP_CASE(64)
+  }
+#undef QES_SMP_CASE
+  qes_set_last_message("qes_sampler_run: too many hidden units for the register-resident theta cache");
+  return QES_ERR_SIZE;
+}
+
+extern "C" int qes_sampler_run(int dtype, const qes_sampler_config* cfg, const void* a, const void* b,
+                               const void* W, const void* flipCt, const void* flipSt, const int32_t* nbr_table,
+                               const int32_t* nbr_pair, const int32_t* pair_i, const int32_t* pair_j, int n_pairs,
+                               const void* pairCt, const void* pairSt, uint32_t* chain_bits, uint64_t* chain_step,
+                               int32_t* proposed, int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi,
+                               void* last_logpsi, void* stream) {
+  QES_ARG_CHECK(cfg != nullptr, "qes_sampler_run: null config");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sampler_run: bad dtype");
+  QES_ARG_CHECK(cfg->ns > 0 && cfg->nh > 0 && cfg->n_chains >= 0 && cfg->num_samples >= 0, "qes_sampler_run: bad sizes");
+  QES_ARG_CHECK(cfg->therm_steps_total >= 0 && cfg->sweep_steps >= 1, "qes_sampler_run: bad schedule");
+  QES_ARG_CHECK(n_words(cfg->ns) <= SMP_MAX_WORDS, "qes_sampler_run: ns > 2048");
+  QES_ARG_CHECK(a && b && W && chain_bits && chain_step && proposed && accepted, "qes_sampler_run: null pointer");
+  QES_ARG_CHECK(cfg->num_samples == 0 || sample_bits, "qes_sampler_run: null sample buffer");
+  if (cfg->rule == QES_RULE_LOCAL) {
+    QES_ARG_CHECK(flipCt && flipSt, "qes_sampler_run: LOCAL needs flip tables");
+  } else if (cfg->rule == QES_RULE_EXCHANGE) {
+    QES_ARG_CHECK(cfg->deg > 0 && nbr_table && nbr_pair && pair_i && pair_j && pairCt && pairSt && n_pairs > 0,
+                  "qes_sampler_run: EXCHANGE needs neighbour and pair tables");
+  } else {
+    QES_ARG_CHECK(false, "qes_sampler_run: unknown rule");
+  }
+  if (cfg->n_chains == 0) return QES_OK;
+  const int mpl = (cfg->nh + 31) / 32;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return launch_sampler<float>(mpl, 64, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j, pairCt,
+                                 pairSt, chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi,
+                                 last_logpsi, st);
+  return launch_sampler<float2>(mpl, 16, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j, pairCt,
+                                pairSt, chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi,
+                                last_logpsi, st);
+}

@@ -1,0 +1,601 @@
+// Stochastic reconfiguration with the RBM's structured log-derivatives.
+//
+// For the RBM, O_s = [sigma_s, t_s, sigma_s (x) t_s] with t = tanh(theta), so
+//   (O v)_s    = sigma_s . v_a + t_s . (v_b + V^T sigma_s)        (V = v_W, ns x nh)
+//   (O^H u)_W  = Sigma^T diag(u) conj(T),  (O^H u)_a = Sigma^T u,  (O^H u)_b = T^H u
+// and the SR matrix is applied as S v = O_c^H O_c v / Ns = O^H (w - mean w) / Ns
+// with w = O v (the centred u sums to zero, so O^H u = O_c^H u).  O (Ns x P)
+// is never formed: one matvec reads the packed spins and T (Ns x nh) only.
+//
+// Precision: per-chunk sums in float32, chunk partials and every CG vector,
+// dot product and scalar in float64 (the reference promotes SR data to
+// float64, tdvp.py:827-858).  CG follows SciPy's rule ||r|| <= max(rtol*||b||,
+// atol); the device freezes x at the first iteration that meets it, so the
+// result does not depend on how often the host checks.
+#include "common.cuh"
+
+#include <algorithm>
+
+#define QES_ARG_CHECK(cond, msg) do { if (!(cond)) { qes_set_last_message(msg); return QES_ERR_ARG; } } while (0)
+
+template <class T> struct VecT;
+template <> struct VecT<float> { using type = double; };
+template <> struct VecT<float2> { using type = double2; };
+
+QES_HD double vzero(double) { return 0.0; }
+QES_HD double2 vzero(double2) { return make_double2(0.0, 0.0); }
+QES_D float to_f(double v) { return (float)v; }
+QES_D float2 to_f(double2 v) { return make_float2((float)v.x, (float)v.y); }
+QES_D double to_d(float v) { return (double)v; }
+QES_D double2 to_d(float2 v) { return make_double2(v.x, v.y); }
+QES_D double vadd(double a, double b) { return a + b; }
+QES_D double2 vadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+QES_D double vscale(double s, double a) { return s * a; }
+QES_D double2 vscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+QES_D double2 vscale(double2 s, double2 a) { return make_double2(s.x * a.x - s.y * a.y, s.x * a.y + s.y * a.x); }
+QES_D double vdotc(double a, double b) { return a * b; }                       // conj(a) b, real part only
+QES_D double vdotc(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }     // Re(conj(a) b)
+// element from the complex eloc / w buffer in the working scalar type
+QES_D float from_c(float2 v, float) { return v.x; }
+QES_D float2 from_c(float2 v, float2) { return v; }
+
+// ----------------------------------------------------------------------------
+// (O v)_s : theta-like pass with V in place of W, fused with the dot with t_s
+// ----------------------------------------------------------------------------
+constexpr int OV_SB = 16;
+constexpr int OV_THREADS = 256;
+
+template <class T, class V>
+__global__ void __launch_bounds__(OV_THREADS) ov_kernel(int ns, int nh, int64_t n_samples,
+                                                        const uint32_t* __restrict__ bits,
+                                                        const T* __restrict__ tanh_theta, const V* __restrict__ v,
+                                                        float2* __restrict__ w_out) {
+  extern __shared__ uint32_t smw[];
+  const int nw = n_words(ns);
+  const int64_t s0 = (int64_t)blockIdx.x * OV_SB;
+  const int nsb = (int)min((int64_t)OV_SB, n_samples - s0);
+  for (int q = threadIdx.x; q < OV_SB * nw; q += blockDim.x) {
+    const int sl = q / nw;
+    smw[q] = (sl < nsb) ? bits[(s0 + sl) * nw + (q % nw)] : 0u;
+  }
+  __syncthreads();
+  const V* va = v;
+  const V* vb = v + ns;
+  const V* vW = v + ns + nh;
+  T part[OV_SB];
+#pragma unroll
+  for (int q = 0; q < OV_SB; ++q) part[q] = ScalarTraits<T>::zero();
+  for (int m = threadIdx.x; m < nh; m += blockDim.x) {
+    const T bm = to_f(vb[m]);
+    T z[OV_SB];
+#pragma unroll
+    for (int q = 0; q < OV_SB; ++q) z[q] = bm;
+    for (int i = 0; i < ns; ++i) {
+      const T x = to_f(vW[(int64_t)i * nh + m]);
+#pragma unroll
+      for (int q = 0; q < OV_SB; ++q) {
+        const uint32_t bit = (smw[q * nw + (i >> 5)] >> (i & 31)) & 1u;
+        z[q] = addx(z[q], bit ? x : scal(-1.f, x));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < OV_SB; ++q)
+      if (q < nsb) part[q] = addx(part[q], mulx(tanh_theta[(s0 + q) * nh + m], z[q]));
+  }
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+    const T x = to_f(va[i]);
+#pragma unroll
+    for (int q = 0; q < OV_SB; ++q) {
+      const uint32_t bit = (smw[q * nw + (i >> 5)] >> (i & 31)) & 1u;
+      part[q] = addx(part[q], bit ? x : scal(-1.f, x));
+    }
+  }
+  __shared__ T red[OV_THREADS / 32][OV_SB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < OV_SB; ++q) {
+    T s = warp_sum(part[q]);
+    if (lane == 0) red[warp][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < nsb) {
+    T s = ScalarTraits<T>::zero();
+    for (int w = 0; w < OV_THREADS / 32; ++w) s = addx(s, red[w][threadIdx.x]);
+    w_out[s0 + threadIdx.x] = to_c(s);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// mean of a complex float32 vector in float64 -> out[0..1]  (one block)
+// ----------------------------------------------------------------------------
+constexpr int MEAN_THREADS = 1024;
+__global__ void __launch_bounds__(MEAN_THREADS) mean_c_kernel(int64_t n, const float2* __restrict__ w,
+                                                              double* __restrict__ out) {
+  double sr = 0, si = 0;
+  for (int64_t k = threadIdx.x; k < n; k += blockDim.x) { sr += w[k].x; si += w[k].y; }
+  __shared__ double rr[MEAN_THREADS / 32], ri[MEAN_THREADS / 32];
+  sr = warp_sum(sr); si = warp_sum(si);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) { rr[warp] = sr; ri[warp] = si; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int q = 0; q < MEAN_THREADS / 32; ++q) { a += rr[q]; b += ri[q]; }
+    out[0] = a / (double)n;
+    out[1] = b / (double)n;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// O^H u with u_s = (w_s - mean) * scale.   Block: 64 hidden units (tx) x
+// 4 rows of 4 sites (ty) over one split of the samples; 32-sample sub-chunks
+// of Q_sm = conj(t_sm) u_s and of the spin words are staged in shared memory.
+// ----------------------------------------------------------------------------
+constexpr int OHU_TM = 64;
+constexpr int OHU_TY = 4;
+constexpr int OHU_SPT = 4;                       // sites per thread
+constexpr int OHU_TI = OHU_TY * OHU_SPT;         // 16 sites per block
+constexpr int OHU_SC = 32;                       // samples per staged sub-chunk
+constexpr int OHU_SPLIT_SAMPLES = 256;           // samples per split
+
+template <class T>
+__global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
+    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ tanh_theta,
+    const float2* __restrict__ w, const double* __restrict__ wmean, double scale, T* __restrict__ partial) {
+  __shared__ T Q[OHU_SC][OHU_TM];
+  __shared__ T U[OHU_SC];
+  __shared__ uint32_t SW[OHU_SC][2];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * OHU_TM + tx;
+  const int m0 = blockIdx.x * OHU_TM, i0 = blockIdx.y * OHU_TI;
+  const int m = m0 + tx;
+  const int64_t sbeg = (int64_t)blockIdx.z * OHU_SPLIT_SAMPLES;
+  const int64_t send = min(n_samples, sbeg + OHU_SPLIT_SAMPLES);
+  const int nw = n_words(ns);
+  const int wlo = i0 >> 5;
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  const float mr = wmean ? (float)wmean[0] : 0.f, mi = wmean ? (float)wmean[1] : 0.f;
+  const float fs = (float)scale;
+
+  T acc[OHU_SPT], accb = ScalarTraits<T>::zero(), acca[OHU_SPT];
+#pragma unroll
+  for (int k = 0; k < OHU_SPT; ++k) { acc[k] = ScalarTraits<T>::zero(); acca[k] = ScalarTraits<T>::zero(); }
+
+  for (int64_t c0 = sbeg; c0 < send; c0 += OHU_SC) {
+    const int nc = (int)min((int64_t)OHU_SC, send - c0);
+    if (tid < OHU_SC) {
+      T u = ScalarTraits<T>::zero();
+      if (tid < nc) {
+        const float2 wv = w[c0 + tid];
+        u = from_c(make_float2((wv.x - mr) * fs, (wv.y - mi) * fs), T());
+      }
+      U[tid] = u;
+      SW[tid][0] = (tid < nc) ? bits[(c0 + tid) * nw + wlo] : 0u;
+      SW[tid][1] = (tid < nc && wlo + 1 < nw) ? bits[(c0 + tid) * nw + wlo + 1] : 0u;
+    }
+    __syncthreads();
+    for (int e = tid; e < OHU_SC * OHU_TM; e += OHU_TM * OHU_TY) {
+      const int sl = e / OHU_TM, ml = e % OHU_TM;
+      T q = ScalarTraits<T>::zero();
+      if (sl < nc && m0 + ml < nh) q = mulx(conjx(tanh_theta[(c0 + sl) * nh + m0 + ml]), U[sl]);
+      Q[sl][ml] = q;
+    }
+    __syncthreads();
+    for (int sl = 0; sl < nc; ++sl) {
+      const T q = Q[sl][tx];
+      const uint64_t wd = ((uint64_t)SW[sl][1] << 32) | SW[sl][0];
+#pragma unroll
+      for (int k = 0; k < OHU_SPT; ++k) {
+        const int il = ty * OHU_SPT + k + (i0 & 31);
+        const bool up = (wd >> il) & 1ull;
+        acc[k] = addx(acc[k], up ? q : scal(-1.f, q));
+      }
+      if (blockIdx.y == 0 && ty == 0) accb = addx(accb, q);
+      if (blockIdx.x == 0 && tx == 0) {
+        const T u = U[sl];
+#pragma unroll
+        for (int k = 0; k < OHU_SPT; ++k) {
+          const int il = ty * OHU_SPT + k + (i0 & 31);
+          const bool up = (wd >> il) & 1ull;
+          acca[k] = addx(acca[k], up ? u : scal(-1.f, u));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  T* out = partial + (int64_t)blockIdx.z * P;
+  if (m < nh) {
+#pragma unroll
+    for (int k = 0; k < OHU_SPT; ++k) {
+      const int i = i0 + ty * OHU_SPT + k;
+      if (i < ns) out[ns + nh + (int64_t)i * nh + m] = acc[k];
+    }
+    if (blockIdx.y == 0 && ty == 0) out[ns + m] = accb;
+  }
+  if (blockIdx.x == 0 && tx == 0) {
+#pragma unroll
+    for (int k = 0; k < OHU_SPT; ++k) {
+      const int i = i0 + ty * OHU_SPT + k;
+      if (i < ns) out[i] = acca[k];
+    }
+  }
+}
+
+// sum the split partials in float64; optional  y = G + shift * p  and  dot partials of p^H y
+constexpr int RED_THREADS = 256;
+constexpr int RED_BLOCKS = 296;
+
+template <class T, class V>
+__global__ void __launch_bounds__(RED_THREADS) reduce_splits_kernel(int64_t P, int nsplit, const T* __restrict__ partial,
+                                                                    double shift, const V* __restrict__ p,
+                                                                    V* __restrict__ y, double* __restrict__ dot_part) {
+  double d = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    V g = vzero(V());
+    for (int z = 0; z < nsplit; ++z) g = vadd(g, to_d(partial[(int64_t)z * P + k]));
+    if (p) {
+      const V pk = p[k];
+      g = vadd(g, vscale(shift, pk));
+      d += vdotc(pk, g);
+    }
+    y[k] = g;
+  }
+  if (dot_part) {
+    __shared__ double red[RED_THREADS / 32];
+    d = warp_sum(d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0;
+      for (int q = 0; q < RED_THREADS / 32; ++q) s += red[q];
+      dot_part[blockIdx.x] = s;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// CG state on the device: scal[0] = rr, [1] = pAp, [2] = rr_new, [3] = thresh^2,
+// [4] = done flag, [5] = iterations (as double), [6] = ||b||^2
+// ----------------------------------------------------------------------------
+__global__ void sum_parts_kernel(int n, const double* __restrict__ parts, double* __restrict__ dst) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0;
+  for (int q = 0; q < n; ++q) s += parts[q];
+  *dst = s;
+}
+
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* __restrict__ p, const V* __restrict__ Ap,
+                                                            V* __restrict__ x, V* __restrict__ r,
+                                                            const double* __restrict__ scal, double* __restrict__ rr_part) {
+  const bool done = scal[4] != 0.0;
+  const double pap = scal[1];
+  const double alpha = (pap > 0.0 && !done) ? scal[0] / pap : 0.0;
+  double d = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    V rk = r[k];
+    if (!done) {
+      x[k] = vadd(x[k], vscale(alpha, p[k]));
+      rk = vadd(rk, vscale(-alpha, Ap[k]));
+      r[k] = rk;
+    }
+    d += vdotc(rk, rk);
+  }
+  __shared__ double red[RED_THREADS / 32];
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) s += red[q];
+    rr_part[blockIdx.x] = s;
+  }
+}
+
+// rr_new = sum parts; convergence test; beta; iteration count
+__global__ void cg_scalar_kernel(int n, const double* __restrict__ parts, double* __restrict__ scal) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (scal[4] != 0.0) return;
+  double s = 0;
+  for (int q = 0; q < n; ++q) s += parts[q];
+  scal[2] = s;
+  scal[5] += 1.0;
+  if (s <= scal[3]) scal[4] = 1.0;
+}
+
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) cg_p_kernel(int64_t P, const V* __restrict__ r, V* __restrict__ p,
+                                                           double* __restrict__ scal, int last_block_updates) {
+  const bool done = scal[4] != 0.0;
+  const double beta = (scal[0] > 0.0) ? scal[2] / scal[0] : 0.0;
+  if (!done) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x)
+      p[k] = vadd(r[k], vscale(beta, p[k]));
+  }
+  (void)last_block_updates;
+}
+
+__global__ void cg_rotate_kernel(double* __restrict__ scal) {
+  if (threadIdx.x == 0 && blockIdx.x == 0 && scal[4] == 0.0) scal[0] = scal[2];
+}
+
+// x = 0, r = p = b, scal init
+template <class V>
+__global__ void cg_init_kernel(int64_t P, const V* __restrict__ b, V* __restrict__ x, V* __restrict__ r,
+                               V* __restrict__ p) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    x[k] = vzero(V());
+    r[k] = b[k];
+    p[k] = b[k];
+  }
+}
+
+__global__ void cg_setup_kernel(int n, const double* __restrict__ parts, double rtol, double atol,
+                                double* __restrict__ scal) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0;
+  for (int q = 0; q < n; ++q) s += parts[q];
+  scal[0] = s;                      // rr = ||b||^2
+  scal[6] = s;
+  const double th = fmax(rtol * sqrt(s), atol);
+  scal[3] = th * th;
+  scal[5] = 0.0;
+  scal[4] = (s <= scal[3]) ? 1.0 : 0.0;
+  scal[1] = 0.0;
+  scal[2] = s;
+}
+
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) norm2_kernel(int64_t P, const V* __restrict__ b, double* __restrict__ part) {
+  double d = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x)
+    d += vdotc(b[k], b[k]);
+  __shared__ double red[RED_THREADS / 32];
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) s += red[q];
+    part[blockIdx.x] = s;
+  }
+}
+
+template <class V>
+__global__ void scale_vec_kernel(int64_t P, double s, V* __restrict__ x) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x)
+    x[k] = vscale(s, x[k]);
+}
+
+// ----------------------------------------------------------------------------
+// workspace layout
+// ----------------------------------------------------------------------------
+struct SRWork {
+  float2* w;          // [Ns]
+  double* wmean;      // [2] (+ pad)
+  void* partial;      // [nsplit][P] of T
+  void* x; void* r; void* p; void* Ap; void* b;   // [P] of V each
+  double* parts;      // [RED_BLOCKS]
+  double* scal;       // [8]
+  size_t total;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base) {
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  const size_t ts = (dtype == QES_DTYPE_C64) ? sizeof(float2) : sizeof(float);
+  const size_t vs = (dtype == QES_DTYPE_C64) ? sizeof(double2) : sizeof(double);
+  const int64_t nsplit = (n_samples + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES;
+  SRWork L;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off += align256(bytes); return p; };
+  L.w = (float2*)take((size_t)n_samples * sizeof(float2));
+  L.wmean = (double*)take(4 * sizeof(double));
+  L.partial = take((size_t)std::max<int64_t>(nsplit, 1) * P * ts);
+  L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
+  L.parts = (double*)take(RED_BLOCKS * sizeof(double));
+  L.scal = (double*)take(8 * sizeof(double));
+  L.total = off;
+  return L;
+}
+
+extern "C" int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes) {
+  QES_ARG_CHECK(bytes && ns > 0 && nh > 0 && n_samples >= 0, "qes_sr_workspace_bytes: bad args");
+  *bytes = sr_layout(dtype, ns, nh, n_samples, nullptr).total;
+  return QES_OK;
+}
+
+// g = O^H ((w - mean(w)) * scale)   [+ shift * p, dot partials]   into y
+template <class T, class V>
+static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
+                     const double* wmean, double scale, const SRWork& L, double shift, const V* p, V* y,
+                     double* dot_part, cudaStream_t st) {
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  const int64_t nsplit = (n_samples + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES;
+  QES_ARG_CHECK(nsplit <= 65535, "SR: too many samples");
+  dim3 grid((nh + OHU_TM - 1) / OHU_TM, (ns + OHU_TI - 1) / OHU_TI, (unsigned)nsplit);
+  dim3 block(OHU_TM, OHU_TY);
+  ohu_kernel<T><<<grid, block, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial);
+  QES_LAUNCH_CHECK();
+  reduce_splits_kernel<T, V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, (int)nsplit, (const T*)L.partial, shift, p, y,
+                                                                 dot_part);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+template <class T, class V>
+static int apply_ov(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const V* v, float2* w,
+                    double* wmean, cudaStream_t st) {
+  const int nw = n_words(ns);
+  const size_t sm = (size_t)OV_SB * nw * sizeof(uint32_t);
+  QES_ARG_CHECK(sm <= 48 * 1024, "SR: ns too large");
+  ov_kernel<T, V><<<(unsigned)((n_samples + OV_SB - 1) / OV_SB), OV_THREADS, sm, st>>>(ns, nh, n_samples, bits, tt,
+                                                                                     v, w);
+  QES_LAUNCH_CHECK();
+  mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, w, wmean);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+template <class T>
+static int sr_force_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* eloc,
+                      typename VecT<T>::type* F, const SRWork& L, cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, eloc, L.wmean);
+  QES_LAUNCH_CHECK();
+  return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, eloc, L.wmean, 1.0 / (double)n_samples, L, 0.0, nullptr, F,
+                         nullptr, st);
+}
+
+static int check_ws(int dtype, int ns, int nh, int64_t n_samples, void* ws, size_t ws_bytes, SRWork* L) {
+  *L = sr_layout(dtype, ns, nh, n_samples, (char*)ws);
+  if (!ws || ws_bytes < L->total) {
+    qes_set_last_message("SR: workspace too small");
+    return QES_ERR_WORKSPACE;
+  }
+  return QES_OK;
+}
+
+extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                            const void* tanh_theta, const void* eloc, void* force_out, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && eloc && force_out, "qes_sr_force: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_force: bad dtype");
+  SRWork L;
+  int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return sr_force_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc,
+                             (double*)force_out, L, st);
+  return sr_force_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc,
+                            (double2*)force_out, L, st);
+}
+
+template <class T>
+static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, double shift,
+                       const typename VecT<T>::type* v, typename VecT<T>::type* y, double* dot_part, const SRWork& L,
+                       cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, st);
+  if (rc) return rc;
+  return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples, L, shift, v, y,
+                         dot_part, st);
+}
+
+extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                             const void* tanh_theta, double shift, const void* v, void* y_out, void* workspace,
+                             size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && v && y_out, "qes_sr_matvec: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_matvec: bad dtype");
+  SRWork L;
+  int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return sr_matvec_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, shift, (const double*)v,
+                              (double*)y_out, nullptr, L, st);
+  return sr_matvec_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, shift, (const double2*)v,
+                             (double2*)y_out, nullptr, L, st);
+}
+
+template <class T>
+static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* eloc,
+                   const qes_sr_options* opt, typename VecT<T>::type* x_out, qes_sr_result* res, const SRWork& L,
+                   cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  V* x = (V*)L.x; V* r = (V*)L.r; V* p = (V*)L.p; V* Ap = (V*)L.Ap; V* b = (V*)L.b;
+  // b = F
+  int rc = sr_force_t<T>(ns, nh, n_samples, bits, tt, eloc, b, L, st);
+  if (rc) return rc;
+  double emean[2] = {0, 0};
+  QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p);
+  norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
+  cg_setup_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
+  QES_LAUNCH_CHECK();
+  const int check = opt->check_every > 0 ? opt->check_every : 8;
+  double hs[8] = {0};
+  int it = 0;
+  bool done = false;
+  QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaStreamSynchronize(st));
+  done = hs[4] != 0.0;
+  while (!done && it < opt->maxiter) {
+    const int nrun = std::min(check, opt->maxiter - it);
+    for (int q = 0; q < nrun; ++q) {
+      rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, p, Ap, L.parts, L, st);
+      if (rc) return rc;
+      sum_parts_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, L.scal + 1);
+      cg_xr_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, p, Ap, x, r, L.scal, L.parts);
+      cg_scalar_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, L.scal);
+      cg_p_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, p, L.scal, 0);
+      cg_rotate_kernel<<<1, 32, 0, st>>>(L.scal);
+      QES_LAUNCH_CHECK();
+    }
+    it += nrun;
+    QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QES_CUDA_CHECK(cudaStreamSynchronize(st));
+    done = hs[4] != 0.0;
+  }
+  // x_out = rhs_prefactor * x
+  QES_CUDA_CHECK(cudaMemcpyAsync(x_out, x, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
+  if (opt->rhs_prefactor != 1.0) scale_vec_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, opt->rhs_prefactor, x_out);
+  QES_LAUNCH_CHECK();
+  if (res) {
+    res->iterations = (int)hs[5];
+    res->converged = done ? 1 : 0;
+    res->residual = sqrt(hs[4] != 0.0 ? hs[2] : hs[0]);
+    res->rhs_norm = sqrt(hs[6]);
+    res->e_mean_re = emean[0];
+    res->e_mean_im = emean[1];
+  }
+  return done ? QES_OK : QES_ERR_NOT_CONVERGED;
+}
+
+extern "C" int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                               const void* tanh_theta, const void* eloc, const qes_sr_options* opt, void* x_out,
+                               qes_sr_result* result, void* workspace, size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && eloc && opt && x_out,
+                "qes_sr_solve_cg: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_solve_cg: bad dtype");
+  QES_ARG_CHECK(opt->maxiter >= 0 && opt->shift >= 0.0, "qes_sr_solve_cg: bad options");
+  SRWork L;
+  int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return sr_cg_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc, opt,
+                          (double*)x_out, result, L, st);
+  return sr_cg_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc, opt,
+                         (double2*)x_out, result, L, st);
+}
+
+// ----------------------------------------------------------------------------
+// vector-Jacobian product of log psi:  grad = O^H g  (no centring, no 1/Ns)
+// ----------------------------------------------------------------------------
+template <class T>
+static int vjp_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* g,
+                 typename VecT<T>::type* out, const SRWork& L, cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, g, nullptr, 1.0, L, 0.0, nullptr, out, nullptr, st);
+}
+
+extern "C" int qes_rbm_logpsi_vjp(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                  const void* tanh_theta, const void* g, void* grad_out, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && g && grad_out,
+                "qes_rbm_logpsi_vjp: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_rbm_logpsi_vjp: bad dtype");
+  SRWork L;
+  int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return vjp_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)g, (double*)grad_out, L,
+                        st);
+  return vjp_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)g, (double2*)grad_out, L,
+                       st);
+}

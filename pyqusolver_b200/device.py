@@ -1,0 +1,262 @@
+"""Torch-tensor wrappers around the C ABI (one function per library entry point).
+
+Tensors are CUDA tensors owned by the caller; every call is enqueued on the
+current torch stream.  Packed spin words are stored in int32 tensors and
+reinterpreted as uint32 by the library.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptr, stream_ptr
+
+
+def _dev(device=None):
+    return torch.device("cuda") if device is None else torch.device(device)
+
+
+def dtype_code(t: torch.Tensor) -> int:
+    if t.dtype == torch.float32:
+        return _lib.DTYPE_F32
+    if t.dtype == torch.complex64:
+        return _lib.DTYPE_C64
+    raise TypeError(f"unsupported parameter dtype {t.dtype}")
+
+
+def n_words(ns: int) -> int:
+    return (ns + 31) // 32
+
+
+def n_params(ns: int, nh: int) -> int:
+    return ns + nh + ns * nh
+
+
+def split_params(flat: torch.Tensor, ns: int, nh: int):
+    a = flat[:ns]
+    b = flat[ns:ns + nh]
+    W = flat[ns + nh:].view(ns, nh)
+    return a, b, W
+
+
+# --------------------------------------------------------------------------------------
+# configurations
+# --------------------------------------------------------------------------------------
+
+def init_chains(kind: int, n_chains: int, ns: int, seed: int, n_up: int = 0, chain_offset: int = 0, device=None):
+    out = torch.empty((n_chains, n_words(ns)), dtype=torch.int32, device=_dev(device))
+    call("qes_init_chains", int(kind), int(n_up), C.c_uint64(int(seed) & (2 ** 64 - 1)), int(chain_offset),
+         int(n_chains), int(ns), ptr(out), stream_ptr())
+    return out
+
+
+def pack_states(states, device=None) -> torch.Tensor:
+    """(B, ns) array of +-0.5 / +-1 / {0,1} values (positive = up) -> packed int32 words on the device."""
+    s = states.detach().cpu().numpy() if isinstance(states, torch.Tensor) else np.asarray(states)
+    s = np.atleast_2d(s) > 0
+    B, ns = s.shape
+    nw = n_words(ns)
+    pad = np.zeros((B, nw * 32), dtype=bool)
+    pad[:, :ns] = s
+    words = np.packbits(pad.reshape(B, nw, 32), axis=2, bitorder="little").view(np.uint32).reshape(B, nw)
+    return torch.from_numpy(words.view(np.int32).copy()).to(_dev(device))
+
+
+def unpack_states(words: torch.Tensor, ns: int, value: float = 0.5) -> torch.Tensor:
+    """Packed int32 words (B, nw) -> float32 (B, ns) with entries +-value (on the same device)."""
+    nw = words.shape[-1]
+    shifts = torch.arange(32, device=words.device, dtype=torch.int32)
+    bits = (words.reshape(-1, nw, 1) >> shifts) & 1
+    bits = bits.reshape(-1, nw * 32)[:, :ns]
+    return (bits.to(torch.float32) * (2 * value) - value)
+
+
+# --------------------------------------------------------------------------------------
+# RBM
+# --------------------------------------------------------------------------------------
+
+def move_tables(flat_params, ns, nh, move_i, move_j, move_kind, move_major: bool):
+    K = int(move_i.shape[0])
+    a, b, W = split_params(flat_params, ns, nh)
+    shape = (K, nh) if move_major else (nh, K)
+    Ct = torch.empty(shape, dtype=flat_params.dtype, device=flat_params.device)
+    St = torch.empty_like(Ct)
+    A = torch.empty((K,), dtype=flat_params.dtype, device=flat_params.device)
+    if K:
+        call("qes_rbm_move_tables", dtype_code(flat_params), ns, nh, ptr(a), ptr(W), K, ptr(move_i), ptr(move_j),
+             ptr(move_kind), 1 if move_major else 0, ptr(Ct), ptr(St), ptr(A), stream_ptr())
+    return Ct, St, A
+
+
+def rbm_forward(flat_params, ns, nh, bits, theta=False, tanh=True, logpsi=True):
+    n = int(bits.shape[0])
+    a, b, W = split_params(flat_params, ns, nh)
+    dt, dev = flat_params.dtype, flat_params.device
+    th = torch.empty((n, nh), dtype=dt, device=dev) if theta else None
+    tn = torch.empty((n, nh), dtype=dt, device=dev) if tanh else None
+    lp = torch.empty((n,), dtype=dt, device=dev) if logpsi else None
+    call("qes_rbm_forward", dtype_code(flat_params), ns, nh, n, ptr(bits), ptr(a), ptr(b), ptr(W), ptr(th), ptr(tn),
+         ptr(lp), stream_ptr())
+    return th, tn, lp
+
+
+def log_derivatives(flat_params, ns, nh, bits, tanh_theta, out=None):
+    n = int(bits.shape[0])
+    P = n_params(ns, nh)
+    if out is None:
+        out = torch.empty((n, P), dtype=flat_params.dtype, device=flat_params.device)
+    call("qes_rbm_log_derivatives", dtype_code(flat_params), ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(out),
+         int(out.stride(0)), stream_ptr())
+    return out
+
+
+# --------------------------------------------------------------------------------------
+# Hamiltonian
+# --------------------------------------------------------------------------------------
+
+class DeviceHamiltonian:
+    """Device copy of a lowered Hamiltonian and its C struct."""
+
+    def __init__(self, lowered, device=None):
+        dev = _dev(device)
+        t = lambda x, dt: torch.as_tensor(np.ascontiguousarray(x), dtype=dt, device=dev)
+        self.lowered = lowered
+        self.ns = lowered.ns
+        self.move_i = t(lowered.move_i, torch.int32)
+        self.move_j = t(lowered.move_j, torch.int32)
+        self.move_kind = t(lowered.move_kind, torch.int32)
+        self.move_coef = t(lowered.move_coef.reshape(-1), torch.float32)
+        self.zf_site = t(lowered.zf_site, torch.int32)
+        self.zf_h = t(lowered.zf_h, torch.float32)
+        self.zz_i = t(lowered.zz_i, torch.int32)
+        self.zz_j = t(lowered.zz_j, torch.int32)
+        self.zz_J = t(lowered.zz_J, torch.float32)
+        self.struct = _lib.Hamiltonian(
+            lowered.n_moves, ptr(self.move_i), ptr(self.move_j), ptr(self.move_kind), ptr(self.move_coef),
+            int(self.zf_site.numel()), ptr(self.zf_site), ptr(self.zf_h),
+            int(self.zz_i.numel()), ptr(self.zz_i), ptr(self.zz_j), ptr(self.zz_J))
+
+    @property
+    def n_moves(self):
+        return self.lowered.n_moves
+
+
+def local_energy_workspace(dtype_c, ns, nh, n, K):
+    nb = C.c_size_t(0)
+    call("qes_local_energy_workspace_bytes", dtype_c, ns, nh, n, K, C.byref(nb))
+    return int(nb.value)
+
+
+def local_energy(flat_params, ns, nh, bits, tanh_theta, ham: DeviceHamiltonian, tables, workspace=None):
+    n = int(bits.shape[0])
+    dc = dtype_code(flat_params)
+    need = local_energy_workspace(dc, ns, nh, n, ham.n_moves)
+    if workspace is None or workspace.numel() < need:
+        workspace = torch.empty((max(need, 1),), dtype=torch.uint8, device=bits.device)
+    Ct, St, A = tables
+    out = torch.empty((n,), dtype=torch.complex64, device=bits.device)
+    call("qes_local_energy", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), C.byref(ham.struct), ptr(Ct), ptr(St),
+         ptr(A), ptr(workspace), int(workspace.numel()), ptr(out), stream_ptr())
+    return out
+
+
+def loss_stats(eloc, probs=None, workspace=None):
+    n = int(eloc.shape[0])
+    nb = C.c_size_t(0)
+    call("qes_loss_stats_workspace_bytes", n, C.byref(nb))
+    if workspace is None or workspace.numel() < nb.value:
+        workspace = torch.empty((int(nb.value),), dtype=torch.uint8, device=eloc.device)
+    out = torch.empty((4,), dtype=torch.float64, device=eloc.device)
+    call("qes_loss_stats", n, ptr(eloc), ptr(probs), ptr(out), ptr(workspace), int(workspace.numel()), stream_ptr())
+    return out
+
+
+# --------------------------------------------------------------------------------------
+# SR
+# --------------------------------------------------------------------------------------
+
+def vec_dtype(param_dtype):
+    return torch.complex128 if param_dtype == torch.complex64 else torch.float64
+
+
+def sr_workspace(dtype_c, ns, nh, n, device):
+    nb = C.c_size_t(0)
+    call("qes_sr_workspace_bytes", dtype_c, ns, nh, n, C.byref(nb))
+    return torch.empty((int(nb.value),), dtype=torch.uint8, device=device)
+
+
+def sr_force(flat_params, ns, nh, bits, tanh_theta, eloc, workspace=None):
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
+    F = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    call("qes_sr_force", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), ptr(F), ptr(ws), int(ws.numel()),
+         stream_ptr())
+    return F
+
+
+def sr_matvec(flat_params, ns, nh, bits, tanh_theta, v, shift=0.0, workspace=None):
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
+    v = v.to(vec_dtype(flat_params.dtype)).contiguous()
+    y = torch.empty_like(v)
+    call("qes_sr_matvec", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), float(shift), ptr(v), ptr(y), ptr(ws),
+         int(ws.numel()), stream_ptr())
+    return y
+
+
+def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
+                check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True):
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
+    x = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor))
+    res = _lib.SRResult()
+    allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_converged else ()
+    call("qes_sr_solve_cg", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), C.byref(opt), ptr(x), C.byref(res),
+         ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
+    info = {"iterations": res.iterations, "converged": bool(res.converged), "residual": res.residual,
+            "rhs_norm": res.rhs_norm, "e_mean": complex(res.e_mean_re, res.e_mean_im)}
+    return x, info
+
+
+def logpsi_vjp(flat_params, ns, nh, bits, tanh_theta, g, workspace=None):
+    """grad = O^H g (hand-written backward of log psi)."""
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
+    g = g.to(torch.complex64).contiguous()
+    out = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    call("qes_rbm_logpsi_vjp", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(g), ptr(out), ptr(ws),
+         int(ws.numel()), stream_ptr())
+    return out
+
+
+def param_update(flat_params, master, x, lr):
+    call("qes_param_update", dtype_code(flat_params), int(flat_params.numel()), float(lr), ptr(x), ptr(master),
+         ptr(flat_params), stream_ptr())
+
+
+# --------------------------------------------------------------------------------------
+# sampler
+# --------------------------------------------------------------------------------------
+
+def sampler_run(flat_params, ns, nh, cfg: _lib.SamplerConfig, flip_tables, exch, chain_bits, chain_step, proposed,
+                accepted, sample_bits, sample_logpsi, last_logpsi):
+    a, b, W = split_params(flat_params, ns, nh)
+    fC, fS = flip_tables if flip_tables is not None else (None, None)
+    if exch is not None:
+        nbr, nbr_pair, pi, pj, pC, pS = exch
+        npairs = int(pi.numel())
+    else:
+        nbr = nbr_pair = pi = pj = pC = pS = None
+        npairs = 0
+    call("qes_sampler_run", dtype_code(flat_params), C.byref(cfg), ptr(a), ptr(b), ptr(W), ptr(fC), ptr(fS),
+         ptr(nbr), ptr(nbr_pair), ptr(pi), ptr(pj), npairs, ptr(pC), ptr(pS), ptr(chain_bits), ptr(chain_step),
+         ptr(proposed), ptr(accepted), ptr(sample_bits), ptr(sample_logpsi), ptr(last_logpsi), stream_ptr())

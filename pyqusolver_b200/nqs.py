@@ -1,0 +1,238 @@
+"""``NQS`` facade for the RBM variational-Monte-Carlo path, on the GPU.
+
+Keeps the reference's entry points and their argument meaning
+(``QES/NQS/nqs.py``): the constructor with ``s_*`` sampler kwargs
+(``:241-591``, defaults ``:1027-1041``), ``sample`` (``:1896-1942``),
+``step`` (``:2353-2424`` -> ``NQSSingleStepResult``), ``log_derivative``
+(``:2134-2188``), ``get_params`` / ``set_params`` and ``train``
+(``:3002-3309``; the loop of ``QES/NQS/src/nqs_train.py:1460-1619``).
+
+One training epoch = sample (persistent sampler kernel) -> theta / tanh for
+the samples (forward kernel) -> E_loc (fused local-energy kernel) ->
+float64 statistics -> SR solve (structured CG) -> float64 Euler/SGD update.
+Only the recognised models (TFIM, XXZ, J1-J2) are accepted as the physics;
+an arbitrary local-energy callable raises, there is no fallback path.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Any, List, Optional
+
+import numpy as np
+import torch
+
+from . import device as dv
+from .hamiltonian import SpinHamiltonian
+from .rbm import RBM
+from .sampler import VMCSampler
+from .tdvp import TDVP
+
+
+@dataclass
+class NQSSingleStepResult:
+    loss: Any
+    loss_mean: Any
+    loss_std: Any
+    grad_flat: Any
+    params_shapes: List
+    params_sizes: List
+    params_cpx: List
+
+
+@dataclass
+class NQSTrainStats:
+    history: List[complex] = field(default_factory=list)
+    history_std: List[float] = field(default_factory=list)
+    sigma2: List[float] = field(default_factory=list)
+    acceptance: List[float] = field(default_factory=list)
+    cg_iterations: List[int] = field(default_factory=list)
+    timings: List[float] = field(default_factory=list)
+    exact: Optional[float] = None
+
+    @property
+    def last_energy(self):
+        return self.history[-1] if self.history else None
+
+
+class NQS:
+    def __init__(self, logansatz="rbm", model: SpinHamiltonian = None, hilbert=None, *, sampler="vmc",
+                 batch_size=None, backend="cuda", dtype=np.complex64, param_dtype=None, seed=0, alpha=1.0,
+                 nparticles=None, device=None, verbose=False, **kwargs):
+        if model is None or not isinstance(model, SpinHamiltonian):
+            raise TypeError("NQS on the GPU path needs a TransverseFieldIsing / XXZ / J1J2Model instance")
+        self._model = model
+        self._hilbert = hilbert if hilbert is not None else model.hilbert_space
+        ns = self._hilbert.ns
+        if isinstance(logansatz, RBM):
+            self._net = logansatz
+        elif str(logansatz).lower() in ("rbm", "r1"):
+            self._net = RBM((ns,), alpha=kwargs.pop("alpha_rbm", alpha), dtype=param_dtype or dtype, seed=seed,
+                            init_scale=kwargs.pop("init_scale", 0.01), device=device)
+        else:
+            raise ValueError(f"ansatz {logansatz!r}: the GPU path implements the RBM")
+        if self._net.ns != ns:
+            raise ValueError("ansatz size does not match the Hilbert space")
+        self._batch_size = batch_size
+        self._nparticles = ns if nparticles is None else int(nparticles)
+        self._seed = seed
+        self._sampler = VMCSampler(
+            self._net, (ns,), upd_fun=kwargs.get("s_upd_fun", "LOCAL"), mu=kwargs.get("s_mu", 2.0),
+            beta=kwargs.get("s_beta", 1.0), therm_steps=kwargs.get("s_therm_steps", 24),
+            sweep_steps=kwargs.get("s_sweep_steps", 48), seed=kwargs.get("s_seed", seed), hilbert=self._hilbert,
+            numsamples=kwargs.get("s_numsamples", 192), numchains=kwargs.get("s_numchains", 24),
+            initstate=kwargs.get("s_initstate", None), logprob_fact=kwargs.get("s_logprob_fact", 0.5),
+            n_particles=self._nparticles, lattice=getattr(model, "lattice", None),
+            recompute_every=kwargs.get("s_recompute_every", None))
+        self._lowered = model.lower()
+        self._dev_ham = dv.DeviceHamiltonian(self._lowered, self._net.device)
+        self._eloc_tables = None
+        self._eloc_tables_version = -1
+        self._eloc_ws = None
+        self._tdvp = None
+        self.exact = None
+
+    # ------------------------------------------------------------------ accessors
+    @property
+    def net(self):
+        return self._net
+
+    @property
+    def sampler(self):
+        return self._sampler
+
+    @property
+    def model(self):
+        return self._model
+
+    @property
+    def hilbert(self):
+        return self._hilbert
+
+    def get_params(self, unravel=False):
+        return self._net.get_params(unravel=unravel)
+
+    def set_params(self, params):
+        self._net.set_params(params)
+
+    @property
+    def num_params(self):
+        return self._net.n_params
+
+    # ------------------------------------------------------------------ evaluation
+    def ansatz(self, states):
+        return self._net.log_psi(states)
+
+    __call__ = ansatz
+
+    def _tables(self):
+        if self._eloc_tables is None or self._eloc_tables_version != self._net.version:
+            h = self._dev_ham
+            self._eloc_tables = dv.move_tables(self._net.flat, self._net.ns, self._net.nh, h.move_i, h.move_j,
+                                               h.move_kind, move_major=False)
+            self._eloc_tables_version = self._net.version
+        return self._eloc_tables
+
+    def local_energy_bits(self, bits, tanh_theta=None):
+        net = self._net
+        if tanh_theta is None:
+            _, tanh_theta, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+        need = dv.local_energy_workspace(dv.dtype_code(net.flat), net.ns, net.nh, int(bits.shape[0]),
+                                         self._dev_ham.n_moves)
+        if self._eloc_ws is None or self._eloc_ws.numel() < need:
+            self._eloc_ws = torch.empty((max(need, 1),), dtype=torch.uint8, device=net.device)
+        return dv.local_energy(net.flat, net.ns, net.nh, bits, tanh_theta, self._dev_ham, self._tables(),
+                               self._eloc_ws)
+
+    def local_energy(self, states):
+        return self.local_energy_bits(self._net.bits(states))
+
+    def log_derivative(self, states, batch_size=None, params=None, *args, **kwargs):
+        if params is not None:
+            self.set_params(params)
+        O = self._net.log_derivative(states)
+        return O, self._net.params_shapes, self._net.params_sizes, self._net.params_cpx
+
+    # ------------------------------------------------------------------ sampling / step
+    def sample(self, num_samples=None, num_chains=None, reset=False, *, params=None, **kwargs):
+        if reset:
+            self._sampler.reset()
+        out = self._sampler.sample(parameters=params, num_samples=num_samples, num_chains=num_chains)
+        if kwargs.get("states", False):
+            return out[1]
+        if kwargs.get("last", False):
+            return out[0]
+        return out
+
+    def step(self, configs=None, configs_ansatze=None, probabilities=None, params=None, **kwargs):
+        if params is not None:
+            self.set_params(params)
+        net = self._net
+        if configs is None:
+            bits, lp = self._sampler.sample_bits(kwargs.get("num_samples", None))
+        else:
+            bits = net.bits(configs)
+        _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+        eloc = self.local_energy_bits(bits, tn)
+        w = None if probabilities is None else torch.as_tensor(probabilities, dtype=torch.float32,
+                                                               device=net.device).reshape(-1)
+        st = dv.loss_stats(eloc, w)
+        O = dv.log_derivatives(net.flat, net.ns, net.nh, bits, tn)
+        mean = torch.complex(st[0], st[1])
+        return NQSSingleStepResult(loss=eloc, loss_mean=mean, loss_std=st[3], grad_flat=O,
+                                   params_shapes=net.params_shapes, params_sizes=net.params_sizes,
+                                   params_cpx=net.params_cpx)
+
+    # ------------------------------------------------------------------ training
+    def train(self, n_epochs=300, checkpoint_every=50, load_checkpoint=False, *, lin_solver="scipy_cg", n_batch=128,
+              num_samples=None, num_chains=None, num_thermal=None, num_sweep=None, lr=1e-2, use_sr=True,
+              use_minsr=False, rhs_prefactor=-1.0, diag_shift=1e-3, exact_predictions=None, upd_fun=None,
+              sr_tol=1e-8, sr_maxiter=1000, grad_clip=None, reset_stats=True, use_pbar=False, callback=None,
+              **kwargs) -> NQSTrainStats:
+        if upd_fun is not None and str(upd_fun).upper() != self._sampler._upd_rule_name:
+            raise ValueError("change the update rule at construction (s_upd_fun)")
+        if num_chains is not None:
+            self._sampler.set_numchains(num_chains)
+        if num_sweep is not None:
+            self._sampler._sweep_steps = int(num_sweep)
+        if num_thermal is not None:
+            self._sampler._therm_steps = int(num_thermal)
+        self._tdvp = TDVP(use_sr=use_sr, use_minsr=use_minsr, rhs_prefactor=rhs_prefactor, sr_lin_solver=lin_solver,
+                          sr_diag_shift=diag_shift, sr_tol=sr_tol, sr_maxiter=sr_maxiter, grad_clip=grad_clip)
+        stats = NQSTrainStats()
+        if exact_predictions is not None:
+            stats.exact = float(np.min(np.real(np.atleast_1d(exact_predictions))))
+            self.exact = stats.exact
+        for epoch in range(int(n_epochs)):
+            t0 = time.perf_counter()
+            info = self.train_step(num_samples=num_samples, lr=lr)
+            torch.cuda.synchronize()
+            stats.timings.append(time.perf_counter() - t0)
+            stats.history.append(info["mean"])
+            stats.history_std.append(info["std"])
+            stats.sigma2.append(info["var"])
+            stats.acceptance.append(info["acceptance"])
+            stats.cg_iterations.append(info["cg_iterations"])
+            if callback is not None:
+                callback(epoch, info)
+            if not np.isfinite(np.real(info["mean"])):
+                break
+        return stats
+
+    def train_step(self, num_samples=None, lr=1e-2, tdvp: Optional[TDVP] = None):
+        """One VMC epoch on the GPU; returns host-side statistics of this epoch."""
+        tdvp = tdvp or self._tdvp or TDVP()
+        net = self._net
+        bits, _ = self._sampler.sample_bits(num_samples)
+        _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+        eloc = self.local_energy_bits(bits, tn)
+        st = dv.loss_stats(eloc)
+        x = tdvp.solve(net, bits, tn, eloc)
+        dv.param_update(net.flat, net.master, x, lr)
+        net.bump()
+        s = st.cpu().numpy()
+        acc = self._sampler.accepted_ratio.mean().item()
+        return {"mean": complex(s[0], s[1]), "var": float(s[2]), "std": float(s[3]), "acceptance": acc,
+                "cg_iterations": int(tdvp.last_info.get("iterations", 0)),
+                "cg_converged": bool(tdvp.last_info.get("converged", True))}

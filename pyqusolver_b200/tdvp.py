@@ -1,0 +1,85 @@
+"""TDVP / stochastic reconfiguration with the reference's options and conventions.
+
+Mirrors ``QES/NQS/src/tdvp.py`` for the RBM path:
+
+* centring and float64 promotion (``get_tdvp_standard`` ``:1056-1132``);
+* force F = O_c^H E_c / Ns, standard SR (O_c^H O_c / Ns + shift) x = F in the
+  GRAM / MATVEC form (``_solve_prepare_matvec`` ``:1138-1197``);
+* x <- rhs_prefactor * x (default -1), optional global-norm clip
+  (``_finalize_solution`` ``:1410-1422``, ``_apply_grad_clip`` ``:882-907``);
+* ``use_sr=False`` returns x = -rhs_prefactor * F ... i.e. the reference's
+  ``-final_b`` branch (``solve`` ``:1561-1569``).
+
+The solve runs on the GPU (``qes_sr_solve_cg``): the RBM's O is applied in
+structured form and never materialised, CG vectors and dots are float64.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+
+from . import device as dv
+
+
+@dataclass
+class TDVPStepInfo:
+    mean_energy: complex
+    std_energy: float
+    iterations: int
+    converged: bool
+    residual: float
+
+
+class TDVP:
+    def __init__(self, use_sr=True, use_minsr=False, rhs_prefactor=-1.0, sr_lin_solver="scipy_cg",
+                 sr_diag_shift=1e-3, sr_tol=1e-8, sr_atol=0.0, sr_maxiter=1000, grad_clip=None,
+                 check_every=16, **kwargs):
+        if use_minsr:
+            raise NotImplementedError("MinSR is not implemented on the GPU path")
+        solver = str(sr_lin_solver).lower()
+        if solver not in ("scipy_cg", "cg"):
+            raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG")
+        self.use_sr = bool(use_sr)
+        self.use_minsr = False
+        self.rhs_prefactor = float(rhs_prefactor)
+        self.sr_diag_shift = float(sr_diag_shift)
+        self.sr_tol = float(sr_tol)
+        self.sr_atol = float(sr_atol)
+        self.sr_maxiter = int(sr_maxiter)
+        self.grad_clip = grad_clip
+        self.check_every = int(check_every)
+        self._workspace = None
+        self.last_info = None
+
+    def set_diag_shift(self, shift):
+        self.sr_diag_shift = float(shift)
+
+    def _ws(self, net, n):
+        dc = dv.dtype_code(net.flat)
+        import ctypes as C
+        from . import _lib
+        nb = C.c_size_t(0)
+        _lib.call("qes_sr_workspace_bytes", dc, net.ns, net.nh, n, C.byref(nb))
+        if self._workspace is None or self._workspace.numel() < nb.value:
+            self._workspace = torch.empty((int(nb.value),), dtype=torch.uint8, device=net.device)
+        return self._workspace
+
+    def solve(self, net, bits, tanh_theta, eloc):
+        """Parameter direction x (float64 / complex128, length P), already scaled by rhs_prefactor."""
+        n = int(bits.shape[0])
+        ws = self._ws(net, n)
+        if not self.use_sr:
+            F = dv.sr_force(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, workspace=ws)
+            x = -(F * self.rhs_prefactor) if self.rhs_prefactor != 1.0 else -F
+            self.last_info = {"iterations": 0, "converged": True, "residual": 0.0}
+        else:
+            x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
+                                     rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,
+                                     check_every=self.check_every, rhs_prefactor=self.rhs_prefactor, workspace=ws)
+            self.last_info = info
+        if self.grad_clip is not None and self.grad_clip > 0:
+            nrm = torch.linalg.vector_norm(x)
+            x = x * torch.clamp(self.grad_clip / (nrm + 1e-12), max=1.0)
+        return x

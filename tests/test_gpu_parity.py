@@ -1,0 +1,299 @@
+"""CUDA path (through the C ABI) against the float64 oracle on identical inputs.
+
+Tolerances: float32 kernels vs the float64 oracle -- 1e-5 relative for theta,
+tanh, log psi, O and E_loc (the plain-FP32 bar), SR vectors 1e-4 relative
+(float32 matvec inside a float64 CG).  Integer work (packed chains, sampler
+trajectories, acceptance counters) is compared bit-exactly.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lattice as olat, hamiltonian as oH, rbm as orbm, estimator as oest, sampler as osm, sr as osr
+from oracle import ed as oed
+import pyqusolver_b200 as qb
+from pyqusolver_b200 import device as dv, _lib
+from pyqusolver_b200.rbm import RBM, RBMLogPsi
+from pyqusolver_b200.sampler import VMCSampler
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+def oracle_params(net: RBM):
+    flat = net.flat.detach().cpu().numpy().astype(np.complex128 if net.is_complex else np.float64)
+    return orbm.RBMParams.from_flat(flat, net.ns, net.nh)
+
+
+def rand_states(n, ns, seed=0):
+    rng = np.random.default_rng(seed)
+    return np.where(rng.random((n, ns)) < 0.5, 0.5, -0.5)
+
+
+def wrap_close(a, b, rtol=RTOL):
+    """log psi comparison: real parts relative, imaginary parts modulo 2 pi."""
+    a, b = np.asarray(a), np.asarray(b)
+    scale = max(1.0, np.max(np.abs(b.real)))
+    assert np.max(np.abs(a.real - b.real)) <= rtol * scale * 10
+    if np.iscomplexobj(b):
+        d = np.angle(np.exp(1j * (a.imag - b.imag)))
+        assert np.max(np.abs(d)) <= rtol * scale * 10
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.max(np.abs(a - b)) / max(1e-30, np.max(np.abs(b)))
+
+
+# ------------------------------------------------------------------------- chains
+@pytest.mark.parametrize("ns", [16, 36, 100, 400])
+def test_init_chains_match_oracle(ns):
+    for kind, okind, nup in [(_lib.INIT_RND, "RND", 0), (_lib.INIT_RND_FIXED, "RND_FIXED", ns // 2)]:
+        w = dv.init_chains(kind, 37, ns, seed=1234567, n_up=nup, chain_offset=5)
+        got = dv.unpack_states(w, ns, 1.0).cpu().numpy()
+        ref = osm.init_states(okind, 37, ns, seed=1234567, n_up=nup, chain_offset=5)
+        assert np.array_equal(got, ref)
+
+
+# ------------------------------------------------------------------------- forward
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("ns,nh", [(16, 16), (36, 144), (100, 200), (33, 70)])
+def test_forward_matches_oracle(cplx, ns, nh):
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=3, init_scale=0.1)
+    st = rand_states(300, ns, seed=1)
+    bits = dv.pack_states(st)
+    th, tn, lp = dv.rbm_forward(net.flat, ns, nh, bits, theta=True, tanh=True, logpsi=True)
+    p = oracle_params(net)
+    sig = orbm.to_sigma(st)
+    th_ref = orbm.theta(p, sig)
+    assert rel_err(th.cpu().numpy(), th_ref) < RTOL
+    assert rel_err(tn.cpu().numpy(), np.tanh(th_ref)) < RTOL
+    wrap_close(lp.cpu().numpy(), orbm.log_psi(p, sig))
+
+
+def test_forward_large_theta_is_finite():
+    net = RBM((20,), n_hidden=8, dtype="complex64", seed=0, init_scale=3.0)
+    st = rand_states(64, 20, seed=2)
+    _, tn, lp = dv.rbm_forward(net.flat, 20, 8, dv.pack_states(st), tanh=True, logpsi=True)
+    p = oracle_params(net)
+    th = orbm.theta(p, orbm.to_sigma(st))
+    assert torch.isfinite(torch.view_as_real(lp)).all()
+    np.testing.assert_allclose(tn.cpu().numpy(), np.tanh(th), rtol=1e-4, atol=1e-5)
+
+
+# ------------------------------------------------------------------------- local energy
+def _model_cases():
+    return [
+        ("tfim1d", lambda: (qb.SquareLattice(1, 16), olat.SquareLattice(1, 16)),
+         lambda L: qb.TransverseFieldIsing(L, j=1.0, hx=1.0, hz=0.0), lambda L: oH.tfim_terms(L, 1.0, 1.0, 0.0), 1.0),
+        ("tfim2d_hz", lambda: (qb.SquareLattice(2, 4, 5), olat.SquareLattice(2, 4, 5)),
+         lambda L: qb.TransverseFieldIsing(L, j=0.8, hx=3.04, hz=0.4), lambda L: oH.tfim_terms(L, 0.8, 3.04, 0.4), 2.0),
+        ("xxx2d", lambda: (qb.SquareLattice(2, 6, 6), olat.SquareLattice(2, 6, 6)),
+         lambda L: qb.XXZ(L, jxy=-1.0, jz=-1.0), lambda L: oH.xxz_terms(L, -1.0, -1.0), 2.0),
+        ("xxz_hx", lambda: (qb.SquareLattice(2, 4, 4), olat.SquareLattice(2, 4, 4)),
+         lambda L: qb.XXZ(L, jxy=-1.0, jz=-0.5, hx=0.3), lambda L: oH.xxz_terms(L, -1.0, -0.5, hx=0.3), 2.0),
+        ("j1j2", lambda: (qb.SquareLattice(2, 6, 6), olat.SquareLattice(2, 6, 6)),
+         lambda L: qb.J1J2Model(L, J1=-1.0, J2=-0.5), lambda L: oH.j1j2_terms(L, -1.0, -0.5), 4.0),
+        ("j1j2_hy", lambda: (qb.SquareLattice(2, 4, 4), olat.SquareLattice(2, 4, 4)),
+         lambda L: qb.J1J2Model(L, J1=-1.0, J2=-0.5, hx=0.2, hy=0.3), lambda L: oH.j1j2_terms(L, -1.0, -0.5, hx=0.2, hy=0.3), 2.0),
+    ]
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("case", _model_cases(), ids=[c[0] for c in _model_cases()])
+def test_local_energy_matches_oracle(case, cplx):
+    name, lats, mk, mko, alpha = case
+    L, OL = lats()
+    model = mk(L)
+    terms = mko(OL)
+    ns = L.ns
+    net = RBM((ns,), alpha=alpha, dtype="complex64" if cplx else "float32", seed=5, init_scale=0.05)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, net.nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    st = rand_states(200, ns, seed=4)
+    if name.startswith("xxx") or name == "j1j2":
+        st = osm.init_states("RND_FIXED", 200, ns, seed=9, n_up=ns // 2) * 0.5
+    bits = dv.pack_states(st)
+    _, tn, _ = dv.rbm_forward(net.flat, ns, net.nh, bits, tanh=True, logpsi=False)
+    e = dv.local_energy(net.flat, ns, net.nh, bits, tn, h, tables).cpu().numpy()
+    ref = oest.local_energy_full(oracle_params(net), terms, st)
+    err = np.max(np.abs(e - ref)) / max(1.0, np.max(np.abs(ref)))
+    assert err < RTOL, err
+
+
+def test_local_energy_edge_cases():
+    # one sample, K not a multiple of 32, trained-looking large weights (renormalisation path)
+    L, OL = qb.SquareLattice(1, 7), olat.SquareLattice(1, 7)
+    model = qb.TransverseFieldIsing(L, j=1.0, hx=0.5, hz=0.0)
+    net = RBM((7,), n_hidden=300, dtype="complex64", seed=1, init_scale=0.6)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, 7, 300, h.move_i, h.move_j, h.move_kind, move_major=False)
+    for n in (1, 33):
+        st = rand_states(n, 7, seed=n)
+        bits = dv.pack_states(st)
+        _, tn, _ = dv.rbm_forward(net.flat, 7, 300, bits, tanh=True, logpsi=False)
+        e = dv.local_energy(net.flat, 7, 300, bits, tn, h, tables).cpu().numpy()
+        ref = oest.local_energy_full(oracle_params(net), oH.tfim_terms(OL, 1.0, 0.5, 0.0), st)
+        assert np.max(np.abs(e - ref)) / max(1.0, np.max(np.abs(ref))) < 1e-4
+
+
+def test_loss_stats_match_numpy():
+    rng = np.random.default_rng(0)
+    e = (rng.normal(size=5000) + 1j * rng.normal(size=5000)).astype(np.complex64) - 40.0
+    w = rng.random(5000).astype(np.float32)
+    w = w / w.sum() * 5000
+    for probs in (None, w):
+        out = dv.loss_stats(torch.as_tensor(e).cuda(), None if probs is None else torch.as_tensor(probs).cuda())
+        mean, std = oest.loss_stats(e.astype(np.complex128), probs)
+        o = out.cpu().numpy()
+        assert abs(complex(o[0], o[1]) - mean) < 1e-9 * abs(mean)
+        assert o[3] == pytest.approx(std, rel=1e-9)
+
+
+# ------------------------------------------------------------------------- log-derivatives / backward
+@pytest.mark.parametrize("cplx", [False, True])
+def test_log_derivatives_match_oracle_and_finite_differences(cplx):
+    ns, nh = 12, 24
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=2, init_scale=0.1)
+    st = rand_states(50, ns, seed=3)
+    O = net.log_derivative(st).cpu().numpy()
+    p = oracle_params(net)
+    Oref = orbm.log_derivatives(p, orbm.to_sigma(st))
+    assert rel_err(O, Oref) < RTOL
+    # central differences of the float64 log psi, step 1e-4
+    flat = p.flat()
+    sig = orbm.to_sigma(st)
+    h = 1e-4
+    rng = np.random.default_rng(0)
+    for k in rng.choice(flat.size, 40, replace=False):
+        e = np.zeros_like(flat)
+        e[k] = h
+        fd = (orbm.log_psi(orbm.RBMParams.from_flat(flat + e, ns, nh), sig)
+              - orbm.log_psi(orbm.RBMParams.from_flat(flat - e, ns, nh), sig)) / (2 * h)
+        np.testing.assert_allclose(O[:, k], fd, rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_autograd_backward_is_conj_O_transpose_g(cplx):
+    ns, nh = 10, 20
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=4, init_scale=0.2)
+    st = rand_states(64, ns, seed=5)
+    lp, p = net.log_psi_autograd(st)
+    rng = np.random.default_rng(1)
+    g = rng.normal(size=64) + (1j * rng.normal(size=64) if cplx else 0)
+    gt = torch.as_tensor(g.astype(np.complex64 if cplx else np.float32)).cuda()
+    (grad,) = torch.autograd.grad(lp, p, grad_outputs=gt)
+    O = orbm.log_derivatives(oracle_params(net), orbm.to_sigma(st))
+    ref = np.conj(O).T @ g if cplx else O.T @ g
+    assert rel_err(grad.cpu().numpy(), ref) < 1e-5
+
+
+# ------------------------------------------------------------------------- SR
+@pytest.mark.parametrize("cplx", [False, True])
+def test_sr_force_matvec_and_cg_match_dense_oracle(cplx):
+    ns, nh, n = 9, 18, 700
+    L = qb.SquareLattice(2, 3, 3)
+    model = qb.XXZ(L, jxy=-1.0, jz=-1.0, hx=0.4)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=6, init_scale=0.2)
+    st = rand_states(n, ns, seed=6)
+    bits = dv.pack_states(st)
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    e = eloc.cpu().numpy().astype(np.complex128)
+    if not cplx:
+        e = e.real
+    O = orbm.log_derivatives(oracle_params(net), orbm.to_sigma(st))
+    ec, Oc, w, _, _ = osr.prepare(e, O)
+    F = osr.force(Oc, ec)
+    Fg = dv.sr_force(net.flat, ns, nh, bits, tn, eloc).cpu().numpy()
+    assert rel_err(Fg, F) < 1e-4
+    S = osr.s_matrix(Oc)
+    v = np.random.default_rng(2).normal(size=O.shape[1]) + (1j if cplx else 0) * np.random.default_rng(3).normal(size=O.shape[1])
+    y = dv.sr_matvec(net.flat, ns, nh, bits, tn, torch.as_tensor(v).cuda(), shift=1e-3).cpu().numpy()
+    assert rel_err(y, S @ v + 1e-3 * v) < 1e-4
+    x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-10, maxiter=2000)
+    xr = -np.linalg.solve(S + 1e-2 * np.eye(S.shape[0]), F)
+    assert info["converged"]
+    assert rel_err(x.cpu().numpy(), xr) < 1e-3
+
+
+# ------------------------------------------------------------------------- sampler
+def _gpu_sampler(net, rule, ns, chains, seed, therm, sweep, lattice=None, init=None, n_up=None):
+    return VMCSampler(net, (ns,), upd_fun=rule, seed=seed, therm_steps=therm, sweep_steps=sweep, numchains=chains,
+                      numsamples=1, lattice=lattice, initstate=init, n_particles=n_up)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_sampler_local_trajectory_matches_oracle(cplx):
+    ns = 10
+    net = RBM((ns,), n_hidden=20, dtype="complex64" if cplx else "float32", seed=8, init_scale=0.3)
+    smp = _gpu_sampler(net, "LOCAL", ns, 64, seed=77, therm=2, sweep=5)
+    bits, lp = smp.sample_bits(num_samples=6)
+    got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
+    ref = osm.MetropolisSampler(ns, 64, rule="LOCAL", seed=77, therm_steps=2, sweep_steps=5)
+    cfg, lp_ref, _ = ref.sample(oracle_params(net), 6)
+    mism = np.mean(np.any(got != cfg, axis=1))
+    assert mism <= 0.02, mism          # float32 vs float64 ties may flip a rare decision
+    same = np.all(got == cfg, axis=1)
+    wrap_close(lp.cpu().numpy()[same], lp_ref[same])
+    assert np.array_equal(smp.proposed.cpu().numpy(), ref.proposed)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_sampler_exchange_trajectory_matches_oracle(cplx):
+    L, OL = qb.SquareLattice(2, 4, 4), olat.SquareLattice(2, 4, 4)
+    ns = 16
+    net = RBM((ns,), n_hidden=32, dtype="complex64" if cplx else "float32", seed=9, init_scale=0.3)
+    smp = _gpu_sampler(net, "EXCHANGE", ns, 64, seed=5, therm=1, sweep=7, lattice=L, init="RND_FIXED", n_up=8)
+    bits, _ = smp.sample_bits(num_samples=5)
+    got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
+    ref = osm.MetropolisSampler(ns, 64, rule="EXCHANGE", neighbor_table=olat.neighbor_table(OL), seed=5,
+                                therm_steps=1, sweep_steps=7, init="RND_FIXED", n_up=8)
+    cfg, _, _ = ref.sample(oracle_params(net), 5)
+    assert np.all((got > 0).sum(1) == 8)
+    assert np.mean(np.any(got != cfg, axis=1)) <= 0.02
+    acc_g = smp.accepted.cpu().numpy()
+    assert np.mean(acc_g != ref.accepted) <= 0.05
+
+
+@pytest.mark.parametrize("rule", ["LOCAL", "EXCHANGE"])
+def test_sampler_matches_exact_distribution(rule):
+    ns = 10
+    L = qb.SquareLattice(1, ns)
+    net = RBM((ns,), n_hidden=10, dtype="complex64", seed=12, init_scale=0.5)
+    n_up = ns // 2 if rule == "EXCHANGE" else None
+    smp = _gpu_sampler(net, rule, ns, 2048, seed=3, therm=4, sweep=10, lattice=L,
+                       init="RND_FIXED" if rule == "EXCHANGE" else None, n_up=n_up)
+    bits, _ = smp.sample_bits(num_samples=40)
+    st = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
+    ints = ((st > 0).astype(np.int64) * (1 << np.arange(ns - 1, -1, -1))).sum(1)
+    basis, w = osm.exact_distribution(oracle_params(net), ns, n_up=n_up)
+    hist = np.bincount(ints, minlength=1 << ns)[basis] / len(ints)
+    tv = 0.5 * np.abs(hist - w).sum()
+    assert tv < 0.03, tv
+
+
+def test_sampler_continues_chains_without_rethermalising():
+    ns = 12
+    net = RBM((ns,), n_hidden=12, dtype="float32", seed=1)
+    smp = _gpu_sampler(net, "LOCAL", ns, 16, seed=2, therm=3, sweep=4)
+    smp.sample_bits(num_samples=2)
+    assert int(smp.proposed[0]) == 3 * 4 * ns + 2 * 4
+    smp.sample_bits(num_samples=3)
+    assert int(smp.proposed[0]) == 3 * 4 * ns + 5 * 4
+
+
+# ------------------------------------------------------------------------- end to end
+def test_nqs_training_tfim_reaches_ed():
+    L, OL = qb.SquareLattice(1, 8), olat.SquareLattice(1, 8)
+    model = qb.TransverseFieldIsing(L, j=1.0, hx=1.0, hz=0.0)
+    e0 = oed.ground_energy(oH.tfim_terms(OL, 1.0, 1.0, 0.0), 8)
+    nqs = qb.NQS("rbm", model, alpha=1.0, dtype="float32", seed=1, s_numchains=256, s_numsamples=8,
+                 s_therm_steps=10, s_sweep_steps=8)
+    stats = nqs.train(n_epochs=150, lr=0.05, diag_shift=1e-3)
+    tail = np.mean([h.real for h in stats.history[-10:]])
+    assert abs(tail - e0) / abs(e0) < 5e-3, (tail, e0)

@@ -1,0 +1,153 @@
+"""Host-side logic of the package against the oracle, and the C-ABI library exports (no GPU)."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lattice as olat, hamiltonian as oH
+import pyqusolver_b200 as qb
+from pyqusolver_b200 import _lib, device as dv
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _models():
+    out = []
+    l1 = qb.SquareLattice(1, 8, bc="pbc")
+    o1 = olat.SquareLattice(1, 8, bc="pbc")
+    out.append(("tfim1d", qb.TransverseFieldIsing(l1, j=1.0, hx=0.7, hz=0.3), oH.tfim_terms(o1, 1.0, 0.7, 0.3), 8))
+    l2 = qb.SquareLattice(2, 4, 4, bc="pbc")
+    o2 = olat.SquareLattice(2, 4, 4, bc="pbc")
+    out.append(("xxz2d", qb.XXZ(l2, jxy=-1.0, jz=-0.7, hx=0.2), oH.xxz_terms(o2, -1.0, -0.7, hx=0.2), 16))
+    out.append(("j1j2", qb.J1J2Model(l2, J1=-1.0, J2=-0.5, hy=0.3, hz=0.1),
+                oH.j1j2_terms(o2, -1.0, -0.5, hy=0.3, hz=0.1), 16))
+    l3 = qb.SquareLattice(1, 6, bc="obc")
+    o3 = olat.SquareLattice(1, 6, bc="obc")
+    out.append(("tfim_obc", qb.TransverseFieldIsing(l3, j=[1.0, 0.5, 0.0, 2.0, 1.0, 1.0], hx=1.0, hz=0.0),
+                oH.tfim_terms(o3, [1.0, 0.5, 0.0, 2.0, 1.0, 1.0], 1.0, 0.0), 6))
+    return out
+
+
+@pytest.mark.parametrize("name,model,terms,ns", _models(), ids=[m[0] for m in _models()])
+def test_term_lists_and_raw_slots_bit_exact(name, model, terms, ns):
+    pkg = [(t.op, t.sites, complex(t.mult)) for t in model.terms]
+    ora = [(t.op, tuple(t.sites), complex(t.mult)) for t in terms]
+    assert pkg == ora
+    rng = np.random.default_rng(0)
+    for _ in range(5):
+        s = np.where(rng.random(ns) < 0.5, 0.5, -0.5)
+        st_p, co_p = model.connected(s)
+        st_o, co_o = oH.connected_raw(terms, s)
+        assert np.array_equal(st_p, st_o)
+        assert np.array_equal(co_p, co_o)
+
+
+def _lowered_merged(low, s):
+    """Evaluate the lowered move table on one state: {sigma' tuple: conj(coefficient)} plus diagonal."""
+    sig = np.where(np.asarray(s) > 0, 1, -1)
+    out = {}
+    diag = float(np.sum(low.zf_h * sig[low.zf_site])) + float(np.sum(low.zz_J * sig[low.zz_i] * sig[low.zz_j]))
+    out[tuple(sig.tolist())] = diag
+    for k in range(low.n_moves):
+        i, j, kind = int(low.move_i[k]), int(low.move_j[k]), int(low.move_kind[k])
+        c = low.move_coef[k]
+        if kind == _lib.MOVE_FLIP1:
+            coef = complex(c[0], c[1]) + sig[i] * complex(c[2], c[3])
+            new = sig.copy()
+            new[i] = -new[i]
+        else:
+            if (kind == _lib.MOVE_PAIR_ANTI) != (sig[i] != sig[j]):
+                continue
+            coef = complex(c[0], c[1])
+            new = sig.copy()
+            new[i] = -new[i]
+            new[j] = -new[j]
+        key = tuple(new.tolist())
+        out[key] = out.get(key, 0) + coef
+    return {k: v for k, v in out.items() if abs(v) > 1e-7}
+
+
+@pytest.mark.parametrize("name,model,terms,ns", _models(), ids=[m[0] for m in _models()])
+def test_lowered_moves_match_merged_connected_set(name, model, terms, ns):
+    low = model.lower()
+    rng = np.random.default_rng(1)
+    for _ in range(8):
+        s = np.where(rng.random(ns) < 0.5, 0.5, -0.5)
+        ref = oH.connected_merged(terms, s)
+        ref = {k: np.conj(v) for k, v in ref.items() if abs(v) > 1e-7}   # E_loc uses conj(<s'|H|s>)
+        got = _lowered_merged(low, s)
+        assert set(ref) == set(got)
+        for k in ref:
+            assert got[k] == pytest.approx(ref[k], abs=1e-6)
+
+
+def test_isotropic_models_have_no_parallel_pair_moves():
+    l2 = qb.SquareLattice(2, 6, 6, bc="pbc")
+    low = qb.J1J2Model(l2, J1=-1.0, J2=-0.5).lower()
+    assert set(low.move_kind.tolist()) == {_lib.MOVE_PAIR_ANTI}
+    assert low.n_moves == 72 + 72
+    low = qb.XXZ(qb.SquareLattice(2, 10, 10), jxy=-1.0, jz=-1.0).lower()
+    assert low.n_moves == 200 and low.zz_i.size == 200
+
+
+def test_neighbor_tables_match_oracle():
+    for dim, lx, ly, bc in [(1, 7, 1, "pbc"), (2, 4, 4, "pbc"), (2, 6, 6, "pbc"), (2, 3, 5, "obc")]:
+        a = qb.get_neighbor_table(qb.SquareLattice(dim, lx, ly, bc=bc))
+        b = olat.neighbor_table(olat.SquareLattice(dim, lx, ly, bc=bc))
+        assert np.array_equal(a, b)
+    a = qb.get_neighbor_table(qb.SquareLattice(2, 5, 5), order=2)
+    b = olat.neighbor_table(olat.SquareLattice(2, 5, 5), order=2)
+    assert np.array_equal(a, b)
+
+
+def test_pack_unpack_round_trip_cpu():
+    rng = np.random.default_rng(5)
+    for ns in (1, 16, 31, 32, 33, 100, 400):
+        s = np.where(rng.random((7, ns)) < 0.5, 0.5, -0.5).astype(np.float32)
+        w = dv.pack_states(s, device="cpu")
+        assert w.shape == (7, (ns + 31) // 32)
+        back = dv.unpack_states(w, ns).numpy()
+        assert np.array_equal(back, s)
+
+
+def test_hilbert_integer_convention():
+    h = qb.HilbertSpace(ns=4)
+    st = h.int_to_state(0b0010)
+    assert st.tolist() == [-0.5, -0.5, 0.5, -0.5]
+    assert h.state_to_int(st) == 2
+
+
+def _header_symbols():
+    text = open(os.path.join(ROOT, "include", "qes_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(qes_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_and_binding_agree():
+    assert _header_symbols() == sorted(_lib.SIGNATURES)
+
+
+def test_library_loads_and_exports_every_header_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    for name in _header_symbols():
+        assert hasattr(lib, name), name
+    # host-only calls need no GPU
+    lib.qes_version.restype = ctypes.c_int
+    assert lib.qes_version() >= 100
+    nb = ctypes.c_size_t(0)
+    _lib.load()
+    assert _lib.call("qes_sr_workspace_bytes", 1, 100, 200, 16384, ctypes.byref(nb)) == 0 and nb.value > 0
+    assert _lib.call("qes_local_energy_workspace_bytes", 1, 100, 200, 16384, 200, ctypes.byref(nb)) == 0
+
+
+def test_library_rejects_bad_arguments_without_gpu():
+    _lib.load()
+    with pytest.raises(_lib.QESError) as e:
+        _lib.call("qes_init_chains", 1, 99, 0, 0, 4, 10, None, None)
+    assert e.value.code == _lib.QES_ERR_ARG
+    with pytest.raises(_lib.QESError):
+        _lib.call("qes_rbm_forward", 7, 4, 4, 1, None, None, None, None, None, None, None, None)

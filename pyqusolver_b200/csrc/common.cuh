@@ -115,25 +115,33 @@ QES_D float log_cosh(float x) {
 QES_D float2 log_cosh(float2 z) {
   const float sg = (z.x < 0.f) ? -1.f : 1.f;
   const float x = sg * z.x, y = sg * z.y;          // Re >= 0
-  const float q = expf(-2.f * x);                  // |w| = q <= 1
-  float sn, cs;
-  sincosf(-2.f * y, &sn, &cs);
-  const float wr = q * cs, wi = q * sn;            // w = exp(-2 s z)
-  const float re = 0.5f * log1pf(2.f * wr + q * q);   // log |1 + w|
-  const float im = atan2f(wi, 1.f + wr);
+  const float em = expm1f(-2.f * x);               // q - 1,  q = exp(-2x) <= 1
+  const float q = 1.f + em;
+  float sy, cy;
+  sincosf(y, &sy, &cy);
+  // 1 + w with w = q exp(-2iy), written without cancellation near cosh(z) = 0:
+  //   Re(1+w) = (1 - q) + 2 q cos^2 y,  Im(1+w) = -2 q sin y cos y
+  const float r1 = -em + 2.f * q * cy * cy;
+  const float i1 = -2.f * q * sy * cy;
+  float re;
+  if (q < 0.25f) re = 0.5f * log1pf(q * (2.f * (2.f * cy * cy - 1.f) + q));   // log|1+w|, small w
+  else re = 0.5f * logf(r1 * r1 + i1 * i1);
+  const float im = atan2f(i1, r1);
   return make_float2(x + re - 0.69314718055994531f, y + im);
 }
 
 // tanh, stable for large |Re z|
 QES_D float tanhx(float x) { return tanhf(x); }
 QES_D float2 tanhx(float2 z) {
-  const float ax = fabsf(z.x);
-  const float q = expf(-2.f * ax);
-  float sn, cs;
-  sincosf(2.f * z.y, &sn, &cs);
-  const float den = 1.f + q * q + 2.f * q * cs;
-  const float re = copysignf(1.f - q * q, z.x) / den;
-  const float im = 2.f * q * sn / den;
+  // tanh(x+iy) = [sign(x)(1 - q^2) + i 4 q sin y cos y] / [(1 - q)^2 + 4 q cos^2 y],
+  // q = exp(-2|x|); both forms avoid cancellation near the poles (x = 0, cos y = 0)
+  const float em = expm1f(-2.f * fabsf(z.x));      // q - 1
+  const float q = 1.f + em;
+  float sy, cy;
+  sincosf(z.y, &sy, &cy);
+  const float den = em * em + 4.f * q * cy * cy;
+  const float re = copysignf(-em * (2.f + em), z.x) / den;
+  const float im = 4.f * q * sy * cy / den;
   return make_float2(re, im);
 }
 

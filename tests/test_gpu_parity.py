@@ -68,8 +68,12 @@ def test_forward_matches_oracle(cplx, ns, nh):
     p = oracle_params(net)
     sig = orbm.to_sigma(st)
     th_ref = orbm.theta(p, sig)
-    assert rel_err(th.cpu().numpy(), th_ref) < RTOL
-    assert rel_err(tn.cpu().numpy(), np.tanh(th_ref)) < RTOL
+    th_g = th.cpu().numpy()
+    assert rel_err(th_g, th_ref) < RTOL
+    # tanh is checked on the kernel's own theta: near the poles of complex tanh
+    # (Im theta ~ pi/2) any float32 rounding of theta is amplified by sech^2
+    t64 = np.tanh(th_g.astype(np.complex128 if cplx else np.float64))
+    assert np.max(np.abs(tn.cpu().numpy() - t64) / np.maximum(1.0, np.abs(t64))) < RTOL
     wrap_close(lp.cpu().numpy(), orbm.log_psi(p, sig))
 
 
@@ -264,9 +268,9 @@ def test_sampler_exchange_trajectory_matches_oracle(cplx):
 def test_sampler_matches_exact_distribution(rule):
     ns = 10
     L = qb.SquareLattice(1, ns)
-    net = RBM((ns,), n_hidden=10, dtype="complex64", seed=12, init_scale=0.5)
+    net = RBM((ns,), n_hidden=10, dtype="complex64", seed=12, init_scale=0.25)
     n_up = ns // 2 if rule == "EXCHANGE" else None
-    smp = _gpu_sampler(net, rule, ns, 2048, seed=3, therm=4, sweep=10, lattice=L,
+    smp = _gpu_sampler(net, rule, ns, 2048, seed=3, therm=20, sweep=20, lattice=L,
                        init="RND_FIXED" if rule == "EXCHANGE" else None, n_up=n_up)
     bits, _ = smp.sample_bits(num_samples=40)
     st = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
@@ -274,7 +278,23 @@ def test_sampler_matches_exact_distribution(rule):
     basis, w = osm.exact_distribution(oracle_params(net), ns, n_up=n_up)
     hist = np.bincount(ints, minlength=1 << ns)[basis] / len(ints)
     tv = 0.5 * np.abs(hist - w).sum()
+    # multinomial noise of 81920 samples over 252 / 1024 states is ~0.01-0.02
     assert tv < 0.03, tv
+
+
+def test_sampler_exchange_process_matches_oracle_histogram():
+    """Short, unthermalised exchange chains: GPU and oracle run the same Markov process."""
+    ns = 10
+    L, OL = qb.SquareLattice(1, ns), olat.SquareLattice(1, ns)
+    net = RBM((ns,), n_hidden=10, dtype="complex64", seed=12, init_scale=0.5)
+    smp = _gpu_sampler(net, "EXCHANGE", ns, 512, seed=3, therm=4, sweep=10, lattice=L, init="RND_FIXED", n_up=5)
+    bits, _ = smp.sample_bits(num_samples=20)
+    got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
+    ref = osm.MetropolisSampler(ns, 512, rule="EXCHANGE", neighbor_table=olat.neighbor_table(OL), seed=3,
+                                therm_steps=4, sweep_steps=10, init="RND_FIXED", n_up=5)
+    cfg, _, _ = ref.sample(oracle_params(net), 20)
+    frac = np.mean(np.any(got != cfg, axis=1))
+    assert frac <= 0.02, frac
 
 
 def test_sampler_continues_chains_without_rethermalising():

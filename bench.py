@@ -1,0 +1,403 @@
+"""Benchmark of one RBM-VMC step (sample -> E_loc -> SR -> update) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config heis10x10] [--impl ours|reference]
+
+Workload (default): Heisenberg XXX on the 10x10 periodic square lattice in
+the Sz = 0 sector (XXZ with jxy = jz = -1 in QES's literal sign convention,
+i.e. the antiferromagnet), complex64 RBM with alpha = 2 (M = 200, P = 20,300),
+init N(0, 0.01), 4096 chains x 4 samples = 16,384 samples per step, exchange
+moves, sweep_steps = N = 100 proposals between samples, SR with diagonal
+shift 1e-3 solved by CG (rtol 1e-8, maxiter 1000), Euler/SGD lr 0.01.
+One step = one VMC epoch: persistent sampler kernel, theta/tanh forward,
+fused local energy, float64 statistics, structured SR CG, float64 update.
+Synthetic data: random-init parameters and random Sz = 0 starting chains.
+
+value = samples/s of the whole job (N GPUs x 16,384 samples per step / time);
+vmc_steps_per_s is reported beside it.  With --gpus N > 1 every rank runs its
+own independent VMC (replicas, weak scaling, no collective on the data path).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "VMC steps/s & samples/s: mixed+batched vs plain FP32 on B200 at equal ΔE vs ED"
+
+CONFIGS = {
+    # name: (dim, lx, ly, model, coupling kwargs, alpha, dtype, chains, samples, rule, sweep, shift, lr, cg rtol)
+    "heis10x10": dict(dim=2, lx=10, ly=10, model="xxz", kw=dict(jxy=-1.0, jz=-1.0), alpha=2, dtype="complex64",
+                      chains=4096, samples=4, rule="EXCHANGE", sweep=100, shift=1e-3, lr=0.01, rtol=1e-8,
+                      maxiter=1000, init="RND_FIXED"),
+    "tfim16": dict(dim=1, lx=16, ly=1, model="tfim", kw=dict(j=1.0, hx=1.0, hz=0.0), alpha=1, dtype="float32",
+                   chains=16, samples=64, rule="LOCAL", sweep=16, shift=1e-3, lr=0.01, rtol=1e-8, maxiter=1000,
+                   init="RND"),
+    "j1j2_6x6": dict(dim=2, lx=6, ly=6, model="j1j2", kw=dict(J1=-1.0, J2=-0.5), alpha=4, dtype="complex64",
+                     chains=2048, samples=4, rule="EXCHANGE", sweep=36, shift=1e-3, lr=0.01, rtol=1e-8,
+                     maxiter=1000, init="RND_FIXED"),
+    "tfim20x20": dict(dim=2, lx=20, ly=20, model="tfim", kw=dict(j=1.0, hx=3.04, hz=0.0), alpha=4, dtype="float32",
+                      chains=4096, samples=4, rule="LOCAL", sweep=400, shift=1e-4, lr=0.01, rtol=1e-8, maxiter=1000,
+                      init="RND"),
+}
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------------------- our arm
+def build_nqs(cfg, seed):
+    import pyqusolver_b200 as qb
+    L = qb.SquareLattice(cfg["dim"], cfg["lx"], cfg["ly"], bc="pbc")
+    if cfg["model"] == "xxz":
+        model = qb.XXZ(L, **cfg["kw"])
+    elif cfg["model"] == "j1j2":
+        model = qb.J1J2Model(L, **cfg["kw"])
+    else:
+        model = qb.TransverseFieldIsing(L, **cfg["kw"])
+    nqs = qb.NQS("rbm", model, alpha=cfg["alpha"], dtype=cfg["dtype"], seed=seed, s_upd_fun=cfg["rule"],
+                 s_initstate=cfg["init"], nparticles=L.ns // 2, s_numchains=cfg["chains"],
+                 s_numsamples=cfg["samples"], s_therm_steps=1, s_sweep_steps=cfg["sweep"], s_seed=seed,
+                 init_scale=0.01)
+    from pyqusolver_b200.tdvp import TDVP
+    tdvp = TDVP(sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
+    return nqs, tdvp
+
+
+def timed_step(nqs, tdvp, cfg, ev):
+    """One VMC step with CUDA events between the phases (all on the current stream)."""
+    import torch
+    from pyqusolver_b200 import device as dv
+    net = nqs.net
+    ev[0].record()
+    bits, _ = nqs.sampler.sample_bits()
+    ev[1].record()
+    _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+    ev[2].record()
+    eloc = nqs.local_energy_bits(bits, tn)
+    ev[3].record()
+    st = dv.loss_stats(eloc)
+    ev[4].record()
+    x = tdvp.solve(net, bits, tn, eloc)
+    ev[5].record()
+    dv.param_update(net.flat, net.master, x, cfg["lr"])
+    net.bump()
+    ev[6].record()
+    return st, tdvp.last_info
+
+
+PHASES = ["sample", "forward", "local_energy", "stats", "sr_solve", "update"]
+
+
+def run_ours(args, cfg, rank, world, local_rank):
+    import torch
+    from pyqusolver_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    nqs, tdvp = build_nqs(cfg, seed=1234 + rank)
+    ns_per_step = cfg["chains"] * cfg["samples"]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
+    mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+    # warm-up (the first call thermalises the chains)
+    for _ in range(args.warmup):
+        timed_step(nqs, tdvp, cfg, mk())
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    _lib.launch_count(reset=True)
+    step_ms, phase_ms, cg_iters = [], {p: [] for p in PHASES}, []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        ev = mk()
+        timed_step(nqs, tdvp, cfg, ev)
+        torch.cuda.synchronize()
+        step_ms.append(ev[0].elapsed_time(ev[6]))
+        for k, p in enumerate(PHASES):
+            phase_ms[p].append(ev[k].elapsed_time(ev[k + 1]))
+        cg_iters.append(tdvp.last_info.get("iterations", 0))
+    launches = _lib.launch_count(reset=True)
+    clk = clocks.stop()
+    total_ms = float(np.sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * ns_per_step * args.steps / (total_ms / 1e3)
+    ms_step = total_ms / args.steps
+
+    # --- end to end through the public API with host buffers (params in, stats + params out)
+    e2e = run_e2e(nqs, cfg, args, dist, world)
+
+    # --- roofline of the dominant kernel (measured live over the timed steps)
+    roof = roofline(cfg, nqs, phase_ms, cg_iters)
+
+    stats = tdvp.last_info
+    line = {
+        "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "vmc_steps_per_s": 1e3 / ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (random-init RBM, random Sz=0 chains)",
+        "config": {"workload": args.config, "lattice": f"{cfg['lx']}x{cfg['ly']} pbc", "model": cfg["model"],
+                   "couplings": cfg["kw"], "alpha": cfg["alpha"], "param_dtype": cfg["dtype"],
+                   "n_params": nqs.net.n_params, "chains": cfg["chains"], "samples_per_chain": cfg["samples"],
+                   "samples_per_step": ns_per_step, "update": cfg["rule"], "sweep_steps": cfg["sweep"],
+                   "sr": f"structured CG fp64, shift {cfg['shift']}, rtol {cfg['rtol']}, maxiter {cfg['maxiter']}",
+                   "lr": cfg["lr"], "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "phase_ms": {p: float(np.mean(v)) for p, v in phase_ms.items()},
+        "cg_iterations_mean": float(np.mean(cg_iters)),
+        "energy_mean_last": float(nqs_energy(stats)),
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "e2e": e2e,
+        "roofline": roof,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def nqs_energy(info):
+    e = info.get("e_mean", 0.0) if isinstance(info, dict) else 0.0
+    return np.real(e)
+
+
+def run_e2e(nqs, cfg, args, dist, world):
+    import torch
+    net = nqs.net
+    host_in = torch.empty_like(net.master, device="cpu").pin_memory()
+    host_in.copy_(net.master.cpu())
+    host_out = torch.empty_like(host_in).pin_memory()
+    host_stats = torch.empty(4, dtype=torch.float64).pin_memory()
+    from pyqusolver_b200.tdvp import TDVP
+    tdvp = TDVP(sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
+    from pyqusolver_b200 import device as dv
+    times = []
+    for _ in range(args.steps):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        net.master.copy_(host_in, non_blocking=True)          # H2D: the step's parameters
+        net.flat.copy_(net.master)
+        net.bump()
+        info = nqs.train_step(lr=cfg["lr"], tdvp=tdvp)          # public API (reads the energy back)
+        host_out.copy_(net.master, non_blocking=True)          # D2H: updated parameters
+        e.record()
+        torch.cuda.synchronize()
+        times.append(s.elapsed_time(e))
+    total = float(np.sum(times))
+    if dist is not None:
+        t = torch.tensor([total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    nbytes = host_in.numel() * host_in.element_size()
+    return {"value": world * cfg["chains"] * cfg["samples"] * args.steps / (total / 1e3), "unit": "samples/s",
+            "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes + 32),
+            "ms_per_step": total / args.steps}
+
+
+def roofline(cfg, nqs, phase_ms, cg_iters):
+    """Roofline of the dominant phase's kernel from the live CUDA-event times."""
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    src = "measured" if "hbm_gbs" in peaks else "fallback"
+    net = nqs.net
+    ns, nh, n = net.ns, net.nh, cfg["chains"] * cfg["samples"]
+    cplx = net.is_complex
+    ts = 8 if cplx else 4
+    mean = {p: float(np.mean(v)) for p, v in phase_ms.items()}
+    dom = max(mean, key=mean.get)
+    out = {"dominant_phase": dom}
+    if dom == "sr_solve":
+        # per CG iteration the matvec streams the packed spins and T = tanh(theta) twice
+        # (O v, then O^H u) plus the float64 vectors; algorithmic bytes per matvec:
+        it = max(1.0, float(np.mean(cg_iters)))
+        nw = (ns + 31) // 32
+        P = ns + nh + ns * nh
+        bytes_mv = 2 * (n * nh * ts + n * nw * 4) + 6 * P * (16 if cplx else 8)
+        t = mean["sr_solve"] / 1e3 / (it + 1)
+        ach = bytes_mv / t / 1e9
+        out.update({"kernel": "sr matvec (ov + ohu)", "bound": "hbm", "achieved": ach, "peak": hbm,
+                    "unit": "GB/s", "frac": ach / hbm, "traffic": None, "peak_source": src,
+                    "algorithmic_bytes_per_launch": bytes_mv})
+    elif dom == "sample":
+        nrec = cfg["samples"] * cfg["sweep"]
+        # per proposal and chain: one table row pair (C, S) of M entries
+        bytes_ = cfg["chains"] * nrec * 2 * nh * ts
+        t = mean["sample"] / 1e3
+        ach = bytes_ / t / 1e9
+        out.update({"kernel": "sampler_kernel", "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                    "frac": ach / hbm, "traffic": None, "peak_source": src,
+                    "algorithmic_bytes_per_launch": bytes_})
+    else:
+        t = mean[dom] / 1e3
+        bytes_ = n * nh * ts
+        ach = bytes_ / t / 1e9
+        out.update({"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                    "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": bytes_})
+    return out
+
+
+# ---------------------------------------------------------------------------------------- CPU (oracle)
+def oracle_setup(cfg, n_chains, seed=0):
+    from oracle import lattice as olat, hamiltonian as oH, rbm as orbm, sampler as osm
+    L = olat.SquareLattice(cfg["dim"], cfg["lx"], cfg["ly"], bc="pbc")
+    if cfg["model"] == "xxz":
+        terms = oH.xxz_terms(L, **cfg["kw"])
+    elif cfg["model"] == "j1j2":
+        terms = oH.j1j2_terms(L, **cfg["kw"])
+    else:
+        terms = oH.tfim_terms(L, **cfg["kw"])
+    ns = L.ns
+    p = orbm.random_params(ns, cfg["alpha"] * ns, complex_=cfg["dtype"].startswith("complex"), scale=0.01, seed=seed)
+    smp = osm.MetropolisSampler(ns, n_chains, rule=cfg["rule"], neighbor_table=olat.neighbor_table(L), seed=seed,
+                                therm_steps=1, sweep_steps=cfg["sweep"],
+                                init=cfg["init"], n_up=ns // 2)
+    smp.needs_therm = False        # throughput only: thermalisation is not part of a steady-state step
+    return p, terms, smp
+
+
+def cpu_step(cfg, p, terms, smp):
+    from oracle import vmc as ovmc
+    return ovmc.vmc_step(p, terms, smp, cfg["samples"], lr=cfg["lr"], shift=cfg["shift"], rtol=cfg["rtol"],
+                         maxiter=cfg["maxiter"])
+
+
+def cpu_baseline(cfg, budget_s=20.0):
+    """The oracle (float64 NumPy restatement of the reference's algorithm) on the host cores."""
+    n_chains = 16
+    p, terms, smp = oracle_setup(cfg, n_chains)
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        p, _ = cpu_step(cfg, p, terms, smp)
+        steps += 1
+        if time.perf_counter() - t0 > budget_s or steps >= 3:
+            break
+    dt = time.perf_counter() - t0
+    samples = steps * n_chains * cfg["samples"]
+    return {"value": samples / dt, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{steps} VMC step(s) of {n_chains} chains x {cfg['samples']} samples (same per-sample "
+                      f"algorithm as the reference: full RBM re-evaluation per connected state and per exchange "
+                      f"proposal, float64 NumPy/OpenBLAS)"}
+
+
+def run_reference(args, cfg, rank, world):
+    if rank != 0:
+        return
+    n_chains = 16
+    p, terms, smp = oracle_setup(cfg, n_chains)
+    for _ in range(args.warmup):
+        p, _ = cpu_step(cfg, p, terms, smp)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        p, _ = cpu_step(cfg, p, terms, smp)
+    dt = time.perf_counter() - t0
+    samples = args.steps * n_chains * cfg["samples"]
+    v = samples / dt
+    sample_desc = (f"each step {n_chains} chains x {cfg['samples']} samples of the {args.config} workload "
+                   f"(bounded sample), oracle port of the reference algorithm on {os.cpu_count()} host threads")
+    line = {"metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": args.config, "samples_per_step": n_chains * cfg["samples"]},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": sample_desc},
+            "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="heis10x10", choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, world, local_rank = env_rank()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg, rank, world)
+    else:
+        run_ours(args, cfg, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

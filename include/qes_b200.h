@@ -58,6 +58,9 @@ extern "C" {
 const char* qes_last_error(void);
 /* Library version: 100*major + minor. */
 int qes_version(void);
+/* Number of kernels this library launched in the process (reset != 0 zeroes
+ * the counter after reading).  Host-side bookkeeping only. */
+long long qes_launch_count(int reset);
 
 /* ------------------------------------------------------------------------ */
 /* Initial chain states.

@@ -76,6 +76,7 @@ class SRResult(C.Structure):
 SIGNATURES = {
     "qes_last_error": [],
     "qes_version": [],
+    "qes_launch_count": [C.c_int],
     "qes_init_chains": [C.c_int, C.c_int, _u64, _i64, C.c_int, C.c_int, _vp, _vp],
     "qes_rbm_move_tables": [C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp],
     "qes_rbm_forward": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
@@ -110,7 +111,7 @@ def load(path: str = LIB_PATH):
     for name, argt in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = argt
-        fn.restype = C.c_char_p if name == "qes_last_error" else C.c_int
+        fn.restype = {"qes_last_error": C.c_char_p, "qes_launch_count": C.c_longlong}.get(name, C.c_int)
     _LIB = lib
     return lib
 
@@ -127,6 +128,10 @@ def call(name, *args, allow=()):
     if rc != QES_OK and rc not in allow:
         check(rc)
     return rc
+
+
+def launch_count(reset=False) -> int:
+    return int(load().qes_launch_count(1 if reset else 0))
 
 
 def ptr(t):

@@ -21,14 +21,19 @@
     if (_e != cudaSuccess) { qes_set_last_error(_e, #expr); return QES_ERR_CUDA; } \
   } while (0)
 
-#define QES_LAUNCH_CHECK()                                     \
+// Every kernel launch is followed by QES_LAUNCH_CHECK_N(number of launches
+// since the last check); the count feeds qes_launch_count().
+#define QES_LAUNCH_CHECK_N(n)                                  \
   do {                                                         \
+    qes_count_launches(n);                                     \
     cudaError_t _e = cudaGetLastError();                       \
     if (_e != cudaSuccess) { qes_set_last_error(_e, "kernel launch"); return QES_ERR_CUDA; } \
   } while (0)
+#define QES_LAUNCH_CHECK() QES_LAUNCH_CHECK_N(1)
 
 void qes_set_last_error(cudaError_t e, const char* what);
 void qes_set_last_message(const char* msg);
+void qes_count_launches(int n);
 
 // ----------------------------------------------------------------------------
 // scalar algebra on float / float2

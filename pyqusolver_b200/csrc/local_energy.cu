@@ -256,6 +256,6 @@ extern "C" int qes_loss_stats(int64_t n_samples, const void* eloc, const float* 
   stats_mean<<<1, 32, 0, st>>>(STATS_BLOCKS, n_samples, part, out);
   stats_pass2<<<STATS_BLOCKS, STATS_THREADS, 0, st>>>(n_samples, (const float2*)eloc, probs, out, part);
   stats_final<<<1, 32, 0, st>>>(STATS_BLOCKS, n_samples, part, out);
-  QES_LAUNCH_CHECK();
+  QES_LAUNCH_CHECK_N(4);
   return QES_OK;
 }

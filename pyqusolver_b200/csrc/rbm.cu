@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <atomic>
 
 static thread_local char g_last_error[512] = "";
 
@@ -13,7 +14,13 @@ void qes_set_last_error(cudaError_t e, const char* what) {
 }
 void qes_set_last_message(const char* msg) { snprintf(g_last_error, sizeof(g_last_error), "%s", msg); }
 
+static std::atomic<long long> g_launches{0};
+void qes_count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 extern "C" const char* qes_last_error(void) { return g_last_error; }
+extern "C" long long qes_launch_count(int reset) {
+  return reset ? g_launches.exchange(0) : g_launches.load();
+}
 extern "C" int qes_version(void) { return 100; }
 
 #define QES_ARG_CHECK(cond, msg) do { if (!(cond)) { qes_set_last_message(msg); return QES_ERR_ARG; } } while (0)

@@ -515,7 +515,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p);
   norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
   cg_setup_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
-  QES_LAUNCH_CHECK();
+  QES_LAUNCH_CHECK_N(3);
   const int check = opt->check_every > 0 ? opt->check_every : 8;
   double hs[8] = {0};
   int it = 0;
@@ -533,7 +533,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       cg_scalar_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, L.scal);
       cg_p_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, p, L.scal, 0);
       cg_rotate_kernel<<<1, 32, 0, st>>>(L.scal);
-      QES_LAUNCH_CHECK();
+      QES_LAUNCH_CHECK_N(5);
     }
     it += nrun;
     QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -542,8 +542,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   }
   // x_out = rhs_prefactor * x
   QES_CUDA_CHECK(cudaMemcpyAsync(x_out, x, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
-  if (opt->rhs_prefactor != 1.0) scale_vec_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, opt->rhs_prefactor, x_out);
-  QES_LAUNCH_CHECK();
+  if (opt->rhs_prefactor != 1.0) {
+    scale_vec_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, opt->rhs_prefactor, x_out);
+    QES_LAUNCH_CHECK();
+  }
   if (res) {
     res->iterations = (int)hs[5];
     res->converged = done ? 1 : 0;

@@ -165,6 +165,24 @@ int qes_local_energy(int dtype, int ns, int nh, int64_t n_samples,
                      const void* A, void* workspace, size_t workspace_bytes,
                      void* eloc_out, void* stream);
 
+/* Allocation-free variant of qes_local_energy -- no counterpart in the
+ * reference.  For callers that cannot allocate device memory (a fixed device
+ * budget handed over at start-up, loops that cannot afford cudaMalloc's
+ * implicit synchronisation, foreign-language hosts without a device
+ * allocator): the scratch lives in a static 8 MiB device array inside the
+ * library, resident on every GPU that loads it until process exit.
+ * Limit: ceil(n_moves/32) * n_samples * 8 bytes <= QES_NOALLOC_ELOC_SCRATCH_BYTES,
+ * else QES_ERR_SIZE.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) and caches it; make that first call
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race on it.  Calls no cudaMalloc/cudaFree.                      */
+#define QES_NOALLOC_ELOC_SCRATCH_BYTES (8u << 20)
+int qes_local_energy_noalloc(int dtype, int ns, int nh, int64_t n_samples,
+                             const uint32_t* bits, const void* tanh_theta,
+                             const qes_hamiltonian* ham, const void* Ct,
+                             const void* St, const void* A, void* eloc_out,
+                             void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Energy statistics in float64 (compensated): out = [mean_re, mean_im, var, std]
  * with weights probs (NULL = uniform).  Replaces the mean/std of

@@ -85,6 +85,8 @@ SIGNATURES = {
     "qes_local_energy_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.c_int, C.POINTER(_sz)],
     "qes_local_energy": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.POINTER(Hamiltonian), _vp, _vp, _vp, _vp,
                          _sz, _vp, _vp],
+    "qes_local_energy_noalloc": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.POINTER(Hamiltonian), _vp, _vp, _vp,
+                                 _vp, _vp],
     "qes_loss_stats_workspace_bytes": [_i64, C.POINTER(_sz)],
     "qes_loss_stats": [_i64, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_rbm_log_derivatives": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _i64, _vp],

@@ -259,3 +259,73 @@ extern "C" int qes_loss_stats(int64_t n_samples, const void* eloc, const float* 
   QES_LAUNCH_CHECK_N(4);
   return QES_OK;
 }
+
+// ----------------------------------------------------------------------------
+// Allocation-free local energy.
+//
+// Some callers cannot allocate device memory at all: hosts that hand this
+// library a fixed device budget at start-up and forbid cudaMalloc afterwards,
+// latency-critical loops where cudaMalloc's implicit device synchronisation is
+// not acceptable, and foreign-language bindings (cgo, JNI, plain C) that have
+// no allocator of their own to hand out scratch buffers.  For them this entry
+// point keeps the local energy's only scratch -- one float2 partial sum per
+// (32-move block, sample) -- in a fixed array compiled into the library.
+//
+// The array lives in every GPU that loads the library until the process
+// exits.  The host never dereferences the symbol itself: the array's device
+// address is looked up with cudaGetSymbolAddress on the first call made on
+// each device (with that device current) and cached, so that first call per
+// device should come before any stream capture.  All calls share the one
+// array: each call overwrites the part it reads before reading it, so no
+// clearing is needed, but calls that overlap on the GPU (several streams or
+// host threads at once) race on it and must be serialised by the caller.
+// ----------------------------------------------------------------------------
+#include <mutex>
+
+static __device__ __align__(256) float2 g_eloc_noalloc_scratch[QES_NOALLOC_ELOC_SCRATCH_BYTES / sizeof(float2)];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+}  // namespace
+
+static int eloc_noalloc_scratch(void** out) {
+  int dev = -1;
+  QES_CUDA_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    qes_set_last_message("qes_local_energy_noalloc: device ordinal beyond the supported 64");
+    return QES_ERR_SIZE;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_eloc_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      qes_set_last_error(e, "qes_local_energy_noalloc: cudaGetSymbolAddress of the static scratch");
+      return QES_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return QES_OK;
+}
+
+extern "C" int qes_local_energy_noalloc(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                        const void* tanh_theta, const qes_hamiltonian* ham, const void* Ct,
+                                        const void* St, const void* A, void* eloc_out, void* stream) {
+  QES_ARG_CHECK(ham != nullptr && ns > 0 && nh > 0 && n_samples >= 0, "qes_local_energy_noalloc: bad sizes");
+  size_t need = 0;
+  const int rc0 = qes_local_energy_workspace_bytes(dtype, ns, nh, n_samples, ham->n_moves, &need);
+  if (rc0 != QES_OK) return rc0;
+  if (need > (size_t)QES_NOALLOC_ELOC_SCRATCH_BYTES) {
+    qes_set_last_message("qes_local_energy_noalloc: ceil(n_moves/32) * n_samples * 8 bytes exceeds the "
+                         "8 MiB static scratch; use qes_local_energy with a caller workspace");
+    return QES_ERR_SIZE;
+  }
+  void* scratch = nullptr;
+  const int rc = eloc_noalloc_scratch(&scratch);
+  if (rc != QES_OK) return rc;
+  return qes_local_energy(dtype, ns, nh, n_samples, bits, tanh_theta, ham, Ct, St, A, scratch,
+                          (size_t)QES_NOALLOC_ELOC_SCRATCH_BYTES, eloc_out, stream);
+}

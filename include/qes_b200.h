@@ -226,6 +226,15 @@ typedef struct {
 
 int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
 
+/* Matvec implementation of the SR calls in this process: 0 = 5th-generation
+ * tensor cores (tcgen05, BF16 hi/lo split, FP32 accumulate) when ns <= 128,
+ * nh <= 256 and the operands fit shared memory, CUDA cores otherwise
+ * (default); 1 = CUDA cores only; 2 = tensor cores required (QES_ERR_SIZE
+ * when the shapes do not allow them).  No counterpart in the reference
+ * (its SR runs on XLA).  qes_sr_force / qes_sr_matvec synchronise the stream
+ * when the tensor-core path ran, to report bounded-wait time-outs.          */
+int qes_set_sr_impl(int impl);
+
 /* F = O_c^H E_c / Ns (force) and the matvec y = (O_c^H O_c / Ns + shift) v. */
 int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples,
                  const uint32_t* bits, const void* tanh_theta, const void* eloc,

@@ -91,6 +91,7 @@ SIGNATURES = {
     "qes_loss_stats": [_i64, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_rbm_log_derivatives": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _i64, _vp],
     "qes_sr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
+    "qes_set_sr_impl": [C.c_int],
     "qes_sr_force": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_sr_matvec": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.c_double, _vp, _vp, _vp, _sz, _vp],
     "qes_sr_solve_cg": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
@@ -130,6 +131,13 @@ def call(name, *args, allow=()):
     if rc != QES_OK and rc not in allow:
         check(rc)
     return rc
+
+
+SR_IMPL_AUTO, SR_IMPL_CUDA_CORES, SR_IMPL_TENSOR_CORES = 0, 1, 2
+
+
+def set_sr_impl(impl: int):
+    call("qes_set_sr_impl", int(impl))
 
 
 def launch_count(reset=False) -> int:

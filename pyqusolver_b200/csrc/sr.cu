@@ -13,8 +13,21 @@
 // atol); the device freezes x at the first iteration that meets it, so the
 // result does not depend on how often the host checks.
 #include "common.cuh"
+#include "sr_tc.h"
 
 #include <algorithm>
+#include <atomic>
+
+// 0 = tensor cores when the shapes allow it, 1 = CUDA cores only, 2 = tensor cores required
+static std::atomic<int> g_sr_impl{0};
+extern "C" int qes_set_sr_impl(int impl) {
+  if (impl < 0 || impl > 2) {
+    qes_set_last_message("qes_set_sr_impl: impl must be 0 (auto), 1 (cuda cores) or 2 (tensor cores)");
+    return QES_ERR_ARG;
+  }
+  g_sr_impl.store(impl);
+  return QES_OK;
+}
 
 #define QES_ARG_CHECK(cond, msg) do { if (!(cond)) { qes_set_last_message(msg); return QES_ERR_ARG; } } while (0)
 
@@ -377,6 +390,10 @@ struct SRWork {
   void* x; void* r; void* p; void* Ap; void* b;   // [P] of V each
   double* parts;      // [RED_BLOCKS]
   double* scal;       // [8]
+  bool tc;            // tensor-core matvec in use
+  TcDims td;
+  TcWork tw;
+  int nsplit;         // partial P-vectors written by the O^H u stage
   size_t total;
 };
 
@@ -386,16 +403,24 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   const size_t ts = (dtype == QES_DTYPE_C64) ? sizeof(float2) : sizeof(float);
   const size_t vs = (dtype == QES_DTYPE_C64) ? sizeof(double2) : sizeof(double);
-  const int64_t nsplit = (n_samples + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES;
+  const int64_t nsplit_simt = (n_samples + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES;
   SRWork L;
+  L.td = TcDims{};
+  const bool tc_ok = tc_plan(dtype, ns, nh, n_samples, &L.td);
+  const int impl = g_sr_impl.load();
+  L.tc = tc_ok && impl != 1;
+  const int64_t nsplit_max = std::max<int64_t>(nsplit_simt, tc_ok ? L.td.n_chunks : 1);
+  L.nsplit = (int)(L.tc ? L.td.n_chunks : nsplit_simt);
   size_t off = 0;
   auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off += align256(bytes); return p; };
   L.w = (float2*)take((size_t)n_samples * sizeof(float2));
   L.wmean = (double*)take(4 * sizeof(double));
-  L.partial = take((size_t)std::max<int64_t>(nsplit, 1) * P * ts);
+  L.partial = take((size_t)std::max<int64_t>(nsplit_max, 1) * P * ts);
   L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
   L.parts = (double*)take(RED_BLOCKS * sizeof(double));
   L.scal = (double*)take(8 * sizeof(double));
+  char* tcb = tc_ok ? take(tc_workspace_bytes(L.td)) : nullptr;
+  L.tw = (tc_ok && base) ? tc_layout(L.td, tcb) : TcWork{};
   L.total = off;
   return L;
 }
@@ -444,6 +469,17 @@ static int sr_force_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, c
   using V = typename VecT<T>::type;
   mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, eloc, L.wmean);
   QES_LAUNCH_CHECK();
+  if (L.tc) {
+    const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
+    int rc = tc_ohu(dtype, L.td, n_samples, bits, tt, eloc, (const double2*)L.wmean, -1, 1.0 / (double)n_samples,
+                    L.partial, L.tw, st);
+    if (rc) return rc;
+    const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+    reduce_splits_kernel<T, V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, L.nsplit, (const T*)L.partial, 0.0, nullptr, F,
+                                                                   nullptr);
+    QES_LAUNCH_CHECK();
+    return QES_OK;
+  }
   return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, eloc, L.wmean, 1.0 / (double)n_samples, L, 0.0, nullptr, F,
                          nullptr, st);
 }
@@ -454,8 +490,16 @@ static int check_ws(int dtype, int ns, int nh, int64_t n_samples, void* ws, size
     qes_set_last_message("SR: workspace too small");
     return QES_ERR_WORKSPACE;
   }
+  if (g_sr_impl.load() == 2 && !L->tc) {
+    qes_set_last_message("SR: tensor-core path required but the shapes are outside its limits "
+                         "(ns <= 128, nh <= 256, shared-memory budget)");
+    return QES_ERR_SIZE;
+  }
   return QES_OK;
 }
+
+static int sr_prepare(int64_t n_samples, const uint32_t* bits, const SRWork& L, cudaStream_t st);
+static int sr_check_status(const SRWork& L, cudaStream_t st);
 
 extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
                             const void* tanh_theta, const void* eloc, void* force_out, void* workspace,
@@ -466,11 +510,16 @@ extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const 
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  rc = sr_prepare(n_samples, bits, L, st);
+  if (rc) return rc;
   if (dtype == QES_DTYPE_F32)
-    return sr_force_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc,
-                             (double*)force_out, L, st);
-  return sr_force_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc,
+    rc = sr_force_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc,
+                           (double*)force_out, L, st);
+  else
+    rc = sr_force_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc,
                             (double2*)force_out, L, st);
+  if (rc) return rc;
+  return sr_check_status(L, st);
 }
 
 template <class T>
@@ -478,10 +527,38 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
                        const typename VecT<T>::type* v, typename VecT<T>::type* y, double* dot_part, const SRWork& L,
                        cudaStream_t st) {
   using V = typename VecT<T>::type;
+  if (L.tc) {
+    const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
+    int rc = tc_matvec(dtype, L.td, n_samples, bits, tt, v, L.w, L.partial, L.tw, st);
+    if (rc) return rc;
+    const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+    reduce_splits_kernel<T, V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, L.nsplit, (const T*)L.partial, shift, v, y,
+                                                                   dot_part);
+    QES_LAUNCH_CHECK();
+    return QES_OK;
+  }
   int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, st);
   if (rc) return rc;
   return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples, L, shift, v, y,
                          dot_part, st);
+}
+
+// per-step operands of the tensor-core path (spins as BF16 tiles) and the status word
+static int sr_prepare(int64_t n_samples, const uint32_t* bits, const SRWork& L, cudaStream_t st) {
+  if (!L.tc) return QES_OK;
+  return tc_prepare_step(L.td, n_samples, bits, L.tw, st);
+}
+
+static int sr_check_status(const SRWork& L, cudaStream_t st) {
+  if (!L.tc) return QES_OK;
+  int h = 0;
+  QES_CUDA_CHECK(cudaMemcpyAsync(&h, L.tw.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaStreamSynchronize(st));
+  if (h != 0) {
+    qes_set_last_message("SR tensor-core matvec: a bounded device wait gave up");
+    return QES_ERR_TIMEOUT;
+  }
+  return QES_OK;
 }
 
 extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
@@ -493,11 +570,16 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  rc = sr_prepare(n_samples, bits, L, st);
+  if (rc) return rc;
   if (dtype == QES_DTYPE_F32)
-    return sr_matvec_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, shift, (const double*)v,
-                              (double*)y_out, nullptr, L, st);
-  return sr_matvec_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, shift, (const double2*)v,
+    rc = sr_matvec_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, shift, (const double*)v,
+                            (double*)y_out, nullptr, L, st);
+  else
+    rc = sr_matvec_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, shift, (const double2*)v,
                              (double2*)y_out, nullptr, L, st);
+  if (rc) return rc;
+  return sr_check_status(L, st);
 }
 
 template <class T>
@@ -507,8 +589,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   using V = typename VecT<T>::type;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   V* x = (V*)L.x; V* r = (V*)L.r; V* p = (V*)L.p; V* Ap = (V*)L.Ap; V* b = (V*)L.b;
+  int rc = sr_prepare(n_samples, bits, L, st);
+  if (rc) return rc;
   // b = F
-  int rc = sr_force_t<T>(ns, nh, n_samples, bits, tt, eloc, b, L, st);
+  rc = sr_force_t<T>(ns, nh, n_samples, bits, tt, eloc, b, L, st);
   if (rc) return rc;
   double emean[2] = {0, 0};
   QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -537,7 +621,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     }
     it += nrun;
     QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    QES_CUDA_CHECK(cudaStreamSynchronize(st));
+    rc = sr_check_status(L, st);          // synchronises the stream
+    if (rc) return rc;
     done = hs[4] != 0.0;
   }
   // x_out = rhs_prefactor * x

@@ -317,3 +317,52 @@ def test_nqs_training_tfim_reaches_ed():
     stats = nqs.train(n_epochs=150, lr=0.05, diag_shift=1e-3)
     tail = np.mean([h.real for h in stats.history[-10:]])
     assert abs(tail - e0) / abs(e0) < 5e-3, (tail, e0)
+
+
+# ------------------------------------------------------------------------- tensor-core SR matvec
+@pytest.fixture
+def sr_impl():
+    yield _lib.set_sr_impl
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+
+
+@pytest.mark.parametrize("cplx,ns,nh,n", [(False, 16, 16, 300), (True, 9, 18, 700), (True, 36, 144, 1000),
+                                           (False, 20, 40, 513), (True, 100, 200, 300)])
+def test_sr_matvec_tensor_cores_match_oracle(sr_impl, cplx, ns, nh, n):
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=21, init_scale=0.1)
+    st = rand_states(n, ns, seed=22)
+    bits = dv.pack_states(st)
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    O = orbm.log_derivatives(oracle_params(net), orbm.to_sigma(st))
+    Oc = O - O.mean(0)
+    rng = np.random.default_rng(5)
+    v = rng.normal(size=O.shape[1]) + (1j * rng.normal(size=O.shape[1]) if cplx else 0)
+    ref = np.conj(Oc).T @ (Oc @ v) / n + 1e-3 * v
+    sr_impl(_lib.SR_IMPL_TENSOR_CORES)
+    y_tc = dv.sr_matvec(net.flat, ns, nh, bits, tn, torch.as_tensor(v).cuda(), shift=1e-3).cpu().numpy()
+    sr_impl(_lib.SR_IMPL_CUDA_CORES)
+    y_cc = dv.sr_matvec(net.flat, ns, nh, bits, tn, torch.as_tensor(v).cuda(), shift=1e-3).cpu().numpy()
+    assert rel_err(y_cc, ref) < 1e-4
+    assert rel_err(y_tc, ref) < 1e-4
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_sr_force_and_cg_tensor_cores_match_cuda_cores(sr_impl, cplx):
+    ns, nh, n = 16, 32, 2000
+    L = qb.SquareLattice(2, 4, 4)
+    model = qb.XXZ(L, jxy=-1.0, jz=-1.0, hx=0.3)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=23, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=24))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    out = {}
+    for impl in (_lib.SR_IMPL_CUDA_CORES, _lib.SR_IMPL_TENSOR_CORES):
+        sr_impl(impl)
+        F = dv.sr_force(net.flat, ns, nh, bits, tn, eloc).cpu().numpy()
+        x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-8, maxiter=1000)
+        assert info["converged"]
+        out[impl] = (F, x.cpu().numpy())
+    assert rel_err(out[2][0], out[1][0]) < 1e-4
+    assert rel_err(out[2][1], out[1][1]) < 1e-3

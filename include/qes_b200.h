@@ -234,6 +234,9 @@ int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t*
  * (its SR runs on XLA).  qes_sr_force / qes_sr_matvec synchronise the stream
  * when the tensor-core path ran, to report bounded-wait time-outs.          */
 int qes_set_sr_impl(int impl);
+/* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
+ * default) or launched one by one on the caller's stream (0).              */
+int qes_set_cg_graphs(int enable);
 
 /* F = O_c^H E_c / Ns (force) and the matvec y = (O_c^H O_c / Ns + shift) v. */
 int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples,

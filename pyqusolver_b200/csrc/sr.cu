@@ -234,56 +234,106 @@ __global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
   }
 }
 
-// sum the split partials in float64; optional  y = G + shift * p  and  dot partials of p^H y
+// sum the split partials in float64; optional  y = G + shift * p  and  dot partials of p^H y.
+// Block = 32 columns x 8 split groups: the 32 threads of a row read 32 consecutive
+// columns of one split (coalesced) and each thread sums only nsplit/8 partials.
 constexpr int RED_THREADS = 256;
-constexpr int RED_BLOCKS = 296;
+constexpr int RED_BLOCKS = 296;          // grid of the element-wise CG kernels
+constexpr int RS_TX = 32, RS_TY = 8;
+constexpr int RS_MAX_BLOCKS = 1184;      // upper bound of dot partials written by the reduction
 
 template <class T, class V>
-__global__ void __launch_bounds__(RED_THREADS) reduce_splits_kernel(int64_t P, int nsplit, const T* __restrict__ partial,
-                                                                    double shift, const V* __restrict__ p,
-                                                                    V* __restrict__ y, double* __restrict__ dot_part) {
+__global__ void __launch_bounds__(RS_TX * RS_TY) reduce_splits_kernel(int64_t P, int nsplit, const T* __restrict__ partial,
+                                                                      double shift, const V* __restrict__ p,
+                                                                      V* __restrict__ y, double* __restrict__ dot_part,
+                                                                      double* __restrict__ scal,
+                                                                      unsigned int* __restrict__ counter) {
+  __shared__ V red[RS_TY][RS_TX];
+  const int tx = threadIdx.x, ty = threadIdx.y;
   double d = 0.0;
-  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t c0 = (int64_t)blockIdx.x * RS_TX; c0 < P; c0 += (int64_t)gridDim.x * RS_TX) {
+    const int64_t k = c0 + tx;
     V g = vzero(V());
-    for (int z = 0; z < nsplit; ++z) g = vadd(g, to_d(partial[(int64_t)z * P + k]));
-    if (p) {
-      const V pk = p[k];
-      g = vadd(g, vscale(shift, pk));
-      d += vdotc(pk, g);
+    if (k < P) {
+#pragma unroll 4
+      for (int z = ty; z < nsplit; z += RS_TY) g = vadd(g, to_d(partial[(int64_t)z * P + k]));
     }
-    y[k] = g;
-  }
-  if (dot_part) {
-    __shared__ double red[RED_THREADS / 32];
-    d = warp_sum(d);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+    red[ty][tx] = g;
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double s = 0;
-      for (int q = 0; q < RED_THREADS / 32; ++q) s += red[q];
-      dot_part[blockIdx.x] = s;
+    if (ty == 0 && k < P) {
+      V t = red[0][tx];
+#pragma unroll
+      for (int q = 1; q < RS_TY; ++q) t = vadd(t, red[q][tx]);
+      if (p) {
+        const V pk = p[k];
+        t = vadd(t, vscale(shift, pk));
+        d += vdotc(pk, t);
+      }
+      y[k] = t;
     }
+    __syncthreads();
+  }
+  if (!dot_part) return;
+  if (ty == 0) {                       // row 0 is warp 0
+    d = warp_sum(d);
+    if (tx == 0) dot_part[blockIdx.x] = d;
+  }
+  if (!scal) return;
+  // the last block to finish sums the dot partials: pAp and alpha = rr / pAp
+  __shared__ bool last;
+  __threadfence();
+  if (tx == 0 && ty == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ double sred[RS_TX * RS_TY / 32];
+  const int tid = ty * RS_TX + tx;
+  double v = 0.0;
+  for (int q = tid; q < (int)gridDim.x; q += RS_TX * RS_TY) v += ((volatile double*)dot_part)[q];
+  v = warp_sum(v);
+  if ((tid & 31) == 0) sred[tid >> 5] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double pap = 0.0;
+    for (int q = 0; q < RS_TX * RS_TY / 32; ++q) pap += sred[q];
+    scal[1] = pap;
+    scal[7] = (scal[4] == 0.0 && pap > 0.0) ? scal[0] / pap : 0.0;
+    *counter = 0u;
   }
 }
 
+static int reduce_blocks(int64_t P) {
+  return (int)std::min<int64_t>((P + RS_TX - 1) / RS_TX, RS_MAX_BLOCKS);
+}
+
 // ----------------------------------------------------------------------------
-// CG state on the device: scal[0] = rr, [1] = pAp, [2] = rr_new, [3] = thresh^2,
-// [4] = done flag, [5] = iterations (as double), [6] = ||b||^2
+// CG state on the device (float64):
+//   scal[0] rr   scal[1] pAp   scal[2] rr_new   scal[3] threshold^2   scal[4] done
+//   scal[5] iterations   scal[6] ||b||^2   scal[7] alpha   scal[8] beta
+// Partial sums are reduced by one block of 1024 threads in a fixed order.
 // ----------------------------------------------------------------------------
-__global__ void sum_parts_kernel(int n, const double* __restrict__ parts, double* __restrict__ dst) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double s = 0;
-  for (int q = 0; q < n; ++q) s += parts[q];
-  *dst = s;
+constexpr int SC_THREADS = 1024;
+
+__device__ __forceinline__ double block_sum_parts(int n, const double* __restrict__ parts) {
+  __shared__ double red[SC_THREADS / 32];
+  double v = 0.0;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) v += parts[q];
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+  return t;                                // valid in thread 0
 }
 
 template <class V>
 __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* __restrict__ p, const V* __restrict__ Ap,
                                                             V* __restrict__ x, V* __restrict__ r,
-                                                            const double* __restrict__ scal, double* __restrict__ rr_part) {
+                                                            double* __restrict__ scal, double* __restrict__ rr_part,
+                                                            unsigned int* __restrict__ counter) {
   const bool done = scal[4] != 0.0;
-  const double pap = scal[1];
-  const double alpha = (pap > 0.0 && !done) ? scal[0] / pap : 0.0;
+  const double alpha = scal[7];
   double d = 0.0;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
     V rk = r[k];
@@ -303,36 +353,53 @@ __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* 
     for (int q = 0; q < RED_THREADS / 32; ++q) s += red[q];
     rr_part[blockIdx.x] = s;
   }
+  // the last block to finish: rr_new, convergence, beta = rr_new / rr, rr <- rr_new
+  __shared__ bool last;
+  __threadfence();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) v += ((volatile double*)rr_part)[q];
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double rr_new = 0.0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) rr_new += red[q];
+    if (scal[4] == 0.0) {
+      scal[2] = rr_new;
+      scal[5] += 1.0;
+      scal[8] = (scal[0] > 0.0) ? rr_new / scal[0] : 0.0;
+      scal[0] = rr_new;
+      if (rr_new <= scal[3]) scal[4] = 1.0;
+    }
+    *counter = 0u;
+  }
 }
 
-// rr_new = sum parts; convergence test; beta; iteration count
-__global__ void cg_scalar_kernel(int n, const double* __restrict__ parts, double* __restrict__ scal) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  if (scal[4] != 0.0) return;
-  double s = 0;
-  for (int q = 0; q < n; ++q) s += parts[q];
-  scal[2] = s;
-  scal[5] += 1.0;
-  if (s <= scal[3]) scal[4] = 1.0;
-}
-
+// p = r + beta p; on the tensor-core path also rewrite the V' operand tiles of the new p
 template <class V>
 __global__ void __launch_bounds__(RED_THREADS) cg_p_kernel(int64_t P, const V* __restrict__ r, V* __restrict__ p,
-                                                           double* __restrict__ scal, int last_block_updates) {
-  const bool done = scal[4] != 0.0;
-  const double beta = (scal[0] > 0.0) ? scal[2] / scal[0] : 0.0;
-  if (!done) {
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x)
-      p[k] = vadd(r[k], vscale(beta, p[k]));
+                                                           const double* __restrict__ scal, TcDims td,
+                                                           uint16_t* __restrict__ vp) {
+  if (scal[4] != 0.0) return;
+  const double beta = scal[8];
+  const int ns = td.ns, nh = td.nh;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V pk = vadd(r[k], vscale(beta, p[k]));
+    p[k] = pk;
+    if (vp && k >= ns) {
+      const int64_t q = k - ns;
+      if (q < nh) tc_put_vp_elem(td, vp, ns, (int)q, pk);               // v_b row
+      else tc_put_vp_elem(td, vp, (int)((q - nh) / nh), (int)((q - nh) % nh), pk);
+    }
   }
-  (void)last_block_updates;
 }
 
-__global__ void cg_rotate_kernel(double* __restrict__ scal) {
-  if (threadIdx.x == 0 && blockIdx.x == 0 && scal[4] == 0.0) scal[0] = scal[2];
-}
-
-// x = 0, r = p = b, scal init
+// x = 0, r = p = b
 template <class V>
 __global__ void cg_init_kernel(int64_t P, const V* __restrict__ b, V* __restrict__ x, V* __restrict__ r,
                                V* __restrict__ p) {
@@ -343,11 +410,10 @@ __global__ void cg_init_kernel(int64_t P, const V* __restrict__ b, V* __restrict
   }
 }
 
-__global__ void cg_setup_kernel(int n, const double* __restrict__ parts, double rtol, double atol,
-                                double* __restrict__ scal) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double s = 0;
-  for (int q = 0; q < n; ++q) s += parts[q];
+__global__ void __launch_bounds__(SC_THREADS) cg_setup_kernel(int n, const double* __restrict__ parts, double rtol,
+                                                              double atol, double* __restrict__ scal) {
+  const double s = block_sum_parts(n, parts);
+  if (threadIdx.x != 0) return;
   scal[0] = s;                      // rr = ||b||^2
   scal[6] = s;
   const double th = fmax(rtol * sqrt(s), atol);
@@ -356,6 +422,8 @@ __global__ void cg_setup_kernel(int n, const double* __restrict__ parts, double 
   scal[4] = (s <= scal[3]) ? 1.0 : 0.0;
   scal[1] = 0.0;
   scal[2] = s;
+  scal[7] = 0.0;
+  scal[8] = 0.0;
 }
 
 template <class V>
@@ -389,7 +457,8 @@ struct SRWork {
   void* partial;      // [nsplit][P] of T
   void* x; void* r; void* p; void* Ap; void* b;   // [P] of V each
   double* parts;      // [RED_BLOCKS]
-  double* scal;       // [8]
+  double* scal;       // [16]
+  unsigned int* counter;  // [2] last-block tickets (reduce, x/r update)
   bool tc;            // tensor-core matvec in use
   TcDims td;
   TcWork tw;
@@ -417,8 +486,9 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   L.wmean = (double*)take(4 * sizeof(double));
   L.partial = take((size_t)std::max<int64_t>(nsplit_max, 1) * P * ts);
   L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
-  L.parts = (double*)take(RED_BLOCKS * sizeof(double));
-  L.scal = (double*)take(8 * sizeof(double));
+  L.parts = (double*)take(std::max(RED_BLOCKS, RS_MAX_BLOCKS) * sizeof(double));
+  L.scal = (double*)take(16 * sizeof(double));
+  L.counter = (unsigned int*)take(4 * sizeof(unsigned int));
   char* tcb = tc_ok ? take(tc_workspace_bytes(L.td)) : nullptr;
   L.tw = (tc_ok && base) ? tc_layout(L.td, tcb) : TcWork{};
   L.total = off;
@@ -443,8 +513,8 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
   dim3 block(OHU_TM, OHU_TY);
   ohu_kernel<T><<<grid, block, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial);
   QES_LAUNCH_CHECK();
-  reduce_splits_kernel<T, V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, (int)nsplit, (const T*)L.partial, shift, p, y,
-                                                                 dot_part);
+  reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, (int)nsplit, (const T*)L.partial, shift, p, y,
+                                                                 dot_part, dot_part ? L.scal : nullptr, L.counter);
   QES_LAUNCH_CHECK();
   return QES_OK;
 }
@@ -471,12 +541,12 @@ static int sr_force_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, c
   QES_LAUNCH_CHECK();
   if (L.tc) {
     const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
-    int rc = tc_ohu(dtype, L.td, n_samples, bits, tt, eloc, (const double2*)L.wmean, -1, 1.0 / (double)n_samples,
-                    L.partial, L.tw, st);
+    int rc = tc_ohu(dtype, L.td, n_samples, eloc, (const double2*)L.wmean, -1, 1.0 / (double)n_samples, L.partial,
+                    L.tw, st);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-    reduce_splits_kernel<T, V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, L.nsplit, (const T*)L.partial, 0.0, nullptr, F,
-                                                                   nullptr);
+    reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, L.nsplit, (const T*)L.partial, 0.0, nullptr, F,
+                                                                   nullptr, nullptr, nullptr);
     QES_LAUNCH_CHECK();
     return QES_OK;
   }
@@ -498,7 +568,8 @@ static int check_ws(int dtype, int ns, int nh, int64_t n_samples, void* ws, size
   return QES_OK;
 }
 
-static int sr_prepare(int64_t n_samples, const uint32_t* bits, const SRWork& L, cudaStream_t st);
+static int sr_prepare(int dtype, int64_t n_samples, const uint32_t* bits, const void* tt, const SRWork& L,
+                      cudaStream_t st);
 static int sr_check_status(const SRWork& L, cudaStream_t st);
 
 extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
@@ -510,7 +581,7 @@ extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const 
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  rc = sr_prepare(n_samples, bits, L, st);
+  rc = sr_prepare(dtype, n_samples, bits, tanh_theta, L, st);
   if (rc) return rc;
   if (dtype == QES_DTYPE_F32)
     rc = sr_force_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc,
@@ -525,15 +596,15 @@ extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const 
 template <class T>
 static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, double shift,
                        const typename VecT<T>::type* v, typename VecT<T>::type* y, double* dot_part, const SRWork& L,
-                       cudaStream_t st) {
+                       cudaStream_t st, bool vp_ready = false) {
   using V = typename VecT<T>::type;
   if (L.tc) {
     const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
-    int rc = tc_matvec(dtype, L.td, n_samples, bits, tt, v, L.w, L.partial, L.tw, st);
+    int rc = tc_matvec(dtype, L.td, n_samples, bits, v, L.w, L.partial, L.tw, st, !vp_ready);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-    reduce_splits_kernel<T, V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, L.nsplit, (const T*)L.partial, shift, v, y,
-                                                                   dot_part);
+    reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, L.nsplit, (const T*)L.partial, shift, v, y,
+                                                                   dot_part, dot_part ? L.scal : nullptr, L.counter);
     QES_LAUNCH_CHECK();
     return QES_OK;
   }
@@ -544,9 +615,10 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
 }
 
 // per-step operands of the tensor-core path (spins as BF16 tiles) and the status word
-static int sr_prepare(int64_t n_samples, const uint32_t* bits, const SRWork& L, cudaStream_t st) {
+static int sr_prepare(int dtype, int64_t n_samples, const uint32_t* bits, const void* tt, const SRWork& L,
+                      cudaStream_t st) {
   if (!L.tc) return QES_OK;
-  return tc_prepare_step(L.td, n_samples, bits, L.tw, st);
+  return tc_prepare_step(dtype, L.td, n_samples, bits, tt, L.tw, st);
 }
 
 static int sr_check_status(const SRWork& L, cudaStream_t st) {
@@ -570,7 +642,7 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  rc = sr_prepare(n_samples, bits, L, st);
+  rc = sr_prepare(dtype, n_samples, bits, tanh_theta, L, st);
   if (rc) return rc;
   if (dtype == QES_DTYPE_F32)
     rc = sr_matvec_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, shift, (const double*)v,
@@ -582,6 +654,42 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
   return sr_check_status(L, st);
 }
 
+// ----------------------------------------------------------------------------
+// CUDA graph of one chunk of CG iterations (matvec + x/r update + direction
+// update, `check_every` times), captured on a private stream and replayed
+// while the kernel arguments stay the same (same buffers, sizes and shift).
+// ----------------------------------------------------------------------------
+#include <mutex>
+#include <cstring>
+
+namespace {
+struct CgGraphKey {
+  const void* bits; const void* tt; const void* ws; int64_t n; int ns, nh, dtype, chunk, tc;
+  double shift;
+  bool operator==(const CgGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+struct CgGraphSlot {
+  bool init = false;
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  CgGraphKey key{};
+  long long nodes = 0;
+};
+constexpr int kMaxGraphDevices = 64;
+std::mutex g_graph_mu;
+CgGraphSlot g_graph[kMaxGraphDevices];
+std::atomic<int> g_use_graphs{1};
+}  // namespace
+
+extern long long qes_launch_count(int reset);
+void qes_count_launches(int n);
+
+extern "C" int qes_set_cg_graphs(int enable) {
+  g_use_graphs.store(enable ? 1 : 0);
+  return QES_OK;
+}
+
 template <class T>
 static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* eloc,
                    const qes_sr_options* opt, typename VecT<T>::type* x_out, qes_sr_result* res, const SRWork& L,
@@ -589,16 +697,18 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   using V = typename VecT<T>::type;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   V* x = (V*)L.x; V* r = (V*)L.r; V* p = (V*)L.p; V* Ap = (V*)L.Ap; V* b = (V*)L.b;
-  int rc = sr_prepare(n_samples, bits, L, st);
+  const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
+  int rc = sr_prepare(dtype, n_samples, bits, tt, L, st);
   if (rc) return rc;
   // b = F
   rc = sr_force_t<T>(ns, nh, n_samples, bits, tt, eloc, b, L, st);
   if (rc) return rc;
   double emean[2] = {0, 0};
   QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 4 * sizeof(unsigned int), st));
   cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p);
   norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
-  cg_setup_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
+  cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
   QES_LAUNCH_CHECK_N(3);
   const int check = opt->check_every > 0 ? opt->check_every : 8;
   double hs[8] = {0};
@@ -607,17 +717,65 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaStreamSynchronize(st));
   done = hs[4] != 0.0;
+  auto run_direct = [&](int nrun, int it0) -> int {
+    for (int q = 0; q < nrun; ++q) {
+      int r2 = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, p, Ap, L.parts, L, st,
+                              /*vp_ready=*/it0 + q > 0);
+      if (r2) return r2;
+      // (alpha is computed by the last block of the matvec's split reduction)
+      cg_xr_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, p, Ap, x, r, L.scal, L.parts, L.counter + 1);
+      cg_p_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, p, L.scal, L.td, L.tc ? L.tw.vp : nullptr);
+      QES_LAUNCH_CHECK_N(2);
+    }
+    return QES_OK;
+  };
+  int dev = 0;
+  QES_CUDA_CHECK(cudaGetDevice(&dev));
+  const bool graphs = g_use_graphs.load() != 0 && dev >= 0 && dev < kMaxGraphDevices;
   while (!done && it < opt->maxiter) {
     const int nrun = std::min(check, opt->maxiter - it);
-    for (int q = 0; q < nrun; ++q) {
-      rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, p, Ap, L.parts, L, st);
+    if (!graphs || it == 0 || nrun != check) {
+      rc = run_direct(nrun, it);
       if (rc) return rc;
-      sum_parts_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, L.scal + 1);
-      cg_xr_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, p, Ap, x, r, L.scal, L.parts);
-      cg_scalar_kernel<<<1, 32, 0, st>>>(RED_BLOCKS, L.parts, L.scal);
-      cg_p_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, p, L.scal, 0);
-      cg_rotate_kernel<<<1, 32, 0, st>>>(L.scal);
-      QES_LAUNCH_CHECK_N(5);
+    } else {
+      std::lock_guard<std::mutex> lock(g_graph_mu);
+      CgGraphSlot& gs = g_graph[dev];
+      if (!gs.init) {
+        QES_CUDA_CHECK(cudaStreamCreateWithFlags(&gs.cs, cudaStreamNonBlocking));
+        QES_CUDA_CHECK(cudaEventCreateWithFlags(&gs.ev_in, cudaEventDisableTiming));
+        QES_CUDA_CHECK(cudaEventCreateWithFlags(&gs.ev_out, cudaEventDisableTiming));
+        gs.init = true;
+      }
+      const CgGraphKey key{bits, tt, L.w, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
+                           L.tc ? 1 : 0, opt->shift};
+      if (gs.exec == nullptr || !(gs.key == key)) {
+        if (gs.exec) {
+          cudaGraphExecDestroy(gs.exec);
+          gs.exec = nullptr;
+        }
+        const long long before = qes_launch_count(0);
+        QES_CUDA_CHECK(cudaStreamBeginCapture(gs.cs, cudaStreamCaptureModeThreadLocal));
+        cudaStream_t saved = st;
+        st = gs.cs;
+        const int rcap = run_direct(nrun, 1);
+        st = saved;
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(gs.cs, &g);
+        if (rcap) return rcap;
+        if (ec != cudaSuccess) { qes_set_last_error(ec, "cudaStreamEndCapture"); return QES_ERR_CUDA; }
+        const cudaError_t ei = cudaGraphInstantiate(&gs.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) { gs.exec = nullptr; qes_set_last_error(ei, "cudaGraphInstantiate"); return QES_ERR_CUDA; }
+        gs.nodes = qes_launch_count(0) - before;
+        qes_count_launches((int)-gs.nodes);     // captured, not run
+        gs.key = key;
+      }
+      QES_CUDA_CHECK(cudaEventRecord(gs.ev_in, st));
+      QES_CUDA_CHECK(cudaStreamWaitEvent(gs.cs, gs.ev_in, 0));
+      QES_CUDA_CHECK(cudaGraphLaunch(gs.exec, gs.cs));
+      QES_CUDA_CHECK(cudaEventRecord(gs.ev_out, gs.cs));
+      QES_CUDA_CHECK(cudaStreamWaitEvent(st, gs.ev_out, 0));
+      qes_count_launches((int)gs.nodes);
     }
     it += nrun;
     QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -1,88 +1,88 @@
 // Tensor-core (tcgen05) halves of the structured SR matvec.
 //
-//   ov :  Z = Sigma V          (128 samples x Kp sites) . (Kp sites x Np)  -> TMEM
-//         w_s = sum_m t_sm (vb_m + Z_sm) + sigma_s . va          (epilogue, CUDA cores)
-//   ohu:  G_W = Sigma^T Q      (128 sites x KC samples) . (KC samples x Np) -> TMEM
-//         Q_sm = conj(t_sm) u_s, u_s = (w_s - mean w) / Ns      (staged by CUDA cores)
+//   ov : Y = T V'^T  with A = T (128 samples x K hidden), B = V' (NB x K)          -> TMEM
+//        (O v)_s = sum_{i<ns} sigma_si Y_si + Y_{s,ns} + sigma_s . va          (epilogue)
+//        V' stacks, per site i, the K-row [Re V_i | -Im V_i] (-> Re Y) and
+//        [Im V_i | Re V_i] (-> Im Y) over the K = [Re t | Im t] axis; the extra
+//        "site" ns carries v_b, so t_s . v_b comes out of the same MMA.
+//   ohu: G_W = Sigma^T Q  with A = Sigma^T (128 sites x KC samples),
+//        B = Q^T (2 Mp x KC), Q_sm = conj(t_sm) u_s, u_s = (w_s - mean w) / Ns    -> TMEM
 //
-// Sigma (+-1) is exact in BF16.  The other operand is split x = hi + lo into
-// two BF16 terms accumulated into the same FP32 TMEM accumulator, which keeps
-// ~16 significant bits of the float32 value (the product with +-1 adds no
-// rounding).  Complex operands are laid out as Np = 2*Mp rows: real parts in
-// rows [0, Mp), imaginary parts in [Mp, 2Mp); the two halves are two MMAs of
-// N = Mp into TMEM columns [0, Mp) and [im_off, im_off + Mp).
+// Operands are stored in global memory as BF16 core-matrix tiles (K-major, no
+// swizzle, see umma.cuh), prepared once per VMC step (T, T^T, Sigma^T) or once
+// per CG iteration (V'), and move into shared memory only by bulk copies.  ov
+// streams K in chunks through a 4-stage mbarrier pipeline (producer thread ->
+// MMA-issuing thread -> producer); ohu bulk-copies T^T for its sample chunk
+// and multiplies it by u in shared memory.
 //
-// Every wait on an mbarrier is bounded; on time-out the kernel records an
-// error code in *status, still waits (bounded) for what it issued, frees its
-// TMEM and returns.  The host reads *status after the solve.
+// Precision: Sigma (+-1) is exact in BF16; every other operand x is split as
+// x = hi + lo (two BF16 terms); ov uses hi*hi + hi*lo + lo*hi, ohu rebuilds Q
+// in float32 and splits it again.  Accumulation is FP32 in TMEM.
+//
+// Every mbarrier wait is bounded; on time-out the kernel records
+// QES_ERR_TIMEOUT in *status, still waits (bounded) for the work it issued,
+// frees its TMEM and returns.  The host reads *status after the solve.
 #include "common.cuh"
 #include "sr_tc.h"
 #include "umma.cuh"
 
+#include <algorithm>
 #include <cuda_bf16.h>
 
 namespace {
 
 constexpr uint32_t kWaitLimit = 1u << 22;     // try_wait polls before giving up
-constexpr int kThreads = 128;                  // 4 warps <-> 4 TMEM lane quarters
+constexpr int kThreads = 512;                  // 16 warps; warp w reads TMEM lane quarter w % 4
+constexpr int kWarps = kThreads / 32;
+constexpr int kColGroups = kWarps / 4;         // warps sharing one lane quarter split the columns
+constexpr int kStages = 4;                     // ov pipeline depth
 
-__device__ __forceinline__ uint16_t bf16_bits(float x) {
-  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
-}
+__device__ __forceinline__ uint16_t bf16_bits(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
 __device__ __forceinline__ float bf16_val(uint16_t b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
 __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) {
   hi = bf16_bits(x);
   lo = bf16_bits(x - bf16_val(hi));
 }
-
 __device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b) { return (uint32_t)a | ((uint32_t)b << 16); }
+__device__ __forceinline__ uint4 pack8(const uint16_t (&v)[8]) {
+  return make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+}
+__device__ __forceinline__ void unpack8(uint4 p, float (&v)[8]) {
+  const uint32_t w[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    v[2 * q] = bf16_val((uint16_t)(w[q] & 0xffffu));
+    v[2 * q + 1] = bf16_val((uint16_t)(w[q] >> 16));
+  }
+}
 
 __device__ __forceinline__ void record_error(int* status, int code) {
   if (status) atomicCAS(status, 0, code);
 }
 
-// values of V (float64 / complex128) as float
 __device__ __forceinline__ float vre(const double* v, int64_t k) { return (float)v[k]; }
 __device__ __forceinline__ float vre(const double2* v, int64_t k) { return (float)v[k].x; }
 __device__ __forceinline__ float vim(const double*, int64_t) { return 0.f; }
 __device__ __forceinline__ float vim(const double2* v, int64_t k) { return (float)v[k].y; }
+__device__ __forceinline__ float tre(const float* t, int64_t k) { return t[k]; }
+__device__ __forceinline__ float tre(const float2* t, int64_t k) { return t[k].x; }
+__device__ __forceinline__ float tim(const float*, int64_t) { return 0.f; }
+__device__ __forceinline__ float tim(const float2* t, int64_t k) { return t[k].y; }
 
 }  // namespace
 
-// ------------------------------------------------------------------------------------------------
-// per-step operands: Sigma in rows-of-samples tiles and in rows-of-sites chunks
-// ------------------------------------------------------------------------------------------------
-// sig_rows: tile t holds samples [128t, 128t+128) x Kp sites; sig_cols: chunk c holds 128 sites x
-// samples [KC c, KC c + KC).  Padding (sites >= ns, samples >= Ns) is zero.
-__global__ void tc_sigma_rows_kernel(int ns, int Kp, int64_t n_samples, int n_tiles, const uint32_t* __restrict__ bits,
-                                     uint16_t* __restrict__ out) {
-  const int nw = n_words(ns);
-  const int64_t items = (int64_t)n_tiles * 128 * (Kp / 8);
-  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
-    const int k8 = (int)(it % (Kp / 8));
-    const int r = (int)((it / (Kp / 8)) % 128);
-    const int64_t t = it / ((int64_t)(Kp / 8) * 128);
-    const int64_t s = t * 128 + r;
-    uint16_t v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int i = 8 * k8 + q;
-      v[q] = 0;
-      if (s < n_samples && i < ns) v[q] = ((bits[s * nw + (i >> 5)] >> (i & 31)) & 1u) ? 0x3F80u : 0xBF80u;
-    }
-    uint4 pk = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
-    uint8_t* base = reinterpret_cast<uint8_t*>(out) + (size_t)t * 128 * Kp * 2;
-    *reinterpret_cast<uint4*>(base + umma::kmajor_offset(r, 8 * k8, 128)) = pk;
-  }
-}
-
+// ================================================================================================
+// per-step operands
+// ================================================================================================
+// sig_cols: chunk c = 128 sites x samples [KC c, KC c + KC): Sigma^T, the ohu A operand.
+// Row 127 (always beyond the last site) is all ones, so the same MMA yields g_b = sum_s Q_s.
 __global__ void tc_sigma_cols_kernel(int ns, int KC, int64_t n_samples, int n_chunks, const uint32_t* __restrict__ bits,
                                      uint16_t* __restrict__ out) {
   const int nw = n_words(ns);
   const int64_t items = (int64_t)n_chunks * 128 * (KC / 8);
   for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
-    const int k8 = (int)(it % (KC / 8));
-    const int r = (int)((it / (KC / 8)) % 128);          // site
+    const int r = (int)(it % 128);                       // site (fastest: consecutive 16-byte stores)
+    const int k8 = (int)((it / 128) % (KC / 8));
     const int64_t c = it / ((int64_t)(KC / 8) * 128);
     uint16_t v[8];
 #pragma unroll
@@ -90,85 +90,156 @@ __global__ void tc_sigma_cols_kernel(int ns, int KC, int64_t n_samples, int n_ch
       const int64_t s = c * KC + 8 * k8 + q;
       v[q] = 0;
       if (s < n_samples && r < ns) v[q] = ((bits[s * nw + (r >> 5)] >> (r & 31)) & 1u) ? 0x3F80u : 0xBF80u;
+      if (s < n_samples && r == 127) v[q] = 0x3F80u;      // row of ones: D[127] = sum_s Q_s = g_b
     }
-    uint4 pk = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
     uint8_t* base = reinterpret_cast<uint8_t*>(out) + (size_t)c * 128 * KC * 2;
-    *reinterpret_cast<uint4*>(base + umma::kmajor_offset(r, 8 * k8, 128)) = pk;
+    *reinterpret_cast<uint4*>(base + umma::kmajor_offset(r, 8 * k8, 128)) = pack8(v);
   }
 }
 
-// ------------------------------------------------------------------------------------------------
-// per-iteration B operand of ov: rows n (hidden, re then im) x Kp sites, hi and lo terms
-// ------------------------------------------------------------------------------------------------
-template <class V>
-__global__ void tc_build_v_kernel(int ns, int nh, int Kp, int Mp, int Np, bool cplx, const V* __restrict__ v,
-                                  uint16_t* __restrict__ bhi, uint16_t* __restrict__ blo) {
-  const int items = Np * (Kp / 8);
-  const V* vW = v + ns + nh;
-  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
-    const int k8 = it % (Kp / 8);
-    const int n = it / (Kp / 8);
-    const bool im = cplx && n >= Mp;
+// t_rows: ov A operand.  Tile t (128 samples), chunk c of KCH columns of the K axis
+// [Re t (Mp) | Im t (Mp)] (complex) or [t] (real), terms hi/lo:
+//   byte offset ((t * nK + c) * 2 + term) * (128 * KCH * 2) + kmajor_offset(r, k % KCH, 128)
+template <class T>
+__global__ void tc_t_rows_kernel(TcDims d, int64_t n_samples, const T* __restrict__ tt, uint16_t* __restrict__ out) {
+  constexpr bool CPLX = ScalarTraits<T>::is_complex;
+  const int nh = d.nh, Kd = d.Kd, KCH = d.KCH, nK = Kd / KCH;
+  const size_t tile_bytes = (size_t)128 * KCH * 2;
+  const int64_t items = (int64_t)d.n_tiles * 128 * (Kd / 8);
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(it % 128);
+    const int k8 = (int)((it / 128) % (Kd / 8));
+    const int64_t t = it / ((int64_t)(Kd / 8) * 128);
+    const int64_t s = t * 128 + r;
+    uint16_t h[8], l[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int k = 8 * k8 + q;
+      float x = 0.f;
+      if (s < n_samples) {
+        if (CPLX) {
+          if (k < d.Mp) {
+            if (k < nh) x = tre(tt, s * nh + k);
+          } else if (k - d.Mp < nh) {
+            x = tim(tt, s * nh + (k - d.Mp));
+          }
+        } else if (k < nh) {
+          x = tre(tt, s * nh + k);
+        }
+      }
+      split_bf16(x, h[q], l[q]);
+    }
+    const int c = (8 * k8) / KCH, kc = (8 * k8) % KCH;
+    uint8_t* base = reinterpret_cast<uint8_t*>(out) + (((size_t)t * nK + c) * 2) * tile_bytes;
+    const uint32_t off = umma::kmajor_offset(r, kc, 128);
+    *reinterpret_cast<uint4*>(base + off) = pack8(h);
+    *reinterpret_cast<uint4*>(base + tile_bytes + off) = pack8(l);
+  }
+}
+
+// t_cols: ohu B operand before the u-scaling.  Chunk c (KC samples): rows n = hidden (re: n < Mp,
+// im: Mp <= n < 2 Mp) x KC samples, terms hi/lo.
+template <class T>
+__global__ void tc_t_cols_kernel(TcDims d, int64_t n_samples, const T* __restrict__ tt, uint16_t* __restrict__ out) {
+  constexpr bool CPLX = ScalarTraits<T>::is_complex;
+  const int nh = d.nh, Mp = d.Mp, Np = d.Np, KC = d.KC;
+  const size_t term_bytes = (size_t)Np * KC * 2;
+  const int64_t items = (int64_t)d.n_chunks * Np * (KC / 8);
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
+    const int n = (int)(it % Np);
+    const int k8 = (int)((it / Np) % (KC / 8));
+    const int64_t c = it / ((int64_t)(KC / 8) * Np);
+    const bool im = CPLX && n >= Mp;
     const int m = im ? n - Mp : n;
     uint16_t h[8], l[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int i = 8 * k8 + q;
+      const int64_t s = c * KC + 8 * k8 + q;
       float x = 0.f;
-      if (i < ns && m < nh) {
-        const int64_t k = (int64_t)i * nh + m;
-        x = im ? vim(vW, k) : vre(vW, k);
-      }
+      if (s < n_samples && m < nh) x = im ? tim(tt, s * nh + m) : tre(tt, s * nh + m);
       split_bf16(x, h[q], l[q]);
     }
+    uint8_t* base = reinterpret_cast<uint8_t*>(out) + (size_t)c * 2 * term_bytes;
     const uint32_t off = umma::kmajor_offset(n, 8 * k8, Np);
-    *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(bhi) + off) =
-        make_uint4(pack2(h[0], h[1]), pack2(h[2], h[3]), pack2(h[4], h[5]), pack2(h[6], h[7]));
-    *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(blo) + off) =
-        make_uint4(pack2(l[0], l[1]), pack2(l[2], l[3]), pack2(l[4], l[5]), pack2(l[6], l[7]));
+    *reinterpret_cast<uint4*>(base + off) = pack8(h);
+    *reinterpret_cast<uint4*>(base + term_bytes + off) = pack8(l);
   }
 }
 
-// ------------------------------------------------------------------------------------------------
-// ov: one CTA per 128-sample tile
-// ------------------------------------------------------------------------------------------------
+// ================================================================================================
+// per-iteration operand of ov: V' (NB rows x Kd), chunked like t_rows:
+//   byte offset (c * 2 + term) * (NB * KCH * 2) + kmajor_offset(n, k % KCH, NB)
+// ================================================================================================
+template <class V>
+__global__ void tc_build_vp_kernel(TcDims d, bool cplx, const V* __restrict__ v, uint16_t* __restrict__ out) {
+  const int ns = d.ns, nh = d.nh, Mp = d.Mp, Kd = d.Kd, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
+  const V* vb = v + ns;
+  const V* vW = v + ns + nh;
+  const size_t term_bytes = (size_t)NB * KCH * 2;
+  const int items = NB * (Kd / 8);
+  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
+    const int n = it % NB, k8 = it / NB;
+    const bool yim = cplx && n >= Sp;                     // row produces Im Y
+    const int i = yim ? n - Sp : n;                        // site (i == ns: the v_b row)
+    uint16_t h[8], l[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int k = 8 * k8 + q;
+      const bool kim = cplx && k >= Mp;                    // K column holds Im t
+      const int m = kim ? k - Mp : k;
+      float x = 0.f;
+      if (m < nh && i <= ns) {
+        const float vr = (i < ns) ? vre(vW, (int64_t)i * nh + m) : vre(vb, m);
+        const float vi = (i < ns) ? vim(vW, (int64_t)i * nh + m) : vim(vb, m);
+        // Re Y = Re t Re v - Im t Im v ;  Im Y = Re t Im v + Im t Re v
+        if (!yim) x = kim ? -vi : vr;
+        else x = kim ? vr : vi;
+      }
+      split_bf16(x, h[q], l[q]);
+    }
+    const int c = (8 * k8) / KCH, kc = (8 * k8) % KCH;
+    uint8_t* base = reinterpret_cast<uint8_t*>(out) + (size_t)c * 2 * term_bytes;
+    const uint32_t off = umma::kmajor_offset(n, kc, NB);
+    *reinterpret_cast<uint4*>(base + off) = pack8(h);
+    *reinterpret_cast<uint4*>(base + term_bytes + off) = pack8(l);
+  }
+}
+
+// ================================================================================================
+// ov: one CTA per 128-sample tile, K streamed through a kStages-deep pipeline
+// ================================================================================================
 template <class T, class V>
 __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_samples, const uint32_t* __restrict__ bits,
-                                                         const T* __restrict__ tanh_theta, const V* __restrict__ v,
-                                                         const uint16_t* __restrict__ sig_rows,
-                                                         const uint16_t* __restrict__ bhi,
-                                                         const uint16_t* __restrict__ blo, float2* __restrict__ w_out,
+                                                         const V* __restrict__ v, const uint16_t* __restrict__ t_rows,
+                                                         const uint16_t* __restrict__ vp, float2* __restrict__ w_out,
                                                          double2* __restrict__ wsum_part, int* __restrict__ status) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
-  const int ns = d.ns, nh = d.nh, Kp = d.Kp, Mp = d.Mp, Np = d.Np;
-  const uint32_t a_bytes = 128u * Kp * 2u, b_bytes = (uint32_t)Np * Kp * 2u;
-  uint8_t* sA = smem;
-  uint8_t* sBh = sA + a_bytes;
-  uint8_t* sBl = sBh + b_bytes;
-  T* s_vb = reinterpret_cast<T*>(sBl + b_bytes);                         // nh
-  T* s_va = s_vb + nh;                                                    // ns
-  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(s_va + ns) +
-                                               ((16 - (reinterpret_cast<uintptr_t>(s_va + ns) & 15)) & 15));
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
-  __shared__ double2 red[kThreads / 32];
-  __shared__ int s_issued;
+  const int ns = d.ns, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
+  const int nK = d.Kd / KCH;
+  const uint32_t a_term = 128u * KCH * 2u, b_term = (uint32_t)NB * KCH * 2u;
+  const uint32_t stage_bytes = 2u * (a_term + b_term);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * stage_bytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* done = empty + kStages;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  T* s_va = reinterpret_cast<T*>(tslot + 4);
+  __shared__ double2 red[4];
+  __shared__ float2 s_part[kColGroups][128];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tile = blockIdx.x;
   if (tid == 0) {
-    umma::mbar_init(&bars[0], 1);
-    umma::mbar_init(&bars[1], 1);
+    for (int q = 0; q < kStages; ++q) {
+      umma::mbar_init(&full[q], 1);
+      umma::mbar_init(&empty[q], 1);
+    }
+    umma::mbar_init(done, 1);
     umma::fence_mbar_init();
   }
   if (warp == 0) {
     umma::tmem_alloc(tslot, d.tmem_cols);
     umma::tmem_relinquish();
-  }
-  // small vectors of the direction (float)
-  for (int m = tid; m < nh; m += kThreads) {
-    if constexpr (CPLX) s_vb[m] = make_float2(vre(v, ns + m), vim(v, ns + m));
-    else s_vb[m] = vre(v, ns + m);
   }
   for (int i = tid; i < ns; i += kThreads) {
     if constexpr (CPLX) s_va[i] = make_float2(vre(v, i), vim(v, i));
@@ -178,109 +249,123 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   __syncthreads();
   umma::tc_fence_after();
   const uint32_t tbase = *tslot;
-  bool ok = true;
-  if (tid == 0) {
-    umma::mbar_arrive_expect_tx(&bars[0], a_bytes + 2 * b_bytes);
-    umma::bulk_g2s(sA, reinterpret_cast<const uint8_t*>(sig_rows) + (size_t)tile * a_bytes, a_bytes, &bars[0]);
-    umma::bulk_g2s(sBh, bhi, b_bytes, &bars[0]);
-    umma::bulk_g2s(sBl, blo, b_bytes, &bars[0]);
-    if (!umma::mbar_wait(&bars[0], 0, kWaitLimit)) {
-      ok = false;
-      record_error(status, QES_ERR_TIMEOUT);
-    }
-    if (ok) {
-      umma::tc_fence_after();
-      const uint32_t idesc = umma::idesc_bf16_f32(128, Mp);
-      const uint32_t aaddr = umma::smem_u32(sA), bh = umma::smem_u32(sBh), bl = umma::smem_u32(sBl);
-      const int halves = CPLX ? 2 : 1;
-      for (int j = 0; j < Kp / 16; ++j) {
-        const uint64_t ad = umma::smem_desc(aaddr + 2u * j * 128u * 16u, 128u * 16u, 128u);
-        for (int term = 0; term < 2; ++term) {
-          const uint32_t bb = term ? bl : bh;
-          for (int h = 0; h < halves; ++h) {
-            const uint64_t bd = umma::smem_desc(bb + (uint32_t)h * (Mp / 8) * 128u + 2u * j * Np * 16u, Np * 16u, 128u);
-            umma::mma_bf16(tbase + (uint32_t)h * d.im_off, ad, bd, idesc, (j > 0 || term > 0) ? 1u : 0u);
-          }
-        }
+
+  if (warp == 0 && lane == 0) {
+    // producer: stage s is refilled once the MMAs that read it have completed
+    const uint8_t* ga = reinterpret_cast<const uint8_t*>(t_rows) + (size_t)tile * nK * 2 * a_term;
+    const uint8_t* gb = reinterpret_cast<const uint8_t*>(vp);
+    for (int c = 0; c < nK; ++c) {
+      const int s = c % kStages;
+      if (c >= kStages && !umma::mbar_wait(&empty[s], ((c / kStages) - 1) & 1, kWaitLimit)) {
+        record_error(status, QES_ERR_TIMEOUT);
+        break;
       }
-      umma::mma_commit(&bars[1]);
-    } else {
-      umma::mbar_wait(&bars[0], 0, kWaitLimit);      // let the copies in flight land before exit
+      uint8_t* st = smem + s * stage_bytes;
+      umma::mbar_arrive_expect_tx(&full[s], stage_bytes);
+      umma::bulk_g2s(st, ga + (size_t)c * 2 * a_term, 2 * a_term, &full[s]);
+      umma::bulk_g2s(st + 2 * a_term, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[s]);
     }
-    s_issued = ok ? 1 : 0;
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer: D (128 x NB) += A_hi B_hi + A_hi B_lo + A_lo B_hi over every 16-wide k-step
+    const uint32_t idesc = umma::idesc_bf16_f32(128, NB);
+    for (int c = 0; c < nK; ++c) {
+      const int s = c % kStages;
+      if (!umma::mbar_wait(&full[s], (c / kStages) & 1, kWaitLimit)) {
+        record_error(status, QES_ERR_TIMEOUT);
+        break;
+      }
+      umma::tc_fence_after();
+      const uint32_t sa = umma::smem_u32(smem + s * stage_bytes);
+      const uint32_t ahi = sa, alo = sa + a_term, bhi = sa + 2 * a_term, blo = bhi + b_term;
+      for (int kk = 0; kk < KCH / 16; ++kk) {
+        const uint32_t ko_a = 2u * kk * 128u * 16u, ko_b = 2u * kk * NB * 16u;
+        const uint64_t dah = umma::smem_desc(ahi + ko_a, 128u * 16u, 128u);
+        const uint64_t dal = umma::smem_desc(alo + ko_a, 128u * 16u, 128u);
+        const uint64_t dbh = umma::smem_desc(bhi + ko_b, NB * 16u, 128u);
+        const uint64_t dbl = umma::smem_desc(blo + ko_b, NB * 16u, 128u);
+        umma::mma_bf16(tbase, dah, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+        umma::mma_bf16(tbase, dah, dbl, idesc, 1u);
+        umma::mma_bf16(tbase, dal, dbh, idesc, 1u);
+      }
+      umma::mma_commit(&empty[s]);
+    }
+    umma::mma_commit(done);                 // arrives once every MMA issued above has completed
   }
   __syncthreads();
-  // every thread waits (bounded) for this CTA's own MMAs, when they were issued
-  if (s_issued && !umma::mbar_wait(&bars[1], 0, kWaitLimit)) record_error(status, QES_ERR_TIMEOUT);
+  if (!umma::mbar_wait(done, 0, kWaitLimit)) record_error(status, QES_ERR_TIMEOUT);
   umma::tc_fence_after();
 
-  // epilogue: this thread owns sample row 32*warp + lane of the tile
-  const int row = 32 * warp + lane;
+  // epilogue: warp w reads lane quarter w % 4 (sample rows) and column group w / 4
+  const int quarter = warp & 3, cg = warp >> 2;
+  const int row = 32 * quarter + lane;
   const int64_t s = (int64_t)tile * 128 + row;
   const bool sval = s < n_samples;
-  const int64_t sc = sval ? s : 0;
-  T acc = ScalarTraits<T>::zero();
-  const T* trow = tanh_theta + sc * nh;
-  const uint32_t lane_addr = tbase + ((uint32_t)(32 * warp) << 16);
-  for (int c0 = 0; c0 < Mp; c0 += 16) {
-    float zr[16], zi[16];
-    umma::tmem_ld16(lane_addr + c0, zr);
-    if constexpr (CPLX) umma::tmem_ld16(lane_addr + d.im_off + c0, zi);
+  const uint32_t* wrd = bits + (sval ? s : 0) * n_words(ns);
+  float2 acc = make_float2(0.f, 0.f);
+  const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+  for (int c = cg; c < NB / 16; c += kColGroups) {
+    float y[16];
+    umma::tmem_ld16(lane_addr + 16 * c, y);
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
-      const int m = c0 + q;
-      if (m < nh) {
-        if constexpr (CPLX) {
-          const float2 z = make_float2(zr[q] + s_vb[m].x, zi[q] + s_vb[m].y);
-          acc = addx(acc, mulx(trow[m], z));
-        } else {
-          acc += trow[m] * (zr[q] + s_vb[m]);
-        }
-      }
+      const int n = 16 * c + q;
+      const bool yim = CPLX && n >= Sp;
+      const int i = yim ? n - Sp : n;
+      float contrib = 0.f;
+      if (i < ns) contrib = ((wrd[i >> 5] >> (i & 31)) & 1u) ? y[q] : -y[q];
+      else if (i == ns) contrib = y[q];
+      if (yim) acc.y += contrib;
+      else acc.x += contrib;
     }
   }
-  const uint32_t* wrd = bits + sc * n_words(ns);
-  for (int i = 0; i < ns; ++i) {
+  for (int i = cg; i < ns; i += kColGroups) {
     const float sg = ((wrd[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
-    acc = addx(acc, scal(sg, s_va[i]));
+    acc = acc + to_c(scal(sg, s_va[i]));
   }
-  float2 wv = sval ? to_c(acc) : make_float2(0.f, 0.f);
-  if (sval) w_out[s] = wv;
-  double2 ps = make_double2(wv.x, wv.y);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    ps.x += __shfl_xor_sync(0xffffffffu, ps.x, o);
-    ps.y += __shfl_xor_sync(0xffffffffu, ps.y, o);
-  }
-  if (lane == 0) red[warp] = ps;
+  s_part[cg][row] = acc;
   umma::tc_fence_before();
+  __syncthreads();
+  if (cg == 0) {
+    float2 wv = s_part[0][row];
+#pragma unroll
+    for (int g = 1; g < kColGroups; ++g) wv = wv + s_part[g][row];
+    if (!sval) wv = make_float2(0.f, 0.f);
+    if (sval) w_out[s] = wv;
+    double2 ps = make_double2(wv.x, wv.y);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ps.x += __shfl_xor_sync(0xffffffffu, ps.x, o);
+      ps.y += __shfl_xor_sync(0xffffffffu, ps.y, o);
+    }
+    if (lane == 0) red[quarter] = ps;
+  }
   __syncthreads();
   if (tid == 0) {
     double2 t = make_double2(0.0, 0.0);
-    for (int q = 0; q < kThreads / 32; ++q) { t.x += red[q].x; t.y += red[q].y; }
+    for (int q = 0; q < 4; ++q) { t.x += red[q].x; t.y += red[q].y; }
     wsum_part[tile] = t;
   }
   if (warp == 0) umma::tmem_dealloc(tbase, d.tmem_cols);
 }
 
-// ------------------------------------------------------------------------------------------------
+// ================================================================================================
 // ohu: one CTA per KC-sample chunk; writes one P-vector of partial sums
-// ------------------------------------------------------------------------------------------------
+// ================================================================================================
 template <class T>
-__global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_samples, const uint32_t* __restrict__ bits,
-                                                          const T* __restrict__ tanh_theta, const float2* __restrict__ w,
-                                                          const double2* __restrict__ wsum_part, int wsum_n, double scale,
-                                                          const uint16_t* __restrict__ sig_cols, T* __restrict__ partial,
+__global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_samples, const float2* __restrict__ w,
+                                                          const double2* __restrict__ wsum_part, int wsum_n,
+                                                          double scale, const uint16_t* __restrict__ sig_cols,
+                                                          const uint16_t* __restrict__ t_cols, T* __restrict__ partial,
                                                           int* __restrict__ status) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   const int ns = d.ns, nh = d.nh, Mp = d.Mp, Np = d.Np, KC = d.KC;
-  const uint32_t a_bytes = 128u * KC * 2u, b_bytes = (uint32_t)Np * KC * 2u;
+  const uint32_t a_bytes = 128u * KC * 2u, b_term = (uint32_t)Np * KC * 2u;
   uint8_t* sA = smem;
   uint8_t* sBh = sA + a_bytes;
-  uint8_t* sBl = sBh + b_bytes;
-  T* s_u = reinterpret_cast<T*>(sBl + b_bytes);            // KC
-  T* s_gb = s_u + KC;                                      // nh (partial g_b of this chunk)
+  uint8_t* sBl = sBh + b_term;
+  T* s_u = reinterpret_cast<T*>(sBl + b_term);            // KC
+  T* s_gb = s_u + KC;                                      // nh
   uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(s_gb + nh) +
                                                ((16 - (reinterpret_cast<uintptr_t>(s_gb + nh) & 15)) & 15));
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
@@ -304,6 +389,7 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
       t = wsum_part[0];              // the mean itself
     }
     s_mean = t;
+    s_issued = 0;
   }
   if (warp == 0) {
     umma::tmem_alloc(tslot, d.tmem_cols);
@@ -314,10 +400,10 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   umma::tc_fence_after();
   const uint32_t tbase = *tslot;
   if (tid == 0) {
-    umma::mbar_arrive_expect_tx(&bars[0], a_bytes);
+    umma::mbar_arrive_expect_tx(&bars[0], a_bytes + 2 * b_term);
     umma::bulk_g2s(sA, reinterpret_cast<const uint8_t*>(sig_cols) + (size_t)chunk * a_bytes, a_bytes, &bars[0]);
+    umma::bulk_g2s(sBh, reinterpret_cast<const uint8_t*>(t_cols) + (size_t)chunk * 2 * b_term, 2 * b_term, &bars[0]);
   }
-  // u_s = (w_s - mean) * scale, zero beyond Ns
   const float mr = (float)s_mean.x, mi = (float)s_mean.y, fs = (float)scale;
   for (int k = tid; k < KC; k += kThreads) {
     const int64_t s = s0 + k;
@@ -329,102 +415,108 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     }
     s_u[k] = u;
   }
-  for (int m = tid; m < nh; m += kThreads) s_gb[m] = ScalarTraits<T>::zero();
   __syncthreads();
-  // Q = conj(t) u, split into hi/lo, written as B rows (re: m, im: Mp + m) x KC samples;
-  // item (m, k8) covers 8 consecutive samples -> one 16-byte store per row and term
+  const bool loaded = umma::mbar_wait(&bars[0], 0, kWaitLimit);
+  if (!loaded) record_error(status, QES_ERR_TIMEOUT);
+  // Q = conj(t) u in place: item (m, k8) = rows m (re) and Mp + m (im) for 8 samples
   const int items = Mp * (KC / 8);
-  for (int it = tid; it < items; it += kThreads) {
+  for (int it = tid; loaded && it < items; it += kThreads) {
     const int m = it % Mp, k8 = it / Mp;
+    const uint32_t offr = umma::kmajor_offset(m, 8 * k8, Np);
+    float trh[8], trl[8], tih[8], til[8];
+    unpack8(*reinterpret_cast<const uint4*>(sBh + offr), trh);
+    unpack8(*reinterpret_cast<const uint4*>(sBl + offr), trl);
+    uint32_t offi = 0;
+    if constexpr (CPLX) {
+      offi = umma::kmajor_offset(Mp + m, 8 * k8, Np);
+      unpack8(*reinterpret_cast<const uint4*>(sBh + offi), tih);
+      unpack8(*reinterpret_cast<const uint4*>(sBl + offi), til);
+    }
     uint16_t rh[8], rl[8], ih[8], il[8];
-    T qs = ScalarTraits<T>::zero();
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int k = 8 * k8 + q;
-      const int64_t s = s0 + k;
-      T qv = ScalarTraits<T>::zero();
-      if (m < nh && s < n_samples) qv = mulx(conjx(tanh_theta[s * nh + m]), s_u[k]);
-      qs = addx(qs, qv);
-      const float qr = to_re(qv);
-      split_bf16(qr, rh[q], rl[q]);
-      if constexpr (CPLX) split_bf16(qv.y, ih[q], il[q]);
-    }
-    const uint32_t off = umma::kmajor_offset(m, 8 * k8, Np);
-    *reinterpret_cast<uint4*>(sBh + off) = make_uint4(pack2(rh[0], rh[1]), pack2(rh[2], rh[3]), pack2(rh[4], rh[5]), pack2(rh[6], rh[7]));
-    *reinterpret_cast<uint4*>(sBl + off) = make_uint4(pack2(rl[0], rl[1]), pack2(rl[2], rl[3]), pack2(rl[4], rl[5]), pack2(rl[6], rl[7]));
-    if constexpr (CPLX) {
-      const uint32_t offi = umma::kmajor_offset(Mp + m, 8 * k8, Np);
-      *reinterpret_cast<uint4*>(sBh + offi) = make_uint4(pack2(ih[0], ih[1]), pack2(ih[2], ih[3]), pack2(ih[4], ih[5]), pack2(ih[6], ih[7]));
-      *reinterpret_cast<uint4*>(sBl + offi) = make_uint4(pack2(il[0], il[1]), pack2(il[2], il[3]), pack2(il[4], il[5]), pack2(il[6], il[7]));
-    }
-    if (m < nh) {
+      const T u = s_u[8 * k8 + q];
+      T qv;
       if constexpr (CPLX) {
-        atomicAdd(&s_gb[m].x, qs.x);
-        atomicAdd(&s_gb[m].y, qs.y);
+        const float a = trh[q] + trl[q], b = tih[q] + til[q];     // t = a + i b
+        qv = make_float2(a * u.x + b * u.y, a * u.y - b * u.x);    // conj(t) u
+        split_bf16(qv.x, rh[q], rl[q]);
+        split_bf16(qv.y, ih[q], il[q]);
       } else {
-        atomicAdd(&s_gb[m], qs);
+        qv = (trh[q] + trl[q]) * u;
+        split_bf16(qv, rh[q], rl[q]);
       }
+    }
+    *reinterpret_cast<uint4*>(sBh + offr) = pack8(rh);
+    *reinterpret_cast<uint4*>(sBl + offr) = pack8(rl);
+    if constexpr (CPLX) {
+      *reinterpret_cast<uint4*>(sBh + offi) = pack8(ih);
+      *reinterpret_cast<uint4*>(sBl + offi) = pack8(il);
     }
   }
   umma::fence_proxy_async_smem();     // generic-proxy stores -> visible to the tensor core
   __syncthreads();
-  bool ok = true;
-  if (tid == 0) {
-    if (!umma::mbar_wait(&bars[0], 0, kWaitLimit)) {
-      ok = false;
-      record_error(status, QES_ERR_TIMEOUT);
-    }
-    if (ok) {
-      umma::tc_fence_after();
-      const uint32_t idesc = umma::idesc_bf16_f32(128, Mp);
-      const uint32_t aaddr = umma::smem_u32(sA), bh = umma::smem_u32(sBh), bl = umma::smem_u32(sBl);
-      const int halves = CPLX ? 2 : 1;
-      for (int j = 0; j < KC / 16; ++j) {
-        const uint64_t ad = umma::smem_desc(aaddr + 2u * j * 128u * 16u, 128u * 16u, 128u);
-        for (int term = 0; term < 2; ++term) {
-          const uint32_t bb = term ? bl : bh;
-          for (int h = 0; h < halves; ++h) {
-            const uint64_t bd = umma::smem_desc(bb + (uint32_t)h * (Mp / 8) * 128u + 2u * j * Np * 16u, Np * 16u, 128u);
-            umma::mma_bf16(tbase + (uint32_t)h * d.im_off, ad, bd, idesc, (j > 0 || term > 0) ? 1u : 0u);
-          }
+  if (tid == 0 && loaded) {
+    umma::tc_fence_after();
+    const uint32_t idesc = umma::idesc_bf16_f32(128, Mp);
+    const uint32_t aaddr = umma::smem_u32(sA), bh = umma::smem_u32(sBh), bl = umma::smem_u32(sBl);
+    const int halves = CPLX ? 2 : 1;
+    for (int j = 0; j < KC / 16; ++j) {
+      const uint64_t ad = umma::smem_desc(aaddr + 2u * j * 128u * 16u, 128u * 16u, 128u);
+      for (int term = 0; term < 2; ++term) {
+        const uint32_t bb = term ? bl : bh;
+        for (int h = 0; h < halves; ++h) {
+          const uint64_t bd = umma::smem_desc(bb + (uint32_t)h * (Mp / 8) * 128u + 2u * j * Np * 16u, Np * 16u, 128u);
+          umma::mma_bf16(tbase + (uint32_t)h * d.im_off, ad, bd, idesc, (j > 0 || term > 0) ? 1u : 0u);
         }
       }
-      umma::mma_commit(&bars[1]);
-    } else {
-      umma::mbar_wait(&bars[0], 0, kWaitLimit);      // let the copy in flight land before exit
     }
-    s_issued = ok ? 1 : 0;
+    umma::mma_commit(&bars[1]);
+    s_issued = 1;
   }
-  // while the tensor core runs: g_a[i] = sum_s sigma_si u_s and g_b of this chunk
+  // while the tensor core runs: g_a[i] = sum_s sigma_si u_s (sigma read from the A tile) and g_b
   T* out = partial + (int64_t)chunk * P;
-  for (int i = tid; i < ns; i += kThreads) {
+  for (int base = 0; base < ns * 4; base += kThreads) {       // uniform trip count for the shuffles
+    const int it = base + tid;
+    const bool act = it < ns * 4;
+    const int i = act ? (it >> 2) : 0, grp = it & 3;
     T ga = ScalarTraits<T>::zero();
-    for (int k = 0; k < KC; ++k) {
-      const int64_t s = s0 + k;
-      if (s >= n_samples) break;
-      const float sg = ((bits[s * n_words(ns) + (i >> 5)] >> (i & 31)) & 1u) ? 1.f : -1.f;
-      ga = addx(ga, scal(sg, s_u[k]));
+    for (int k = grp; act && loaded && k < KC; k += 4) {
+      const uint16_t sb = *reinterpret_cast<const uint16_t*>(sA + umma::kmajor_offset(i, k, 128));
+      ga = addx(ga, scal(bf16_val(sb), s_u[k]));
     }
-    out[i] = ga;
+    if constexpr (CPLX) {
+      ga.x += __shfl_xor_sync(0xffffffffu, ga.x, 1);
+      ga.y += __shfl_xor_sync(0xffffffffu, ga.y, 1);
+      ga.x += __shfl_xor_sync(0xffffffffu, ga.x, 2);
+      ga.y += __shfl_xor_sync(0xffffffffu, ga.y, 2);
+    } else {
+      ga += __shfl_xor_sync(0xffffffffu, ga, 1);
+      ga += __shfl_xor_sync(0xffffffffu, ga, 2);
+    }
+    if (act && grp == 0) out[i] = ga;
   }
-  for (int m = tid; m < nh; m += kThreads) out[ns + m] = s_gb[m];
   __syncthreads();
   if (s_issued && !umma::mbar_wait(&bars[1], 0, kWaitLimit)) record_error(status, QES_ERR_TIMEOUT);
   umma::tc_fence_after();
-  const int i = 32 * warp + lane;                         // site row of the accumulator
-  const uint32_t lane_addr = tbase + ((uint32_t)(32 * warp) << 16);
-  for (int c0 = 0; c0 < Mp; c0 += 16) {
-    float gr[16], gi[16];
-    umma::tmem_ld16(lane_addr + c0, gr);
-    if constexpr (CPLX) umma::tmem_ld16(lane_addr + d.im_off + c0, gi);
-    if (i < ns) {
-      T* row = out + ns + nh + (int64_t)i * nh;
+  const int quarter = warp & 3, cg = warp >> 2;
+  const int i = 32 * quarter + lane;                      // site row of the accumulator
+  const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+  if (s_issued) {
+    for (int c = cg; c < Mp / 16; c += kColGroups) {
+      const int c0 = 16 * c;
+      float gr[16], gi[16];
+      umma::tmem_ld16(lane_addr + c0, gr);
+      if constexpr (CPLX) umma::tmem_ld16(lane_addr + d.im_off + c0, gi);
+      if (i < ns || i == 127) {
+        T* rowp = (i == 127) ? out + ns : out + ns + nh + (int64_t)i * nh;   // row 127 = g_b
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int m = c0 + q;
-        if (m < nh) {
-          if constexpr (CPLX) row[m] = make_float2(gr[q], gi[q]);
-          else row[m] = gr[q];
+        for (int q = 0; q < 16; ++q) {
+          const int m = c0 + q;
+          if (m < nh) {
+            if constexpr (CPLX) rowp[m] = make_float2(gr[q], gi[q]);
+            else rowp[m] = gr[q];
+          }
         }
       }
     }
@@ -434,34 +526,38 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   if (warp == 0) umma::tmem_dealloc(tbase, d.tmem_cols);
 }
 
-// ------------------------------------------------------------------------------------------------
+// ================================================================================================
 // host side
-// ------------------------------------------------------------------------------------------------
+// ================================================================================================
 static int pow2_at_least(int x) {
   int p = 32;
   while (p < x) p <<= 1;
   return p;
 }
 
-bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* d) {
+bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   const bool cplx = dtype == QES_DTYPE_C64;
   TcDims t{};
   t.ns = ns;
   t.nh = nh;
-  t.Kp = (ns + 15) / 16 * 16;
+  t.KCH = 32;
   t.Mp = (nh + 15) / 16 * 16;
   t.Np = cplx ? 2 * t.Mp : t.Mp;
-  if (ns > 128 || t.Mp > 256 || n_samples < 1) return false;
+  t.Kd = cplx ? 2 * t.Mp : (nh + 31) / 32 * 32;               // multiple of KCH
+  t.Sp = cplx ? (ns + 1 + 7) / 8 * 8 : (ns + 1 + 15) / 16 * 16;  // sites + the v_b row
+  t.NB = cplx ? 2 * t.Sp : t.Sp;
+  if (ns > 127 || t.Mp > 256 || t.NB > 256 || n_samples < 1) return false;   // row 127 holds the ones
+  if (t.Kd % t.KCH != 0) return false;
   t.im_off = pow2_at_least(t.Mp);
-  t.tmem_cols = cplx ? 2 * t.im_off : t.im_off;
+  t.tmem_cols = pow2_at_least(std::max(cplx ? 2 * t.im_off : t.im_off, t.NB));
   if (t.tmem_cols > 512) return false;
   const size_t tsz = cplx ? 8 : 4;
-  const size_t ov_smem = 128u * t.Kp * 2 + 2u * t.Np * t.Kp * 2 + (ns + nh) * tsz + 64;
+  const size_t stage = 2u * (128u * t.KCH * 2 + (size_t)t.NB * t.KCH * 2);
+  const size_t ov_smem = kStages * stage + 8 * (2 * kStages + 1) + 16 + (size_t)ns * tsz + 64;
   if (ov_smem > kTcSmemLimit) return false;
-  // largest multiple of 16 (<= 256) whose ohu shared memory fits
   int kc = 256;
   while (kc >= 16) {
-    const size_t sm = 128u * kc * 2 + 2u * t.Np * kc * 2 + (kc + nh) * tsz + 64;
+    const size_t sm = 128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64;
     if (sm <= kTcSmemLimit) break;
     kc -= 16;
   }
@@ -470,81 +566,99 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* d) {
   t.n_tiles = (int)((n_samples + 127) / 128);
   t.n_chunks = (int)((n_samples + kc - 1) / kc);
   t.ov_smem = (int)ov_smem;
-  t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (kc + nh) * tsz + 64);
-  *d = t;
+  t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64);
+  *dout = t;
   return true;
 }
 
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+static size_t sz_t_rows(const TcDims& d) { return (size_t)d.n_tiles * 128 * d.Kd * 2 * 2; }
+static size_t sz_t_cols(const TcDims& d) { return (size_t)d.n_chunks * d.Np * d.KC * 2 * 2; }
+static size_t sz_sig_cols(const TcDims& d) { return (size_t)d.n_chunks * 128 * d.KC * 2; }
+static size_t sz_vp(const TcDims& d) { return (size_t)d.NB * d.Kd * 2 * 2; }
+
 size_t tc_workspace_bytes(const TcDims& d) {
-  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  return al((size_t)d.n_tiles * 128 * d.Kp * 2) + al((size_t)d.n_chunks * 128 * d.KC * 2) +
-         2 * al((size_t)d.Np * d.Kp * 2) + al((size_t)d.n_tiles * sizeof(double2)) + al(sizeof(int) * 4);
+  return al256(sz_t_rows(d)) + al256(sz_t_cols(d)) + al256(sz_sig_cols(d)) + al256(sz_vp(d)) +
+         al256((size_t)d.n_tiles * sizeof(double2)) + al256(sizeof(int) * 4);
 }
 
 TcWork tc_layout(const TcDims& d, char* base) {
-  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   TcWork w{};
   size_t off = 0;
-  w.sig_rows = (uint16_t*)(base + off); off += al((size_t)d.n_tiles * 128 * d.Kp * 2);
-  w.sig_cols = (uint16_t*)(base + off); off += al((size_t)d.n_chunks * 128 * d.KC * 2);
-  w.bhi = (uint16_t*)(base + off); off += al((size_t)d.Np * d.Kp * 2);
-  w.blo = (uint16_t*)(base + off); off += al((size_t)d.Np * d.Kp * 2);
-  w.wsum = (double2*)(base + off); off += al((size_t)d.n_tiles * sizeof(double2));
-  w.status = (int*)(base + off); off += al(sizeof(int) * 4);
+  w.t_rows = (uint16_t*)(base + off); off += al256(sz_t_rows(d));
+  w.t_cols = (uint16_t*)(base + off); off += al256(sz_t_cols(d));
+  w.sig_cols = (uint16_t*)(base + off); off += al256(sz_sig_cols(d));
+  w.vp = (uint16_t*)(base + off); off += al256(sz_vp(d));
+  w.wsum = (double2*)(base + off); off += al256((size_t)d.n_tiles * sizeof(double2));
+  w.status = (int*)(base + off); off += al256(sizeof(int) * 4);
   return w;
 }
 
-int tc_prepare_step(const TcDims& d, int64_t n_samples, const uint32_t* bits, const TcWork& w, cudaStream_t st) {
+template <class T, class V>
+static int tc_set_attrs() {
+  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ov_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemLimit));
+  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemLimit));
+  return QES_OK;
+}
+
+int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
+                    const TcWork& w, cudaStream_t st) {
+  int rc = (dtype == QES_DTYPE_C64) ? tc_set_attrs<float2, double2>() : tc_set_attrs<float, double>();
+  if (rc) return rc;
   QES_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int), st));
-  tc_sigma_rows_kernel<<<592, 256, 0, st>>>(d.ns, d.Kp, n_samples, d.n_tiles, bits, w.sig_rows);
+  tc_sigma_cols_kernel<<<1184, 256, 0, st>>>(d.ns, d.KC, n_samples, d.n_chunks, bits, w.sig_cols);
   QES_LAUNCH_CHECK();
-  tc_sigma_cols_kernel<<<592, 256, 0, st>>>(d.ns, d.KC, n_samples, d.n_chunks, bits, w.sig_cols);
-  QES_LAUNCH_CHECK();
+  if (dtype == QES_DTYPE_C64) {
+    tc_t_rows_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_rows);
+    QES_LAUNCH_CHECK();
+    tc_t_cols_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_cols);
+    QES_LAUNCH_CHECK();
+  } else {
+    tc_t_rows_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_rows);
+    QES_LAUNCH_CHECK();
+    tc_t_cols_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_cols);
+    QES_LAUNCH_CHECK();
+  }
   return QES_OK;
 }
 
 template <class T, class V>
-static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const T* tt, const V* v,
-                       float2* w_out, T* partial, const TcWork& w, cudaStream_t st) {
-  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ov_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemLimit));
-  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemLimit));
+static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const V* v, float2* w_out,
+                       T* partial, const TcWork& w, cudaStream_t st, bool build_vp) {
   const bool cplx = ScalarTraits<T>::is_complex;
-  const int items = d.Np * (d.Kp / 8);
-  tc_build_v_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d.ns, d.nh, d.Kp, d.Mp, d.Np, cplx, v, w.bhi, w.blo);
+  if (build_vp) {
+    const int items = d.NB * (d.Kd / 8);
+    tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
+    QES_LAUNCH_CHECK();
+  }
+  tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
+                                                           w.status);
   QES_LAUNCH_CHECK();
-  tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, tt, v, w.sig_rows, w.bhi, w.blo, w_out,
-                                                           w.wsum, w.status);
-  QES_LAUNCH_CHECK();
-  tc_ohu_kernel<T><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, bits, tt, w_out, w.wsum, d.n_tiles,
-                                                             1.0 / (double)n_samples, w.sig_cols, partial, w.status);
+  tc_ohu_kernel<T><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, w_out, w.wsum, d.n_tiles,
+                                                             1.0 / (double)n_samples, w.sig_cols, w.t_cols, partial,
+                                                             w.status);
   QES_LAUNCH_CHECK();
   return QES_OK;
 }
 
-int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
-              const void* v, float2* w_out, void* partial, const TcWork& w, cudaStream_t st) {
+int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
+              void* partial, const TcWork& w, cudaStream_t st, bool build_vp) {
   if (dtype == QES_DTYPE_C64)
-    return tc_matvec_t<float2, double2>(d, n_samples, bits, (const float2*)tanh_theta, (const double2*)v, w_out,
-                                        (float2*)partial, w, st);
-  return tc_matvec_t<float, double>(d, n_samples, bits, (const float*)tanh_theta, (const double*)v, w_out,
-                                    (float*)partial, w, st);
+    return tc_matvec_t<float2, double2>(d, n_samples, bits, (const double2*)v, w_out, (float2*)partial, w, st,
+                                        build_vp);
+  return tc_matvec_t<float, double>(d, n_samples, bits, (const double*)v, w_out, (float*)partial, w, st, build_vp);
 }
 
-// O^H ((g - [mean g]) * scale) alone (force / VJP): the ohu kernel with the caller's vector
-int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
-           const float2* g, const double2* gsum_part, int gsum_n, double scale, void* partial, const TcWork& w,
-           cudaStream_t st) {
-  if (dtype == QES_DTYPE_C64) {
-    QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemLimit));
-    tc_ohu_kernel<float2><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, bits, (const float2*)tanh_theta, g,
-                                                                    gsum_part, gsum_n, scale, w.sig_cols,
-                                                                    (float2*)partial, w.status);
-  } else {
-    QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemLimit));
-    tc_ohu_kernel<float><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, bits, (const float*)tanh_theta, g,
-                                                                   gsum_part, gsum_n, scale, w.sig_cols,
-                                                                   (float*)partial, w.status);
-  }
+int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
+           double scale, void* partial, const TcWork& w, cudaStream_t st) {
+  if (dtype == QES_DTYPE_C64)
+    tc_ohu_kernel<float2><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, g, gsum_part, gsum_n, scale,
+                                                                    w.sig_cols, w.t_cols, (float2*)partial, w.status);
+  else
+    tc_ohu_kernel<float><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, g, gsum_part, gsum_n, scale,
+                                                                   w.sig_cols, w.t_cols, (float*)partial, w.status);
   QES_LAUNCH_CHECK();
   return QES_OK;
 }

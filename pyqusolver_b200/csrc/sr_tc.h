@@ -7,11 +7,14 @@
 
 struct TcDims {
   int ns, nh;        // sites, hidden units
-  int Kp;            // sites padded to 16 (K of the ov GEMM)
-  int Mp;            // hidden units padded to 16 (N of one MMA)
-  int Np;            // operand rows: 2*Mp (complex) or Mp (real)
+  int Mp;            // hidden units padded to 16 (N of one ohu MMA)
+  int Np;            // ohu B rows: 2*Mp (complex) or Mp (real)
+  int Kd;            // ov K: 2*Mp (complex: [Re t | Im t]) or nh padded to KCH (real)
+  int KCH;           // ov K chunk per pipeline stage
+  int Sp;            // sites + the v_b row, padded (rows of one Y half)
+  int NB;            // ov N: 2*Sp (complex) or Sp (real)
   int KC;            // samples per ohu chunk (K of the ohu GEMM, multiple of 16)
-  int im_off;        // TMEM column offset of the imaginary half
+  int im_off;        // TMEM column offset of the imaginary half (ohu)
   int tmem_cols;     // TMEM columns allocated per CTA
   int n_tiles;       // ceil(Ns / 128)
   int n_chunks;      // ceil(Ns / KC)
@@ -19,10 +22,10 @@ struct TcDims {
 };
 
 struct TcWork {
-  uint16_t* sig_rows;   // n_tiles x (128 x Kp) bf16, canonical K-major
-  uint16_t* sig_cols;   // n_chunks x (128 x KC) bf16, canonical K-major
-  uint16_t* bhi;        // Np x Kp bf16
-  uint16_t* blo;
+  uint16_t* t_rows;     // ov A: per tile and K chunk, hi/lo BF16 tiles of T
+  uint16_t* t_cols;     // ohu B before scaling: per sample chunk, hi/lo BF16 tiles of T^T
+  uint16_t* sig_cols;   // ohu A: per sample chunk, Sigma^T (128 x KC) BF16
+  uint16_t* vp;         // ov B: V' hi/lo BF16 tiles (per CG iteration)
   double2* wsum;        // n_tiles partial sums of w = O v
   int* status;          // first error code of a bounded wait
 };
@@ -32,11 +35,40 @@ constexpr size_t kTcSmemLimit = 220 * 1024;
 bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* d);
 size_t tc_workspace_bytes(const TcDims& d);
 TcWork tc_layout(const TcDims& d, char* base);
-int tc_prepare_step(const TcDims& d, int64_t n_samples, const uint32_t* bits, const TcWork& w, cudaStream_t st);
-int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
-              const void* v, float2* w_out, void* partial, const TcWork& w, cudaStream_t st);
-// g centring: gsum_n > 0 -> gsum_part holds gsum_n partial sums (mean = sum / Ns);
-// gsum_n < 0 -> gsum_part[0] is the mean; gsum_part == nullptr -> no centring
-int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
-           const float2* g, const double2* gsum_part, int gsum_n, double scale, void* partial, const TcWork& w,
-           cudaStream_t st);
+// once per VMC step: BF16 tiles of T, T^T and Sigma^T
+int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
+                    const TcWork& w, cudaStream_t st);
+// w_out = O v, partial[chunk] = O^H ((w - mean w) / Ns)
+int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
+              void* partial, const TcWork& w, cudaStream_t st, bool build_vp = true);
+// partial[chunk] = O^H ((g - mean) * scale): gsum_n > 0 -> gsum_part holds gsum_n partial sums
+// (mean = sum / Ns); gsum_n < 0 -> gsum_part[0] is the mean; gsum_part == nullptr -> no centring
+int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
+           double scale, void* partial, const TcWork& w, cudaStream_t st);
+
+// Writes the V' operand entries of one element of the direction vector (site i, hidden unit m;
+// i == ns for the v_b part) straight into the chunked BF16 hi/lo tiles: used by the CG direction
+// update so that no separate operand-building pass is needed.
+#ifdef __CUDACC__
+#include <cuda_bf16.h>
+#include "umma.cuh"
+__device__ __forceinline__ void tc_put_vp(const TcDims& d, uint16_t* vp, int n, int k, float x) {
+  const uint16_t hi = __bfloat16_as_ushort(__float2bfloat16_rn(x));
+  const uint16_t lo = __bfloat16_as_ushort(__float2bfloat16_rn(x - __bfloat162float(__ushort_as_bfloat16(hi))));
+  const size_t term_bytes = (size_t)d.NB * d.KCH * 2;
+  uint8_t* base = reinterpret_cast<uint8_t*>(vp) + (size_t)(k / d.KCH) * 2 * term_bytes;
+  const uint32_t off = umma::kmajor_offset((uint32_t)n, (uint32_t)(k % d.KCH), (uint32_t)d.NB);
+  *reinterpret_cast<uint16_t*>(base + off) = hi;
+  *reinterpret_cast<uint16_t*>(base + term_bytes + off) = lo;
+}
+__device__ __forceinline__ void tc_put_vp_elem(const TcDims& d, uint16_t* vp, int i, int m, double vr) {
+  tc_put_vp(d, vp, i, m, (float)vr);                         // real RBM: row i, column m
+}
+__device__ __forceinline__ void tc_put_vp_elem(const TcDims& d, uint16_t* vp, int i, int m, double2 v) {
+  const float vr = (float)v.x, vi = (float)v.y;
+  tc_put_vp(d, vp, i, m, vr);                                // Re Y row: [Re v | -Im v]
+  tc_put_vp(d, vp, i, d.Mp + m, -vi);
+  tc_put_vp(d, vp, d.Sp + i, m, vi);                         // Im Y row: [Im v | Re v]
+  tc_put_vp(d, vp, d.Sp + i, d.Mp + m, vr);
+}
+#endif

@@ -366,3 +366,26 @@ def test_sr_force_and_cg_tensor_cores_match_cuda_cores(sr_impl, cplx):
         out[impl] = (F, x.cpu().numpy())
     assert rel_err(out[2][0], out[1][0]) < 1e-4
     assert rel_err(out[2][1], out[1][1]) < 1e-3
+
+
+def test_cg_graph_replay_matches_direct_launches():
+    ns, nh, n = 16, 32, 3000
+    L = qb.SquareLattice(2, 4, 4)
+    model = qb.XXZ(L, jxy=-1.0, jz=-1.0)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64", seed=31, init_scale=0.2)
+    bits = dv.init_chains(_lib.INIT_RND_FIXED, n, ns, seed=5, n_up=8)
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    out = []
+    try:
+        for g in (0, 1, 1):
+            _lib.call("qes_set_cg_graphs", g)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-3, rtol=1e-10, maxiter=400,
+                                     check_every=8)
+            out.append((x.cpu().numpy(), info["iterations"]))
+    finally:
+        _lib.call("qes_set_cg_graphs", 1)
+    assert out[0][1] == out[1][1] == out[2][1]
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[1][0], out[2][0])

@@ -376,20 +376,36 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   const int chunk = blockIdx.x;
   const int64_t s0 = (int64_t)chunk * KC;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  __shared__ double2 s_red[kWarps];
   if (tid == 0) {
     umma::mbar_init(&bars[0], 1);
     umma::mbar_init(&bars[1], 1);
     umma::fence_mbar_init();
-    double2 t = make_double2(0.0, 0.0);
-    if (wsum_part && wsum_n > 0) {
-      for (int q = 0; q < wsum_n; ++q) { t.x += wsum_part[q].x; t.y += wsum_part[q].y; }
-      t.x /= (double)n_samples;
-      t.y /= (double)n_samples;
-    } else if (wsum_part) {
-      t = wsum_part[0];              // the mean itself
-    }
-    s_mean = t;
     s_issued = 0;
+  }
+  // mean of w: the per-tile partial sums are reduced by the whole block (fixed order)
+  {
+    double2 t = make_double2(0.0, 0.0);
+    if (wsum_part && wsum_n > 0)
+      for (int q = tid; q < wsum_n; q += kThreads) { t.x += wsum_part[q].x; t.y += wsum_part[q].y; }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+    }
+    if (lane == 0) s_red[warp] = t;
+    __syncthreads();
+    if (tid == 0) {
+      double2 m = make_double2(0.0, 0.0);
+      if (wsum_part && wsum_n > 0) {
+        for (int q = 0; q < kWarps; ++q) { m.x += s_red[q].x; m.y += s_red[q].y; }
+        m.x /= (double)n_samples;
+        m.y /= (double)n_samples;
+      } else if (wsum_part) {
+        m = wsum_part[0];            // the mean itself
+      }
+      s_mean = m;
+    }
   }
   if (warp == 0) {
     umma::tmem_alloc(tslot, d.tmem_cols);
@@ -510,12 +526,25 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
       if constexpr (CPLX) umma::tmem_ld16(lane_addr + d.im_off + c0, gi);
       if (i < ns || i == 127) {
         T* rowp = (i == 127) ? out + ns : out + ns + nh + (int64_t)i * nh;   // row 127 = g_b
+        // 16-byte stores when the row chunk is aligned and complete, element stores otherwise
+        const bool vec = (c0 + 16 <= nh) && ((reinterpret_cast<uintptr_t>(rowp + c0) & 15) == 0);
+        if (vec) {
+          float4* dst = reinterpret_cast<float4*>(rowp + c0);
+          if constexpr (CPLX) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int m = c0 + q;
-          if (m < nh) {
-            if constexpr (CPLX) rowp[m] = make_float2(gr[q], gi[q]);
-            else rowp[m] = gr[q];
+            for (int q = 0; q < 8; ++q) dst[q] = make_float4(gr[2 * q], gi[2 * q], gr[2 * q + 1], gi[2 * q + 1]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dst[q] = make_float4(gr[4 * q], gr[4 * q + 1], gr[4 * q + 2], gr[4 * q + 3]);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int m = c0 + q;
+            if (m < nh) {
+              if constexpr (CPLX) rowp[m] = make_float2(gr[q], gi[q]);
+              else rowp[m] = gr[q];
+            }
           }
         }
       }

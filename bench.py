@@ -37,16 +37,16 @@ METRIC = "VMC steps/s & samples/s: mixed+batched vs plain FP32 on B200 at equal 
 
 CONFIGS = {
     # name: (dim, lx, ly, model, coupling kwargs, alpha, dtype, chains, samples, rule, sweep, shift, lr, cg rtol)
-    "heis10x10": dict(dim=2, lx=10, ly=10, model="xxz", kw=dict(jxy=-1.0, jz=-1.0), alpha=2, dtype="complex64",
+    "heis10x10": dict(name="heis10x10", dim=2, lx=10, ly=10, model="xxz", kw=dict(jxy=-1.0, jz=-1.0), alpha=2, dtype="complex64",
                       chains=4096, samples=4, rule="EXCHANGE", sweep=100, shift=1e-3, lr=0.01, rtol=1e-8,
                       maxiter=1000, init="RND_FIXED"),
-    "tfim16": dict(dim=1, lx=16, ly=1, model="tfim", kw=dict(j=1.0, hx=1.0, hz=0.0), alpha=1, dtype="float32",
+    "tfim16": dict(name="tfim16", dim=1, lx=16, ly=1, model="tfim", kw=dict(j=1.0, hx=1.0, hz=0.0), alpha=1, dtype="float32",
                    chains=16, samples=64, rule="LOCAL", sweep=16, shift=1e-3, lr=0.01, rtol=1e-8, maxiter=1000,
                    init="RND"),
-    "j1j2_6x6": dict(dim=2, lx=6, ly=6, model="j1j2", kw=dict(J1=-1.0, J2=-0.5), alpha=4, dtype="complex64",
+    "j1j2_6x6": dict(name="j1j2_6x6", dim=2, lx=6, ly=6, model="j1j2", kw=dict(J1=-1.0, J2=-0.5), alpha=4, dtype="complex64",
                      chains=2048, samples=4, rule="EXCHANGE", sweep=36, shift=1e-3, lr=0.01, rtol=1e-8,
                      maxiter=1000, init="RND_FIXED"),
-    "tfim20x20": dict(dim=2, lx=20, ly=20, model="tfim", kw=dict(j=1.0, hx=3.04, hz=0.0), alpha=4, dtype="float32",
+    "tfim20x20": dict(name="tfim20x20", dim=2, lx=20, ly=20, model="tfim", kw=dict(j=1.0, hx=3.04, hz=0.0), alpha=4, dtype="float32",
                       chains=4096, samples=4, rule="LOCAL", sweep=400, shift=1e-4, lr=0.01, rtol=1e-8, maxiter=1000,
                       init="RND"),
 }
@@ -70,7 +70,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -147,30 +147,16 @@ def timed_step(nqs, tdvp, cfg, ev):
 PHASES = ["sample", "forward", "local_energy", "stats", "sr_solve", "update"]
 
 
-def run_ours(args, cfg, rank, world, local_rank):
+def timed_loop(nqs, tdvp, cfg, steps, flush, profile=False):
     import torch
     from pyqusolver_b200 import _lib
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    nqs, tdvp = build_nqs(cfg, seed=1234 + rank)
-    ns_per_step = cfg["chains"] * cfg["samples"]
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
     mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(7)]
-    # warm-up (the first call thermalises the chains)
-    for _ in range(args.warmup):
-        timed_step(nqs, tdvp, cfg, mk())
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
+    if profile:
+        _lib.profile_read(reset=True)
+        _lib.profile_enable(True)
     _lib.launch_count(reset=True)
     step_ms, phase_ms, cg_iters = [], {p: [] for p in PHASES}, []
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.fill_(1.0)
         ev = mk()
         timed_step(nqs, tdvp, cfg, ev)
@@ -180,22 +166,72 @@ def run_ours(args, cfg, rank, world, local_rank):
             phase_ms[p].append(ev[k].elapsed_time(ev[k + 1]))
         cg_iters.append(tdvp.last_info.get("iterations", 0))
     launches = _lib.launch_count(reset=True)
-    clk = clocks.stop()
-    total_ms = float(np.sum(step_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    prof = None
+    if profile:
+        prof = _lib.profile_read(reset=True)
+        _lib.profile_enable(False)
+    return step_ms, phase_ms, cg_iters, launches, prof
+
+
+def run_ours(args, cfg, rank, world, local_rank):
+    import torch
+    from pyqusolver_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ns_per_step = cfg["chains"] * cfg["samples"]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * ns_per_step * args.steps / (total_ms / 1e3)
-    ms_step = total_ms / args.steps
+        return float(t.item())
+
+    forms = {}
+    # plain FP32 form: every SR contraction on CUDA cores in float32 (float64 CG vectors)
+    # mixed form: SR contractions on tcgen05 tensor cores (BF16 hi/lo split, FP32 accumulate)
+    for form, impl in (("plain_fp32", _lib.SR_IMPL_CUDA_CORES), ("mixed", _lib.SR_IMPL_AUTO)):
+        _lib.set_sr_impl(impl)
+        nqs, tdvp = build_nqs(cfg, seed=1234 + rank)
+        for _ in range(args.warmup):                        # the first call thermalises the chains
+            timed_step(nqs, tdvp, cfg, [torch.cuda.Event(enable_timing=True) for _ in range(7)])
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        clocks = ClockSampler(local_rank) if form == "mixed" else None
+        if clocks:
+            clocks.start()
+        step_ms, phase_ms, cg_iters, launches, prof = timed_loop(nqs, tdvp, cfg, args.steps, flush,
+                                                                 profile=(form == "mixed"))
+        clk = clocks.stop() if clocks else None
+        total_ms = max_over_ranks(float(np.sum(step_ms)))
+        forms[form] = {"nqs": nqs, "tdvp": tdvp, "total_ms": total_ms, "phase_ms": phase_ms, "cg_iters": cg_iters,
+                       "launches": launches, "prof": prof, "clocks": clk,
+                       "energy": float(nqs_energy(tdvp.last_info))}
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+    mixed, plain = forms["mixed"], forms["plain_fp32"]
+    value = world * ns_per_step * args.steps / (mixed["total_ms"] / 1e3)
+    ms_step = mixed["total_ms"] / args.steps
+    nqs, tdvp = mixed["nqs"], mixed["tdvp"]
 
     # --- end to end through the public API with host buffers (params in, stats + params out)
     e2e = run_e2e(nqs, cfg, args, dist, world)
 
     # --- roofline of the dominant kernel (measured live over the timed steps)
-    roof = roofline(cfg, nqs, phase_ms, cg_iters)
+    roof = roofline(cfg, nqs, mixed)
 
-    stats = tdvp.last_info
+    def form_summary(f):
+        ms = f["total_ms"] / args.steps
+        return {"ms_per_step": ms, "vmc_steps_per_s": 1e3 / ms,
+                "samples_per_s": world * ns_per_step * 1e3 / ms,
+                "phase_ms": {p: float(np.mean(v)) for p, v in f["phase_ms"].items()},
+                "cg_iterations_mean": float(np.mean(f["cg_iters"])), "energy_mean_last": f["energy"]}
+
     line = {
         "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "vmc_steps_per_s": 1e3 / ms_step,
@@ -208,11 +244,13 @@ def run_ours(args, cfg, rank, world, local_rank):
                    "sr": f"structured CG fp64, shift {cfg['shift']}, rtol {cfg['rtol']}, maxiter {cfg['maxiter']}",
                    "lr": cfg["lr"], "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "phase_ms": {p: float(np.mean(v)) for p, v in phase_ms.items()},
-        "cg_iterations_mean": float(np.mean(cg_iters)),
-        "energy_mean_last": float(nqs_energy(stats)),
-        "gpu_launches": int(launches),
-        "clocks": clk,
+        "phase_ms": {p: float(np.mean(v)) for p, v in mixed["phase_ms"].items()},
+        "cg_iterations_mean": float(np.mean(mixed["cg_iters"])),
+        "energy_mean_last": mixed["energy"],
+        "forms": {"mixed": form_summary(mixed), "plain_fp32": form_summary(plain),
+                  "mixed_over_plain_steps_per_s": plain["total_ms"] / mixed["total_ms"]},
+        "gpu_launches": int(mixed["launches"]),
+        "clocks": mixed["clocks"],
         "e2e": e2e,
         "roofline": roof,
     }
@@ -264,8 +302,39 @@ def run_e2e(nqs, cfg, args, dist, world):
             "ms_per_step": total / args.steps}
 
 
-def roofline(cfg, nqs, phase_ms, cg_iters):
-    """Roofline of the dominant phase's kernel from the live CUDA-event times."""
+def kernel_bytes(cfg, nqs, kind, tc):
+    """Algorithmic bytes of one launch: every operand read once plus every output written once."""
+    net = nqs.net
+    ns, nh, n = net.ns, net.nh, cfg["chains"] * cfg["samples"]
+    cplx = net.is_complex
+    ts, vs = (8, 16) if cplx else (4, 8)
+    nw = (ns + 31) // 32
+    P = ns + nh + ns * nh
+    if tc:
+        Mp = (nh + 15) // 16 * 16
+        Np = 2 * Mp if cplx else Mp
+        Kd = 2 * Mp if cplx else (nh + 31) // 32 * 32
+        Sp = (ns + 1 + 7) // 8 * 8 if cplx else (ns + 1 + 15) // 16 * 16
+        NB = 2 * Sp if cplx else Sp
+        kc = 256
+        while kc >= 16 and 128 * kc * 2 + 2 * Np * kc * 2 + (kc + nh) * ts + 64 > 220 * 1024:
+            kc -= 16
+        n_tiles, n_chunks = (n + 127) // 128, (n + kc - 1) // kc
+        if kind == "ov":
+            return n_tiles * 128 * Kd * 4 + NB * Kd * 4 + n * nw * 4 + n * 8
+        if kind == "ohu":
+            return n_chunks * 128 * kc * 2 + n_chunks * Np * kc * 4 + n * 8 + n_chunks * P * ts
+        return n_chunks * P * ts + 2 * P * vs
+    nsplit = (n + 255) // 256
+    if kind == "ov":
+        return n * nh * ts + n * nw * 4 + P * vs + n * 8
+    if kind == "ohu":
+        return n * nh * ts + n * nw * 4 + n * 8 + nsplit * P * ts
+    return nsplit * P * ts + 2 * P * vs
+
+
+def roofline(cfg, nqs, form):
+    """Roofline of the kernel with the largest share of the timed steps (live CUDA-event times)."""
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -273,40 +342,38 @@ def roofline(cfg, nqs, phase_ms, cg_iters):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     src = "measured" if "hbm_gbs" in peaks else "fallback"
-    net = nqs.net
-    ns, nh, n = net.ns, net.nh, cfg["chains"] * cfg["samples"]
-    cplx = net.is_complex
-    ts = 8 if cplx else 4
-    mean = {p: float(np.mean(v)) for p, v in phase_ms.items()}
-    dom = max(mean, key=mean.get)
-    out = {"dominant_phase": dom}
-    if dom == "sr_solve":
-        # per CG iteration the matvec streams the packed spins and T = tanh(theta) twice
-        # (O v, then O^H u) plus the float64 vectors; algorithmic bytes per matvec:
-        it = max(1.0, float(np.mean(cg_iters)))
-        nw = (ns + 31) // 32
-        P = ns + nh + ns * nh
-        bytes_mv = 2 * (n * nh * ts + n * nw * 4) + 6 * P * (16 if cplx else 8)
-        t = mean["sr_solve"] / 1e3 / (it + 1)
-        ach = bytes_mv / t / 1e9
-        out.update({"kernel": "sr matvec (ov + ohu)", "bound": "hbm", "achieved": ach, "peak": hbm,
-                    "unit": "GB/s", "frac": ach / hbm, "traffic": None, "peak_source": src,
-                    "algorithmic_bytes_per_launch": bytes_mv})
-    elif dom == "sample":
-        nrec = cfg["samples"] * cfg["sweep"]
-        # per proposal and chain: one table row pair (C, S) of M entries
-        bytes_ = cfg["chains"] * nrec * 2 * nh * ts
-        t = mean["sample"] / 1e3
-        ach = bytes_ / t / 1e9
-        out.update({"kernel": "sampler_kernel", "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                    "frac": ach / hbm, "traffic": None, "peak_source": src,
-                    "algorithmic_bytes_per_launch": bytes_})
+    traffic_db = {}
+    try:
+        traffic_db = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic_per_launch.json")))
+    except (OSError, ValueError):
+        pass
+    steps = len(form["cg_iters"])
+    cands = {}
+    for k, (ms, cnt) in (form["prof"] or {}).items():
+        if cnt:
+            cands[k] = (ms, cnt)
+    for p in ("sample", "local_energy", "forward"):
+        cands[p] = (float(np.sum(form["phase_ms"][p])), steps)
+    dom = max(cands, key=lambda k: cands[k][0])
+    total_ms, cnt = cands[dom]
+    avg_s = total_ms / cnt / 1e3
+    names = {"ov": "tc_ov_kernel (O v, tcgen05)", "ohu": "tc_ohu_kernel (O^H u, tcgen05)",
+             "reduce": "reduce_splits_kernel", "sample": "sampler_kernel", "local_energy": "eloc_moves_kernel",
+             "forward": "rbm_forward_kernel"}
+    out = {"kernel": names.get(dom, dom), "launches_timed": cnt, "avg_launch_us": avg_s * 1e6,
+           "share_of_timed_region": total_ms / float(np.sum([np.sum(v) for v in form["phase_ms"].values()])),
+           "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src}
+    if dom in ("ov", "ohu", "reduce"):
+        b = kernel_bytes(cfg, nqs, dom, tc=True)
+        ach = b / avg_s / 1e9
+        tr = traffic_db.get(cfg.get("name", ""), {}).get(dom)
+        out.update({"achieved": ach, "frac": ach / hbm, "algorithmic_bytes_per_launch": b, "traffic": tr})
     else:
-        t = mean[dom] / 1e3
-        bytes_ = n * nh * ts
-        ach = bytes_ / t / 1e9
-        out.update({"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                    "traffic": None, "peak_source": src, "algorithmic_bytes_per_launch": bytes_})
+        net = nqs.net
+        n = cfg["chains"] * cfg["samples"]
+        b = n * net.nh * (8 if net.is_complex else 4) + n * ((net.ns + 31) // 32) * 4
+        ach = b / avg_s / 1e9
+        out.update({"achieved": ach, "frac": ach / hbm, "algorithmic_bytes_per_launch": b, "traffic": None})
     return out
 
 
@@ -383,7 +450,7 @@ def run_reference(args, cfg, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="heis10x10", choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

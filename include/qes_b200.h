@@ -238,6 +238,15 @@ int qes_set_sr_impl(int impl);
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);
 
+/* Per-kernel CUDA-event timing of the SR matvec halves, for measurement:
+ * while enabled, every launch of class k (0: O v, 1: O^H u, 2: split
+ * reduction) is bracketed by two events on its launch stream and CG graphs
+ * are bypassed.  qes_profile_read synchronises the device and returns the
+ * accumulated milliseconds and launch counts (reset != 0 zeroes them).
+ * No counterpart in the reference (it has no per-kernel timing).          */
+int qes_profile_enable(int enable);
+int qes_profile_read(int reset, double* total_ms, long long* counts, int n);
+
 /* F = O_c^H E_c / Ns (force) and the matvec y = (O_c^H O_c / Ns + shift) v. */
 int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples,
                  const uint32_t* bits, const void* tanh_theta, const void* eloc,

@@ -93,6 +93,8 @@ SIGNATURES = {
     "qes_sr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
     "qes_set_sr_impl": [C.c_int],
     "qes_set_cg_graphs": [C.c_int],
+    "qes_profile_enable": [C.c_int],
+    "qes_profile_read": [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int],
     "qes_sr_force": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_sr_matvec": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.c_double, _vp, _vp, _vp, _sz, _vp],
     "qes_sr_solve_cg": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
@@ -139,6 +141,21 @@ SR_IMPL_AUTO, SR_IMPL_CUDA_CORES, SR_IMPL_TENSOR_CORES = 0, 1, 2
 
 def set_sr_impl(impl: int):
     call("qes_set_sr_impl", int(impl))
+
+
+PROFILE_CLASSES = ("ov", "ohu", "reduce")
+
+
+def profile_enable(on: bool):
+    call("qes_profile_enable", 1 if on else 0)
+
+
+def profile_read(reset=True):
+    n = len(PROFILE_CLASSES)
+    ms = (C.c_double * n)()
+    cnt = (C.c_longlong * n)()
+    call("qes_profile_read", 1 if reset else 0, ms, cnt, n)
+    return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(PROFILE_CLASSES)}
 
 
 def launch_count(reset=False) -> int:

@@ -35,6 +35,13 @@ void qes_set_last_error(cudaError_t e, const char* what);
 void qes_set_last_message(const char* msg);
 void qes_count_launches(int n);
 
+// Per-kernel-class CUDA-event timing (enabled by qes_profile_enable): a launch site
+// brackets its kernel with qes_prof_begin / qes_prof_end on the launch stream.
+enum { QES_PROF_OV = 0, QES_PROF_OHU = 1, QES_PROF_REDUCE = 2, QES_PROF_CLASSES = 3 };
+bool qes_prof_on();
+int qes_prof_begin(int cls, cudaStream_t st);        // returns a slot or -1
+void qes_prof_end(int slot, cudaStream_t st);
+
 // ----------------------------------------------------------------------------
 // scalar algebra on float / float2
 // ----------------------------------------------------------------------------

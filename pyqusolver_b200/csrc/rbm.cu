@@ -18,6 +18,75 @@ static std::atomic<long long> g_launches{0};
 void qes_count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 extern "C" const char* qes_last_error(void) { return g_last_error; }
+
+// ---------------------------------------------------------------- per-kernel event timing
+#include <mutex>
+namespace {
+constexpr int kProfSlots = 8192;
+std::mutex g_prof_mu;
+std::atomic<int> g_prof_enabled{0};
+cudaEvent_t g_prof_ev[kProfSlots][2];
+int g_prof_cls[kProfSlots];
+int g_prof_used = 0;
+bool g_prof_created = false;
+double g_prof_ms[QES_PROF_CLASSES];
+long long g_prof_cnt[QES_PROF_CLASSES];
+}  // namespace
+
+bool qes_prof_on() { return g_prof_enabled.load(std::memory_order_relaxed) != 0; }
+
+int qes_prof_begin(int cls, cudaStream_t st) {
+  if (!qes_prof_on()) return -1;
+  std::lock_guard<std::mutex> lock(g_prof_mu);
+  if (!g_prof_created || g_prof_used >= kProfSlots) return -1;
+  const int slot = g_prof_used++;
+  g_prof_cls[slot] = cls;
+  if (cudaEventRecord(g_prof_ev[slot][0], st) != cudaSuccess) return -1;
+  return slot;
+}
+
+void qes_prof_end(int slot, cudaStream_t st) {
+  if (slot < 0) return;
+  cudaEventRecord(g_prof_ev[slot][1], st);
+}
+
+// folds the recorded pairs into the totals (the caller has synchronised)
+static void prof_collect() {
+  for (int q = 0; q < g_prof_used; ++q) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, g_prof_ev[q][0], g_prof_ev[q][1]) == cudaSuccess) {
+      g_prof_ms[g_prof_cls[q]] += ms;
+      g_prof_cnt[g_prof_cls[q]] += 1;
+    }
+  }
+  g_prof_used = 0;
+}
+
+extern "C" int qes_profile_enable(int enable) {
+  std::lock_guard<std::mutex> lock(g_prof_mu);
+  if (enable && !g_prof_created) {
+    for (int q = 0; q < kProfSlots; ++q) {
+      QES_CUDA_CHECK(cudaEventCreate(&g_prof_ev[q][0]));
+      QES_CUDA_CHECK(cudaEventCreate(&g_prof_ev[q][1]));
+    }
+    g_prof_created = true;
+  }
+  g_prof_enabled.store(enable ? 1 : 0);
+  return QES_OK;
+}
+
+extern "C" int qes_profile_read(int reset, double* total_ms, long long* counts, int n) {
+  std::lock_guard<std::mutex> lock(g_prof_mu);
+  QES_CUDA_CHECK(cudaDeviceSynchronize());
+  prof_collect();
+  for (int k = 0; k < n && k < QES_PROF_CLASSES; ++k) {
+    if (total_ms) total_ms[k] = g_prof_ms[k];
+    if (counts) counts[k] = g_prof_cnt[k];
+  }
+  if (reset)
+    for (int k = 0; k < QES_PROF_CLASSES; ++k) { g_prof_ms[k] = 0.0; g_prof_cnt[k] = 0; }
+  return QES_OK;
+}
 extern "C" long long qes_launch_count(int reset) {
   return reset ? g_launches.exchange(0) : g_launches.load();
 }

@@ -511,11 +511,15 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
   QES_ARG_CHECK(nsplit <= 65535, "SR: too many samples");
   dim3 grid((nh + OHU_TM - 1) / OHU_TM, (ns + OHU_TI - 1) / OHU_TI, (unsigned)nsplit);
   dim3 block(OHU_TM, OHU_TY);
+  const int pf = qes_prof_begin(QES_PROF_OHU, st);
   ohu_kernel<T><<<grid, block, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial);
   QES_LAUNCH_CHECK();
+  qes_prof_end(pf, st);
+  const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
   reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, (int)nsplit, (const T*)L.partial, shift, p, y,
                                                                  dot_part, dot_part ? L.scal : nullptr, L.counter);
   QES_LAUNCH_CHECK();
+  qes_prof_end(pfr, st);
   return QES_OK;
 }
 
@@ -525,9 +529,11 @@ static int apply_ov(int ns, int nh, int64_t n_samples, const uint32_t* bits, con
   const int nw = n_words(ns);
   const size_t sm = (size_t)OV_SB * nw * sizeof(uint32_t);
   QES_ARG_CHECK(sm <= 48 * 1024, "SR: ns too large");
+  const int pf = qes_prof_begin(QES_PROF_OV, st);
   ov_kernel<T, V><<<(unsigned)((n_samples + OV_SB - 1) / OV_SB), OV_THREADS, sm, st>>>(ns, nh, n_samples, bits, tt,
                                                                                      v, w);
   QES_LAUNCH_CHECK();
+  qes_prof_end(pf, st);
   mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, w, wmean);
   QES_LAUNCH_CHECK();
   return QES_OK;
@@ -603,9 +609,11 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
     int rc = tc_matvec(dtype, L.td, n_samples, bits, v, L.w, L.partial, L.tw, st, !vp_ready);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+    const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
     reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, L.nsplit, (const T*)L.partial, shift, v, y,
                                                                    dot_part, dot_part ? L.scal : nullptr, L.counter);
     QES_LAUNCH_CHECK();
+    qes_prof_end(pfr, st);
     return QES_OK;
   }
   int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, st);
@@ -731,7 +739,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   };
   int dev = 0;
   QES_CUDA_CHECK(cudaGetDevice(&dev));
-  const bool graphs = g_use_graphs.load() != 0 && dev >= 0 && dev < kMaxGraphDevices;
+  const bool graphs = g_use_graphs.load() != 0 && !qes_prof_on() && dev >= 0 && dev < kMaxGraphDevices;
   while (!done && it < opt->maxiter) {
     const int nrun = std::min(check, opt->maxiter - it);
     if (!graphs || it == 0 || nrun != check) {

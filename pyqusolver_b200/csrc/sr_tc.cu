@@ -662,13 +662,17 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
     tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
     QES_LAUNCH_CHECK();
   }
+  int pf = qes_prof_begin(QES_PROF_OV, st);
   tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
                                                            w.status);
   QES_LAUNCH_CHECK();
+  qes_prof_end(pf, st);
+  pf = qes_prof_begin(QES_PROF_OHU, st);
   tc_ohu_kernel<T><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, w_out, w.wsum, d.n_tiles,
                                                              1.0 / (double)n_samples, w.sig_cols, w.t_cols, partial,
                                                              w.status);
   QES_LAUNCH_CHECK();
+  qes_prof_end(pf, st);
   return QES_OK;
 }
 

@@ -191,6 +191,16 @@ int qes_loss_stats_workspace_bytes(int64_t n_samples, size_t* bytes);
 int qes_loss_stats(int64_t n_samples, const void* eloc, const float* probs,
                    double* out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Step diagnostics in float64: out = [r_hat, sigma2].  r_hat is the
+ * Gelman-Rubin statistic of Re E_loc split into n_chains contiguous blocks
+ * (NaN when n_chains <= 1, n_samples <= n_chains, n_samples % n_chains != 0
+ * or a block has one sample); sigma2 = var(Re E_loc), uniform weights,
+ * ddof 0.  Replaces TDVP._compute_step_rhat and the sigma2 of
+ * QES/NQS/src/tdvp.py:1487-1518, 1642-1643.                                */
+int qes_loss_rhat_workspace_bytes(int64_t n_samples, int n_chains, size_t* bytes);
+int qes_loss_rhat(int64_t n_samples, int n_chains, const void* eloc, double* out,
+                  void* workspace, size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Per-sample log-derivatives O (rows of P = ns + nh + ns*nh, leading dim ldo):
  * O_a = sigma_i, O_b = tanh theta_m, O_W = sigma_i tanh theta_m.
@@ -227,7 +237,7 @@ typedef struct {
 int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
 
 /* Matvec implementation of the SR calls in this process: 0 = 5th-generation
- * tensor cores (tcgen05, BF16 hi/lo split, FP32 accumulate) when ns <= 128,
+ * tensor cores (tcgen05, BF16 hi/lo split, FP32 accumulate) when ns <= 127,
  * nh <= 256 and the operands fit shared memory, CUDA cores otherwise
  * (default); 1 = CUDA cores only; 2 = tensor cores required (QES_ERR_SIZE
  * when the shapes do not allow them).  No counterpart in the reference
@@ -274,6 +284,92 @@ int qes_rbm_logpsi_vjp(int dtype, int ns, int nh, int64_t n_samples,
  * Replaces NQSTrainer._apply_parameter_update (QES/NQS/src/nqs_train.py:1235-1262). */
 int qes_param_update(int dtype, int64_t n_params, double lr, const void* x,
                      void* master, void* params, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched independent problems.  Many (RBM, Hamiltonian, chain set) triples
+ * of uneven size advance together: every phase of the VMC step is one
+ * launch over all problems.  The reference runs one NQS per problem
+ * (QES/NQS/nqs.py:241); these calls replace a Python loop over such objects.
+ *
+ * `inst` is a DEVICE array of n_inst descriptors.  Buffers are the
+ * concatenation of the per-problem buffers; each offset below is in elements
+ * (words for bit buffers) of the buffer it names.  Work lists are DEVICE
+ * arrays of int32 quadruples built by the host from the descriptors (the
+ * Python host orders them by decreasing cost); their meaning is given per
+ * call.  Problem b's sampler is bit-identical to qes_sampler_run with
+ * seed = inst[b].seed and chain_offset = 0.                                 */
+typedef struct {
+    int32_t ns, nh;                 /* sites, hidden units                          */
+    int32_t n_moves, n_zz, n_zfield;/* lowered Hamiltonian sizes                    */
+    int32_t n_chains, num_samples;  /* chains; recorded samples per chain per call  */
+    int32_t sweep_steps;            /* proposals between recorded samples           */
+    int64_t therm_steps_total;      /* proposals before the first record            */
+    uint64_t seed;                  /* Philox key of this problem                   */
+    int64_t param_off;              /* [a, b, W] in params and in every P-vector    */
+    int64_t chain_off;              /* chain_step / proposed / accepted / last_logpsi */
+    int64_t chain_word_off;         /* chain_bits                                   */
+    int64_t sample_off;             /* sample rows: logpsi, eloc (rows = n_chains*num_samples, sample-major) */
+    int64_t sample_word_off;        /* sample_bits                                  */
+    int64_t tanh_off;               /* tanh(theta) rows x nh                        */
+    int64_t flip_off;               /* single-flip tables, ns x nh (sampler)        */
+    int64_t move_table_off;         /* local-energy tables, nh x n_moves            */
+    int64_t move_off, zz_off, zf_off; /* move / zz / z-field arrays and move A values */
+    int64_t eloc_part_off;          /* local-energy partials, ceil(n_moves/32) x rows */
+    int64_t sr_part_off;            /* SR split partials, ceil(rows/256) x P        */
+} qes_batch_instance;
+
+/* ns x nh single-flip tables (mode 0, items (b, first element / 256, 0, 0),
+ * tables at flip_off, move-major) or the nh x n_moves local-energy tables
+ * (mode 1, tables at move_table_off, m-major, A at move_off) of every
+ * problem.  Same values as qes_rbm_move_tables.                            */
+int qes_batch_move_tables(int dtype, int n_inst, const qes_batch_instance* inst, int mode, int n_items,
+                          const int32_t* items, const void* params, const int32_t* move_i,
+                          const int32_t* move_j, const int32_t* move_kind, void* Ct, void* St, void* A,
+                          void* stream);
+/* Single-flip Metropolis sampling of every problem's chains in one
+ * persistent launch: n_blocks blocks of warps_per_block warps take chains
+ * (items (b, chain, 0, 0)) from a device queue; counter = 4 bytes of device
+ * scratch; max_nh = largest nh (sizes the register-resident theta cache).
+ * therm_steps_total is honoured when thermalize != 0.                      */
+int qes_batch_sampler_run(int dtype, int n_inst, const qes_batch_instance* inst, int max_nh,
+                          int n_items, const int32_t* items, int warps_per_block, int n_blocks, int thermalize,
+                          float mu, float beta, int recompute_every, const void* params,
+                          const void* flipCt, const void* flipSt, uint32_t* chain_bits,
+                          uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
+                          uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
+                          unsigned int* counter, void* stream);
+/* tanh(theta) (at tanh_off) and log psi (at sample_off, may be NULL) of the
+ * recorded samples; items (b, sample block of 16, 0, 0).                   */
+int qes_batch_rbm_forward(int dtype, int n_inst, const qes_batch_instance* inst, int n_items,
+                          const int32_t* items, const void* params, const uint32_t* sample_bits,
+                          void* tanh_out, void* logpsi_out, void* stream);
+/* E_loc of every sample; move items (b, move block of 32, sample block of
+ * 32, 0), reduce items (b, sample block of 256, 0, 0); partial = scratch of
+ * sum_b ceil(n_moves/32) * rows complex64.                                 */
+int qes_batch_local_energy(int dtype, int n_inst, const qes_batch_instance* inst, int n_move_items,
+                           const int32_t* move_items, int n_red_items, const int32_t* red_items,
+                           const uint32_t* sample_bits, const void* tanh_theta, const int32_t* move_i,
+                           const int32_t* move_j, const int32_t* move_kind, const float* move_coef,
+                           const void* Ct, const void* St, const void* A, const int32_t* zf_site,
+                           const float* zf_h, const int32_t* zz_i, const int32_t* zz_j, const float* zz_J,
+                           void* partial, void* eloc_out, void* stream);
+/* out[b] = [mean_re, mean_im, var, std] of problem b's E_loc in float64.   */
+int qes_batch_loss_stats(int n_inst, const qes_batch_instance* inst, const void* eloc, double* out,
+                         void* stream);
+/* Per-problem SR solve (S_b + shift) x_b = F_b by CG, all problems in
+ * lockstep launches, each frozen at its own convergence; x at param_off
+ * (float64 / complex128), scaled by rhs_prefactor.  ov items (b, sample
+ * block of 16, 0, 0); ohu items (b, 64-unit block, 16-site block, split of
+ * 256 samples).  sr_part_total = sum_b ceil(rows_b/256) * P_b.  results:
+ * HOST array of n_inst.                                                    */
+int qes_batch_sr_workspace_bytes(int dtype, int n_inst, int64_t n_params_total, int64_t n_samples_total,
+                                 int64_t sr_part_total, size_t* bytes);
+int qes_batch_sr_solve_cg(int dtype, int n_inst, const qes_batch_instance* inst, int n_ov_items,
+                          const int32_t* ov_items, int n_ohu_items, const int32_t* ohu_items,
+                          int64_t n_params_total, int64_t n_samples_total, int64_t sr_part_total,
+                          const uint32_t* sample_bits, const void* tanh_theta, const void* eloc,
+                          const qes_sr_options* opts, void* x_out, qes_sr_result* results,
+                          void* workspace, size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

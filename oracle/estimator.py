@@ -67,6 +67,30 @@ def loss_stats(e_loc, probs=None):
     return mean, std
 
 
+def step_rhat(e_loc, num_chains=1):
+    """Gelman-Rubin R-hat of Re E_loc (``QES/NQS/src/tdvp.py:1487-1518``).
+
+    The flattened batch is reshaped to (num_chains, chain_len) literally, as the
+    reference does; NaN for an invalid split.
+    """
+    vals = np.real(np.asarray(e_loc)).reshape(-1).astype(np.float64)
+    nch = max(int(num_chains), 1)
+    n_tot = vals.shape[0]
+    if nch <= 1 or n_tot <= nch or n_tot % nch != 0 or n_tot // nch <= 1:
+        return float("nan")
+    L = n_tot // nch
+    chains = vals.reshape(nch, L)
+    w = np.mean(np.var(chains, axis=1, ddof=1))
+    b = L * np.var(np.mean(chains, axis=1), ddof=1)
+    var_hat = ((L - 1.0) / L) * w + b / L
+    return float(np.sqrt(var_hat / max(w, 1e-12)))
+
+
+def step_sigma2(e_loc):
+    """sigma^2 = var(Re E_loc), uniform, ddof 0 (``QES/NQS/src/tdvp.py:1642``)."""
+    return float(np.var(np.real(np.asarray(e_loc)).astype(np.float64)))
+
+
 def sample_probs(log_ansatz, total_samples, exponent):
     """Reweighting factors (``vmc.py:1173-1184``)."""
     lu = exponent * np.real(np.asarray(log_ansatz))

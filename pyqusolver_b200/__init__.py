@@ -14,7 +14,7 @@ from .hamiltonian import TransverseFieldIsing, XXZ, J1J2Model, SpinHamiltonian
 
 __all__ = [
     "SquareLattice", "get_neighbor_table", "HilbertSpace", "TransverseFieldIsing", "XXZ", "J1J2Model",
-    "SpinHamiltonian", "RBM", "VMCSampler", "TDVP", "NQS", "NQSSingleStepResult", "NQSTrainStats",
+    "SpinHamiltonian", "RBM", "VMCSampler", "TDVP", "NQS", "NQSSingleStepResult", "NQSTrainStats", "NQSBatch",
 ]
 
 
@@ -31,4 +31,7 @@ def __getattr__(name):
     if name in ("NQS", "NQSSingleStepResult", "NQSTrainStats"):
         from . import nqs
         return getattr(nqs, name)
+    if name in ("NQSBatch", "NQSBatchStats"):
+        from . import batch
+        return getattr(batch, name)
     raise AttributeError(name)

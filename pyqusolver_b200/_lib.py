@@ -50,6 +50,18 @@ class SamplerConfig(C.Structure):
     ]
 
 
+class BatchInstance(C.Structure):
+    """``qes_batch_instance``: one problem of a batch (offsets in elements / words)."""
+    _fields_ = [
+        ("ns", _i32), ("nh", _i32), ("n_moves", _i32), ("n_zz", _i32), ("n_zfield", _i32),
+        ("n_chains", _i32), ("num_samples", _i32), ("sweep_steps", _i32),
+        ("therm_steps_total", _i64), ("seed", _u64),
+        ("param_off", _i64), ("chain_off", _i64), ("chain_word_off", _i64), ("sample_off", _i64),
+        ("sample_word_off", _i64), ("tanh_off", _i64), ("flip_off", _i64), ("move_table_off", _i64),
+        ("move_off", _i64), ("zz_off", _i64), ("zf_off", _i64), ("eloc_part_off", _i64), ("sr_part_off", _i64),
+    ]
+
+
 class Hamiltonian(C.Structure):
     _fields_ = [
         ("n_moves", C.c_int), ("move_i", _vp), ("move_j", _vp), ("move_kind", _vp), ("move_coef", _vp),
@@ -89,6 +101,8 @@ SIGNATURES = {
                                  _vp, _vp],
     "qes_loss_stats_workspace_bytes": [_i64, C.POINTER(_sz)],
     "qes_loss_stats": [_i64, _vp, _vp, _vp, _vp, _sz, _vp],
+    "qes_loss_rhat_workspace_bytes": [_i64, C.c_int, C.POINTER(_sz)],
+    "qes_loss_rhat": [_i64, C.c_int, _vp, _vp, _vp, _sz, _vp],
     "qes_rbm_log_derivatives": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _i64, _vp],
     "qes_sr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
     "qes_set_sr_impl": [C.c_int],
@@ -101,6 +115,17 @@ SIGNATURES = {
                         C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_rbm_logpsi_vjp": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_param_update": [C.c_int, _i64, C.c_double, _vp, _vp, _vp, _vp],
+    "qes_batch_move_tables": [C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                              _vp],
+    "qes_batch_sampler_run": [C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_float,
+                              C.c_float, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "qes_batch_rbm_forward": [C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp],
+    "qes_batch_local_energy": [C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                               _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "qes_batch_loss_stats": [C.c_int, _vp, _vp, _vp, _vp],
+    "qes_batch_sr_workspace_bytes": [C.c_int, C.c_int, _i64, _i64, _i64, C.POINTER(_sz)],
+    "qes_batch_sr_solve_cg": [C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _i64, _i64, _i64, _vp, _vp, _vp,
+                              C.POINTER(SROptions), _vp, _vp, _vp, _sz, _vp],
 }
 
 _LIB = None

@@ -23,15 +23,16 @@ constexpr int ELOC_ROWS = 8;    // sample groups per block
 constexpr int ELOC_SB = ELOC_SPT * ELOC_ROWS;   // samples per block
 constexpr int ELOC_RENORM = 16; // hidden units between renormalisations
 
+// Move block kb (32 moves) x sample block sb (ELOC_SB samples) of one problem.
 template <class T>
-__global__ void __launch_bounds__(32 * ELOC_ROWS) eloc_moves_kernel(
-    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ tanh_theta,
-    int K, const int32_t* __restrict__ mi, const int32_t* __restrict__ mj, const int32_t* __restrict__ mkind,
-    const float4* __restrict__ mcoef, const T* __restrict__ Ct, const T* __restrict__ St,
-    const T* __restrict__ A, float2* __restrict__ partial /* [gridDim.x][n_samples] */) {
+QES_D void eloc_moves_block(int kb, int64_t sb, int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits,
+                            const T* __restrict__ tanh_theta, int K, const int32_t* __restrict__ mi,
+                            const int32_t* __restrict__ mj, const int32_t* __restrict__ mkind,
+                            const float4* __restrict__ mcoef, const T* __restrict__ Ct, const T* __restrict__ St,
+                            const T* __restrict__ A, float2* __restrict__ partial /* [kblocks][n_samples] */) {
   const int nw = n_words(ns);
-  const int k = blockIdx.x * 32 + threadIdx.x;
-  const int64_t s_base = (int64_t)blockIdx.y * ELOC_SB + (int64_t)threadIdx.y * ELOC_SPT;
+  const int k = kb * 32 + threadIdx.x;
+  const int64_t s_base = sb * ELOC_SB + (int64_t)threadIdx.y * ELOC_SPT;
   const bool kval = k < K;
 
   int kind = 0, i = 0, j = 0;
@@ -93,18 +94,27 @@ __global__ void __launch_bounds__(32 * ELOC_ROWS) eloc_moves_kernel(
     v = warp_sum(v);
     if (threadIdx.x == 0) {
       const int64_t s = s_base + q;
-      if (s < n_samples) partial[(int64_t)blockIdx.x * n_samples + s] = v;
+      if (s < n_samples) partial[(int64_t)kb * n_samples + s] = v;
     }
   }
 }
 
-__global__ void eloc_reduce_kernel(int ns, int64_t n_samples, const uint32_t* __restrict__ bits, int nkb,
-                                   const float2* __restrict__ partial, int n_zf, const int32_t* __restrict__ zf_site,
-                                   const float* __restrict__ zf_h, int n_zz, const int32_t* __restrict__ zz_i,
-                                   const int32_t* __restrict__ zz_j, const float* __restrict__ zz_J,
-                                   float2* __restrict__ eloc) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_samples) return;
+template <class T>
+__global__ void __launch_bounds__(32 * ELOC_ROWS) eloc_moves_kernel(
+    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ tanh_theta,
+    int K, const int32_t* __restrict__ mi, const int32_t* __restrict__ mj, const int32_t* __restrict__ mkind,
+    const float4* __restrict__ mcoef, const T* __restrict__ Ct, const T* __restrict__ St,
+    const T* __restrict__ A, float2* __restrict__ partial /* [gridDim.x][n_samples] */) {
+  eloc_moves_block<T>(blockIdx.x, blockIdx.y, ns, nh, n_samples, bits, tanh_theta, K, mi, mj, mkind, mcoef, Ct, St, A,
+                      partial);
+}
+
+// diagonal part + move partials of sample s
+QES_D void eloc_reduce_sample(int64_t s, int ns, int64_t n_samples, const uint32_t* __restrict__ bits, int nkb,
+                              const float2* __restrict__ partial, int n_zf, const int32_t* __restrict__ zf_site,
+                              const float* __restrict__ zf_h, int n_zz, const int32_t* __restrict__ zz_i,
+                              const int32_t* __restrict__ zz_j, const float* __restrict__ zz_J,
+                              float2* __restrict__ eloc) {
   const int nw = n_words(ns);
   const uint32_t* w = bits + s * nw;
   float d = 0.f;
@@ -115,7 +125,17 @@ __global__ void eloc_reduce_kernel(int ns, int64_t n_samples, const uint32_t* __
   eloc[s] = e;
 }
 
-static int eloc_kblocks(int K) { return (K + 31) / 32; }
+__global__ void eloc_reduce_kernel(int ns, int64_t n_samples, const uint32_t* __restrict__ bits, int nkb,
+                                   const float2* __restrict__ partial, int n_zf, const int32_t* __restrict__ zf_site,
+                                   const float* __restrict__ zf_h, int n_zz, const int32_t* __restrict__ zz_i,
+                                   const int32_t* __restrict__ zz_j, const float* __restrict__ zz_J,
+                                   float2* __restrict__ eloc) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_samples) return;
+  eloc_reduce_sample(s, ns, n_samples, bits, nkb, partial, n_zf, zf_site, zf_h, n_zz, zz_i, zz_j, zz_J, eloc);
+}
+
+QES_HD int eloc_kblocks(int K) { return (K + 31) / 32; }
 
 extern "C" int qes_local_energy_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, int n_moves,
                                                 size_t* bytes) {
@@ -261,6 +281,97 @@ extern "C" int qes_loss_stats(int64_t n_samples, const void* eloc, const float* 
 }
 
 // ----------------------------------------------------------------------------
+// Step diagnostics: Gelman-Rubin R-hat over n_groups contiguous blocks of
+// Re E_loc and sigma^2 = var(Re E_loc) (uniform weights, ddof 0), float64.
+// One warp per block computes its mean and ddof-1 variance (two passes); a
+// single CTA then combines the blocks in a fixed order.
+// ----------------------------------------------------------------------------
+constexpr int RHAT_FINAL_THREADS = 1024;
+
+__global__ void rhat_groups_kernel(int64_t n_groups, int64_t glen, const float2* __restrict__ e,
+                                   double2* __restrict__ gstat) {
+  const int lane = threadIdx.x & 31;
+  const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (g >= n_groups) return;
+  const float2* x = e + g * glen;
+  double s = 0;
+  for (int64_t k = lane; k < glen; k += 32) s += (double)x[k].x;
+  const double m = warp_sum(s) / (double)glen;
+  double v = 0;
+  for (int64_t k = lane; k < glen; k += 32) {
+    const double d = (double)x[k].x - m;
+    v += d * d;
+  }
+  v = warp_sum(v);
+  if (lane == 0) gstat[g] = make_double2(m, glen > 1 ? v / (double)(glen - 1) : 0.0);
+}
+
+__global__ void __launch_bounds__(RHAT_FINAL_THREADS) rhat_final_kernel(int64_t n_groups, int64_t glen, int valid,
+                                                                      const double2* __restrict__ gstat,
+                                                                      double* __restrict__ out) {
+  __shared__ double red[2][RHAT_FINAL_THREADS];
+  double sm = 0, sv = 0;
+  for (int64_t g = threadIdx.x; g < n_groups; g += blockDim.x) { sm += gstat[g].x; sv += gstat[g].y; }
+  red[0][threadIdx.x] = sm; red[1][threadIdx.x] = sv;
+  __syncthreads();
+  for (int o = RHAT_FINAL_THREADS / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { red[0][threadIdx.x] += red[0][threadIdx.x + o]; red[1][threadIdx.x] += red[1][threadIdx.x + o]; }
+    __syncthreads();
+  }
+  const double mm = red[0][0] / (double)n_groups;   // grand mean (equal block lengths)
+  const double W = red[1][0] / (double)n_groups;    // mean within-block variance
+  __syncthreads();
+  double sb = 0;
+  for (int64_t g = threadIdx.x; g < n_groups; g += blockDim.x) {
+    const double d = gstat[g].x - mm;
+    sb += d * d;
+  }
+  red[0][threadIdx.x] = sb;
+  __syncthreads();
+  for (int o = RHAT_FINAL_THREADS / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[0][threadIdx.x] += red[0][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double L = (double)glen, G = (double)n_groups, ssb = red[0][0];
+    // total variance of the n = G*L values, ddof 0: within + between blocks
+    out[1] = ((L - 1.0) * W * G + L * ssb) / (G * L);
+    if (valid) {
+      const double B = L * ssb / (G - 1.0);
+      const double var_hat = ((L - 1.0) / L) * W + B / L;
+      out[0] = sqrt(var_hat / fmax(W, 1e-12));
+    } else {
+      out[0] = nan("");
+    }
+  }
+}
+
+extern "C" int qes_loss_rhat_workspace_bytes(int64_t n_samples, int n_chains, size_t* bytes) {
+  QES_ARG_CHECK(bytes != nullptr && n_samples >= 0, "qes_loss_rhat_workspace_bytes: bad args");
+  *bytes = (size_t)std::max<int64_t>(1, std::max<int64_t>(n_chains, 1)) * sizeof(double2);
+  return QES_OK;
+}
+
+extern "C" int qes_loss_rhat(int64_t n_samples, int n_chains, const void* eloc, double* out, void* workspace,
+                             size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(n_samples > 0 && eloc && out && workspace, "qes_loss_rhat: bad args");
+  const int64_t nch = std::max(n_chains, 1);
+  const bool valid = nch > 1 && n_samples > nch && n_samples % nch == 0 && n_samples / nch > 1;
+  const int64_t G = valid ? nch : 1, L = n_samples / G;
+  if (workspace_bytes < (size_t)G * sizeof(double2)) {
+    qes_set_last_message("qes_loss_rhat: workspace too small");
+    return QES_ERR_WORKSPACE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  double2* gstat = (double2*)workspace;
+  const int warps = 8;
+  rhat_groups_kernel<<<(unsigned)((G + warps - 1) / warps), 32 * warps, 0, st>>>(G, L, (const float2*)eloc, gstat);
+  rhat_final_kernel<<<1, RHAT_FINAL_THREADS, 0, st>>>(G, L, valid ? 1 : 0, gstat, out);
+  QES_LAUNCH_CHECK_N(2);
+  return QES_OK;
+}
+
+// ----------------------------------------------------------------------------
 // Allocation-free local energy.
 //
 // Some callers cannot allocate device memory at all: hosts that hand this
@@ -328,4 +439,121 @@ extern "C" int qes_local_energy_noalloc(int dtype, int ns, int nh, int64_t n_sam
   if (rc != QES_OK) return rc;
   return qes_local_energy(dtype, ns, nh, n_samples, bits, tanh_theta, ham, Ct, St, A, scratch,
                           (size_t)QES_NOALLOC_ELOC_SCRATCH_BYTES, eloc_out, stream);
+}
+
+// ----------------------------------------------------------------------------
+// Batched problems
+// ----------------------------------------------------------------------------
+// move items (b, move block, sample block)
+template <class T>
+__global__ void __launch_bounds__(32 * ELOC_ROWS) batch_eloc_moves_kernel(
+    const qes_batch_instance* __restrict__ inst, const int4* __restrict__ items, const uint32_t* __restrict__ bits,
+    const T* __restrict__ tanh_theta, const int32_t* __restrict__ mi, const int32_t* __restrict__ mj,
+    const int32_t* __restrict__ mkind, const float4* __restrict__ mcoef, const T* __restrict__ Ct,
+    const T* __restrict__ St, const T* __restrict__ A, float2* __restrict__ partial) {
+  const int4 it = items[blockIdx.x];
+  const qes_batch_instance I = inst[it.x];
+  const int64_t rows = (int64_t)I.n_chains * I.num_samples;
+  eloc_moves_block<T>(it.y, it.z, I.ns, I.nh, rows, bits + I.sample_word_off, tanh_theta + I.tanh_off, I.n_moves,
+                      mi + I.move_off, mj + I.move_off, mkind + I.move_off, mcoef + I.move_off,
+                      Ct + I.move_table_off, St + I.move_table_off, A + I.move_off, partial + I.eloc_part_off);
+}
+
+// reduce items (b, sample block of 256)
+__global__ void batch_eloc_reduce_kernel(const qes_batch_instance* __restrict__ inst, const int4* __restrict__ items,
+                                         const uint32_t* __restrict__ bits, const float2* __restrict__ partial,
+                                         const int32_t* __restrict__ zf_site, const float* __restrict__ zf_h,
+                                         const int32_t* __restrict__ zz_i, const int32_t* __restrict__ zz_j,
+                                         const float* __restrict__ zz_J, float2* __restrict__ eloc) {
+  const int4 it = items[blockIdx.x];
+  const qes_batch_instance I = inst[it.x];
+  const int64_t rows = (int64_t)I.n_chains * I.num_samples;
+  const int64_t s = (int64_t)it.y * blockDim.x + threadIdx.x;
+  if (s >= rows) return;
+  eloc_reduce_sample(s, I.ns, rows, bits + I.sample_word_off, I.n_moves > 0 ? eloc_kblocks(I.n_moves) : 0,
+                     partial + I.eloc_part_off, I.n_zfield, zf_site + I.zf_off, zf_h + I.zf_off, I.n_zz,
+                     zz_i + I.zz_off, zz_j + I.zz_off, zz_J + I.zz_off, eloc + I.sample_off);
+}
+
+extern "C" int qes_batch_local_energy(int dtype, int n_inst, const qes_batch_instance* inst, int n_move_items,
+                                      const int32_t* move_items, int n_red_items, const int32_t* red_items,
+                                      const uint32_t* sample_bits, const void* tanh_theta, const int32_t* move_i,
+                                      const int32_t* move_j, const int32_t* move_kind, const float* move_coef,
+                                      const void* Ct, const void* St, const void* A, const int32_t* zf_site,
+                                      const float* zf_h, const int32_t* zz_i, const int32_t* zz_j,
+                                      const float* zz_J, void* partial, void* eloc_out, void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_batch_local_energy: bad dtype");
+  QES_ARG_CHECK(n_inst >= 0 && n_move_items >= 0 && n_red_items >= 0, "qes_batch_local_energy: bad sizes");
+  if (n_red_items == 0) return QES_OK;
+  QES_ARG_CHECK(inst && red_items && sample_bits && eloc_out, "qes_batch_local_energy: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_move_items > 0) {
+    QES_ARG_CHECK(move_items && tanh_theta && move_i && move_j && move_kind && move_coef && Ct && St && A && partial,
+                  "qes_batch_local_energy: null move pointer");
+    dim3 block(32, ELOC_ROWS);
+    if (dtype == QES_DTYPE_F32)
+      batch_eloc_moves_kernel<float><<<n_move_items, block, 0, st>>>(
+          inst, (const int4*)move_items, sample_bits, (const float*)tanh_theta, move_i, move_j, move_kind,
+          (const float4*)move_coef, (const float*)Ct, (const float*)St, (const float*)A, (float2*)partial);
+    else
+      batch_eloc_moves_kernel<float2><<<n_move_items, block, 0, st>>>(
+          inst, (const int4*)move_items, sample_bits, (const float2*)tanh_theta, move_i, move_j, move_kind,
+          (const float4*)move_coef, (const float2*)Ct, (const float2*)St, (const float2*)A, (float2*)partial);
+    QES_LAUNCH_CHECK();
+  }
+  batch_eloc_reduce_kernel<<<n_red_items, 256, 0, st>>>(inst, (const int4*)red_items, sample_bits,
+                                                        (const float2*)partial, zf_site, zf_h, zz_i, zz_j, zz_J,
+                                                        (float2*)eloc_out);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+// one block per problem: float64 mean (complex), variance, std of its E_loc rows (uniform weights)
+constexpr int BSTAT_THREADS = 256;
+__global__ void __launch_bounds__(BSTAT_THREADS) batch_stats_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                   const float2* __restrict__ eloc,
+                                                                   double* __restrict__ out) {
+  const qes_batch_instance I = inst[blockIdx.x];
+  const int64_t rows = (int64_t)I.n_chains * I.num_samples;
+  const float2* e = eloc + I.sample_off;
+  __shared__ double red[2][BSTAT_THREADS];
+  double sr = 0, si = 0;
+  for (int64_t k = threadIdx.x; k < rows; k += blockDim.x) { sr += e[k].x; si += e[k].y; }
+  red[0][threadIdx.x] = sr; red[1][threadIdx.x] = si;
+  __syncthreads();
+  for (int o = BSTAT_THREADS / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { red[0][threadIdx.x] += red[0][threadIdx.x + o]; red[1][threadIdx.x] += red[1][threadIdx.x + o]; }
+    __syncthreads();
+  }
+  const double n = (double)(rows > 0 ? rows : 1);
+  const double mr = red[0][0] / n, mi = red[1][0] / n;
+  __syncthreads();
+  double v = 0;
+  for (int64_t k = threadIdx.x; k < rows; k += blockDim.x) {
+    const double dr = e[k].x - mr, di = e[k].y - mi;
+    v += dr * dr + di * di;
+  }
+  red[0][threadIdx.x] = v;
+  __syncthreads();
+  for (int o = BSTAT_THREADS / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[0][threadIdx.x] += red[0][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double var = red[0][0] / n;
+    out[4 * blockIdx.x + 0] = mr;
+    out[4 * blockIdx.x + 1] = mi;
+    out[4 * blockIdx.x + 2] = var;
+    out[4 * blockIdx.x + 3] = sqrt(var);
+  }
+}
+
+extern "C" int qes_batch_loss_stats(int n_inst, const qes_batch_instance* inst, const void* eloc, double* out,
+                                    void* stream) {
+  QES_ARG_CHECK(n_inst >= 0, "qes_batch_loss_stats: bad sizes");
+  if (n_inst == 0) return QES_OK;
+  QES_ARG_CHECK(inst && eloc && out, "qes_batch_loss_stats: null pointer");
+  batch_stats_kernel<<<n_inst, BSTAT_THREADS, 0, (cudaStream_t)stream>>>(inst, (const float2*)eloc, out);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
 }

@@ -230,14 +230,13 @@ extern "C" int qes_rbm_move_tables(int dtype, int ns, int nh, const void* a, con
 constexpr int FWD_SB = 16;
 constexpr int FWD_THREADS = 256;
 
+// One block of FWD_SB samples starting at row s0 (smem_words: FWD_SB * n_words(ns) words).
 template <class T>
-__global__ void __launch_bounds__(FWD_THREADS) rbm_forward_kernel(
-    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ a,
-    const T* __restrict__ b, const T* __restrict__ W, T* __restrict__ theta_out, T* __restrict__ tanh_out,
-    T* __restrict__ logpsi_out) {
-  extern __shared__ uint32_t smem_words[];
+QES_D void rbm_forward_block(int64_t s0, uint32_t* smem_words, int ns, int nh, int64_t n_samples,
+                             const uint32_t* __restrict__ bits, const T* __restrict__ a, const T* __restrict__ b,
+                             const T* __restrict__ W, T* __restrict__ theta_out, T* __restrict__ tanh_out,
+                             T* __restrict__ logpsi_out) {
   const int nw = n_words(ns);
-  const int64_t s0 = (int64_t)blockIdx.x * FWD_SB;
   const int nsb = (int)min((int64_t)FWD_SB, n_samples - s0);
   for (int q = threadIdx.x; q < FWD_SB * nw; q += blockDim.x) {
     const int sl = q / nw;
@@ -295,6 +294,16 @@ __global__ void __launch_bounds__(FWD_THREADS) rbm_forward_kernel(
     for (int w = 0; w < FWD_THREADS / 32; ++w) v = addx(v, red[w][threadIdx.x]);
     logpsi_out[s0 + threadIdx.x] = v;
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(FWD_THREADS) rbm_forward_kernel(
+    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ a,
+    const T* __restrict__ b, const T* __restrict__ W, T* __restrict__ theta_out, T* __restrict__ tanh_out,
+    T* __restrict__ logpsi_out) {
+  extern __shared__ uint32_t smem_words[];
+  rbm_forward_block<T>((int64_t)blockIdx.x * FWD_SB, smem_words, ns, nh, n_samples, bits, a, b, W, theta_out,
+                       tanh_out, logpsi_out);
 }
 
 extern "C" int qes_rbm_forward(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits, const void* a,
@@ -395,6 +404,113 @@ extern "C" int qes_param_update(int dtype, int64_t n_params, double lr, const vo
   const unsigned grid = (unsigned)std::min<int64_t>((n + bs - 1) / bs, 4096);
   param_update_kernel<<<grid, bs, 0, (cudaStream_t)stream>>>(n, lr, (const double*)x, (double*)master,
                                                              (float*)params);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+// ----------------------------------------------------------------------------
+// Batched problems
+// ----------------------------------------------------------------------------
+constexpr int BMT_THREADS = 256;
+
+// items (b, first element / BMT_THREADS): one thread per table element
+template <class T>
+__global__ void __launch_bounds__(BMT_THREADS) batch_move_tables_kernel(
+    const qes_batch_instance* __restrict__ inst, int mode, const int4* __restrict__ items,
+    const T* __restrict__ params, const int32_t* __restrict__ mi, const int32_t* __restrict__ mj,
+    const int32_t* __restrict__ mk, T* __restrict__ Ct, T* __restrict__ St, T* __restrict__ A) {
+  const int4 it = items[blockIdx.x];
+  const qes_batch_instance I = inst[it.x];
+  const int nh = I.nh;
+  const T* a = params + I.param_off;
+  const T* W = a + I.ns + nh;
+  const int K = (mode == 0) ? I.ns : I.n_moves;
+  const int64_t idx = (int64_t)it.y * BMT_THREADS + threadIdx.x;
+  if (idx >= (int64_t)K * nh) return;
+  int m, k, i, j, kind;
+  if (mode == 0) {                       // single flips, move-major
+    m = (int)(idx % nh); k = (int)(idx / nh);
+    i = k; j = k; kind = QES_MOVE_FLIP1;
+  } else {                               // lowered moves, m-major
+    m = (int)(idx / K); k = (int)(idx % K);
+    i = mi[I.move_off + k]; j = mj[I.move_off + k]; kind = mk[I.move_off + k];
+  }
+  T d;
+  if (kind == QES_MOVE_FLIP1) d = W[(int64_t)i * nh + m];
+  else if (kind == QES_MOVE_PAIR_ANTI) d = addx(W[(int64_t)i * nh + m], scal(-1.f, W[(int64_t)j * nh + m]));
+  else d = addx(W[(int64_t)i * nh + m], W[(int64_t)j * nh + m]);
+  T c, s;
+  cosh_sinh2(d, c, s);
+  const int64_t off = (mode == 0) ? I.flip_off : I.move_table_off;
+  Ct[off + idx] = c;
+  St[off + idx] = s;
+  if (mode == 1 && m == 0 && A) {
+    T av = a[i];
+    if (kind == QES_MOVE_PAIR_ANTI) av = addx(av, scal(-1.f, a[j]));
+    else if (kind == QES_MOVE_PAIR_PAR) av = addx(av, a[j]);
+    A[I.move_off + k] = av;
+  }
+}
+
+extern "C" int qes_batch_move_tables(int dtype, int n_inst, const qes_batch_instance* inst, int mode, int n_items,
+                                     const int32_t* items, const void* params, const int32_t* move_i,
+                                     const int32_t* move_j, const int32_t* move_kind, void* Ct, void* St, void* A,
+                                     void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_batch_move_tables: bad dtype");
+  QES_ARG_CHECK(mode == 0 || mode == 1, "qes_batch_move_tables: mode must be 0 (flips) or 1 (moves)");
+  QES_ARG_CHECK(n_inst >= 0 && n_items >= 0, "qes_batch_move_tables: bad sizes");
+  if (n_items == 0) return QES_OK;
+  QES_ARG_CHECK(inst && items && params && Ct && St, "qes_batch_move_tables: null pointer");
+  QES_ARG_CHECK(mode == 0 || (move_i && move_j && move_kind && A), "qes_batch_move_tables: null move arrays");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    batch_move_tables_kernel<float><<<n_items, BMT_THREADS, 0, st>>>(inst, mode, (const int4*)items,
+                                                                     (const float*)params, move_i, move_j, move_kind,
+                                                                     (float*)Ct, (float*)St, (float*)A);
+  else
+    batch_move_tables_kernel<float2><<<n_items, BMT_THREADS, 0, st>>>(inst, mode, (const int4*)items,
+                                                                      (const float2*)params, move_i, move_j,
+                                                                      move_kind, (float2*)Ct, (float2*)St,
+                                                                      (float2*)A);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+// items (b, sample block of FWD_SB)
+template <class T>
+__global__ void __launch_bounds__(FWD_THREADS) batch_forward_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                   const int4* __restrict__ items,
+                                                                   const T* __restrict__ params,
+                                                                   const uint32_t* __restrict__ bits,
+                                                                   T* __restrict__ tanh_out, T* __restrict__ logpsi_out) {
+  extern __shared__ uint32_t smem_words[];
+  const int4 it = items[blockIdx.x];
+  const qes_batch_instance I = inst[it.x];
+  const T* a = params + I.param_off;
+  const T* b = a + I.ns;
+  const T* W = b + I.nh;
+  const int64_t rows = (int64_t)I.n_chains * I.num_samples;
+  rbm_forward_block<T>((int64_t)it.y * FWD_SB, smem_words, I.ns, I.nh, rows, bits + I.sample_word_off, a, b, W,
+                       nullptr, tanh_out ? tanh_out + I.tanh_off : nullptr,
+                       logpsi_out ? logpsi_out + I.sample_off : nullptr);
+}
+
+extern "C" int qes_batch_rbm_forward(int dtype, int n_inst, const qes_batch_instance* inst, int n_items,
+                                     const int32_t* items, const void* params, const uint32_t* sample_bits,
+                                     void* tanh_out, void* logpsi_out, void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_batch_rbm_forward: bad dtype");
+  QES_ARG_CHECK(n_inst >= 0 && n_items >= 0, "qes_batch_rbm_forward: bad sizes");
+  if (n_items == 0) return QES_OK;
+  QES_ARG_CHECK(inst && items && params && sample_bits, "qes_batch_rbm_forward: null pointer");
+  const size_t sm = (size_t)FWD_SB * 64 * sizeof(uint32_t);      // ns <= 2048
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    batch_forward_kernel<float><<<n_items, FWD_THREADS, sm, st>>>(inst, (const int4*)items, (const float*)params,
+                                                                  sample_bits, (float*)tanh_out, (float*)logpsi_out);
+  else
+    batch_forward_kernel<float2><<<n_items, FWD_THREADS, sm, st>>>(inst, (const int4*)items, (const float2*)params,
+                                                                   sample_bits, (float2*)tanh_out,
+                                                                   (float2*)logpsi_out);
   QES_LAUNCH_CHECK();
   return QES_OK;
 }

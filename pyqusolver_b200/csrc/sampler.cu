@@ -63,40 +63,49 @@ QES_D T chain_logpsi(int ns, int nh, int lane, const uint32_t* cfg, const T* __r
   return warp_sum(s);
 }
 
+// Everything one chain needs; pointers are already offset to the chain's problem.
+template <class T>
+struct ChainCtx {
+  int ns, nh, n_chains, deg, sweep_steps, recompute_every, num_samples;
+  int64_t therm_steps_total;
+  float beta_mu;
+  uint32_t k0, k1;
+  int64_t chain_id;                         // global chain id (Philox counter word 0)
+  const T *a, *b, *W, *flipC, *flipS, *pairC, *pairS;
+  const int32_t *nbr, *nbr_pair, *pair_i, *pair_j;
+};
+
+// Runs proposals for chain `chain` (index within its problem) with the
+// problem's packed spins staged in `cw` (shared memory, one warp).
 template <class T, int MPL, int RULE>
-__global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
-    qes_sampler_config cfg, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ W,
-    const T* __restrict__ flipC, const T* __restrict__ flipS, const int32_t* __restrict__ nbr,
-    const int32_t* __restrict__ nbr_pair, const int32_t* __restrict__ pair_i, const int32_t* __restrict__ pair_j,
-    const T* __restrict__ pairC, const T* __restrict__ pairS, uint32_t* __restrict__ chain_bits,
-    uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed, int32_t* __restrict__ accepted,
-    uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
-  __shared__ uint32_t cfg_sm[SMP_WARPS][SMP_MAX_WORDS];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int chain = blockIdx.x * SMP_WARPS + wid;
-  if (chain >= cfg.n_chains) return;            // whole warp leaves together
-  const int ns = cfg.ns, nh = cfg.nh, nw = n_words(ns);
-  uint32_t* cw = cfg_sm[wid];
+QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __restrict__ chain_bits,
+                     uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed,
+                     int32_t* __restrict__ accepted, uint32_t* __restrict__ sample_bits,
+                     T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
+  const int lane = threadIdx.x & 31;
+  const int ns = P.ns, nh = P.nh, nw = n_words(ns);
+  const T* __restrict__ a = P.a;
+  const T* __restrict__ b = P.b;
+  const T* __restrict__ W = P.W;
   for (int q = lane; q < nw; q += 32) cw[q] = chain_bits[(int64_t)chain * nw + q];
   __syncwarp();
 
-  const uint32_t k0 = (uint32_t)(cfg.seed & 0xffffffffu), k1 = (uint32_t)(cfg.seed >> 32);
-  const uint32_t cid = (uint32_t)(cfg.chain_offset + chain);
+  const uint32_t cid = (uint32_t)P.chain_id;
   uint64_t step = chain_step[chain];
   int32_t n_prop = proposed[chain], n_acc = accepted[chain];
-  const int recompute = cfg.recompute_every > 0 ? cfg.recompute_every : ns;
-  const float bm = cfg.beta * cfg.mu;
+  const int recompute = P.recompute_every > 0 ? P.recompute_every : ns;
+  const float bm = P.beta_mu;
 
   T th[MPL], tn[MPL];
   full_theta<T, MPL>(ns, nh, lane, cw, b, W, th, tn);
   int since = 0;
 
-  const int64_t total = cfg.therm_steps_total + (int64_t)cfg.num_samples * cfg.sweep_steps;
+  const int64_t total = P.therm_steps_total + (int64_t)P.num_samples * P.sweep_steps;
   int64_t rec = 0;
-  int64_t next_record = cfg.therm_steps_total + cfg.sweep_steps;
+  int64_t next_record = P.therm_steps_total + P.sweep_steps;
 
   for (int64_t it = 0; it < total; ++it) {
-    const Philox4 r = philox4x32_10(cid, (uint32_t)step, (uint32_t)(step >> 32), QES_STREAM_PROPOSAL, k0, k1);
+    const Philox4 r = philox4x32_10(cid, (uint32_t)step, (uint32_t)(step >> 32), QES_STREAM_PROPOSAL, P.k0, P.k1);
     const int i = (int)bounded_u32(r.x, (uint32_t)ns);
     bool moved;
     int i0 = i, j0 = -1;        // sites flipped (j0 = -1 for a single flip)
@@ -104,22 +113,22 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
     const T* Srow;
     if (RULE == QES_RULE_LOCAL) {
       moved = true;
-      Crow = flipC + (int64_t)i * nh;
-      Srow = flipS + (int64_t)i * nh;
+      Crow = P.flipC + (int64_t)i * nh;
+      Srow = P.flipS + (int64_t)i * nh;
     } else {
-      const int kk = (int)bounded_u32(r.y, (uint32_t)cfg.deg);
-      const int j = nbr[i * cfg.deg + kk];
+      const int kk = (int)bounded_u32(r.y, (uint32_t)P.deg);
+      const int j = P.nbr[i * P.deg + kk];
       moved = false;
-      Crow = flipC; Srow = flipS;
+      Crow = P.flipC; Srow = P.flipS;
       if (j >= 0) {
         const uint32_t bi = (cw[i >> 5] >> (i & 31)) & 1u;
         const uint32_t bj = (cw[j >> 5] >> (j & 31)) & 1u;
         if (bi != bj) {
-          const int p = nbr_pair[i * cfg.deg + kk];
+          const int p = P.nbr_pair[i * P.deg + kk];
           moved = true;
-          i0 = pair_i[p]; j0 = pair_j[p];
-          Crow = pairC + (int64_t)p * nh;
-          Srow = pairS + (int64_t)p * nh;
+          i0 = P.pair_i[p]; j0 = P.pair_j[p];
+          Crow = P.pairC + (int64_t)p * nh;
+          Srow = P.pairS + (int64_t)p * nh;
         }
       }
     }
@@ -171,12 +180,12 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
       since = 0;
     }
     if (it + 1 == next_record) {
-      const int64_t row = rec * cfg.n_chains + chain;
+      const int64_t row = rec * P.n_chains + chain;
       for (int q = lane; q < nw; q += 32) sample_bits[row * nw + q] = cw[q];
       const T lp = chain_logpsi<T, MPL>(ns, nh, lane, cw, a, th);
       if (lane == 0 && sample_logpsi) sample_logpsi[row] = lp;
       ++rec;
-      next_record += cfg.sweep_steps;
+      next_record += P.sweep_steps;
     }
   }
   for (int q = lane; q < nw; q += 32) chain_bits[(int64_t)chain * nw + q] = cw[q];
@@ -187,6 +196,31 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
     accepted[chain] = n_acc;
     if (last_logpsi) last_logpsi[chain] = lp;
   }
+  __syncwarp();
+}
+
+template <class T, int MPL, int RULE>
+__global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
+    qes_sampler_config cfg, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ W,
+    const T* __restrict__ flipC, const T* __restrict__ flipS, const int32_t* __restrict__ nbr,
+    const int32_t* __restrict__ nbr_pair, const int32_t* __restrict__ pair_i, const int32_t* __restrict__ pair_j,
+    const T* __restrict__ pairC, const T* __restrict__ pairS, uint32_t* __restrict__ chain_bits,
+    uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed, int32_t* __restrict__ accepted,
+    uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
+  __shared__ uint32_t cfg_sm[SMP_WARPS][SMP_MAX_WORDS];
+  const int wid = threadIdx.x >> 5;
+  const int chain = blockIdx.x * SMP_WARPS + wid;
+  if (chain >= cfg.n_chains) return;            // whole warp leaves together
+  ChainCtx<T> P;
+  P.ns = cfg.ns; P.nh = cfg.nh; P.n_chains = cfg.n_chains; P.deg = cfg.deg; P.sweep_steps = cfg.sweep_steps;
+  P.recompute_every = cfg.recompute_every; P.num_samples = cfg.num_samples;
+  P.therm_steps_total = cfg.therm_steps_total; P.beta_mu = cfg.beta * cfg.mu;
+  P.k0 = (uint32_t)(cfg.seed & 0xffffffffu); P.k1 = (uint32_t)(cfg.seed >> 32);
+  P.chain_id = cfg.chain_offset + chain;
+  P.a = a; P.b = b; P.W = W; P.flipC = flipC; P.flipS = flipS; P.pairC = pairC; P.pairS = pairS;
+  P.nbr = nbr; P.nbr_pair = nbr_pair; P.pair_i = pair_i; P.pair_j = pair_j;
+  run_chain<T, MPL, RULE>(P, chain, cfg_sm[wid], chain_bits, chain_step, proposed, accepted, sample_bits,
+                          sample_logpsi, last_logpsi);
 }
 
 template <class T, int MPL>
@@ -266,4 +300,106 @@ extern "C" int qes_sampler_run(int dtype, const qes_sampler_config* cfg, const v
   return launch_sampler<float2>(mpl, 16, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j, pairCt,
                                 pairSt, chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi,
                                 last_logpsi, st);
+}
+
+// ----------------------------------------------------------------------------
+// Batched problems: persistent warps take (problem, chain) items from a
+// device queue, heaviest first, so problems of uneven size share one launch.
+// ----------------------------------------------------------------------------
+template <class T, int MPL>
+__global__ void batch_sampler_kernel(const qes_batch_instance* __restrict__ inst, int n_items,
+                                     const int4* __restrict__ items, int thermalize, float beta_mu,
+                                     int recompute_every, const T* __restrict__ params,
+                                     const T* __restrict__ flipC, const T* __restrict__ flipS,
+                                     uint32_t* __restrict__ chain_bits, uint64_t* __restrict__ chain_step,
+                                     int32_t* __restrict__ proposed, int32_t* __restrict__ accepted,
+                                     uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi,
+                                     T* __restrict__ last_logpsi, unsigned int* __restrict__ counter) {
+  extern __shared__ uint32_t batch_cfg_sm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t* cw = batch_cfg_sm + wid * SMP_MAX_WORDS;
+  for (;;) {
+    unsigned int q = 0;
+    if (lane == 0) q = atomicAdd(counter, 1u);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= (unsigned int)n_items) break;
+    const int4 it = items[q];
+    const qes_batch_instance I = inst[it.x];
+    ChainCtx<T> P;
+    P.ns = I.ns; P.nh = I.nh; P.n_chains = I.n_chains; P.deg = 0; P.sweep_steps = I.sweep_steps;
+    P.recompute_every = recompute_every; P.num_samples = I.num_samples;
+    P.therm_steps_total = thermalize ? I.therm_steps_total : 0; P.beta_mu = beta_mu;
+    P.k0 = (uint32_t)(I.seed & 0xffffffffu); P.k1 = (uint32_t)(I.seed >> 32);
+    P.chain_id = it.y;
+    P.a = params + I.param_off; P.b = P.a + I.ns; P.W = P.b + I.nh;
+    P.flipC = flipC + I.flip_off; P.flipS = flipS + I.flip_off;
+    P.pairC = nullptr; P.pairS = nullptr; P.nbr = nullptr; P.nbr_pair = nullptr; P.pair_i = nullptr;
+    P.pair_j = nullptr;
+    run_chain<T, MPL, QES_RULE_LOCAL>(P, it.y, cw, chain_bits + I.chain_word_off, chain_step + I.chain_off,
+                                      proposed + I.chain_off, accepted + I.chain_off,
+                                      sample_bits + I.sample_word_off,
+                                      sample_logpsi ? sample_logpsi + I.sample_off : nullptr,
+                                      last_logpsi ? last_logpsi + I.chain_off : nullptr);
+  }
+}
+
+template <class T, int MPL>
+static int launch_batch_sampler_mpl(int n_inst, const qes_batch_instance* inst, int n_items, const int32_t* items,
+                                    int warps, int blocks, int thermalize, float beta_mu, int recompute_every,
+                                    const void* params, const void* flipC, const void* flipS, uint32_t* chain_bits,
+                                    uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
+                                    uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
+                                    unsigned int* counter, cudaStream_t st) {
+  (void)n_inst;
+  QES_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st));
+  const size_t smem = (size_t)warps * SMP_MAX_WORDS * sizeof(uint32_t);
+  batch_sampler_kernel<T, MPL><<<blocks, 32 * warps, smem, st>>>(
+      inst, n_items, (const int4*)items, thermalize, beta_mu, recompute_every, (const T*)params, (const T*)flipC,
+      (const T*)flipS, chain_bits, chain_step, proposed, accepted, sample_bits, (T*)sample_logpsi, (T*)last_logpsi,
+      counter);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+extern "C" int qes_batch_sampler_run(int dtype, int n_inst, const qes_batch_instance* inst, int max_nh,
+                                     int n_items, const int32_t* items, int warps_per_block, int n_blocks,
+                                     int thermalize, float mu, float beta, int recompute_every,
+                                     const void* params, const void* flipCt, const void* flipSt,
+                                     uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed,
+                                     int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi,
+                                     void* last_logpsi, unsigned int* counter, void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_batch_sampler_run: bad dtype");
+  QES_ARG_CHECK(n_inst >= 0 && n_items >= 0 && max_nh > 0, "qes_batch_sampler_run: bad sizes");
+  QES_ARG_CHECK(warps_per_block >= 1 && warps_per_block <= 16 && n_blocks >= 1,
+                "qes_batch_sampler_run: warps_per_block must be 1..16 and n_blocks >= 1");
+  if (n_items == 0) return QES_OK;
+  QES_ARG_CHECK(inst && items && params && flipCt && flipSt && chain_bits && chain_step && proposed && accepted &&
+                    sample_bits && counter,
+                "qes_batch_sampler_run: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  const float bm = beta * mu;
+  const int mpl = (max_nh + 31) / 32;
+#define QES_BSMP_CASE(TT, M)                                                                                      \
+  if (mpl <= M)                                                                                                  \
+    return launch_batch_sampler_mpl<TT, M>(n_inst, inst, n_items, items, warps_per_block, n_blocks, thermalize, bm, \
+                                           recompute_every, params, flipCt, flipSt, chain_bits, chain_step,      \
+                                           proposed, accepted, sample_bits, sample_logpsi, last_logpsi, counter, st);
+  if (dtype == QES_DTYPE_F32) {
+    QES_BSMP_CASE(float, 1)
+    QES_BSMP_CASE(float, 2)
+    QES_BSMP_CASE(float, 4)
+    QES_BSMP_CASE(float, 8)
+    QES_BSMP_CASE(float, 16)
+    QES_BSMP_CASE(float, 32)
+    QES_BSMP_CASE(float, 64)
+  } else {
+    QES_BSMP_CASE(float2, 1)
+    QES_BSMP_CASE(float2, 2)
+    QES_BSMP_CASE(float2, 4)
+    QES_BSMP_CASE(float2, 8)
+    QES_BSMP_CASE(float2, 16)
+  }
+#undef QES_BSMP_CASE
+  qes_set_last_message("qes_batch_sampler_run: too many hidden units for the register-resident theta cache");
+  return QES_ERR_SIZE;
 }

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <vector>
 
 // 0 = tensor cores when the shapes allow it, 1 = CUDA cores only, 2 = tensor cores required
 static std::atomic<int> g_sr_impl{0};
@@ -58,14 +59,11 @@ QES_D float2 from_c(float2 v, float2) { return v; }
 constexpr int OV_SB = 16;
 constexpr int OV_THREADS = 256;
 
+// samples [s0, s0 + OV_SB) of one problem; smw holds OV_SB * n_words(ns) words
 template <class T, class V>
-__global__ void __launch_bounds__(OV_THREADS) ov_kernel(int ns, int nh, int64_t n_samples,
-                                                        const uint32_t* __restrict__ bits,
-                                                        const T* __restrict__ tanh_theta, const V* __restrict__ v,
-                                                        float2* __restrict__ w_out) {
-  extern __shared__ uint32_t smw[];
+QES_D void ov_block(int64_t s0, uint32_t* smw, int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits,
+                    const T* __restrict__ tanh_theta, const V* __restrict__ v, float2* __restrict__ w_out) {
   const int nw = n_words(ns);
-  const int64_t s0 = (int64_t)blockIdx.x * OV_SB;
   const int nsb = (int)min((int64_t)OV_SB, n_samples - s0);
   for (int q = threadIdx.x; q < OV_SB * nw; q += blockDim.x) {
     const int sl = q / nw;
@@ -118,6 +116,15 @@ __global__ void __launch_bounds__(OV_THREADS) ov_kernel(int ns, int nh, int64_t 
   }
 }
 
+template <class T, class V>
+__global__ void __launch_bounds__(OV_THREADS) ov_kernel(int ns, int nh, int64_t n_samples,
+                                                        const uint32_t* __restrict__ bits,
+                                                        const T* __restrict__ tanh_theta, const V* __restrict__ v,
+                                                        float2* __restrict__ w_out) {
+  extern __shared__ uint32_t smw[];
+  ov_block<T, V>((int64_t)blockIdx.x * OV_SB, smw, ns, nh, n_samples, bits, tanh_theta, v, w_out);
+}
+
 // ----------------------------------------------------------------------------
 // mean of a complex float32 vector in float64 -> out[0..1]  (one block)
 // ----------------------------------------------------------------------------
@@ -151,18 +158,19 @@ constexpr int OHU_TI = OHU_TY * OHU_SPT;         // 16 sites per block
 constexpr int OHU_SC = 32;                       // samples per staged sub-chunk
 constexpr int OHU_SPLIT_SAMPLES = 256;           // samples per split
 
+// tile (bx: 64 hidden units, by: 16 sites, bz: one split of samples) of one problem
 template <class T>
-__global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
-    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ tanh_theta,
-    const float2* __restrict__ w, const double* __restrict__ wmean, double scale, T* __restrict__ partial) {
+QES_D void ohu_block(int bx, int by, int bz, int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits,
+                     const T* __restrict__ tanh_theta, const float2* __restrict__ w,
+                     const double* __restrict__ wmean, double scale, T* __restrict__ partial) {
   __shared__ T Q[OHU_SC][OHU_TM];
   __shared__ T U[OHU_SC];
   __shared__ uint32_t SW[OHU_SC][2];
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * OHU_TM + tx;
-  const int m0 = blockIdx.x * OHU_TM, i0 = blockIdx.y * OHU_TI;
+  const int m0 = bx * OHU_TM, i0 = by * OHU_TI;
   const int m = m0 + tx;
-  const int64_t sbeg = (int64_t)blockIdx.z * OHU_SPLIT_SAMPLES;
+  const int64_t sbeg = (int64_t)bz * OHU_SPLIT_SAMPLES;
   const int64_t send = min(n_samples, sbeg + OHU_SPLIT_SAMPLES);
   const int nw = n_words(ns);
   const int wlo = i0 >> 5;
@@ -203,8 +211,8 @@ __global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
         const bool up = (wd >> il) & 1ull;
         acc[k] = addx(acc[k], up ? q : scal(-1.f, q));
       }
-      if (blockIdx.y == 0 && ty == 0) accb = addx(accb, q);
-      if (blockIdx.x == 0 && tx == 0) {
+      if (by == 0 && ty == 0) accb = addx(accb, q);
+      if (bx == 0 && tx == 0) {
         const T u = U[sl];
 #pragma unroll
         for (int k = 0; k < OHU_SPT; ++k) {
@@ -216,22 +224,29 @@ __global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
     }
     __syncthreads();
   }
-  T* out = partial + (int64_t)blockIdx.z * P;
+  T* out = partial + (int64_t)bz * P;
   if (m < nh) {
 #pragma unroll
     for (int k = 0; k < OHU_SPT; ++k) {
       const int i = i0 + ty * OHU_SPT + k;
       if (i < ns) out[ns + nh + (int64_t)i * nh + m] = acc[k];
     }
-    if (blockIdx.y == 0 && ty == 0) out[ns + m] = accb;
+    if (by == 0 && ty == 0) out[ns + m] = accb;
   }
-  if (blockIdx.x == 0 && tx == 0) {
+  if (bx == 0 && tx == 0) {
 #pragma unroll
     for (int k = 0; k < OHU_SPT; ++k) {
       const int i = i0 + ty * OHU_SPT + k;
       if (i < ns) out[i] = acca[k];
     }
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
+    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ tanh_theta,
+    const float2* __restrict__ w, const double* __restrict__ wmean, double scale, T* __restrict__ partial) {
+  ohu_block<T>(blockIdx.x, blockIdx.y, blockIdx.z, ns, nh, n_samples, bits, tanh_theta, w, wmean, scale, partial);
 }
 
 // sum the split partials in float64; optional  y = G + shift * p  and  dot partials of p^H y.
@@ -851,4 +866,290 @@ extern "C" int qes_rbm_logpsi_vjp(int dtype, int ns, int nh, int64_t n_samples, 
                         st);
   return vjp_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)g, (double2*)grad_out, L,
                        st);
+}
+
+// ----------------------------------------------------------------------------
+// Batched problems: one CG per problem, all problems in lockstep launches.
+// Per-problem state bscal[b][16]: the CG slots of the single-problem solver
+// (0 rr, 1 pAp, 2 rr_new, 3 threshold^2, 4 done, 5 iterations, 6 ||b||^2,
+// 7 alpha, 8 beta), 9-10 mean of the current w, 11-12 mean of E_loc.
+// Blocks of a converged problem return at once, so its x stays frozen.
+// ----------------------------------------------------------------------------
+constexpr int BSC = 16;
+constexpr int BCG_THREADS = 1024;
+
+QES_D int64_t batch_rows(const qes_batch_instance& I) { return (int64_t)I.n_chains * I.num_samples; }
+QES_D int64_t batch_P(const qes_batch_instance& I) { return (int64_t)I.ns + I.nh + (int64_t)I.ns * I.nh; }
+QES_D int batch_nsplit(const qes_batch_instance& I) {
+  return (int)((batch_rows(I) + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES);
+}
+
+// fixed-order block sum (valid in every thread)
+QES_D double block_allsum(double v, double* red) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[q];
+  return t;
+}
+
+// mean of w (or E_loc) rows of problem blockIdx.x -> bscal[b][slot], [slot+1]
+__global__ void __launch_bounds__(BCG_THREADS) batch_mean_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                const float2* __restrict__ w, double* __restrict__ bscal,
+                                                                int slot, int skip_done) {
+  const qes_batch_instance I = inst[blockIdx.x];
+  double* sc = bscal + (int64_t)blockIdx.x * BSC;
+  if (skip_done && sc[4] != 0.0) return;
+  const int64_t rows = batch_rows(I);
+  const float2* x = w + I.sample_off;
+  double sr = 0, si = 0;
+  for (int64_t k = threadIdx.x; k < rows; k += blockDim.x) { sr += x[k].x; si += x[k].y; }
+  __shared__ double red[BCG_THREADS / 32];
+  sr = block_allsum(sr, red);
+  si = block_allsum(si, red);
+  if (threadIdx.x == 0) {
+    sc[slot] = sr / (double)rows;
+    sc[slot + 1] = si / (double)rows;
+  }
+}
+
+// items (b, sample block of OV_SB)
+template <class T, class V>
+__global__ void __launch_bounds__(OV_THREADS) batch_ov_kernel(const qes_batch_instance* __restrict__ inst,
+                                                             const int4* __restrict__ items,
+                                                             const uint32_t* __restrict__ bits,
+                                                             const T* __restrict__ tt, const V* __restrict__ v,
+                                                             float2* __restrict__ w, const double* __restrict__ bscal) {
+  extern __shared__ uint32_t smw[];
+  const int4 it = items[blockIdx.x];
+  if (bscal[(int64_t)it.x * BSC + 4] != 0.0) return;
+  const qes_batch_instance I = inst[it.x];
+  ov_block<T, V>((int64_t)it.y * OV_SB, smw, I.ns, I.nh, batch_rows(I), bits + I.sample_word_off, tt + I.tanh_off,
+                 v + I.param_off, w + I.sample_off);
+}
+
+// items (b, bx, by, bz); u = (w - bscal[b][mslot]) / rows
+template <class T>
+__global__ void __launch_bounds__(OHU_TM * OHU_TY) batch_ohu_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                   const int4* __restrict__ items,
+                                                                   const uint32_t* __restrict__ bits,
+                                                                   const T* __restrict__ tt,
+                                                                   const float2* __restrict__ w,
+                                                                   const double* __restrict__ bscal, int mslot,
+                                                                   int skip_done, T* __restrict__ partial) {
+  const int4 it = items[blockIdx.x];
+  const double* sc = bscal + (int64_t)it.x * BSC;
+  if (skip_done && sc[4] != 0.0) return;
+  const qes_batch_instance I = inst[it.x];
+  const int64_t rows = batch_rows(I);
+  ohu_block<T>(it.y, it.z, it.w, I.ns, I.nh, rows, bits + I.sample_word_off, tt + I.tanh_off, w + I.sample_off,
+               sc + mslot, 1.0 / (double)rows, partial + I.sr_part_off);
+}
+
+// b = sum of the force partials; x = 0, r = p = b; CG scalars (one block per problem)
+template <class T, class V>
+__global__ void __launch_bounds__(BCG_THREADS) batch_cg_setup_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                    const T* __restrict__ partial, double rtol,
+                                                                    double atol, V* __restrict__ x, V* __restrict__ r,
+                                                                    V* __restrict__ p, V* __restrict__ bvec,
+                                                                    double* __restrict__ bscal,
+                                                                    unsigned int* __restrict__ n_done) {
+  const qes_batch_instance I = inst[blockIdx.x];
+  double* sc = bscal + (int64_t)blockIdx.x * BSC;
+  const int64_t P = batch_P(I), o = I.param_off;
+  const int nz = batch_nsplit(I);
+  const T* part = partial + I.sr_part_off;
+  double d = 0.0;
+  for (int64_t k = threadIdx.x; k < P; k += blockDim.x) {
+    V g = vzero(V());
+    for (int z = 0; z < nz; ++z) g = vadd(g, to_d(part[(int64_t)z * P + k]));
+    bvec[o + k] = g;
+    x[o + k] = vzero(V());
+    r[o + k] = g;
+    p[o + k] = g;
+    d += vdotc(g, g);
+  }
+  __shared__ double red[BCG_THREADS / 32];
+  d = block_allsum(d, red);
+  if (threadIdx.x == 0) {
+    const double th = fmax(rtol * sqrt(d), atol);
+    sc[0] = d; sc[1] = 0.0; sc[2] = d; sc[3] = th * th;
+    sc[5] = 0.0; sc[6] = d; sc[7] = 0.0; sc[8] = 0.0;
+    sc[11] = sc[9]; sc[12] = sc[10];
+    sc[4] = (d <= sc[3]) ? 1.0 : 0.0;
+    if (sc[4] != 0.0) atomicAdd(n_done, 1u);
+  }
+}
+
+// y = sum of the matvec partials + shift p; alpha; x += alpha p; r -= alpha y; beta; p = r + beta p
+template <class T, class V>
+__global__ void __launch_bounds__(BCG_THREADS) batch_cg_update_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                     const T* __restrict__ partial, double shift,
+                                                                     V* __restrict__ x, V* __restrict__ r,
+                                                                     V* __restrict__ p, V* __restrict__ Ap,
+                                                                     double* __restrict__ bscal,
+                                                                     unsigned int* __restrict__ n_done) {
+  double* sc = bscal + (int64_t)blockIdx.x * BSC;
+  if (sc[4] != 0.0) return;
+  const qes_batch_instance I = inst[blockIdx.x];
+  const int64_t P = batch_P(I), o = I.param_off;
+  const int nz = batch_nsplit(I);
+  const T* part = partial + I.sr_part_off;
+  __shared__ double red[BCG_THREADS / 32];
+  double d = 0.0;
+  for (int64_t k = threadIdx.x; k < P; k += blockDim.x) {
+    V g = vzero(V());
+    for (int z = 0; z < nz; ++z) g = vadd(g, to_d(part[(int64_t)z * P + k]));
+    const V pk = p[o + k];
+    g = vadd(g, vscale(shift, pk));
+    Ap[o + k] = g;
+    d += vdotc(pk, g);
+  }
+  const double pap = block_allsum(d, red);
+  const double alpha = (pap > 0.0) ? sc[0] / pap : 0.0;
+  double e = 0.0;
+  for (int64_t k = threadIdx.x; k < P; k += blockDim.x) {
+    x[o + k] = vadd(x[o + k], vscale(alpha, p[o + k]));
+    const V rk = vadd(r[o + k], vscale(-alpha, Ap[o + k]));
+    r[o + k] = rk;
+    e += vdotc(rk, rk);
+  }
+  const double rr_new = block_allsum(e, red);
+  const double beta = (sc[0] > 0.0) ? rr_new / sc[0] : 0.0;
+  const bool conv = rr_new <= sc[3];
+  if (!conv)
+    for (int64_t k = threadIdx.x; k < P; k += blockDim.x) p[o + k] = vadd(r[o + k], vscale(beta, p[o + k]));
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sc[1] = pap; sc[7] = alpha; sc[2] = rr_new; sc[8] = beta; sc[0] = rr_new;
+    sc[5] += 1.0;
+    if (conv) {
+      sc[4] = 1.0;
+      atomicAdd(n_done, 1u);
+    }
+  }
+}
+
+struct BatchSRWork {
+  double* bscal;        // [n_inst][BSC]
+  unsigned int* n_done; // [1] (+pad)
+  float2* w;            // [n_samples_total]
+  void* partial;        // [sr_part_total] of T
+  void *r, *p, *Ap, *b; // [n_params_total] of V each
+};
+
+static size_t batch_sr_layout(int dtype, int n_inst, int64_t n_params_total, int64_t n_samples_total,
+                              int64_t sr_part_total, char* base, BatchSRWork* L) {
+  const size_t ts = (dtype == QES_DTYPE_C64) ? sizeof(float2) : sizeof(float);
+  const size_t vs = (dtype == QES_DTYPE_C64) ? sizeof(double2) : sizeof(double);
+  auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* q = base ? base + off : nullptr; off += up(bytes); return q; };
+  BatchSRWork W;
+  W.bscal = (double*)take((size_t)n_inst * BSC * sizeof(double));
+  W.n_done = (unsigned int*)take(256);
+  W.w = (float2*)take((size_t)n_samples_total * sizeof(float2));
+  W.partial = take((size_t)sr_part_total * ts);
+  W.r = take((size_t)n_params_total * vs);
+  W.p = take((size_t)n_params_total * vs);
+  W.Ap = take((size_t)n_params_total * vs);
+  W.b = take((size_t)n_params_total * vs);
+  if (L) *L = W;
+  return off;
+}
+
+extern "C" int qes_batch_sr_workspace_bytes(int dtype, int n_inst, int64_t n_params_total, int64_t n_samples_total,
+                                            int64_t sr_part_total, size_t* bytes) {
+  QES_ARG_CHECK(bytes && n_inst >= 0 && n_params_total >= 0 && n_samples_total >= 0 && sr_part_total >= 0,
+                "qes_batch_sr_workspace_bytes: bad args");
+  *bytes = batch_sr_layout(dtype, n_inst, n_params_total, n_samples_total, sr_part_total, nullptr, nullptr);
+  return QES_OK;
+}
+
+template <class T>
+static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, const int4* ov_items, int n_ohu,
+                         const int4* ohu_items, int64_t n_params_total, const uint32_t* bits, const T* tt,
+                         const float2* eloc, const qes_sr_options* opt, typename VecT<T>::type* x,
+                         qes_sr_result* res, const BatchSRWork& L, cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  T* partial = (T*)L.partial;
+  V* r = (V*)L.r; V* p = (V*)L.p; V* Ap = (V*)L.Ap; V* b = (V*)L.b;
+  const dim3 ohu_block_dim(OHU_TM, OHU_TY);
+  const size_t ov_smem = (size_t)OV_SB * 64 * sizeof(uint32_t);
+  QES_CUDA_CHECK(cudaMemsetAsync(L.n_done, 0, sizeof(unsigned int), st));
+  // force: mean of E_loc, O^H (E - mean) / rows, then CG set-up
+  batch_mean_kernel<<<n_inst, BCG_THREADS, 0, st>>>(inst, eloc, L.bscal, 9, 0);
+  batch_ohu_kernel<T><<<n_ohu, ohu_block_dim, 0, st>>>(inst, ohu_items, bits, tt, eloc, L.bscal, 9, 0, partial);
+  batch_cg_setup_kernel<T, V><<<n_inst, BCG_THREADS, 0, st>>>(inst, partial, opt->rtol, opt->atol, x, r, p, b,
+                                                              L.bscal, L.n_done);
+  QES_LAUNCH_CHECK_N(3);
+  const int check = opt->check_every > 0 ? opt->check_every : 8;
+  unsigned int done = 0;
+  QES_CUDA_CHECK(cudaMemcpyAsync(&done, L.n_done, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaStreamSynchronize(st));
+  int it = 0;
+  while ((int)done < n_inst && it < opt->maxiter) {
+    const int nrun = std::min(check, opt->maxiter - it);
+    for (int q = 0; q < nrun; ++q) {
+      batch_ov_kernel<T, V><<<n_ov, OV_THREADS, ov_smem, st>>>(inst, ov_items, bits, tt, p, L.w, L.bscal);
+      batch_mean_kernel<<<n_inst, BCG_THREADS, 0, st>>>(inst, L.w, L.bscal, 9, 1);
+      batch_ohu_kernel<T><<<n_ohu, ohu_block_dim, 0, st>>>(inst, ohu_items, bits, tt, L.w, L.bscal, 9, 1, partial);
+      batch_cg_update_kernel<T, V><<<n_inst, BCG_THREADS, 0, st>>>(inst, partial, opt->shift, x, r, p, Ap, L.bscal,
+                                                                   L.n_done);
+      QES_LAUNCH_CHECK_N(4);
+    }
+    it += nrun;
+    QES_CUDA_CHECK(cudaMemcpyAsync(&done, L.n_done, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    QES_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+  if (opt->rhs_prefactor != 1.0) {
+    scale_vec_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n_params_total, opt->rhs_prefactor, x);
+    QES_LAUNCH_CHECK();
+  }
+  if (res) {
+    std::vector<double> hs((size_t)n_inst * BSC);
+    QES_CUDA_CHECK(cudaMemcpyAsync(hs.data(), L.bscal, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QES_CUDA_CHECK(cudaStreamSynchronize(st));
+    for (int q = 0; q < n_inst; ++q) {
+      const double* h = hs.data() + (size_t)q * BSC;
+      res[q].iterations = (int)h[5];
+      res[q].converged = h[4] != 0.0 ? 1 : 0;
+      res[q].residual = sqrt(h[0]);
+      res[q].rhs_norm = sqrt(h[6]);
+      res[q].e_mean_re = h[11];
+      res[q].e_mean_im = h[12];
+    }
+  }
+  return (int)done == n_inst ? QES_OK : QES_ERR_NOT_CONVERGED;
+}
+
+extern "C" int qes_batch_sr_solve_cg(int dtype, int n_inst, const qes_batch_instance* inst, int n_ov_items,
+                                     const int32_t* ov_items, int n_ohu_items, const int32_t* ohu_items,
+                                     int64_t n_params_total, int64_t n_samples_total, int64_t sr_part_total,
+                                     const uint32_t* sample_bits, const void* tanh_theta, const void* eloc,
+                                     const qes_sr_options* opts, void* x_out, qes_sr_result* results,
+                                     void* workspace, size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_batch_sr_solve_cg: bad dtype");
+  QES_ARG_CHECK(n_inst > 0 && n_ov_items > 0 && n_ohu_items > 0 && n_params_total > 0 && n_samples_total > 0,
+                "qes_batch_sr_solve_cg: bad sizes");
+  QES_ARG_CHECK(inst && ov_items && ohu_items && sample_bits && tanh_theta && eloc && opts && x_out,
+                "qes_batch_sr_solve_cg: null pointer");
+  QES_ARG_CHECK(opts->maxiter >= 0 && opts->shift >= 0.0, "qes_batch_sr_solve_cg: bad options");
+  const size_t need = batch_sr_layout(dtype, n_inst, n_params_total, n_samples_total, sr_part_total, nullptr, nullptr);
+  if (!workspace || workspace_bytes < need) {
+    qes_set_last_message("qes_batch_sr_solve_cg: workspace too small");
+    return QES_ERR_WORKSPACE;
+  }
+  BatchSRWork L;
+  batch_sr_layout(dtype, n_inst, n_params_total, n_samples_total, sr_part_total, (char*)workspace, &L);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return batch_sr_cg_t<float>(n_inst, inst, n_ov_items, (const int4*)ov_items, n_ohu_items, (const int4*)ohu_items,
+                                n_params_total, sample_bits, (const float*)tanh_theta, (const float2*)eloc, opts,
+                                (double*)x_out, results, L, st);
+  return batch_sr_cg_t<float2>(n_inst, inst, n_ov_items, (const int4*)ov_items, n_ohu_items, (const int4*)ohu_items,
+                               n_params_total, sample_bits, (const float2*)tanh_theta, (const float2*)eloc, opts,
+                               (double2*)x_out, results, L, st);
 }

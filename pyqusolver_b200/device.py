@@ -175,6 +175,18 @@ def loss_stats(eloc, probs=None, workspace=None):
     return out
 
 
+def loss_rhat(eloc, n_chains, workspace=None):
+    """[r_hat, sigma2] (float64 device tensor) of E_loc split into n_chains contiguous blocks."""
+    n = int(eloc.shape[0])
+    nb = C.c_size_t(0)
+    call("qes_loss_rhat_workspace_bytes", n, int(n_chains), C.byref(nb))
+    if workspace is None or workspace.numel() < nb.value:
+        workspace = torch.empty((int(nb.value),), dtype=torch.uint8, device=eloc.device)
+    out = torch.empty((2,), dtype=torch.float64, device=eloc.device)
+    call("qes_loss_rhat", n, int(n_chains), ptr(eloc), ptr(out), ptr(workspace), int(workspace.numel()), stream_ptr())
+    return out
+
+
 # --------------------------------------------------------------------------------------
 # SR
 # --------------------------------------------------------------------------------------

@@ -43,12 +43,18 @@ class NQSSingleStepResult:
 
 @dataclass
 class NQSTrainStats:
+    """Per-epoch history, with the reference's field names (``QES/NQS/src/nqs_train.py:136-148``)."""
     history: List[complex] = field(default_factory=list)
     history_std: List[float] = field(default_factory=list)
-    sigma2: List[float] = field(default_factory=list)
+    lr_history: List[float] = field(default_factory=list)
+    diag_history: List[float] = field(default_factory=list)
+    sigma2_history: List[float] = field(default_factory=list)
+    rhat_history: List[float] = field(default_factory=list)
     acceptance: List[float] = field(default_factory=list)
     cg_iterations: List[int] = field(default_factory=list)
     timings: List[float] = field(default_factory=list)
+    seed: Optional[int] = None
+    exact_predictions: Optional[np.ndarray] = None
     exact: Optional[float] = None
 
     @property
@@ -200,9 +206,10 @@ class NQS:
             self._sampler._therm_steps = int(num_thermal)
         self._tdvp = TDVP(use_sr=use_sr, use_minsr=use_minsr, rhs_prefactor=rhs_prefactor, sr_lin_solver=lin_solver,
                           sr_diag_shift=diag_shift, sr_tol=sr_tol, sr_maxiter=sr_maxiter, grad_clip=grad_clip)
-        stats = NQSTrainStats()
+        stats = NQSTrainStats(seed=self._seed)
         if exact_predictions is not None:
-            stats.exact = float(np.min(np.real(np.atleast_1d(exact_predictions))))
+            stats.exact_predictions = np.atleast_1d(np.asarray(exact_predictions))
+            stats.exact = float(np.min(np.real(stats.exact_predictions)))
             self.exact = stats.exact
         for epoch in range(int(n_epochs)):
             t0 = time.perf_counter()
@@ -211,7 +218,10 @@ class NQS:
             stats.timings.append(time.perf_counter() - t0)
             stats.history.append(info["mean"])
             stats.history_std.append(info["std"])
-            stats.sigma2.append(info["var"])
+            stats.lr_history.append(float(lr))
+            stats.diag_history.append(float(diag_shift))
+            stats.sigma2_history.append(info["sigma2"])
+            stats.rhat_history.append(info["r_hat"])
             stats.acceptance.append(info["acceptance"])
             stats.cg_iterations.append(info["cg_iterations"])
             if callback is not None:
@@ -228,11 +238,14 @@ class NQS:
         _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
         eloc = self.local_energy_bits(bits, tn)
         st = dv.loss_stats(eloc)
+        rh = dv.loss_rhat(eloc, self._sampler.numchains)
         x = tdvp.solve(net, bits, tn, eloc)
         dv.param_update(net.flat, net.master, x, lr)
         net.bump()
         s = st.cpu().numpy()
+        r = rh.cpu().numpy()
         acc = self._sampler.accepted_ratio.mean().item()
         return {"mean": complex(s[0], s[1]), "var": float(s[2]), "std": float(s[3]), "acceptance": acc,
+                "r_hat": float(r[0]), "sigma2": float(r[1]),
                 "cg_iterations": int(tdvp.last_info.get("iterations", 0)),
                 "cg_converged": bool(tdvp.last_info.get("converged", True))}

@@ -156,6 +156,20 @@ def test_loss_stats_match_numpy():
         assert o[3] == pytest.approx(std, rel=1e-9)
 
 
+@pytest.mark.parametrize("n,nch", [(16384, 4096), (5000, 8), (4096, 1), (4096, 5000), (5000, 3), (64, 64)])
+def test_loss_rhat_matches_oracle(n, nch):
+    rng = np.random.default_rng(n + nch)
+    e = (rng.normal(size=n) + 1j * rng.normal(size=n)).astype(np.complex64) - 40.0
+    e[: n // 2] += 0.3        # a between-block spread so R-hat differs from 1
+    out = dv.loss_rhat(torch.as_tensor(e).cuda(), nch).cpu().numpy()
+    ref = oest.step_rhat(e.astype(np.complex128), nch)
+    if np.isnan(ref):
+        assert np.isnan(out[0])
+    else:
+        assert out[0] == pytest.approx(ref, rel=1e-10)
+    assert out[1] == pytest.approx(oest.step_sigma2(e.astype(np.complex128)), rel=1e-10)
+
+
 # ------------------------------------------------------------------------- log-derivatives / backward
 @pytest.mark.parametrize("cplx", [False, True])
 def test_log_derivatives_match_oracle_and_finite_differences(cplx):

@@ -286,6 +286,21 @@ int qes_param_update(int dtype, int64_t n_params, double lr, const void* x,
                      void* master, void* params, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Exact ground energy (the ED reference of the energy-error metric): Lanczos
+ * over the full 2^ns S^z product basis (ns <= 32; basis bit i = site i,
+ * 1 = up) with the Hamiltonian applied matrix-free from `ham` (the same
+ * lowered terms the local energy reads; real matrix elements only).
+ * y = H x for qes_ed_matvec.  Lanczos stops when the lowest Ritz value
+ * changes by <= tol * max(1, |E|) between iterations (QES_ERR_NOT_CONVERGED
+ * after max_iter).  Replaces model.diagonalize(method='lanczos')
+ * (QES/Algebra/hamil.py:1809; its solver lives in the absent eigen module). */
+int qes_ed_workspace_bytes(int ns, size_t* bytes);
+int qes_ed_matvec(int ns, const qes_hamiltonian* ham, const double* x, double* y, void* stream);
+int qes_ed_lanczos(int ns, const qes_hamiltonian* ham, int max_iter, double tol, uint64_t seed,
+                   double* e0_out, int* iterations_out, void* workspace, size_t workspace_bytes,
+                   void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Batched independent problems.  Many (RBM, Hamiltonian, chain set) triples
  * of uneven size advance together: every phase of the VMC step is one
  * launch over all problems.  The reference runs one NQS per problem

@@ -115,6 +115,10 @@ SIGNATURES = {
                         C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_rbm_logpsi_vjp": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_param_update": [C.c_int, _i64, C.c_double, _vp, _vp, _vp, _vp],
+    "qes_ed_workspace_bytes": [C.c_int, C.POINTER(_sz)],
+    "qes_ed_matvec": [C.c_int, C.POINTER(Hamiltonian), _vp, _vp, _vp],
+    "qes_ed_lanczos": [C.c_int, C.POINTER(Hamiltonian), C.c_int, C.c_double, _u64, C.POINTER(C.c_double),
+                       C.POINTER(C.c_int), _vp, _sz, _vp],
     "qes_batch_move_tables": [C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                               _vp],
     "qes_batch_sampler_run": [C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_float,

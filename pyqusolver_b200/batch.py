@@ -85,6 +85,9 @@ class NQSBatch:
 
         ns = np.array([m.ns for m in self.models], dtype=np.int64)
         nh = np.array([int(round(alpha * n)) for n in ns], dtype=np.int64)
+        if ns.max() > 2048 or nh.max() > (512 if self.is_complex else 2048):
+            raise ValueError("the batched sampler holds ns <= 2048 spins and nh <= 2048 (real) / 512 (complex) "
+                             "hidden units per chain")
         chains = np.full(self.n_inst, int(s_numchains), dtype=np.int64)
         nsamp = np.full(self.n_inst, int(s_numsamples), dtype=np.int64)
         sweep = ns.copy() if s_sweep_steps is None else np.full(self.n_inst, int(s_sweep_steps), dtype=np.int64)
@@ -364,10 +367,18 @@ class NQSBatch:
             ts = []
             for _ in range(repeats + 1):
                 ev0.record()
-                self._run_sampler(w, bps, False, cb, cs, pp, aa)
+                try:
+                    self._run_sampler(w, bps, False, cb, cs, pp, aa)
+                except _lib.QESError as e:
+                    if e.code != _lib.QES_ERR_ARG:
+                        raise
+                    ts = []
+                    break                      # block size beyond the kernel's register budget
                 ev1.record()
                 torch.cuda.synchronize()
                 ts.append(ev0.elapsed_time(ev1))
+            if len(ts) < 2:
+                continue
             t = min(ts[1:])
             if t < best_t:
                 best, best_t = (w, bps), t

@@ -351,6 +351,12 @@ static int launch_batch_sampler_mpl(int n_inst, const qes_batch_instance* inst, 
                                     uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
                                     unsigned int* counter, cudaStream_t st) {
   (void)n_inst;
+  cudaFuncAttributes fa;
+  QES_CUDA_CHECK(cudaFuncGetAttributes(&fa, batch_sampler_kernel<T, MPL>));
+  if (32 * warps > fa.maxThreadsPerBlock) {
+    qes_set_last_message("qes_batch_sampler_run: warps_per_block exceeds the kernel's register-limited block size");
+    return QES_ERR_ARG;
+  }
   QES_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st));
   const size_t smem = (size_t)warps * SMP_MAX_WORDS * sizeof(uint32_t);
   batch_sampler_kernel<T, MPL><<<blocks, 32 * warps, smem, st>>>(

@@ -131,6 +131,37 @@ class SpinHamiltonian:
     def get_loc_energy_fun(self):
         return self.connected
 
+    # -- exact ground energy -------------------------------------------------------------
+    def diagonalize(self, method: str = "lanczos", k: int = 1, tol: float = 1e-12, maxiter: int = 600,
+                    seed: int = 7, **kwargs):
+        """Ground energy by Lanczos on the GPU over the full 2^ns basis (``qes_ed_lanczos``).
+
+        Mirrors ``model.diagonalize(method='lanczos')`` (``QES/Algebra/hamil.py:1809``) for the
+        lowest eigenvalue: the result is stored in ``eig_val`` (ascending, length 1).
+        """
+        if str(method).lower() not in ("lanczos", "auto", "exact"):
+            raise NotImplementedError(f"diagonalize(method={method!r}): the GPU path implements Lanczos")
+        if int(k) != 1:
+            raise NotImplementedError("the GPU Lanczos returns the ground energy only (k=1)")
+        import ctypes as C
+        import torch
+        from . import _lib, device as dv
+        dh = dv.DeviceHamiltonian(self.lower())
+        nb = C.c_size_t(0)
+        _lib.call("qes_ed_workspace_bytes", self.ns, C.byref(nb))
+        ws = torch.empty((int(nb.value),), dtype=torch.uint8, device="cuda")
+        e0, its = C.c_double(0.0), C.c_int(0)
+        _lib.call("qes_ed_lanczos", self.ns, C.byref(dh.struct), int(maxiter), float(tol),
+                  C.c_uint64(int(seed)), C.byref(e0), C.byref(its), _lib.ptr(ws), int(ws.numel()),
+                  _lib.stream_ptr())
+        self._eig_val = np.array([e0.value])
+        self.lanczos_iterations = its.value
+        return self._eig_val
+
+    @property
+    def eig_val(self):
+        return getattr(self, "_eig_val", None)
+
     # -- lowering -----------------------------------------------------------------------
     def lower(self) -> LoweredHamiltonian:
         zf: Dict[int, complex] = {}

@@ -54,7 +54,10 @@ def test_batch_matches_single_problem_path(dtype):
             bb, blp = B.samples(b)
             assert torch.equal(bits.cpu(), bb.cpu()), f"problem {b}: samples differ"
             assert torch.equal(lp.cpu(), blp.cpu())
-            assert acc[b] == pytest.approx(q.sampler.accepted_ratio.mean().item(), abs=0)
+            o = int(B.chain_off[b])
+            assert torch.equal(B.accepted[o:o + chains].cpu(), q.sampler.accepted.cpu())
+            assert torch.equal(B.proposed[o:o + chains].cpu(), q.sampler.proposed.cpu())
+            assert acc[b] == pytest.approx(q.sampler.accepted_ratio.mean().item(), rel=1e-12)
             _, tn, _ = dv.rbm_forward(q.net.flat, q.net.ns, q.net.nh, bits, theta=False, tanh=True, logpsi=False)
             assert torch.equal(tn.cpu(), B.tanh_theta(b).cpu())
             e = q.local_energy_bits(bits, tn)

@@ -1,0 +1,66 @@
+"""GPU Lanczos ground energy and matrix-free H x against the oracle's sparse S^z-basis H."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import lattice as olat, hamiltonian as oH, ed as oed
+import pyqusolver_b200 as qb
+from pyqusolver_b200 import device as dv, _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _models():
+    return [
+        ("tfim_chain12", qb.TransverseFieldIsing(qb.SquareLattice(1, 12, 1, bc="pbc"), j=1.0, hx=0.7, hz=0.0),
+         oH.tfim_terms(olat.SquareLattice(1, 12, 1, "pbc"), 1.0, 0.7, 0.0)),
+        ("tfim_4x4_hz", qb.TransverseFieldIsing(qb.SquareLattice(2, 4, 4, bc="pbc"), j=1.0, hx=3.04, hz=0.2),
+         oH.tfim_terms(olat.SquareLattice(2, 4, 4, "pbc"), 1.0, 3.04, 0.2)),
+        ("xxz_4x4", qb.XXZ(qb.SquareLattice(2, 4, 4, bc="pbc"), jxy=-1.0, jz=-1.0),
+         oH.xxz_terms(olat.SquareLattice(2, 4, 4, "pbc"), -1.0, -1.0)),
+        ("j1j2_4x4", qb.J1J2Model(qb.SquareLattice(2, 4, 4, bc="pbc"), J1=-1.0, J2=-0.5),
+         oH.j1j2_terms(olat.SquareLattice(2, 4, 4, "pbc"), -1.0, -0.5)),
+    ]
+
+
+def _bitrev(idx, ns):
+    out = np.zeros_like(idx)
+    for i in range(ns):
+        out |= ((idx >> (ns - 1 - i)) & 1) << i
+    return out
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_ed_matvec_matches_oracle_matrix(k):
+    name, model, terms = _models()[k]
+    ns = model.ns
+    H, basis = oH.sparse_hamiltonian(terms, ns, n_up=None)
+    rng = np.random.default_rng(k)
+    x_or = rng.normal(size=1 << ns)
+    y_or = (H @ x_or).real
+    perm = _bitrev(basis, ns)             # oracle row r (site i = bit ns-1-i) -> library index (site i = bit i)
+    x = np.empty_like(x_or)
+    x[perm] = x_or
+    dh = dv.DeviceHamiltonian(model.lower())
+    xd = torch.as_tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    _lib.call("qes_ed_matvec", ns, C.byref(dh.struct), _lib.ptr(xd), _lib.ptr(yd), _lib.stream_ptr())
+    y = yd.cpu().numpy()[perm]
+    assert np.max(np.abs(y - y_or)) <= 1e-5 * np.max(np.abs(y_or)), name   # float32 coefficients
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_ed_lanczos_ground_energy_matches_oracle(k):
+    name, model, terms = _models()[k]
+    e_ref = oed.ground_energy(terms, model.ns, n_up=None)
+    e = model.diagonalize(method="lanczos")[0]
+    assert abs(e - e_ref) <= 1e-6 * abs(e_ref), (name, e, e_ref)
+
+
+def test_ed_rejects_large_or_bad_input():
+    model = qb.TransverseFieldIsing(qb.SquareLattice(1, 40, 1, bc="pbc"), j=1.0, hx=1.0, hz=0.0)
+    with pytest.raises(_lib.QESError):
+        model.diagonalize()

@@ -373,9 +373,10 @@ int qes_batch_loss_stats(int n_inst, const qes_batch_instance* inst, const void*
                          void* stream);
 /* Per-problem SR solve (S_b + shift) x_b = F_b by CG, all problems in
  * lockstep launches, each frozen at its own convergence; x at param_off
- * (float64 / complex128), scaled by rhs_prefactor.  ov items (b, sample
- * block of 16, 0, 0); ohu items (b, 64-unit block, 16-site block, split of
- * 256 samples).  sr_part_total = sum_b ceil(rows_b/256) * P_b.  results:
+ * (float64 / complex128), scaled by rhs_prefactor.  ov items (b, first
+ * row, rows <= 64, 0); ohu items (b, split of 256 samples, 0, 0).  Each
+ * problem needs ns * nh <= 16384 (real) / 8192 (complex) and nh <= 512
+ * (QES_ERR_SIZE otherwise): the batch is meant for many small problems.  sr_part_total = sum_b ceil(rows_b/256) * P_b.  results:
  * HOST array of n_inst.                                                    */
 int qes_batch_sr_workspace_bytes(int dtype, int n_inst, int64_t n_params_total, int64_t n_samples_total,
                                  int64_t sr_part_total, size_t* bytes);

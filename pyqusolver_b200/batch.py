@@ -35,8 +35,8 @@ from . import device as dv
 from ._lib import call, ptr, stream_ptr
 from .hamiltonian import SpinHamiltonian
 
-OHU_TM, OHU_TI, OHU_SPLIT = 64, 16, 256     # tile of the O^H u kernel (sr.cu)
-OV_SB, FWD_SB, ELOC_SB, RED_SB = 16, 16, 32, 256
+OHU_SPLIT = 256                             # samples per split of the O^H u partials (sr.cu)
+OV_ROWS, FWD_SB, ELOC_SB, RED_SB = 64, 16, 32, 256
 
 
 def _ceil(a, b):
@@ -197,9 +197,9 @@ class NQSBatch:
         self.n_items_eloc = len(eloc_items)
         self.items_eloc = L(eloc_items or [(0, 0, 0, 0)])
         self.items_red = L([(b, q, 0, 0) for b in order for q in range(_ceil(int(rows[b]), RED_SB))])
-        self.items_ov = L([(b, q, 0, 0) for b in order for q in range(_ceil(int(rows[b]), OV_SB))])
-        self.items_ohu = L([(b, bx, by, bz) for b in order for bx in range(_ceil(int(nh[b]), OHU_TM))
-                            for by in range(_ceil(int(ns[b]), OHU_TI)) for bz in range(int(nsplit[b]))])
+        self.items_ov = L([(b, r0, min(OV_ROWS, int(rows[b]) - r0), 0) for b in order
+                           for r0 in range(0, int(rows[b]), OV_ROWS)])
+        self.items_ohu = L([(b, z, 0, 0) for b in order for z in range(int(nsplit[b]))])
         self.max_nh = int(nh.max())
         props = torch.cuda.get_device_properties(self.device)
         self.n_sm = props.multi_processor_count

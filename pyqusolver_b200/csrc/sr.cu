@@ -915,37 +915,213 @@ __global__ void __launch_bounds__(BCG_THREADS) batch_mean_kernel(const qes_batch
   }
 }
 
-// items (b, sample block of OV_SB)
-template <class T, class V>
-__global__ void __launch_bounds__(OV_THREADS) batch_ov_kernel(const qes_batch_instance* __restrict__ inst,
-                                                             const int4* __restrict__ items,
-                                                             const uint32_t* __restrict__ bits,
-                                                             const T* __restrict__ tt, const V* __restrict__ v,
-                                                             float2* __restrict__ w, const double* __restrict__ bscal) {
-  extern __shared__ uint32_t smw[];
+// ---- matvec halves of the batched solve (small problems) -------------------------------------
+// ov  item (b, first row, rows <= BOV_ROWS, 0): the block stages V = v_W (float32), v_b, v_a and
+//     the spins of its rows (as +-1 floats, site-major) in shared memory; each warp advances
+//     BOV_GROUP samples at once, lanes over hidden units:
+//       z_m = v_b,m + sum_i sigma_i V_im ,  (O v)_s = sum_m t_sm z_m + sigma . v_a
+// ohu item (b, split z, 0, 0): the block owns every (site, hidden unit) entry of the split's
+//     partial; thread = (hidden unit m, group of Kg consecutive sites); per staged sample it
+//     reads q_sm = conj(t_sm) u_s once and the group's signs as float4 broadcasts.  A virtual
+//     site ns with sigma = +1 yields g_b = sum_s q_s; g_a = sum_s sigma_s u_s is accumulated by
+//     threads i < ns while staging.
+constexpr int BOV_ROWS = 64;
+constexpr int BOV_THREADS = 256;
+constexpr int BOV_GROUP = 4;
+constexpr int BOHU_THREADS = 512;
+constexpr int BOHU_SC = 32;
+
+QES_HD int64_t bsmall_align16(int64_t bytes) { return (bytes + 15) & ~(int64_t)15; }
+
+template <class T>
+QES_HD size_t batch_ov_smem(int ns, int nh) {
+  return (size_t)bsmall_align16((int64_t)((int64_t)ns * nh + nh + ns) * sizeof(T)) +
+         (size_t)ns * BOV_ROWS * sizeof(float);
+}
+
+template <class T, class V, int MPL>
+__global__ void __launch_bounds__(BOV_THREADS) batch_ov_small_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                    const int4* __restrict__ items,
+                                                                    const uint32_t* __restrict__ bits,
+                                                                    const T* __restrict__ tt, const V* __restrict__ v,
+                                                                    float2* __restrict__ w,
+                                                                    const double* __restrict__ bscal) {
+  extern __shared__ __align__(16) uint8_t bov_sm[];
   const int4 it = items[blockIdx.x];
   if (bscal[(int64_t)it.x * BSC + 4] != 0.0) return;
   const qes_batch_instance I = inst[it.x];
-  ov_block<T, V>((int64_t)it.y * OV_SB, smw, I.ns, I.nh, batch_rows(I), bits + I.sample_word_off, tt + I.tanh_off,
-                 v + I.param_off, w + I.sample_off);
+  const int ns = I.ns, nh = I.nh, nw = n_words(ns);
+  const int64_t r0 = it.y;
+  const int nr = it.z;
+  T* Vs = reinterpret_cast<T*>(bov_sm);
+  T* vbs = Vs + (int64_t)ns * nh;
+  T* vas = vbs + nh;
+  float* sigT = reinterpret_cast<float*>(bov_sm + bsmall_align16((int64_t)((int64_t)ns * nh + nh + ns) * sizeof(T)));
+  const V* pv = v + I.param_off;
+  for (int e = threadIdx.x; e < ns * nh; e += blockDim.x) Vs[e] = to_f(pv[ns + nh + e]);
+  for (int m = threadIdx.x; m < nh; m += blockDim.x) vbs[m] = to_f(pv[ns + m]);
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) vas[i] = to_f(pv[i]);
+  const uint32_t* bw = bits + I.sample_word_off;
+  for (int e = threadIdx.x; e < ns * BOV_ROWS; e += blockDim.x) {
+    const int i = e / BOV_ROWS, q = e % BOV_ROWS;
+    float sg = 0.f;
+    if (q < nr) sg = ((bw[(r0 + q) * nw + (i >> 5)] >> (i & 31)) & 1u) ? 1.f : -1.f;
+    sigT[e] = sg;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const T* tb = tt + I.tanh_off;
+  float2* wo = w + I.sample_off;
+  for (int g0 = warp * BOV_GROUP; g0 < nr; g0 += (BOV_THREADS / 32) * BOV_GROUP) {
+    T z[BOV_GROUP][MPL];
+#pragma unroll
+    for (int r = 0; r < MPL; ++r) {
+      const int m = lane + 32 * r;
+      const T b0 = (m < nh) ? vbs[m] : ScalarTraits<T>::zero();
+#pragma unroll
+      for (int j = 0; j < BOV_GROUP; ++j) z[j][r] = b0;
+    }
+    for (int i = 0; i < ns; ++i) {
+      const float4 sg = *reinterpret_cast<const float4*>(sigT + i * BOV_ROWS + g0);
+      const T* vr = Vs + (int64_t)i * nh;
+#pragma unroll
+      for (int r = 0; r < MPL; ++r) {
+        const int m = lane + 32 * r;
+        if (m < nh) {
+          const T x = vr[m];
+          z[0][r] = addx(z[0][r], scal(sg.x, x));
+          z[1][r] = addx(z[1][r], scal(sg.y, x));
+          z[2][r] = addx(z[2][r], scal(sg.z, x));
+          z[3][r] = addx(z[3][r], scal(sg.w, x));
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < BOV_GROUP; ++j) {
+      const int q = g0 + j;
+      T acc = ScalarTraits<T>::zero();
+      if (q < nr) {
+        const T* trow = tb + (r0 + q) * nh;
+#pragma unroll
+        for (int r = 0; r < MPL; ++r) {
+          const int m = lane + 32 * r;
+          if (m < nh) acc = addx(acc, mulx(trow[m], z[j][r]));
+        }
+        for (int i = lane; i < ns; i += 32) acc = addx(acc, scal(sigT[i * BOV_ROWS + q], vas[i]));
+      }
+      acc = warp_sum(acc);
+      if (lane == 0 && q < nr) wo[r0 + q] = to_c(acc);
+    }
+  }
 }
 
-// items (b, bx, by, bz); u = (w - bscal[b][mslot]) / rows
+// threads: m = tid % nh, site group g = tid / nh (G = BOHU_THREADS / nh groups of Kg sites,
+// Kg a multiple of 4 with G * Kg >= ns + 1); shared: Q[BOHU_SC][nh], U[BOHU_SC], sig[BOHU_SC][G*Kg]
+QES_HD int batch_ohu_kg(int ns, int nh) {
+  const int G = BOHU_THREADS / nh;
+  const int kg = (ns + 1 + G - 1) / G;
+  return (kg + 3) & ~3;
+}
 template <class T>
-__global__ void __launch_bounds__(OHU_TM * OHU_TY) batch_ohu_kernel(const qes_batch_instance* __restrict__ inst,
-                                                                   const int4* __restrict__ items,
-                                                                   const uint32_t* __restrict__ bits,
-                                                                   const T* __restrict__ tt,
-                                                                   const float2* __restrict__ w,
-                                                                   const double* __restrict__ bscal, int mslot,
-                                                                   int skip_done, T* __restrict__ partial) {
+QES_HD size_t batch_ohu_smem(int ns, int nh) {
+  const int G = BOHU_THREADS / nh;
+  return (size_t)bsmall_align16((int64_t)BOHU_SC * nh * sizeof(T) + BOHU_SC * sizeof(T)) +
+         (size_t)BOHU_SC * G * batch_ohu_kg(ns, nh) * sizeof(float);
+}
+
+template <class T, int KMAX>
+__global__ void __launch_bounds__(BOHU_THREADS) batch_ohu_small_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                      const int4* __restrict__ items,
+                                                                      const uint32_t* __restrict__ bits,
+                                                                      const T* __restrict__ tt,
+                                                                      const float2* __restrict__ w,
+                                                                      const double* __restrict__ bscal, int mslot,
+                                                                      int skip_done, T* __restrict__ partial) {
+  extern __shared__ __align__(16) uint8_t boh_sm[];
   const int4 it = items[blockIdx.x];
   const double* sc = bscal + (int64_t)it.x * BSC;
   if (skip_done && sc[4] != 0.0) return;
   const qes_batch_instance I = inst[it.x];
+  const int ns = I.ns, nh = I.nh, nw = n_words(ns);
   const int64_t rows = batch_rows(I);
-  ohu_block<T>(it.y, it.z, it.w, I.ns, I.nh, rows, bits + I.sample_word_off, tt + I.tanh_off, w + I.sample_off,
-               sc + mslot, 1.0 / (double)rows, partial + I.sr_part_off);
+  const int G = BOHU_THREADS / nh;
+  const int Kg = batch_ohu_kg(ns, nh), SW = G * Kg;      // sig row stride (>= ns + 1)
+  T* Q = reinterpret_cast<T*>(boh_sm);
+  T* U = Q + BOHU_SC * nh;
+  float* sig = reinterpret_cast<float*>(boh_sm + bsmall_align16((int64_t)BOHU_SC * nh * sizeof(T) + BOHU_SC * sizeof(T)));
+  const int tid = threadIdx.x;
+  const int m = tid % nh, g = tid / nh;
+  const bool active = g < G;
+  const int i0 = g * Kg;
+  const float mr = (float)sc[mslot], mi = (float)sc[mslot + 1];
+  const float fs = (float)(1.0 / (double)rows);
+  const uint32_t* bw = bits + I.sample_word_off;
+  const T* tb = tt + I.tanh_off;
+  const float2* wb = w + I.sample_off;
+  const int64_t sbeg = (int64_t)it.y * OHU_SPLIT_SAMPLES;
+  const int64_t send = min(rows, sbeg + OHU_SPLIT_SAMPLES);
+  T acc[KMAX];
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) acc[k] = ScalarTraits<T>::zero();
+  T acca = ScalarTraits<T>::zero();                       // g_a of site tid (tid < ns)
+  for (int64_t c0 = sbeg; c0 < send; c0 += BOHU_SC) {
+    const int nc = (int)min((int64_t)BOHU_SC, send - c0);
+    for (int sl = tid; sl < BOHU_SC; sl += blockDim.x) {
+      T u = ScalarTraits<T>::zero();
+      if (sl < nc) {
+        const float2 wv = wb[c0 + sl];
+        u = from_c(make_float2((wv.x - mr) * fs, (wv.y - mi) * fs), T());
+      }
+      U[sl] = u;
+    }
+    for (int e = tid; e < BOHU_SC * SW; e += blockDim.x) {
+      const int sl = e / SW, i = e % SW;
+      float sg = 0.f;
+      if (sl < nc) {
+        if (i < ns) sg = ((bw[(c0 + sl) * nw + (i >> 5)] >> (i & 31)) & 1u) ? 1.f : -1.f;
+        else if (i == ns) sg = 1.f;                       // virtual site: g_b
+      }
+      sig[e] = sg;
+    }
+    __syncthreads();
+    for (int e = tid; e < BOHU_SC * nh; e += blockDim.x) {
+      const int sl = e / nh, mm = e % nh;
+      Q[e] = (sl < nc) ? mulx(conjx(tb[(c0 + sl) * nh + mm]), U[sl]) : ScalarTraits<T>::zero();
+    }
+    if (tid < ns)
+      for (int sl = 0; sl < nc; ++sl) acca = addx(acca, scal(sig[sl * SW + tid], U[sl]));
+    __syncthreads();
+    if (active) {
+      for (int sl = 0; sl < nc; ++sl) {
+        const T q = Q[sl * nh + m];
+        const float* srow = sig + sl * SW + i0;
+#pragma unroll
+        for (int k = 0; k < KMAX; k += 4) {
+          if (k < Kg) {
+            const float4 s4 = *reinterpret_cast<const float4*>(srow + k);
+            acc[k] = addx(acc[k], scal(s4.x, q));
+            acc[k + 1] = addx(acc[k + 1], scal(s4.y, q));
+            acc[k + 2] = addx(acc[k + 2], scal(s4.z, q));
+            acc[k + 3] = addx(acc[k + 3], scal(s4.w, q));
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  T* out = partial + I.sr_part_off + (int64_t)it.y * P;
+  if (active) {
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) {
+      const int i = i0 + k;
+      if (k < Kg) {
+        if (i < ns) out[ns + nh + (int64_t)i * nh + m] = acc[k];
+        else if (i == ns) out[ns + m] = acc[k];
+      }
+    }
+  }
+  if (tid < ns) out[tid] = acca;
 }
 
 // b = sum of the force partials; x = 0, r = p = b; CG scalars (one block per problem)
@@ -1068,20 +1244,74 @@ extern "C" int qes_batch_sr_workspace_bytes(int dtype, int n_inst, int64_t n_par
   return QES_OK;
 }
 
+template <class T, class V, int MPL>
+static int launch_batch_ov(int n_ov, size_t smem, const qes_batch_instance* inst, const int4* items,
+                           const uint32_t* bits, const T* tt, const V* p, float2* w, const double* bscal,
+                           cudaStream_t st) {
+  QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ov_small_kernel<T, V, MPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+  batch_ov_small_kernel<T, V, MPL><<<n_ov, BOV_THREADS, smem, st>>>(inst, items, bits, tt, p, w, bscal);
+  return QES_OK;
+}
+
+template <class T, int KMAX>
+static int launch_batch_ohu(int n_ohu, size_t smem, const qes_batch_instance* inst, const int4* items,
+                            const uint32_t* bits, const T* tt, const float2* w, const double* bscal, int skip_done,
+                            T* partial, cudaStream_t st) {
+  QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ohu_small_kernel<T, KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+  batch_ohu_small_kernel<T, KMAX><<<n_ohu, BOHU_THREADS, smem, st>>>(inst, items, bits, tt, w, bscal, 9, skip_done,
+                                                                     partial);
+  return QES_OK;
+}
+
 template <class T>
 static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, const int4* ov_items, int n_ohu,
                          const int4* ohu_items, int64_t n_params_total, const uint32_t* bits, const T* tt,
                          const float2* eloc, const qes_sr_options* opt, typename VecT<T>::type* x,
                          qes_sr_result* res, const BatchSRWork& L, cudaStream_t st) {
   using V = typename VecT<T>::type;
+  constexpr bool CPLX = ScalarTraits<T>::is_complex;
   T* partial = (T*)L.partial;
   V* r = (V*)L.r; V* p = (V*)L.p; V* Ap = (V*)L.Ap; V* b = (V*)L.b;
-  const dim3 ohu_block_dim(OHU_TM, OHU_TY);
-  const size_t ov_smem = (size_t)OV_SB * 64 * sizeof(uint32_t);
+  // the shapes pick the kernel variants: read the descriptors once
+  std::vector<qes_batch_instance> hi(n_inst);
+  QES_CUDA_CHECK(cudaMemcpyAsync(hi.data(), inst, n_inst * sizeof(qes_batch_instance), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaStreamSynchronize(st));
+  int max_nh = 1, max_kg = 4;
+  size_t ov_smem = 0, ohu_smem = 0;
+  for (const auto& d : hi) {
+    if (d.ns <= 0 || d.nh <= 0 || d.nh > BOHU_THREADS || d.ns >= BOHU_THREADS ||
+        (int64_t)d.ns * d.nh > (CPLX ? 8192 : 16384)) {
+      qes_set_last_message("qes_batch_sr_solve_cg: a problem exceeds ns*nh <= 16384 (real) / 8192 (complex), "
+                           "nh <= 512");
+      return QES_ERR_SIZE;
+    }
+    max_nh = std::max(max_nh, d.nh);
+    max_kg = std::max(max_kg, batch_ohu_kg(d.ns, d.nh));
+    ov_smem = std::max(ov_smem, batch_ov_smem<T>(d.ns, d.nh));
+    ohu_smem = std::max(ohu_smem, batch_ohu_smem<T>(d.ns, d.nh));
+  }
+  const int mpl = (max_nh + 31) / 32;
+  auto ov = [&](const V* vec) -> int {
+#define QES_BOV(M) if (mpl <= M) return launch_batch_ov<T, V, M>(n_ov, ov_smem, inst, ov_items, bits, tt, vec, L.w, L.bscal, st);
+    QES_BOV(1) QES_BOV(2) QES_BOV(4) QES_BOV(8) QES_BOV(16)
+#undef QES_BOV
+    qes_set_last_message("qes_batch_sr_solve_cg: nh too large");
+    return QES_ERR_SIZE;
+  };
+  auto ohu = [&](const float2* g, int skip) -> int {
+#define QES_BOHU(K) if (max_kg <= K) return launch_batch_ohu<T, K>(n_ohu, ohu_smem, inst, ohu_items, bits, tt, g, L.bscal, skip, partial, st);
+    QES_BOHU(4) QES_BOHU(8) QES_BOHU(16) QES_BOHU(24) QES_BOHU(32) QES_BOHU(48) QES_BOHU(64)
+#undef QES_BOHU
+    qes_set_last_message("qes_batch_sr_solve_cg: too many sites per thread group");
+    return QES_ERR_SIZE;
+  };
+  int rc;
   QES_CUDA_CHECK(cudaMemsetAsync(L.n_done, 0, sizeof(unsigned int), st));
   // force: mean of E_loc, O^H (E - mean) / rows, then CG set-up
   batch_mean_kernel<<<n_inst, BCG_THREADS, 0, st>>>(inst, eloc, L.bscal, 9, 0);
-  batch_ohu_kernel<T><<<n_ohu, ohu_block_dim, 0, st>>>(inst, ohu_items, bits, tt, eloc, L.bscal, 9, 0, partial);
+  if ((rc = ohu(eloc, 0))) return rc;
   batch_cg_setup_kernel<T, V><<<n_inst, BCG_THREADS, 0, st>>>(inst, partial, opt->rtol, opt->atol, x, r, p, b,
                                                               L.bscal, L.n_done);
   QES_LAUNCH_CHECK_N(3);
@@ -1093,9 +1323,9 @@ static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, c
   while ((int)done < n_inst && it < opt->maxiter) {
     const int nrun = std::min(check, opt->maxiter - it);
     for (int q = 0; q < nrun; ++q) {
-      batch_ov_kernel<T, V><<<n_ov, OV_THREADS, ov_smem, st>>>(inst, ov_items, bits, tt, p, L.w, L.bscal);
+      if ((rc = ov(p))) return rc;
       batch_mean_kernel<<<n_inst, BCG_THREADS, 0, st>>>(inst, L.w, L.bscal, 9, 1);
-      batch_ohu_kernel<T><<<n_ohu, ohu_block_dim, 0, st>>>(inst, ohu_items, bits, tt, L.w, L.bscal, 9, 1, partial);
+      if ((rc = ohu(L.w, 1))) return rc;
       batch_cg_update_kernel<T, V><<<n_inst, BCG_THREADS, 0, st>>>(inst, partial, opt->shift, x, r, p, Ap, L.bscal,
                                                                    L.n_done);
       QES_LAUNCH_CHECK_N(4);

@@ -46,6 +46,11 @@ CONFIGS = {
     "j1j2_6x6": dict(name="j1j2_6x6", dim=2, lx=6, ly=6, model="j1j2", kw=dict(J1=-1.0, J2=-0.5), alpha=4, dtype="complex64",
                      chains=2048, samples=4, rule="EXCHANGE", sweep=36, shift=1e-3, lr=0.01, rtol=1e-8,
                      maxiter=1000, init="RND_FIXED"),
+    # 64 independent TFIM chains, L ~ U{12..64}, hx ~ U[0.5, 1.5], J = 1, PBC; real RBM alpha = 2 each;
+    # 256 chains x 8 samples per problem; single flips; one launch per phase over all problems
+    "tfim_batch64": dict(name="tfim_batch64", batch=True, n_inst=64, L_lo=12, L_hi=64, hx_lo=0.5, hx_hi=1.5,
+                         draw_seed=2024, alpha=2, dtype="float32", chains=256, samples=8, rule="LOCAL",
+                         shift=1e-3, lr=0.02, rtol=1e-8, maxiter=1000, model="tfim", kw=dict(j=1.0)),
     "tfim20x20": dict(name="tfim20x20", dim=2, lx=20, ly=20, model="tfim", kw=dict(j=1.0, hx=3.04, hz=0.0), alpha=4, dtype="float32",
                       chains=4096, samples=4, rule="LOCAL", sweep=400, shift=1e-4, lr=0.01, rtol=1e-8, maxiter=1000,
                       init="RND"),
@@ -173,6 +178,202 @@ def timed_loop(nqs, tdvp, cfg, steps, flush, profile=False):
     return step_ms, phase_ms, cg_iters, launches, prof
 
 
+def accuracy_check(epochs, name="tfim16"):
+    """Equal-Delta-E evidence: train the ED-checkable workload in both forms from the same start and
+    compare the final energies with the exact ground energy (GPU Lanczos, ``qes_ed_lanczos``)."""
+    import torch
+    from pyqusolver_b200 import _lib
+    cfg = CONFIGS[name]
+    out = {"workload": name, "epochs": int(epochs), "lr": cfg["lr"], "shift": cfg["shift"],
+           "exact_method": "GPU Lanczos over the full 2^N basis (qes_ed_lanczos)"}
+    e_exact = None
+    for form, impl in (("plain_fp32", _lib.SR_IMPL_CUDA_CORES), ("mixed", _lib.SR_IMPL_AUTO)):
+        _lib.set_sr_impl(impl)
+        nqs, tdvp = build_nqs(cfg, seed=1)
+        if e_exact is None:
+            e_exact = float(nqs.model.diagonalize(method="lanczos")[0])
+        hist = []
+        t0 = time.perf_counter()
+        for _ in range(int(epochs)):
+            info = nqs.train_step(lr=cfg["lr"], tdvp=tdvp)
+            hist.append(info["mean"].real)
+        torch.cuda.synchronize()
+        tail = np.array(hist[-30:])
+        e = float(tail.mean())
+        out[form] = {"energy": e, "stderr": float(tail.std() / np.sqrt(len(tail))),
+                     "rel_err": abs(e - e_exact) / abs(e_exact), "seconds": time.perf_counter() - t0}
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+    out["e_exact"] = e_exact
+    out["equal_dE_1e-4"] = bool(out["mixed"]["rel_err"] <= 1e-4 and out["plain_fp32"]["rel_err"] <= 1e-4)
+    return out
+
+
+def build_batch(cfg, seed):
+    import pyqusolver_b200 as qb
+    from pyqusolver_b200.batch import NQSBatch
+    rng = np.random.default_rng(cfg["draw_seed"])
+    Ls = rng.integers(cfg["L_lo"], cfg["L_hi"] + 1, size=cfg["n_inst"])
+    hx = rng.uniform(cfg["hx_lo"], cfg["hx_hi"], size=cfg["n_inst"])
+    models = [qb.TransverseFieldIsing(qb.SquareLattice(1, int(L), 1, bc="pbc"), j=1.0, hx=float(h), hz=0.0)
+              for L, h in zip(Ls, hx)]
+    B = NQSBatch(models, alpha=cfg["alpha"], dtype=cfg["dtype"], seeds=[seed * 1000 + b for b in range(len(models))],
+                 s_numchains=cfg["chains"], s_numsamples=cfg["samples"], autotune=True)
+    return B, Ls, hx
+
+
+BATCH_PHASES = ["sample", "forward", "local_energy", "stats", "sr_solve", "update"]
+
+
+def run_batch(args, cfg, rank, world, local_rank):
+    """Batched uneven problems (one launch per phase over all problems); one form (float32 CUDA cores)."""
+    import torch
+    from pyqusolver_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    B, Ls, hx = build_batch(cfg, seed=1 + rank)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    kw = dict(shift=cfg["shift"], rtol=cfg["rtol"], maxiter=cfg["maxiter"], check_every=32)
+
+    def step(ev):
+        ev[0].record(); B.sample()
+        ev[1].record(); B.forward()
+        ev[2].record(); B.local_energy()
+        ev[3].record(); st = B.loss_stats()
+        ev[4].record(); _, res = B.sr_solve(**kw)
+        ev[5].record(); B.update(cfg["lr"])
+        ev[6].record()
+        return st, res
+
+    mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+    for _ in range(args.warmup):
+        step(mk())
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    _lib.profile_read(reset=True)
+    _lib.profile_enable(True)
+    _lib.launch_count(reset=True)
+    step_ms, phase_ms, cg = [], {p: [] for p in BATCH_PHASES}, []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        ev = mk()
+        st, res = step(ev)
+        torch.cuda.synchronize()
+        step_ms.append(ev[0].elapsed_time(ev[6]))
+        for k, p in enumerate(BATCH_PHASES):
+            phase_ms[p].append(ev[k].elapsed_time(ev[k + 1]))
+        cg.append(max(r.iterations for r in res))
+    launches = _lib.launch_count(reset=True)
+    prof = _lib.profile_read(reset=True)
+    _lib.profile_enable(False)
+    clk = clocks.stop()
+    total = float(np.sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    n_step = B.n_samples_total
+    value = world * n_step * args.steps / (total / 1e3)
+    ms = total / args.steps
+
+    # end to end: parameters in from pinned host memory, statistics and parameters back
+    host_in = torch.empty_like(B.master, device="cpu").pin_memory()
+    host_in.copy_(B.master.cpu())
+    host_out = torch.empty_like(host_in).pin_memory()
+    times = []
+    for _ in range(args.steps):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        B.master.copy_(host_in, non_blocking=True)
+        B.flat.copy_(B.master)
+        B._tables_dirty = True
+        B.train_step(lr=cfg["lr"], diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"])
+        host_out.copy_(B.master, non_blocking=True)
+        s1.record()
+        torch.cuda.synchronize()
+        times.append(s0.elapsed_time(s1))
+    e2e_total = float(np.sum(times))
+    nb = host_in.numel() * host_in.element_size()
+    e2e = {"value": world * n_step * args.steps / (e2e_total / 1e3), "unit": "samples/s",
+           "h2d_bytes_per_step": int(nb), "d2h_bytes_per_step": int(nb + 32 * B.n_inst),
+           "ms_per_step": e2e_total / args.steps}
+
+    # roofline: dominant profiled kernel class (batched ov / ohu / CG update) or phase
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    rows, ns, nh, P = B.rows, B.ns, B.nh, B.P
+    nw = (ns + 31) // 32
+    nsplit = (rows + 255) // 256
+    algo = {"ov": int((rows * nh * 4 + rows * nw * 4 + P * 8 + rows * 8).sum()),
+            "ohu": int((rows * nh * 4 + rows * nw * 4 + rows * 8 + nsplit * P * 4).sum()),
+            "reduce": int((nsplit * P * 4 + 5 * P * 8).sum())}
+    names = {"ov": "batch_ov_small_kernel", "ohu": "batch_ohu_small_kernel", "reduce": "batch_cg_update_kernel"}
+    cands = {k: v for k, v in prof.items() if v[1]}
+    dom = max(cands, key=lambda k: cands[k][0])
+    avg_s = cands[dom][0] / cands[dom][1] / 1e3
+    ach = algo[dom] / avg_s / 1e9
+    roof = {"kernel": names[dom], "launches_timed": cands[dom][1], "avg_launch_us": avg_s * 1e6,
+            "share_of_timed_region": cands[dom][0] / total, "bound": "hbm", "achieved": ach, "peak": hbm,
+            "unit": "GB/s", "frac": ach / hbm, "algorithmic_bytes_per_launch": algo[dom],
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "traffic": json.load(open(os.path.join(ROOT, "profiles", "dram_traffic_per_launch.json"))).get(
+                cfg["name"], {}).get(dom) if os.path.exists(os.path.join(ROOT, "profiles",
+                                                                          "dram_traffic_per_launch.json")) else None}
+    line = {
+        "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "vmc_steps_per_s": 1e3 / ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (random-init RBMs, random chains)",
+        "config": {"workload": args.config, "problems": int(B.n_inst), "L_range": [int(Ls.min()), int(Ls.max())],
+                   "hx_range": [float(hx.min()), float(hx.max())], "alpha": cfg["alpha"],
+                   "chains_per_problem": cfg["chains"], "samples_per_chain": cfg["samples"],
+                   "samples_per_step": int(n_step), "n_params_total": int(B.n_params_total),
+                   "sampler_warps_per_block": B.warps_per_block, "sampler_blocks_per_sm": B.blocks_per_sm,
+                   "sr": f"per-problem structured CG fp64 in lockstep, shift {cfg['shift']}, rtol {cfg['rtol']}",
+                   "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "phase_ms": {p: float(np.mean(v)) for p, v in phase_ms.items()},
+        "cg_iterations_max_mean": float(np.mean(cg)),
+        "gpu_launches": int(launches), "clocks": clk, "e2e": e2e, "roofline": roof,
+    }
+    if rank == 0 and args.accuracy_epochs > 0:
+        line["accuracy"] = batch_accuracy(B, cfg, args.accuracy_epochs, Ls)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def batch_accuracy(B, cfg, epochs, Ls):
+    """Train every problem for `epochs` more epochs; energy error per problem against the GPU Lanczos
+    ground energy for L <= 20."""
+    hist = []
+    for _ in range(int(epochs)):
+        info = B.train_step(lr=cfg["lr"], diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"])
+        hist.append(info["mean"].real)
+    tail = np.array(hist[-20:]).mean(axis=0)
+    rows = []
+    for b, m in enumerate(B.models):
+        if m.ns <= 20:
+            e0 = float(m.diagonalize(method="lanczos")[0])
+            rows.append({"problem": b, "L": int(m.ns), "e_exact": e0, "energy": float(tail[b]),
+                         "rel_err": abs(float(tail[b]) - e0) / abs(e0)})
+    return {"epochs": int(epochs), "checked_problems": len(rows),
+            "max_rel_err": max((r["rel_err"] for r in rows), default=None), "problems": rows}
+
+
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     from pyqusolver_b200 import _lib
@@ -259,6 +460,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         "e2e": e2e,
         "roofline": roof,
     }
+    if rank == 0 and args.accuracy_epochs > 0:
+        line["accuracy"] = accuracy_check(args.accuracy_epochs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
     if dist is not None:
@@ -407,8 +610,34 @@ def cpu_step(cfg, p, terms, smp):
                          maxiter=cfg["maxiter"])
 
 
+def batch_problem_cfgs(cfg):
+    """Per-problem single-workload configs of a batched workload (same draws as build_batch)."""
+    rng = np.random.default_rng(cfg["draw_seed"])
+    Ls = rng.integers(cfg["L_lo"], cfg["L_hi"] + 1, size=cfg["n_inst"])
+    hx = rng.uniform(cfg["hx_lo"], cfg["hx_hi"], size=cfg["n_inst"])
+    return [dict(name=f"{cfg['name']}[{b}]", dim=1, lx=int(L), ly=1, model="tfim", kw=dict(j=1.0, hx=float(h), hz=0.0),
+                 alpha=cfg["alpha"], dtype=cfg["dtype"], chains=cfg["chains"], samples=cfg["samples"], rule="LOCAL",
+                 sweep=int(L), shift=cfg["shift"], lr=cfg["lr"], rtol=cfg["rtol"], maxiter=cfg["maxiter"], init="RND")
+            for b, (L, h) in enumerate(zip(Ls, hx))]
+
+
 def cpu_baseline(cfg, budget_s=20.0):
     """The oracle (float64 NumPy restatement of the reference's algorithm) on the host cores."""
+    if cfg.get("batch"):
+        # bounded sample: one VMC step of 16 chains on successive problems until the budget is used
+        t0 = time.perf_counter()
+        samples, done = 0, 0
+        for pc in batch_problem_cfgs(cfg):
+            p, terms, smp = oracle_setup(pc, 16)
+            cpu_step(pc, p, terms, smp)
+            samples += 16 * pc["samples"]
+            done += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        dt = time.perf_counter() - t0
+        return {"value": samples / dt, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
+                "sample": f"one VMC step of 16 chains x {cfg['samples']} samples on each of the first {done} "
+                          f"problems (float64 NumPy oracle, problems one after another)"}
     n_chains = 16
     p, terms, smp = oracle_setup(cfg, n_chains)
     t0 = time.perf_counter()
@@ -428,6 +657,21 @@ def cpu_baseline(cfg, budget_s=20.0):
 
 def run_reference(args, cfg, rank, world):
     if rank != 0:
+        return
+    if cfg.get("batch"):
+        cb = None
+        t_all = []
+        for _ in range(args.warmup + args.steps):
+            cb = cpu_baseline(cfg, budget_s=min(args.cpu_budget, 10.0))
+            t_all.append(cb["value"])
+        v = float(np.mean(t_all[args.warmup:]))
+        cb["value"] = v
+        line = {"metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "config": {"workload": args.config}, "impl": "reference",
+                "cpu_baseline": cb,
+                "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
         return
     n_chains = 16
     p, terms, smp = oracle_setup(cfg, n_chains)
@@ -462,12 +706,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="plain_fp32,mixed", help="comma list of plain_fp32, mixed (mixed is required)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--accuracy-epochs", type=int, default=300,
+                    help="epochs of the ED-checked mixed vs plain comparison on tfim16 (0 = skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local_rank = env_rank()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":
         run_reference(args, cfg, rank, world)
+    elif cfg.get("batch"):
+        run_batch(args, cfg, rank, world, local_rank)
     else:
         run_ours(args, cfg, rank, world, local_rank)
 

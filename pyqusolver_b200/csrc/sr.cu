@@ -1250,7 +1250,9 @@ static int launch_batch_ov(int n_ov, size_t smem, const qes_batch_instance* inst
                            cudaStream_t st) {
   QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ov_small_kernel<T, V, MPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
+  const int pf = qes_prof_begin(QES_PROF_OV, st);
   batch_ov_small_kernel<T, V, MPL><<<n_ov, BOV_THREADS, smem, st>>>(inst, items, bits, tt, p, w, bscal);
+  qes_prof_end(pf, st);
   return QES_OK;
 }
 
@@ -1260,8 +1262,10 @@ static int launch_batch_ohu(int n_ohu, size_t smem, const qes_batch_instance* in
                             T* partial, cudaStream_t st) {
   QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ohu_small_kernel<T, KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
+  const int pf = qes_prof_begin(QES_PROF_OHU, st);
   batch_ohu_small_kernel<T, KMAX><<<n_ohu, BOHU_THREADS, smem, st>>>(inst, items, bits, tt, w, bscal, 9, skip_done,
                                                                      partial);
+  qes_prof_end(pf, st);
   return QES_OK;
 }
 
@@ -1326,8 +1330,10 @@ static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, c
       if ((rc = ov(p))) return rc;
       batch_mean_kernel<<<n_inst, BCG_THREADS, 0, st>>>(inst, L.w, L.bscal, 9, 1);
       if ((rc = ohu(L.w, 1))) return rc;
+      const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
       batch_cg_update_kernel<T, V><<<n_inst, BCG_THREADS, 0, st>>>(inst, partial, opt->shift, x, r, p, Ap, L.bscal,
                                                                    L.n_done);
+      qes_prof_end(pfr, st);
       QES_LAUNCH_CHECK_N(4);
     }
     it += nrun;

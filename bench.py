@@ -511,7 +511,9 @@ def run_e2e(nqs, cfg, args, dist, world):
 
 
 def kernel_bytes(cfg, nqs, kind, tc):
-    """Algorithmic bytes of one launch: every operand read once plus every output written once."""
+    """Algorithmic bytes of one launch: every operand read once plus every output written once.
+    Tensor-core operands are counted in the BF16 tile form the kernels stream (plan from the library)."""
+    from pyqusolver_b200 import _lib, device as dv
     net = nqs.net
     ns, nh, n = net.ns, net.nh, cfg["chains"] * cfg["samples"]
     cplx = net.is_complex
@@ -519,20 +521,15 @@ def kernel_bytes(cfg, nqs, kind, tc):
     nw = (ns + 31) // 32
     P = ns + nh + ns * nh
     if tc:
-        Mp = (nh + 15) // 16 * 16
-        Np = 2 * Mp if cplx else Mp
-        Kd = 2 * Mp if cplx else (nh + 31) // 32 * 32
-        Sp = (ns + 1 + 7) // 8 * 8 if cplx else (ns + 1 + 15) // 16 * 16
-        NB = 2 * Sp if cplx else Sp
-        kc = 256
-        while kc >= 16 and 128 * kc * 2 + 2 * Np * kc * 2 + (kc + nh) * ts + 64 > 220 * 1024:
-            kc -= 16
-        n_tiles, n_chunks = (n + 127) // 128, (n + kc - 1) // kc
+        pl = _lib.sr_tc_plan(dv.dtype_code(net.flat), ns, nh, n)
+        kc, nch, nsp = pl["KC"], pl["n_chunks"], pl["nsplit"]
         if kind == "ov":
-            return n_tiles * 128 * Kd * 4 + NB * Kd * 4 + n * nw * 4 + n * 8
+            return pl["n_tiles"] * 128 * pl["Kd"] * 4 + pl["NB"] * pl["Kd"] * 4 + n * nw * 4 + n * 8
         if kind == "ohu":
-            return n_chunks * 128 * kc * 2 + n_chunks * Np * kc * 4 + n * 8 + n_chunks * P * ts
-        return n_chunks * P * ts + 2 * P * vs
+            if pl["big"]:
+                return nch * (pl["MT"] * 128 * kc * 2 + pl["nnc"] * pl["NR"] * kc * 4) + n * 8 + nsp * P * ts
+            return nch * 128 * kc * 2 + nch * pl["Np"] * kc * 4 + n * 8 + nsp * P * ts
+        return nsp * P * ts + 2 * P * vs
     nsplit = (n + 255) // 256
     if kind == "ov":
         return n * nh * ts + n * nw * 4 + P * vs + n * 8
@@ -565,14 +562,18 @@ def roofline(cfg, nqs, form):
     dom = max(cands, key=lambda k: cands[k][0])
     total_ms, cnt = cands[dom]
     avg_s = total_ms / cnt / 1e3
-    names = {"ov": "tc_ov_kernel (O v, tcgen05)", "ohu": "tc_ohu_kernel (O^H u, tcgen05)",
+    from pyqusolver_b200 import _lib, device as dv
+    net = nqs.net
+    tc = _lib.sr_uses_tensor_cores(dv.dtype_code(net.flat), net.ns, net.nh, cfg["chains"] * cfg["samples"])
+    names = {"ov": "tc_ov_kernel (O v, tcgen05)" if tc else "ov_kernel (O v, CUDA cores)",
+             "ohu": "tc_ohu_kernel (O^H u, tcgen05)" if tc else "ohu_kernel (O^H u, CUDA cores)",
              "reduce": "reduce_splits_kernel", "sample": "sampler_kernel", "local_energy": "eloc_moves_kernel",
              "forward": "rbm_forward_kernel"}
     out = {"kernel": names.get(dom, dom), "launches_timed": cnt, "avg_launch_us": avg_s * 1e6,
            "share_of_timed_region": total_ms / float(np.sum([np.sum(v) for v in form["phase_ms"].values()])),
            "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src}
     if dom in ("ov", "ohu", "reduce"):
-        b = kernel_bytes(cfg, nqs, dom, tc=True)
+        b = kernel_bytes(cfg, nqs, dom, tc=tc)
         ach = b / avg_s / 1e9
         tr = traffic_db.get(cfg.get("name", ""), {}).get(dom)
         out.update({"achieved": ach, "frac": ach / hbm, "algorithmic_bytes_per_launch": b, "traffic": tr})

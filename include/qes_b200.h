@@ -244,6 +244,13 @@ int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t*
  * (its SR runs on XLA).  qes_sr_force / qes_sr_matvec synchronise the stream
  * when the tensor-core path ran, to report bounded-wait time-outs.          */
 int qes_set_sr_impl(int impl);
+/* *uses = 1 when the SR calls for these shapes run on the tensor cores under
+ * the current qes_set_sr_impl setting, else 0.                             */
+int qes_sr_uses_tensor_cores(int dtype, int ns, int nh, int64_t n_samples, int* uses);
+/* Tiling of the tensor-core path for these shapes (for roofline accounting):
+ * out = [uses, big, KC, n_chunks, nsplit, n_tiles, Kd, NB, Np, MT, NC, NR,
+ * nnc, SPC, ov_stages] (first n_out entries).                              */
+int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int32_t* out, int n_out);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);

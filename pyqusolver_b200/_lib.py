@@ -106,6 +106,8 @@ SIGNATURES = {
     "qes_rbm_log_derivatives": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _i64, _vp],
     "qes_sr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
     "qes_set_sr_impl": [C.c_int],
+    "qes_sr_uses_tensor_cores": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(C.c_int)],
+    "qes_sr_tc_plan": [C.c_int, C.c_int, C.c_int, _i64, _vp, C.c_int],
     "qes_set_cg_graphs": [C.c_int],
     "qes_profile_enable": [C.c_int],
     "qes_profile_read": [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int],
@@ -170,6 +172,23 @@ SR_IMPL_AUTO, SR_IMPL_CUDA_CORES, SR_IMPL_TENSOR_CORES = 0, 1, 2
 
 def set_sr_impl(impl: int):
     call("qes_set_sr_impl", int(impl))
+
+
+TC_PLAN_FIELDS = ("uses", "big", "KC", "n_chunks", "nsplit", "n_tiles", "Kd", "NB", "Np", "MT", "NC", "NR", "nnc",
+                  "SPC", "ov_stages")
+
+
+def sr_tc_plan(dtype_code: int, ns: int, nh: int, n_samples: int) -> dict:
+    buf = (C.c_int32 * len(TC_PLAN_FIELDS))()
+    call("qes_sr_tc_plan", int(dtype_code), int(ns), int(nh), int(n_samples), C.cast(buf, C.c_void_p),
+         len(TC_PLAN_FIELDS))
+    return {k: int(buf[i]) for i, k in enumerate(TC_PLAN_FIELDS)}
+
+
+def sr_uses_tensor_cores(dtype_code: int, ns: int, nh: int, n_samples: int) -> bool:
+    u = C.c_int(0)
+    call("qes_sr_uses_tensor_cores", int(dtype_code), int(ns), int(nh), int(n_samples), C.byref(u))
+    return bool(u.value)
 
 
 PROFILE_CLASSES = ("ov", "ohu", "reduce")

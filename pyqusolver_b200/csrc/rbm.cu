@@ -21,16 +21,33 @@ extern "C" const char* qes_last_error(void) { return g_last_error; }
 
 // ---------------------------------------------------------------- per-kernel event timing
 #include <mutex>
+#include <vector>
 namespace {
-constexpr int kProfSlots = 8192;
+// Event pairs are created on demand in blocks and kept for reuse; between two reads at most
+// kProfMaxSlots launches are recorded (later ones are skipped, never blocked on).
+constexpr int kProfBlock = 4096;
+constexpr int kProfMaxSlots = 1 << 20;
 std::mutex g_prof_mu;
 std::atomic<int> g_prof_enabled{0};
-cudaEvent_t g_prof_ev[kProfSlots][2];
-int g_prof_cls[kProfSlots];
+std::vector<cudaEvent_t> g_prof_ev;   // 2 per slot
+std::vector<int> g_prof_cls;
 int g_prof_used = 0;
-bool g_prof_created = false;
 double g_prof_ms[QES_PROF_CLASSES];
 long long g_prof_cnt[QES_PROF_CLASSES];
+
+bool prof_grow() {
+  const size_t have = g_prof_cls.size();
+  if ((int)have >= kProfMaxSlots) return false;
+  for (int q = 0; q < kProfBlock; ++q) {
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess) return false;
+    if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return false; }
+    g_prof_ev.push_back(a);
+    g_prof_ev.push_back(b);
+    g_prof_cls.push_back(0);
+  }
+  return true;
+}
 }  // namespace
 
 bool qes_prof_on() { return g_prof_enabled.load(std::memory_order_relaxed) != 0; }
@@ -38,23 +55,24 @@ bool qes_prof_on() { return g_prof_enabled.load(std::memory_order_relaxed) != 0;
 int qes_prof_begin(int cls, cudaStream_t st) {
   if (!qes_prof_on()) return -1;
   std::lock_guard<std::mutex> lock(g_prof_mu);
-  if (!g_prof_created || g_prof_used >= kProfSlots) return -1;
+  if (g_prof_used >= (int)g_prof_cls.size() && !prof_grow()) return -1;
   const int slot = g_prof_used++;
   g_prof_cls[slot] = cls;
-  if (cudaEventRecord(g_prof_ev[slot][0], st) != cudaSuccess) return -1;
+  if (cudaEventRecord(g_prof_ev[2 * slot], st) != cudaSuccess) return -1;
   return slot;
 }
 
 void qes_prof_end(int slot, cudaStream_t st) {
   if (slot < 0) return;
-  cudaEventRecord(g_prof_ev[slot][1], st);
+  std::lock_guard<std::mutex> lock(g_prof_mu);
+  cudaEventRecord(g_prof_ev[2 * slot + 1], st);
 }
 
 // folds the recorded pairs into the totals (the caller has synchronised)
 static void prof_collect() {
   for (int q = 0; q < g_prof_used; ++q) {
     float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, g_prof_ev[q][0], g_prof_ev[q][1]) == cudaSuccess) {
+    if (cudaEventElapsedTime(&ms, g_prof_ev[2 * q], g_prof_ev[2 * q + 1]) == cudaSuccess) {
       g_prof_ms[g_prof_cls[q]] += ms;
       g_prof_cnt[g_prof_cls[q]] += 1;
     }
@@ -64,12 +82,9 @@ static void prof_collect() {
 
 extern "C" int qes_profile_enable(int enable) {
   std::lock_guard<std::mutex> lock(g_prof_mu);
-  if (enable && !g_prof_created) {
-    for (int q = 0; q < kProfSlots; ++q) {
-      QES_CUDA_CHECK(cudaEventCreate(&g_prof_ev[q][0]));
-      QES_CUDA_CHECK(cudaEventCreate(&g_prof_ev[q][1]));
-    }
-    g_prof_created = true;
+  if (enable && g_prof_cls.empty() && !prof_grow()) {
+    qes_set_last_message("qes_profile_enable: cannot create CUDA events");
+    return QES_ERR_CUDA;
   }
   g_prof_enabled.store(enable ? 1 : 0);
   return QES_OK;

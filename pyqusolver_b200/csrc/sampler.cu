@@ -35,7 +35,7 @@ QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __
     const int m = lane + 32 * r;
     th[r] = (m < nh) ? b[m] : ScalarTraits<T>::zero();
   }
-  for (int i = 0; i < ns; ++i) {
+  auto site = [&](int i) {
     const float sg = ((cfg[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
     const T* wr = W + (int64_t)i * nh;
 #pragma unroll
@@ -43,6 +43,12 @@ QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __
       const int m = lane + 32 * r;
       if (m < nh) th[r] = addx(th[r], scal(sg, wr[m]));
     }
+  };
+  if constexpr (MPL >= 16) {
+#pragma unroll 4
+    for (int i = 0; i < ns; ++i) site(i);
+  } else {
+    for (int i = 0; i < ns; ++i) site(i);
   }
 #pragma unroll
   for (int r = 0; r < MPL; ++r) tn[r] = tanhx(th[r]);
@@ -138,11 +144,42 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
       g = ((cw[i0 >> 5] >> (i0 & 31)) & 1u) ? -1.f : 1.f;      // -sigma_i0
       T prod = ScalarTraits<T>::one();
       int ex = 0;
+      if constexpr (MPL >= 16) {
+        // the table row is fetched a chunk ahead of the product so that its L2 round trips overlap;
+        // units beyond nh read as (C, S) = (1, 0), an exact factor of one
+        constexpr int PF = 16;
+        T cb[2][PF], sb[2][PF];
 #pragma unroll
-      for (int rr = 0; rr < MPL; ++rr) {
-        const int m = lane + 32 * rr;
-        if (m < nh) prod = mulx(prod, ratio_factor(Crow[m], g, tn[rr], Srow[m]));
-        if ((rr & 7) == 7) renorm(prod, ex);
+        for (int q = 0; q < PF; ++q) {
+          const int m = lane + 32 * q;
+          cb[0][q] = (m < nh) ? Crow[m] : ScalarTraits<T>::one();
+          sb[0][q] = (m < nh) ? Srow[m] : ScalarTraits<T>::zero();
+        }
+#pragma unroll
+        for (int c0 = 0; c0 < MPL; c0 += PF) {
+          const int cur = (c0 / PF) & 1;
+          if (c0 + PF < MPL) {
+#pragma unroll
+            for (int q = 0; q < PF; ++q) {
+              const int m = lane + 32 * (c0 + PF + q);
+              cb[cur ^ 1][q] = (m < nh) ? Crow[m] : ScalarTraits<T>::one();
+              sb[cur ^ 1][q] = (m < nh) ? Srow[m] : ScalarTraits<T>::zero();
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < PF; ++q) {
+            const int rr = c0 + q;
+            prod = mulx(prod, ratio_factor(cb[cur][q], g, tn[rr], sb[cur][q]));
+            if ((rr & 7) == 7) renorm(prod, ex);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int rr = 0; rr < MPL; ++rr) {
+          const int m = lane + 32 * rr;
+          if (m < nh) prod = mulx(prod, ratio_factor(Crow[m], g, tn[rr], Srow[m]));
+          if ((rr & 7) == 7) renorm(prod, ex);
+        }
       }
       float la = log_abs<T>(prod) + 0.69314718055994531f * (float)ex;
       la = warp_sum(la);
@@ -155,14 +192,36 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
     if (keep && moved) {
       const T* wi = W + (int64_t)i0 * nh;
       const T* wj = W + (int64_t)(j0 >= 0 ? j0 : i0) * nh;
+      if constexpr (MPL >= 16) {
+        constexpr int PU = 16;
 #pragma unroll
-      for (int rr = 0; rr < MPL; ++rr) {
-        const int m = lane + 32 * rr;
-        if (m < nh) {
-          T d = wi[m];
-          if (j0 >= 0) d = addx(d, scal(-1.f, wj[m]));
-          th[rr] = addx(th[rr], scal(2.f * g, d));
-          tn[rr] = tanhx(th[rr]);
+        for (int c0 = 0; c0 < MPL; c0 += PU) {
+          T d[PU];
+#pragma unroll
+          for (int q = 0; q < PU; ++q) {          // all loads of the chunk first
+            const int m = lane + 32 * (c0 + q);
+            d[q] = (m < nh) ? wi[m] : ScalarTraits<T>::zero();
+            if (j0 >= 0) d[q] = addx(d[q], scal(-1.f, (m < nh) ? wj[m] : ScalarTraits<T>::zero()));
+          }
+#pragma unroll
+          for (int q = 0; q < PU; ++q) {
+            const int rr = c0 + q;
+            if (lane + 32 * rr < nh) {
+              th[rr] = addx(th[rr], scal(2.f * g, d[q]));
+              tn[rr] = tanhx(th[rr]);
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int rr = 0; rr < MPL; ++rr) {
+          const int m = lane + 32 * rr;
+          if (m < nh) {
+            T d = wi[m];
+            if (j0 >= 0) d = addx(d, scal(-1.f, wj[m]));
+            th[rr] = addx(th[rr], scal(2.f * g, d));
+            tn[rr] = tanhx(th[rr]);
+          }
         }
       }
       __syncwarp();

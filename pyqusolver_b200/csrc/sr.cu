@@ -493,8 +493,8 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   const bool tc_ok = tc_plan(dtype, ns, nh, n_samples, &L.td);
   const int impl = g_sr_impl.load();
   L.tc = tc_ok && impl != 1;
-  const int64_t nsplit_max = std::max<int64_t>(nsplit_simt, tc_ok ? L.td.n_chunks : 1);
-  L.nsplit = (int)(L.tc ? L.td.n_chunks : nsplit_simt);
+  const int64_t nsplit_max = std::max<int64_t>(nsplit_simt, tc_ok ? L.td.nsplit : 1);
+  L.nsplit = (int)(L.tc ? L.td.nsplit : nsplit_simt);
   size_t off = 0;
   auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off += align256(bytes); return p; };
   L.w = (float2*)take((size_t)n_samples * sizeof(float2));
@@ -583,9 +583,27 @@ static int check_ws(int dtype, int ns, int nh, int64_t n_samples, void* ws, size
   }
   if (g_sr_impl.load() == 2 && !L->tc) {
     qes_set_last_message("SR: tensor-core path required but the shapes are outside its limits "
-                         "(ns <= 128, nh <= 256, shared-memory budget)");
+                         "(ns <= 127, nh <= 256, shared-memory budget)");
     return QES_ERR_SIZE;
   }
+  return QES_OK;
+}
+
+extern "C" int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int32_t* out, int n_out) {
+  QES_ARG_CHECK(out && n_out > 0 && ns > 0 && nh > 0 && n_samples > 0, "qes_sr_tc_plan: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_tc_plan: bad dtype");
+  const SRWork L = sr_layout(dtype, ns, nh, n_samples, nullptr);
+  const TcDims& d = L.td;
+  const int32_t f[15] = {L.tc ? 1 : 0, d.big ? 1 : 0, d.KC, d.n_chunks, d.nsplit, d.n_tiles, d.Kd, d.NB, d.Np,
+                         d.MT, d.NC, d.NR, d.nnc, d.SPC, d.ov_stages};
+  for (int k = 0; k < n_out; ++k) out[k] = k < 15 ? f[k] : 0;
+  return QES_OK;
+}
+
+extern "C" int qes_sr_uses_tensor_cores(int dtype, int ns, int nh, int64_t n_samples, int* uses) {
+  QES_ARG_CHECK(uses && ns > 0 && nh > 0 && n_samples > 0, "qes_sr_uses_tensor_cores: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_uses_tensor_cores: bad dtype");
+  *uses = sr_layout(dtype, ns, nh, n_samples, nullptr).tc ? 1 : 0;
   return QES_OK;
 }
 

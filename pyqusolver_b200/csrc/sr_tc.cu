@@ -35,7 +35,6 @@ constexpr uint32_t kWaitLimit = 1u << 22;     // try_wait polls before giving up
 constexpr int kThreads = 512;                  // 16 warps; warp w reads TMEM lane quarter w % 4
 constexpr int kWarps = kThreads / 32;
 constexpr int kColGroups = kWarps / 4;         // warps sharing one lane quarter split the columns
-constexpr int kStages = 4;                     // ov pipeline depth
 
 __device__ __forceinline__ uint16_t bf16_bits(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
 __device__ __forceinline__ float bf16_val(uint16_t b) { return __bfloat162float(__ushort_as_bfloat16(b)); }
@@ -206,7 +205,7 @@ __global__ void tc_build_vp_kernel(TcDims d, bool cplx, const V* __restrict__ v,
 }
 
 // ================================================================================================
-// ov: one CTA per 128-sample tile, K streamed through a kStages-deep pipeline
+// ov: one CTA per 128-sample tile, K streamed through a d.ov_stages-deep pipeline
 // ================================================================================================
 template <class T, class V>
 __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_samples, const uint32_t* __restrict__ bits,
@@ -219,9 +218,10 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   const int nK = d.Kd / KCH;
   const uint32_t a_term = 128u * KCH * 2u, b_term = (uint32_t)NB * KCH * 2u;
   const uint32_t stage_bytes = 2u * (a_term + b_term);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * stage_bytes);
-  uint64_t* empty = full + kStages;
-  uint64_t* done = empty + kStages;
+  const int S = d.ov_stages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * stage_bytes);
+  uint64_t* empty = full + S;
+  uint64_t* done = empty + S;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   T* s_va = reinterpret_cast<T*>(tslot + 4);
   __shared__ double2 red[4];
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tile = blockIdx.x;
   if (tid == 0) {
-    for (int q = 0; q < kStages; ++q) {
+    for (int q = 0; q < S; ++q) {
       umma::mbar_init(&full[q], 1);
       umma::mbar_init(&empty[q], 1);
     }
@@ -255,8 +255,8 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
     const uint8_t* ga = reinterpret_cast<const uint8_t*>(t_rows) + (size_t)tile * nK * 2 * a_term;
     const uint8_t* gb = reinterpret_cast<const uint8_t*>(vp);
     for (int c = 0; c < nK; ++c) {
-      const int s = c % kStages;
-      if (c >= kStages && !umma::mbar_wait(&empty[s], ((c / kStages) - 1) & 1, kWaitLimit)) {
+      const int s = c % S;
+      if (c >= S && !umma::mbar_wait(&empty[s], ((c / S) - 1) & 1, kWaitLimit)) {
         record_error(status, QES_ERR_TIMEOUT);
         break;
       }
@@ -266,11 +266,13 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
       umma::bulk_g2s(st + 2 * a_term, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[s]);
     }
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer: D (128 x NB) += A_hi B_hi + A_hi B_lo + A_lo B_hi over every 16-wide k-step
-    const uint32_t idesc = umma::idesc_bf16_f32(128, NB);
+    // MMA issuer: D (128 x NB) += A_hi B_hi + A_hi B_lo + A_lo B_hi over every 16-wide k-step;
+    // NB > 256 is issued as two N parts (rows [0, 256) and [256, NB) of V') into adjacent TMEM columns
+    const int n_parts = NB > 256 ? 2 : 1;
+    const uint32_t np0 = NB > 256 ? 256u : (uint32_t)NB;
     for (int c = 0; c < nK; ++c) {
-      const int s = c % kStages;
-      if (!umma::mbar_wait(&full[s], (c / kStages) & 1, kWaitLimit)) {
+      const int s = c % S;
+      if (!umma::mbar_wait(&full[s], (c / S) & 1, kWaitLimit)) {
         record_error(status, QES_ERR_TIMEOUT);
         break;
       }
@@ -281,11 +283,16 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
         const uint32_t ko_a = 2u * kk * 128u * 16u, ko_b = 2u * kk * NB * 16u;
         const uint64_t dah = umma::smem_desc(ahi + ko_a, 128u * 16u, 128u);
         const uint64_t dal = umma::smem_desc(alo + ko_a, 128u * 16u, 128u);
-        const uint64_t dbh = umma::smem_desc(bhi + ko_b, NB * 16u, 128u);
-        const uint64_t dbl = umma::smem_desc(blo + ko_b, NB * 16u, 128u);
-        umma::mma_bf16(tbase, dah, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
-        umma::mma_bf16(tbase, dah, dbl, idesc, 1u);
-        umma::mma_bf16(tbase, dal, dbh, idesc, 1u);
+        for (int pt = 0; pt < n_parts; ++pt) {
+          const uint32_t n0 = pt ? np0 : 0u, nn = pt ? (uint32_t)NB - np0 : np0;
+          const uint32_t idesc = umma::idesc_bf16_f32(128, nn);
+          const uint32_t rb = (n0 / 8u) * 128u;        // first 8-row group of this part
+          const uint64_t dbh = umma::smem_desc(bhi + ko_b + rb, NB * 16u, 128u);
+          const uint64_t dbl = umma::smem_desc(blo + ko_b + rb, NB * 16u, 128u);
+          umma::mma_bf16(tbase + n0, dah, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+          umma::mma_bf16(tbase + n0, dah, dbl, idesc, 1u);
+          umma::mma_bf16(tbase + n0, dal, dbh, idesc, 1u);
+        }
       }
       umma::mma_commit(&empty[s]);
     }
@@ -556,6 +563,300 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
 }
 
 // ================================================================================================
+// large problems: operands tiled in M (sites) and N (hidden units)
+// ================================================================================================
+// sig_cols (big): chunk c = MT*128 site rows x KC samples; rows >= ns are zero except row ns,
+// which is all ones (D row ns = sum_s Q_s = g_b)
+__global__ void tc_sigma_cols_big_kernel(int ns, int R, int KC, int64_t n_samples, int n_chunks,
+                                         const uint32_t* __restrict__ bits, uint16_t* __restrict__ out) {
+  const int nw = n_words(ns);
+  const int64_t items = (int64_t)n_chunks * R * (KC / 8);
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(it % R);
+    const int k8 = (int)((it / R) % (KC / 8));
+    const int64_t c = it / ((int64_t)(KC / 8) * R);
+    uint16_t v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int64_t s = c * KC + 8 * k8 + q;
+      v[q] = 0;
+      if (s < n_samples) {
+        if (r < ns) v[q] = ((bits[s * nw + (r >> 5)] >> (r & 31)) & 1u) ? 0x3F80u : 0xBF80u;
+        else if (r == ns) v[q] = 0x3F80u;
+      }
+    }
+    uint8_t* base = reinterpret_cast<uint8_t*>(out) + (size_t)c * R * KC * 2;
+    *reinterpret_cast<uint4*>(base + umma::kmajor_offset(r, 8 * k8, R)) = pack8(v);
+  }
+}
+
+// t_cols (big): tile (chunk c, N chunk q, term) = NR rows x KC samples; row n < NC is Re t of hidden
+// unit q*NC + n, row NC + n (complex) its Im t
+template <class T>
+__global__ void tc_t_cols_big_kernel(TcDims d, int64_t n_samples, const T* __restrict__ tt, uint16_t* __restrict__ out) {
+  constexpr bool CPLX = ScalarTraits<T>::is_complex;
+  const int nh = d.nh, NC = d.NC, NR = d.NR, KC = d.KC, nnc = d.nnc;
+  const size_t term_bytes = (size_t)NR * KC * 2;
+  const int64_t items = (int64_t)d.n_chunks * nnc * NR * (KC / 8);
+  for (int64_t it = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it < items; it += (int64_t)gridDim.x * blockDim.x) {
+    const int n = (int)(it % NR);
+    const int k8 = (int)((it / NR) % (KC / 8));
+    const int64_t cq = it / ((int64_t)(KC / 8) * NR);         // c * nnc + q
+    const int q = (int)(cq % nnc);
+    const int64_t c = cq / nnc;
+    const bool im = CPLX && n >= NC;
+    const int m = q * NC + (im ? n - NC : n);
+    uint16_t h[8], l[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int64_t s = c * KC + 8 * k8 + e;
+      float x = 0.f;
+      if (s < n_samples && m < nh) x = im ? tim(tt, s * nh + m) : tre(tt, s * nh + m);
+      split_bf16(x, h[e], l[e]);
+    }
+    uint8_t* base = reinterpret_cast<uint8_t*>(out) + (size_t)cq * 2 * term_bytes;
+    const uint32_t off = umma::kmajor_offset(n, 8 * k8, NR);
+    *reinterpret_cast<uint4*>(base + off) = pack8(h);
+    *reinterpret_cast<uint4*>(base + term_bytes + off) = pack8(l);
+  }
+}
+
+// O^H u for large problems.  Grid (N chunk, group of SPC sample chunks).  Each sample chunk is
+// bulk-copied (Sigma^T: MT*128 x KC, T^T tile: 2 terms x NR x KC) into one of two shared-memory
+// buffers while the tensor core works on the other; Q = conj(t) u is formed in place and MT x
+// terms x halves MMAs accumulate D[mt][h] (128 sites x NC units) in TMEM across the group.
+template <class T>
+__global__ void __launch_bounds__(kThreads) tc_ohu_big_kernel(TcDims d, int64_t n_samples, const float2* __restrict__ w,
+                                                              const double2* __restrict__ wsum_part, int wsum_n,
+                                                              double scale, const uint16_t* __restrict__ sig_cols,
+                                                              const uint16_t* __restrict__ t_cols,
+                                                              T* __restrict__ partial, int* __restrict__ status) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  constexpr bool CPLX = ScalarTraits<T>::is_complex;
+  constexpr int H = CPLX ? 2 : 1;
+  const int ns = d.ns, nh = d.nh, KC = d.KC, MT = d.MT, NC = d.NC, NR = d.NR, nnc = d.nnc;
+  const int R = MT * 128;
+  const uint32_t a_bytes = (uint32_t)R * KC * 2u, b_term = (uint32_t)NR * KC * 2u;
+  const uint32_t buf_bytes = a_bytes + 2u * b_term;
+  T* s_u = reinterpret_cast<T*>(smem + 2 * buf_bytes);                // [2][KC]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(s_u + 2 * KC) +
+                                               ((16 - (reinterpret_cast<uintptr_t>(s_u + 2 * KC) & 15)) & 15));
+  uint64_t* full = bars;          // [2]
+  uint64_t* mdone = bars + 2;     // [2]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 4);
+  __shared__ double2 s_mean;
+  __shared__ double2 s_red[kWarps];
+  __shared__ int s_fail;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int q = blockIdx.x;                                   // N chunk
+  const int g = blockIdx.y;                                   // group of sample chunks
+  const int c_first = g * d.SPC;
+  const int n_my = min(d.SPC, d.n_chunks - c_first);
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  const int n0 = q * NC;
+  if (tid == 0) {
+    for (int k = 0; k < 4; ++k) umma::mbar_init(&bars[k], 1);
+    umma::fence_mbar_init();
+    s_fail = 0;
+  }
+  {
+    double2 t = make_double2(0.0, 0.0);
+    if (wsum_part && wsum_n > 0)
+      for (int k = tid; k < wsum_n; k += kThreads) { t.x += wsum_part[k].x; t.y += wsum_part[k].y; }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+    }
+    if (lane == 0) s_red[warp] = t;
+    __syncthreads();
+    if (tid == 0) {
+      double2 m = make_double2(0.0, 0.0);
+      if (wsum_part && wsum_n > 0) {
+        for (int k = 0; k < kWarps; ++k) { m.x += s_red[k].x; m.y += s_red[k].y; }
+        m.x /= (double)n_samples;
+        m.y /= (double)n_samples;
+      } else if (wsum_part) {
+        m = wsum_part[0];
+      }
+      s_mean = m;
+    }
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, d.tmem_cols);
+    umma::tmem_relinquish();
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tbase = *tslot;
+  auto issue_load = [&](int j) {               // thread 0 only
+    const int c = c_first + j, b = j & 1;
+    uint8_t* sb = smem + b * buf_bytes;
+    umma::mbar_arrive_expect_tx(&full[b], buf_bytes);
+    umma::bulk_g2s(sb, reinterpret_cast<const uint8_t*>(sig_cols) + (size_t)c * a_bytes, a_bytes, &full[b]);
+    umma::bulk_g2s(sb + a_bytes, reinterpret_cast<const uint8_t*>(t_cols) + ((size_t)c * nnc + q) * 2 * b_term,
+                   2 * b_term, &full[b]);
+  };
+  if (tid == 0) {
+    issue_load(0);
+    if (n_my > 1) issue_load(1);
+  }
+  const float mr = (float)s_mean.x, mi = (float)s_mean.y, fs = (float)scale;
+  T ga = ScalarTraits<T>::zero();               // g_a of site tid (q == 0 CTAs)
+  bool ok = true;
+  for (int j = 0; j < n_my; ++j) {
+    const int b = j & 1;
+    const int64_t s0 = (int64_t)(c_first + j) * KC;
+    uint8_t* sA = smem + b * buf_bytes;
+    uint8_t* sBh = sA + a_bytes;
+    uint8_t* sBl = sBh + b_term;
+    T* u_b = s_u + b * KC;
+    for (int k = tid; k < KC; k += kThreads) {
+      const int64_t s = s0 + k;
+      T u = ScalarTraits<T>::zero();
+      if (s < n_samples) {
+        const float2 wv = w[s];
+        if constexpr (CPLX) u = make_float2((wv.x - mr) * fs, (wv.y - mi) * fs);
+        else u = (wv.x - mr) * fs;
+      }
+      u_b[k] = u;
+    }
+    __syncthreads();
+    if (ok && !umma::mbar_wait(&full[b], (j >> 1) & 1, kWaitLimit)) {
+      record_error(status, QES_ERR_TIMEOUT);
+      ok = false;
+      s_fail = 1;
+    }
+    // Q = conj(t) u in place: item (n, k8) = row n (re) and NC + n (im) for 8 samples
+    const int items = NC * (KC / 8);
+    for (int it = tid; ok && it < items; it += kThreads) {
+      const int n = it % NC, k8 = it / NC;
+      const uint32_t offr = umma::kmajor_offset(n, 8 * k8, NR);
+      float trh[8], trl[8], tih[8], til[8];
+      unpack8(*reinterpret_cast<const uint4*>(sBh + offr), trh);
+      unpack8(*reinterpret_cast<const uint4*>(sBl + offr), trl);
+      uint32_t offi = 0;
+      if constexpr (CPLX) {
+        offi = umma::kmajor_offset(NC + n, 8 * k8, NR);
+        unpack8(*reinterpret_cast<const uint4*>(sBh + offi), tih);
+        unpack8(*reinterpret_cast<const uint4*>(sBl + offi), til);
+      }
+      uint16_t rh[8], rl[8], ih[8], il[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const T u = u_b[8 * k8 + e];
+        if constexpr (CPLX) {
+          const float a = trh[e] + trl[e], bb = tih[e] + til[e];
+          const float2 qv = make_float2(a * u.x + bb * u.y, a * u.y - bb * u.x);
+          split_bf16(qv.x, rh[e], rl[e]);
+          split_bf16(qv.y, ih[e], il[e]);
+        } else {
+          split_bf16((trh[e] + trl[e]) * u, rh[e], rl[e]);
+        }
+      }
+      *reinterpret_cast<uint4*>(sBh + offr) = pack8(rh);
+      *reinterpret_cast<uint4*>(sBl + offr) = pack8(rl);
+      if constexpr (CPLX) {
+        *reinterpret_cast<uint4*>(sBh + offi) = pack8(ih);
+        *reinterpret_cast<uint4*>(sBl + offi) = pack8(il);
+      }
+    }
+    umma::fence_proxy_async_smem();
+    __syncthreads();
+    ok = ok && !s_fail;
+    if (tid == 0 && ok) {
+      umma::tc_fence_after();
+      const uint32_t idesc = umma::idesc_bf16_f32(128, NC);
+      const uint32_t aaddr = umma::smem_u32(sA), bh = umma::smem_u32(sBh), bl = umma::smem_u32(sBl);
+      for (int kk = 0; kk < KC / 16; ++kk) {
+        for (int mt = 0; mt < MT; ++mt) {
+          const uint64_t ad = umma::smem_desc(aaddr + (uint32_t)mt * 2048u + 2u * kk * R * 16u, R * 16u, 128u);
+          for (int term = 0; term < 2; ++term) {
+            const uint32_t bb = term ? bl : bh;
+            for (int h = 0; h < H; ++h) {
+              const uint64_t bd =
+                  umma::smem_desc(bb + (uint32_t)h * (NC / 8) * 128u + 2u * kk * NR * 16u, NR * 16u, 128u);
+              umma::mma_bf16(tbase + (uint32_t)((mt * H + h) * NC), ad, bd, idesc,
+                             (j > 0 || kk > 0 || term > 0) ? 1u : 0u);
+            }
+          }
+        }
+      }
+      umma::mma_commit(&mdone[b]);
+    }
+    // g_a (first N chunk only): thread i sums sigma_si u_s over the chunk from the A tile
+    if (q == 0 && ok && tid < ns)
+      for (int k = 0; k < KC; ++k) {
+        const uint16_t sb = *reinterpret_cast<const uint16_t*>(sA + umma::kmajor_offset(tid, k, R));
+        ga = addx(ga, scal(bf16_val(sb), u_b[k]));
+      }
+    __syncthreads();
+    // refill this buffer with chunk j + 2 once the MMAs reading it have completed
+    if (tid == 0 && ok && j + 2 < n_my) {
+      if (!umma::mbar_wait(&mdone[b], (j >> 1) & 1, kWaitLimit)) {
+        record_error(status, QES_ERR_TIMEOUT);
+        s_fail = 1;
+      } else {
+        issue_load(j + 2);
+      }
+    }
+    __syncthreads();
+    ok = ok && !s_fail;
+  }
+  // wait for the last MMAs (each buffer's final commit)
+  if (ok) {
+    for (int j = max(0, n_my - 2); j < n_my; ++j)
+      if (!umma::mbar_wait(&mdone[j & 1], (j >> 1) & 1, kWaitLimit)) {
+        record_error(status, QES_ERR_TIMEOUT);
+        ok = false;
+      }
+  }
+  umma::tc_fence_after();
+  T* out = partial + (int64_t)g * P;
+  if (q == 0 && tid < ns) out[tid] = ga;
+  const int quarter = warp & 3, cg = warp >> 2;
+  for (int mt = 0; ok && mt < MT; ++mt) {
+    const int i = mt * 128 + 32 * quarter + lane;             // site row
+    const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+    for (int c = cg; c < NC / 16; c += kColGroups) {
+      const int c0 = 16 * c;
+      float gr[16], gi[16];
+      umma::tmem_ld16(lane_addr + (uint32_t)(mt * H * NC + c0), gr);
+      if constexpr (CPLX) umma::tmem_ld16(lane_addr + (uint32_t)((mt * H + 1) * NC + c0), gi);
+      if (i <= ns) {
+        T* rowp = (i == ns) ? out + ns : out + ns + nh + (int64_t)i * nh;
+        const int mb = n0 + c0;
+        const bool vec = (mb + 16 <= nh) && ((reinterpret_cast<uintptr_t>(rowp + mb) & 15) == 0);
+        if (vec) {
+          float4* dst = reinterpret_cast<float4*>(rowp + mb);
+          if constexpr (CPLX) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) dst[e] = make_float4(gr[2 * e], gi[2 * e], gr[2 * e + 1], gi[2 * e + 1]);
+          } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) dst[e] = make_float4(gr[4 * e], gr[4 * e + 1], gr[4 * e + 2], gr[4 * e + 3]);
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            const int m = mb + e;
+            if (m < nh) {
+              if constexpr (CPLX) rowp[m] = make_float2(gr[e], gi[e]);
+              else rowp[m] = gr[e];
+            }
+          }
+        }
+      }
+    }
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tbase, d.tmem_cols);
+}
+
+// ================================================================================================
 // host side
 // ================================================================================================
 static int pow2_at_least(int x) {
@@ -566,6 +867,7 @@ static int pow2_at_least(int x) {
 
 bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   const bool cplx = dtype == QES_DTYPE_C64;
+  const int H = cplx ? 2 : 1;
   TcDims t{};
   t.ns = ns;
   t.nh = nh;
@@ -575,35 +877,72 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   t.Kd = cplx ? 2 * t.Mp : (nh + 31) / 32 * 32;               // multiple of KCH
   t.Sp = cplx ? (ns + 1 + 7) / 8 * 8 : (ns + 1 + 15) / 16 * 16;  // sites + the v_b row
   t.NB = cplx ? 2 * t.Sp : t.Sp;
-  if (ns > 127 || t.Mp > 256 || t.NB > 256 || n_samples < 1) return false;   // row 127 holds the ones
-  if (t.Kd % t.KCH != 0) return false;
-  t.im_off = pow2_at_least(t.Mp);
-  t.tmem_cols = pow2_at_least(std::max(cplx ? 2 * t.im_off : t.im_off, t.NB));
-  if (t.tmem_cols > 512) return false;
+  if (n_samples < 1 || t.Kd % t.KCH != 0 || t.NB > 512) return false;
   const size_t tsz = cplx ? 8 : 4;
+  // ov: as many pipeline stages (2..4) as shared memory holds
   const size_t stage = 2u * (128u * t.KCH * 2 + (size_t)t.NB * t.KCH * 2);
-  const size_t ov_smem = kStages * stage + 8 * (2 * kStages + 1) + 16 + (size_t)ns * tsz + 64;
-  if (ov_smem > kTcSmemLimit) return false;
+  const size_t ov_extra = 8 * (2 * 4 + 1) + 16 + (size_t)ns * tsz + 64;
+  const int S = (int)std::min<size_t>(4, (kTcSmemLimit - ov_extra) / stage);
+  if (S < 2) return false;
+  t.ov_stages = S;
+  t.ov_smem = (int)(S * stage + ov_extra);
+  t.n_tiles = (int)((n_samples + 127) / 128);
+  t.big = ns > 127 || t.Mp > 256 || t.NB > 256;
+  if (!t.big) {
+    t.im_off = pow2_at_least(t.Mp);
+    t.tmem_cols = pow2_at_least(std::max(cplx ? 2 * t.im_off : t.im_off, t.NB));
+    if (t.tmem_cols > 512) return false;
+    int kc = 256;
+    while (kc >= 16) {
+      const size_t sm = 128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64;
+      if (sm <= kTcSmemLimit) break;
+      kc -= 16;
+    }
+    if (kc < 16) return false;
+    t.KC = kc;
+    t.n_chunks = (int)((n_samples + kc - 1) / kc);
+    t.nsplit = t.n_chunks;
+    t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64);
+    *dout = t;
+    return true;
+  }
+  // large problems: O^H u tiled in M (sites + ones row) and N (hidden units)
+  t.MT = (ns + 1 + 127) / 128;
+  if (t.MT > 4) return false;                                  // TMEM: MT * H * NC <= 512 with NC >= 16
+  int nc = (512 / (t.MT * H)) / 16 * 16;
+  nc = std::min(nc, 256);
+  nc = std::min(nc, t.Mp);
+  if (nc < 16) return false;
+  t.NC = nc;
+  t.NR = H * nc;
+  t.nnc = (nh + nc - 1) / nc;
+  const size_t R = (size_t)t.MT * 128;
   int kc = 256;
   while (kc >= 16) {
-    const size_t sm = 128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64;
+    const size_t sm = 2u * (R * kc * 2 + 2u * t.NR * kc * 2) + 2u * kc * tsz + 16 + 8 * 4 + 16 + 64;
     if (sm <= kTcSmemLimit) break;
     kc -= 16;
   }
   if (kc < 16) return false;
   t.KC = kc;
-  t.n_tiles = (int)((n_samples + 127) / 128);
   t.n_chunks = (int)((n_samples + kc - 1) / kc);
-  t.ov_smem = (int)ov_smem;
-  t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64);
+  const int groups_target = std::max(1, (2 * 148 + t.nnc - 1) / t.nnc);
+  t.SPC = std::max(1, (t.n_chunks + groups_target - 1) / groups_target);
+  t.nsplit = (t.n_chunks + t.SPC - 1) / t.SPC;
+  t.ohu_smem = (int)(2u * (R * kc * 2 + 2u * t.NR * kc * 2) + 2u * kc * tsz + 16 + 8 * 4 + 16 + 64);
+  t.im_off = 0;
+  t.tmem_cols = pow2_at_least(std::max(t.MT * H * t.NC, t.NB));
+  if (t.tmem_cols > 512) return false;
   *dout = t;
   return true;
 }
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 static size_t sz_t_rows(const TcDims& d) { return (size_t)d.n_tiles * 128 * d.Kd * 2 * 2; }
-static size_t sz_t_cols(const TcDims& d) { return (size_t)d.n_chunks * d.Np * d.KC * 2 * 2; }
-static size_t sz_sig_cols(const TcDims& d) { return (size_t)d.n_chunks * 128 * d.KC * 2; }
+static size_t sz_t_cols(const TcDims& d) {
+  return d.big ? (size_t)d.n_chunks * d.nnc * d.NR * d.KC * 2 * 2 : (size_t)d.n_chunks * d.Np * d.KC * 2 * 2;
+}
+static size_t sz_sig_cols(const TcDims& d) { return (size_t)d.n_chunks * (d.big ? d.MT * 128 : 128) * d.KC * 2; }
 static size_t sz_vp(const TcDims& d) { return (size_t)d.NB * d.Kd * 2 * 2; }
 
 size_t tc_workspace_bytes(const TcDims& d) {
@@ -629,6 +968,8 @@ static int tc_set_attrs() {
                                       (int)kTcSmemLimit));
   QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
+  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_big_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemLimit));
   return QES_OK;
 }
 
@@ -637,18 +978,21 @@ int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_
   int rc = (dtype == QES_DTYPE_C64) ? tc_set_attrs<float2, double2>() : tc_set_attrs<float, double>();
   if (rc) return rc;
   QES_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int), st));
-  tc_sigma_cols_kernel<<<1184, 256, 0, st>>>(d.ns, d.KC, n_samples, d.n_chunks, bits, w.sig_cols);
+  if (d.big)
+    tc_sigma_cols_big_kernel<<<1184, 256, 0, st>>>(d.ns, d.MT * 128, d.KC, n_samples, d.n_chunks, bits, w.sig_cols);
+  else
+    tc_sigma_cols_kernel<<<1184, 256, 0, st>>>(d.ns, d.KC, n_samples, d.n_chunks, bits, w.sig_cols);
   QES_LAUNCH_CHECK();
   if (dtype == QES_DTYPE_C64) {
     tc_t_rows_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_rows);
-    QES_LAUNCH_CHECK();
-    tc_t_cols_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_cols);
-    QES_LAUNCH_CHECK();
+    if (d.big) tc_t_cols_big_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_cols);
+    else tc_t_cols_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_cols);
+    QES_LAUNCH_CHECK_N(2);
   } else {
     tc_t_rows_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_rows);
-    QES_LAUNCH_CHECK();
-    tc_t_cols_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_cols);
-    QES_LAUNCH_CHECK();
+    if (d.big) tc_t_cols_big_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_cols);
+    else tc_t_cols_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_cols);
+    QES_LAUNCH_CHECK_N(2);
   }
   return QES_OK;
 }
@@ -668,9 +1012,13 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   pf = qes_prof_begin(QES_PROF_OHU, st);
-  tc_ohu_kernel<T><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, w_out, w.wsum, d.n_tiles,
-                                                             1.0 / (double)n_samples, w.sig_cols, w.t_cols, partial,
-                                                             w.status);
+  if (d.big)
+    tc_ohu_big_kernel<T><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
+        d, n_samples, w_out, w.wsum, d.n_tiles, 1.0 / (double)n_samples, w.sig_cols, w.t_cols, partial, w.status);
+  else
+    tc_ohu_kernel<T><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, w_out, w.wsum, d.n_tiles,
+                                                               1.0 / (double)n_samples, w.sig_cols, w.t_cols, partial,
+                                                               w.status);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;
@@ -686,12 +1034,20 @@ int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bit
 
 int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
            double scale, void* partial, const TcWork& w, cudaStream_t st) {
-  if (dtype == QES_DTYPE_C64)
+  if (d.big) {
+    if (dtype == QES_DTYPE_C64)
+      tc_ohu_big_kernel<float2><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
+          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float2*)partial, w.status);
+    else
+      tc_ohu_big_kernel<float><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
+          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float*)partial, w.status);
+  } else if (dtype == QES_DTYPE_C64) {
     tc_ohu_kernel<float2><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, g, gsum_part, gsum_n, scale,
                                                                     w.sig_cols, w.t_cols, (float2*)partial, w.status);
-  else
+  } else {
     tc_ohu_kernel<float><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, g, gsum_part, gsum_n, scale,
                                                                    w.sig_cols, w.t_cols, (float*)partial, w.status);
+  }
   QES_LAUNCH_CHECK();
   return QES_OK;
 }

@@ -19,6 +19,13 @@ struct TcDims {
   int n_tiles;       // ceil(Ns / 128)
   int n_chunks;      // ceil(Ns / KC)
   int ov_smem, ohu_smem;
+  int ov_stages;     // ov pipeline depth (2..4, as many as fit shared memory)
+  int nsplit;        // partial P-vectors written by one O^H u pass
+  // large problems (ns > 127 or more hidden units than one MMA N): the O^H u GEMM is tiled in
+  // M (MT tiles of 128 sites, the ones row at site index ns) and N (nnc chunks of NC hidden units,
+  // NR = NC (real) or 2 NC (complex) operand rows), and one CTA folds SPC sample chunks into TMEM
+  bool big;
+  int MT, NC, NR, nnc, SPC;
 };
 
 struct TcWork {

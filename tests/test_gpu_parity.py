@@ -341,7 +341,8 @@ def sr_impl():
 
 
 @pytest.mark.parametrize("cplx,ns,nh,n", [(False, 16, 16, 300), (True, 9, 18, 700), (True, 36, 144, 1000),
-                                           (False, 20, 40, 513), (True, 100, 200, 300)])
+                                           (False, 20, 40, 513), (True, 100, 200, 300),
+                                           (False, 150, 300, 700), (True, 130, 100, 500)])
 def test_sr_matvec_tensor_cores_match_oracle(sr_impl, cplx, ns, nh, n):
     net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=21, init_scale=0.1)
     st = rand_states(n, ns, seed=22)
@@ -358,6 +359,27 @@ def test_sr_matvec_tensor_cores_match_oracle(sr_impl, cplx, ns, nh, n):
     y_cc = dv.sr_matvec(net.flat, ns, nh, bits, tn, torch.as_tensor(v).cuda(), shift=1e-3).cpu().numpy()
     assert rel_err(y_cc, ref) < 1e-4
     assert rel_err(y_tc, ref) < 1e-4
+
+
+@pytest.mark.parametrize("cplx,ns,nh,n", [(False, 200, 800, 12000), (True, 140, 280, 12000),
+                                           (False, 400, 1600, 2048)])
+def test_sr_matvec_tensor_cores_large_match_cuda_cores(sr_impl, cplx, ns, nh, n):
+    """Large shapes take the M/N-tiled tensor-core path (several sample chunks per CTA); the
+    CUDA-core matvec, itself checked against the oracle above, is the reference."""
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=41, init_scale=0.05)
+    bits = dv.pack_states(rand_states(n, ns, seed=42))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    P = ns + nh + ns * nh
+    rng = np.random.default_rng(6)
+    v = rng.normal(size=P) + (1j * rng.normal(size=P) if cplx else 0)
+    vt = torch.as_tensor(v).cuda()
+    dc = _lib.DTYPE_C64 if cplx else _lib.DTYPE_F32
+    sr_impl(_lib.SR_IMPL_TENSOR_CORES)
+    assert _lib.sr_uses_tensor_cores(dc, ns, nh, n)
+    y_tc = dv.sr_matvec(net.flat, ns, nh, bits, tn, vt, shift=1e-3).cpu().numpy()
+    sr_impl(_lib.SR_IMPL_CUDA_CORES)
+    y_cc = dv.sr_matvec(net.flat, ns, nh, bits, tn, vt, shift=1e-3).cpu().numpy()
+    assert rel_err(y_tc, y_cc) < 1e-4
 
 
 @pytest.mark.parametrize("cplx", [False, True])

@@ -31,6 +31,9 @@ def __getattr__(name):
     if name in ("NQS", "NQSSingleStepResult", "NQSTrainStats"):
         from . import nqs
         return getattr(nqs, name)
+    if name == "ops":
+        from . import ops
+        return ops
     if name in ("NQSBatch", "NQSBatchStats"):
         from . import batch
         return getattr(batch, name)

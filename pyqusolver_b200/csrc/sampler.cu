@@ -27,40 +27,76 @@ QES_D float log_abs<float>(float v) { return logf(fabsf(v)); }
 template <>
 QES_D float log_abs<float2>(float2 v) { return 0.5f * logf(v.x * v.x + v.y * v.y); }
 
+// theta / tanh(theta) of one chain: lane l owns hidden units m = l + 32 r (r < MPL), held in
+// registers (narrow caches) or in a per-warp slice of shared memory (wide caches, where a
+// register-resident cache would cap the SM at a few warps)
+template <class T, int MPL, bool SMEM>
+struct ThetaCache;
 template <class T, int MPL>
+struct ThetaCache<T, MPL, false> {
+  static constexpr int kMPL = MPL;
+  static constexpr bool kSmem = false;
+  T th_[MPL], tn_[MPL];
+  QES_D void bind(T*, int) {}
+  QES_D T& th(int r) { return th_[r]; }
+  QES_D T& tn(int r) { return tn_[r]; }
+};
+template <class T, int MPL>
+struct ThetaCache<T, MPL, true> {
+  static constexpr int kMPL = MPL;
+  static constexpr bool kSmem = true;
+  T* th_;
+  T* tn_;
+  QES_D void bind(T* warp_slice, int lane) { th_ = warp_slice + lane; tn_ = warp_slice + 32 * MPL + lane; }
+  QES_D T& th(int r) { return th_[32 * r]; }
+  QES_D T& tn(int r) { return tn_[32 * r]; }
+};
+
+template <class T, class Cache>
 QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ b,
-                      const T* __restrict__ W, T (&th)[MPL], T (&tn)[MPL]) {
+                      const T* __restrict__ W, Cache& c) {
+  constexpr int MPL = Cache::kMPL;
+  // accumulate CH units per lane in registers, then store (CH = MPL for register caches)
+  constexpr int CH = Cache::kSmem ? 16 : MPL;
 #pragma unroll
-  for (int r = 0; r < MPL; ++r) {
-    const int m = lane + 32 * r;
-    th[r] = (m < nh) ? b[m] : ScalarTraits<T>::zero();
-  }
-  auto site = [&](int i) {
-    const float sg = ((cfg[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
-    const T* wr = W + (int64_t)i * nh;
+  for (int c0 = 0; c0 < MPL; c0 += CH) {
+    T acc[CH];
 #pragma unroll
-    for (int r = 0; r < MPL; ++r) {
-      const int m = lane + 32 * r;
-      if (m < nh) th[r] = addx(th[r], scal(sg, wr[m]));
+    for (int r = 0; r < CH; ++r) {
+      const int m = lane + 32 * (c0 + r);
+      acc[r] = (m < nh) ? b[m] : ScalarTraits<T>::zero();
     }
-  };
-  if constexpr (MPL >= 16) {
-#pragma unroll 4
-    for (int i = 0; i < ns; ++i) site(i);
-  } else {
-    for (int i = 0; i < ns; ++i) site(i);
-  }
+    auto site = [&](int i) {
+      const float sg = ((cfg[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
+      const T* wr = W + (int64_t)i * nh;
 #pragma unroll
-  for (int r = 0; r < MPL; ++r) tn[r] = tanhx(th[r]);
+      for (int r = 0; r < CH; ++r) {
+        const int m = lane + 32 * (c0 + r);
+        if (m < nh) acc[r] = addx(acc[r], scal(sg, wr[m]));
+      }
+    };
+    if constexpr (CH >= 16) {
+#pragma unroll 4
+      for (int i = 0; i < ns; ++i) site(i);
+    } else {
+      for (int i = 0; i < ns; ++i) site(i);
+    }
+#pragma unroll
+    for (int r = 0; r < CH; ++r) {
+      c.th(c0 + r) = acc[r];
+      c.tn(c0 + r) = tanhx(acc[r]);
+    }
+  }
 }
 
-template <class T, int MPL>
-QES_D T chain_logpsi(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ a, const T (&th)[MPL]) {
+template <class T, class Cache>
+QES_D T chain_logpsi(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ a, Cache& c) {
+  constexpr int MPL = Cache::kMPL;
   T s = ScalarTraits<T>::zero();
 #pragma unroll
   for (int r = 0; r < MPL; ++r) {
     const int m = lane + 32 * r;
-    if (m < nh) s = addx(s, log_cosh(th[r]));
+    if (m < nh) s = addx(s, log_cosh(c.th(r)));
   }
   for (int i = lane; i < ns; i += 32) {
     const float sg = ((cfg[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
@@ -83,8 +119,8 @@ struct ChainCtx {
 
 // Runs proposals for chain `chain` (index within its problem) with the
 // problem's packed spins staged in `cw` (shared memory, one warp).
-template <class T, int MPL, int RULE>
-QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __restrict__ chain_bits,
+template <class T, int MPL, int RULE, bool SMEM = false>
+QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_slice, uint32_t* __restrict__ chain_bits,
                      uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed,
                      int32_t* __restrict__ accepted, uint32_t* __restrict__ sample_bits,
                      T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
@@ -102,8 +138,9 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
   const int recompute = P.recompute_every > 0 ? P.recompute_every : ns;
   const float bm = P.beta_mu;
 
-  T th[MPL], tn[MPL];
-  full_theta<T, MPL>(ns, nh, lane, cw, b, W, th, tn);
+  ThetaCache<T, MPL, SMEM> cache;
+  cache.bind(theta_slice, lane);
+  full_theta<T>(ns, nh, lane, cw, b, W, cache);
   int since = 0;
 
   const int64_t total = P.therm_steps_total + (int64_t)P.num_samples * P.sweep_steps;
@@ -169,7 +206,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
 #pragma unroll
           for (int q = 0; q < PF; ++q) {
             const int rr = c0 + q;
-            prod = mulx(prod, ratio_factor(cb[cur][q], g, tn[rr], sb[cur][q]));
+            prod = mulx(prod, ratio_factor(cb[cur][q], g, cache.tn(rr), sb[cur][q]));
             if ((rr & 7) == 7) renorm(prod, ex);
           }
         }
@@ -177,7 +214,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
 #pragma unroll
         for (int rr = 0; rr < MPL; ++rr) {
           const int m = lane + 32 * rr;
-          if (m < nh) prod = mulx(prod, ratio_factor(Crow[m], g, tn[rr], Srow[m]));
+          if (m < nh) prod = mulx(prod, ratio_factor(Crow[m], g, cache.tn(rr), Srow[m]));
           if ((rr & 7) == 7) renorm(prod, ex);
         }
       }
@@ -207,8 +244,9 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
           for (int q = 0; q < PU; ++q) {
             const int rr = c0 + q;
             if (lane + 32 * rr < nh) {
-              th[rr] = addx(th[rr], scal(2.f * g, d[q]));
-              tn[rr] = tanhx(th[rr]);
+              const T t2 = addx(cache.th(rr), scal(2.f * g, d[q]));
+              cache.th(rr) = t2;
+              cache.tn(rr) = tanhx(t2);
             }
           }
         }
@@ -219,8 +257,9 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
           if (m < nh) {
             T d = wi[m];
             if (j0 >= 0) d = addx(d, scal(-1.f, wj[m]));
-            th[rr] = addx(th[rr], scal(2.f * g, d));
-            tn[rr] = tanhx(th[rr]);
+            const T t2 = addx(cache.th(rr), scal(2.f * g, d));
+            cache.th(rr) = t2;
+            cache.tn(rr) = tanhx(t2);
           }
         }
       }
@@ -235,20 +274,20 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
     n_acc += keep ? 1 : 0;
     ++step;
     if (++since >= recompute) {
-      full_theta<T, MPL>(ns, nh, lane, cw, b, W, th, tn);
+      full_theta<T>(ns, nh, lane, cw, b, W, cache);
       since = 0;
     }
     if (it + 1 == next_record) {
       const int64_t row = rec * P.n_chains + chain;
       for (int q = lane; q < nw; q += 32) sample_bits[row * nw + q] = cw[q];
-      const T lp = chain_logpsi<T, MPL>(ns, nh, lane, cw, a, th);
+      const T lp = chain_logpsi<T>(ns, nh, lane, cw, a, cache);
       if (lane == 0 && sample_logpsi) sample_logpsi[row] = lp;
       ++rec;
       next_record += P.sweep_steps;
     }
   }
   for (int q = lane; q < nw; q += 32) chain_bits[(int64_t)chain * nw + q] = cw[q];
-  const T lp = chain_logpsi<T, MPL>(ns, nh, lane, cw, a, th);
+  const T lp = chain_logpsi<T>(ns, nh, lane, cw, a, cache);
   if (lane == 0) {
     chain_step[chain] = step;
     proposed[chain] = n_prop;
@@ -258,7 +297,8 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, uint32_t* __
   __syncwarp();
 }
 
-template <class T, int MPL, int RULE>
+// Wide theta caches (SMEM = true) live in dynamic shared memory, 2 * 32 * MPL elements per warp.
+template <class T, int MPL, int RULE, bool SMEM>
 __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
     qes_sampler_config cfg, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ W,
     const T* __restrict__ flipC, const T* __restrict__ flipS, const int32_t* __restrict__ nbr,
@@ -267,6 +307,7 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
     uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed, int32_t* __restrict__ accepted,
     uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
   __shared__ uint32_t cfg_sm[SMP_WARPS][SMP_MAX_WORDS];
+  extern __shared__ __align__(16) uint8_t theta_sm[];
   const int wid = threadIdx.x >> 5;
   const int chain = blockIdx.x * SMP_WARPS + wid;
   if (chain >= cfg.n_chains) return;            // whole warp leaves together
@@ -278,9 +319,14 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
   P.chain_id = cfg.chain_offset + chain;
   P.a = a; P.b = b; P.W = W; P.flipC = flipC; P.flipS = flipS; P.pairC = pairC; P.pairS = pairS;
   P.nbr = nbr; P.nbr_pair = nbr_pair; P.pair_i = pair_i; P.pair_j = pair_j;
-  run_chain<T, MPL, RULE>(P, chain, cfg_sm[wid], chain_bits, chain_step, proposed, accepted, sample_bits,
-                          sample_logpsi, last_logpsi);
+  T* slice = SMEM ? reinterpret_cast<T*>(theta_sm) + (size_t)wid * 2 * 32 * MPL : nullptr;
+  run_chain<T, MPL, RULE, SMEM>(P, chain, cfg_sm[wid], slice, chain_bits, chain_step, proposed, accepted,
+                                sample_bits, sample_logpsi, last_logpsi);
 }
+
+// register caches up to 16 units per lane (real) / 8 (complex); wider ones in shared memory
+template <class T, int MPL>
+constexpr bool sampler_smem_cache() { return MPL > (ScalarTraits<T>::is_complex ? 8 : 16); }
 
 template <class T, int MPL>
 static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, const void* b, const void* W,
@@ -288,17 +334,26 @@ static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, cons
                               const int32_t* pi, const int32_t* pj, const void* pairC, const void* pairS,
                               uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
                               uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi, cudaStream_t st) {
+  constexpr bool SM = sampler_smem_cache<T, MPL>();
   const unsigned grid = (unsigned)((cfg->n_chains + SMP_WARPS - 1) / SMP_WARPS);
-  if (cfg->rule == QES_RULE_LOCAL)
-    sampler_kernel<T, MPL, QES_RULE_LOCAL><<<grid, 32 * SMP_WARPS, 0, st>>>(
+  const size_t smem = SM ? (size_t)SMP_WARPS * 2 * 32 * MPL * sizeof(T) : 0;
+  if (cfg->rule == QES_RULE_LOCAL) {
+    if (SM)
+      QES_CUDA_CHECK(cudaFuncSetAttribute(sampler_kernel<T, MPL, QES_RULE_LOCAL, SM>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    sampler_kernel<T, MPL, QES_RULE_LOCAL, SM><<<grid, 32 * SMP_WARPS, smem, st>>>(
         *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
         (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
         (T*)sample_logpsi, (T*)last_logpsi);
-  else
-    sampler_kernel<T, MPL, QES_RULE_EXCHANGE><<<grid, 32 * SMP_WARPS, 0, st>>>(
+  } else {
+    if (SM)
+      QES_CUDA_CHECK(cudaFuncSetAttribute(sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM><<<grid, 32 * SMP_WARPS, smem, st>>>(
         *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
         (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
         (T*)sample_logpsi, (T*)last_logpsi);
+  }
   QES_LAUNCH_CHECK();
   return QES_OK;
 }
@@ -394,7 +449,7 @@ __global__ void batch_sampler_kernel(const qes_batch_instance* __restrict__ inst
     P.flipC = flipC + I.flip_off; P.flipS = flipS + I.flip_off;
     P.pairC = nullptr; P.pairS = nullptr; P.nbr = nullptr; P.nbr_pair = nullptr; P.pair_i = nullptr;
     P.pair_j = nullptr;
-    run_chain<T, MPL, QES_RULE_LOCAL>(P, it.y, cw, chain_bits + I.chain_word_off, chain_step + I.chain_off,
+    run_chain<T, MPL, QES_RULE_LOCAL>(P, it.y, cw, nullptr, chain_bits + I.chain_word_off, chain_step + I.chain_off,
                                       proposed + I.chain_off, accepted + I.chain_off,
                                       sample_bits + I.sample_word_off,
                                       sample_logpsi ? sample_logpsi + I.sample_off : nullptr,

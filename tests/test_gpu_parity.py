@@ -245,10 +245,12 @@ def _gpu_sampler(net, rule, ns, chains, seed, therm, sweep, lattice=None, init=N
                       numsamples=1, lattice=lattice, initstate=init, n_particles=n_up)
 
 
-@pytest.mark.parametrize("cplx", [False, True])
-def test_sampler_local_trajectory_matches_oracle(cplx):
+@pytest.mark.parametrize("cplx,nh", [(False, 20), (True, 20), (False, 600), (True, 300)])
+def test_sampler_local_trajectory_matches_oracle(cplx, nh):
+    """nh = 600 (real) / 300 (complex) run the shared-memory theta cache of the sampler."""
     ns = 10
-    net = RBM((ns,), n_hidden=20, dtype="complex64" if cplx else "float32", seed=8, init_scale=0.3)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=8,
+              init_scale=0.3 if nh <= 32 else 0.05)
     smp = _gpu_sampler(net, "LOCAL", ns, 64, seed=77, therm=2, sweep=5)
     bits, lp = smp.sample_bits(num_samples=6)
     got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
@@ -425,3 +427,20 @@ def test_cg_graph_replay_matches_direct_launches():
         _lib.call("qes_set_cg_graphs", 1)
     assert out[0][1] == out[1][1] == out[2][1]
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[1][0], out[2][0])
+
+
+def test_torch_ops_match_direct_calls():
+    import pyqusolver_b200.ops  # noqa: F401
+    ns, nh, n = 12, 24, 200
+    net = RBM((ns,), n_hidden=nh, dtype="complex64", seed=51, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=52))
+    tn, lp = torch.ops.qes_b200.rbm_forward(net.flat, bits, ns, nh)
+    _, tn2, lp2 = dv.rbm_forward(net.flat, ns, nh, bits)
+    assert torch.equal(tn, tn2) and torch.equal(lp, lp2)
+    O = torch.ops.qes_b200.log_derivatives(net.flat, bits, tn, ns, nh)
+    assert torch.equal(O, dv.log_derivatives(net.flat, ns, nh, bits, tn))
+    g = torch.randn(n, dtype=torch.complex64, device="cuda")
+    assert torch.allclose(torch.ops.qes_b200.logpsi_vjp(net.flat, bits, tn, g, ns, nh),
+                          dv.logpsi_vjp(net.flat, ns, nh, bits, tn, g), rtol=1e-12, atol=1e-12)
+    st = torch.ops.qes_b200.loss_stats(lp.to(torch.complex64))
+    assert st.shape == (4,) and st.dtype == torch.float64

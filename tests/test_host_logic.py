@@ -151,3 +151,10 @@ def test_library_rejects_bad_arguments_without_gpu():
     assert e.value.code == _lib.QES_ERR_ARG
     with pytest.raises(_lib.QESError):
         _lib.call("qes_rbm_forward", 7, 4, 4, 1, None, None, None, None, None, None, None, None)
+
+
+def test_torch_ops_are_registered():
+    import torch
+    import pyqusolver_b200.ops  # noqa: F401  (registration only; no GPU call)
+    for name in ("rbm_forward", "log_derivatives", "logpsi_vjp", "sr_matvec", "sr_solve_cg", "loss_stats"):
+        assert hasattr(torch.ops.qes_b200, name)

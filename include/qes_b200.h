@@ -129,6 +129,33 @@ int qes_sampler_run(int dtype, const qes_sampler_config* cfg,
                     uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
                     void* stream);
 
+/* As qes_sampler_run with one beta per chain (chain_beta[n_chains], float32;
+ * cfg->beta is ignored): the replica slots of parallel tempering.          */
+int qes_sampler_run_betas(int dtype, const qes_sampler_config* cfg, const float* chain_beta,
+                          const void* a, const void* b, const void* W,
+                          const void* flipCt, const void* flipSt, const int32_t* nbr_table,
+                          const int32_t* nbr_pair, const int32_t* pair_i, const int32_t* pair_j,
+                          int n_pairs, const void* pairCt, const void* pairSt,
+                          uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed,
+                          int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi,
+                          void* last_logpsi, void* stream);
+
+/* Parallel tempering (QES/Solver/MonteCarlo/vmc.py:1289-1507).  Chains are
+ * n_replicas slots x n_chains (chain index r * n_chains + c); chain_beta holds
+ * each chain's current beta.  qes_pt_swap exchanges beta labels between
+ * adjacent slots (r, r+1), r of one parity per round (Philox counter
+ * (round, 0, 0, 4) picks the parity; pair r of chain c draws counter
+ * (c, round, r, 5)), accepting iff log u < min((b_r - b_r+1) mu
+ * (Re lpsi_r+1 - Re lpsi_r), 0); swaps_accepted[r] (optional) counts swaps.
+ * qes_pt_collect copies, per chain c, the slot whose beta equals
+ * target_beta (|diff| < 1e-5, the first such slot) into row c of out_bits /
+ * out_logpsi.                                                              */
+int qes_pt_swap(int dtype, int n_replicas, int n_chains, const void* logpsi, float* chain_beta, float mu,
+                uint64_t seed, int64_t round, int* swaps_accepted, void* stream);
+int qes_pt_collect(int dtype, int n_replicas, int n_chains, int ns, const float* chain_beta,
+                   float target_beta, const uint32_t* chain_bits, const void* logpsi,
+                   uint32_t* out_bits, void* out_logpsi, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Hamiltonian lowered to moves (off-diagonal) and diagonal terms.
  * Off-diagonal move k contributes  conj(c_k(s)) psi(s')/psi(s)  with

@@ -32,6 +32,8 @@ _MASK32 = np.uint64(0xFFFFFFFF)
 STREAM_PROPOSAL = 0
 STREAM_INIT_RND = 1
 STREAM_INIT_FIXED = 2
+STREAM_PT_PHASE = 4
+STREAM_PT_SWAP = 5
 
 
 def philox4x32_10(c0, c1, c2, c3, k0, k1):

@@ -147,6 +147,79 @@ class MetropolisSampler:
         return configs, logpsi, probs
 
 
+class ParallelTemperingSampler:
+    """Replica exchange of beta labels (``QES/Solver/MonteCarlo/vmc.py:1289-1507``).
+
+    Slots r = 0..R-1 hold n_chains chains each (chain id r * n_chains + c, the ids of one
+    ``MetropolisSampler`` over R * n_chains chains).  One round = ``sweep_steps`` Metropolis
+    steps of every chain at its current beta (``_run_pt_round_jax``), then a swap of beta
+    labels between adjacent slots of one parity (``_replica_exchange_kernel_jax_betas``):
+    accept iff log u < min((b_r - b_r+1) mu (Re lpsi_r+1 - Re lpsi_r), 0).  Thermalisation
+    runs max(1, ceil(therm_updates / sweep_steps)) rounds on every call, with therm_updates
+    = therm_steps * sweep_steps * N on the first call and 0 afterwards (``:1439``, ``:1585``).
+    After each sampling round the physical slot (beta == pt_betas[0]) of every chain is
+    recorded (``_collect_pt_physical_samples_jax``).  Random draws: the phase is Philox counter
+    (round, 0, 0, STREAM_PT_PHASE) word 0 & 1; the swap uniform of pair r in chain c is
+    counter (c, round, r, STREAM_PT_SWAP) word 0 (the reference uses JAX keys).  Betas are
+    float32 values, as the device stores them.
+    """
+
+    def __init__(self, ns, n_chains, pt_betas, **kw):
+        self.pt_betas = np.asarray(pt_betas, dtype=np.float32).astype(np.float64)
+        self.R = len(self.pt_betas)
+        self.C = int(n_chains)
+        self.base = MetropolisSampler(ns, self.R * self.C, **kw)
+        # every slot starts from the same base states (``vmc.py:397-405``)
+        base = init_states(kw.get("init", "RND"), self.C, ns, kw.get("seed", 0), n_up=kw.get("n_up"),
+                           chain_offset=kw.get("chain_offset", 0))
+        self.base.states = np.tile(base, (self.R, 1))
+        self.betas = np.repeat(self.pt_betas[:, None], self.C, axis=1)
+        self.round = 0
+        self.swaps = np.zeros(max(self.R - 1, 1), dtype=np.int64)
+
+    def _round(self, params):
+        b = self.base
+        b.beta = self.betas.reshape(-1)
+        lp = b.run_steps(params, b.sweep_steps).reshape(self.R, self.C)
+        k0, k1 = philox.seed_key(b.seed)
+        rnd = np.uint64(self.round)
+        ph = philox.philox4x32_10(rnd & np.uint64(0xFFFFFFFF), rnd >> np.uint64(32), 0,
+                                  philox.STREAM_PT_PHASE, k0, k1)[0]
+        phase = int(ph) & 1
+        cols = np.arange(self.C, dtype=np.uint64)
+        for r in range(phase, self.R - 1, 2):
+            bi, bj = self.betas[r].copy(), self.betas[r + 1].copy()
+            log_acc = (bi - bj) * b.mu * (np.real(lp[r + 1]) - np.real(lp[r]))
+            u = philox.uniform_open(philox.philox4x32_10(cols, self.round, r, philox.STREAM_PT_SWAP, k0, k1)[0])
+            acc = np.log(u) < np.minimum(log_acc, 0.0)
+            self.betas[r] = np.where(acc, bj, bi)
+            self.betas[r + 1] = np.where(acc, bi, bj)
+            self.swaps[r] += int(acc.sum())
+        self.round += 1
+        return lp
+
+    def sample(self, params, num_samples):
+        b = self.base
+        therm_updates = b.therm_steps * b.sweep_steps * b.ns if b.needs_therm else 0
+        for _ in range(max(1, -(-therm_updates // b.sweep_steps))):
+            self._round(params)
+        b.needs_therm = False
+        cfg, lps = [], []
+        states = lambda: b.states.reshape(self.R, self.C, b.ns)
+        for _ in range(num_samples):
+            lp = self._round(params)
+            phys = np.abs(self.betas - self.pt_betas[0]) < 1e-5
+            slot = np.argmax(phys, axis=0)
+            cols = np.arange(self.C)
+            cfg.append(states()[slot, cols].copy())
+            lps.append(lp[slot, cols].copy())
+        configs = np.concatenate(cfg)
+        logpsi = np.concatenate(lps)
+        exponent = 1.0 / b.logprob_fact - b.mu * self.pt_betas[0]
+        probs = None if exponent == 0.0 else sample_probs(logpsi, configs.shape[0], exponent)
+        return configs, logpsi, probs
+
+
 def exact_distribution(params, ns, n_up=None):
     """|psi|^2 over the full (or fixed-n_up) basis, in the big-endian integer order."""
     allb = np.arange(1 << ns, dtype=np.int64)

@@ -99,6 +99,10 @@ SIGNATURES = {
                          _sz, _vp, _vp],
     "qes_local_energy_noalloc": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.POINTER(Hamiltonian), _vp, _vp, _vp,
                                  _vp, _vp],
+    "qes_sampler_run_betas": [C.c_int, C.POINTER(SamplerConfig), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                              C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "qes_pt_swap": [C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_float, _u64, _i64, _vp, _vp],
+    "qes_pt_collect": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_float, _vp, _vp, _vp, _vp, _vp],
     "qes_loss_stats_workspace_bytes": [_i64, C.POINTER(_sz)],
     "qes_loss_stats": [_i64, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_loss_rhat_workspace_bytes": [_i64, C.c_int, C.POINTER(_sz)],

@@ -305,7 +305,8 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
     const int32_t* __restrict__ nbr_pair, const int32_t* __restrict__ pair_i, const int32_t* __restrict__ pair_j,
     const T* __restrict__ pairC, const T* __restrict__ pairS, uint32_t* __restrict__ chain_bits,
     uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed, int32_t* __restrict__ accepted,
-    uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
+    uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi,
+    const float* __restrict__ chain_beta) {
   __shared__ uint32_t cfg_sm[SMP_WARPS][SMP_MAX_WORDS];
   extern __shared__ __align__(16) uint8_t theta_sm[];
   const int wid = threadIdx.x >> 5;
@@ -314,7 +315,8 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
   ChainCtx<T> P;
   P.ns = cfg.ns; P.nh = cfg.nh; P.n_chains = cfg.n_chains; P.deg = cfg.deg; P.sweep_steps = cfg.sweep_steps;
   P.recompute_every = cfg.recompute_every; P.num_samples = cfg.num_samples;
-  P.therm_steps_total = cfg.therm_steps_total; P.beta_mu = cfg.beta * cfg.mu;
+  P.therm_steps_total = cfg.therm_steps_total;
+  P.beta_mu = (chain_beta ? chain_beta[chain] : cfg.beta) * cfg.mu;     // per-chain beta: replica slots
   P.k0 = (uint32_t)(cfg.seed & 0xffffffffu); P.k1 = (uint32_t)(cfg.seed >> 32);
   P.chain_id = cfg.chain_offset + chain;
   P.a = a; P.b = b; P.W = W; P.flipC = flipC; P.flipS = flipS; P.pairC = pairC; P.pairS = pairS;
@@ -333,7 +335,8 @@ static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, cons
                               const void* flipC, const void* flipS, const int32_t* nbr, const int32_t* nbr_pair,
                               const int32_t* pi, const int32_t* pj, const void* pairC, const void* pairS,
                               uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
-                              uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi, cudaStream_t st) {
+                              uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi, const float* chain_beta,
+                              cudaStream_t st) {
   constexpr bool SM = sampler_smem_cache<T, MPL>();
   const unsigned grid = (unsigned)((cfg->n_chains + SMP_WARPS - 1) / SMP_WARPS);
   const size_t smem = SM ? (size_t)SMP_WARPS * 2 * 32 * MPL * sizeof(T) : 0;
@@ -344,7 +347,7 @@ static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, cons
     sampler_kernel<T, MPL, QES_RULE_LOCAL, SM><<<grid, 32 * SMP_WARPS, smem, st>>>(
         *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
         (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
-        (T*)sample_logpsi, (T*)last_logpsi);
+        (T*)sample_logpsi, (T*)last_logpsi, chain_beta);
   } else {
     if (SM)
       QES_CUDA_CHECK(cudaFuncSetAttribute(sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM>,
@@ -352,7 +355,7 @@ static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, cons
     sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM><<<grid, 32 * SMP_WARPS, smem, st>>>(
         *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
         (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
-        (T*)sample_logpsi, (T*)last_logpsi);
+        (T*)sample_logpsi, (T*)last_logpsi, chain_beta);
   }
   QES_LAUNCH_CHECK();
   return QES_OK;
@@ -364,11 +367,12 @@ static int launch_sampler(int mpl_needed, int mpl_max, const qes_sampler_config*
                           const int32_t* nbr_pair, const int32_t* pi, const int32_t* pj, const void* pairC,
                           const void* pairS, uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed,
                           int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
-                          cudaStream_t st) {
+                          const float* chain_beta, cudaStream_t st) {
 #define QES_SMP_CASE(M)                                                                                          \
   if (mpl_needed <= M && M <= mpl_max)                                                                           \
     return launch_sampler_mpl<T, M>(cfg, a, b, W, flipC, flipS, nbr, nbr_pair, pi, pj, pairC, pairS, chain_bits, \
-                                    chain_step, proposed, accepted, sample_bits, sample_logpsi, last_logpsi, st);
+                                    chain_step, proposed, accepted, sample_bits, sample_logpsi, last_logpsi,      \
+                                    chain_beta, st);
   QES_SMP_CASE(1)
   QES_SMP_CASE(2)
   QES_SMP_CASE(4)
@@ -383,12 +387,12 @@ static int launch_sampler(int mpl_needed, int mpl_max, const qes_sampler_config*
   return QES_ERR_SIZE;
 }
 
-extern "C" int qes_sampler_run(int dtype, const qes_sampler_config* cfg, const void* a, const void* b,
-                               const void* W, const void* flipCt, const void* flipSt, const int32_t* nbr_table,
-                               const int32_t* nbr_pair, const int32_t* pair_i, const int32_t* pair_j, int n_pairs,
-                               const void* pairCt, const void* pairSt, uint32_t* chain_bits, uint64_t* chain_step,
-                               int32_t* proposed, int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi,
-                               void* last_logpsi, void* stream) {
+static int sampler_run_impl(int dtype, const qes_sampler_config* cfg, const float* chain_beta, const void* a,
+                            const void* b, const void* W, const void* flipCt, const void* flipSt,
+                            const int32_t* nbr_table, const int32_t* nbr_pair, const int32_t* pair_i,
+                            const int32_t* pair_j, int n_pairs, const void* pairCt, const void* pairSt,
+                            uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
+                            uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi, void* stream) {
   QES_ARG_CHECK(cfg != nullptr, "qes_sampler_run: null config");
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sampler_run: bad dtype");
   QES_ARG_CHECK(cfg->ns > 0 && cfg->nh > 0 && cfg->n_chains >= 0 && cfg->num_samples >= 0, "qes_sampler_run: bad sizes");
@@ -410,10 +414,118 @@ extern "C" int qes_sampler_run(int dtype, const qes_sampler_config* cfg, const v
   if (dtype == QES_DTYPE_F32)
     return launch_sampler<float>(mpl, 64, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j, pairCt,
                                  pairSt, chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi,
-                                 last_logpsi, st);
+                                 last_logpsi, chain_beta, st);
   return launch_sampler<float2>(mpl, 16, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j, pairCt,
                                 pairSt, chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi,
-                                last_logpsi, st);
+                                last_logpsi, chain_beta, st);
+}
+
+extern "C" int qes_sampler_run(int dtype, const qes_sampler_config* cfg, const void* a, const void* b,
+                               const void* W, const void* flipCt, const void* flipSt, const int32_t* nbr_table,
+                               const int32_t* nbr_pair, const int32_t* pair_i, const int32_t* pair_j, int n_pairs,
+                               const void* pairCt, const void* pairSt, uint32_t* chain_bits, uint64_t* chain_step,
+                               int32_t* proposed, int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi,
+                               void* last_logpsi, void* stream) {
+  return sampler_run_impl(dtype, cfg, nullptr, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j, n_pairs,
+                          pairCt, pairSt, chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi,
+                          last_logpsi, stream);
+}
+
+extern "C" int qes_sampler_run_betas(int dtype, const qes_sampler_config* cfg, const float* chain_beta,
+                                     const void* a, const void* b, const void* W, const void* flipCt,
+                                     const void* flipSt, const int32_t* nbr_table, const int32_t* nbr_pair,
+                                     const int32_t* pair_i, const int32_t* pair_j, int n_pairs, const void* pairCt,
+                                     const void* pairSt, uint32_t* chain_bits, uint64_t* chain_step,
+                                     int32_t* proposed, int32_t* accepted, uint32_t* sample_bits,
+                                     void* sample_logpsi, void* last_logpsi, void* stream) {
+  QES_ARG_CHECK(chain_beta != nullptr, "qes_sampler_run_betas: null chain_beta");
+  return sampler_run_impl(dtype, cfg, chain_beta, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j,
+                          n_pairs, pairCt, pairSt, chain_bits, chain_step, proposed, accepted, sample_bits,
+                          sample_logpsi, last_logpsi, stream);
+}
+
+// ----------------------------------------------------------------------------
+// Parallel tempering: replica slots r = 0..R-1 of n_chains chains each (chain
+// index r * n_chains + c) carry beta labels; after each round adjacent slots
+// (r, r+1) with r % 2 == phase exchange labels per chain with probability
+// min(1, exp((beta_r - beta_r+1) mu (Re log psi_r+1 - Re log psi_r))).
+// The phase is one Philox draw per round (counter (round, 0, 0, 4)); the
+// uniform of pair r in chain c is counter (c, round, r, 5).
+// ----------------------------------------------------------------------------
+constexpr uint32_t QES_STREAM_PT_PHASE = 4, QES_STREAM_PT_SWAP = 5;
+
+template <class T>
+__global__ void pt_swap_kernel(int R, int n_chains, const T* __restrict__ logpsi, float* __restrict__ beta, float mu,
+                               uint32_t k0, uint32_t k1, int64_t round, int* __restrict__ swaps) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_chains) return;
+  const Philox4 ph = philox4x32_10((uint32_t)round, (uint32_t)(round >> 32), 0u, QES_STREAM_PT_PHASE, k0, k1);
+  const int phase = (int)(ph.x & 1u);
+  for (int r = phase; r + 1 < R; r += 2) {
+    const float bi = beta[(int64_t)r * n_chains + c], bj = beta[(int64_t)(r + 1) * n_chains + c];
+    const double li = (double)to_re(logpsi[(int64_t)r * n_chains + c]);
+    const double lj = (double)to_re(logpsi[(int64_t)(r + 1) * n_chains + c]);
+    const double log_acc = ((double)bi - (double)bj) * (double)mu * (lj - li);
+    const Philox4 u = philox4x32_10((uint32_t)c, (uint32_t)round, (uint32_t)r, QES_STREAM_PT_SWAP, k0, k1);
+    if (log((double)uniform_open(u.x)) < fmin(log_acc, 0.0)) {
+      beta[(int64_t)r * n_chains + c] = bj;
+      beta[(int64_t)(r + 1) * n_chains + c] = bi;
+      if (swaps) atomicAdd(&swaps[r], 1);
+    }
+  }
+}
+
+// copies, for every chain c, the slot whose beta equals target (the physical sector) to record row c
+template <class T>
+__global__ void pt_collect_kernel(int R, int n_chains, int nw, const float* __restrict__ beta, float target,
+                                  const uint32_t* __restrict__ chain_bits, const T* __restrict__ logpsi,
+                                  uint32_t* __restrict__ out_bits, T* __restrict__ out_logpsi) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_chains) return;
+  int slot = 0;
+  for (int r = R - 1; r >= 0; --r)
+    if (fabsf(beta[(int64_t)r * n_chains + c] - target) < 1e-5f) slot = r;   // first match
+  const int64_t src = (int64_t)slot * n_chains + c;
+  for (int q = 0; q < nw; ++q) out_bits[(int64_t)c * nw + q] = chain_bits[src * nw + q];
+  if (out_logpsi) out_logpsi[c] = logpsi[src];
+}
+
+extern "C" int qes_pt_swap(int dtype, int n_replicas, int n_chains, const void* logpsi, float* chain_beta, float mu,
+                           uint64_t seed, int64_t round, int* swaps_accepted, void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_pt_swap: bad dtype");
+  QES_ARG_CHECK(n_replicas >= 1 && n_chains >= 0 && round >= 0, "qes_pt_swap: bad sizes");
+  if (n_chains == 0 || n_replicas < 2) return QES_OK;
+  QES_ARG_CHECK(logpsi && chain_beta, "qes_pt_swap: null pointer");
+  const int bs = 128;
+  const uint32_t k0 = (uint32_t)(seed & 0xffffffffu), k1 = (uint32_t)(seed >> 32);
+  if (dtype == QES_DTYPE_F32)
+    pt_swap_kernel<float><<<(n_chains + bs - 1) / bs, bs, 0, (cudaStream_t)stream>>>(
+        n_replicas, n_chains, (const float*)logpsi, chain_beta, mu, k0, k1, round, swaps_accepted);
+  else
+    pt_swap_kernel<float2><<<(n_chains + bs - 1) / bs, bs, 0, (cudaStream_t)stream>>>(
+        n_replicas, n_chains, (const float2*)logpsi, chain_beta, mu, k0, k1, round, swaps_accepted);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+extern "C" int qes_pt_collect(int dtype, int n_replicas, int n_chains, int ns, const float* chain_beta,
+                              float target_beta, const uint32_t* chain_bits, const void* logpsi, uint32_t* out_bits,
+                              void* out_logpsi, void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_pt_collect: bad dtype");
+  QES_ARG_CHECK(n_replicas >= 1 && n_chains >= 0 && ns > 0, "qes_pt_collect: bad sizes");
+  if (n_chains == 0) return QES_OK;
+  QES_ARG_CHECK(chain_beta && chain_bits && logpsi && out_bits, "qes_pt_collect: null pointer");
+  const int bs = 128;
+  if (dtype == QES_DTYPE_F32)
+    pt_collect_kernel<float><<<(n_chains + bs - 1) / bs, bs, 0, (cudaStream_t)stream>>>(
+        n_replicas, n_chains, n_words(ns), chain_beta, target_beta, chain_bits, (const float*)logpsi, out_bits,
+        (float*)out_logpsi);
+  else
+    pt_collect_kernel<float2><<<(n_chains + bs - 1) / bs, bs, 0, (cudaStream_t)stream>>>(
+        n_replicas, n_chains, n_words(ns), chain_beta, target_beta, chain_bits, (const float2*)logpsi, out_bits,
+        (float2*)out_logpsi);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
 }
 
 // ----------------------------------------------------------------------------

@@ -260,7 +260,7 @@ def param_update(flat_params, master, x, lr):
 # --------------------------------------------------------------------------------------
 
 def sampler_run(flat_params, ns, nh, cfg: _lib.SamplerConfig, flip_tables, exch, chain_bits, chain_step, proposed,
-                accepted, sample_bits, sample_logpsi, last_logpsi):
+                accepted, sample_bits, sample_logpsi, last_logpsi, chain_beta=None):
     a, b, W = split_params(flat_params, ns, nh)
     fC, fS = flip_tables if flip_tables is not None else (None, None)
     if exch is not None:
@@ -269,6 +269,12 @@ def sampler_run(flat_params, ns, nh, cfg: _lib.SamplerConfig, flip_tables, exch,
     else:
         nbr = nbr_pair = pi = pj = pC = pS = None
         npairs = 0
+    if chain_beta is not None:
+        call("qes_sampler_run_betas", dtype_code(flat_params), C.byref(cfg), ptr(chain_beta), ptr(a), ptr(b), ptr(W),
+             ptr(fC), ptr(fS), ptr(nbr), ptr(nbr_pair), ptr(pi), ptr(pj), npairs, ptr(pC), ptr(pS), ptr(chain_bits),
+             ptr(chain_step), ptr(proposed), ptr(accepted), ptr(sample_bits), ptr(sample_logpsi), ptr(last_logpsi),
+             stream_ptr())
+        return
     call("qes_sampler_run", dtype_code(flat_params), C.byref(cfg), ptr(a), ptr(b), ptr(W), ptr(fC), ptr(fS),
          ptr(nbr), ptr(nbr_pair), ptr(pi), ptr(pj), npairs, ptr(pC), ptr(pS), ptr(chain_bits), ptr(chain_step),
          ptr(proposed), ptr(accepted), ptr(sample_bits), ptr(sample_logpsi), ptr(last_logpsi), stream_ptr())

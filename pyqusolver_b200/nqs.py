@@ -65,7 +65,7 @@ class NQSTrainStats:
 class NQS:
     def __init__(self, logansatz="rbm", model: SpinHamiltonian = None, hilbert=None, *, sampler="vmc",
                  batch_size=None, backend="cuda", dtype=np.complex64, param_dtype=None, seed=0, alpha=1.0,
-                 nparticles=None, device=None, verbose=False, **kwargs):
+                 nparticles=None, device=None, verbose=False, replica: int = 1, **kwargs):
         if model is None or not isinstance(model, SpinHamiltonian):
             raise TypeError("NQS on the GPU path needs a TransverseFieldIsing / XXZ / J1J2Model instance")
         self._model = model
@@ -90,7 +90,9 @@ class NQS:
             numsamples=kwargs.get("s_numsamples", 192), numchains=kwargs.get("s_numchains", 24),
             initstate=kwargs.get("s_initstate", None), logprob_fact=kwargs.get("s_logprob_fact", 0.5),
             n_particles=self._nparticles, lattice=getattr(model, "lattice", None),
-            recompute_every=kwargs.get("s_recompute_every", None))
+            recompute_every=kwargs.get("s_recompute_every", None),
+            # parallel tempering: `replica` slots on a geometric ladder, or an explicit `pt_betas`
+            pt_replicas=int(replica) if int(replica) > 1 else None, pt_betas=kwargs.get("pt_betas", None))
         self._lowered = model.lower()
         self._dev_ham = dv.DeviceHamiltonian(self._lowered, self._net.device)
         self._eloc_tables = None
@@ -125,6 +127,28 @@ class NQS:
     @property
     def num_params(self):
         return self._net.n_params
+
+    # ------------------------------------------------------------------ checkpoints
+    def save_checkpoint(self, directory, step, metadata=None, stats: Optional["NQSTrainStats"] = None):
+        """Flat float64/complex128 parameters + metadata (``NQSCheckpointManager`` layout of this package)."""
+        from .checkpoint import NQSCheckpointManager
+        meta = {"model": type(self._model).__name__, "ns": self._net.ns, "nh": self._net.nh,
+                "dtype": str(self._net.dtype), "seed": self._seed,
+                "sampler": {"numchains": self._sampler.numchains, "numsamples": self._sampler.numsamples,
+                            "rule": self._sampler._upd_rule_name}}
+        if stats is not None:
+            meta["history"] = [complex(h) for h in stats.history]
+            meta["history_std"] = list(stats.history_std)
+        meta.update(metadata or {})
+        params = {k: v.detach().cpu().numpy() for k, v in self._net.get_params().items()}
+        return NQSCheckpointManager(directory).save(step, params, meta)
+
+    def load_checkpoint(self, directory, step=None):
+        from .checkpoint import NQSCheckpointManager
+        mgr = NQSCheckpointManager(directory)
+        flat = mgr.load(step)
+        self._net.set_params(flat)
+        return mgr.load_metadata(step)
 
     # ------------------------------------------------------------------ evaluation
     def ansatz(self, states):
@@ -195,7 +219,7 @@ class NQS:
               num_samples=None, num_chains=None, num_thermal=None, num_sweep=None, lr=1e-2, use_sr=True,
               use_minsr=False, rhs_prefactor=-1.0, diag_shift=1e-3, exact_predictions=None, upd_fun=None,
               sr_tol=1e-8, sr_maxiter=1000, grad_clip=None, reset_stats=True, use_pbar=False, callback=None,
-              **kwargs) -> NQSTrainStats:
+              pt_betas=None, **kwargs) -> NQSTrainStats:
         if upd_fun is not None and str(upd_fun).upper() != self._sampler._upd_rule_name:
             raise ValueError("change the update rule at construction (s_upd_fun)")
         if num_chains is not None:
@@ -204,6 +228,8 @@ class NQS:
             self._sampler._sweep_steps = int(num_sweep)
         if num_thermal is not None:
             self._sampler._therm_steps = int(num_thermal)
+        if pt_betas is not None:
+            self._sampler.set_pt_betas(pt_betas)
         self._tdvp = TDVP(use_sr=use_sr, use_minsr=use_minsr, rhs_prefactor=rhs_prefactor, sr_lin_solver=lin_solver,
                           sr_diag_shift=diag_shift, sr_tol=sr_tol, sr_maxiter=sr_maxiter, grad_clip=grad_clip)
         stats = NQSTrainStats(seed=self._seed)

@@ -34,7 +34,8 @@ class VMCSampler:
     def __init__(self, net, shape, *, rng=None, rng_k=None, upd_fun=None, mu=2.0, beta=1.0, therm_steps=None,
                  sweep_steps=None, seed=None, hilbert=None, numsamples=1, numchains=1, numupd=1, initstate=None,
                  backend="default", logprob_fact=0.5, statetype=np.float32, n_particles=None, lattice=None,
-                 recompute_every=None, exchange_order=1, chain_offset=0, **kwargs):
+                 recompute_every=None, exchange_order=1, chain_offset=0, pt_betas=None, pt_replicas=None,
+                 **kwargs):
         if net is None:
             raise ValueError("A network (or callable) must be provided for evaluation.")
         if not hasattr(net, "flat") or not hasattr(net, "nh"):
@@ -85,7 +86,13 @@ class VMCSampler:
             raise ValueError(f"initial state {initstate!r} is not supported")
         self._tables = None
         self._tables_version = -1
-        self.reset()
+        self._pt_betas = None
+        self._n_replicas = 1
+        self._pt_round = 0
+        if pt_betas is not None or (pt_replicas is not None and int(pt_replicas) > 1):
+            self.set_replicas(pt_betas, pt_replicas)
+        else:
+            self.reset()
 
     # ------------------------------------------------------------------ state
     def _build_exchange(self, nt):
@@ -115,13 +122,106 @@ class VMCSampler:
 
     def reset(self):
         net = self._net
-        self._states = dv.init_chains(self._init_kind, self._numchains, net.ns, self._seed, self._n_up,
-                                      self._chain_offset, net.device)
-        self._step = torch.zeros((self._numchains,), dtype=torch.int64, device=net.device)
-        self._num_proposed = torch.zeros((self._numchains,), dtype=torch.int32, device=net.device)
-        self._num_accepted = torch.zeros((self._numchains,), dtype=torch.int32, device=net.device)
+        R, nc = self._n_replicas, self._numchains
+        base = dv.init_chains(self._init_kind, nc, net.ns, self._seed, self._n_up, self._chain_offset, net.device)
+        # parallel tempering: every replica slot starts from the same base states (vmc.py:397-405)
+        self._states = base.repeat(R, 1).contiguous() if R > 1 else base
+        self._step = torch.zeros((R * nc,), dtype=torch.int64, device=net.device)
+        self._num_proposed = torch.zeros((R * nc,), dtype=torch.int32, device=net.device)
+        self._num_accepted = torch.zeros((R * nc,), dtype=torch.int32, device=net.device)
+        if R > 1:
+            b = torch.as_tensor(np.asarray(self._pt_betas, dtype=np.float32), device=net.device)
+            self._chain_beta = b[:, None].repeat(1, nc).reshape(-1).contiguous()
+            self._pt_swaps = torch.zeros((R,), dtype=torch.int32, device=net.device)
+        self._pt_round = 0
         self._logprobas = None
         self._needs_thermalization = True
+
+    # ------------------------------------------------------------------ parallel tempering
+    def set_replicas(self, betas=None, n_replicas=None, min_beta=None):
+        """Beta ladder of parallel tempering (``vmc.py:1880-1911``): an explicit descending ladder, or
+        ``n_replicas`` log-spaced values from the sampler's beta down to ``min_beta`` (beta / 10)."""
+        if betas is None and n_replicas is not None and int(n_replicas) > 1:
+            max_beta = float(self._beta)
+            min_beta = float(min_beta if min_beta is not None else max_beta / 10.0)
+            if max_beta <= 0.0 or min_beta <= 0.0:
+                raise ValueError("PT beta ladder values must be positive.")
+            betas = np.logspace(np.log10(max_beta), np.log10(min_beta), int(n_replicas))
+        elif betas is not None:
+            betas = np.asarray(betas, dtype=np.float64)
+            if betas.ndim != 1:
+                raise ValueError("PT beta ladder must be a one-dimensional array.")
+            if np.any(betas <= 0.0):
+                raise ValueError("PT beta ladder values must be positive.")
+            if betas.shape[0] <= 1:
+                betas = None
+        cur = self._pt_betas
+        if (cur is None and betas is None) or (cur is not None and betas is not None and len(cur) == len(betas)
+                                                and np.allclose(cur, betas)):
+            if not hasattr(self, "_states"):
+                self.reset()
+            return
+        self._pt_betas = betas
+        self._n_replicas = len(betas) if betas is not None else 1
+        self.reset()
+
+    set_pt_betas = set_replicas
+
+    @property
+    def is_pt(self):
+        return self._pt_betas is not None
+
+    @property
+    def n_replicas(self):
+        return self._n_replicas
+
+    @property
+    def pt_betas(self):
+        return None if self._pt_betas is None else np.asarray(self._pt_betas, dtype=np.float32)
+
+    @property
+    def chain_betas(self):
+        """Current beta label of every (slot, chain), shape (n_replicas, numchains)."""
+        if not self.is_pt:
+            return None
+        return self._chain_beta.view(self._n_replicas, self._numchains)
+
+    def _sample_bits_pt(self, num_samples, therm_steps):
+        net = self._net
+        R, nc = self._n_replicas, self._numchains
+        nw = dv.n_words(net.ns)
+        therm_updates = therm_steps * self._sweep_steps * net.ns if self._needs_thermalization else 0
+        n_therm = max(1, -(-therm_updates // self._sweep_steps))
+        flip, exch = self._sampler_tables()
+        cfg = _lib.SamplerConfig(self._rule, net.ns, net.nh, R * nc, self._chain_offset, 0, self._sweep_steps,
+                                 self._sweep_steps, self._recompute_every, self._mu, self._beta,
+                                 self._seed & (2 ** 64 - 1), self._deg if exch is not None else 0)
+        last_lp = torch.empty((R * nc,), dtype=net.dtype, device=net.device)
+        sample_bits = torch.empty((num_samples * nc, nw), dtype=torch.int32, device=net.device)
+        sample_lp = torch.empty((num_samples * nc,), dtype=net.dtype, device=net.device)
+        dc = dv.dtype_code(net.flat)
+        target = float(np.float32(self._pt_betas[0]))
+
+        def one_round():
+            dv.sampler_run(net.flat, net.ns, net.nh, cfg, flip, exch, self._states, self._step, self._num_proposed,
+                           self._num_accepted, None, None, last_lp, chain_beta=self._chain_beta)
+            _lib.call("qes_pt_swap", dc, R, nc, _lib.ptr(last_lp), _lib.ptr(self._chain_beta), float(self._mu),
+                      _lib.C.c_uint64(self._seed & (2 ** 64 - 1)), int(self._pt_round), _lib.ptr(self._pt_swaps),
+                      _lib.stream_ptr())
+            self._pt_round += 1
+
+        for _ in range(n_therm):
+            one_round()
+        for k in range(num_samples):
+            one_round()
+            _lib.call("qes_pt_collect", dc, R, nc, net.ns, _lib.ptr(self._chain_beta), target, _lib.ptr(self._states),
+                      _lib.ptr(last_lp), _lib.ptr(sample_bits[k * nc:(k + 1) * nc]),
+                      _lib.ptr(sample_lp[k * nc:(k + 1) * nc]), _lib.stream_ptr())
+        self._needs_thermalization = False
+        self._logprobas = last_lp
+        self.last_sample_bits = sample_bits
+        self.last_sample_logpsi = sample_lp
+        return sample_bits, sample_lp
 
     def _sampler_tables(self):
         net = self._net
@@ -166,8 +266,12 @@ class VMCSampler:
         return (self._num_accepted.to(torch.float64) / torch.clamp(p, min=1.0))
 
     @property
+    def _phys_beta(self):
+        return float(self._pt_betas[0]) if self._pt_betas is not None else self._beta
+
+    @property
     def has_uniform_weights(self):
-        return (1.0 / self._logprob_fact - self._mu * self._beta) == 0.0
+        return (1.0 / self._logprob_fact - self._mu * self._phys_beta) == 0.0
 
     def set_numchains(self, n):
         if int(n) != self._numchains:
@@ -183,6 +287,8 @@ class VMCSampler:
         net = self._net
         ns_ = self._numsamples if num_samples is None else int(num_samples)
         therm = self._therm_steps if num_therm is None else int(num_therm)
+        if self.is_pt:
+            return self._sample_bits_pt(ns_, therm)
         therm_total = therm * self._sweep_steps * net.ns if self._needs_thermalization else 0
         nc = self._numchains
         nw = dv.n_words(net.ns)
@@ -203,7 +309,7 @@ class VMCSampler:
 
     def sample(self, parameters=None, num_samples=None, *, num_chains=None, num_therm=None, betas=None):
         if betas is not None:
-            raise NotImplementedError("parallel tempering is not part of the GPU sampler")
+            self.set_replicas(betas)
         if parameters is not None:
             self._net.set_params(parameters)
         if num_chains is not None:
@@ -212,9 +318,12 @@ class VMCSampler:
         states = dv.unpack_states(bits, self._net.ns)
         probs = None
         if not self.has_uniform_weights:
-            exponent = 1.0 / self._logprob_fact - self._mu * self._beta
+            exponent = 1.0 / self._logprob_fact - self._mu * self._phys_beta
             lu = exponent * lp.real.to(torch.float64)
             pr = torch.exp(lu - lu.max())
             probs = (pr / torch.clamp(pr.sum(), min=1e-10) * lp.shape[0]).to(torch.float32)
-        last = (dv.unpack_states(self._states, self._net.ns), self._logprobas)
+        last_states = dv.unpack_states(self._states, self._net.ns)
+        if self.is_pt:
+            last_states = last_states.view(self._n_replicas, self._numchains, self._net.ns)
+        last = (last_states, self._logprobas)
         return last, (states, lp), probs

@@ -444,3 +444,51 @@ def test_torch_ops_match_direct_calls():
                           dv.logpsi_vjp(net.flat, ns, nh, bits, tn, g), rtol=1e-12, atol=1e-12)
     st = torch.ops.qes_b200.loss_stats(lp.to(torch.complex64))
     assert st.shape == (4,) and st.dtype == torch.float64
+
+
+# ------------------------------------------------------------------------- parallel tempering
+@pytest.mark.parametrize("rule", ["LOCAL", "EXCHANGE"])
+def test_parallel_tempering_matches_oracle(rule):
+    L, OL = qb.SquareLattice(2, 4, 4), olat.SquareLattice(2, 4, 4)
+    ns, C, betas = 16, 64, [1.0, 0.6, 0.35, 0.2]
+    net = RBM((ns,), n_hidden=32, dtype="complex64", seed=61, init_scale=0.3)
+    init, n_up = ("RND_FIXED", 8) if rule == "EXCHANGE" else (None, None)
+    smp = VMCSampler(net, (ns,), upd_fun=rule, seed=9, therm_steps=1, sweep_steps=5, numchains=C, numsamples=1,
+                     lattice=L, initstate=init, n_particles=n_up, pt_betas=betas)
+    assert smp.is_pt and smp.n_replicas == 4
+    bits, lp = smp.sample_bits(num_samples=4)
+    got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
+    ref = osm.ParallelTemperingSampler(ns, C, betas, rule=rule, neighbor_table=olat.neighbor_table(OL), seed=9,
+                                       therm_steps=1, sweep_steps=5, init=init or "RND", n_up=n_up)
+    cfg, lp_ref, _ = ref.sample(oracle_params(net), 4)
+    assert np.mean(np.any(got != cfg, axis=1)) <= 0.03
+    gb = smp.chain_betas.cpu().numpy().astype(np.float64)
+    assert np.mean(np.any(gb != ref.betas, axis=0)) <= 0.05
+    assert smp._pt_round == ref.round
+
+
+def test_parallel_tempering_ladder_and_weights():
+    net = RBM((4,), n_hidden=3, dtype="float32", seed=37)
+    smp = VMCSampler(net, (4,), seed=5, therm_steps=1, sweep_steps=1, numchains=2, numsamples=1, beta=0.8)
+    smp.set_replicas(None, n_replicas=3)
+    b = smp.pt_betas
+    assert b[0] == pytest.approx(0.8) and b[-1] == pytest.approx(0.08)
+    smp2 = VMCSampler(net, (4,), seed=5, therm_steps=1, sweep_steps=1, numchains=2, numsamples=1)
+    smp2.set_pt_betas([1.0, 0.5, 0.25])
+    assert smp2.is_pt and smp2.n_replicas == 3
+    (last, _), _, probs = smp2.sample()
+    assert tuple(last.shape) == (3, 2, 4)
+    assert smp2.has_uniform_weights and probs is None
+
+
+def test_parallel_tempering_matches_exact_distribution():
+    ns = 10
+    net = RBM((ns,), n_hidden=10, dtype="complex64", seed=12, init_scale=0.4)
+    smp = VMCSampler(net, (ns,), seed=3, therm_steps=20, sweep_steps=20, numchains=2048, numsamples=1,
+                     pt_betas=[1.0, 0.5, 0.25])
+    bits, _ = smp.sample_bits(num_samples=40)
+    st = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
+    ints = ((st > 0).astype(np.int64) * (1 << np.arange(ns - 1, -1, -1))).sum(1)
+    basis, w = osm.exact_distribution(oracle_params(net), ns)
+    hist = np.bincount(ints, minlength=1 << ns)[basis] / len(ints)
+    assert 0.5 * np.abs(hist - w).sum() < 0.03

@@ -158,3 +158,20 @@ def test_torch_ops_are_registered():
     import pyqusolver_b200.ops  # noqa: F401  (registration only; no GPU call)
     for name in ("rbm_forward", "log_derivatives", "logpsi_vjp", "sr_matvec", "sr_solve_cg", "loss_stats"):
         assert hasattr(torch.ops.qes_b200, name)
+
+
+def test_checkpoint_manager_roundtrip(tmp_path):
+    from pyqusolver_b200.checkpoint import NQSCheckpointManager
+    mgr = NQSCheckpointManager(tmp_path, max_to_keep=2)
+    rng = np.random.default_rng(0)
+    params = {"visible_bias": rng.normal(size=4) + 1j, "hidden_bias": rng.normal(size=8) + 0j,
+              "W": rng.normal(size=(4, 8)) - 2j}
+    for step in (1, 2, 3):
+        mgr.save(step, params, {"energy": complex(-1.5, 0.0), "lr": 0.01})
+    assert mgr.list_checkpoints() == [2, 3]                 # max_to_keep prunes the oldest
+    assert mgr.latest_step() == 3
+    flat = mgr.load()
+    ref = np.concatenate([params["visible_bias"], params["hidden_bias"], params["W"].reshape(-1)])
+    assert flat.dtype == np.complex128 and np.array_equal(flat, ref)
+    meta = mgr.load_metadata(3)
+    assert meta["step"] == 3 and meta["lr"] == 0.01 and meta["energy"] == {"re": -1.5, "im": 0.0}

@@ -261,3 +261,19 @@ def test_oracle_sampler_matches_exact_distribution():
     hist = np.bincount(ints, minlength=64) / len(ints)
     tv = 0.5 * np.abs(hist - w).sum()
     assert tv < 0.05
+
+
+def test_oracle_parallel_tempering_samples_physical_distribution():
+    """Replica exchange keeps detailed balance: physical-slot samples follow |psi|^2."""
+    p = rbm.random_params(6, 6, complex_=True, scale=0.6, seed=13)
+    pt = osm.ParallelTemperingSampler(6, 256, [1.0, 0.5, 0.2], rule="LOCAL", seed=4, therm_steps=4, sweep_steps=6)
+    cfg, lp, probs = pt.sample(p, 40)
+    assert probs is None                               # 1/lpf - mu*beta_phys = 0 at beta = 1
+    assert cfg.shape == (40 * 256, 6)
+    assert pt.swaps.sum() > 0
+    ints = ((cfg > 0).astype(int) * (1 << np.arange(5, -1, -1))).sum(1)
+    basis, w = osm.exact_distribution(p, 6)
+    hist = np.bincount(ints, minlength=64) / len(ints)
+    assert 0.5 * np.abs(hist - w).sum() < 0.05
+    # every column holds each ladder value exactly once (labels are permuted, never lost)
+    assert np.all(np.sort(pt.betas, axis=0) == np.sort(pt.pt_betas)[:, None])

@@ -319,6 +319,24 @@ int qes_rbm_logpsi_vjp(int dtype, int ns, int nh, int64_t n_samples,
 int qes_param_update(int dtype, int64_t n_params, double lr, const void* x,
                      void* master, void* params, void* stream);
 
+/* MinSR (QES/NQS/src/tdvp.py:1199-1226, 1393-1408): solve
+ * (O_c O_c^H / Ns + shift) y = E_c / Ns by CG in sample space (float64,
+ * SciPy's stopping rule on that system) and return x = rhs_prefactor O_c^H y
+ * (length P).  Matrix-free: each iteration applies O_c^H then O_c with the
+ * kernels of qes_sr_matvec (tensor cores under qes_set_sr_impl as there).
+ * Workspace from qes_sr_minsr_workspace_bytes.                             */
+int qes_sr_minsr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
+int qes_sr_solve_minsr(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                       const void* tanh_theta, const void* eloc, const qes_sr_options* opt,
+                       void* x_out, qes_sr_result* result, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/* Replica swap of the sites in mask_words (packed like a configuration) between
+ * two sample batches: out_a = (a outside A, b inside A), out_b the opposite.
+ * The Renyi-2 swap estimator of QES/NQS/src/nqs_entropy.py:311-460.        */
+int qes_swap_region(int64_t n_samples, int ns, const uint32_t* mask_words, const uint32_t* bits_a,
+                    const uint32_t* bits_b, uint32_t* out_a, uint32_t* out_b, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Exact ground energy (the ED reference of the energy-error metric): Lanczos
  * over the full 2^ns S^z product basis (ns <= 32; basis bit i = site i,

@@ -119,8 +119,12 @@ SIGNATURES = {
     "qes_sr_matvec": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.c_double, _vp, _vp, _vp, _sz, _vp],
     "qes_sr_solve_cg": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
                         C.POINTER(SRResult), _vp, _sz, _vp],
+    "qes_sr_minsr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
+    "qes_sr_solve_minsr": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
+                           C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_rbm_logpsi_vjp": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_param_update": [C.c_int, _i64, C.c_double, _vp, _vp, _vp, _vp],
+    "qes_swap_region": [_i64, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp],
     "qes_ed_workspace_bytes": [C.c_int, C.POINTER(_sz)],
     "qes_ed_matvec": [C.c_int, C.POINTER(Hamiltonian), _vp, _vp, _vp],
     "qes_ed_lanczos": [C.c_int, C.POINTER(Hamiltonian), C.c_int, C.c_double, _u64, C.POINTER(C.c_double),

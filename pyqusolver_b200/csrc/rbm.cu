@@ -529,3 +529,32 @@ extern "C" int qes_batch_rbm_forward(int dtype, int n_inst, const qes_batch_inst
   QES_LAUNCH_CHECK();
   return QES_OK;
 }
+
+// ----------------------------------------------------------------------------
+// replica swap of a region (Renyi-2 estimator): out_a takes region A from b and
+// the rest from a, out_b the opposite (QES/NQS/src/nqs_entropy.py:311-460)
+// ----------------------------------------------------------------------------
+__global__ void swap_region_kernel(int64_t n_words_total, int nw, const uint32_t* __restrict__ mask,
+                                   const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                   uint32_t* __restrict__ oa, uint32_t* __restrict__ ob) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n_words_total;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t m = mask[k % nw], x = a[k], y = b[k];
+    oa[k] = (x & ~m) | (y & m);
+    ob[k] = (y & ~m) | (x & m);
+  }
+}
+
+extern "C" int qes_swap_region(int64_t n_samples, int ns, const uint32_t* mask_words, const uint32_t* bits_a,
+                               const uint32_t* bits_b, uint32_t* out_a, uint32_t* out_b, void* stream) {
+  QES_ARG_CHECK(n_samples >= 0 && ns > 0, "qes_swap_region: bad sizes");
+  if (n_samples == 0) return QES_OK;
+  QES_ARG_CHECK(mask_words && bits_a && bits_b && out_a && out_b, "qes_swap_region: null pointer");
+  const int nw = n_words(ns);
+  const int64_t total = n_samples * nw;
+  const int bs = 256;
+  const unsigned grid = (unsigned)std::min<int64_t>((total + bs - 1) / bs, 148 * 16);
+  swap_region_kernel<<<grid, bs, 0, (cudaStream_t)stream>>>(total, nw, mask_words, bits_a, bits_b, out_a, out_b);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}

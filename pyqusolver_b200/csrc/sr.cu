@@ -860,6 +860,233 @@ extern "C" int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples, con
 }
 
 // ----------------------------------------------------------------------------
+// MinSR (QES/NQS/src/tdvp.py:1199-1226, 1393-1408): solve (T + shift) y = E_c / Ns
+// in sample space, T = O_c O_c^H / Ns, and return x = O_c^H y.  Matrix-free with
+// the same two contractions in the opposite order: T y = (O g - mean(O g)) / Ns
+// with g = O^H (y - mean y).  CG in float64 over Ns-vectors; by the
+// push-through identity x equals the parameter-space SR solution.
+// ----------------------------------------------------------------------------
+// b_s = (E_s - mean E) / n  (real part for a real RBM)
+template <class V>
+__global__ void minsr_rhs_kernel(int64_t n, const float2* __restrict__ e, const double* __restrict__ mean,
+                                 V* __restrict__ b) {
+  const double mr = mean[0], mi = mean[1];
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    if constexpr (sizeof(V) == sizeof(double2)) {
+      V v; v.x = ((double)e[k].x - mr) / (double)n; v.y = ((double)e[k].y - mi) / (double)n;
+      b[k] = v;
+    } else {
+      b[k] = ((double)e[k].x - mr) / (double)n;
+    }
+  }
+}
+
+// float32 copy of an Ns-vector (input of the O^H u stage)
+template <class V>
+__global__ void vec_to_f2_kernel(int64_t n, const V* __restrict__ v, float2* __restrict__ out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    if constexpr (sizeof(V) == sizeof(double2)) out[k] = make_float2((float)v[k].x, (float)v[k].y);
+    else out[k] = make_float2((float)v[k], 0.f);
+  }
+}
+
+// Ap = (w - mean w) / n + shift p ; dot partials of p^H Ap, last block: pAp, alpha
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) minsr_ap_kernel(int64_t n, const float2* __restrict__ w,
+                                                              const double* __restrict__ wmean, double shift,
+                                                              const V* __restrict__ p, V* __restrict__ Ap,
+                                                              double* __restrict__ dot_part, double* __restrict__ scal,
+                                                              unsigned int* __restrict__ counter) {
+  const double mr = wmean[0], mi = wmean[1];
+  double d = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    V a;
+    if constexpr (sizeof(V) == sizeof(double2)) {
+      a.x = ((double)w[k].x - mr) / (double)n + shift * p[k].x;
+      a.y = ((double)w[k].y - mi) / (double)n + shift * p[k].y;
+    } else {
+      a = ((double)w[k].x - mr) / (double)n + shift * p[k];
+    }
+    Ap[k] = a;
+    d += vdotc(p[k], a);
+  }
+  __shared__ double red[RED_THREADS / 32];
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) t += red[q];
+    dot_part[blockIdx.x] = t;
+  }
+  __shared__ bool last;
+  __threadfence();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) v += ((volatile double*)dot_part)[q];
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double pap = 0.0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) pap += red[q];
+    scal[1] = pap;
+    scal[7] = (scal[4] == 0.0 && pap > 0.0) ? scal[0] / pap : 0.0;
+    *counter = 0u;
+  }
+}
+
+struct MinSRWork {
+  float2* uf;      // [Ns] float32 copy of the sample-space vector
+  double* umean;   // [2]
+  void* g;         // [P] of V
+  void *y, *r, *p, *Ap, *b;   // [Ns] of V each
+};
+
+static size_t minsr_layout(int dtype, int ns, int nh, int64_t n, char* base, MinSRWork* M) {
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  const size_t vs = (dtype == QES_DTYPE_C64) ? sizeof(double2) : sizeof(double);
+  const size_t head = sr_layout(dtype, ns, nh, n, nullptr).total;
+  size_t off = head;
+  auto take = [&](size_t bytes) { char* q = base ? base + off : nullptr; off += align256(bytes); return q; };
+  MinSRWork W;
+  W.uf = (float2*)take((size_t)n * sizeof(float2));
+  W.umean = (double*)take(4 * sizeof(double));
+  W.g = take((size_t)P * vs);
+  W.y = take((size_t)n * vs);
+  W.r = take((size_t)n * vs);
+  W.p = take((size_t)n * vs);
+  W.Ap = take((size_t)n * vs);
+  W.b = take((size_t)n * vs);
+  if (M) *M = W;
+  return off;
+}
+
+extern "C" int qes_sr_minsr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes) {
+  QES_ARG_CHECK(bytes && ns > 0 && nh > 0 && n_samples > 0, "qes_sr_minsr_workspace_bytes: bad args");
+  *bytes = minsr_layout(dtype, ns, nh, n_samples, nullptr, nullptr);
+  return QES_OK;
+}
+
+// g = O^H (u - mean u) for a sample-space float64 vector u (tensor cores or CUDA cores)
+template <class T>
+static int minsr_ohu(int ns, int nh, int64_t n, const uint32_t* bits, const T* tt, const typename VecT<T>::type* u,
+                     typename VecT<T>::type* g, const SRWork& L, const MinSRWork& M, cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  vec_to_f2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, u, M.uf);
+  mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n, M.uf, M.umean);
+  QES_LAUNCH_CHECK_N(2);
+  if (L.tc) {
+    const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
+    int rc = tc_ohu(dtype, L.td, n, M.uf, (const double2*)M.umean, -1, 1.0, L.partial, L.tw, st);
+    if (rc) return rc;
+    const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+    reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, L.nsplit, (const T*)L.partial, 0.0,
+                                                                              nullptr, g, nullptr, nullptr, nullptr);
+    QES_LAUNCH_CHECK();
+    return QES_OK;
+  }
+  return apply_ohu<T, V>(ns, nh, n, bits, tt, M.uf, M.umean, 1.0, L, 0.0, nullptr, g, nullptr, st);
+}
+
+template <class T>
+static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* tt, const float2* eloc,
+                      const qes_sr_options* opt, typename VecT<T>::type* x_out, qes_sr_result* res, const SRWork& L,
+                      const MinSRWork& M, cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  V* y = (V*)M.y; V* r = (V*)M.r; V* p = (V*)M.p; V* Ap = (V*)M.Ap; V* b = (V*)M.b; V* g = (V*)M.g;
+  int rc = sr_prepare(dtype, n, bits, tt, L, st);
+  if (rc) return rc;
+  mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n, eloc, L.wmean);
+  minsr_rhs_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, eloc, L.wmean, b);
+  QES_LAUNCH_CHECK_N(2);
+  double emean[2] = {0, 0};
+  QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 4 * sizeof(unsigned int), st));
+  cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, b, y, r, p);
+  norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, b, L.parts);
+  cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
+  QES_LAUNCH_CHECK_N(3);
+  const int check = opt->check_every > 0 ? opt->check_every : 8;
+  double hs[8] = {0};
+  QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaStreamSynchronize(st));
+  bool done = hs[4] != 0.0;
+  int it = 0;
+  while (!done && it < opt->maxiter) {
+    const int nrun = std::min(check, opt->maxiter - it);
+    for (int q = 0; q < nrun; ++q) {
+      if ((rc = minsr_ohu<T>(ns, nh, n, bits, tt, p, g, L, M, st))) return rc;       // g = O_c^H p
+      if (L.tc) {                                                                     // w = O g
+        if ((rc = tc_ov(dtype, L.td, n, bits, g, L.w, L.tw, st))) return rc;
+      } else {
+        const int nw = n_words(ns);
+        ov_kernel<T, V><<<(unsigned)((n + OV_SB - 1) / OV_SB), OV_THREADS, (size_t)OV_SB * nw * sizeof(uint32_t), st>>>(
+            ns, nh, n, bits, tt, g, L.w);
+        QES_LAUNCH_CHECK();
+      }
+      mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n, L.w, L.wmean);
+      minsr_ap_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, L.w, L.wmean, opt->shift, p, Ap, L.parts, L.scal,
+                                                             L.counter);
+      cg_xr_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, p, Ap, y, r, L.scal, L.parts, L.counter + 1);
+      cg_p_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, r, p, L.scal, L.td, nullptr);
+      QES_LAUNCH_CHECK_N(4);
+    }
+    it += nrun;
+    QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if ((rc = sr_check_status(L, st))) return rc;
+    done = hs[4] != 0.0;
+  }
+  // x = rhs_prefactor * O_c^H y
+  if ((rc = minsr_ohu<T>(ns, nh, n, bits, tt, y, x_out, L, M, st))) return rc;
+  if (opt->rhs_prefactor != 1.0) {
+    scale_vec_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, opt->rhs_prefactor, x_out);
+    QES_LAUNCH_CHECK();
+  }
+  if ((rc = sr_check_status(L, st))) return rc;
+  if (res) {
+    res->iterations = (int)hs[5];
+    res->converged = done ? 1 : 0;
+    res->residual = sqrt(hs[4] != 0.0 ? hs[2] : hs[0]);
+    res->rhs_norm = sqrt(hs[6]);
+    res->e_mean_re = emean[0];
+    res->e_mean_im = emean[1];
+  }
+  return done ? QES_OK : QES_ERR_NOT_CONVERGED;
+}
+
+extern "C" int qes_sr_solve_minsr(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                  const void* tanh_theta, const void* eloc, const qes_sr_options* opt, void* x_out,
+                                  qes_sr_result* result, void* workspace, size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && eloc && opt && x_out,
+                "qes_sr_solve_minsr: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_solve_minsr: bad dtype");
+  QES_ARG_CHECK(opt->maxiter >= 0 && opt->shift >= 0.0, "qes_sr_solve_minsr: bad options");
+  SRWork L;
+  int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
+  if (rc) return rc;
+  const size_t need = minsr_layout(dtype, ns, nh, n_samples, nullptr, nullptr);
+  if (workspace_bytes < need) {
+    qes_set_last_message("qes_sr_solve_minsr: workspace too small");
+    return QES_ERR_WORKSPACE;
+  }
+  MinSRWork M;
+  minsr_layout(dtype, ns, nh, n_samples, (char*)workspace, &M);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return sr_minsr_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc, opt,
+                             (double*)x_out, result, L, M, st);
+  return sr_minsr_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc, opt,
+                            (double2*)x_out, result, L, M, st);
+}
+
+// ----------------------------------------------------------------------------
 // vector-Jacobian product of log psi:  grad = O^H g  (no centring, no 1/Ns)
 // ----------------------------------------------------------------------------
 template <class T>

@@ -1024,6 +1024,27 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
   return QES_OK;
 }
 
+template <class T, class V>
+static int tc_ov_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const V* v, float2* w_out,
+                   const TcWork& w, cudaStream_t st) {
+  const bool cplx = ScalarTraits<T>::is_complex;
+  const int items = d.NB * (d.Kd / 8);
+  tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
+  QES_LAUNCH_CHECK();
+  const int pf = qes_prof_begin(QES_PROF_OV, st);
+  tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
+                                                           w.status);
+  QES_LAUNCH_CHECK();
+  qes_prof_end(pf, st);
+  return QES_OK;
+}
+
+int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
+          const TcWork& w, cudaStream_t st) {
+  if (dtype == QES_DTYPE_C64) return tc_ov_t<float2, double2>(d, n_samples, bits, (const double2*)v, w_out, w, st);
+  return tc_ov_t<float, double>(d, n_samples, bits, (const double*)v, w_out, w, st);
+}
+
 int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
               void* partial, const TcWork& w, cudaStream_t st, bool build_vp) {
   if (dtype == QES_DTYPE_C64)

@@ -48,6 +48,9 @@ int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_
 // w_out = O v, partial[chunk] = O^H ((w - mean w) / Ns)
 int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
               void* partial, const TcWork& w, cudaStream_t st, bool build_vp = true);
+// w_out = O v only (builds the V' operand from v first)
+int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
+          const TcWork& w, cudaStream_t st);
 // partial[chunk] = O^H ((g - mean) * scale): gsum_n > 0 -> gsum_part holds gsum_n partial sums
 // (mean = sum / Ns); gsum_n < 0 -> gsum_part[0] is the mean; gsum_part == nullptr -> no centring
 int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,

@@ -238,6 +238,26 @@ def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8
     return x, info
 
 
+def sr_solve_minsr(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
+                   check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True):
+    """MinSR: x = rhs_prefactor * O_c^H y with (O_c O_c^H / Ns + shift) y = E_c / Ns (sample-space CG)."""
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    nb = C.c_size_t(0)
+    call("qes_sr_minsr_workspace_bytes", dc, ns, nh, n, C.byref(nb))
+    ws = workspace if workspace is not None and workspace.numel() >= nb.value else torch.empty(
+        (int(nb.value),), dtype=torch.uint8, device=bits.device)
+    x = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor))
+    res = _lib.SRResult()
+    allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_converged else ()
+    call("qes_sr_solve_minsr", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), C.byref(opt), ptr(x),
+         C.byref(res), ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
+    info = {"iterations": res.iterations, "converged": bool(res.converged), "residual": res.residual,
+            "rhs_norm": res.rhs_norm, "e_mean": complex(res.e_mean_re, res.e_mean_im)}
+    return x, info, ws
+
+
 def logpsi_vjp(flat_params, ns, nh, bits, tanh_theta, g, workspace=None):
     """grad = O^H g (hand-written backward of log psi)."""
     dc = dtype_code(flat_params)

@@ -128,6 +128,58 @@ class NQS:
     def num_params(self):
         return self._net.n_params
 
+    # ------------------------------------------------------------------ overlaps and entropies
+    @staticmethod
+    def compute_overlap(nqs_a: "NQS", nqs_b: "NQS", *, num_samples: int = 4096, num_chains=None,
+                        operator=None, operator_args=None) -> float:
+        """F = |<A|B>|^2 / (<A|A><B|B>) = E_A[psi_B/psi_A] E_B[psi_A/psi_B] (``nqs.py:3819-3903``)."""
+        if nqs_a.net.ns != nqs_b.net.ns:
+            raise ValueError("NQS instances must have the same number of visible units to compute overlap.")
+        if operator is not None:
+            raise NotImplementedError("operator insertion is not part of the GPU path")
+
+        def log_mean_ratio(src, other):
+            bits, lp_src = src.sampler.sample_bits(num_samples)
+            _, _, lp_other = dv.rbm_forward(other.net.flat, other.net.ns, other.net.nh, bits, tanh=False)
+            lr = (lp_other.to(torch.complex128) - lp_src.to(torch.complex128))
+            return torch.logsumexp(lr, dim=0) - np.log(lr.shape[0])
+
+        lm = log_mean_ratio(nqs_a, nqs_b) + log_mean_ratio(nqs_b, nqs_a)
+        return float(torch.exp(lm).real.item())
+
+    @staticmethod
+    def compute_renyi2(nqs: "NQS", region=None, *, num_samples=None, num_chains=None, exact_sum=False,
+                       return_swap_mean=False, return_error=False, min_swap_value=1e-15):
+        """Second Renyi entropy of region A by the two-replica swap estimator
+        (``nqs.py:3905-3942`` -> ``nqs_entropy.py:311``): two successive sample batches of the sampler,
+        Tr rho_A^2 = mean[psi(A1,B0) psi(A0,B1) / (psi(A0,B0) psi(A1,B1))], S2 = -ln Tr rho_A^2."""
+        if exact_sum:
+            raise NotImplementedError("exact_sum: use the exact wavefunction on the host")
+        net = nqs.net
+        ns = net.ns
+        region = np.arange(ns // 2) if region is None else np.asarray(region, dtype=np.int64).reshape(-1)
+        mask = np.zeros(dv.n_words(ns), dtype=np.uint32)
+        for i in region:
+            mask[i >> 5] |= np.uint32(1) << np.uint32(i & 31)
+        mask_d = torch.as_tensor(mask.view(np.int32), device=net.device)
+        if num_chains is not None:
+            nqs.sampler.set_numchains(num_chains)
+        b0, _ = nqs.sampler.sample_bits(num_samples)
+        b0 = b0.clone()
+        b1, _ = nqs.sampler.sample_bits(num_samples)
+        sa, sb = torch.empty_like(b0), torch.empty_like(b0)
+        from . import _lib
+        _lib.call("qes_swap_region", int(b0.shape[0]), ns, _lib.ptr(mask_d), _lib.ptr(b0), _lib.ptr(b1),
+                  _lib.ptr(sa), _lib.ptr(sb), _lib.stream_ptr())
+        lp = lambda b: dv.rbm_forward(net.flat, ns, net.nh, b, tanh=False)[2].to(torch.complex128)
+        ratio = torch.exp(lp(sa) + lp(sb) - lp(b0) - lp(b1)).real
+        tr = float(ratio.mean().item())
+        err = float(ratio.std().item() / np.sqrt(ratio.numel()))
+        if return_swap_mean:
+            return (tr, err) if return_error else tr
+        s2 = -np.log(max(tr, min_swap_value))
+        return (s2, err / max(tr, min_swap_value)) if return_error else s2
+
     # ------------------------------------------------------------------ checkpoints
     def save_checkpoint(self, directory, step, metadata=None, stats: Optional["NQSTrainStats"] = None):
         """Flat float64/complex128 parameters + metadata (``NQSCheckpointManager`` layout of this package)."""

@@ -8,7 +8,10 @@ Mirrors ``QES/NQS/src/tdvp.py`` for the RBM path:
 * x <- rhs_prefactor * x (default -1), optional global-norm clip
   (``_finalize_solution`` ``:1410-1422``, ``_apply_grad_clip`` ``:882-907``);
 * ``use_sr=False`` returns x = -rhs_prefactor * F ... i.e. the reference's
-  ``-final_b`` branch (``solve`` ``:1561-1569``).
+  ``-final_b`` branch (``solve`` ``:1561-1569``);
+* ``use_minsr=True`` solves the sample-space system (O_c O_c^H / Ns + shift) y = E_c / Ns
+  and returns O_c^H y (``_solve_prepare_s_and_loss`` ``:1199-1226``, ``_project_minsr_result``
+  ``:1393-1408``), matrix-free on the same kernels.
 
 The solve runs on the GPU (``qes_sr_solve_cg``): the RBM's O is applied in
 structured form and never materialised, CG vectors and dots are float64.
@@ -36,13 +39,12 @@ class TDVP:
     def __init__(self, use_sr=True, use_minsr=False, rhs_prefactor=-1.0, sr_lin_solver="scipy_cg",
                  sr_diag_shift=1e-3, sr_tol=1e-8, sr_atol=0.0, sr_maxiter=1000, grad_clip=None,
                  check_every=16, **kwargs):
-        if use_minsr:
-            raise NotImplementedError("MinSR is not implemented on the GPU path")
         solver = str(sr_lin_solver).lower()
         if solver not in ("scipy_cg", "cg"):
             raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG")
         self.use_sr = bool(use_sr)
-        self.use_minsr = False
+        self.use_minsr = bool(use_minsr)
+        self._minsr_ws = None
         self.rhs_prefactor = float(rhs_prefactor)
         self.sr_diag_shift = float(sr_diag_shift)
         self.sr_tol = float(sr_tol)
@@ -74,6 +76,12 @@ class TDVP:
             F = dv.sr_force(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, workspace=ws)
             x = -(F * self.rhs_prefactor) if self.rhs_prefactor != 1.0 else -F
             self.last_info = {"iterations": 0, "converged": True, "residual": 0.0}
+        elif self.use_minsr:
+            x, info, self._minsr_ws = dv.sr_solve_minsr(
+                net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift, rtol=self.sr_tol,
+                atol=self.sr_atol, maxiter=self.sr_maxiter, check_every=self.check_every,
+                rhs_prefactor=self.rhs_prefactor, workspace=self._minsr_ws)
+            self.last_info = info
         else:
             x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
                                      rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,

@@ -239,6 +239,32 @@ def test_sr_force_matvec_and_cg_match_dense_oracle(cplx):
     assert rel_err(x.cpu().numpy(), xr) < 1e-3
 
 
+@pytest.mark.parametrize("cplx,impl", [(False, 1), (True, 1), (False, 0), (True, 0)])
+def test_minsr_matches_oracle_and_push_through(sr_impl, cplx, impl):
+    """MinSR (sample-space CG) against the oracle's dense MinSR solve and, by the push-through
+    identity, against the parameter-space SR solution of the same data."""
+    ns, nh, n = 9, 18, 400
+    model = qb.XXZ(qb.SquareLattice(2, 3, 3), jxy=-1.0, jz=-1.0, hx=0.4)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=16, init_scale=0.2)
+    st = rand_states(n, ns, seed=17)
+    bits = dv.pack_states(st)
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    e = eloc.cpu().numpy().astype(np.complex128)
+    if not cplx:
+        e = e.real
+    O = orbm.log_derivatives(oracle_params(net), orbm.to_sigma(st))
+    xr, _ = osr.solve_sr(e, O, shift=1e-2, use_minsr=True)
+    sr_impl(impl)
+    x, info, _ = dv.sr_solve_minsr(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-10, maxiter=3000)
+    assert info["converged"]
+    assert rel_err(x.cpu().numpy(), xr) < 1e-3
+    x_sr, _ = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-10, maxiter=3000)
+    assert rel_err(x.cpu().numpy(), x_sr.cpu().numpy()) < 1e-3
+
+
 # ------------------------------------------------------------------------- sampler
 def _gpu_sampler(net, rule, ns, chains, seed, therm, sweep, lattice=None, init=None, n_up=None):
     return VMCSampler(net, (ns,), upd_fun=rule, seed=seed, therm_steps=therm, sweep_steps=sweep, numchains=chains,

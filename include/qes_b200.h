@@ -281,6 +281,12 @@ int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int32_t* out, i
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);
+/* Keep the tensor-core operand tiles resident in L2 across CG iterations
+ * through a persisting access-policy window on the solve's streams (1; the
+ * window and the persisting lines are released after each solve) or not (0,
+ * the default: the tiles already stay in L2 between the iterations of the
+ * bench workloads).  Numerical results do not depend on it.               */
+int qes_set_l2_persist(int enable);
 
 /* Per-kernel CUDA-event timing of the SR matvec halves, for measurement:
  * while enabled, every launch of class k (0: O v, 1: O^H u, 2: split

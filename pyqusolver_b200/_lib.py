@@ -113,6 +113,7 @@ SIGNATURES = {
     "qes_sr_uses_tensor_cores": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(C.c_int)],
     "qes_sr_tc_plan": [C.c_int, C.c_int, C.c_int, _i64, _vp, C.c_int],
     "qes_set_cg_graphs": [C.c_int],
+    "qes_set_l2_persist": [C.c_int],
     "qes_profile_enable": [C.c_int],
     "qes_profile_read": [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int],
     "qes_sr_force": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],

@@ -705,7 +705,7 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
 
 namespace {
 struct CgGraphKey {
-  const void* bits; const void* tt; const void* ws; int64_t n; int ns, nh, dtype, chunk, tc;
+  const void* bits; const void* tt; const void* ws; int64_t n; int ns, nh, dtype, chunk, tc, l2;
   double shift;
   bool operator==(const CgGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
@@ -721,7 +721,46 @@ constexpr int kMaxGraphDevices = 64;
 std::mutex g_graph_mu;
 CgGraphSlot g_graph[kMaxGraphDevices];
 std::atomic<int> g_use_graphs{1};
+std::atomic<int> g_l2_persist{0};
+
+// L2 persistence of the tensor-core operands across the CG iterations: an access-policy window
+// over the BF16 tiles (T rows, T^T, Sigma^T, V') on the launching stream, sized to the device's
+// persisting-L2 limit; cleared (and the persisting lines released) after the solve.
+struct L2Props { bool init = false; size_t max_persist = 0, max_window = 0; };
+L2Props g_l2_props[kMaxGraphDevices];
+
+void l2_window(cudaStream_t st, int dev, const void* base, size_t bytes) {
+  if (dev < 0 || dev >= kMaxGraphDevices) return;
+  L2Props& pr = g_l2_props[dev];
+  if (!pr.init) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxPersistingL2CacheSize, dev) == cudaSuccess) pr.max_persist = (size_t)v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxAccessPolicyWindowSize, dev) == cudaSuccess) pr.max_window = (size_t)v;
+    pr.init = true;
+  }
+  if (pr.max_persist == 0 || pr.max_window == 0) return;
+  cudaStreamAttrValue a;
+  std::memset(&a, 0, sizeof(a));
+  if (bytes > 0) {
+    const size_t nb = std::min(bytes, pr.max_window);
+    const size_t lim = std::min(nb, pr.max_persist);
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim);
+    a.accessPolicyWindow.base_ptr = const_cast<void*>(base);
+    a.accessPolicyWindow.num_bytes = nb;
+    a.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)lim / (double)nb);
+    a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  }
+  cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &a);
+  if (bytes == 0) cudaCtxResetPersistingL2Cache();
+  cudaGetLastError();           // an unsupported policy leaves the solve unaffected
+}
 }  // namespace
+
+extern "C" int qes_set_l2_persist(int enable) {
+  g_l2_persist.store(enable ? 1 : 0);
+  return QES_OK;
+}
 
 extern long long qes_launch_count(int reset);
 void qes_count_launches(int n);
@@ -773,6 +812,12 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   int dev = 0;
   QES_CUDA_CHECK(cudaGetDevice(&dev));
   const bool graphs = g_use_graphs.load() != 0 && !qes_prof_on() && dev >= 0 && dev < kMaxGraphDevices;
+  const bool l2 = L.tc && g_l2_persist.load() != 0;
+  const size_t l2_bytes = l2 ? (size_t)((const char*)L.tw.wsum - (const char*)L.tw.t_rows) : 0;
+  if (l2) {
+    l2_window(st, dev, L.tw.t_rows, l2_bytes);
+    if (graphs && g_graph[dev].init) l2_window(g_graph[dev].cs, dev, L.tw.t_rows, l2_bytes);
+  }
   while (!done && it < opt->maxiter) {
     const int nrun = std::min(check, opt->maxiter - it);
     if (!graphs || it == 0 || nrun != check) {
@@ -786,9 +831,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         QES_CUDA_CHECK(cudaEventCreateWithFlags(&gs.ev_in, cudaEventDisableTiming));
         QES_CUDA_CHECK(cudaEventCreateWithFlags(&gs.ev_out, cudaEventDisableTiming));
         gs.init = true;
+        if (l2) l2_window(gs.cs, dev, L.tw.t_rows, l2_bytes);
       }
       const CgGraphKey key{bits, tt, L.w, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
-                           L.tc ? 1 : 0, opt->shift};
+                           L.tc ? 1 : 0, l2 ? 1 : 0, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {
           cudaGraphExecDestroy(gs.exec);
@@ -823,6 +869,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     rc = sr_check_status(L, st);          // synchronises the stream
     if (rc) return rc;
     done = hs[4] != 0.0;
+  }
+  if (l2) {
+    l2_window(st, dev, nullptr, 0);
+    if (graphs && g_graph[dev].init) l2_window(g_graph[dev].cs, dev, nullptr, 0);
   }
   // x_out = rhs_prefactor * x
   QES_CUDA_CHECK(cudaMemcpyAsync(x_out, x, P * sizeof(V), cudaMemcpyDeviceToDevice, st));

@@ -151,7 +151,8 @@ class NQS:
     def compute_renyi2(nqs: "NQS", region=None, *, num_samples=None, num_chains=None, exact_sum=False,
                        return_swap_mean=False, return_error=False, min_swap_value=1e-15):
         """Second Renyi entropy of region A by the two-replica swap estimator
-        (``nqs.py:3905-3942`` -> ``nqs_entropy.py:311``): two successive sample batches of the sampler,
+        (``nqs.py:3905-3942`` -> ``nqs_entropy.py:311``): two successive sample batches of the sampler
+        paired across different chains,
         Tr rho_A^2 = mean[psi(A1,B0) psi(A0,B1) / (psi(A0,B0) psi(A1,B1))], S2 = -ln Tr rho_A^2."""
         if exact_sum:
             raise NotImplementedError("exact_sum: use the exact wavefunction on the host")
@@ -167,6 +168,10 @@ class NQS:
         b0, _ = nqs.sampler.sample_bits(num_samples)
         b0 = b0.clone()
         b1, _ = nqs.sampler.sample_bits(num_samples)
+        # pair each row of the first batch with the next chain's row of the second batch, so that the two
+        # replicas come from different Markov chains (same-chain pairs a sweep apart are correlated and
+        # bias Tr rho_A^2 upwards)
+        b1 = torch.roll(b1, shifts=1, dims=0).contiguous()
         sa, sb = torch.empty_like(b0), torch.empty_like(b0)
         from . import _lib
         _lib.call("qes_swap_region", int(b0.shape[0]), ns, _lib.ptr(mask_d), _lib.ptr(b0), _lib.ptr(b1),

@@ -518,3 +518,38 @@ def test_parallel_tempering_matches_exact_distribution():
     basis, w = osm.exact_distribution(oracle_params(net), ns)
     hist = np.bincount(ints, minlength=1 << ns)[basis] / len(ints)
     assert 0.5 * np.abs(hist - w).sum() < 0.03
+
+
+# ------------------------------------------------------------------------- overlaps and Renyi-2
+def _exact_psi(net, ns):
+    basis = np.arange(1 << ns)
+    sig = np.where(((basis[:, None] >> np.arange(ns - 1, -1, -1)) & 1) == 1, 1.0, -1.0)
+    lp = orbm.log_psi(oracle_params(net), sig)
+    psi = np.exp(lp - np.max(np.real(lp)))
+    return psi / np.linalg.norm(psi)
+
+
+def test_renyi2_swap_estimator_matches_exact():
+    ns = 8
+    model = qb.TransverseFieldIsing(qb.SquareLattice(1, ns, 1, bc="pbc"), j=1.0, hx=1.0, hz=0.0)
+    nqs = qb.NQS("rbm", model, alpha=1, dtype="complex64", seed=3, s_upd_fun="LOCAL", s_numchains=1024,
+                 s_numsamples=16, s_sweep_steps=8, s_therm_steps=20, init_scale=0.5)
+    psi = _exact_psi(nqs.net, ns).reshape(1 << (ns // 2), 1 << (ns // 2))   # sites 0..3 = most significant bits
+    rho = psi @ psi.conj().T
+    s2_exact = -np.log(np.real(np.trace(rho @ rho)))
+    s2, err = qb.NQS.compute_renyi2(nqs, region=np.arange(ns // 2), return_error=True)
+    assert abs(s2 - s2_exact) < 5 * err + 0.02, (s2, s2_exact, err)
+
+
+def test_overlap_of_identical_and_different_states():
+    ns = 8
+    model = qb.TransverseFieldIsing(qb.SquareLattice(1, ns, 1, bc="pbc"), j=1.0, hx=1.0, hz=0.0)
+    kw = dict(alpha=1, dtype="complex64", s_upd_fun="LOCAL", s_numchains=1024, s_numsamples=8, s_sweep_steps=8,
+              s_therm_steps=20, init_scale=0.4)
+    a = qb.NQS("rbm", model, seed=4, **kw)
+    a2 = qb.NQS("rbm", model, seed=4, **kw)
+    assert qb.NQS.compute_overlap(a, a2, num_samples=8) == pytest.approx(1.0, abs=1e-4)
+    b = qb.NQS("rbm", model, seed=5, **kw)
+    f_exact = abs(np.vdot(_exact_psi(a.net, ns), _exact_psi(b.net, ns))) ** 2
+    f = qb.NQS.compute_overlap(a, b, num_samples=8)
+    assert abs(f - f_exact) < 0.05, (f, f_exact)

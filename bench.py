@@ -135,7 +135,7 @@ def timed_step(nqs, tdvp, cfg, ev):
     ev[0].record()
     bits, _ = nqs.sampler.sample_bits()
     ev[1].record()
-    _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+    _, tn, _ = dv.rbm_forward_step(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
     ev[2].record()
     eloc = nqs.local_energy_bits(bits, tn)
     ev[3].record()
@@ -256,8 +256,6 @@ def run_batch(args, cfg, rank, world, local_rank):
         dist.barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    _lib.profile_read(reset=True)
-    _lib.profile_enable(True)
     _lib.launch_count(reset=True)
     step_ms, phase_ms, cg = [], {p: [] for p in BATCH_PHASES}, []
     for _ in range(args.steps):
@@ -270,9 +268,19 @@ def run_batch(args, cfg, rank, world, local_rank):
             phase_ms[p].append(ev[k].elapsed_time(ev[k + 1]))
         cg.append(max(r.iterations for r in res))
     launches = _lib.launch_count(reset=True)
+    clk = clocks.stop()
+    # per-kernel CUDA-event timing for the roofline, in separate steps
+    _lib.profile_read(reset=True)
+    _lib.profile_enable(True)
+    prof_total = 0.0
+    for _ in range(min(args.steps, 3)):
+        flush.fill_(1.0)
+        ev = mk()
+        step(ev)
+        torch.cuda.synchronize()
+        prof_total += ev[0].elapsed_time(ev[6])
     prof = _lib.profile_read(reset=True)
     _lib.profile_enable(False)
-    clk = clocks.stop()
     total = float(np.sum(step_ms))
     if dist is not None:
         t = torch.tensor([total], dtype=torch.float64, device="cuda")
@@ -323,7 +331,7 @@ def run_batch(args, cfg, rank, world, local_rank):
     avg_s = cands[dom][0] / cands[dom][1] / 1e3
     ach = algo[dom] / avg_s / 1e9
     roof = {"kernel": names[dom], "launches_timed": cands[dom][1], "avg_launch_us": avg_s * 1e6,
-            "share_of_timed_region": cands[dom][0] / total, "bound": "hbm", "achieved": ach, "peak": hbm,
+            "share_of_timed_region": cands[dom][0] / prof_total, "bound": "hbm", "achieved": ach, "peak": hbm,
             "unit": "GB/s", "frac": ach / hbm, "algorithmic_bytes_per_launch": algo[dom],
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "traffic": json.load(open(os.path.join(ROOT, "profiles", "dram_traffic_per_launch.json"))).get(
@@ -410,13 +418,17 @@ def run_ours(args, cfg, rank, world, local_rank):
         clocks = ClockSampler(local_rank) if form == "mixed" else None
         if clocks:
             clocks.start()
-        step_ms, phase_ms, cg_iters, launches, prof = timed_loop(nqs, tdvp, cfg, args.steps, flush,
-                                                                 profile=(form == "mixed"))
+        step_ms, phase_ms, cg_iters, launches, _ = timed_loop(nqs, tdvp, cfg, args.steps, flush, profile=False)
         clk = clocks.stop() if clocks else None
         total_ms = max_over_ranks(float(np.sum(step_ms)))
+        prof = prof_phases = prof_iters = None
+        if form == "mixed":
+            # per-kernel CUDA-event timing (roofline) in separate steps: the event pairs and the graph-less CG
+            # they need would otherwise slow the timed steps
+            _, prof_phases, prof_iters, _, prof = timed_loop(nqs, tdvp, cfg, min(args.steps, 5), flush, profile=True)
         forms[form] = {"nqs": nqs, "tdvp": tdvp, "total_ms": total_ms, "phase_ms": phase_ms, "cg_iters": cg_iters,
-                       "launches": launches, "prof": prof, "clocks": clk,
-                       "energy": float(nqs_energy(tdvp.last_info))}
+                       "launches": launches, "prof": prof, "prof_phase_ms": prof_phases, "prof_cg_iters": prof_iters,
+                       "clocks": clk, "energy": float(nqs_energy(tdvp.last_info))}
     _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
     mixed = forms["mixed"]
     plain = forms.get("plain_fp32")
@@ -552,13 +564,14 @@ def roofline(cfg, nqs, form):
         traffic_db = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic_per_launch.json")))
     except (OSError, ValueError):
         pass
-    steps = len(form["cg_iters"])
+    phases = form.get("prof_phase_ms") or form["phase_ms"]
+    steps = len(form.get("prof_cg_iters") or form["cg_iters"])
     cands = {}
     for k, (ms, cnt) in (form["prof"] or {}).items():
         if cnt:
             cands[k] = (ms, cnt)
     for p in ("sample", "local_energy", "forward"):
-        cands[p] = (float(np.sum(form["phase_ms"][p])), steps)
+        cands[p] = (float(np.sum(phases[p])), steps)
     dom = max(cands, key=lambda k: cands[k][0])
     total_ms, cnt = cands[dom]
     avg_s = total_ms / cnt / 1e3
@@ -568,9 +581,10 @@ def roofline(cfg, nqs, form):
     names = {"ov": "tc_ov_kernel (O v, tcgen05)" if tc else "ov_kernel (O v, CUDA cores)",
              "ohu": "tc_ohu_kernel (O^H u, tcgen05)" if tc else "ohu_kernel (O^H u, CUDA cores)",
              "reduce": "reduce_splits_kernel", "sample": "sampler_kernel", "local_energy": "eloc_moves_kernel",
-             "forward": "rbm_forward_kernel"}
+             "forward": "theta_tc_kernel (tcgen05)" if dv.forward_uses_tensor_cores(
+                 net.flat, net.ns, net.nh, cfg["chains"] * cfg["samples"]) else "rbm_forward_kernel"}
     out = {"kernel": names.get(dom, dom), "launches_timed": cnt, "avg_launch_us": avg_s * 1e6,
-           "share_of_timed_region": total_ms / float(np.sum([np.sum(v) for v in form["phase_ms"].values()])),
+           "share_of_timed_region": total_ms / float(np.sum([np.sum(v) for v in phases.values()])),
            "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src}
     if dom in ("ov", "ohu", "reduce"):
         b = kernel_bytes(cfg, nqs, dom, tc=tc)

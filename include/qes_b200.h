@@ -278,9 +278,31 @@ int qes_sr_uses_tensor_cores(int dtype, int ns, int nh, int64_t n_samples, int* 
  * out = [uses, big, KC, n_chunks, nsplit, n_tiles, Kd, NB, Np, MT, NC, NR,
  * nnc, SPC, ov_stages] (first n_out entries).                              */
 int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int32_t* out, int n_out);
+/* Tiling of the tensor-core O^H u in this process: mode 0 = automatic (the
+ * single-M-tile kernel when the shapes allow it), 1 = single-M-tile kernel
+ * only, 2 = M/N-tiled kernel; nc = hidden units per N chunk (multiple of 16,
+ * 0 = largest that fits TMEM); ctas = target CTA count (0 = 296).          */
+int qes_sr_set_tiling(int mode, int nc, int ctas);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);
+/* The vector part of each CG iteration (split-partial reduction, x/r and
+ * direction updates) as one cooperative kernel with two bounded grid
+ * barriers: 2 = always, 1 = when its grid is at most 32 CTAs (the default:
+ * small parameter vectors, where launch latency dominates), 0 = never
+ * (three kernels).                                                         */
+int qes_set_cg_fused(int mode);
+
+/* RBM forward on the tensor cores: theta = Sigma W + b with W split into
+ * three BF16 terms (exact for float32 W) and float32 accumulation; outputs
+ * as qes_rbm_forward.  Workspace from qes_rbm_forward_tc_workspace_bytes
+ * (QES_ERR_SIZE when the shapes are outside its limits).  Replaces the
+ * network apply of QES/Solver/MonteCarlo/vmc.py:1113-1147 for a batch.      */
+int qes_rbm_forward_tc_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
+int qes_rbm_forward_tc(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                       const void* a, const void* b, const void* W, void* theta_out,
+                       void* tanh_out, void* logpsi_out, void* workspace, size_t workspace_bytes,
+                       void* stream);
 /* Keep the tensor-core operand tiles resident in L2 across CG iterations
  * through a persisting access-policy window on the solve's streams (1; the
  * window and the persisting lines are released after each solve) or not (0,

@@ -112,7 +112,11 @@ SIGNATURES = {
     "qes_set_sr_impl": [C.c_int],
     "qes_sr_uses_tensor_cores": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(C.c_int)],
     "qes_sr_tc_plan": [C.c_int, C.c_int, C.c_int, _i64, _vp, C.c_int],
+    "qes_sr_set_tiling": [C.c_int, C.c_int, C.c_int],
     "qes_set_cg_graphs": [C.c_int],
+    "qes_set_cg_fused": [C.c_int],
+    "qes_rbm_forward_tc_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
+    "qes_rbm_forward_tc": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_set_l2_persist": [C.c_int],
     "qes_profile_enable": [C.c_int],
     "qes_profile_read": [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int],
@@ -179,8 +183,18 @@ def call(name, *args, allow=()):
 SR_IMPL_AUTO, SR_IMPL_CUDA_CORES, SR_IMPL_TENSOR_CORES = 0, 1, 2
 
 
+_SR_IMPL = [0]
+
+
 def set_sr_impl(impl: int):
+    """0 = tensor cores where the shapes allow (mixed form), 1 = CUDA cores only (plain FP32 form), 2 = tensor
+    cores required.  Also selects the forward (theta) path used by the training step."""
     call("qes_set_sr_impl", int(impl))
+    _SR_IMPL[0] = int(impl)
+
+
+def sr_impl() -> int:
+    return _SR_IMPL[0]
 
 
 TC_PLAN_FIELDS = ("uses", "big", "KC", "n_chunks", "nsplit", "n_tiles", "Kd", "NB", "Np", "MT", "NC", "NR", "nnc",

@@ -464,6 +464,126 @@ __global__ void scale_vec_kernel(int64_t P, double s, V* __restrict__ x) {
 }
 
 // ----------------------------------------------------------------------------
+// One kernel for the vector part of a CG iteration: Ap = sum of the split
+// partials + shift p (pAp), alpha; x += alpha p, r -= alpha Ap (rr_new), beta;
+// p = r + beta p (+ the V' tiles of the tensor-core path).  The two global
+// dependencies are grid barriers of a cooperative launch (all CTAs resident);
+// each barrier wait is bounded and records a time-out in *err.
+// ----------------------------------------------------------------------------
+constexpr int CF_TX = 32, CF_TY = 16;            // 512 threads: 32 columns x 16 split groups
+constexpr uint32_t kGridBarLimit = 1u << 24;     // polls (with a short sleep) before giving up
+
+// count and gen live in different 128-byte lines; waiters poll gen with plain volatile loads so
+// that the arrivals (atomics on count) do not queue behind polling atomics
+__device__ __forceinline__ void grid_barrier(unsigned int* count, unsigned int* gen, unsigned int nb, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    volatile unsigned int* vgen = gen;
+    const unsigned int g = *vgen;
+    __threadfence();
+    if (atomicAdd(count, 1u) == nb - 1) {
+      *count = 0u;
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      uint32_t it = 0;
+      while (*vgen == g) {
+        if (++it > kGridBarLimit) { atomicExch(err, 1); break; }
+        __nanosleep(20);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int nsplit, const T* __restrict__ partial,
+                                                                 double shift, V* __restrict__ x, V* __restrict__ r,
+                                                                 V* __restrict__ p, V* __restrict__ Ap,
+                                                                 double* __restrict__ scal, double* __restrict__ part,
+                                                                 unsigned int* __restrict__ bar, int* __restrict__ err,
+                                                                 TcDims td, uint16_t* __restrict__ vp) {
+  const double rr = scal[0], thresh = scal[3];
+  if (scal[4] != 0.0) return;                      // converged: every CTA leaves (scal only changes below)
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CF_TX + tx;
+  const unsigned int nb = gridDim.x;
+  __shared__ V red[CF_TY][CF_TX];
+  __shared__ double sred[CF_TX * CF_TY / 32];
+  // phase 1: Ap and p^H Ap
+  double d = 0.0;
+  for (int64_t c0 = (int64_t)blockIdx.x * CF_TX; c0 < P; c0 += (int64_t)nb * CF_TX) {
+    const int64_t k = c0 + tx;
+    V g = vzero(V());
+    if (k < P) {
+#pragma unroll 4
+      for (int z = ty; z < nsplit; z += CF_TY) g = vadd(g, to_d(partial[(int64_t)z * P + k]));
+    }
+    red[ty][tx] = g;
+    __syncthreads();
+    if (ty == 0 && k < P) {
+      V t = red[0][tx];
+#pragma unroll
+      for (int q = 1; q < CF_TY; ++q) t = vadd(t, red[q][tx]);
+      const V pk = p[k];
+      t = vadd(t, vscale(shift, pk));
+      Ap[k] = t;
+      d += vdotc(pk, t);
+    }
+    __syncthreads();
+  }
+  auto block_sum = [&](double v) -> double {
+    v = warp_sum(v);
+    if ((tid & 31) == 0) sred[tid >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int q = 0; q < CF_TX * CF_TY / 32; ++q) t += sred[q];
+    __syncthreads();
+    return t;
+  };
+  d = block_sum(d);
+  if (tid == 0) part[blockIdx.x] = d;
+  grid_barrier(bar, bar + 32, nb, err);
+  double pap = 0.0;
+  for (unsigned int b = 0; b < nb; ++b) pap += ((volatile double*)part)[b];
+  const double alpha = (pap > 0.0) ? rr / pap : 0.0;
+  // phase 2: x, r and r^H r
+  double e = 0.0;
+  const int64_t stride = (int64_t)nb * CF_TX * CF_TY;
+  for (int64_t k = (int64_t)blockIdx.x * CF_TX * CF_TY + tid; k < P; k += stride) {
+    x[k] = vadd(x[k], vscale(alpha, p[k]));
+    const V rk = vadd(r[k], vscale(-alpha, Ap[k]));
+    r[k] = rk;
+    e += vdotc(rk, rk);
+  }
+  e = block_sum(e);
+  if (tid == 0) part[nb + blockIdx.x] = e;
+  grid_barrier(bar, bar + 32, nb, err);
+  double rr_new = 0.0;
+  for (unsigned int b = 0; b < nb; ++b) rr_new += ((volatile double*)part)[nb + b];
+  const double beta = (rr > 0.0) ? rr_new / rr : 0.0;
+  const bool conv = rr_new <= thresh;
+  // phase 3: direction update (same index map as phase 2: each thread updates what it wrote)
+  if (!conv) {
+    const int ns = td.ns, nh = td.nh;
+    for (int64_t k = (int64_t)blockIdx.x * CF_TX * CF_TY + tid; k < P; k += stride) {
+      const V pk = vadd(r[k], vscale(beta, p[k]));
+      p[k] = pk;
+      if (vp && k >= ns) {
+        const int64_t q = k - ns;
+        if (q < nh) tc_put_vp_elem(td, vp, ns, (int)q, pk);
+        else tc_put_vp_elem(td, vp, (int)((q - nh) / nh), (int)((q - nh) % nh), pk);
+      }
+    }
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    scal[1] = pap; scal[7] = alpha; scal[2] = rr_new; scal[8] = beta; scal[0] = rr_new;
+    scal[5] += 1.0;
+    if (conv) scal[4] = 1.0;
+  }
+}
+
+// ----------------------------------------------------------------------------
 // workspace layout
 // ----------------------------------------------------------------------------
 struct SRWork {
@@ -503,7 +623,7 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
   L.parts = (double*)take(std::max(RED_BLOCKS, RS_MAX_BLOCKS) * sizeof(double));
   L.scal = (double*)take(16 * sizeof(double));
-  L.counter = (unsigned int*)take(4 * sizeof(unsigned int));
+  L.counter = (unsigned int*)take(128 * sizeof(unsigned int));     // tickets, barrier words (own lines)
   char* tcb = tc_ok ? take(tc_workspace_bytes(L.td)) : nullptr;
   L.tw = (tc_ok && base) ? tc_layout(L.td, tcb) : TcWork{};
   L.total = off;
@@ -706,6 +826,7 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
 namespace {
 struct CgGraphKey {
   const void* bits; const void* tt; const void* ws; int64_t n; int ns, nh, dtype, chunk, tc, l2;
+  int big, kc, nsplit, nnc, nc, spc;      // tiling of the captured kernels
   double shift;
   bool operator==(const CgGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
@@ -722,6 +843,7 @@ std::mutex g_graph_mu;
 CgGraphSlot g_graph[kMaxGraphDevices];
 std::atomic<int> g_use_graphs{1};
 std::atomic<int> g_l2_persist{0};
+std::atomic<int> g_cg_fused{1};            // automatic
 
 // L2 persistence of the tensor-core operands across the CG iterations: an access-policy window
 // over the BF16 tiles (T rows, T^T, Sigma^T, V') on the launching stream, sized to the device's
@@ -757,6 +879,15 @@ void l2_window(cudaStream_t st, int dev, const void* base, size_t bytes) {
 }
 }  // namespace
 
+extern "C" int qes_set_cg_fused(int mode) {
+  if (mode < 0 || mode > 2) {
+    qes_set_last_message("qes_set_cg_fused: mode 0 (off), 1 (automatic) or 2 (always)");
+    return QES_ERR_ARG;
+  }
+  g_cg_fused.store(mode);
+  return QES_OK;
+}
+
 extern "C" int qes_set_l2_persist(int enable) {
   g_l2_persist.store(enable ? 1 : 0);
   return QES_OK;
@@ -785,7 +916,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   if (rc) return rc;
   double emean[2] = {0, 0};
   QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-  QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 4 * sizeof(unsigned int), st));
+  QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 128 * sizeof(unsigned int), st));
   cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p);
   norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
   cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
@@ -797,8 +928,56 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaStreamSynchronize(st));
   done = hs[4] != 0.0;
+  // fused vector kernel: always (2), never (0), or automatically (1) when its grid is small -- its two
+  // grid barriers cost more than the launches they save once the grid spans the GPU (measured)
+  const int fused_mode = g_cg_fused.load();
+  bool fused = fused_mode != 0;
+  int fused_grid = 0;
+  if (fused) {
+    int dv_ = 0, nsm = 0, per_sm = 0;
+    QES_CUDA_CHECK(cudaGetDevice(&dv_));
+    QES_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dv_));
+    QES_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fused_kernel<T, V>, CF_TX * CF_TY, 0));
+    fused_grid = (int)std::min<int64_t>((int64_t)nsm * std::max(per_sm, 1), std::min<int64_t>(RED_BLOCKS, (P + CF_TX - 1) / CF_TX));
+    fused_grid = std::max(fused_grid, 1);
+    if (fused_mode == 1 && fused_grid > 32) fused = false;
+  }
   auto run_direct = [&](int nrun, int it0) -> int {
     for (int q = 0; q < nrun; ++q) {
+      if (fused) {
+        // O v and O^H u (split partials), then the fused vector kernel
+        if (L.tc) {
+          const int dtype_ = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
+          int r2 = tc_matvec(dtype_, L.td, n_samples, bits, p, L.w, L.partial, L.tw, st, it0 + q == 0);
+          if (r2) return r2;
+        } else {
+          int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, st);
+          if (r2) return r2;
+          dim3 grid((nh + OHU_TM - 1) / OHU_TM, (ns + OHU_TI - 1) / OHU_TI, (unsigned)L.nsplit);
+          const int pf = qes_prof_begin(QES_PROF_OHU, st);
+          ohu_kernel<T><<<grid, dim3(OHU_TM, OHU_TY), 0, st>>>(ns, nh, n_samples, bits, tt, L.w, L.wmean,
+                                                             1.0 / (double)n_samples, (T*)L.partial);
+          QES_LAUNCH_CHECK();
+          qes_prof_end(pf, st);
+        }
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(fused_grid);
+        lc.blockDim = dim3(CF_TX, CF_TY);
+        lc.dynamicSmemBytes = 0;
+        lc.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
+        QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V>, P, L.nsplit, (const T*)L.partial, opt->shift,
+                                          x, r, p, Ap, L.scal, L.parts, L.counter + 32, (int*)(L.counter + 4), L.td,
+                                          L.tc ? L.tw.vp : (uint16_t*)nullptr));
+        qes_prof_end(pfr, st);
+        QES_LAUNCH_CHECK();
+        continue;
+      }
       int r2 = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, p, Ap, L.parts, L, st,
                               /*vp_ready=*/it0 + q > 0);
       if (r2) return r2;
@@ -834,7 +1013,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         if (l2) l2_window(gs.cs, dev, L.tw.t_rows, l2_bytes);
       }
       const CgGraphKey key{bits, tt, L.w, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
-                           L.tc ? 1 : 0, l2 ? 1 : 0, opt->shift};
+                           L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0), L.td.big ? 1 : 0, L.td.KC, L.nsplit,
+                           L.td.nnc, L.td.NC, L.td.SPC, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {
           cudaGraphExecDestroy(gs.exec);
@@ -873,6 +1053,17 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   if (l2) {
     l2_window(st, dev, nullptr, 0);
     if (graphs && g_graph[dev].init) l2_window(g_graph[dev].cs, dev, nullptr, 0);
+  }
+  // a bounded wait of the force pass must surface even when CG needed no iteration
+  if ((rc = sr_check_status(L, st))) return rc;
+  if (fused) {
+    int berr = 0;
+    QES_CUDA_CHECK(cudaMemcpyAsync(&berr, L.counter + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QES_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (berr) {
+      qes_set_last_message("SR CG: a bounded grid-barrier wait gave up");
+      return QES_ERR_TIMEOUT;
+    }
   }
   // x_out = rhs_prefactor * x
   QES_CUDA_CHECK(cudaMemcpyAsync(x_out, x, P * sizeof(V), cudaMemcpyDeviceToDevice, st));

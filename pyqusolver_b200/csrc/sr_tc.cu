@@ -27,6 +27,7 @@
 #include "umma.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cuda_bf16.h>
 
 namespace {
@@ -865,6 +866,20 @@ static int pow2_at_least(int x) {
   return p;
 }
 
+// tiling overrides (qes_sr_set_tiling): 0 = automatic, 1 = single-M-tile kernel, 2 = M/N-tiled kernel;
+// hidden units per N chunk and target CTA count of the M/N-tiled O^H u (0 = automatic)
+static std::atomic<int> g_tile_mode{0}, g_tile_nc{0}, g_tile_ctas{0};
+extern "C" int qes_sr_set_tiling(int mode, int nc, int ctas) {
+  if (mode < 0 || mode > 2 || nc < 0 || (nc % 16) != 0 || ctas < 0) {
+    qes_set_last_message("qes_sr_set_tiling: mode 0..2, nc a multiple of 16 (or 0), ctas >= 0");
+    return QES_ERR_ARG;
+  }
+  g_tile_mode.store(mode);
+  g_tile_nc.store(nc);
+  g_tile_ctas.store(ctas);
+  return QES_OK;
+}
+
 bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   const bool cplx = dtype == QES_DTYPE_C64;
   const int H = cplx ? 2 : 1;
@@ -888,6 +903,9 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   t.ov_smem = (int)(S * stage + ov_extra);
   t.n_tiles = (int)((n_samples + 127) / 128);
   t.big = ns > 127 || t.Mp > 256 || t.NB > 256;
+  const int mode = g_tile_mode.load();
+  if (mode == 2) t.big = true;
+  if (mode == 1 && t.big) return false;
   if (!t.big) {
     t.im_off = pow2_at_least(t.Mp);
     t.tmem_cols = pow2_at_least(std::max(cplx ? 2 * t.im_off : t.im_off, t.NB));
@@ -912,6 +930,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   int nc = (512 / (t.MT * H)) / 16 * 16;
   nc = std::min(nc, 256);
   nc = std::min(nc, t.Mp);
+  if (g_tile_nc.load() > 0) nc = std::min(nc, g_tile_nc.load());
   if (nc < 16) return false;
   t.NC = nc;
   t.NR = H * nc;
@@ -926,7 +945,8 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   if (kc < 16) return false;
   t.KC = kc;
   t.n_chunks = (int)((n_samples + kc - 1) / kc);
-  const int groups_target = std::max(1, (2 * 148 + t.nnc - 1) / t.nnc);
+  const int ctas = g_tile_ctas.load() > 0 ? g_tile_ctas.load() : 2 * 148;
+  const int groups_target = std::max(1, (ctas + t.nnc - 1) / t.nnc);
   t.SPC = std::max(1, (t.n_chunks + groups_target - 1) / groups_target);
   t.nsplit = (t.n_chunks + t.SPC - 1) / t.SPC;
   t.ohu_smem = (int)(2u * (R * kc * 2 + 2u * t.NR * kc * 2) + 2u * kc * tsz + 16 + 8 * 4 + 16 + 64);

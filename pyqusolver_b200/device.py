@@ -92,16 +92,47 @@ def move_tables(flat_params, ns, nh, move_i, move_j, move_kind, move_major: bool
     return Ct, St, A
 
 
-def rbm_forward(flat_params, ns, nh, bits, theta=False, tanh=True, logpsi=True):
+_FWD_WS = {}
+
+
+def rbm_forward(flat_params, ns, nh, bits, theta=False, tanh=True, logpsi=True, tensor_cores=False):
+    """theta, tanh(theta), log psi of a batch (CUDA cores, or tensor cores when ``tensor_cores``)."""
     n = int(bits.shape[0])
     a, b, W = split_params(flat_params, ns, nh)
     dt, dev = flat_params.dtype, flat_params.device
     th = torch.empty((n, nh), dtype=dt, device=dev) if theta else None
     tn = torch.empty((n, nh), dtype=dt, device=dev) if tanh else None
     lp = torch.empty((n,), dtype=dt, device=dev) if logpsi else None
+    if tensor_cores and n > 0:
+        nb = C.c_size_t(0)
+        call("qes_rbm_forward_tc_workspace_bytes", dtype_code(flat_params), ns, nh, n, C.byref(nb))
+        ws = _FWD_WS.get(dev)
+        if ws is None or ws.numel() < nb.value:
+            ws = torch.empty((int(nb.value),), dtype=torch.uint8, device=dev)
+            _FWD_WS[dev] = ws
+        call("qes_rbm_forward_tc", dtype_code(flat_params), ns, nh, n, ptr(bits), ptr(a), ptr(b), ptr(W), ptr(th),
+             ptr(tn), ptr(lp), ptr(ws), int(ws.numel()), stream_ptr())
+        return th, tn, lp
     call("qes_rbm_forward", dtype_code(flat_params), ns, nh, n, ptr(bits), ptr(a), ptr(b), ptr(W), ptr(th), ptr(tn),
          ptr(lp), stream_ptr())
     return th, tn, lp
+
+
+def forward_uses_tensor_cores(flat_params, ns, nh, n) -> bool:
+    """The training step's forward runs on the tensor cores in the mixed form (SR impl 0 or 2) when the
+    shapes fit the tensor-core forward."""
+    if _lib.sr_impl() == _lib.SR_IMPL_CUDA_CORES or n <= 0:
+        return False
+    nb = C.c_size_t(0)
+    rc = call("qes_rbm_forward_tc_workspace_bytes", dtype_code(flat_params), ns, nh, int(n), C.byref(nb),
+              allow=(_lib.QES_ERR_SIZE,))
+    return rc == _lib.QES_OK
+
+
+def rbm_forward_step(flat_params, ns, nh, bits, theta=False, tanh=True, logpsi=True):
+    """Forward of the VMC step: tensor cores in the mixed form, CUDA cores in the plain form."""
+    tc = forward_uses_tensor_cores(flat_params, ns, nh, int(bits.shape[0]))
+    return rbm_forward(flat_params, ns, nh, bits, theta=theta, tanh=tanh, logpsi=logpsi, tensor_cores=tc)
 
 
 def log_derivatives(flat_params, ns, nh, bits, tanh_theta, out=None):

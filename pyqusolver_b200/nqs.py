@@ -318,7 +318,7 @@ class NQS:
         tdvp = tdvp or self._tdvp or TDVP()
         net = self._net
         bits, _ = self._sampler.sample_bits(num_samples)
-        _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+        _, tn, _ = dv.rbm_forward_step(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
         eloc = self.local_energy_bits(bits, tn)
         st = dv.loss_stats(eloc)
         rh = dv.loss_rhat(eloc, self._sampler.numchains)

@@ -74,7 +74,7 @@ def test_batch_matches_single_problem_path(dtype):
             x1 = x1.cpu().numpy()
             assert np.max(np.abs(xb - x1)) <= 1e-4 * np.max(np.abs(x1)), f"problem {b}: SR solution differs"
             assert res[b].converged == int(info["converged"])
-            assert abs(res[b].iterations - info["iterations"]) <= 3
+            assert abs(res[b].iterations - info["iterations"]) <= max(3, 0.05 * info["iterations"])
     finally:
         _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
 

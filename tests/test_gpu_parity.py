@@ -553,3 +553,48 @@ def test_overlap_of_identical_and_different_states():
     f_exact = abs(np.vdot(_exact_psi(a.net, ns), _exact_psi(b.net, ns))) ** 2
     f = qb.NQS.compute_overlap(a, b, num_samples=8)
     assert abs(f - f_exact) < 0.05, (f, f_exact)
+
+
+def test_tilings_agree_and_graphs_follow_tiling_changes(sr_impl):
+    """The O^H u tilings give the same solution, and a CG graph captured under one tiling is not
+    replayed under another."""
+    ns, nh, n = 36, 144, 4096
+    model = qb.XXZ(qb.SquareLattice(2, 6, 6), jxy=-1.0, jz=-1.0)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64", seed=71, init_scale=0.1)
+    bits = dv.init_chains(_lib.INIT_RND_FIXED, n, ns, seed=7, n_up=18)
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    xs = []
+    try:
+        for st in [(0, 0, 0), (2, 64, 296), (2, 128, 148), (2, 0, 148), (0, 0, 0)]:
+            _lib.call("qes_sr_set_tiling", *st)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-9, maxiter=400,
+                                     check_every=8)
+            assert info["iterations"] > 8
+            xs.append(x.cpu().numpy())
+    finally:
+        _lib.call("qes_sr_set_tiling", 0, 0, 0)
+    # float32 products summed in a different order; CG carries that through the conditioning of S
+    assert rel_err(xs[-1], xs[0]) < 1e-12          # same tiling again (graph replay): identical
+    for x in xs[1:-1]:
+        assert rel_err(x, xs[0]) < 1e-3
+
+
+@pytest.mark.parametrize("cplx,ns,nh,n", [(False, 16, 16, 300), (True, 100, 200, 1000), (True, 36, 144, 700),
+                                           (False, 400, 1600, 300), (False, 10, 600, 257), (True, 10, 300, 129)])
+def test_forward_tensor_cores_match_cuda_cores_and_oracle(cplx, ns, nh, n):
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=81, init_scale=0.1)
+    st = rand_states(n, ns, seed=82)
+    bits = dv.pack_states(st)
+    th0, tn0, lp0 = dv.rbm_forward(net.flat, ns, nh, bits, theta=True)
+    th1, tn1, lp1 = dv.rbm_forward(net.flat, ns, nh, bits, theta=True, tensor_cores=True)
+    assert rel_err(th1.cpu().numpy(), th0.cpu().numpy()) < 1e-5
+    # tanh of a complex theta near a pole amplifies the 1e-7 theta difference of the two summation
+    # orders, so tanh is checked against float64 tanh of the path's own theta
+    t1 = th1.cpu().numpy().astype(np.complex128 if cplx else np.float64)
+    assert rel_err(tn1.cpu().numpy(), np.tanh(t1)) < 1e-5
+    wrap_close(lp1.cpu().numpy(), lp0.cpu().numpy())
+    p = oracle_params(net)
+    wrap_close(lp1.cpu().numpy(), orbm.log_psi(p, orbm.to_sigma(st)))

@@ -32,6 +32,19 @@ extern "C" int qes_set_sr_impl(int impl) {
 
 #define QES_ARG_CHECK(cond, msg) do { if (!(cond)) { qes_set_last_message(msg); return QES_ERR_ARG; } } while (0)
 
+// SM count of the current device (cached per device)
+static int qes_sm_count() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
+
 template <class T> struct VecT;
 template <> struct VecT<float> { using type = double; };
 template <> struct VecT<float2> { using type = double2; };
@@ -250,75 +263,137 @@ __global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
 }
 
 // sum the split partials in float64; optional  y = G + shift * p  and  dot partials of p^H y.
-// Block = 32 columns x 8 split groups: the 32 threads of a row read 32 consecutive
-// columns of one split (coalesced) and each thread sums only nsplit/8 partials.
+// A block covers cv column vectors (16 bytes: 2 complex / 4 real columns when VEC, else one
+// column) x RS_THREADS / cv split groups; each thread issues the loads of up to RS_BATCH splits
+// before it sums any of them, so that a block needs one round trip to L2 when
+// nsplit <= groups * RS_BATCH.  The host picks cv so that the grid is about two resident blocks
+// per SM.  Sums run in a fixed order (deterministic).
 constexpr int RED_THREADS = 256;
 constexpr int RED_BLOCKS = 296;          // grid of the element-wise CG kernels
-constexpr int RS_TX = 32, RS_TY = 8;
+constexpr int RS_THREADS = 512, RS_BATCH = 12;
 constexpr int RS_MAX_BLOCKS = 1184;      // upper bound of dot partials written by the reduction
 
-template <class T, class V>
-__global__ void __launch_bounds__(RS_TX * RS_TY) reduce_splits_kernel(int64_t P, int nsplit, const T* __restrict__ partial,
-                                                                      double shift, const V* __restrict__ p,
-                                                                      V* __restrict__ y, double* __restrict__ dot_part,
+QES_D void acc4(double* g, float4 q) { g[0] += q.x; g[1] += q.y; g[2] += q.z; g[3] += q.w; }
+QES_D void acc4(double2* g, float4 q) { g[0].x += q.x; g[0].y += q.y; g[1].x += q.z; g[1].y += q.w; }
+
+template <class T, class V, bool VEC>
+__global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P, int nsplit, int cv,
+                                                                      const T* __restrict__ partial, double shift,
+                                                                      const V* __restrict__ p, V* __restrict__ y,
+                                                                      double* __restrict__ dot_part,
                                                                       double* __restrict__ scal,
                                                                       unsigned int* __restrict__ counter) {
-  __shared__ V red[RS_TY][RS_TX];
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  constexpr int E = VEC ? (int)(16 / sizeof(T)) : 1;      // columns per vector
+  __shared__ V red[RS_THREADS * E];                        // [split group][column vector][E]
+  const int tid = threadIdx.x;
+  const int groups = RS_THREADS / cv, c = tid % cv, sg = tid / cv;
+  const int64_t nvec = P / E;                              // P % E == 0 when VEC
   double d = 0.0;
-  for (int64_t c0 = (int64_t)blockIdx.x * RS_TX; c0 < P; c0 += (int64_t)gridDim.x * RS_TX) {
-    const int64_t k = c0 + tx;
-    V g = vzero(V());
-    if (k < P) {
-#pragma unroll 4
-      for (int z = ty; z < nsplit; z += RS_TY) g = vadd(g, to_d(partial[(int64_t)z * P + k]));
-    }
-    red[ty][tx] = g;
-    __syncthreads();
-    if (ty == 0 && k < P) {
-      V t = red[0][tx];
+  for (int64_t v0 = (int64_t)blockIdx.x * cv; v0 < nvec; v0 += (int64_t)gridDim.x * cv) {
+    const int64_t vi = v0 + c;
+    V g[E];
 #pragma unroll
-      for (int q = 1; q < RS_TY; ++q) t = vadd(t, red[q][tx]);
-      if (p) {
-        const V pk = p[k];
-        t = vadd(t, vscale(shift, pk));
-        d += vdotc(pk, t);
+    for (int e = 0; e < E; ++e) g[e] = vzero(V());
+    if (sg < groups && vi < nvec) {
+      for (int z0 = sg; z0 < nsplit; z0 += groups * RS_BATCH) {
+        if constexpr (VEC) {
+          float4 q[RS_BATCH];
+          const float4* src = reinterpret_cast<const float4*>(partial) + vi;
+#pragma unroll
+          for (int b = 0; b < RS_BATCH; ++b) {
+            const int z = z0 + b * groups;
+            q[b] = (z < nsplit) ? __ldcg(src + (int64_t)z * nvec) : make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+#pragma unroll
+          for (int b = 0; b < RS_BATCH; ++b) acc4(g, q[b]);
+        } else {
+          T q[RS_BATCH];
+#pragma unroll
+          for (int b = 0; b < RS_BATCH; ++b) {
+            const int z = z0 + b * groups;
+            q[b] = (z < nsplit) ? partial[(int64_t)z * P + vi] : T{};
+          }
+#pragma unroll
+          for (int b = 0; b < RS_BATCH; ++b) g[0] = vadd(g[0], to_d(q[b]));
+        }
       }
-      y[k] = t;
+    }
+    if (sg < groups) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) red[(sg * cv + c) * E + e] = g[e];
+    }
+    __syncthreads();
+    if (tid < cv * E) {
+      const int64_t kk = v0 * E + tid;
+      if (kk < P) {
+        V t = red[tid];
+        for (int q = 1; q < groups; ++q) t = vadd(t, red[q * cv * E + tid]);
+        if (p) {
+          const V pk = p[kk];
+          t = vadd(t, vscale(shift, pk));
+          d += vdotc(pk, t);
+        }
+        y[kk] = t;
+      }
     }
     __syncthreads();
   }
   if (!dot_part) return;
-  if (ty == 0) {                       // row 0 is warp 0
-    d = warp_sum(d);
-    if (tx == 0) dot_part[blockIdx.x] = d;
+  __shared__ double sred[RS_THREADS / 32];
+  __shared__ bool last;
+  d = warp_sum(d);
+  if ((tid & 31) == 0) sred[tid >> 5] = d;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int q = 0; q < RS_THREADS / 32; ++q) s += sred[q];
+    dot_part[blockIdx.x] = s;
+    // the last block to finish sums the dot partials: pAp and alpha = rr / pAp
+    if (scal) {
+      __threadfence();
+      last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
   }
   if (!scal) return;
-  // the last block to finish sums the dot partials: pAp and alpha = rr / pAp
-  __shared__ bool last;
-  __threadfence();
-  if (tx == 0 && ty == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
   __syncthreads();
   if (!last) return;
   __threadfence();
-  __shared__ double sred[RS_TX * RS_TY / 32];
-  const int tid = ty * RS_TX + tx;
   double v = 0.0;
-  for (int q = tid; q < (int)gridDim.x; q += RS_TX * RS_TY) v += ((volatile double*)dot_part)[q];
+  for (int q = tid; q < (int)gridDim.x; q += RS_THREADS) v += ((volatile double*)dot_part)[q];
   v = warp_sum(v);
+  __syncthreads();
   if ((tid & 31) == 0) sred[tid >> 5] = v;
   __syncthreads();
   if (tid == 0) {
     double pap = 0.0;
-    for (int q = 0; q < RS_TX * RS_TY / 32; ++q) pap += sred[q];
+    for (int q = 0; q < RS_THREADS / 32; ++q) pap += sred[q];
     scal[1] = pap;
     scal[7] = (scal[4] == 0.0 && pap > 0.0) ? scal[0] / pap : 0.0;
     *counter = 0u;
   }
 }
 
-static int reduce_blocks(int64_t P) {
-  return (int)std::min<int64_t>((P + RS_TX - 1) / RS_TX, RS_MAX_BLOCKS);
+// y = sum of the nsplit partial P-vectors (+ shift * p, dot partials, alpha): the vector form
+// when every split row starts on a 16-byte boundary
+template <class T, class V>
+static void launch_reduce_splits(int64_t P, int nsplit, const void* partial, double shift, const V* p, V* y,
+                                 double* dot_part, double* scal, unsigned int* counter, cudaStream_t st) {
+  constexpr int EV = (int)(16 / sizeof(T));
+  const bool vec = (P % EV == 0) && ((reinterpret_cast<uintptr_t>(partial) & 15) == 0);
+  const int64_t nvec = vec ? P / EV : P;
+  const int target = 2 * qes_sm_count();                   // two resident blocks per SM
+  int64_t cv = (nvec + target - 1) / target;
+  cv = std::max<int64_t>(cv, RS_THREADS / std::max(nsplit, 1));            // no idle split groups
+  const int64_t need = (nsplit + RS_BATCH - 1) / RS_BATCH;                  // groups for one batch
+  cv = std::min<int64_t>(cv, std::max<int64_t>(RS_THREADS / std::max<int64_t>(need, 1), 1));
+  cv = std::max<int64_t>(1, std::min<int64_t>(cv, 128));
+  const int grid = (int)std::min<int64_t>((nvec + cv - 1) / cv, RS_MAX_BLOCKS);
+  if (vec)
+    reduce_splits_kernel<T, V, true><<<grid, RS_THREADS, 0, st>>>(P, nsplit, (int)cv, (const T*)partial, shift, p, y,
+                                                                 dot_part, scal, counter);
+  else
+    reduce_splits_kernel<T, V, false><<<grid, RS_THREADS, 0, st>>>(P, nsplit, (int)cv, (const T*)partial, shift, p,
+                                                                  y, dot_part, scal, counter);
 }
 
 // ----------------------------------------------------------------------------
@@ -370,8 +445,10 @@ __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* 
   }
   // the last block to finish: rr_new, convergence, beta = rr_new / rr, rr <- rr_new
   __shared__ bool last;
-  __threadfence();
-  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) {            // only thread 0 wrote this block's partial
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
   __syncthreads();
   if (!last) return;
   __threadfence();
@@ -651,8 +728,8 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
-  reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, (int)nsplit, (const T*)L.partial, shift, p, y,
-                                                                 dot_part, dot_part ? L.scal : nullptr, L.counter);
+  launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
+      dot_part, dot_part ? L.scal : nullptr, L.counter, st);
   QES_LAUNCH_CHECK();
   qes_prof_end(pfr, st);
   return QES_OK;
@@ -686,8 +763,8 @@ static int sr_force_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, c
                     L.tw, st);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-    reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, L.nsplit, (const T*)L.partial, 0.0, nullptr, F,
-                                                                   nullptr, nullptr, nullptr);
+    launch_reduce_splits<T, V>(P, L.nsplit, L.partial, 0.0, nullptr, F,
+        nullptr, nullptr, nullptr, st);
     QES_LAUNCH_CHECK();
     return QES_OK;
   }
@@ -763,8 +840,8 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
     const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
-    reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, L.nsplit, (const T*)L.partial, shift, v, y,
-                                                                   dot_part, dot_part ? L.scal : nullptr, L.counter);
+    launch_reduce_splits<T, V>(P, L.nsplit, L.partial, shift, v, y,
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st);
     QES_LAUNCH_CHECK();
     qes_prof_end(pfr, st);
     return QES_OK;
@@ -1161,8 +1238,10 @@ __global__ void __launch_bounds__(RED_THREADS) minsr_ap_kernel(int64_t n, const 
     dot_part[blockIdx.x] = t;
   }
   __shared__ bool last;
-  __threadfence();
-  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) {            // only thread 0 wrote this block's partial
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
   __syncthreads();
   if (!last) return;
   __threadfence();
@@ -1226,8 +1305,8 @@ static int minsr_ohu(int ns, int nh, int64_t n, const uint32_t* bits, const T* t
     int rc = tc_ohu(dtype, L.td, n, M.uf, (const double2*)M.umean, -1, 1.0, L.partial, L.tw, st);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-    reduce_splits_kernel<T, V><<<reduce_blocks(P), dim3(RS_TX, RS_TY), 0, st>>>(P, L.nsplit, (const T*)L.partial, 0.0,
-                                                                              nullptr, g, nullptr, nullptr, nullptr);
+    launch_reduce_splits<T, V>(P, L.nsplit, L.partial, 0.0,
+        nullptr, g, nullptr, nullptr, nullptr, st);
     QES_LAUNCH_CHECK();
     return QES_OK;
   }

@@ -526,13 +526,44 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   const int quarter = warp & 3, cg = warp >> 2;
   const int i = 32 * quarter + lane;                      // site row of the accumulator
   const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+  // The W block of the partial (ns rows of nh) is contiguous in global memory.  When it fits in
+  // the operand buffers (free once the MMAs have completed) it is staged there row by row with a
+  // padded stride (16-byte row starts, an odd number of 16-byte units: conflict-free vector
+  // stores) and then written out by whole warps along each row, so that every store instruction
+  // covers consecutive addresses.
+  constexpr int EV = 16 / (int)sizeof(T);                 // elements per 16-byte vector
+  int ldm = (nh + EV - 1) / EV * EV;
+  if (((ldm / EV) & 1) == 0) ldm += EV;
+  const bool staged = (size_t)ns * ldm * sizeof(T) <= (size_t)a_bytes + 2u * b_term;
+  T* stage = reinterpret_cast<T*>(smem);
   if (s_issued) {
     for (int c = cg; c < Mp / 16; c += kColGroups) {
       const int c0 = 16 * c;
       float gr[16], gi[16];
       umma::tmem_ld16(lane_addr + c0, gr);
       if constexpr (CPLX) umma::tmem_ld16(lane_addr + d.im_off + c0, gi);
-      if (i < ns || i == 127) {
+      if (staged && i < ns) {
+        T* rows = stage + (size_t)i * ldm;
+        if (c0 + 16 <= ldm) {
+          float4* dst = reinterpret_cast<float4*>(rows + c0);
+          if constexpr (CPLX) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) dst[q] = make_float4(gr[2 * q], gi[2 * q], gr[2 * q + 1], gi[2 * q + 1]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) dst[q] = make_float4(gr[4 * q], gr[4 * q + 1], gr[4 * q + 2], gr[4 * q + 3]);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int m = c0 + q;
+            if (m < nh) {
+              if constexpr (CPLX) rows[m] = make_float2(gr[q], gi[q]);
+              else rows[m] = gr[q];
+            }
+          }
+        }
+      } else if (i < ns || i == 127) {
         T* rowp = (i == 127) ? out + ns : out + ns + nh + (int64_t)i * nh;   // row 127 = g_b
         // 16-byte stores when the row chunk is aligned and complete, element stores otherwise
         const bool vec = (c0 + 16 <= nh) && ((reinterpret_cast<uintptr_t>(rowp + c0) & 15) == 0);
@@ -555,6 +586,21 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
             }
           }
         }
+      }
+    }
+  }
+  if (staged && s_issued) {
+    __syncthreads();
+    T* dstW = out + ns + nh;
+    const bool vec = ((reinterpret_cast<uintptr_t>(dstW) & 15) == 0) && (nh % EV == 0);
+    for (int r = warp; r < ns; r += kWarps) {
+      const T* src = stage + (size_t)r * ldm;
+      T* dst = dstW + (int64_t)r * nh;
+      if (vec) {
+        for (int q = lane; q < nh / EV; q += 32)
+          reinterpret_cast<float4*>(dst)[q] = reinterpret_cast<const float4*>(src)[q];
+      } else {
+        for (int q = lane; q < nh; q += 32) dst[q] = src[q];
       }
     }
   }

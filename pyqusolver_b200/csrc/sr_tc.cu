@@ -43,6 +43,14 @@ __device__ __forceinline__ void split_bf16(float x, uint16_t& hi, uint16_t& lo) 
   hi = bf16_bits(x);
   lo = bf16_bits(x - bf16_val(hi));
 }
+// the same split for two values at once, packed as bf16x2 (first value in the low half)
+__device__ __forceinline__ void split2_bf16(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
 __device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b) { return (uint32_t)a | ((uint32_t)b << 16); }
 __device__ __forceinline__ uint4 pack8(const uint16_t (&v)[8]) {
   return make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
@@ -205,6 +213,39 @@ __global__ void tc_build_vp_kernel(TcDims d, bool cplx, const V* __restrict__ v,
   }
 }
 
+// ov epilogue helpers.  wrd[128 w] is spin word w of the sample row (bit i % 32 of word i / 32 is
+// site i, set = spin up).  spin_window(i0): bit q = spin of site i0 + q (i0 >= -31; sites below 0
+// read as 0).  low_mask(c): the lowest c bits (c clamped to [0, 32]).
+__device__ __forceinline__ uint32_t spin_window(const uint32_t* wrd, int nw, int i0) {
+  if (i0 < 0) return wrd[0] << (-i0);
+  const int w = i0 >> 5, sh = i0 & 31;
+  const uint32_t lo = wrd[128 * w], hi = (w + 1 < nw) ? wrd[128 * (w + 1)] : 0u;
+  return __funnelshift_r(lo, hi, sh);
+}
+__device__ __forceinline__ uint32_t low_mask(int c) {
+  return c <= 0 ? 0u : (c >= 32 ? 0xffffffffu : ((1u << c) - 1u));
+}
+// fold 16 accumulator columns [n0, n0 + 16) of one sample row into (O v)_s: column n < Sp is
+// (Re) Y of site n, n >= Sp (complex) is Im Y of site n - Sp; a site below ns with spin down
+// flips the sign (a sign-bit xor), site ns (the v_b row) and the zero padding add as they are.
+template <bool CPLX>
+__device__ __forceinline__ void ov_fold16(int n0, const float (&y)[16], int ns, int Sp, const uint32_t* wrd, int nw,
+                                          float2& acc) {
+  const int nre = CPLX ? (Sp - n0) : 16;                  // columns of the real half in this group
+  uint32_t neg = 0;
+  if (nre > 0) neg |= ~spin_window(wrd, nw, n0) & low_mask(ns - n0) & low_mask(nre);
+  if (CPLX && nre < 16) neg |= ~spin_window(wrd, nw, n0 - Sp) & low_mask(ns - (n0 - Sp)) & ~low_mask(nre);
+  float sre = 0.f, sim = 0.f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const float v = __int_as_float(__float_as_int(y[q]) ^ (int)(((neg >> q) & 1u) << 31));
+    if (!CPLX || q < nre) sre += v;
+    else sim += v;
+  }
+  acc.x += sre;
+  acc.y += sim;
+}
+
 // ================================================================================================
 // ov: one CTA per 128-sample tile, K streamed through a d.ov_stages-deep pipeline
 // ================================================================================================
@@ -225,11 +266,17 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   uint64_t* done = empty + S;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   T* s_va = reinterpret_cast<T*>(tslot + 4);
+  const int nw = n_words(ns);
+  // spin words of the tile, word-major ([word][row]) so that a warp reads consecutive rows
+  uint32_t* s_bits = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(s_va) +
+                                                 (((size_t)ns * sizeof(T) + 15) & ~(size_t)15));
   __shared__ double2 red[4];
   __shared__ float2 s_part[kColGroups][128];
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tile = blockIdx.x;
+  const uint8_t* ga = reinterpret_cast<const uint8_t*>(t_rows) + (size_t)tile * nK * 2 * a_term;
+  const uint8_t* gb = reinterpret_cast<const uint8_t*>(vp);
   if (tid == 0) {
     for (int q = 0; q < S; ++q) {
       umma::mbar_init(&full[q], 1);
@@ -237,27 +284,41 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
     }
     umma::mbar_init(done, 1);
     umma::fence_mbar_init();
+    // the first S stages go out before the TMEM allocation and the block-wide setup
+    for (int c = 0; c < S && c < nK; ++c) {
+      uint8_t* st = smem + c * stage_bytes;
+      umma::mbar_arrive_expect_tx(&full[c], stage_bytes);
+      umma::bulk_g2s(st, ga + (size_t)c * 2 * a_term, 2 * a_term, &full[c]);
+      umma::bulk_g2s(st + 2 * a_term, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[c]);
+    }
   }
   if (warp == 0) {
     umma::tmem_alloc(tslot, d.tmem_cols);
     umma::tmem_relinquish();
-  }
-  for (int i = tid; i < ns; i += kThreads) {
-    if constexpr (CPLX) s_va[i] = make_float2(vre(v, i), vim(v, i));
-    else s_va[i] = vre(v, i);
   }
   umma::tc_fence_before();
   __syncthreads();
   umma::tc_fence_after();
   const uint32_t tbase = *tslot;
 
-  if (warp == 0 && lane == 0) {
+  if (warp >= 2) {
+    // while the pipeline runs: v_a and the tile's spin words into shared memory (epilogue inputs)
+    const int t2 = tid - 64, n2 = kThreads - 64;
+    for (int i = t2; i < ns; i += n2) {
+      if constexpr (CPLX) s_va[i] = make_float2(vre(v, i), vim(v, i));
+      else s_va[i] = vre(v, i);
+    }
+    const int64_t r0 = (int64_t)tile * 128;
+    const int rows = (n_samples - r0 < 128) ? (int)(n_samples - r0) : 128;
+    for (int q = t2; q < 128 * nw; q += n2) {
+      const int r = q / nw, w = q - r * nw;
+      s_bits[w * 128 + r] = (r < rows) ? bits[r0 * nw + q] : 0u;
+    }
+  } else if (warp == 0 && lane == 0) {
     // producer: stage s is refilled once the MMAs that read it have completed
-    const uint8_t* ga = reinterpret_cast<const uint8_t*>(t_rows) + (size_t)tile * nK * 2 * a_term;
-    const uint8_t* gb = reinterpret_cast<const uint8_t*>(vp);
-    for (int c = 0; c < nK; ++c) {
+    for (int c = S; c < nK; ++c) {
       const int s = c % S;
-      if (c >= S && !umma::mbar_wait(&empty[s], ((c / S) - 1) & 1, kWaitLimit)) {
+      if (!umma::mbar_wait(&empty[s], ((c / S) - 1) & 1, kWaitLimit)) {
         record_error(status, QES_ERR_TIMEOUT);
         break;
       }
@@ -308,27 +369,39 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   const int row = 32 * quarter + lane;
   const int64_t s = (int64_t)tile * 128 + row;
   const bool sval = s < n_samples;
-  const uint32_t* wrd = bits + (sval ? s : 0) * n_words(ns);
+  const uint32_t* wrd = s_bits + row;                     // word w of this row at wrd[128 w]
   float2 acc = make_float2(0.f, 0.f);
   const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
-  for (int c = cg; c < NB / 16; c += kColGroups) {
+  int c = cg;
+  // two column groups per TMEM wait
+  for (; c + kColGroups < NB / 16; c += 2 * kColGroups) {
+    float y0[16], y1[16];
+    umma::tmem_ld16x2(lane_addr + 16 * c, lane_addr + 16 * (c + kColGroups), y0, y1);
+    ov_fold16<CPLX>(16 * c, y0, ns, Sp, wrd, nw, acc);
+    ov_fold16<CPLX>(16 * (c + kColGroups), y1, ns, Sp, wrd, nw, acc);
+  }
+  if (c < NB / 16) {
     float y[16];
     umma::tmem_ld16(lane_addr + 16 * c, y);
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int n = 16 * c + q;
-      const bool yim = CPLX && n >= Sp;
-      const int i = yim ? n - Sp : n;
-      float contrib = 0.f;
-      if (i < ns) contrib = ((wrd[i >> 5] >> (i & 31)) & 1u) ? y[q] : -y[q];
-      else if (i == ns) contrib = y[q];
-      if (yim) acc.y += contrib;
-      else acc.x += contrib;
-    }
+    ov_fold16<CPLX>(16 * c, y, ns, Sp, wrd, nw, acc);
   }
-  for (int i = cg; i < ns; i += kColGroups) {
-    const float sg = ((wrd[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
-    acc = acc + to_c(scal(sg, s_va[i]));
+  // + sigma_s . v_a: column group cg takes the sites of spin words cg, cg + 4, ...
+  for (int w = cg; w < nw; w += kColGroups) {
+    const uint32_t word = wrd[128 * w];
+    const int i1 = (32 * w + 32 < ns) ? 32 * w + 32 : ns;
+    float sre = 0.f, sim = 0.f;
+    for (int i = 32 * w; i < i1; ++i) {
+      const int sgn = (int)((~word >> (i & 31)) & 1u) << 31;
+      const T va = s_va[i];
+      if constexpr (CPLX) {
+        sre += __int_as_float(__float_as_int(va.x) ^ sgn);
+        sim += __int_as_float(__float_as_int(va.y) ^ sgn);
+      } else {
+        sre += __int_as_float(__float_as_int(va) ^ sgn);
+      }
+    }
+    acc.x += sre;
+    acc.y += sim;
   }
   s_part[cg][row] = acc;
   umma::tc_fence_before();
@@ -390,6 +463,10 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     umma::mbar_init(&bars[1], 1);
     umma::fence_mbar_init();
     s_issued = 0;
+    // operands first: the copy overlaps the mean and the TMEM allocation
+    umma::mbar_arrive_expect_tx(&bars[0], a_bytes + 2 * b_term);
+    umma::bulk_g2s(sA, reinterpret_cast<const uint8_t*>(sig_cols) + (size_t)chunk * a_bytes, a_bytes, &bars[0]);
+    umma::bulk_g2s(sBh, reinterpret_cast<const uint8_t*>(t_cols) + (size_t)chunk * 2 * b_term, 2 * b_term, &bars[0]);
   }
   // mean of w: the per-tile partial sums are reduced by the whole block (fixed order)
   {
@@ -423,11 +500,6 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   __syncthreads();
   umma::tc_fence_after();
   const uint32_t tbase = *tslot;
-  if (tid == 0) {
-    umma::mbar_arrive_expect_tx(&bars[0], a_bytes + 2 * b_term);
-    umma::bulk_g2s(sA, reinterpret_cast<const uint8_t*>(sig_cols) + (size_t)chunk * a_bytes, a_bytes, &bars[0]);
-    umma::bulk_g2s(sBh, reinterpret_cast<const uint8_t*>(t_cols) + (size_t)chunk * 2 * b_term, 2 * b_term, &bars[0]);
-  }
   const float mr = (float)s_mean.x, mi = (float)s_mean.y, fs = (float)scale;
   for (int k = tid; k < KC; k += kThreads) {
     const int64_t s = s0 + k;
@@ -444,8 +516,9 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   if (!loaded) record_error(status, QES_ERR_TIMEOUT);
   // Q = conj(t) u in place: item (m, k8) = rows m (re) and Mp + m (im) for 8 samples
   const int items = Mp * (KC / 8);
+  int m = tid % Mp, k8 = tid / Mp;                        // item it = k8 * Mp + m, stepped by kThreads
+  const int dm = kThreads % Mp, dk = kThreads / Mp;
   for (int it = tid; loaded && it < items; it += kThreads) {
-    const int m = it % Mp, k8 = it / Mp;
     const uint32_t offr = umma::kmajor_offset(m, 8 * k8, Np);
     float trh[8], trl[8], tih[8], til[8];
     unpack8(*reinterpret_cast<const uint4*>(sBh + offr), trh);
@@ -456,27 +529,29 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
       unpack8(*reinterpret_cast<const uint4*>(sBh + offi), tih);
       unpack8(*reinterpret_cast<const uint4*>(sBl + offi), til);
     }
-    uint16_t rh[8], rl[8], ih[8], il[8];
+    uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const T u = s_u[8 * k8 + q];
-      T qv;
+    for (int q2 = 0; q2 < 4; ++q2) {
+      const int q = 2 * q2;
+      const T u0 = s_u[8 * k8 + q], u1 = s_u[8 * k8 + q + 1];
       if constexpr (CPLX) {
-        const float a = trh[q] + trl[q], b = tih[q] + til[q];     // t = a + i b
-        qv = make_float2(a * u.x + b * u.y, a * u.y - b * u.x);    // conj(t) u
-        split_bf16(qv.x, rh[q], rl[q]);
-        split_bf16(qv.y, ih[q], il[q]);
+        const float a0 = trh[q] + trl[q], b0 = tih[q] + til[q];              // t = a + i b
+        const float a1 = trh[q + 1] + trl[q + 1], b1 = tih[q + 1] + til[q + 1];
+        split2_bf16(a0 * u0.x + b0 * u0.y, a1 * u1.x + b1 * u1.y, rh[q2], rl[q2]);   // conj(t) u
+        split2_bf16(a0 * u0.y - b0 * u0.x, a1 * u1.y - b1 * u1.x, ih[q2], il[q2]);
       } else {
-        qv = (trh[q] + trl[q]) * u;
-        split_bf16(qv, rh[q], rl[q]);
+        split2_bf16((trh[q] + trl[q]) * u0, (trh[q + 1] + trl[q + 1]) * u1, rh[q2], rl[q2]);
       }
     }
-    *reinterpret_cast<uint4*>(sBh + offr) = pack8(rh);
-    *reinterpret_cast<uint4*>(sBl + offr) = pack8(rl);
+    *reinterpret_cast<uint4*>(sBh + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+    *reinterpret_cast<uint4*>(sBl + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
     if constexpr (CPLX) {
-      *reinterpret_cast<uint4*>(sBh + offi) = pack8(ih);
-      *reinterpret_cast<uint4*>(sBl + offi) = pack8(il);
+      *reinterpret_cast<uint4*>(sBh + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+      *reinterpret_cast<uint4*>(sBl + offi) = make_uint4(il[0], il[1], il[2], il[3]);
     }
+    m += dm;
+    k8 += dk;
+    if (m >= Mp) { m -= Mp; ++k8; }
   }
   umma::fence_proxy_async_smem();     // generic-proxy stores -> visible to the tensor core
   __syncthreads();
@@ -540,8 +615,8 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     for (int c = cg; c < Mp / 16; c += kColGroups) {
       const int c0 = 16 * c;
       float gr[16], gi[16];
-      umma::tmem_ld16(lane_addr + c0, gr);
-      if constexpr (CPLX) umma::tmem_ld16(lane_addr + d.im_off + c0, gi);
+      if constexpr (CPLX) umma::tmem_ld16x2(lane_addr + c0, lane_addr + d.im_off + c0, gr, gi);
+      else umma::tmem_ld16(lane_addr + c0, gr);
       if (staged && i < ns) {
         T* rows = stage + (size_t)i * ldm;
         if (c0 + 16 <= ldm) {
@@ -942,7 +1017,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   const size_t tsz = cplx ? 8 : 4;
   // ov: as many pipeline stages (2..4) as shared memory holds
   const size_t stage = 2u * (128u * t.KCH * 2 + (size_t)t.NB * t.KCH * 2);
-  const size_t ov_extra = 8 * (2 * 4 + 1) + 16 + (size_t)ns * tsz + 64;
+  const size_t ov_extra = 8 * (2 * 4 + 1) + 16 + ((size_t)ns * tsz + 15) / 16 * 16 + 128u * 4u * ((ns + 31) / 32) + 64;
   const int S = (int)std::min<size_t>(4, (kTcSmemLimit - ov_extra) / stage);
   if (S < 2) return false;
   t.ov_stages = S;

@@ -325,7 +325,7 @@ def run_batch(args, cfg, rank, world, local_rank):
     algo = {"ov": int((rows * nh * 4 + rows * nw * 4 + P * 8 + rows * 8).sum()),
             "ohu": int((rows * nh * 4 + rows * nw * 4 + rows * 8 + nsplit * P * 4).sum()),
             "reduce": int((nsplit * P * 4 + 5 * P * 8).sum())}
-    names = {"ov": "batch_ov_small_kernel", "ohu": "batch_ohu_small_kernel", "reduce": "batch_cg_update_kernel"}
+    names = {"ov": "batch_ov_tile_kernel", "ohu": "batch_ohu_tile_kernel", "reduce": "batch_cg_update_kernel"}
     cands = {k: v for k, v in prof.items() if v[1]}
     dom = max(cands, key=lambda k: cands[k][0])
     avg_s = cands[dom][0] / cands[dom][1] / 1e3

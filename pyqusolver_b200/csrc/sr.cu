@@ -1482,142 +1482,168 @@ __global__ void __launch_bounds__(BCG_THREADS) batch_mean_kernel(const qes_batch
 
 // ---- matvec halves of the batched solve (small problems) -------------------------------------
 // ov  item (b, first row, rows <= BOV_ROWS, 0): the block stages V = v_W (float32), v_b, v_a and
-//     the spins of its rows (as +-1 floats, site-major) in shared memory; each warp advances
-//     BOV_GROUP samples at once, lanes over hidden units:
+//     the spins of its rows (as +-1 floats, site-major) in shared memory and computes
 //       z_m = v_b,m + sum_i sigma_i V_im ,  (O v)_s = sum_m t_sm z_m + sigma . v_a
+//     in 4 x 4 register tiles (batch_ov_tile_kernel below).
 // ohu item (b, split z, 0, 0): the block owns every (site, hidden unit) entry of the split's
-//     partial; thread = (hidden unit m, group of Kg consecutive sites); per staged sample it
-//     reads q_sm = conj(t_sm) u_s once and the group's signs as float4 broadcasts.  A virtual
-//     site ns with sigma = +1 yields g_b = sum_s q_s; g_a = sum_s sigma_s u_s is accumulated by
-//     threads i < ns while staging.
+//     partial, in 4 x 4 register tiles (batch_ohu_tile_kernel below).
 constexpr int BOV_ROWS = 64;
-constexpr int BOV_THREADS = 256;
-constexpr int BOV_GROUP = 4;
-constexpr int BOHU_THREADS = 512;
-constexpr int BOHU_SC = 32;
+// block size limit of the tile kernels (complex tiles hold twice the registers: half the block)
+template <class T>
+constexpr int bohu_max_threads() { return ScalarTraits<T>::is_complex ? 512 : 1024; }
 
 QES_HD int64_t bsmall_align16(int64_t bytes) { return (bytes + 15) & ~(int64_t)15; }
 
+// ov tiles: thread t owns 4 rows x 4 hidden units (tm = t % n_mt fastest) of
+// z_sm = v_b,m + sum_i sigma_si V_im; per site it reads one float4 of signs (4 rows, site-major
+// staging) and four V values for 16 multiply-adds, then folds its units into sum_m t_sm z_sm.
+// The per-unit-group partial sums meet in shared memory and are added in a fixed order.
+QES_HD int bov_round4(int x) { return (x + 3) & ~3; }
 template <class T>
 QES_HD size_t batch_ov_smem(int ns, int nh) {
-  return (size_t)bsmall_align16((int64_t)((int64_t)ns * nh + nh + ns) * sizeof(T)) +
-         (size_t)ns * BOV_ROWS * sizeof(float);
+  const int nmt = bov_round4(nh) / 4;
+  return (size_t)bsmall_align16((int64_t)((int64_t)ns * bov_round4(nh) + bov_round4(nh) + ns) * sizeof(T)) +
+         (size_t)bsmall_align16((int64_t)ns * BOV_ROWS * sizeof(float)) + (size_t)BOV_ROWS * nmt * sizeof(T);
 }
 
-template <class T, class V, int MPL>
-__global__ void __launch_bounds__(BOV_THREADS) batch_ov_small_kernel(const qes_batch_instance* __restrict__ inst,
-                                                                    const int4* __restrict__ items,
-                                                                    const uint32_t* __restrict__ bits,
-                                                                    const T* __restrict__ tt, const V* __restrict__ v,
-                                                                    float2* __restrict__ w,
-                                                                    const double* __restrict__ bscal) {
+template <class T, class V>
+__global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ov_tile_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                             const int4* __restrict__ items,
+                                                                             const uint32_t* __restrict__ bits,
+                                                                             const T* __restrict__ tt,
+                                                                             const V* __restrict__ v,
+                                                                             float2* __restrict__ w,
+                                                                             const double* __restrict__ bscal) {
   extern __shared__ __align__(16) uint8_t bov_sm[];
   const int4 it = items[blockIdx.x];
   if (bscal[(int64_t)it.x * BSC + 4] != 0.0) return;
   const qes_batch_instance I = inst[it.x];
   const int ns = I.ns, nh = I.nh, nw = n_words(ns);
+  const int nhp = bov_round4(nh), nmt = nhp / 4, n_tiles = (BOV_ROWS / 4) * nmt;
   const int64_t r0 = it.y;
   const int nr = it.z;
-  T* Vs = reinterpret_cast<T*>(bov_sm);
-  T* vbs = Vs + (int64_t)ns * nh;
-  T* vas = vbs + nh;
-  float* sigT = reinterpret_cast<float*>(bov_sm + bsmall_align16((int64_t)((int64_t)ns * nh + nh + ns) * sizeof(T)));
+  T* Vs = reinterpret_cast<T*>(bov_sm);                      // [ns][nhp]
+  T* vbs = Vs + (int64_t)ns * nhp;                            // [nhp]
+  T* vas = vbs + nhp;                                         // [ns]
+  float* sigT = reinterpret_cast<float*>(bov_sm + bsmall_align16((int64_t)((int64_t)ns * nhp + nhp + ns) * sizeof(T)));
+  T* red = reinterpret_cast<T*>(reinterpret_cast<uint8_t*>(sigT) + bsmall_align16((int64_t)ns * BOV_ROWS * sizeof(float)));
+  const int tid = threadIdx.x, nthr = blockDim.x;
   const V* pv = v + I.param_off;
-  for (int e = threadIdx.x; e < ns * nh; e += blockDim.x) Vs[e] = to_f(pv[ns + nh + e]);
-  for (int m = threadIdx.x; m < nh; m += blockDim.x) vbs[m] = to_f(pv[ns + m]);
-  for (int i = threadIdx.x; i < ns; i += blockDim.x) vas[i] = to_f(pv[i]);
+  {
+    const int cm = tid % nhp, ci0 = tid / nhp, cid = nthr / nhp;   // V entry (i, m), divided once
+    if (ci0 < cid)
+      for (int i = ci0; i < ns; i += cid) Vs[i * nhp + cm] = (cm < nh) ? to_f(pv[ns + nh + (int64_t)i * nh + cm]) : ScalarTraits<T>::zero();
+  }
+  for (int m = tid; m < nhp; m += nthr) vbs[m] = (m < nh) ? to_f(pv[ns + m]) : ScalarTraits<T>::zero();
+  for (int i = tid; i < ns; i += nthr) vas[i] = to_f(pv[i]);
   const uint32_t* bw = bits + I.sample_word_off;
-  for (int e = threadIdx.x; e < ns * BOV_ROWS; e += blockDim.x) {
-    const int i = e / BOV_ROWS, q = e % BOV_ROWS;
-    float sg = 0.f;
-    if (q < nr) sg = ((bw[(r0 + q) * nw + (i >> 5)] >> (i & 31)) & 1u) ? 1.f : -1.f;
-    sigT[e] = sg;
+  {
+    const int q = tid % BOV_ROWS, i0 = tid / BOV_ROWS, di = nthr / BOV_ROWS;
+    for (int i = i0; i < ns; i += di) {
+      float sg = 0.f;
+      if (q < nr) sg = ((bw[(r0 + q) * nw + (i >> 5)] >> (i & 31)) & 1u) ? 1.f : -1.f;
+      sigT[i * BOV_ROWS + q] = sg;
+    }
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T* tb = tt + I.tanh_off;
+  for (int t0 = 0; t0 < n_tiles; t0 += nthr) {
+    const int t = t0 + tid;
+    if (t < n_tiles) {
+      const int tm = t % nmt, sg = t / nmt;
+      T z[4][4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const T vb = vbs[4 * tm + b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) z[a][b] = vb;
+      }
+      for (int i = 0; i < ns; ++i) {
+        const float4 s4 = *reinterpret_cast<const float4*>(sigT + i * BOV_ROWS + 4 * sg);
+        const T* vr = Vs + (int64_t)i * nhp + 4 * tm;
+        T vv[4];
+        if constexpr (ScalarTraits<T>::is_complex) {
+          const float4 a01 = reinterpret_cast<const float4*>(vr)[0], a23 = reinterpret_cast<const float4*>(vr)[1];
+          vv[0] = make_float2(a01.x, a01.y); vv[1] = make_float2(a01.z, a01.w);
+          vv[2] = make_float2(a23.x, a23.y); vv[3] = make_float2(a23.z, a23.w);
+        } else {
+          const float4 a4 = *reinterpret_cast<const float4*>(vr);
+          vv[0] = a4.x; vv[1] = a4.y; vv[2] = a4.z; vv[3] = a4.w;
+        }
+        const float sv[4] = {s4.x, s4.y, s4.z, s4.w};
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) z[a][b] = addx(z[a][b], scal(sv[a], vv[b]));
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int q = 4 * sg + a;
+        T acc = ScalarTraits<T>::zero();
+        if (q < nr) {
+          const T* trow = tb + (r0 + q) * nh;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int m = 4 * tm + b;
+            if (m < nh) acc = addx(acc, mulx(trow[m], z[a][b]));
+          }
+        }
+        red[q * nmt + tm] = acc;
+      }
+    }
+  }
+  __syncthreads();
   float2* wo = w + I.sample_off;
-  for (int g0 = warp * BOV_GROUP; g0 < nr; g0 += (BOV_THREADS / 32) * BOV_GROUP) {
-    T z[BOV_GROUP][MPL];
-#pragma unroll
-    for (int r = 0; r < MPL; ++r) {
-      const int m = lane + 32 * r;
-      const T b0 = (m < nh) ? vbs[m] : ScalarTraits<T>::zero();
-#pragma unroll
-      for (int j = 0; j < BOV_GROUP; ++j) z[j][r] = b0;
-    }
-    for (int i = 0; i < ns; ++i) {
-      const float4 sg = *reinterpret_cast<const float4*>(sigT + i * BOV_ROWS + g0);
-      const T* vr = Vs + (int64_t)i * nh;
-#pragma unroll
-      for (int r = 0; r < MPL; ++r) {
-        const int m = lane + 32 * r;
-        if (m < nh) {
-          const T x = vr[m];
-          z[0][r] = addx(z[0][r], scal(sg.x, x));
-          z[1][r] = addx(z[1][r], scal(sg.y, x));
-          z[2][r] = addx(z[2][r], scal(sg.z, x));
-          z[3][r] = addx(z[3][r], scal(sg.w, x));
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < BOV_GROUP; ++j) {
-      const int q = g0 + j;
-      T acc = ScalarTraits<T>::zero();
-      if (q < nr) {
-        const T* trow = tb + (r0 + q) * nh;
-#pragma unroll
-        for (int r = 0; r < MPL; ++r) {
-          const int m = lane + 32 * r;
-          if (m < nh) acc = addx(acc, mulx(trow[m], z[j][r]));
-        }
-        for (int i = lane; i < ns; i += 32) acc = addx(acc, scal(sigT[i * BOV_ROWS + q], vas[i]));
-      }
-      acc = warp_sum(acc);
-      if (lane == 0 && q < nr) wo[r0 + q] = to_c(acc);
-    }
+  for (int q = tid; q < nr; q += nthr) {
+    T acc = ScalarTraits<T>::zero();
+    for (int g = 0; g < nmt; ++g) acc = addx(acc, red[q * nmt + g]);
+    for (int i = 0; i < ns; ++i) acc = addx(acc, scal(sigT[i * BOV_ROWS + q], vas[i]));
+    wo[r0 + q] = to_c(acc);
   }
 }
 
-// threads: m = tid % nh, site group g = tid / nh (G = BOHU_THREADS / nh groups of Kg sites,
-// Kg a multiple of 4 with G * Kg >= ns + 1); shared: Q[BOHU_SC][nh], U[BOHU_SC], sig[BOHU_SC][G*Kg]
-QES_HD int batch_ohu_kg(int ns, int nh) {
-  const int G = BOHU_THREADS / nh;
-  const int kg = (ns + 1 + G - 1) / G;
-  return (kg + 3) & ~3;
-}
+// ohu tiles: the split's partial is the (ns + 1) x (nh + 1) matrix  sum_s sigma'_si q'_sm  with a
+// virtual site ns (sigma' = 1: row ns is g_b = sum_s q_s) and a virtual hidden unit nh
+// (q' = u: column nh is g_a = sum_s sigma_s u_s); entry (ns, nh) is unused.  Thread t owns a
+// 4 x 4 tile (sites 4 ti.., units 4 tm..), tm = t % n_mt fastest; per staged sample it reads one
+// float4 of signs and four q values from shared memory for 16 multiply-adds.  Tiles beyond the
+// block size take further passes over the samples.  (8 x 4 tiles, fewer threads per block, ran
+// slower: the staging latency, not the multiply-adds, sets the pace.)
+
+constexpr size_t BOHU_SMEM_TARGET = 96 * 1024;
+
+QES_HD int bohu_round4(int x) { return (x + 3) & ~3; }
+QES_HD int batch_ohu_tiles(int ns, int nh) { return (bohu_round4(ns + 1) / 4) * (bohu_round4(nh + 1) / 4); }
+// staged samples per pass for rows of (nh + 1) q values and (ns + 1) signs
 template <class T>
-QES_HD size_t batch_ohu_smem(int ns, int nh) {
-  const int G = BOHU_THREADS / nh;
-  return (size_t)bsmall_align16((int64_t)BOHU_SC * nh * sizeof(T) + BOHU_SC * sizeof(T)) +
-         (size_t)BOHU_SC * G * batch_ohu_kg(ns, nh) * sizeof(float);
+QES_HD int batch_ohu_sc(int ns_max_row, int nh_max_row) {
+  const size_t row = (size_t)bohu_round4(nh_max_row + 1) * sizeof(T) + (size_t)bohu_round4(ns_max_row + 1) * 4;
+  int sc = (int)(BOHU_SMEM_TARGET / row);
+  sc = sc > 64 ? 64 : sc;
+  return sc < 4 ? 4 : sc;
 }
 
-template <class T, int KMAX>
-__global__ void __launch_bounds__(BOHU_THREADS) batch_ohu_small_kernel(const qes_batch_instance* __restrict__ inst,
-                                                                      const int4* __restrict__ items,
-                                                                      const uint32_t* __restrict__ bits,
-                                                                      const T* __restrict__ tt,
-                                                                      const float2* __restrict__ w,
-                                                                      const double* __restrict__ bscal, int mslot,
-                                                                      int skip_done, T* __restrict__ partial) {
+template <class T>
+__global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ohu_tile_kernel(const qes_batch_instance* __restrict__ inst,
+                                                                         const int4* __restrict__ items,
+                                                                         const uint32_t* __restrict__ bits,
+                                                                         const T* __restrict__ tt,
+                                                                         const float2* __restrict__ w,
+                                                                         const double* __restrict__ bscal, int mslot,
+                                                                         int skip_done, int SC, int qstride,
+                                                                         int sstride, T* __restrict__ partial) {
   extern __shared__ __align__(16) uint8_t boh_sm[];
   const int4 it = items[blockIdx.x];
   const double* sc = bscal + (int64_t)it.x * BSC;
   if (skip_done && sc[4] != 0.0) return;
   const qes_batch_instance I = inst[it.x];
   const int ns = I.ns, nh = I.nh, nw = n_words(ns);
+  const int nsp = bohu_round4(ns + 1), nqp = bohu_round4(nh + 1);
+  const int nst = nsp / 4, nmt = nqp / 4, n_tiles = nst * nmt;
   const int64_t rows = batch_rows(I);
-  const int G = BOHU_THREADS / nh;
-  const int Kg = batch_ohu_kg(ns, nh), SW = G * Kg;      // sig row stride (>= ns + 1)
-  T* Q = reinterpret_cast<T*>(boh_sm);
-  T* U = Q + BOHU_SC * nh;
-  float* sig = reinterpret_cast<float*>(boh_sm + bsmall_align16((int64_t)BOHU_SC * nh * sizeof(T) + BOHU_SC * sizeof(T)));
-  const int tid = threadIdx.x;
-  const int m = tid % nh, g = tid / nh;
-  const bool active = g < G;
-  const int i0 = g * Kg;
+  T* Q = reinterpret_cast<T*>(boh_sm);                                       // [SC][qstride]
+  float* sig = reinterpret_cast<float*>(boh_sm + bsmall_align16((int64_t)SC * qstride * sizeof(T)));   // [SC][sstride]
+  const int tid = threadIdx.x, nthr = blockDim.x;
   const float mr = (float)sc[mslot], mi = (float)sc[mslot + 1];
   const float fs = (float)(1.0 / (double)rows);
   const uint32_t* bw = bits + I.sample_word_off;
@@ -1625,68 +1651,81 @@ __global__ void __launch_bounds__(BOHU_THREADS) batch_ohu_small_kernel(const qes
   const float2* wb = w + I.sample_off;
   const int64_t sbeg = (int64_t)it.y * OHU_SPLIT_SAMPLES;
   const int64_t send = min(rows, sbeg + OHU_SPLIT_SAMPLES);
-  T acc[KMAX];
+  // staging coordinates, divided once: Q entry (sl, m) and sign entry (sl, i)
+  const int qm = tid % nqp, qs0 = tid / nqp, qsd = nthr / nqp;
+  const int si = tid % nsp, ss0 = tid / nsp, ssd = nthr / nsp;
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  T* out = partial + I.sr_part_off + (int64_t)it.y * P;
+  for (int t0 = 0; t0 < n_tiles; t0 += nthr) {
+    const int t = t0 + tid;
+    const bool active = t < n_tiles;
+    const int tm = active ? t % nmt : 0, ti = active ? t / nmt : 0;
+    T acc[4][4];
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k) acc[k] = ScalarTraits<T>::zero();
-  T acca = ScalarTraits<T>::zero();                       // g_a of site tid (tid < ns)
-  for (int64_t c0 = sbeg; c0 < send; c0 += BOHU_SC) {
-    const int nc = (int)min((int64_t)BOHU_SC, send - c0);
-    for (int sl = tid; sl < BOHU_SC; sl += blockDim.x) {
-      T u = ScalarTraits<T>::zero();
-      if (sl < nc) {
-        const float2 wv = wb[c0 + sl];
-        u = from_c(make_float2((wv.x - mr) * fs, (wv.y - mi) * fs), T());
-      }
-      U[sl] = u;
-    }
-    for (int e = tid; e < BOHU_SC * SW; e += blockDim.x) {
-      const int sl = e / SW, i = e % SW;
-      float sg = 0.f;
-      if (sl < nc) {
-        if (i < ns) sg = ((bw[(c0 + sl) * nw + (i >> 5)] >> (i & 31)) & 1u) ? 1.f : -1.f;
-        else if (i == ns) sg = 1.f;                       // virtual site: g_b
-      }
-      sig[e] = sg;
-    }
-    __syncthreads();
-    for (int e = tid; e < BOHU_SC * nh; e += blockDim.x) {
-      const int sl = e / nh, mm = e % nh;
-      Q[e] = (sl < nc) ? mulx(conjx(tb[(c0 + sl) * nh + mm]), U[sl]) : ScalarTraits<T>::zero();
-    }
-    if (tid < ns)
-      for (int sl = 0; sl < nc; ++sl) acca = addx(acca, scal(sig[sl * SW + tid], U[sl]));
-    __syncthreads();
-    if (active) {
-      for (int sl = 0; sl < nc; ++sl) {
-        const T q = Q[sl * nh + m];
-        const float* srow = sig + sl * SW + i0;
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int k = 0; k < KMAX; k += 4) {
-          if (k < Kg) {
-            const float4 s4 = *reinterpret_cast<const float4*>(srow + k);
-            acc[k] = addx(acc[k], scal(s4.x, q));
-            acc[k + 1] = addx(acc[k + 1], scal(s4.y, q));
-            acc[k + 2] = addx(acc[k + 2], scal(s4.z, q));
-            acc[k + 3] = addx(acc[k + 3], scal(s4.w, q));
+      for (int b = 0; b < 4; ++b) acc[a][b] = ScalarTraits<T>::zero();
+    for (int64_t c0 = sbeg; c0 < send; c0 += SC) {
+      const int nc = (int)min((int64_t)SC, send - c0);
+      if (qs0 < qsd) {
+        for (int sl = qs0; sl < SC; sl += qsd) {
+          T q = ScalarTraits<T>::zero();
+          if (sl < nc) {
+            const float2 wv = wb[c0 + sl];
+            const T u = from_c(make_float2((wv.x - mr) * fs, (wv.y - mi) * fs), T());
+            if (qm < nh) q = mulx(conjx(tb[(c0 + sl) * nh + qm]), u);
+            else if (qm == nh) q = u;                                      // virtual unit: g_a
           }
+          Q[sl * qstride + qm] = q;
+        }
+      }
+      if (ss0 < ssd) {
+        for (int sl = ss0; sl < SC; sl += ssd) {
+          float sg = 0.f;
+          if (sl < nc) {
+            if (si < ns) sg = ((bw[(c0 + sl) * nw + (si >> 5)] >> (si & 31)) & 1u) ? 1.f : -1.f;
+            else if (si == ns) sg = 1.f;                                   // virtual site: g_b
+          }
+          sig[sl * sstride + si] = sg;
+        }
+      }
+      __syncthreads();
+      if (active) {
+        for (int sl = 0; sl < nc; ++sl) {
+          const float4 s4 = *reinterpret_cast<const float4*>(sig + sl * sstride + 4 * ti);
+          T q[4];
+          if constexpr (ScalarTraits<T>::is_complex) {
+            const float4* qr = reinterpret_cast<const float4*>(Q + sl * qstride + 4 * tm);
+            const float4 q01 = qr[0], q23 = qr[1];
+            q[0] = make_float2(q01.x, q01.y); q[1] = make_float2(q01.z, q01.w);
+            q[2] = make_float2(q23.x, q23.y); q[3] = make_float2(q23.z, q23.w);
+          } else {
+            const float4 q4 = *reinterpret_cast<const float4*>(Q + sl * qstride + 4 * tm);
+            q[0] = q4.x; q[1] = q4.y; q[2] = q4.z; q[3] = q4.w;
+          }
+          const float sv[4] = {s4.x, s4.y, s4.z, s4.w};
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = addx(acc[a][b], scal(sv[a], q[b]));
+        }
+      }
+      __syncthreads();
+    }
+    if (active) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = 4 * ti + a;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int m = 4 * tm + b;
+          if (i < ns && m < nh) out[ns + nh + (int64_t)i * nh + m] = acc[a][b];
+          else if (i == ns && m < nh) out[ns + m] = acc[a][b];
+          else if (i < ns && m == nh) out[i] = acc[a][b];
         }
       }
     }
-    __syncthreads();
   }
-  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-  T* out = partial + I.sr_part_off + (int64_t)it.y * P;
-  if (active) {
-#pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
-      const int i = i0 + k;
-      if (k < Kg) {
-        if (i < ns) out[ns + nh + (int64_t)i * nh + m] = acc[k];
-        else if (i == ns) out[ns + m] = acc[k];
-      }
-    }
-  }
-  if (tid < ns) out[tid] = acca;
 }
 
 // b = sum of the force partials; x = 0, r = p = b; CG scalars (one block per problem)
@@ -1809,27 +1848,27 @@ extern "C" int qes_batch_sr_workspace_bytes(int dtype, int n_inst, int64_t n_par
   return QES_OK;
 }
 
-template <class T, class V, int MPL>
-static int launch_batch_ov(int n_ov, size_t smem, const qes_batch_instance* inst, const int4* items,
+template <class T, class V>
+static int launch_batch_ov(int n_ov, int threads, size_t smem, const qes_batch_instance* inst, const int4* items,
                            const uint32_t* bits, const T* tt, const V* p, float2* w, const double* bscal,
                            cudaStream_t st) {
-  QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ov_small_kernel<T, V, MPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ov_tile_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
   const int pf = qes_prof_begin(QES_PROF_OV, st);
-  batch_ov_small_kernel<T, V, MPL><<<n_ov, BOV_THREADS, smem, st>>>(inst, items, bits, tt, p, w, bscal);
+  batch_ov_tile_kernel<T, V><<<n_ov, threads, smem, st>>>(inst, items, bits, tt, p, w, bscal);
   qes_prof_end(pf, st);
   return QES_OK;
 }
 
-template <class T, int KMAX>
-static int launch_batch_ohu(int n_ohu, size_t smem, const qes_batch_instance* inst, const int4* items,
-                            const uint32_t* bits, const T* tt, const float2* w, const double* bscal, int skip_done,
-                            T* partial, cudaStream_t st) {
-  QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ohu_small_kernel<T, KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <class T>
+static int launch_batch_ohu(int n_ohu, int threads, int SC, int qstride, int sstride, size_t smem,
+                            const qes_batch_instance* inst, const int4* items, const uint32_t* bits, const T* tt,
+                            const float2* w, const double* bscal, int skip_done, T* partial, cudaStream_t st) {
+  QES_CUDA_CHECK(cudaFuncSetAttribute(batch_ohu_tile_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
   const int pf = qes_prof_begin(QES_PROF_OHU, st);
-  batch_ohu_small_kernel<T, KMAX><<<n_ohu, BOHU_THREADS, smem, st>>>(inst, items, bits, tt, w, bscal, 9, skip_done,
-                                                                     partial);
+  batch_ohu_tile_kernel<T><<<n_ohu, threads, smem, st>>>(inst, items, bits, tt, w, bscal, 9, skip_done, SC, qstride,
+                                                         sstride, partial);
   qes_prof_end(pf, st);
   return QES_OK;
 }
@@ -1847,34 +1886,38 @@ static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, c
   std::vector<qes_batch_instance> hi(n_inst);
   QES_CUDA_CHECK(cudaMemcpyAsync(hi.data(), inst, n_inst * sizeof(qes_batch_instance), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaStreamSynchronize(st));
-  int max_nh = 1, max_kg = 4;
-  size_t ov_smem = 0, ohu_smem = 0;
+  int max_nh = 1, max_ns = 1, max_tiles = 1;
+  size_t ov_smem = 0;
   for (const auto& d : hi) {
-    if (d.ns <= 0 || d.nh <= 0 || d.nh > BOHU_THREADS || d.ns >= BOHU_THREADS ||
-        (int64_t)d.ns * d.nh > (CPLX ? 8192 : 16384)) {
+    if (d.ns <= 0 || d.nh <= 0 || d.nh > 512 || d.ns >= 512 || (int64_t)d.ns * d.nh > (CPLX ? 8192 : 16384)) {
       qes_set_last_message("qes_batch_sr_solve_cg: a problem exceeds ns*nh <= 16384 (real) / 8192 (complex), "
                            "nh <= 512");
       return QES_ERR_SIZE;
     }
     max_nh = std::max(max_nh, d.nh);
-    max_kg = std::max(max_kg, batch_ohu_kg(d.ns, d.nh));
+    max_ns = std::max(max_ns, d.ns);
+    max_tiles = std::max(max_tiles, batch_ohu_tiles(d.ns, d.nh));
     ov_smem = std::max(ov_smem, batch_ov_smem<T>(d.ns, d.nh));
-    ohu_smem = std::max(ohu_smem, batch_ohu_smem<T>(d.ns, d.nh));
   }
-  const int mpl = (max_nh + 31) / 32;
+  // O^H u: one block size for every split (enough threads for the largest problem's tiles)
+  const int ohu_qstride = bohu_round4(max_nh + 1), ohu_sstride = bohu_round4(max_ns + 1);
+  // at least one thread per staged row entry (q values and signs), at most 1024 (real) / 512
+  // (complex); tiles beyond take further passes
+  const int ohu_threads =
+      std::min(bohu_max_threads<T>(), (std::max({max_tiles, ohu_qstride, ohu_sstride}) + 31) / 32 * 32);
+  const int ohu_sc = batch_ohu_sc<T>(max_ns, max_nh);
+  const size_t ohu_smem = (size_t)bsmall_align16((int64_t)ohu_sc * ohu_qstride * sizeof(T)) +
+                          (size_t)ohu_sc * ohu_sstride * sizeof(float);
+  // O v: enough threads for the staging rows (BOV_ROWS signs, nh + ... V columns) and the tiles
+  const int ov_threads = std::min(bohu_max_threads<T>(),
+                                  (std::max({(BOV_ROWS / 4) * (bov_round4(max_nh) / 4), bov_round4(max_nh), BOV_ROWS}) +
+                                   31) / 32 * 32);
   auto ov = [&](const V* vec) -> int {
-#define QES_BOV(M) if (mpl <= M) return launch_batch_ov<T, V, M>(n_ov, ov_smem, inst, ov_items, bits, tt, vec, L.w, L.bscal, st);
-    QES_BOV(1) QES_BOV(2) QES_BOV(4) QES_BOV(8) QES_BOV(16)
-#undef QES_BOV
-    qes_set_last_message("qes_batch_sr_solve_cg: nh too large");
-    return QES_ERR_SIZE;
+    return launch_batch_ov<T, V>(n_ov, ov_threads, ov_smem, inst, ov_items, bits, tt, vec, L.w, L.bscal, st);
   };
   auto ohu = [&](const float2* g, int skip) -> int {
-#define QES_BOHU(K) if (max_kg <= K) return launch_batch_ohu<T, K>(n_ohu, ohu_smem, inst, ohu_items, bits, tt, g, L.bscal, skip, partial, st);
-    QES_BOHU(4) QES_BOHU(8) QES_BOHU(16) QES_BOHU(24) QES_BOHU(32) QES_BOHU(48) QES_BOHU(64)
-#undef QES_BOHU
-    qes_set_last_message("qes_batch_sr_solve_cg: too many sites per thread group");
-    return QES_ERR_SIZE;
+    return launch_batch_ohu<T>(n_ohu, ohu_threads, ohu_sc, ohu_qstride, ohu_sstride, ohu_smem, inst, ohu_items, bits,
+                               tt, g, L.bscal, skip, partial, st);
   };
   int rc;
   QES_CUDA_CHECK(cudaMemsetAsync(L.n_done, 0, sizeof(unsigned int), st));

@@ -485,10 +485,20 @@ __global__ void __launch_bounds__(RED_THREADS) cg_p_kernel(int64_t P, const V* _
     p[k] = pk;
     if (vp && k >= ns) {
       const int64_t q = k - ns;
-      if (q < nh) tc_put_vp_elem(td, vp, ns, (int)q, pk);               // v_b row
-      else tc_put_vp_elem(td, vp, (int)((q - nh) / nh), (int)((q - nh) % nh), pk);
+      if (q < nh) {
+        tc_put_vp_elem(td, vp, ns, (int)q, pk);                          // v_b row
+      } else {
+        const uint32_t qw = (uint32_t)(q - nh);                          // ns * nh < 2^32 on this path
+        tc_put_vp_elem(td, vp, (int)(qw / (uint32_t)nh), (int)(qw % (uint32_t)nh), pk);
+      }
     }
   }
+}
+
+// grid of the per-iteration vector kernels: one element per thread up to RED_BLOCKS blocks (fewer
+// blocks, fewer tickets on the last-block counter for small parameter vectors)
+static int vec_blocks(int64_t n) {
+  return (int)std::min<int64_t>(RED_BLOCKS, std::max<int64_t>(1, (n + RED_THREADS - 1) / RED_THREADS));
 }
 
 // x = 0, r = p = b
@@ -1059,8 +1069,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
                               /*vp_ready=*/it0 + q > 0);
       if (r2) return r2;
       // (alpha is computed by the last block of the matvec's split reduction)
-      cg_xr_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, p, Ap, x, r, L.scal, L.parts, L.counter + 1);
-      cg_p_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, p, L.scal, L.td, L.tc ? L.tw.vp : nullptr);
+      cg_xr_kernel<V><<<vec_blocks(P), RED_THREADS, 0, st>>>(P, p, Ap, x, r, L.scal, L.parts, L.counter + 1);
+      cg_p_kernel<V><<<vec_blocks(P), RED_THREADS, 0, st>>>(P, r, p, L.scal, L.td, L.tc ? L.tw.vp : nullptr);
       QES_LAUNCH_CHECK_N(2);
     }
     return QES_OK;
@@ -1354,8 +1364,8 @@ static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* 
       mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n, L.w, L.wmean);
       minsr_ap_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, L.w, L.wmean, opt->shift, p, Ap, L.parts, L.scal,
                                                              L.counter);
-      cg_xr_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, p, Ap, y, r, L.scal, L.parts, L.counter + 1);
-      cg_p_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, r, p, L.scal, L.td, nullptr);
+      cg_xr_kernel<V><<<vec_blocks(n), RED_THREADS, 0, st>>>(n, p, Ap, y, r, L.scal, L.parts, L.counter + 1);
+      cg_p_kernel<V><<<vec_blocks(n), RED_THREADS, 0, st>>>(n, r, p, L.scal, L.td, nullptr);
       QES_LAUNCH_CHECK_N(4);
     }
     it += nrun;

@@ -555,7 +555,8 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   }
   umma::fence_proxy_async_smem();     // generic-proxy stores -> visible to the tensor core
   __syncthreads();
-  if (tid == 0 && loaded) {
+  // the MMAs are issued by the last thread, which has no g_a work below (ns * 4 <= 508 sites x groups)
+  if (tid == kThreads - 1 && loaded) {
     umma::tc_fence_after();
     const uint32_t idesc = umma::idesc_bf16_f32(128, Mp);
     const uint32_t aaddr = umma::smem_u32(sA), bh = umma::smem_u32(sBh), bl = umma::smem_u32(sBl);

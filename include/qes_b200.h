@@ -140,6 +140,13 @@ int qes_sampler_run_betas(int dtype, const qes_sampler_config* cfg, const float*
                           int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi,
                           void* last_logpsi, void* stream);
 
+/* Programmatic dependent launch of the conjugate-gradient kernels (process-wide,
+ * default on): each kernel of a CG iteration may start its prologue and the
+ * prefetch of the per-step operands while its predecessor drains, and waits in
+ * the kernel for the predecessor's results.  0 turns it off (plain stream
+ * order); results are the same either way.                                  */
+int qes_set_pdl(int on);
+
 /* Parallel tempering (QES/Solver/MonteCarlo/vmc.py:1289-1507).  Chains are
  * n_replicas slots x n_chains (chain index r * n_chains + c); chain_beta holds
  * each chain's current beta.  qes_pt_swap exchanges beta labels between

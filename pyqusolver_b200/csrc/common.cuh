@@ -42,6 +42,31 @@ bool qes_prof_on();
 int qes_prof_begin(int cls, cudaStream_t st);        // returns a slot or -1
 void qes_prof_end(int slot, cudaStream_t st);
 
+// Programmatic dependent launch of the per-iteration SR kernels.  A kernel launched through
+// qes_launch_pdl may start (prologue, prefetch of operands older than its predecessor) while its
+// predecessor in the stream drains; pdl_wait() blocks the calling thread until the predecessor
+// has completed and its writes are visible.  Every kernel on such a chain calls pdl_wait() before
+// it can finish, so "the predecessor has completed" carries down the chain.  Kernels launched the
+// ordinary way see both calls as no-ops.  qes_set_pdl(0) turns the attribute off.
+bool qes_pdl_on();
+template <class... KArgs, class... Args>
+inline cudaError_t qes_launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                  Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = qes_pdl_on() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+QES_D void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+QES_D void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ----------------------------------------------------------------------------
 // scalar algebra on float / float2
 // ----------------------------------------------------------------------------

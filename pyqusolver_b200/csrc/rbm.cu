@@ -17,6 +17,13 @@ void qes_set_last_message(const char* msg) { snprintf(g_last_error, sizeof(g_las
 static std::atomic<long long> g_launches{0};
 void qes_count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+static std::atomic<int> g_pdl{1};
+bool qes_pdl_on() { return g_pdl.load(std::memory_order_relaxed) != 0; }
+extern "C" int qes_set_pdl(int on) {
+  g_pdl.store(on ? 1 : 0);
+  return QES_OK;
+}
+
 extern "C" const char* qes_last_error(void) { return g_last_error; }
 
 // ---------------------------------------------------------------- per-kernel event timing

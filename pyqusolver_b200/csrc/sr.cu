@@ -285,6 +285,8 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
                                                                       unsigned int* __restrict__ counter) {
   constexpr int E = VEC ? (int)(16 / sizeof(T)) : 1;      // columns per vector
   __shared__ V red[RS_THREADS * E];                        // [split group][column vector][E]
+  pdl_trigger();
+  pdl_wait();                                              // the partials: previous kernel
   const int tid = threadIdx.x;
   const int groups = RS_THREADS / cv, c = tid % cv, sg = tid / cv;
   const int64_t nvec = P / E;                              // P % E == 0 when VEC
@@ -376,8 +378,8 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
 // y = sum of the nsplit partial P-vectors (+ shift * p, dot partials, alpha): the vector form
 // when every split row starts on a 16-byte boundary
 template <class T, class V>
-static void launch_reduce_splits(int64_t P, int nsplit, const void* partial, double shift, const V* p, V* y,
-                                 double* dot_part, double* scal, unsigned int* counter, cudaStream_t st) {
+static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, double shift, const V* p, V* y,
+                                double* dot_part, double* scal, unsigned int* counter, cudaStream_t st) {
   constexpr int EV = (int)(16 / sizeof(T));
   const bool vec = (P % EV == 0) && ((reinterpret_cast<uintptr_t>(partial) & 15) == 0);
   const int64_t nvec = vec ? P / EV : P;
@@ -389,11 +391,12 @@ static void launch_reduce_splits(int64_t P, int nsplit, const void* partial, dou
   cv = std::max<int64_t>(1, std::min<int64_t>(cv, 128));
   const int grid = (int)std::min<int64_t>((nvec + cv - 1) / cv, RS_MAX_BLOCKS);
   if (vec)
-    reduce_splits_kernel<T, V, true><<<grid, RS_THREADS, 0, st>>>(P, nsplit, (int)cv, (const T*)partial, shift, p, y,
-                                                                 dot_part, scal, counter);
+    QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, true>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
+                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter));
   else
-    reduce_splits_kernel<T, V, false><<<grid, RS_THREADS, 0, st>>>(P, nsplit, (int)cv, (const T*)partial, shift, p,
-                                                                  y, dot_part, scal, counter);
+    QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
+                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter));
+  return QES_OK;
 }
 
 // ----------------------------------------------------------------------------
@@ -422,6 +425,8 @@ __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* 
                                                             V* __restrict__ x, V* __restrict__ r,
                                                             double* __restrict__ scal, double* __restrict__ rr_part,
                                                             unsigned int* __restrict__ counter) {
+  pdl_trigger();
+  pdl_wait();                                              // Ap and alpha: previous kernel
   const bool done = scal[4] != 0.0;
   const double alpha = scal[7];
   double d = 0.0;
@@ -477,6 +482,8 @@ template <class V>
 __global__ void __launch_bounds__(RED_THREADS) cg_p_kernel(int64_t P, const V* __restrict__ r, V* __restrict__ p,
                                                            const double* __restrict__ scal, TcDims td,
                                                            uint16_t* __restrict__ vp) {
+  pdl_trigger();
+  pdl_wait();                                              // r and beta: previous kernel
   if (scal[4] != 0.0) return;
   const double beta = scal[8];
   const int ns = td.ns, nh = td.nh;
@@ -738,8 +745,8 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
-  launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
-      dot_part, dot_part ? L.scal : nullptr, L.counter, st);
+  if (int rc_ = launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
+      dot_part, dot_part ? L.scal : nullptr, L.counter, st)) return rc_;
   QES_LAUNCH_CHECK();
   qes_prof_end(pfr, st);
   return QES_OK;
@@ -773,8 +780,8 @@ static int sr_force_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, c
                     L.tw, st);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-    launch_reduce_splits<T, V>(P, L.nsplit, L.partial, 0.0, nullptr, F,
-        nullptr, nullptr, nullptr, st);
+    if (int rc_ = launch_reduce_splits<T, V>(P, L.nsplit, L.partial, 0.0, nullptr, F,
+        nullptr, nullptr, nullptr, st)) return rc_;
     QES_LAUNCH_CHECK();
     return QES_OK;
   }
@@ -850,8 +857,8 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
     const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
-    launch_reduce_splits<T, V>(P, L.nsplit, L.partial, shift, v, y,
-        dot_part, dot_part ? L.scal : nullptr, L.counter, st);
+    if (int rc_ = launch_reduce_splits<T, V>(P, L.nsplit, L.partial, shift, v, y,
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st)) return rc_;
     QES_LAUNCH_CHECK();
     qes_prof_end(pfr, st);
     return QES_OK;
@@ -1069,8 +1076,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
                               /*vp_ready=*/it0 + q > 0);
       if (r2) return r2;
       // (alpha is computed by the last block of the matvec's split reduction)
-      cg_xr_kernel<V><<<vec_blocks(P), RED_THREADS, 0, st>>>(P, p, Ap, x, r, L.scal, L.parts, L.counter + 1);
-      cg_p_kernel<V><<<vec_blocks(P), RED_THREADS, 0, st>>>(P, r, p, L.scal, L.td, L.tc ? L.tw.vp : nullptr);
+      QES_CUDA_CHECK(qes_launch_pdl(cg_xr_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P, (const V*)p,
+                                    (const V*)Ap, x, r, L.scal, L.parts, L.counter + 1));
+      QES_CUDA_CHECK(qes_launch_pdl(cg_p_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P, (const V*)r, p,
+                                    (const double*)L.scal, L.td, L.tc ? L.tw.vp : (uint16_t*)nullptr));
       QES_LAUNCH_CHECK_N(2);
     }
     return QES_OK;
@@ -1315,8 +1324,8 @@ static int minsr_ohu(int ns, int nh, int64_t n, const uint32_t* bits, const T* t
     int rc = tc_ohu(dtype, L.td, n, M.uf, (const double2*)M.umean, -1, 1.0, L.partial, L.tw, st);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-    launch_reduce_splits<T, V>(P, L.nsplit, L.partial, 0.0,
-        nullptr, g, nullptr, nullptr, nullptr, st);
+    if (int rc_ = launch_reduce_splits<T, V>(P, L.nsplit, L.partial, 0.0,
+        nullptr, g, nullptr, nullptr, nullptr, st)) return rc_;
     QES_LAUNCH_CHECK();
     return QES_OK;
   }

@@ -180,6 +180,8 @@ __global__ void tc_t_cols_kernel(TcDims d, int64_t n_samples, const T* __restric
 // ================================================================================================
 template <class V>
 __global__ void tc_build_vp_kernel(TcDims d, bool cplx, const V* __restrict__ v, uint16_t* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();                                             // v comes from the previous kernel
   const int ns = d.ns, nh = d.nh, Mp = d.Mp, Kd = d.Kd, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
   const V* vb = v + ns;
   const V* vW = v + ns + nh;
@@ -277,6 +279,7 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   const int tile = blockIdx.x;
   const uint8_t* ga = reinterpret_cast<const uint8_t*>(t_rows) + (size_t)tile * nK * 2 * a_term;
   const uint8_t* gb = reinterpret_cast<const uint8_t*>(vp);
+  pdl_trigger();
   if (tid == 0) {
     for (int q = 0; q < S; ++q) {
       umma::mbar_init(&full[q], 1);
@@ -284,13 +287,17 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
     }
     umma::mbar_init(done, 1);
     umma::fence_mbar_init();
-    // the first S stages go out before the TMEM allocation and the block-wide setup
+    // the first S stages go out before the TMEM allocation and the block-wide setup; the T tiles
+    // (per-step operands) even before the previous kernel, which writes V', has completed
     for (int c = 0; c < S && c < nK; ++c) {
-      uint8_t* st = smem + c * stage_bytes;
       umma::mbar_arrive_expect_tx(&full[c], stage_bytes);
-      umma::bulk_g2s(st, ga + (size_t)c * 2 * a_term, 2 * a_term, &full[c]);
-      umma::bulk_g2s(st + 2 * a_term, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[c]);
+      umma::bulk_g2s(smem + c * stage_bytes, ga + (size_t)c * 2 * a_term, 2 * a_term, &full[c]);
     }
+  }
+  pdl_wait();
+  if (tid == 0) {
+    for (int c = 0; c < S && c < nK; ++c)
+      umma::bulk_g2s(smem + c * stage_bytes + 2 * a_term, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[c]);
   }
   if (warp == 0) {
     umma::tmem_alloc(tslot, d.tmem_cols);
@@ -455,6 +462,7 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int chunk = blockIdx.x;
+  pdl_trigger();
   const int64_t s0 = (int64_t)chunk * KC;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   __shared__ double2 s_red[kWarps];
@@ -463,11 +471,13 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     umma::mbar_init(&bars[1], 1);
     umma::fence_mbar_init();
     s_issued = 0;
-    // operands first: the copy overlaps the mean and the TMEM allocation
+    // operands first (per-step tiles, older than the previous kernel): the copy overlaps the
+    // previous kernel's tail, the mean and the TMEM allocation
     umma::mbar_arrive_expect_tx(&bars[0], a_bytes + 2 * b_term);
     umma::bulk_g2s(sA, reinterpret_cast<const uint8_t*>(sig_cols) + (size_t)chunk * a_bytes, a_bytes, &bars[0]);
     umma::bulk_g2s(sBh, reinterpret_cast<const uint8_t*>(t_cols) + (size_t)chunk * 2 * b_term, 2 * b_term, &bars[0]);
   }
+  pdl_wait();                                             // w and its partial sums: previous kernel
   // mean of w: the per-tile partial sums are reduced by the whole block (fixed order)
   {
     double2 t = make_double2(0.0, 0.0);
@@ -757,6 +767,8 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_big_kernel(TcDims d, int64_t 
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   constexpr int H = CPLX ? 2 : 1;
+  pdl_trigger();
+  pdl_wait();                                             // w and its partial sums: previous kernel
   const int ns = d.ns, nh = d.nh, KC = d.KC, MT = d.MT, NC = d.NC, NR = d.NR, nnc = d.nnc;
   const int R = MT * 128;
   const uint32_t a_bytes = (uint32_t)R * KC * 2u, b_term = (uint32_t)NR * KC * 2u;
@@ -1143,24 +1155,29 @@ template <class T, class V>
 static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const V* v, float2* w_out,
                        T* partial, const TcWork& w, cudaStream_t st, bool build_vp) {
   const bool cplx = ScalarTraits<T>::is_complex;
+  // the CG iteration's kernels form a programmatic-dependent-launch chain (qes_launch_pdl)
   if (build_vp) {
     const int items = d.NB * (d.Kd / 8);
-    tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
+    QES_CUDA_CHECK(qes_launch_pdl(tc_build_vp_kernel<V>, dim3((items + 255) / 256), dim3(256), 0, st, d, cplx, v,
+                                  w.vp));
     QES_LAUNCH_CHECK();
   }
   int pf = qes_prof_begin(QES_PROF_OV, st);
-  tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
-                                                           w.status);
+  QES_CUDA_CHECK(qes_launch_pdl(tc_ov_kernel<T, V>, dim3(d.n_tiles), dim3(kThreads), (size_t)d.ov_smem, st, d,
+                                n_samples, bits, v, (const uint16_t*)w.t_rows, (const uint16_t*)w.vp, w_out, w.wsum,
+                                w.status));
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   pf = qes_prof_begin(QES_PROF_OHU, st);
+  const double inv_n = 1.0 / (double)n_samples;
   if (d.big)
-    tc_ohu_big_kernel<T><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
-        d, n_samples, w_out, w.wsum, d.n_tiles, 1.0 / (double)n_samples, w.sig_cols, w.t_cols, partial, w.status);
+    QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_big_kernel<T>, dim3(d.nnc, d.nsplit), dim3(kThreads), (size_t)d.ohu_smem, st,
+                                  d, n_samples, (const float2*)w_out, (const double2*)w.wsum, d.n_tiles, inv_n,
+                                  (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status));
   else
-    tc_ohu_kernel<T><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, w_out, w.wsum, d.n_tiles,
-                                                               1.0 / (double)n_samples, w.sig_cols, w.t_cols, partial,
-                                                               w.status);
+    QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_kernel<T>, dim3(d.n_chunks), dim3(kThreads), (size_t)d.ohu_smem, st, d,
+                                  n_samples, (const float2*)w_out, (const double2*)w.wsum, d.n_tiles, inv_n,
+                                  (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status));
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;

@@ -283,13 +283,20 @@ int qes_set_sr_impl(int impl);
 int qes_sr_uses_tensor_cores(int dtype, int ns, int nh, int64_t n_samples, int* uses);
 /* Tiling of the tensor-core path for these shapes (for roofline accounting):
  * out = [uses, big, KC, n_chunks, nsplit, n_tiles, Kd, NB, Np, MT, NC, NR,
- * nnc, SPC, ov_stages] (first n_out entries).                              */
+ * nnc, SPC, ov_stages, cl] (first n_out entries); cl = 2 when the O^H u CTAs
+ * run as pairs that add their partials on chip.                            */
 int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int32_t* out, int n_out);
 /* Tiling of the tensor-core O^H u in this process: mode 0 = automatic (the
  * single-M-tile kernel when the shapes allow it), 1 = single-M-tile kernel
  * only, 2 = M/N-tiled kernel; nc = hidden units per N chunk (multiple of 16,
  * 0 = largest that fits TMEM); ctas = target CTA count (0 = 296).          */
 int qes_sr_set_tiling(int mode, int nc, int ctas);
+/* O^H u of the single-M-tile kernel as thread-block clusters of two CTAs that
+ * add their split-K partials through distributed shared memory before writing
+ * one per pair (1, where the W block fits the staging buffers) or one partial
+ * per CTA (0, the default: the pairs measured slower on B200).  Same sums in a
+ * fixed order either way.                                                  */
+int qes_sr_set_ohu_pairs(int on);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);

@@ -114,6 +114,7 @@ SIGNATURES = {
     "qes_sr_uses_tensor_cores": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(C.c_int)],
     "qes_sr_tc_plan": [C.c_int, C.c_int, C.c_int, _i64, _vp, C.c_int],
     "qes_sr_set_tiling": [C.c_int, C.c_int, C.c_int],
+    "qes_sr_set_ohu_pairs": [C.c_int],
     "qes_set_cg_graphs": [C.c_int],
     "qes_set_cg_fused": [C.c_int],
     "qes_rbm_forward_tc_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
@@ -199,7 +200,7 @@ def sr_impl() -> int:
 
 
 TC_PLAN_FIELDS = ("uses", "big", "KC", "n_chunks", "nsplit", "n_tiles", "Kd", "NB", "Np", "MT", "NC", "NR", "nnc",
-                  "SPC", "ov_stages")
+                  "SPC", "ov_stages", "cl")
 
 
 def sr_tc_plan(dtype_code: int, ns: int, nh: int, n_samples: int) -> dict:

@@ -808,9 +808,9 @@ extern "C" int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int3
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_tc_plan: bad dtype");
   const SRWork L = sr_layout(dtype, ns, nh, n_samples, nullptr);
   const TcDims& d = L.td;
-  const int32_t f[15] = {L.tc ? 1 : 0, d.big ? 1 : 0, d.KC, d.n_chunks, d.nsplit, d.n_tiles, d.Kd, d.NB, d.Np,
-                         d.MT, d.NC, d.NR, d.nnc, d.SPC, d.ov_stages};
-  for (int k = 0; k < n_out; ++k) out[k] = k < 15 ? f[k] : 0;
+  const int32_t f[16] = {L.tc ? 1 : 0, d.big ? 1 : 0, d.KC, d.n_chunks, d.nsplit, d.n_tiles, d.Kd, d.NB, d.Np,
+                         d.MT, d.NC, d.NR, d.nnc, d.SPC, d.ov_stages, d.cl};
+  for (int k = 0; k < n_out; ++k) out[k] = k < 16 ? f[k] : 0;
   return QES_OK;
 }
 
@@ -920,10 +920,12 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
 namespace {
 struct CgGraphKey {
   const void* bits; const void* tt; const void* ws; int64_t n; int ns, nh, dtype, chunk, tc, l2;
-  int big, kc, nsplit, nnc, nc, spc;      // tiling of the captured kernels
+  int big, kc, nsplit, nnc, nc, spc, cl;  // tiling of the captured kernels
+  int pad;                                 // keeps the struct free of padding bytes (memcmp)
   double shift;
   bool operator==(const CgGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
+static_assert(sizeof(CgGraphKey) == 3 * sizeof(void*) + 8 + 14 * 4 + 8, "CgGraphKey has padding bytes (memcmp key)");
 struct CgGraphSlot {
   bool init = false;
   cudaStream_t cs = nullptr;
@@ -1110,7 +1112,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       }
       const CgGraphKey key{bits, tt, L.w, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
                            L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0), L.td.big ? 1 : 0, L.td.KC, L.nsplit,
-                           L.td.nnc, L.td.NC, L.td.SPC, opt->shift};
+                           L.td.nnc, L.td.NC, L.td.SPC, L.td.cl, 0, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {
           cudaGraphExecDestroy(gs.exec);

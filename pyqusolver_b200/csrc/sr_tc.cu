@@ -24,6 +24,8 @@
 // frees its TMEM and returns.  The host reads *status after the solve.
 #include "common.cuh"
 #include "sr_tc.h"
+
+#include <cooperative_groups.h>
 #include "umma.cuh"
 
 #include <algorithm>
@@ -439,7 +441,10 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
 // ================================================================================================
 // ohu: one CTA per KC-sample chunk; writes one P-vector of partial sums
 // ================================================================================================
-template <class T>
+// CL = 2: the CTAs run in clusters of two (chunks 2c, 2c + 1); after staging, each adds its half
+// of the rows of both CTAs' partials through distributed shared memory and writes one partial per
+// pair, so the split-K partials that go through L2 and the reduction are halved.
+template <class T, int CL>
 __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_samples, const float2* __restrict__ w,
                                                           const double2* __restrict__ wsum_part, int wsum_n,
                                                           double scale, const uint16_t* __restrict__ sig_cols,
@@ -453,15 +458,17 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   uint8_t* sBh = sA + a_bytes;
   uint8_t* sBl = sBh + b_term;
   T* s_u = reinterpret_cast<T*>(sBl + b_term);            // KC
-  T* s_gb = s_u + KC;                                      // nh
-  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(s_gb + nh) +
-                                               ((16 - (reinterpret_cast<uintptr_t>(s_gb + nh) & 15)) & 15));
+  T* s_gb = s_u + KC;                                      // nh (g_b staging, CL = 2)
+  T* s_ga = s_gb + nh;                                     // ns (g_a staging, CL = 2)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(s_ga + ns) +
+                                               ((16 - (reinterpret_cast<uintptr_t>(s_ga + ns) & 15)) & 15));
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
   __shared__ double2 s_mean;
   __shared__ int s_issued;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int chunk = blockIdx.x;
+  const bool valid = chunk < d.n_chunks;                  // CL = 2 pads the grid to an even size
   pdl_trigger();
   const int64_t s0 = (int64_t)chunk * KC;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
@@ -473,9 +480,12 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     s_issued = 0;
     // operands first (per-step tiles, older than the previous kernel): the copy overlaps the
     // previous kernel's tail, the mean and the TMEM allocation
-    umma::mbar_arrive_expect_tx(&bars[0], a_bytes + 2 * b_term);
-    umma::bulk_g2s(sA, reinterpret_cast<const uint8_t*>(sig_cols) + (size_t)chunk * a_bytes, a_bytes, &bars[0]);
-    umma::bulk_g2s(sBh, reinterpret_cast<const uint8_t*>(t_cols) + (size_t)chunk * 2 * b_term, 2 * b_term, &bars[0]);
+    if (valid) {
+      umma::mbar_arrive_expect_tx(&bars[0], a_bytes + 2 * b_term);
+      umma::bulk_g2s(sA, reinterpret_cast<const uint8_t*>(sig_cols) + (size_t)chunk * a_bytes, a_bytes, &bars[0]);
+      umma::bulk_g2s(sBh, reinterpret_cast<const uint8_t*>(t_cols) + (size_t)chunk * 2 * b_term, 2 * b_term,
+                     &bars[0]);
+    }
   }
   pdl_wait();                                             // w and its partial sums: previous kernel
   // mean of w: the per-tile partial sums are reduced by the whole block (fixed order)
@@ -522,8 +532,8 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     s_u[k] = u;
   }
   __syncthreads();
-  const bool loaded = umma::mbar_wait(&bars[0], 0, kWaitLimit);
-  if (!loaded) record_error(status, QES_ERR_TIMEOUT);
+  const bool loaded = valid && umma::mbar_wait(&bars[0], 0, kWaitLimit);
+  if (valid && !loaded) record_error(status, QES_ERR_TIMEOUT);
   // Q = conj(t) u in place: item (m, k8) = rows m (re) and Mp + m (im) for 8 samples
   const int items = Mp * (KC / 8);
   int m = tid % Mp, k8 = tid / Mp;                        // item it = k8 * Mp + m, stepped by kThreads
@@ -585,7 +595,7 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     s_issued = 1;
   }
   // while the tensor core runs: g_a[i] = sum_s sigma_si u_s (sigma read from the A tile) and g_b
-  T* out = partial + (int64_t)chunk * P;
+  T* out = partial + (int64_t)(CL == 2 ? (chunk >> 1) : chunk) * P;
   for (int base = 0; base < ns * 4; base += kThreads) {       // uniform trip count for the shuffles
     const int it = base + tid;
     const bool act = it < ns * 4;
@@ -604,7 +614,10 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
       ga += __shfl_xor_sync(0xffffffffu, ga, 1);
       ga += __shfl_xor_sync(0xffffffffu, ga, 2);
     }
-    if (act && grp == 0) out[i] = ga;
+    if (act && grp == 0) {
+      if constexpr (CL == 2) s_ga[i] = ga;
+      else out[i] = ga;
+    }
   }
   __syncthreads();
   if (s_issued && !umma::mbar_wait(&bars[1], 0, kWaitLimit)) record_error(status, QES_ERR_TIMEOUT);
@@ -649,6 +662,17 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
             }
           }
         }
+      } else if (CL == 2) {
+        if (i == 127) {                                   // row 127 = g_b, staged for the pair sum
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int m = c0 + q;
+            if (m < nh) {
+              if constexpr (CPLX) s_gb[m] = make_float2(gr[q], gi[q]);
+              else s_gb[m] = gr[q];
+            }
+          }
+        }
       } else if (i < ns || i == 127) {
         T* rowp = (i == 127) ? out + ns : out + ns + nh + (int64_t)i * nh;   // row 127 = g_b
         // 16-byte stores when the row chunk is aligned and complete, element stores otherwise
@@ -675,7 +699,43 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
       }
     }
   }
-  if (staged && s_issued) {
+  if constexpr (CL == 2) {
+    if (!s_issued) {                                      // padding chunk or a timed-out load: adds zero
+      for (int e = tid; e < ns * ldm; e += kThreads) stage[e] = ScalarTraits<T>::zero();
+      for (int e = tid; e < nh; e += kThreads) s_gb[e] = ScalarTraits<T>::zero();
+    }
+    namespace cgrp = cooperative_groups;
+    cgrp::cluster_group cl = cgrp::this_cluster();
+    cl.sync();                                            // both partials staged
+    const unsigned rank = cl.block_rank();
+    const T* peer = cl.map_shared_rank(stage, rank ^ 1u);
+    const T* p0 = rank == 0 ? stage : peer;               // rank 0's partial first: fixed order
+    const T* p1 = rank == 0 ? peer : stage;
+    const int h = (ns + 1) / 2, rb = rank ? h : 0, re = rank ? ns : h;
+    T* dstW = out + ns + nh;
+    const bool vec = ((reinterpret_cast<uintptr_t>(dstW) & 15) == 0) && (nh % EV == 0);
+    for (int r = rb + warp; r < re; r += kWarps) {
+      const T* s0r = p0 + (size_t)r * ldm;
+      const T* s1r = p1 + (size_t)r * ldm;
+      T* dst = dstW + (int64_t)r * nh;
+      if (vec) {
+        for (int q = lane; q < nh / EV; q += 32) {
+          const float4 a = reinterpret_cast<const float4*>(s0r)[q], b = reinterpret_cast<const float4*>(s1r)[q];
+          reinterpret_cast<float4*>(dst)[q] = make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+        }
+      } else {
+        for (int q = lane; q < nh; q += 32) dst[q] = addx(s0r[q], s1r[q]);
+      }
+    }
+    if (rank == 0) {
+      const T* pga = cl.map_shared_rank(s_ga, 1u);
+      for (int e = tid; e < ns; e += kThreads) out[e] = addx(s_ga[e], pga[e]);
+    } else {
+      const T* pgb = cl.map_shared_rank(s_gb, 0u);
+      for (int e = tid; e < nh; e += kThreads) out[ns + e] = addx(pgb[e], s_gb[e]);
+    }
+    cl.sync();                                            // the peer has read this CTA's staging
+  } else if (staged && s_issued) {
     __syncthreads();
     T* dstW = out + ns + nh;
     const bool vec = ((reinterpret_cast<uintptr_t>(dstW) & 15) == 0) && (nh % EV == 0);
@@ -1003,6 +1063,11 @@ static int pow2_at_least(int x) {
 // tiling overrides (qes_sr_set_tiling): 0 = automatic, 1 = single-M-tile kernel, 2 = M/N-tiled kernel;
 // hidden units per N chunk and target CTA count of the M/N-tiled O^H u (0 = automatic)
 static std::atomic<int> g_tile_mode{0}, g_tile_nc{0}, g_tile_ctas{0};
+static std::atomic<int> g_ohu_pairs{0};      // measured slower on B200 (heis 10x10: 49.5 vs 46.2 us per CG iteration)
+extern "C" int qes_sr_set_ohu_pairs(int on) {
+  g_ohu_pairs.store(on ? 1 : 0);
+  return QES_OK;
+}
 extern "C" int qes_sr_set_tiling(int mode, int nc, int ctas) {
   if (mode < 0 || mode > 2 || nc < 0 || (nc % 16) != 0 || ctas < 0) {
     qes_set_last_message("qes_sr_set_tiling: mode 0..2, nc a multiple of 16 (or 0), ctas >= 0");
@@ -1046,15 +1111,22 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
     if (t.tmem_cols > 512) return false;
     int kc = 256;
     while (kc >= 16) {
-      const size_t sm = 128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64;
+      const size_t sm = 128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh + ns) * tsz + 64;
       if (sm <= kTcSmemLimit) break;
       kc -= 16;
     }
     if (kc < 16) return false;
     t.KC = kc;
     t.n_chunks = (int)((n_samples + kc - 1) / kc);
-    t.nsplit = t.n_chunks;
-    t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh) * tsz + 64);
+    // pairs of O^H u CTAs (thread-block clusters of two) when the W block of a partial fits the
+    // operand buffers (the kernel's staging stride: 16-byte rows, an odd number of 16-byte units)
+    const int ev = (int)(16 / tsz);
+    int ldm = (nh + ev - 1) / ev * ev;
+    if (((ldm / ev) & 1) == 0) ldm += ev;
+    const bool fits = (size_t)ns * ldm * tsz <= 128u * kc * 2 + 2u * t.Np * kc * 2;
+    t.cl = (g_ohu_pairs.load() && fits && t.n_chunks >= 2) ? 2 : 1;
+    t.nsplit = (t.n_chunks + t.cl - 1) / t.cl;
+    t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh + ns) * tsz + 64);
     *dout = t;
     return true;
   }
@@ -1085,6 +1157,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   t.nsplit = (t.n_chunks + t.SPC - 1) / t.SPC;
   t.ohu_smem = (int)(2u * (R * kc * 2 + 2u * t.NR * kc * 2) + 2u * kc * tsz + 16 + 8 * 4 + 16 + 64);
   t.im_off = 0;
+  t.cl = 1;
   t.tmem_cols = pow2_at_least(std::max(t.MT * H * t.NC, t.NB));
   if (t.tmem_cols > 512) return false;
   *dout = t;
@@ -1120,10 +1193,42 @@ template <class T, class V>
 static int tc_set_attrs() {
   QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ov_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
-  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemLimit));
+  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
   QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_big_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
+  return QES_OK;
+}
+
+// O^H u of the single-M-tile path: one CTA per sample chunk, or clusters of two CTAs (d.cl == 2, the
+// grid padded to an even size) that add their partials on chip; chained to the previous kernel by PDL
+template <class T>
+static int launch_tc_ohu(const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
+                         double scale, const TcWork& w, T* partial, cudaStream_t st) {
+  if (d.cl == 2) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((d.n_chunks + 1) & ~1));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = (size_t)d.ohu_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = qes_pdl_on() ? 2 : 1;
+    QES_CUDA_CHECK(cudaLaunchKernelEx(&cfg, tc_ohu_kernel<T, 2>, d, n_samples, g, gsum_part, gsum_n, scale,
+                                      (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status));
+  } else {
+    QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_kernel<T, 1>, dim3(d.n_chunks), dim3(kThreads), (size_t)d.ohu_smem, st, d,
+                                  n_samples, g, gsum_part, gsum_n, scale, (const uint16_t*)w.sig_cols,
+                                  (const uint16_t*)w.t_cols, partial, w.status));
+  }
   return QES_OK;
 }
 
@@ -1174,10 +1279,8 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
     QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_big_kernel<T>, dim3(d.nnc, d.nsplit), dim3(kThreads), (size_t)d.ohu_smem, st,
                                   d, n_samples, (const float2*)w_out, (const double2*)w.wsum, d.n_tiles, inv_n,
                                   (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status));
-  else
-    QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_kernel<T>, dim3(d.n_chunks), dim3(kThreads), (size_t)d.ohu_smem, st, d,
-                                  n_samples, (const float2*)w_out, (const double2*)w.wsum, d.n_tiles, inv_n,
-                                  (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status));
+  else if (int rc = launch_tc_ohu<T>(d, n_samples, w_out, w.wsum, d.n_tiles, inv_n, w, partial, st))
+    return rc;
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;
@@ -1222,11 +1325,9 @@ int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const
       tc_ohu_big_kernel<float><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
           d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float*)partial, w.status);
   } else if (dtype == QES_DTYPE_C64) {
-    tc_ohu_kernel<float2><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, g, gsum_part, gsum_n, scale,
-                                                                    w.sig_cols, w.t_cols, (float2*)partial, w.status);
+    if (int rc = launch_tc_ohu<float2>(d, n_samples, g, gsum_part, gsum_n, scale, w, (float2*)partial, st)) return rc;
   } else {
-    tc_ohu_kernel<float><<<d.n_chunks, kThreads, d.ohu_smem, st>>>(d, n_samples, g, gsum_part, gsum_n, scale,
-                                                                   w.sig_cols, w.t_cols, (float*)partial, w.status);
+    if (int rc = launch_tc_ohu<float>(d, n_samples, g, gsum_part, gsum_n, scale, w, (float*)partial, st)) return rc;
   }
   QES_LAUNCH_CHECK();
   return QES_OK;

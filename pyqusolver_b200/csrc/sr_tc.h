@@ -21,6 +21,7 @@ struct TcDims {
   int ov_smem, ohu_smem;
   int ov_stages;     // ov pipeline depth (2..4, as many as fit shared memory)
   int nsplit;        // partial P-vectors written by one O^H u pass
+  int cl;            // O^H u CTAs per thread-block cluster (2: pairs sum their partials on chip)
   // large problems (ns > 127 or more hidden units than one MMA N): the O^H u GEMM is tiled in
   // M (MT tiles of 128 sites, the ones row at site index ns) and N (nnc chunks of NC hidden units,
   // NR = NC (real) or 2 NC (complex) operand rows), and one CTA folds SPC sample chunks into TMEM

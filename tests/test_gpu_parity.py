@@ -389,6 +389,38 @@ def test_sr_matvec_tensor_cores_match_oracle(sr_impl, cplx, ns, nh, n):
     assert rel_err(y_tc, ref) < 1e-4
 
 
+@pytest.mark.parametrize("cplx", [False, True])
+def test_ohu_cta_pairs_match_single_ctas(sr_impl, cplx):
+    """O^H u as clusters of two CTAs that add their partials on chip (an odd chunk count, so one
+    pair holds an empty padding chunk) against one partial per CTA: same matvec and SR solution."""
+    ns, nh, n = 30, 60, 4800
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=61, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=62))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    P = ns + nh + ns * nh
+    rng = np.random.default_rng(63)
+    v = torch.as_tensor(rng.normal(size=P) + (1j * rng.normal(size=P) if cplx else 0)).cuda()
+    sr_impl(_lib.SR_IMPL_TENSOR_CORES)
+    ys, xs, plans = [], [], []
+    try:
+        for on in (1, 0):
+            _lib.call("qes_sr_set_ohu_pairs", on)
+            plans.append(_lib.sr_tc_plan(dv.dtype_code(net.flat), ns, nh, n))
+            ys.append(dv.sr_matvec(net.flat, ns, nh, bits, tn, v, shift=1e-3).cpu().numpy())
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-10, maxiter=2000)
+            assert info["converged"]
+            xs.append(x.cpu().numpy())
+    finally:
+        _lib.call("qes_sr_set_ohu_pairs", 0)
+    assert plans[0]["cl"] == 2 and plans[0]["n_chunks"] % 2 == 1 and plans[1]["cl"] == 1
+    assert plans[0]["nsplit"] == (plans[1]["nsplit"] + 1) // 2
+    assert rel_err(ys[0], ys[1]) < 1e-5
+    assert rel_err(xs[0], xs[1]) < 1e-4
+
+
 @pytest.mark.parametrize("cplx,ns,nh,n", [(False, 200, 800, 12000), (True, 140, 280, 12000),
                                            (False, 400, 1600, 2048)])
 def test_sr_matvec_tensor_cores_large_match_cuda_cores(sr_impl, cplx, ns, nh, n):

@@ -345,6 +345,17 @@ int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples,
                     const uint32_t* bits, const void* tanh_theta, const void* eloc,
                     const qes_sr_options* opt, void* x_out, qes_sr_result* result,
                     void* workspace, size_t workspace_bytes, void* stream);
+/* As qes_sr_solve_cg with an initial guess x0 (device, P float64 / complex128)
+ * of the unscaled system (S + shift) x = F, i.e. a previous x_out divided by
+ * rhs_prefactor; r0 = F - (S + shift) x0 costs one extra matvec and the stop
+ * rule stays ||r|| <= max(rtol ||F||, atol).  x0 = NULL starts from zero.
+ * Replaces the initial-guess handling of TDVP.solve (sr_lin_x0 and
+ * use_old_result, QES/NQS/src/tdvp.py:1346-1380).                          */
+int qes_sr_solve_cg_x0(int dtype, int ns, int nh, int64_t n_samples,
+                       const uint32_t* bits, const void* tanh_theta, const void* eloc,
+                       const qes_sr_options* opt, const void* x0, void* x_out,
+                       qes_sr_result* result, void* workspace, size_t workspace_bytes,
+                       void* stream);
 
 /* Vector-Jacobian product of log psi for the hand-written backward:
  * grad = O^H g  (g: complex64 per sample; real part used for a real RBM),

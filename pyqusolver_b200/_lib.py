@@ -126,6 +126,8 @@ SIGNATURES = {
     "qes_sr_matvec": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, C.c_double, _vp, _vp, _vp, _sz, _vp],
     "qes_sr_solve_cg": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
                         C.POINTER(SRResult), _vp, _sz, _vp],
+    "qes_sr_solve_cg_x0": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp, _vp,
+                           C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_sr_minsr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
     "qes_sr_solve_minsr": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
                            C.POINTER(SRResult), _vp, _sz, _vp],

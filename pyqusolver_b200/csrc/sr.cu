@@ -508,6 +508,17 @@ static int vec_blocks(int64_t n) {
   return (int)std::min<int64_t>(RED_BLOCKS, std::max<int64_t>(1, (n + RED_THREADS - 1) / RED_THREADS));
 }
 
+// r = p = b - A x0 (x already holds x0, Ap holds A x0)
+template <class V>
+__global__ void cg_init_x0_kernel(int64_t P, const V* __restrict__ b, const V* __restrict__ Ax0, V* __restrict__ r,
+                                  V* __restrict__ p) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V rk = vadd(b[k], vscale(-1.0, Ax0[k]));
+    r[k] = rk;
+    p[k] = rk;
+  }
+}
+
 // x = 0, r = p = b
 template <class V>
 __global__ void cg_init_kernel(int64_t P, const V* __restrict__ b, V* __restrict__ x, V* __restrict__ r,
@@ -519,18 +530,25 @@ __global__ void cg_init_kernel(int64_t P, const V* __restrict__ b, V* __restrict
   }
 }
 
+// parts_r: dot partials of ||r0||^2 for a start x0 != 0 (nullptr: r0 = b)
 __global__ void __launch_bounds__(SC_THREADS) cg_setup_kernel(int n, const double* __restrict__ parts, double rtol,
-                                                              double atol, double* __restrict__ scal) {
+                                                              double atol, double* __restrict__ scal,
+                                                              const double* __restrict__ parts_r = nullptr) {
   const double s = block_sum_parts(n, parts);
+  double rr0 = s;
+  if (parts_r) {
+    __syncthreads();                                      // block_sum_parts reuses its shared buffer
+    rr0 = block_sum_parts(n, parts_r);
+  }
   if (threadIdx.x != 0) return;
-  scal[0] = s;                      // rr = ||b||^2
-  scal[6] = s;
+  scal[0] = rr0;                    // rr = ||r0||^2
+  scal[6] = s;                      // ||b||^2
   const double th = fmax(rtol * sqrt(s), atol);
   scal[3] = th * th;
   scal[5] = 0.0;
-  scal[4] = (s <= scal[3]) ? 1.0 : 0.0;
+  scal[4] = (rr0 <= scal[3]) ? 1.0 : 0.0;
   scal[1] = 0.0;
-  scal[2] = s;
+  scal[2] = rr0;
   scal[7] = 0.0;
   scal[8] = 0.0;
 }
@@ -997,10 +1015,11 @@ extern "C" int qes_set_cg_graphs(int enable) {
   return QES_OK;
 }
 
+// x0: start of the iteration for the unscaled system (nullptr: zero)
 template <class T>
 static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* eloc,
                    const qes_sr_options* opt, typename VecT<T>::type* x_out, qes_sr_result* res, const SRWork& L,
-                   cudaStream_t st) {
+                   cudaStream_t st, const typename VecT<T>::type* x0 = nullptr) {
   using V = typename VecT<T>::type;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   V* x = (V*)L.x; V* r = (V*)L.r; V* p = (V*)L.p; V* Ap = (V*)L.Ap; V* b = (V*)L.b;
@@ -1013,10 +1032,22 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   double emean[2] = {0, 0};
   QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 128 * sizeof(unsigned int), st));
-  cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p);
-  norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
-  cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
-  QES_LAUNCH_CHECK_N(3);
+  if (x0) {
+    // warm start: x = x0, r = p = b - (S + shift) x0; the threshold stays rtol * ||b||
+    QES_CUDA_CHECK(cudaMemcpyAsync(x, x0, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
+    rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, x, Ap, nullptr, L, st, false);
+    if (rc) return rc;
+    cg_init_x0_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, Ap, r, p);
+    norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
+    norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, L.parts + RED_BLOCKS);
+    cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal, L.parts + RED_BLOCKS);
+    QES_LAUNCH_CHECK_N(4);
+  } else {
+    cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p);
+    norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
+    cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
+    QES_LAUNCH_CHECK_N(3);
+  }
   const int check = opt->check_every > 0 ? opt->check_every : 8;
   double hs[8] = {0};
   int it = 0;
@@ -1180,9 +1211,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   return done ? QES_OK : QES_ERR_NOT_CONVERGED;
 }
 
-extern "C" int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
-                               const void* tanh_theta, const void* eloc, const qes_sr_options* opt, void* x_out,
-                               qes_sr_result* result, void* workspace, size_t workspace_bytes, void* stream) {
+extern "C" int qes_sr_solve_cg_x0(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                  const void* tanh_theta, const void* eloc, const qes_sr_options* opt,
+                                  const void* x0, void* x_out, qes_sr_result* result, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
   QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && eloc && opt && x_out,
                 "qes_sr_solve_cg: bad args");
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_solve_cg: bad dtype");
@@ -1193,9 +1225,16 @@ extern "C" int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples, con
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == QES_DTYPE_F32)
     return sr_cg_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc, opt,
-                          (double*)x_out, result, L, st);
+                          (double*)x_out, result, L, st, (const double*)x0);
   return sr_cg_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc, opt,
-                         (double2*)x_out, result, L, st);
+                         (double2*)x_out, result, L, st, (const double2*)x0);
+}
+
+extern "C" int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                               const void* tanh_theta, const void* eloc, const qes_sr_options* opt, void* x_out,
+                               qes_sr_result* result, void* workspace, size_t workspace_bytes, void* stream) {
+  return qes_sr_solve_cg_x0(dtype, ns, nh, n_samples, bits, tanh_theta, eloc, opt, nullptr, x_out, result, workspace,
+                            workspace_bytes, stream);
 }
 
 // ----------------------------------------------------------------------------

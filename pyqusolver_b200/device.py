@@ -254,16 +254,22 @@ def sr_matvec(flat_params, ns, nh, bits, tanh_theta, v, shift=0.0, workspace=Non
 
 
 def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
-                check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True):
+                check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True, x0=None):
+    """x0: initial guess of the unscaled system (S + shift) x = F (a previous solution divided by
+    rhs_prefactor), float64 / complex128 of length P on the device; None starts from zero."""
     dc = dtype_code(flat_params)
     n = int(bits.shape[0])
     ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
     x = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    if x0 is not None:
+        x0 = x0.to(device=bits.device, dtype=x.dtype).contiguous()
+        if x0.numel() != x.numel():
+            raise ValueError(f"x0 has {x0.numel()} entries, the parameter vector {x.numel()}")
     opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor))
     res = _lib.SRResult()
     allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_converged else ()
-    call("qes_sr_solve_cg", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), C.byref(opt), ptr(x), C.byref(res),
-         ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
+    call("qes_sr_solve_cg_x0", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), C.byref(opt), ptr(x0), ptr(x),
+         C.byref(res), ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
     info = {"iterations": res.iterations, "converged": bool(res.converged), "residual": res.residual,
             "rhs_norm": res.rhs_norm, "e_mean": complex(res.e_mean_re, res.e_mean_im)}
     return x, info

@@ -38,7 +38,7 @@ class TDVPStepInfo:
 class TDVP:
     def __init__(self, use_sr=True, use_minsr=False, rhs_prefactor=-1.0, sr_lin_solver="scipy_cg",
                  sr_diag_shift=1e-3, sr_tol=1e-8, sr_atol=0.0, sr_maxiter=1000, grad_clip=None,
-                 check_every=16, **kwargs):
+                 check_every=16, sr_lin_x0=None, use_old_result=False, **kwargs):
         solver = str(sr_lin_solver).lower()
         if solver not in ("scipy_cg", "cg"):
             raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG")
@@ -54,6 +54,12 @@ class TDVP:
         self.check_every = int(check_every)
         self._workspace = None
         self.last_info = None
+        # initial guess of the CG (QES/NQS/src/tdvp.py:1346-1380): a fixed vector sr_lin_x0, or with
+        # use_old_result the previous solution (stored scaled, divided by rhs_prefactor for the
+        # unscaled system); zeros when neither applies or the shape does not match
+        self._x0 = sr_lin_x0
+        self.use_old_result = bool(use_old_result)
+        self._solution = None
 
     def set_diag_shift(self, shift):
         self.sr_diag_shift = float(shift)
@@ -68,10 +74,21 @@ class TDVP:
             self._workspace = torch.empty((int(nb.value),), dtype=torch.uint8, device=net.device)
         return self._workspace
 
-    def solve(self, net, bits, tanh_theta, eloc):
+    def _solve_handle_x0(self, P, use_old_result):
+        x0 = self._x0
+        if use_old_result and self._solution is not None:
+            x0 = self._solution
+            if self.rhs_prefactor != 1.0 and abs(self.rhs_prefactor) > 1e-12:
+                x0 = x0 / self.rhs_prefactor
+        if x0 is None or int(torch.as_tensor(x0).numel()) != P:
+            return None
+        return torch.as_tensor(x0)
+
+    def solve(self, net, bits, tanh_theta, eloc, use_old_result=None):
         """Parameter direction x (float64 / complex128, length P), already scaled by rhs_prefactor."""
         n = int(bits.shape[0])
         ws = self._ws(net, n)
+        use_old = self.use_old_result if use_old_result is None else bool(use_old_result)
         if not self.use_sr:
             F = dv.sr_force(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, workspace=ws)
             x = -(F * self.rhs_prefactor) if self.rhs_prefactor != 1.0 else -F
@@ -83,10 +100,13 @@ class TDVP:
                 rhs_prefactor=self.rhs_prefactor, workspace=self._minsr_ws)
             self.last_info = info
         else:
+            x0 = self._solve_handle_x0(dv.n_params(net.ns, net.nh), use_old)
             x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
                                      rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,
-                                     check_every=self.check_every, rhs_prefactor=self.rhs_prefactor, workspace=ws)
+                                     check_every=self.check_every, rhs_prefactor=self.rhs_prefactor, workspace=ws,
+                                     x0=x0)
             self.last_info = info
+            self._solution = x.detach().clone()
         if self.grad_clip is not None and self.grad_clip > 0:
             nrm = torch.linalg.vector_norm(x)
             x = x * torch.clamp(self.grad_clip / (nrm + 1e-12), max=1.0)

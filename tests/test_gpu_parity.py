@@ -389,6 +389,48 @@ def test_sr_matvec_tensor_cores_match_oracle(sr_impl, cplx, ns, nh, n):
     assert rel_err(y_tc, ref) < 1e-4
 
 
+@pytest.mark.parametrize("cplx,impl", [(False, 0), (True, 0), (True, 1)])
+def test_sr_cg_initial_guess(sr_impl, cplx, impl):
+    """CG from an initial guess (qes_sr_solve_cg_x0): from a random start it reaches the zero-start
+    solution; from its own solution it stops at once; TDVP's use_old_result reuses the previous
+    (scaled) solution."""
+    from pyqusolver_b200.tdvp import TDVP
+    ns, nh, n = 12, 24, 1500
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=71, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=72))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    sr_impl(impl)
+    # tight tolerance: a random start reaches the zero-start solution
+    kw = dict(shift=1e-2, rtol=1e-10, maxiter=3000, rhs_prefactor=-1.0)
+    x_ref, info0 = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, **kw)
+    assert info0["converged"] and info0["iterations"] > 5
+    P = ns + nh + ns * nh
+    rng = np.random.default_rng(73)
+    # a random start of the solution's norm (the float32 contractions of A x0 carry errors
+    # relative to |A x0|, so a start far larger than the solution costs accuracy)
+    xr = torch.as_tensor(rng.normal(size=P) + (1j * rng.normal(size=P) if cplx else 0))
+    xr = xr * (float(torch.linalg.vector_norm(x_ref.cpu())) / float(torch.linalg.vector_norm(xr)))
+    x_rand, info2 = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, x0=xr, **kw)
+    assert info2["converged"]
+    assert rel_err(x_rand.cpu().numpy(), x_ref.cpu().numpy()) < 1e-4
+    # a tolerance above the float32 floor of the contractions: from its own solution the CG stops
+    # at once (at 1e-10 the true residual of a float32 matvec sits above the threshold)
+    kl = dict(shift=1e-2, rtol=1e-5, maxiter=3000, rhs_prefactor=-1.0)
+    x_l, info_l = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, **kl)
+    x_l2, info_l2 = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, x0=x_l / -1.0, **kl)
+    assert info_l2["converged"] and info_l2["iterations"] <= 2 < info_l["iterations"]
+    assert rel_err(x_l2.cpu().numpy(), x_l.cpu().numpy()) < 1e-5
+    td = TDVP(rhs_prefactor=-1.0, sr_diag_shift=1e-2, sr_tol=1e-5, sr_maxiter=3000, use_old_result=True)
+    xa = td.solve(net, bits, tn, eloc)
+    it_a = td.last_info["iterations"]
+    xb = td.solve(net, bits, tn, eloc)
+    assert td.last_info["iterations"] <= 2 < it_a
+    assert rel_err(xb.cpu().numpy(), xa.cpu().numpy()) < 1e-5
+
+
 @pytest.mark.parametrize("cplx", [False, True])
 def test_ohu_cta_pairs_match_single_ctas(sr_impl, cplx):
     """O^H u as clusters of two CTAs that add their partials on chip (an odd chunk count, so one

@@ -175,3 +175,21 @@ def test_checkpoint_manager_roundtrip(tmp_path):
     assert flat.dtype == np.complex128 and np.array_equal(flat, ref)
     meta = mgr.load_metadata(3)
     assert meta["step"] == 3 and meta["lr"] == 0.01 and meta["energy"] == {"re": -1.5, "im": 0.0}
+
+
+def test_tdvp_initial_guess_selection():
+    """TDVP._solve_handle_x0 mirrors QES/NQS/src/tdvp.py:1346-1380: a fixed sr_lin_x0, or the previous
+    solution divided by rhs_prefactor when use_old_result is set; None (zero start) when the shape
+    does not match."""
+    import torch
+    from pyqusolver_b200.tdvp import TDVP
+    td = TDVP(rhs_prefactor=-2.0)
+    assert td._solve_handle_x0(5, False) is None
+    td._solution = torch.arange(5, dtype=torch.float64)
+    assert td._solve_handle_x0(5, False) is None
+    x0 = td._solve_handle_x0(5, True)
+    assert torch.allclose(x0, torch.arange(5, dtype=torch.float64) / -2.0)
+    assert td._solve_handle_x0(6, True) is None
+    td2 = TDVP(rhs_prefactor=-1.0, sr_lin_x0=torch.ones(4, dtype=torch.float64))
+    assert torch.equal(td2._solve_handle_x0(4, False), torch.ones(4, dtype=torch.float64))
+    assert td2._solve_handle_x0(3, False) is None

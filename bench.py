@@ -438,7 +438,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     nqs, tdvp = mixed["nqs"], mixed["tdvp"]
 
     # --- end to end through the public API with host buffers (params in, stats + params out)
-    e2e = run_e2e(nqs, cfg, args, dist, world)
+    e2e = run_e2e(cfg, args, dist, world, seed=1234 + rank)
 
     # --- roofline of the dominant kernel (measured live over the timed steps)
     roof = roofline(cfg, nqs, mixed)
@@ -489,32 +489,34 @@ def nqs_energy(info):
     return np.real(e)
 
 
-def run_e2e(nqs, cfg, args, dist, world):
+def run_e2e(cfg, args, dist, world, seed):
+    """The mixed form's training run once more through the public API, now host-driven: a fresh NQS
+    built like the timed one (same parameters, chains and trajectory), and every step uploads the
+    parameters from pinned host memory, runs NQS.train_step (which reads the statistics back) and
+    downloads the updated parameters, which the next step uploads again."""
     import torch
+    nqs, _ = build_nqs(cfg, seed=seed)
     net = nqs.net
     host_in = torch.empty_like(net.master, device="cpu").pin_memory()
     host_in.copy_(net.master.cpu())
     host_out = torch.empty_like(host_in).pin_memory()
-    host_stats = torch.empty(4, dtype=torch.float64).pin_memory()
     from pyqusolver_b200.tdvp import TDVP
     tdvp = TDVP(sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
-    from pyqusolver_b200 import device as dv
     times = []
-    # the same warm-up as the device-timed loop: the first call of a fresh TDVP allocates its
-    # workspace and captures the CG graphs (about 70 ms), which the timed steps must not carry
-    for k in range(args.warmup + args.steps):
+    for k in range(args.warmup + args.steps):                 # warm-up steps untimed, as in the timed loop
         s = torch.cuda.Event(enable_timing=True)
         e = torch.cuda.Event(enable_timing=True)
         s.record()
         net.master.copy_(host_in, non_blocking=True)          # H2D: the step's parameters
         net.flat.copy_(net.master)
         net.bump()
-        info = nqs.train_step(lr=cfg["lr"], tdvp=tdvp)          # public API (reads the energy back)
+        nqs.train_step(lr=cfg["lr"], tdvp=tdvp)                # public API (reads the statistics back)
         host_out.copy_(net.master, non_blocking=True)          # D2H: updated parameters
         e.record()
         torch.cuda.synchronize()
         if k >= args.warmup:
             times.append(s.elapsed_time(e))
+        host_in, host_out = host_out, host_in                  # the next step starts from them
     total = float(np.sum(times))
     if dist is not None:
         t = torch.tensor([total], dtype=torch.float64, device="cuda")

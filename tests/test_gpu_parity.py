@@ -432,6 +432,32 @@ def test_sr_cg_initial_guess(sr_impl, cplx, impl):
 
 
 @pytest.mark.parametrize("cplx", [False, True])
+def test_cg_programmatic_launch_is_bit_identical(sr_impl, cplx):
+    """Programmatic dependent launch only changes when the CG kernels start: the solution, its
+    iteration count and residual are bit-identical with the attribute on and off (every reduction
+    runs in a fixed order)."""
+    ns, nh, n = 24, 48, 3000
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=81, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=82))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    sr_impl(_lib.SR_IMPL_TENSOR_CORES)
+    out = []
+    try:
+        for on in (1, 0):
+            _lib.call("qes_set_pdl", on)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-9, maxiter=2000,
+                                     check_every=8)
+            out.append((x.cpu().numpy(), info["iterations"], info["residual"]))
+    finally:
+        _lib.call("qes_set_pdl", 1)
+    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+    assert np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.parametrize("cplx", [False, True])
 def test_ohu_cta_pairs_match_single_ctas(sr_impl, cplx):
     """O^H u as clusters of two CTAs that add their partials on chip (an odd chunk count, so one
     pair holds an empty padding chunk) against one partial per CTA: same matvec and SR solution."""

@@ -290,7 +290,12 @@ def run_batch(args, cfg, rank, world, local_rank):
     value = world * n_step * args.steps / (total / 1e3)
     ms = total / args.steps
 
-    # end to end: parameters in from pinned host memory, statistics and parameters back
+    # end to end: the same training run once more through the public API (a fresh batch built like
+    # the timed one), host-driven: parameters in from pinned host memory, statistics and parameters
+    # back every step, the downloaded parameters uploaded by the next step
+    smp_shape = (B.warps_per_block, B.blocks_per_sm)
+    del B
+    B, _, _ = build_batch(cfg, seed=1 + rank)
     host_in = torch.empty_like(B.master, device="cpu").pin_memory()
     host_in.copy_(B.master.cpu())
     host_out = torch.empty_like(host_in).pin_memory()
@@ -307,6 +312,7 @@ def run_batch(args, cfg, rank, world, local_rank):
         torch.cuda.synchronize()
         if k >= args.warmup:
             times.append(s0.elapsed_time(s1))
+        host_in, host_out = host_out, host_in
     e2e_total = float(np.sum(times))
     nb = host_in.numel() * host_in.element_size()
     e2e = {"value": world * n_step * args.steps / (e2e_total / 1e3), "unit": "samples/s",
@@ -346,7 +352,7 @@ def run_batch(args, cfg, rank, world, local_rank):
                    "hx_range": [float(hx.min()), float(hx.max())], "alpha": cfg["alpha"],
                    "chains_per_problem": cfg["chains"], "samples_per_chain": cfg["samples"],
                    "samples_per_step": int(n_step), "n_params_total": int(B.n_params_total),
-                   "sampler_warps_per_block": B.warps_per_block, "sampler_blocks_per_sm": B.blocks_per_sm,
+                   "sampler_warps_per_block": smp_shape[0], "sampler_blocks_per_sm": smp_shape[1],
                    "sr": f"per-problem structured CG fp64 in lockstep, shift {cfg['shift']}, rtol {cfg['rtol']}",
                    "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

@@ -302,9 +302,9 @@ int qes_sr_set_ohu_pairs(int on);
 int qes_set_cg_graphs(int enable);
 /* The vector part of each CG iteration (split-partial reduction, x/r and
  * direction updates) as one cooperative kernel with two bounded grid
- * barriers: 2 = always, 1 = when its grid is at most 32 CTAs (the default:
- * small parameter vectors, where launch latency dominates), 0 = never
- * (three kernels).                                                         */
+ * barriers: 2 = always, 1 = when its grid is at most 160 CTAs (the default:
+ * parameter vectors up to a few thousand entries, where launch latency
+ * dominates), 0 = never (three kernels).                                   */
 int qes_set_cg_fused(int mode);
 
 /* RBM forward on the tensor cores: theta = Sigma W + b with W split into

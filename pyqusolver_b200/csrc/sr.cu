@@ -609,8 +609,11 @@ __device__ __forceinline__ void grid_barrier(unsigned int* count, unsigned int* 
   __syncthreads();
 }
 
-template <class T, class V>
-__global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int nsplit, const T* __restrict__ partial,
+// cv: column vectors per block pass (16-byte vectors when VEC), chosen by the host like the
+// standalone split reduction (every thread issues its split loads in one batch)
+template <class T, class V, bool VEC>
+__global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int nsplit, int cv,
+                                                                 const T* __restrict__ partial,
                                                                  double shift, V* __restrict__ x, V* __restrict__ r,
                                                                  V* __restrict__ p, V* __restrict__ Ap,
                                                                  double* __restrict__ scal, double* __restrict__ part,
@@ -618,31 +621,64 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
                                                                  TcDims td, uint16_t* __restrict__ vp) {
   const double rr = scal[0], thresh = scal[3];
   if (scal[4] != 0.0) return;                      // converged: every CTA leaves (scal only changes below)
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CF_TX + tx;
+  constexpr int NT = CF_TX * CF_TY;
+  constexpr int E = VEC ? (int)(16 / sizeof(T)) : 1;      // columns per vector
+  const int tid = threadIdx.y * CF_TX + threadIdx.x;
   const unsigned int nb = gridDim.x;
-  __shared__ V red[CF_TY][CF_TX];
-  __shared__ double sred[CF_TX * CF_TY / 32];
-  // phase 1: Ap and p^H Ap
+  __shared__ V red[NT * E];                                // [split group][column vector][E]
+  __shared__ double sred[NT / 32];
+  // phase 1: Ap and p^H Ap (the split reduction of reduce_splits_kernel)
   double d = 0.0;
-  for (int64_t c0 = (int64_t)blockIdx.x * CF_TX; c0 < P; c0 += (int64_t)nb * CF_TX) {
-    const int64_t k = c0 + tx;
-    V g = vzero(V());
-    if (k < P) {
-#pragma unroll 4
-      for (int z = ty; z < nsplit; z += CF_TY) g = vadd(g, to_d(partial[(int64_t)z * P + k]));
-    }
-    red[ty][tx] = g;
-    __syncthreads();
-    if (ty == 0 && k < P) {
-      V t = red[0][tx];
+  {
+    const int groups = NT / cv, c = tid % cv, sg = tid / cv;
+    const int64_t nvec = P / E;
+    for (int64_t v0 = (int64_t)blockIdx.x * cv; v0 < nvec; v0 += (int64_t)nb * cv) {
+      const int64_t vi = v0 + c;
+      V g[E];
 #pragma unroll
-      for (int q = 1; q < CF_TY; ++q) t = vadd(t, red[q][tx]);
-      const V pk = p[k];
-      t = vadd(t, vscale(shift, pk));
-      Ap[k] = t;
-      d += vdotc(pk, t);
+      for (int e = 0; e < E; ++e) g[e] = vzero(V());
+      if (sg < groups && vi < nvec) {
+        for (int z0 = sg; z0 < nsplit; z0 += groups * RS_BATCH) {
+          if constexpr (VEC) {
+            float4 q[RS_BATCH];
+            const float4* src = reinterpret_cast<const float4*>(partial) + vi;
+#pragma unroll
+            for (int b = 0; b < RS_BATCH; ++b) {
+              const int z = z0 + b * groups;
+              q[b] = (z < nsplit) ? __ldcg(src + (int64_t)z * nvec) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int b = 0; b < RS_BATCH; ++b) acc4(g, q[b]);
+          } else {
+            T q[RS_BATCH];
+#pragma unroll
+            for (int b = 0; b < RS_BATCH; ++b) {
+              const int z = z0 + b * groups;
+              q[b] = (z < nsplit) ? partial[(int64_t)z * P + vi] : T{};
+            }
+#pragma unroll
+            for (int b = 0; b < RS_BATCH; ++b) g[0] = vadd(g[0], to_d(q[b]));
+          }
+        }
+      }
+      if (sg < groups) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) red[(sg * cv + c) * E + e] = g[e];
+      }
+      __syncthreads();
+      if (tid < cv * E) {
+        const int64_t kk = v0 * E + tid;
+        if (kk < P) {
+          V t = red[tid];
+          for (int q = 1; q < groups; ++q) t = vadd(t, red[q * cv * E + tid]);
+          const V pk = p[kk];
+          t = vadd(t, vscale(shift, pk));
+          Ap[kk] = t;
+          d += vdotc(pk, t);
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   auto block_sum = [&](double v) -> double {
     v = warp_sum(v);
@@ -656,13 +692,18 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
   d = block_sum(d);
   if (tid == 0) part[blockIdx.x] = d;
   grid_barrier(bar, bar + 32, nb, err);
-  double pap = 0.0;
-  for (unsigned int b = 0; b < nb; ++b) pap += ((volatile double*)part)[b];
+  // every CTA sums the nb partials with the whole block (same fixed order in every CTA)
+  auto sum_parts = [&](const double* src) -> double {
+    double v = 0.0;
+    for (unsigned int b = tid; b < nb; b += CF_TX * CF_TY) v += __ldcg(src + b);
+    return block_sum(v);
+  };
+  const double pap = sum_parts(part);
   const double alpha = (pap > 0.0) ? rr / pap : 0.0;
   // phase 2: x, r and r^H r
   double e = 0.0;
-  const int64_t stride = (int64_t)nb * CF_TX * CF_TY;
-  for (int64_t k = (int64_t)blockIdx.x * CF_TX * CF_TY + tid; k < P; k += stride) {
+  const int64_t stride = (int64_t)nb * NT;
+  for (int64_t k = (int64_t)blockIdx.x * NT + tid; k < P; k += stride) {
     x[k] = vadd(x[k], vscale(alpha, p[k]));
     const V rk = vadd(r[k], vscale(-alpha, Ap[k]));
     r[k] = rk;
@@ -671,14 +712,13 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
   e = block_sum(e);
   if (tid == 0) part[nb + blockIdx.x] = e;
   grid_barrier(bar, bar + 32, nb, err);
-  double rr_new = 0.0;
-  for (unsigned int b = 0; b < nb; ++b) rr_new += ((volatile double*)part)[nb + b];
+  const double rr_new = sum_parts(part + nb);
   const double beta = (rr > 0.0) ? rr_new / rr : 0.0;
   const bool conv = rr_new <= thresh;
   // phase 3: direction update (same index map as phase 2: each thread updates what it wrote)
   if (!conv) {
     const int ns = td.ns, nh = td.nh;
-    for (int64_t k = (int64_t)blockIdx.x * CF_TX * CF_TY + tid; k < P; k += stride) {
+    for (int64_t k = (int64_t)blockIdx.x * NT + tid; k < P; k += stride) {
       const V pk = vadd(r[k], vscale(beta, p[k]));
       p[k] = pk;
       if (vp && k >= ns) {
@@ -1055,19 +1095,37 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaStreamSynchronize(st));
   done = hs[4] != 0.0;
-  // fused vector kernel: always (2), never (0), or automatically (1) when its grid is small -- its two
-  // grid barriers cost more than the launches they save once the grid spans the GPU (measured)
+  // fused vector kernel (split reduction, x/r and direction updates with two grid barriers):
+  // always (2), never (0), or automatically (1) for grids of up to 160 CTAs
   const int fused_mode = g_cg_fused.load();
   bool fused = fused_mode != 0;
-  int fused_grid = 0;
+  int fused_grid = 0, fused_cv = 1;
+  constexpr int FEV = (int)(16 / sizeof(T));
+  const bool fused_vec = (P % FEV == 0) && ((reinterpret_cast<uintptr_t>(L.partial) & 15) == 0);
   if (fused) {
     int dv_ = 0, nsm = 0, per_sm = 0;
     QES_CUDA_CHECK(cudaGetDevice(&dv_));
     QES_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dv_));
-    QES_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fused_kernel<T, V>, CF_TX * CF_TY, 0));
-    fused_grid = (int)std::min<int64_t>((int64_t)nsm * std::max(per_sm, 1), std::min<int64_t>(RED_BLOCKS, (P + CF_TX - 1) / CF_TX));
-    fused_grid = std::max(fused_grid, 1);
-    if (fused_mode == 1 && fused_grid > 32) fused = false;
+    if (fused_vec)
+      QES_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fused_kernel<T, V, true>,
+                                                                   CF_TX * CF_TY, 0));
+    else
+      QES_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fused_kernel<T, V, false>,
+                                                                   CF_TX * CF_TY, 0));
+    // column vectors per block pass as in the standalone split reduction, the grid within residency
+    const int64_t cap = std::min<int64_t>((int64_t)nsm * std::max(per_sm, 1), RED_BLOCKS);
+    const int64_t nvec = fused_vec ? P / FEV : P;
+    int64_t cv = (nvec + cap - 1) / cap;
+    const int nthr = CF_TX * CF_TY;
+    cv = std::max<int64_t>(cv, nthr / std::max(L.nsplit, 1));
+    const int64_t need = (L.nsplit + RS_BATCH - 1) / RS_BATCH;
+    cv = std::min<int64_t>(cv, std::max<int64_t>(nthr / std::max<int64_t>(need, 1), 1));
+    cv = std::max<int64_t>(1, std::min<int64_t>(cv, 128));
+    fused_cv = (int)cv;
+    fused_grid = (int)std::max<int64_t>(1, std::min<int64_t>(cap, (nvec + cv - 1) / cv));
+    // automatic: up to 160 CTAs (measured per CG iteration, fused vs three kernels: TFIM-16 19.9 vs
+    // 22.7 us, 6x6 J1-J2 (158 CTAs) 44.6 vs 45.7 us, 10x10 Heisenberg (290 CTAs) 46.3 vs 45.5 us)
+    if (fused_mode == 1 && fused_grid > 160) fused = false;
   }
   auto run_direct = [&](int nrun, int it0) -> int {
     for (int q = 0; q < nrun; ++q) {
@@ -1098,9 +1156,16 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         lc.attrs = at;
         lc.numAttrs = 1;
         const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
-        QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V>, P, L.nsplit, (const T*)L.partial, opt->shift,
-                                          x, r, p, Ap, L.scal, L.parts, L.counter + 32, (int*)(L.counter + 4), L.td,
-                                          L.tc ? L.tw.vp : (uint16_t*)nullptr));
+        if (fused_vec)
+          QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, true>, P, L.nsplit, fused_cv,
+                                            (const T*)L.partial, opt->shift, x, r, p, Ap, L.scal, L.parts,
+                                            L.counter + 32, (int*)(L.counter + 4), L.td,
+                                            L.tc ? L.tw.vp : (uint16_t*)nullptr));
+        else
+          QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, false>, P, L.nsplit, fused_cv,
+                                            (const T*)L.partial, opt->shift, x, r, p, Ap, L.scal, L.parts,
+                                            L.counter + 32, (int*)(L.counter + 4), L.td,
+                                            L.tc ? L.tw.vp : (uint16_t*)nullptr));
         qes_prof_end(pfr, st);
         QES_LAUNCH_CHECK();
         continue;

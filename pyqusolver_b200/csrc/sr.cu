@@ -1904,10 +1904,19 @@ __global__ void __launch_bounds__(BCG_THREADS) batch_cg_update_kernel(const qes_
   const T* part = partial + I.sr_part_off;
   __shared__ double red[BCG_THREADS / 32];
   double d = 0.0;
+  // the split loads of an element are issued together (fixed summation order)
   for (int64_t k = threadIdx.x; k < P; k += blockDim.x) {
-    V g = vzero(V());
-    for (int z = 0; z < nz; ++z) g = vadd(g, to_d(part[(int64_t)z * P + k]));
     const V pk = p[o + k];
+    V g = vzero(V());
+    int z = 0;
+    for (; z + 8 <= nz; z += 8) {
+      T q[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) q[b] = part[(int64_t)(z + b) * P + k];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) g = vadd(g, to_d(q[b]));
+    }
+    for (; z < nz; ++z) g = vadd(g, to_d(part[(int64_t)z * P + k]));
     g = vadd(g, vscale(shift, pk));
     Ap[o + k] = g;
     d += vdotc(pk, g);

@@ -1735,7 +1735,7 @@ __global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ov_tile_kernel(co
 // block size take further passes over the samples.  (8 x 4 tiles, fewer threads per block, ran
 // slower: the staging latency, not the multiply-adds, sets the pace.)
 
-constexpr size_t BOHU_SMEM_TARGET = 96 * 1024;
+constexpr size_t BOHU_SMEM_TARGET = 200 * 1024;   // up to a whole split (256 samples) staged at once
 
 QES_HD int bohu_round4(int x) { return (x + 3) & ~3; }
 QES_HD int batch_ohu_tiles(int ns, int nh) { return (bohu_round4(ns + 1) / 4) * (bohu_round4(nh + 1) / 4); }
@@ -1744,7 +1744,7 @@ template <class T>
 QES_HD int batch_ohu_sc(int ns_max_row, int nh_max_row) {
   const size_t row = (size_t)bohu_round4(nh_max_row + 1) * sizeof(T) + (size_t)bohu_round4(ns_max_row + 1) * 4;
   int sc = (int)(BOHU_SMEM_TARGET / row);
-  sc = sc > 64 ? 64 : sc;
+  sc = sc > OHU_SPLIT_SAMPLES ? OHU_SPLIT_SAMPLES : sc;
   return sc < 4 ? 4 : sc;
 }
 
@@ -1793,6 +1793,7 @@ __global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ohu_tile_kernel(c
     for (int64_t c0 = sbeg; c0 < send; c0 += SC) {
       const int nc = (int)min((int64_t)SC, send - c0);
       if (qs0 < qsd) {
+#pragma unroll 8
         for (int sl = qs0; sl < SC; sl += qsd) {
           T q = ScalarTraits<T>::zero();
           if (sl < nc) {
@@ -1805,6 +1806,7 @@ __global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ohu_tile_kernel(c
         }
       }
       if (ss0 < ssd) {
+#pragma unroll 8
         for (int sl = ss0; sl < SC; sl += ssd) {
           float sg = 0.f;
           if (sl < nc) {

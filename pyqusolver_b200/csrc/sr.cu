@@ -1792,28 +1792,54 @@ __global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ohu_tile_kernel(c
       for (int b = 0; b < 4; ++b) acc[a][b] = ScalarTraits<T>::zero();
     for (int64_t c0 = sbeg; c0 < send; c0 += SC) {
       const int nc = (int)min((int64_t)SC, send - c0);
+      // staging in batches of SB rows per thread: the global loads of a batch are issued together
+      constexpr int SB = ScalarTraits<T>::is_complex ? 8 : 4;   // real: within the 64-register budget
       if (qs0 < qsd) {
-#pragma unroll 8
-        for (int sl = qs0; sl < SC; sl += qsd) {
-          T q = ScalarTraits<T>::zero();
-          if (sl < nc) {
-            const float2 wv = wb[c0 + sl];
-            const T u = from_c(make_float2((wv.x - mr) * fs, (wv.y - mi) * fs), T());
-            if (qm < nh) q = mulx(conjx(tb[(c0 + sl) * nh + qm]), u);
-            else if (qm == nh) q = u;                                      // virtual unit: g_a
+        for (int sl0 = qs0; sl0 < SC; sl0 += SB * qsd) {
+          T tv[SB];
+          float2 wv[SB];
+#pragma unroll
+          for (int b = 0; b < SB; ++b) {
+            const int sl = sl0 + b * qsd;
+            const bool ok = sl < nc;
+            wv[b] = ok ? wb[c0 + sl] : make_float2(0.f, 0.f);
+            tv[b] = (ok && qm < nh) ? tb[(c0 + sl) * nh + qm] : ScalarTraits<T>::zero();
           }
-          Q[sl * qstride + qm] = q;
+#pragma unroll
+          for (int b = 0; b < SB; ++b) {
+            const int sl = sl0 + b * qsd;
+            if (sl < SC) {
+              T q = ScalarTraits<T>::zero();
+              if (sl < nc) {
+                const T u = from_c(make_float2((wv[b].x - mr) * fs, (wv[b].y - mi) * fs), T());
+                if (qm < nh) q = mulx(conjx(tv[b]), u);
+                else if (qm == nh) q = u;                                  // virtual unit: g_a
+              }
+              Q[sl * qstride + qm] = q;
+            }
+          }
         }
       }
       if (ss0 < ssd) {
-#pragma unroll 8
-        for (int sl = ss0; sl < SC; sl += ssd) {
-          float sg = 0.f;
-          if (sl < nc) {
-            if (si < ns) sg = ((bw[(c0 + sl) * nw + (si >> 5)] >> (si & 31)) & 1u) ? 1.f : -1.f;
-            else if (si == ns) sg = 1.f;                                   // virtual site: g_b
+        for (int sl0 = ss0; sl0 < SC; sl0 += SB * ssd) {
+          uint32_t wd[SB];
+#pragma unroll
+          for (int b = 0; b < SB; ++b) {
+            const int sl = sl0 + b * ssd;
+            wd[b] = (sl < nc && si < ns) ? bw[(c0 + sl) * nw + (si >> 5)] : 0u;
           }
-          sig[sl * sstride + si] = sg;
+#pragma unroll
+          for (int b = 0; b < SB; ++b) {
+            const int sl = sl0 + b * ssd;
+            if (sl < SC) {
+              float sg = 0.f;
+              if (sl < nc) {
+                if (si < ns) sg = ((wd[b] >> (si & 31)) & 1u) ? 1.f : -1.f;
+                else if (si == ns) sg = 1.f;                               // virtual site: g_b
+              }
+              sig[sl * sstride + si] = sg;
+            }
+          }
         }
       }
       __syncthreads();

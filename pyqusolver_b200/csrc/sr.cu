@@ -1781,9 +1781,13 @@ __global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ohu_tile_kernel(c
   const int si = tid % nsp, ss0 = tid / nsp, ssd = nthr / nsp;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   T* out = partial + I.sr_part_off + (int64_t)it.y * P;
+  // small problems: the block's threads form G sample groups over the tiles (group g takes the
+  // samples g, g + G, ...), summed in a fixed order at the end; large ones take passes over the tiles
+  const int G = (n_tiles <= nthr) ? nthr / n_tiles : 1;
   for (int t0 = 0; t0 < n_tiles; t0 += nthr) {
-    const int t = t0 + tid;
-    const bool active = t < n_tiles;
+    const int t = (G > 1) ? tid % n_tiles : t0 + tid;
+    const int grp = (G > 1) ? tid / n_tiles : 0;
+    const bool active = (G > 1) ? grp < G : t < n_tiles;
     const int tm = active ? t % nmt : 0, ti = active ? t / nmt : 0;
     T acc[4][4];
 #pragma unroll
@@ -1844,7 +1848,7 @@ __global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ohu_tile_kernel(c
       }
       __syncthreads();
       if (active) {
-        for (int sl = 0; sl < nc; ++sl) {
+        for (int sl = grp; sl < nc; sl += G) {
           const float4 s4 = *reinterpret_cast<const float4*>(sig + sl * sstride + 4 * ti);
           T q[4];
           if constexpr (ScalarTraits<T>::is_complex) {
@@ -1865,7 +1869,25 @@ __global__ void __launch_bounds__(bohu_max_threads<T>()) batch_ohu_tile_kernel(c
       }
       __syncthreads();
     }
-    if (active) {
+    if (G > 1) {
+      // group partials through shared memory (the staging buffers are free), group 0 adds them
+      T* gred = reinterpret_cast<T*>(boh_sm);             // [G][n_tiles][16]
+      if (active) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) gred[((size_t)grp * n_tiles + t) * 16 + a * 4 + b] = acc[a][b];
+      }
+      __syncthreads();
+      if (active && grp == 0) {
+        for (int g = 1; g < G; ++g)
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = addx(acc[a][b], gred[((size_t)g * n_tiles + t) * 16 + a * 4 + b]);
+      }
+    }
+    if (active && grp == 0) {
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         const int i = 4 * ti + a;
@@ -2068,8 +2090,9 @@ static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, c
   const int ohu_threads =
       std::min(bohu_max_threads<T>(), (std::max({max_tiles, ohu_qstride, ohu_sstride}) + 31) / 32 * 32);
   const int ohu_sc = batch_ohu_sc<T>(max_ns, max_nh);
-  const size_t ohu_smem = (size_t)bsmall_align16((int64_t)ohu_sc * ohu_qstride * sizeof(T)) +
-                          (size_t)ohu_sc * ohu_sstride * sizeof(float);
+  const size_t ohu_smem = std::max((size_t)bsmall_align16((int64_t)ohu_sc * ohu_qstride * sizeof(T)) +
+                                       (size_t)ohu_sc * ohu_sstride * sizeof(float),
+                                   (size_t)ohu_threads * 16 * sizeof(T));      // sample-group partials
   // O v: enough threads for the staging rows (BOV_ROWS signs, nh + ... V columns) and the tiles
   const int ov_threads = std::min(bohu_max_threads<T>(),
                                   (std::max({(BOV_ROWS / 4) * (bov_round4(max_nh) / 4), bov_round4(max_nh), BOV_ROWS}) +

@@ -147,6 +147,13 @@ int qes_sampler_run_betas(int dtype, const qes_sampler_config* cfg, const float*
  * order); results are the same either way.                                  */
 int qes_set_pdl(int on);
 
+/* Which sampler kernel runs a chain set whose theta caches live in registers
+ * (process-wide): 0 = the uncapped kernel (up to 128 registers, 16 chains per
+ * SM); 1 = the kernel capped at 72 registers (28 chains per SM) when that
+ * needs fewer waves of resident chains and spills no more (default);
+ * 2 = the capped kernel always.  Samples are the same in every mode.        */
+int qes_sampler_set_capped(int mode);
+
 /* Parallel tempering (QES/Solver/MonteCarlo/vmc.py:1289-1507).  Chains are
  * n_replicas slots x n_chains (chain index r * n_chains + c); chain_beta holds
  * each chain's current beta.  qes_pt_swap exchanges beta labels between

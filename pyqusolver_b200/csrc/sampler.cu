@@ -13,6 +13,9 @@
 //   log_acc = min(beta*mu*Re dlogpsi, 0); accept iff log u < log_acc;
 //   exchange with an invalid slot or equal spins is a no-op with dlogpsi = 0,
 //   accepted (u < 1); proposed += 1 and accepted += keep for every proposal.
+#include <algorithm>
+#include <atomic>
+
 #include "common.cuh"
 
 #define QES_ARG_CHECK(cond, msg) do { if (!(cond)) { qes_set_last_message(msg); return QES_ERR_ARG; } } while (0)
@@ -298,8 +301,9 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
 }
 
 // Wide theta caches (SMEM = true) live in dynamic shared memory, 2 * 32 * MPL elements per warp.
-template <class T, int MPL, int RULE, bool SMEM>
-__global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
+// MINB > 1 caps the registers so that MINB blocks share an SM (more chains resident at once).
+template <class T, int MPL, int RULE, bool SMEM, int MINB = 1>
+__global__ void __launch_bounds__(32 * SMP_WARPS, MINB) sampler_kernel(
     qes_sampler_config cfg, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ W,
     const T* __restrict__ flipC, const T* __restrict__ flipS, const int32_t* __restrict__ nbr,
     const int32_t* __restrict__ nbr_pair, const int32_t* __restrict__ pair_i, const int32_t* __restrict__ pair_j,
@@ -330,6 +334,66 @@ __global__ void __launch_bounds__(32 * SMP_WARPS) sampler_kernel(
 template <class T, int MPL>
 constexpr bool sampler_smem_cache() { return MPL > (ScalarTraits<T>::is_complex ? 8 : 16); }
 
+template <class T, int MPL, int RULE, bool SM, int MINB>
+static int launch_sampler_kernel(unsigned grid, size_t smem, const qes_sampler_config* cfg, const void* a,
+                                 const void* b, const void* W, const void* flipC, const void* flipS,
+                                 const int32_t* nbr, const int32_t* nbr_pair, const int32_t* pi, const int32_t* pj,
+                                 const void* pairC, const void* pairS, uint32_t* chain_bits, uint64_t* chain_step,
+                                 int32_t* proposed, int32_t* accepted, uint32_t* sample_bits, void* sample_logpsi,
+                                 void* last_logpsi, const float* chain_beta, cudaStream_t st) {
+  if (SM)
+    QES_CUDA_CHECK(cudaFuncSetAttribute(sampler_kernel<T, MPL, RULE, SM, MINB>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  sampler_kernel<T, MPL, RULE, SM, MINB><<<grid, 32 * SMP_WARPS, smem, st>>>(
+      *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
+      (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
+      (T*)sample_logpsi, (T*)last_logpsi, chain_beta);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
+// Register-resident caches: the kernel with the register cap (7 blocks of 4 chains per SM) runs
+// when it needs fewer waves of resident chains than the uncapped one (more chains than one wave
+// of the latter) and spills no more than it; otherwise the uncapped kernel.  Both run the same
+// arithmetic in the same order, so the choice never changes a sample.
+// qes_sampler_set_capped: 0 never, 1 by the wave count (default), 2 always where instantiated.
+constexpr int SMP_CAPPED_BLOCKS = 7;
+static std::atomic<int> g_smp_capped{1};
+extern "C" int qes_sampler_set_capped(int mode) {
+  if (mode < 0 || mode > 2) {
+    qes_set_last_message("qes_sampler_set_capped: mode must be 0, 1 or 2");
+    return QES_ERR_ARG;
+  }
+  g_smp_capped.store(mode);
+  return QES_OK;
+}
+
+template <class T, int MPL, int RULE>
+static int sampler_pick_capped(const qes_sampler_config* cfg, bool* capped) {
+  *capped = false;
+  const int mode = g_smp_capped.load(std::memory_order_relaxed);
+  if (mode == 0) return QES_OK;
+  if (mode == 2) {
+    *capped = true;
+    return QES_OK;
+  }
+  cudaFuncAttributes f1{}, f7{};
+  QES_CUDA_CHECK(cudaFuncGetAttributes(&f1, sampler_kernel<T, MPL, RULE, false, 1>));
+  QES_CUDA_CHECK(cudaFuncGetAttributes(&f7, sampler_kernel<T, MPL, RULE, false, SMP_CAPPED_BLOCKS>));
+  if (f7.localSizeBytes > f1.localSizeBytes) return QES_OK;
+  int dev = 0, nsm = 0, b1 = 0, b7 = 0;
+  QES_CUDA_CHECK(cudaGetDevice(&dev));
+  QES_CUDA_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  QES_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, sampler_kernel<T, MPL, RULE, false, 1>,
+                                                               32 * SMP_WARPS, 0));
+  QES_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &b7, sampler_kernel<T, MPL, RULE, false, SMP_CAPPED_BLOCKS>, 32 * SMP_WARPS, 0));
+  const int64_t n = cfg->n_chains;
+  const int64_t cap1 = (int64_t)std::max(b1, 1) * SMP_WARPS * nsm, cap7 = (int64_t)std::max(b7, 1) * SMP_WARPS * nsm;
+  *capped = (n + cap7 - 1) / cap7 < (n + cap1 - 1) / cap1;
+  return QES_OK;
+}
+
 template <class T, int MPL>
 static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, const void* b, const void* W,
                               const void* flipC, const void* flipS, const int32_t* nbr, const int32_t* nbr_pair,
@@ -340,25 +404,23 @@ static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, cons
   constexpr bool SM = sampler_smem_cache<T, MPL>();
   const unsigned grid = (unsigned)((cfg->n_chains + SMP_WARPS - 1) / SMP_WARPS);
   const size_t smem = SM ? (size_t)SMP_WARPS * 2 * 32 * MPL * sizeof(T) : 0;
+#define QES_SMP_ARGS grid, smem, cfg, a, b, W, flipC, flipS, nbr, nbr_pair, pi, pj, pairC, pairS, chain_bits, \
+                     chain_step, proposed, accepted, sample_bits, sample_logpsi, last_logpsi, chain_beta, st
   if (cfg->rule == QES_RULE_LOCAL) {
-    if (SM)
-      QES_CUDA_CHECK(cudaFuncSetAttribute(sampler_kernel<T, MPL, QES_RULE_LOCAL, SM>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    sampler_kernel<T, MPL, QES_RULE_LOCAL, SM><<<grid, 32 * SMP_WARPS, smem, st>>>(
-        *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
-        (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
-        (T*)sample_logpsi, (T*)last_logpsi, chain_beta);
-  } else {
-    if (SM)
-      QES_CUDA_CHECK(cudaFuncSetAttribute(sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM><<<grid, 32 * SMP_WARPS, smem, st>>>(
-        *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,
-        (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits,
-        (T*)sample_logpsi, (T*)last_logpsi, chain_beta);
+    if constexpr (!SM) {
+      bool capped = false;
+      if (int rc = sampler_pick_capped<T, MPL, QES_RULE_LOCAL>(cfg, &capped)) return rc;
+      if (capped) return launch_sampler_kernel<T, MPL, QES_RULE_LOCAL, false, SMP_CAPPED_BLOCKS>(QES_SMP_ARGS);
+    }
+    return launch_sampler_kernel<T, MPL, QES_RULE_LOCAL, SM, 1>(QES_SMP_ARGS);
   }
-  QES_LAUNCH_CHECK();
-  return QES_OK;
+  if constexpr (!SM) {
+    bool capped = false;
+    if (int rc = sampler_pick_capped<T, MPL, QES_RULE_EXCHANGE>(cfg, &capped)) return rc;
+    if (capped) return launch_sampler_kernel<T, MPL, QES_RULE_EXCHANGE, false, SMP_CAPPED_BLOCKS>(QES_SMP_ARGS);
+  }
+  return launch_sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM, 1>(QES_SMP_ARGS);
+#undef QES_SMP_ARGS
 }
 
 template <class T>

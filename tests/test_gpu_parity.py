@@ -306,6 +306,33 @@ def test_sampler_exchange_trajectory_matches_oracle(cplx):
     assert np.mean(acc_g != ref.accepted) <= 0.05
 
 
+@pytest.mark.parametrize("rule,cplx,nh", [("LOCAL", False, 64), ("EXCHANGE", True, 200), ("EXCHANGE", False, 20)])
+def test_capped_sampler_kernel_is_bit_identical(rule, cplx, nh):
+    """The register-capped sampler kernel (more chains resident per SM) and the uncapped one
+    draw the same chains: identical samples, log-amplitudes and acceptance counts; the capped
+    run also follows the oracle's trajectory."""
+    L, OL = qb.SquareLattice(2, 4, 4), olat.SquareLattice(2, 4, 4)
+    ns = 16
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=19, init_scale=0.1)
+    kw = dict(lattice=L, init="RND_FIXED", n_up=8) if rule == "EXCHANGE" else {}
+    out = []
+    try:
+        for mode in (0, 2):
+            _lib.call("qes_sampler_set_capped", mode)
+            smp = _gpu_sampler(net, rule, ns, 256, seed=23, therm=2, sweep=6, **kw)
+            bits, lp = smp.sample_bits(num_samples=4)
+            out.append((bits.cpu().numpy(), lp.cpu().numpy(), smp.accepted.cpu().numpy()))
+    finally:
+        _lib.call("qes_sampler_set_capped", 1)
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
+    okw = dict(neighbor_table=olat.neighbor_table(OL), init="RND_FIXED", n_up=8) if rule == "EXCHANGE" else {}
+    ref = osm.MetropolisSampler(ns, 256, rule=rule, seed=23, therm_steps=2, sweep_steps=6, **okw)
+    cfg, _, _ = ref.sample(oracle_params(net), 4)
+    got = dv.unpack_states(torch.as_tensor(out[1][0]).cuda(), ns, 1.0).cpu().numpy()
+    assert np.mean(np.any(got != cfg, axis=1)) <= 0.02
+
+
 @pytest.mark.parametrize("rule", ["LOCAL", "EXCHANGE"])
 def test_sampler_matches_exact_distribution(rule):
     ns = 10

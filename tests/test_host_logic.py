@@ -151,6 +151,9 @@ def test_library_rejects_bad_arguments_without_gpu():
     assert e.value.code == _lib.QES_ERR_ARG
     with pytest.raises(_lib.QESError):
         _lib.call("qes_rbm_forward", 7, 4, 4, 1, None, None, None, None, None, None, None, None)
+    with pytest.raises(_lib.QESError) as e:
+        _lib.call("qes_sampler_set_capped", 3)
+    assert e.value.code == _lib.QES_ERR_ARG
 
 
 def test_torch_ops_are_registered():

@@ -40,7 +40,7 @@ struct ThetaCache<T, MPL, false> {
   static constexpr int kMPL = MPL;
   static constexpr bool kSmem = false;
   T th_[MPL], tn_[MPL];
-  QES_D void bind(T*, int) {}
+  QES_D void bind(T*, int, int) {}
   QES_D T& th(int r) { return th_[r]; }
   QES_D T& tn(int r) { return tn_[r]; }
 };
@@ -50,7 +50,9 @@ struct ThetaCache<T, MPL, true> {
   static constexpr bool kSmem = true;
   T* th_;
   T* tn_;
-  QES_D void bind(T* warp_slice, int lane) { th_ = warp_slice + lane; tn_ = warp_slice + 32 * MPL + lane; }
+  // the warp's slice holds rows = ceil(nh / 32) rows of theta, then as many of tanh(theta); rows at
+  // or past `rows` do not exist and are never touched
+  QES_D void bind(T* warp_slice, int lane, int rows) { th_ = warp_slice + lane; tn_ = warp_slice + 32 * rows + lane; }
   QES_D T& th(int r) { return th_[32 * r]; }
   QES_D T& tn(int r) { return tn_[32 * r]; }
 };
@@ -86,8 +88,10 @@ QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __
     }
 #pragma unroll
     for (int r = 0; r < CH; ++r) {
-      c.th(c0 + r) = acc[r];
-      c.tn(c0 + r) = tanhx(acc[r]);
+      if (!Cache::kSmem || 32 * (c0 + r) < nh) {
+        c.th(c0 + r) = acc[r];
+        c.tn(c0 + r) = tanhx(acc[r]);
+      }
     }
   }
 }
@@ -142,7 +146,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
   const float bm = P.beta_mu;
 
   ThetaCache<T, MPL, SMEM> cache;
-  cache.bind(theta_slice, lane);
+  cache.bind(theta_slice, lane, (nh + 31) >> 5);
   full_theta<T>(ns, nh, lane, cw, b, W, cache);
   int since = 0;
 
@@ -209,7 +213,8 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
 #pragma unroll
           for (int q = 0; q < PF; ++q) {
             const int rr = c0 + q;
-            prod = mulx(prod, ratio_factor(cb[cur][q], g, cache.tn(rr), sb[cur][q]));
+            const T t = (!SMEM || 32 * rr < nh) ? cache.tn(rr) : ScalarTraits<T>::zero();
+            prod = mulx(prod, ratio_factor(cb[cur][q], g, t, sb[cur][q]));
             if ((rr & 7) == 7) renorm(prod, ex);
           }
         }
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(32 * SMP_WARPS, MINB) sampler_kernel(
   P.chain_id = cfg.chain_offset + chain;
   P.a = a; P.b = b; P.W = W; P.flipC = flipC; P.flipS = flipS; P.pairC = pairC; P.pairS = pairS;
   P.nbr = nbr; P.nbr_pair = nbr_pair; P.pair_i = pair_i; P.pair_j = pair_j;
-  T* slice = SMEM ? reinterpret_cast<T*>(theta_sm) + (size_t)wid * 2 * 32 * MPL : nullptr;
+  T* slice = SMEM ? reinterpret_cast<T*>(theta_sm) + (size_t)wid * 2 * 32 * ((cfg.nh + 31) >> 5) : nullptr;
   run_chain<T, MPL, RULE, SMEM>(P, chain, cfg_sm[wid], slice, chain_bits, chain_step, proposed, accepted,
                                 sample_bits, sample_logpsi, last_logpsi);
 }
@@ -358,6 +363,9 @@ static int launch_sampler_kernel(unsigned grid, size_t smem, const qes_sampler_c
 // arithmetic in the same order, so the choice never changes a sample.
 // qes_sampler_set_capped: 0 never, 1 by the wave count (default), 2 always where instantiated.
 constexpr int SMP_CAPPED_BLOCKS = 7;
+// Shared-memory caches (wide hidden layers): capped at 128 registers so that four blocks (16
+// chains) share an SM where their slices fit; uncapped, up to 255 registers left two.
+constexpr int SMP_SMEM_BLOCKS = 4;
 static std::atomic<int> g_smp_capped{1};
 extern "C" int qes_sampler_set_capped(int mode) {
   if (mode < 0 || mode > 2) {
@@ -403,7 +411,8 @@ static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, cons
                               cudaStream_t st) {
   constexpr bool SM = sampler_smem_cache<T, MPL>();
   const unsigned grid = (unsigned)((cfg->n_chains + SMP_WARPS - 1) / SMP_WARPS);
-  const size_t smem = SM ? (size_t)SMP_WARPS * 2 * 32 * MPL * sizeof(T) : 0;
+  // shared-memory caches are sized to the hidden layer (ceil(nh / 32) rows), not to MPL
+  const size_t smem = SM ? (size_t)SMP_WARPS * 2 * 32 * ((cfg->nh + 31) / 32) * sizeof(T) : 0;
 #define QES_SMP_ARGS grid, smem, cfg, a, b, W, flipC, flipS, nbr, nbr_pair, pi, pj, pairC, pairS, chain_bits, \
                      chain_step, proposed, accepted, sample_bits, sample_logpsi, last_logpsi, chain_beta, st
   if (cfg->rule == QES_RULE_LOCAL) {
@@ -412,14 +421,14 @@ static int launch_sampler_mpl(const qes_sampler_config* cfg, const void* a, cons
       if (int rc = sampler_pick_capped<T, MPL, QES_RULE_LOCAL>(cfg, &capped)) return rc;
       if (capped) return launch_sampler_kernel<T, MPL, QES_RULE_LOCAL, false, SMP_CAPPED_BLOCKS>(QES_SMP_ARGS);
     }
-    return launch_sampler_kernel<T, MPL, QES_RULE_LOCAL, SM, 1>(QES_SMP_ARGS);
+    return launch_sampler_kernel<T, MPL, QES_RULE_LOCAL, SM, SM ? SMP_SMEM_BLOCKS : 1>(QES_SMP_ARGS);
   }
   if constexpr (!SM) {
     bool capped = false;
     if (int rc = sampler_pick_capped<T, MPL, QES_RULE_EXCHANGE>(cfg, &capped)) return rc;
     if (capped) return launch_sampler_kernel<T, MPL, QES_RULE_EXCHANGE, false, SMP_CAPPED_BLOCKS>(QES_SMP_ARGS);
   }
-  return launch_sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM, 1>(QES_SMP_ARGS);
+  return launch_sampler_kernel<T, MPL, QES_RULE_EXCHANGE, SM, SM ? SMP_SMEM_BLOCKS : 1>(QES_SMP_ARGS);
 #undef QES_SMP_ARGS
 }
 

@@ -30,6 +30,16 @@ QES_D float log_abs<float>(float v) { return logf(fabsf(v)); }
 template <>
 QES_D float log_abs<float2>(float2 v) { return 0.5f * logf(v.x * v.x + v.y * v.y); }
 
+// tanh(theta) for the acceptance cache.  Real units: tanh x = 1 - 2 / (e^{2x} + 1) with the
+// hardware exponential and reciprocal approximations, a handful of instructions against the
+// branchy accurate tanhf that dominated the accepted-move update.  The absolute error stays below
+// about 5e-7 (the identity never divides by less than one; e^{2x} overflows to +inf and underflows
+// to 0, giving exactly +-1), and the cache enters the ratio only as C + g t S with |S| small against
+// C, so the acceptance ratio moves by a relative ~1e-7, the size of its own float32 rounding.
+// Complex units keep the accurate complex tanh (poles of tanh need the careful form).
+QES_D float tanh_cache(float x) { return 1.f - __fdividef(2.f, __expf(2.f * x) + 1.f); }
+QES_D float2 tanh_cache(float2 z) { return tanhx(z); }
+
 // theta / tanh(theta) of one chain: lane l owns hidden units m = l + 32 r (r < MPL), held in
 // registers (narrow caches) or in a per-warp slice of shared memory (wide caches, where a
 // register-resident cache would cap the SM at a few warps)
@@ -90,7 +100,7 @@ QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __
     for (int r = 0; r < CH; ++r) {
       if (!Cache::kSmem || 32 * (c0 + r) < nh) {
         c.th(c0 + r) = acc[r];
-        c.tn(c0 + r) = tanhx(acc[r]);
+        c.tn(c0 + r) = tanh_cache(acc[r]);
       }
     }
   }
@@ -254,7 +264,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
             if (lane + 32 * rr < nh) {
               const T t2 = addx(cache.th(rr), scal(2.f * g, d[q]));
               cache.th(rr) = t2;
-              cache.tn(rr) = tanhx(t2);
+              cache.tn(rr) = tanh_cache(t2);
             }
           }
         }
@@ -267,7 +277,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
             if (j0 >= 0) d = addx(d, scal(-1.f, wj[m]));
             const T t2 = addx(cache.th(rr), scal(2.f * g, d));
             cache.th(rr) = t2;
-            cache.tn(rr) = tanhx(t2);
+            cache.tn(rr) = tanh_cache(t2);
           }
         }
       }

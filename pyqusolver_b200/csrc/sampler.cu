@@ -201,7 +201,9 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
       if constexpr (MPL >= 16) {
         // the table row is fetched a chunk ahead of the product so that its L2 round trips overlap;
         // units beyond nh read as (C, S) = (1, 0), an exact factor of one
-        constexpr int PF = 16;
+        // 12 units per chunk for real shared-memory caches (measured faster than 8 or 16 on nh = 1600:
+        // fewer registers live at 128); chunks past MPL read as factors of one
+        constexpr int PF = (SMEM && !ScalarTraits<T>::is_complex) ? 12 : 16;
         T cb[2][PF], sb[2][PF];
 #pragma unroll
         for (int q = 0; q < PF; ++q) {

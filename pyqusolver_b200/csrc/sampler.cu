@@ -30,15 +30,34 @@ QES_D float log_abs<float>(float v) { return logf(fabsf(v)); }
 template <>
 QES_D float log_abs<float2>(float2 v) { return 0.5f * logf(v.x * v.x + v.y * v.y); }
 
-// tanh(theta) for the acceptance cache.  Real units: tanh x = 1 - 2 / (e^{2x} + 1) with the
-// hardware exponential and reciprocal approximations, a handful of instructions against the
-// branchy accurate tanhf that dominated the accepted-move update.  The absolute error stays below
-// about 5e-7 (the identity never divides by less than one; e^{2x} overflows to +inf and underflows
-// to 0, giving exactly +-1), and the cache enters the ratio only as C + g t S with |S| small against
-// C, so the acceptance ratio moves by a relative ~1e-7, the size of its own float32 rounding.
-// Complex units keep the accurate complex tanh (poles of tanh need the careful form).
+// tanh(theta) for the acceptance cache, from the hardware exponential, sine/cosine and reciprocal
+// approximations: a handful of instructions against the accurate library forms, whose cost
+// dominated the accepted-move update (most proposals are accepted near initialisation).  The cache
+// enters the ratio only as C + g t S, so an absolute error of a few 1e-7 in t moves the acceptance
+// ratio by a relative ~1e-7, the size of its own float32 rounding; theta itself stays exact (it
+// feeds log psi) and the forward, local-energy and SR kernels keep the accurate tanh.
+//
+// Real: tanh x = 1 - 2 / (e^{2x} + 1).  The divisor is at least one, so the absolute error stays
+// below about 5e-7; e^{2x} overflows to +inf or underflows to 0 and gives exactly +-1, never NaN.
 QES_D float tanh_cache(float x) { return 1.f - __fdividef(2.f, __expf(2.f * x) + 1.f); }
-QES_D float2 tanh_cache(float2 z) { return tanhx(z); }
+// Complex: the pole-safe form of tanhx, tanh(x+iy) = [sign(x)(1 - q^2) + i 4 q sin y cos y] /
+// [(1 - q)^2 + 4 q cos^2 y] with q = e^{-2|x|} in (0, 1], so no term cancels except near the poles
+// (x = 0, cos y = 0) where t is large in any evaluation.  y is first reduced to [-pi, pi] by
+// Cody-Waite reduction (2 pi split into a float head and tail) because the hardware sine/cosine
+// is accurate (abs error ~4e-7) only on that interval.
+QES_D float2 tanh_cache(float2 z) {
+  const float q = __expf(-2.f * fabsf(z.x));
+  const float em = q - 1.f;                                      // q - 1, exact subtraction
+  const float k = rintf(z.y * 0.15915494309189535f);             // y / (2 pi), nearest integer
+  float y = fmaf(-k, 6.28318548202514648f, z.y);                 // float(2 pi)
+  y = fmaf(-k, -1.7484555314695172e-7f, y);                      // 2 pi - float(2 pi)
+  float sy, cy;
+  __sincosf(y, &sy, &cy);
+  const float den = em * em + 4.f * q * cy * cy;
+  const float re = __fdividef(copysignf(-em * (2.f + em), z.x), den);
+  const float im = __fdividef(4.f * q * sy * cy, den);
+  return make_float2(re, im);
+}
 
 // theta / tanh(theta) of one chain: lane l owns hidden units m = l + 32 r (r < MPL), held in
 // registers (narrow caches) or in a per-warp slice of shared memory (wide caches, where a

@@ -154,6 +154,12 @@ int qes_set_pdl(int on);
  * 2 = the capped kernel always.  Samples are the same in every mode.        */
 int qes_sampler_set_capped(int mode);
 
+/* The sampler's tanh of its acceptance cache applied elementwise (y = tanh x,
+ * n elements of dtype): hardware exponential / sine / cosine / reciprocal
+ * approximations, absolute error a few 1e-7 away from the poles of complex
+ * tanh.  Exposed so that the error bound can be checked against float64.    */
+int qes_sampler_tanh_cache(int dtype, int64_t n, const void* x, void* y, void* stream);
+
 /* Parallel tempering (QES/Solver/MonteCarlo/vmc.py:1289-1507).  Chains are
  * n_replicas slots x n_chains (chain index r * n_chains + c); chain_beta holds
  * each chain's current beta.  qes_pt_swap exchanges beta labels between

@@ -103,6 +103,7 @@ SIGNATURES = {
                               C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "qes_set_pdl": [C.c_int],
     "qes_sampler_set_capped": [C.c_int],
+    "qes_sampler_tanh_cache": [C.c_int, _i64, _vp, _vp, _vp],
     "qes_pt_swap": [C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_float, _u64, _i64, _vp, _vp],
     "qes_pt_collect": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_float, _vp, _vp, _vp, _vp, _vp],
     "qes_loss_stats_workspace_bytes": [_i64, C.POINTER(_sz)],

@@ -592,6 +592,27 @@ __global__ void pt_collect_kernel(int R, int n_chains, int nw, const float* __re
   if (out_logpsi) out_logpsi[c] = logpsi[src];
 }
 
+template <class T>
+__global__ void tanh_cache_kernel(int64_t n, const T* __restrict__ x, T* __restrict__ y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = tanh_cache(x[i]);
+}
+
+extern "C" int qes_sampler_tanh_cache(int dtype, int64_t n, const void* x, void* y, void* stream) {
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sampler_tanh_cache: bad dtype");
+  QES_ARG_CHECK(n >= 0, "qes_sampler_tanh_cache: bad size");
+  if (n == 0) return QES_OK;
+  QES_ARG_CHECK(x && y, "qes_sampler_tanh_cache: null pointer");
+  const int bs = 256;
+  const unsigned grid = (unsigned)((n + bs - 1) / bs);
+  if (dtype == QES_DTYPE_F32)
+    tanh_cache_kernel<float><<<grid, bs, 0, (cudaStream_t)stream>>>(n, (const float*)x, (float*)y);
+  else
+    tanh_cache_kernel<float2><<<grid, bs, 0, (cudaStream_t)stream>>>(n, (const float2*)x, (float2*)y);
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
+
 extern "C" int qes_pt_swap(int dtype, int n_replicas, int n_chains, const void* logpsi, float* chain_beta, float mu,
                            uint64_t seed, int64_t round, int* swaps_accepted, void* stream) {
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_pt_swap: bad dtype");

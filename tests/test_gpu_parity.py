@@ -333,6 +333,32 @@ def test_capped_sampler_kernel_is_bit_identical(rule, cplx, nh):
     assert np.mean(np.any(got != cfg, axis=1)) <= 0.02
 
 
+def test_sampler_tanh_cache_error_bound():
+    """The sampler's acceptance-cache tanh (hardware approximations) against float64 tanh of the
+    same float32 inputs: absolute error below 1e-6, scaled by 1 + |t|^2 for complex arguments
+    (the sensitivity of tanh near its poles); large |Im| exercises the reduction to [-pi, pi]."""
+    rng = np.random.default_rng(5)
+    xr = np.concatenate([np.linspace(-60, 60, 20001), rng.normal(scale=1e-3, size=4000),
+                         [0.0, -0.0, 1e-30, -1e-30, 88.0, -88.0, 1e4, -1e4]]).astype(np.float32)
+    yr = torch.empty(len(xr), dtype=torch.float32, device="cuda")
+    _lib.call("qes_sampler_tanh_cache", _lib.DTYPE_F32, len(xr), _lib.ptr(torch.as_tensor(xr).cuda()), _lib.ptr(yr),
+              _lib.stream_ptr())
+    got = yr.cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(got))
+    assert np.max(np.abs(got - np.tanh(xr.astype(np.float64)))) < 1e-6
+    n = 200000
+    z = (rng.uniform(-6, 6, n) + 1j * rng.uniform(-40, 40, n)).astype(np.complex64)
+    z[:1000] = (rng.normal(scale=1e-3, size=1000) + 1j * rng.uniform(-3, 3, 1000)).astype(np.complex64)
+    zt = torch.as_tensor(z).cuda()
+    yt = torch.empty_like(zt)
+    torch.cuda.synchronize()
+    _lib.call("qes_sampler_tanh_cache", _lib.DTYPE_C64, n, _lib.ptr(zt), _lib.ptr(yt), _lib.stream_ptr())
+    got = yt.cpu().numpy().astype(np.complex128)
+    ref = np.tanh(z.astype(np.complex128))
+    err = np.abs(got - ref) / (1.0 + np.abs(ref) ** 2)
+    assert np.max(err) < 1e-6, np.max(err)
+
+
 @pytest.mark.parametrize("rule", ["LOCAL", "EXCHANGE"])
 def test_sampler_matches_exact_distribution(rule):
     ns = 10

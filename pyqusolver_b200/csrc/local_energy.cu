@@ -66,11 +66,27 @@ QES_D void eloc_moves_block(int kb, int64_t sb, int ns, int nh, int64_t n_sample
   for (int q = 0; q < ELOC_SPT; ++q) { acc[q] = ScalarTraits<T>::one(); ex[q] = 0; }
 
   if (kval) {
-    for (int m0 = 0; m0 < nh; m0 += ELOC_RENORM) {
-      const int m1 = min(nh, m0 + ELOC_RENORM);
-      for (int m = m0; m < m1; ++m) {
-        const T c = Ct[(int64_t)m * K + k];
-        const T s = St[(int64_t)m * K + k];
+    // whole blocks of ELOC_RENORM units unrolled, then the tail; the same factor order and the same
+    // renormalisation points as one loop over m
+    const T* cp = Ct + k;
+    const T* sp = St + k;
+    int m0 = 0;
+    for (; m0 + ELOC_RENORM <= nh; m0 += ELOC_RENORM) {
+#pragma unroll
+      for (int u = 0; u < ELOC_RENORM; ++u) {
+        const int m = m0 + u;
+        const T c = cp[(int64_t)m * K];
+        const T s = sp[(int64_t)m * K];
+#pragma unroll
+        for (int q = 0; q < ELOC_SPT; ++q) acc[q] = mulx(acc[q], ratio_factor(c, g[q], trow[q][m], s));
+      }
+#pragma unroll
+      for (int q = 0; q < ELOC_SPT; ++q) renorm(acc[q], ex[q]);
+    }
+    if (m0 < nh) {
+      for (int m = m0; m < nh; ++m) {
+        const T c = cp[(int64_t)m * K];
+        const T s = sp[(int64_t)m * K];
 #pragma unroll
         for (int q = 0; q < ELOC_SPT; ++q) acc[q] = mulx(acc[q], ratio_factor(c, g[q], trow[q][m], s));
       }

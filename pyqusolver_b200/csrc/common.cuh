@@ -67,6 +67,18 @@ inline cudaError_t qes_launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block,
 QES_D void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 QES_D void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Converged flag of a CG solve, read by the matvec kernels of later iterations before they wait
+// on their predecessor: once set (by the x/r update of the converging iteration) it stays set
+// until the next solve's setup, so a CTA that sees it may skip its work (the solution is final);
+// a CTA that reads a stale zero does the work, which nothing consumes any more.  One thread
+// reads it and the block follows that thread's value.
+QES_D bool cg_block_done(const double* flag) {
+  __shared__ int s_done;
+  if (threadIdx.x == 0) s_done = (flag != nullptr && *reinterpret_cast<const volatile double*>(flag) != 0.0) ? 1 : 0;
+  __syncthreads();
+  return s_done != 0;
+}
+
 // ----------------------------------------------------------------------------
 // scalar algebra on float / float2
 // ----------------------------------------------------------------------------

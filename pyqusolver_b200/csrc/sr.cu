@@ -133,8 +133,9 @@ template <class T, class V>
 __global__ void __launch_bounds__(OV_THREADS) ov_kernel(int ns, int nh, int64_t n_samples,
                                                         const uint32_t* __restrict__ bits,
                                                         const T* __restrict__ tanh_theta, const V* __restrict__ v,
-                                                        float2* __restrict__ w_out) {
+                                                        float2* __restrict__ w_out, const double* __restrict__ cg_done) {
   extern __shared__ uint32_t smw[];
+  if (cg_done && *cg_done != 0.0) return;                  // converged CG (stream order: exact)
   ov_block<T, V>((int64_t)blockIdx.x * OV_SB, smw, ns, nh, n_samples, bits, tanh_theta, v, w_out);
 }
 
@@ -258,7 +259,9 @@ QES_D void ohu_block(int bx, int by, int bz, int ns, int nh, int64_t n_samples, 
 template <class T>
 __global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
     int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ tanh_theta,
-    const float2* __restrict__ w, const double* __restrict__ wmean, double scale, T* __restrict__ partial) {
+    const float2* __restrict__ w, const double* __restrict__ wmean, double scale, T* __restrict__ partial,
+    const double* __restrict__ cg_done) {
+  if (cg_done && *cg_done != 0.0) return;                  // converged CG (stream order: exact)
   ohu_block<T>(blockIdx.x, blockIdx.y, blockIdx.z, ns, nh, n_samples, bits, tanh_theta, w, wmean, scale, partial);
 }
 
@@ -282,11 +285,13 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
                                                                       const V* __restrict__ p, V* __restrict__ y,
                                                                       double* __restrict__ dot_part,
                                                                       double* __restrict__ scal,
-                                                                      unsigned int* __restrict__ counter) {
+                                                                      unsigned int* __restrict__ counter,
+                                                                      const double* __restrict__ cg_done) {
   constexpr int E = VEC ? (int)(16 / sizeof(T)) : 1;      // columns per vector
   __shared__ V red[RS_THREADS * E];                        // [split group][column vector][E]
   pdl_trigger();
   pdl_wait();                                              // the partials: previous kernel
+  if (cg_done && *cg_done != 0.0) return;                  // converged CG: y is not read any more
   const int tid = threadIdx.x;
   const int groups = RS_THREADS / cv, c = tid % cv, sg = tid / cv;
   const int64_t nvec = P / E;                              // P % E == 0 when VEC
@@ -379,7 +384,8 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
 // when every split row starts on a 16-byte boundary
 template <class T, class V>
 static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, double shift, const V* p, V* y,
-                                double* dot_part, double* scal, unsigned int* counter, cudaStream_t st) {
+                                double* dot_part, double* scal, unsigned int* counter, cudaStream_t st,
+                                const double* cg_done = nullptr) {
   constexpr int EV = (int)(16 / sizeof(T));
   const bool vec = (P % EV == 0) && ((reinterpret_cast<uintptr_t>(partial) & 15) == 0);
   const int64_t nvec = vec ? P / EV : P;
@@ -392,10 +398,10 @@ static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, doub
   const int grid = (int)std::min<int64_t>((nvec + cv - 1) / cv, RS_MAX_BLOCKS);
   if (vec)
     QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, true>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
-                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter));
+                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done));
   else
     QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
-                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter));
+                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done));
   return QES_OK;
 }
 
@@ -427,16 +433,14 @@ __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* 
                                                             unsigned int* __restrict__ counter) {
   pdl_trigger();
   pdl_wait();                                              // Ap and alpha: previous kernel
-  const bool done = scal[4] != 0.0;
+  if (scal[4] != 0.0) return;                              // converged: x and r are final (every block)
   const double alpha = scal[7];
   double d = 0.0;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
     V rk = r[k];
-    if (!done) {
-      x[k] = vadd(x[k], vscale(alpha, p[k]));
-      rk = vadd(rk, vscale(-alpha, Ap[k]));
-      r[k] = rk;
-    }
+    x[k] = vadd(x[k], vscale(alpha, p[k]));
+    rk = vadd(rk, vscale(-alpha, Ap[k]));
+    r[k] = rk;
     d += vdotc(rk, rk);
   }
   __shared__ double red[RED_THREADS / 32];
@@ -792,19 +796,19 @@ extern "C" int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_sampl
 template <class T, class V>
 static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
                      const double* wmean, double scale, const SRWork& L, double shift, const V* p, V* y,
-                     double* dot_part, cudaStream_t st) {
+                     double* dot_part, cudaStream_t st, const double* cg_done = nullptr) {
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   const int64_t nsplit = (n_samples + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES;
   QES_ARG_CHECK(nsplit <= 65535, "SR: too many samples");
   dim3 grid((nh + OHU_TM - 1) / OHU_TM, (ns + OHU_TI - 1) / OHU_TI, (unsigned)nsplit);
   dim3 block(OHU_TM, OHU_TY);
   const int pf = qes_prof_begin(QES_PROF_OHU, st);
-  ohu_kernel<T><<<grid, block, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial);
+  ohu_kernel<T><<<grid, block, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial, cg_done);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
   if (int rc_ = launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
-      dot_part, dot_part ? L.scal : nullptr, L.counter, st)) return rc_;
+      dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
   QES_LAUNCH_CHECK();
   qes_prof_end(pfr, st);
   return QES_OK;
@@ -812,13 +816,13 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
 
 template <class T, class V>
 static int apply_ov(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const V* v, float2* w,
-                    double* wmean, cudaStream_t st) {
+                    double* wmean, cudaStream_t st, const double* cg_done = nullptr) {
   const int nw = n_words(ns);
   const size_t sm = (size_t)OV_SB * nw * sizeof(uint32_t);
   QES_ARG_CHECK(sm <= 48 * 1024, "SR: ns too large");
   const int pf = qes_prof_begin(QES_PROF_OV, st);
   ov_kernel<T, V><<<(unsigned)((n_samples + OV_SB - 1) / OV_SB), OV_THREADS, sm, st>>>(ns, nh, n_samples, bits, tt,
-                                                                                     v, w);
+                                                                                     v, w, cg_done);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, w, wmean);
@@ -907,24 +911,24 @@ extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const 
 template <class T>
 static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, double shift,
                        const typename VecT<T>::type* v, typename VecT<T>::type* y, double* dot_part, const SRWork& L,
-                       cudaStream_t st, bool vp_ready = false) {
+                       cudaStream_t st, bool vp_ready = false, const double* cg_done = nullptr) {
   using V = typename VecT<T>::type;
   if (L.tc) {
     const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
-    int rc = tc_matvec(dtype, L.td, n_samples, bits, v, L.w, L.partial, L.tw, st, !vp_ready);
+    int rc = tc_matvec(dtype, L.td, n_samples, bits, v, L.w, L.partial, L.tw, st, !vp_ready, cg_done);
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
     const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
     if (int rc_ = launch_reduce_splits<T, V>(P, L.nsplit, L.partial, shift, v, y,
-        dot_part, dot_part ? L.scal : nullptr, L.counter, st)) return rc_;
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
     QES_LAUNCH_CHECK();
     qes_prof_end(pfr, st);
     return QES_OK;
   }
-  int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, st);
+  int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, st, cg_done);
   if (rc) return rc;
   return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples, L, shift, v, y,
-                         dot_part, st);
+                         dot_part, st, cg_done);
 }
 
 // per-step operands of the tensor-core path (spins as BF16 tiles) and the status word
@@ -1133,15 +1137,16 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         // O v and O^H u (split partials), then the fused vector kernel
         if (L.tc) {
           const int dtype_ = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
-          int r2 = tc_matvec(dtype_, L.td, n_samples, bits, p, L.w, L.partial, L.tw, st, it0 + q == 0);
+          int r2 = tc_matvec(dtype_, L.td, n_samples, bits, p, L.w, L.partial, L.tw, st, it0 + q == 0,
+                             L.scal + 4);
           if (r2) return r2;
         } else {
-          int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, st);
+          int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, st, L.scal + 4);
           if (r2) return r2;
           dim3 grid((nh + OHU_TM - 1) / OHU_TM, (ns + OHU_TI - 1) / OHU_TI, (unsigned)L.nsplit);
           const int pf = qes_prof_begin(QES_PROF_OHU, st);
           ohu_kernel<T><<<grid, dim3(OHU_TM, OHU_TY), 0, st>>>(ns, nh, n_samples, bits, tt, L.w, L.wmean,
-                                                             1.0 / (double)n_samples, (T*)L.partial);
+                                                             1.0 / (double)n_samples, (T*)L.partial, L.scal + 4);
           QES_LAUNCH_CHECK();
           qes_prof_end(pf, st);
         }
@@ -1171,7 +1176,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         continue;
       }
       int r2 = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, p, Ap, L.parts, L, st,
-                              /*vp_ready=*/it0 + q > 0);
+                              /*vp_ready=*/it0 + q > 0, L.scal + 4);
       if (r2) return r2;
       // (alpha is computed by the last block of the matvec's split reduction)
       QES_CUDA_CHECK(qes_launch_pdl(cg_xr_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P, (const V*)p,
@@ -1473,7 +1478,7 @@ static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* 
       } else {
         const int nw = n_words(ns);
         ov_kernel<T, V><<<(unsigned)((n + OV_SB - 1) / OV_SB), OV_THREADS, (size_t)OV_SB * nw * sizeof(uint32_t), st>>>(
-            ns, nh, n, bits, tt, g, L.w);
+            ns, nh, n, bits, tt, g, L.w, nullptr);
         QES_LAUNCH_CHECK();
       }
       mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n, L.w, L.wmean);

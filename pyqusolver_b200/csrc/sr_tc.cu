@@ -257,7 +257,8 @@ template <class T, class V>
 __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_samples, const uint32_t* __restrict__ bits,
                                                          const V* __restrict__ v, const uint16_t* __restrict__ t_rows,
                                                          const uint16_t* __restrict__ vp, float2* __restrict__ w_out,
-                                                         double2* __restrict__ wsum_part, int* __restrict__ status) {
+                                                         double2* __restrict__ wsum_part, int* __restrict__ status,
+                                                         const double* __restrict__ cg_done) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   const int ns = d.ns, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
@@ -282,6 +283,10 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   const uint8_t* ga = reinterpret_cast<const uint8_t*>(t_rows) + (size_t)tile * nK * 2 * a_term;
   const uint8_t* gb = reinterpret_cast<const uint8_t*>(vp);
   pdl_trigger();
+  if (cg_block_done(cg_done)) {         // converged CG: nothing issued yet, nothing to drain
+    pdl_wait();
+    return;
+  }
   if (tid == 0) {
     for (int q = 0; q < S; ++q) {
       umma::mbar_init(&full[q], 1);
@@ -449,7 +454,7 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
                                                           const double2* __restrict__ wsum_part, int wsum_n,
                                                           double scale, const uint16_t* __restrict__ sig_cols,
                                                           const uint16_t* __restrict__ t_cols, T* __restrict__ partial,
-                                                          int* __restrict__ status) {
+                                                          int* __restrict__ status, const double* __restrict__ cg_done) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   const int ns = d.ns, nh = d.nh, Mp = d.Mp, Np = d.Np, KC = d.KC;
@@ -470,6 +475,11 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   const int chunk = blockIdx.x;
   const bool valid = chunk < d.n_chunks;                  // CL = 2 pads the grid to an even size
   pdl_trigger();
+  // converged CG: single CTAs leave at once (the pairs of CL = 2 must stay together, so they run)
+  if (CL == 1 && cg_block_done(cg_done)) {
+    pdl_wait();
+    return;
+  }
   const int64_t s0 = (int64_t)chunk * KC;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   __shared__ double2 s_red[kWarps];
@@ -823,12 +833,14 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_big_kernel(TcDims d, int64_t 
                                                               const double2* __restrict__ wsum_part, int wsum_n,
                                                               double scale, const uint16_t* __restrict__ sig_cols,
                                                               const uint16_t* __restrict__ t_cols,
-                                                              T* __restrict__ partial, int* __restrict__ status) {
+                                                              T* __restrict__ partial, int* __restrict__ status,
+                                                              const double* __restrict__ cg_done) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   constexpr int H = CPLX ? 2 : 1;
   pdl_trigger();
   pdl_wait();                                             // w and its partial sums: previous kernel
+  if (cg_block_done(cg_done)) return;                     // converged CG
   const int ns = d.ns, nh = d.nh, KC = d.KC, MT = d.MT, NC = d.NC, NR = d.NR, nnc = d.nnc;
   const int R = MT * 128;
   const uint32_t a_bytes = (uint32_t)R * KC * 2u, b_term = (uint32_t)NR * KC * 2u;
@@ -1206,7 +1218,8 @@ static int tc_set_attrs() {
 // grid padded to an even size) that add their partials on chip; chained to the previous kernel by PDL
 template <class T>
 static int launch_tc_ohu(const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
-                         double scale, const TcWork& w, T* partial, cudaStream_t st) {
+                         double scale, const TcWork& w, T* partial, cudaStream_t st,
+                         const double* cg_done = nullptr) {
   if (d.cl == 2) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)((d.n_chunks + 1) & ~1));
@@ -1223,11 +1236,12 @@ static int launch_tc_ohu(const TcDims& d, int64_t n_samples, const float2* g, co
     cfg.attrs = at;
     cfg.numAttrs = qes_pdl_on() ? 2 : 1;
     QES_CUDA_CHECK(cudaLaunchKernelEx(&cfg, tc_ohu_kernel<T, 2>, d, n_samples, g, gsum_part, gsum_n, scale,
-                                      (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status));
+                                      (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status,
+                                      cg_done));
   } else {
     QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_kernel<T, 1>, dim3(d.n_chunks), dim3(kThreads), (size_t)d.ohu_smem, st, d,
                                   n_samples, g, gsum_part, gsum_n, scale, (const uint16_t*)w.sig_cols,
-                                  (const uint16_t*)w.t_cols, partial, w.status));
+                                  (const uint16_t*)w.t_cols, partial, w.status, cg_done));
   }
   return QES_OK;
 }
@@ -1258,19 +1272,21 @@ int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_
 
 template <class T, class V>
 static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const V* v, float2* w_out,
-                       T* partial, const TcWork& w, cudaStream_t st, bool build_vp) {
+                       T* partial, const TcWork& w, cudaStream_t st, bool build_vp, const double* cg_done) {
   const bool cplx = ScalarTraits<T>::is_complex;
   // the CG iteration's kernels form a programmatic-dependent-launch chain (qes_launch_pdl)
   if (build_vp) {
+    // first iteration: an ordinary launch, so that everything before it (the setup that clears the
+    // converged flag of the previous solve) has completed before the PDL chain begins; the flag is
+    // read by tc_ov / tc_ohu before they wait on their predecessor
     const int items = d.NB * (d.Kd / 8);
-    QES_CUDA_CHECK(qes_launch_pdl(tc_build_vp_kernel<V>, dim3((items + 255) / 256), dim3(256), 0, st, d, cplx, v,
-                                  w.vp));
+    tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
     QES_LAUNCH_CHECK();
   }
   int pf = qes_prof_begin(QES_PROF_OV, st);
   QES_CUDA_CHECK(qes_launch_pdl(tc_ov_kernel<T, V>, dim3(d.n_tiles), dim3(kThreads), (size_t)d.ov_smem, st, d,
                                 n_samples, bits, v, (const uint16_t*)w.t_rows, (const uint16_t*)w.vp, w_out, w.wsum,
-                                w.status));
+                                w.status, cg_done));
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   pf = qes_prof_begin(QES_PROF_OHU, st);
@@ -1278,8 +1294,9 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
   if (d.big)
     QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_big_kernel<T>, dim3(d.nnc, d.nsplit), dim3(kThreads), (size_t)d.ohu_smem, st,
                                   d, n_samples, (const float2*)w_out, (const double2*)w.wsum, d.n_tiles, inv_n,
-                                  (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status));
-  else if (int rc = launch_tc_ohu<T>(d, n_samples, w_out, w.wsum, d.n_tiles, inv_n, w, partial, st))
+                                  (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status,
+                                  cg_done));
+  else if (int rc = launch_tc_ohu<T>(d, n_samples, w_out, w.wsum, d.n_tiles, inv_n, w, partial, st, cg_done))
     return rc;
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
@@ -1295,7 +1312,7 @@ static int tc_ov_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, con
   QES_LAUNCH_CHECK();
   const int pf = qes_prof_begin(QES_PROF_OV, st);
   tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
-                                                           w.status);
+                                                           w.status, nullptr);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;
@@ -1308,11 +1325,12 @@ int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, c
 }
 
 int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
-              void* partial, const TcWork& w, cudaStream_t st, bool build_vp) {
+              void* partial, const TcWork& w, cudaStream_t st, bool build_vp, const double* cg_done) {
   if (dtype == QES_DTYPE_C64)
     return tc_matvec_t<float2, double2>(d, n_samples, bits, (const double2*)v, w_out, (float2*)partial, w, st,
-                                        build_vp);
-  return tc_matvec_t<float, double>(d, n_samples, bits, (const double*)v, w_out, (float*)partial, w, st, build_vp);
+                                        build_vp, cg_done);
+  return tc_matvec_t<float, double>(d, n_samples, bits, (const double*)v, w_out, (float*)partial, w, st, build_vp,
+                                    cg_done);
 }
 
 int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
@@ -1320,10 +1338,10 @@ int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const
   if (d.big) {
     if (dtype == QES_DTYPE_C64)
       tc_ohu_big_kernel<float2><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
-          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float2*)partial, w.status);
+          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float2*)partial, w.status, nullptr);
     else
       tc_ohu_big_kernel<float><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
-          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float*)partial, w.status);
+          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float*)partial, w.status, nullptr);
   } else if (dtype == QES_DTYPE_C64) {
     if (int rc = launch_tc_ohu<float2>(d, n_samples, g, gsum_part, gsum_n, scale, w, (float2*)partial, st)) return rc;
   } else {

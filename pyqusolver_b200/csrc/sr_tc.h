@@ -46,9 +46,11 @@ TcWork tc_layout(const TcDims& d, char* base);
 // once per VMC step: BF16 tiles of T, T^T and Sigma^T
 int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
                     const TcWork& w, cudaStream_t st);
-// w_out = O v, partial[chunk] = O^H ((w - mean w) / Ns)
+// w_out = O v, partial[chunk] = O^H ((w - mean w) / Ns); cg_done (optional): a CG solve's converged
+// flag, on which the kernels skip their work
 int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
-              void* partial, const TcWork& w, cudaStream_t st, bool build_vp = true);
+              void* partial, const TcWork& w, cudaStream_t st, bool build_vp = true,
+              const double* cg_done = nullptr);
 // w_out = O v only (builds the V' operand from v first)
 int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
           const TcWork& w, cudaStream_t st);

@@ -510,6 +510,36 @@ def test_cg_programmatic_launch_is_bit_identical(sr_impl, cplx):
     assert np.array_equal(out[0][0], out[1][0])
 
 
+@pytest.mark.parametrize("impl", [_lib.SR_IMPL_TENSOR_CORES, _lib.SR_IMPL_CUDA_CORES])
+@pytest.mark.parametrize("fused", [0, 1])
+def test_cg_iterations_after_convergence_change_nothing(sr_impl, impl, fused):
+    """The host checks convergence every `check_every` iterations; the iterations launched after the
+    converging one skip their work on the device (matvec, reduction and updates read the converged
+    flag).  Solutions, iteration counts and residuals are bit-identical for check_every = 1 and 64,
+    with the cooperative vector kernel and with the separate kernels."""
+    ns, nh, n = 20, 40, 2500
+    net = RBM((ns,), n_hidden=nh, dtype="complex64", seed=91, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=92))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    sr_impl(impl)
+    out = []
+    try:
+        _lib.call("qes_set_cg_fused", 2 if fused else 0)
+        for ce in (1, 64):
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-9, maxiter=2000,
+                                     check_every=ce)
+            out.append((x.cpu().numpy(), info["iterations"], info["residual"], info["converged"]))
+    finally:
+        _lib.call("qes_set_cg_fused", 1)
+    assert out[0][3] and out[1][3]
+    assert out[0][1] == out[1][1] and out[0][1] % 64 != 0
+    assert out[0][2] == out[1][2]
+    assert np.array_equal(out[0][0], out[1][0])
+
+
 @pytest.mark.parametrize("cplx", [False, True])
 def test_ohu_cta_pairs_match_single_ctas(sr_impl, cplx):
     """O^H u as clusters of two CTAs that add their partials on chip (an odd chunk count, so one

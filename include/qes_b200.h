@@ -147,6 +147,14 @@ int qes_sampler_run_betas(int dtype, const qes_sampler_config* cfg, const float*
  * order); results are the same either way.                                  */
 int qes_set_pdl(int on);
 
+/* Device-driven CG loop (process-wide, default on): after the first chunk of
+ * check_every iterations, the remaining full chunks run in one launch of a
+ * CUDA graph whose conditional WHILE node repeats the chunk until the
+ * converged flag is set (or the iteration limit), instead of one host
+ * round trip per chunk.  Where the driver rejects such a graph the chunks
+ * stay host-driven.  0 turns it off; results are the same either way.      */
+int qes_set_cg_device_loop(int enable);
+
 /* Which sampler kernel runs a chain set whose theta caches live in registers
  * (process-wide): 0 = the uncapped kernel (up to 128 registers, 16 chains per
  * SM); 1 = the kernel capped at 72 registers (28 chains per SM) when that

@@ -995,6 +995,12 @@ struct CgGraphSlot {
   cudaGraphExec_t exec = nullptr;
   CgGraphKey key{};
   long long nodes = 0;
+  // device loop: a counter reset, then a WHILE node whose body is one chunk + the loop condition
+  cudaGraphExec_t lexec = nullptr;
+  CgGraphKey lkey{};
+  unsigned lmax = 0;
+  long long lnodes = 0;            // launches of one body (the chunk and the condition kernel)
+  bool lfailed = false;            // this key could not be built as a device loop: host-driven chunks
 };
 constexpr int kMaxGraphDevices = 64;
 std::mutex g_graph_mu;
@@ -1002,6 +1008,7 @@ CgGraphSlot g_graph[kMaxGraphDevices];
 std::atomic<int> g_use_graphs{1};
 std::atomic<int> g_l2_persist{0};
 std::atomic<int> g_cg_fused{1};            // automatic
+std::atomic<int> g_cg_loop{1};             // device-side loop over the CG chunks
 
 // L2 persistence of the tensor-core operands across the CG iterations: an access-policy window
 // over the BF16 tiles (T rows, T^T, Sigma^T, V') on the launching stream, sized to the device's
@@ -1036,6 +1043,24 @@ void l2_window(cudaStream_t st, int dev, const void* base, size_t bytes) {
   cudaGetLastError();           // an unsupported policy leaves the solve unaffected
 }
 }  // namespace
+
+// The loop condition of the device-driven CG: one more chunk while the solve has not converged,
+// no bounded wait has given up, and fewer than max_chunks chunks have run.  The counter makes the
+// loop finite whatever the other kernels do.
+__global__ void cg_loop_reset_kernel(unsigned int* count) { *count = 0u; }
+__global__ void cg_loop_cond_kernel(cudaGraphConditionalHandle h, const double* __restrict__ scal,
+                                    unsigned int* __restrict__ count, unsigned int max_chunks,
+                                    const int* __restrict__ status) {
+  const unsigned int c = *count + 1u;
+  *count = c;
+  const bool more = scal[4] == 0.0 && c < max_chunks && (status == nullptr || *status == 0);
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+extern "C" int qes_set_cg_device_loop(int enable) {
+  g_cg_loop.store(enable ? 1 : 0);
+  return QES_OK;
+}
 
 extern "C" int qes_set_cg_fused(int mode) {
   if (mode < 0 || mode > 2) {
@@ -1235,6 +1260,104 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         gs.nodes = qes_launch_count(0) - before;
         qes_count_launches((int)-gs.nodes);     // captured, not run
         gs.key = key;
+      }
+      // Device loop: the remaining full chunks in one launch of a graph whose WHILE node repeats
+      // the chunk until the converged flag is set (no host round trip per chunk).  Built once per
+      // key; where the driver rejects it, the chunks stay host-driven.
+      const unsigned lmax = (unsigned)((opt->maxiter - it) / check);
+      unsigned int* lcount = L.counter + 96;  // own 128-byte line
+      if (g_cg_loop.load() != 0 && lmax >= 2 &&
+          !(gs.lfailed && gs.lkey == key && gs.lmax == lmax)) {
+        if (gs.lexec == nullptr || !(gs.lkey == key) || gs.lmax != lmax) {
+          if (gs.lexec) {
+            cudaGraphExecDestroy(gs.lexec);
+            gs.lexec = nullptr;
+          }
+          gs.lkey = key;
+          gs.lmax = lmax;
+          gs.lfailed = true;                  // until the build below succeeds
+          cudaGraph_t g = nullptr;
+          bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+          cudaGraphNode_t n0 = nullptr, n1 = nullptr;
+          cudaGraphConditionalHandle hnd = 0;
+          if (ok) {
+            void* kargs[] = {(void*)&lcount};
+            cudaKernelNodeParams kp = {};
+            kp.func = (void*)cg_loop_reset_kernel;
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(1);
+            kp.kernelParams = kargs;
+            ok = cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp) == cudaSuccess &&
+                 cudaGraphConditionalHandleCreate(&hnd, g, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+          }
+          cudaGraph_t body = nullptr;
+          if (ok) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = hnd;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            ok = cudaGraphAddNode(&n1, g, &n0, 1, &cp) == cudaSuccess;
+            if (ok) body = cp.conditional.phGraph_out[0];
+          }
+          long long bnodes = 0;
+          if (ok) {
+            const long long before = qes_launch_count(0);
+            ok = cudaStreamBeginCaptureToGraph(gs.cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                 cudaSuccess;
+            if (ok) {
+              cudaStream_t saved = st;
+              st = gs.cs;
+              int rcap = run_direct(check, 1);
+              if (!rcap) {
+                cg_loop_cond_kernel<<<1, 1, 0, gs.cs>>>(hnd, L.scal, lcount, lmax, L.tc ? L.tw.status : nullptr);
+                if (cudaPeekAtLastError() != cudaSuccess) rcap = QES_ERR_CUDA;
+                else qes_count_launches(1);
+              }
+              st = saved;
+              cudaGraph_t bout = nullptr;
+              const cudaError_t ec = cudaStreamEndCapture(gs.cs, &bout);
+              ok = rcap == QES_OK && ec == cudaSuccess;
+            }
+            bnodes = qes_launch_count(0) - before;
+            qes_count_launches((int)-bnodes);   // captured, not run
+          }
+          if (ok) ok = cudaGraphInstantiate(&gs.lexec, g, 0) == cudaSuccess;
+          if (!ok) gs.lexec = nullptr;
+          if (g) cudaGraphDestroy(g);
+          cudaGetLastError();                   // a rejected build leaves no error behind
+          if (ok) {
+            gs.lfailed = false;
+            gs.lnodes = bnodes;
+          }
+        }
+        if (gs.lexec) {
+          QES_CUDA_CHECK(cudaEventRecord(gs.ev_in, st));
+          QES_CUDA_CHECK(cudaStreamWaitEvent(gs.cs, gs.ev_in, 0));
+          if (cudaGraphLaunch(gs.lexec, gs.cs) != cudaSuccess) {
+            cudaGetLastError();                 // rejected at launch: host-driven chunks from now on
+            cudaGraphExecDestroy(gs.lexec);
+            gs.lexec = nullptr;
+            gs.lfailed = true;
+          }
+        }
+        if (gs.lexec) {
+          QES_CUDA_CHECK(cudaEventRecord(gs.ev_out, gs.cs));
+          QES_CUDA_CHECK(cudaStreamWaitEvent(st, gs.ev_out, 0));
+          unsigned int chunks = 0;
+          QES_CUDA_CHECK(cudaMemcpyAsync(&chunks, lcount, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+          QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+          rc = sr_check_status(L, st);        // synchronises the stream
+          if (rc) return rc;
+          if (chunks < 1 || chunks > lmax) {
+            qes_set_last_message("SR CG: the device loop ran an impossible number of chunks");
+            return QES_ERR_CUDA;
+          }
+          qes_count_launches((int)(1 + (long long)chunks * gs.lnodes));
+          it += (int)chunks * check;
+          done = hs[4] != 0.0;
+          continue;
+        }
       }
       QES_CUDA_CHECK(cudaEventRecord(gs.ev_in, st));
       QES_CUDA_CHECK(cudaStreamWaitEvent(gs.cs, gs.ev_in, 0));

@@ -540,6 +540,60 @@ def test_cg_iterations_after_convergence_change_nothing(sr_impl, impl, fused):
     assert np.array_equal(out[0][0], out[1][0])
 
 
+@pytest.mark.parametrize("impl", [_lib.SR_IMPL_TENSOR_CORES, _lib.SR_IMPL_CUDA_CORES])
+@pytest.mark.parametrize("fused", [0, 2])
+def test_cg_device_loop_matches_host_loop(sr_impl, impl, fused):
+    """The CG chunks repeated on the device by a graph's WHILE node, against one host round trip
+    per chunk: the same kernels in the same order, so the solution, iteration count and residual
+    are bit-identical; a second solve reuses the loop graph."""
+    ns, nh, n = 24, 48, 3000
+    net = RBM((ns,), n_hidden=nh, dtype="complex64", seed=71, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=72))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    sr_impl(impl)
+    out = []
+    try:
+        _lib.call("qes_set_cg_fused", fused)
+        for loop in (0, 1, 1):
+            _lib.call("qes_set_cg_device_loop", loop)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-9, maxiter=2000,
+                                     check_every=8)
+            out.append((x.cpu().numpy(), info["iterations"], info["residual"], info["converged"]))
+    finally:
+        _lib.call("qes_set_cg_fused", 1)
+        _lib.call("qes_set_cg_device_loop", 1)
+    assert all(o[3] for o in out) and out[0][1] > 16
+    for o in out[1:]:
+        assert o[1] == out[0][1] and o[2] == out[0][2]
+        assert np.array_equal(o[0], out[0][0])
+
+
+def test_cg_device_loop_respects_maxiter(sr_impl):
+    """A solve that cannot converge within maxiter stops at maxiter with the device loop too."""
+    ns, nh, n = 24, 48, 3000
+    net = RBM((ns,), n_hidden=nh, dtype="float32", seed=73, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=74))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    sr_impl(_lib.SR_IMPL_TENSOR_CORES)
+    res = []
+    try:
+        for loop in (0, 1):
+            _lib.call("qes_set_cg_device_loop", loop)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-6, rtol=1e-14, maxiter=37,
+                                     check_every=4)
+            res.append((x.cpu().numpy(), info["iterations"], info["converged"]))
+    finally:
+        _lib.call("qes_set_cg_device_loop", 1)
+    assert res[0][1] == res[1][1] == 37 and not res[0][2] and not res[1][2]
+    assert np.array_equal(res[0][0], res[1][0])
+
+
 @pytest.mark.parametrize("cplx", [False, True])
 def test_ohu_cta_pairs_match_single_ctas(sr_impl, cplx):
     """O^H u as clusters of two CTAs that add their partials on chip (an odd chunk count, so one

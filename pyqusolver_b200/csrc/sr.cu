@@ -1223,6 +1223,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   }
   while (!done && it < opt->maxiter) {
     const int nrun = std::min(check, opt->maxiter - it);
+    // set when the device loop was launched: its chunk count is read back after the lock is released
+    unsigned int* loop_count = nullptr;
+    unsigned loop_max = 0;
+    long long loop_nodes = 0;
     if (!graphs || it == 0 || nrun != check) {
       rc = run_direct(nrun, it);
       if (rc) return rc;
@@ -1344,27 +1348,34 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         if (gs.lexec) {
           QES_CUDA_CHECK(cudaEventRecord(gs.ev_out, gs.cs));
           QES_CUDA_CHECK(cudaStreamWaitEvent(st, gs.ev_out, 0));
-          unsigned int chunks = 0;
-          QES_CUDA_CHECK(cudaMemcpyAsync(&chunks, lcount, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
-          QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
-          rc = sr_check_status(L, st);        // synchronises the stream
-          if (rc) return rc;
-          if (chunks < 1 || chunks > lmax) {
-            qes_set_last_message("SR CG: the device loop ran an impossible number of chunks");
-            return QES_ERR_CUDA;
-          }
-          qes_count_launches((int)(1 + (long long)chunks * gs.lnodes));
-          it += (int)chunks * check;
-          done = hs[4] != 0.0;
-          continue;
+          loop_count = lcount;
+          loop_max = lmax;
+          loop_nodes = gs.lnodes;
         }
       }
-      QES_CUDA_CHECK(cudaEventRecord(gs.ev_in, st));
-      QES_CUDA_CHECK(cudaStreamWaitEvent(gs.cs, gs.ev_in, 0));
-      QES_CUDA_CHECK(cudaGraphLaunch(gs.exec, gs.cs));
-      QES_CUDA_CHECK(cudaEventRecord(gs.ev_out, gs.cs));
-      QES_CUDA_CHECK(cudaStreamWaitEvent(st, gs.ev_out, 0));
-      qes_count_launches((int)gs.nodes);
+      if (!loop_count) {
+        QES_CUDA_CHECK(cudaEventRecord(gs.ev_in, st));
+        QES_CUDA_CHECK(cudaStreamWaitEvent(gs.cs, gs.ev_in, 0));
+        QES_CUDA_CHECK(cudaGraphLaunch(gs.exec, gs.cs));
+        QES_CUDA_CHECK(cudaEventRecord(gs.ev_out, gs.cs));
+        QES_CUDA_CHECK(cudaStreamWaitEvent(st, gs.ev_out, 0));
+        qes_count_launches((int)gs.nodes);
+      }
+    }
+    if (loop_count) {
+      unsigned int chunks = 0;
+      QES_CUDA_CHECK(cudaMemcpyAsync(&chunks, loop_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+      QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      rc = sr_check_status(L, st);            // synchronises the stream
+      if (rc) return rc;
+      if (chunks < 1 || chunks > loop_max) {
+        qes_set_last_message("SR CG: the device loop ran an impossible number of chunks");
+        return QES_ERR_CUDA;
+      }
+      qes_count_launches((int)(1 + (long long)chunks * loop_nodes));
+      it += (int)chunks * check;
+      done = hs[4] != 0.0;
+      continue;
     }
     it += nrun;
     QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -123,7 +123,7 @@ def build_nqs(cfg, seed):
                  s_numsamples=cfg["samples"], s_therm_steps=1, s_sweep_steps=cfg["sweep"], s_seed=seed,
                  init_scale=0.01)
     from pyqusolver_b200.tdvp import TDVP
-    tdvp = TDVP(sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
+    tdvp = TDVP(rhs_prefactor=-1.0, sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
     return nqs, tdvp
 
 
@@ -328,10 +328,10 @@ def run_batch(args, cfg, rank, world, local_rank):
     hbm = peaks.get("hbm_gbs", 6650.0)
     rows, ns, nh, P = B.rows, B.ns, B.nh, B.P
     nw = (ns + 31) // 32
-    nsplit = (rows + 255) // 256
+    # algorithmic bytes (operands once, outputs once; no split partials), as kernel_bytes()
     algo = {"ov": int((rows * nh * 4 + rows * nw * 4 + P * 8 + rows * 8).sum()),
-            "ohu": int((rows * nh * 4 + rows * nw * 4 + rows * 8 + nsplit * P * 4).sum()),
-            "reduce": int((nsplit * P * 4 + 5 * P * 8).sum())}
+            "ohu": int((rows * nh * 4 + rows * nw * 4 + rows * 8 + P * 8).sum()),
+            "reduce": int((5 * P * 8).sum())}
     names = {"ov": "batch_ov_tile_kernel", "ohu": "batch_ohu_tile_kernel", "reduce": "batch_cg_update_kernel"}
     cands = {k: v for k, v in prof.items() if v[1]}
     dom = max(cands, key=lambda k: cands[k][0])
@@ -432,7 +432,10 @@ def run_ours(args, cfg, rank, world, local_rank):
         if form == "mixed":
             # per-kernel CUDA-event timing (roofline) in separate steps: the event pairs and the graph-less CG
             # they need would otherwise slow the timed steps
+            ce = tdvp.check_every
+            tdvp.check_every = 1          # no launch after convergence: every bracketed launch did work
             _, prof_phases, prof_iters, _, prof = timed_loop(nqs, tdvp, cfg, min(args.steps, 5), flush, profile=True)
+            tdvp.check_every = ce
         forms[form] = {"nqs": nqs, "tdvp": tdvp, "total_ms": total_ms, "phase_ms": phase_ms, "cg_iters": cg_iters,
                        "launches": launches, "prof": prof, "prof_phase_ms": prof_phases, "prof_cg_iters": prof_iters,
                        "clocks": clk, "energy": float(nqs_energy(tdvp.last_info))}
@@ -478,6 +481,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         "clocks": mixed["clocks"],
         "e2e": e2e,
         "roofline": roof,
+        "issue_rooflines": issue_rooflines(cfg, nqs, mixed, mixed["clocks"]),
     }
     if rank == 0 and args.accuracy_epochs > 0:
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
@@ -507,7 +511,7 @@ def run_e2e(cfg, args, dist, world, seed):
     host_in.copy_(net.master.cpu())
     host_out = torch.empty_like(host_in).pin_memory()
     from pyqusolver_b200.tdvp import TDVP
-    tdvp = TDVP(sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
+    tdvp = TDVP(rhs_prefactor=-1.0, sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
     times = []
     for k in range(args.warmup + args.steps):                 # warm-up steps untimed, as in the timed loop
         s = torch.cuda.Event(enable_timing=True)
@@ -535,35 +539,62 @@ def run_e2e(cfg, args, dist, world, seed):
 
 
 def kernel_bytes(cfg, nqs, kind, tc):
-    """Algorithmic bytes of one launch: every operand read once plus every output written once.
-    Tensor-core operands are counted in the BF16 tile form the kernels stream (plan from the library)."""
-    from pyqusolver_b200 import _lib, device as dv
+    """Algorithmic bytes of one launch: the operands the contraction needs, read once, and its
+    outputs, written once, at their unpadded sizes.  T (Ns x M) counts once at its float32 size
+    (the BF16 hi + lo pair of the tensor-core form is the same number of bytes), the spins as packed
+    words, u or w as one complex64 per sample, v or the output as one float64 / complex128 per
+    parameter.  Split-K partial P-vectors, padded or expanded operand tiles and re-reads are not
+    algorithmic: they are the kernels' own traffic (``traffic`` reports what DRAM saw)."""
     net = nqs.net
     ns, nh, n = net.ns, net.nh, cfg["chains"] * cfg["samples"]
-    cplx = net.is_complex
-    ts, vs = (8, 16) if cplx else (4, 8)
+    ts, vs = (8, 16) if net.is_complex else (4, 8)
     nw = (ns + 31) // 32
     P = ns + nh + ns * nh
-    if tc:
-        pl = _lib.sr_tc_plan(dv.dtype_code(net.flat), ns, nh, n)
-        kc, nch, nsp = pl["KC"], pl["n_chunks"], pl["nsplit"]
-        if kind == "ov":
-            return pl["n_tiles"] * 128 * pl["Kd"] * 4 + pl["NB"] * pl["Kd"] * 4 + n * nw * 4 + n * 8
-        if kind == "ohu":
-            if pl["big"]:
-                return nch * (pl["MT"] * 128 * kc * 2 + pl["nnc"] * pl["NR"] * kc * 4) + n * 8 + nsp * P * ts
-            return nch * 128 * kc * 2 + nch * pl["Np"] * kc * 4 + n * 8 + nsp * P * ts
-        return nsp * P * ts + 2 * P * vs
-    nsplit = (n + 255) // 256
-    if kind == "ov":
-        return n * nh * ts + n * nw * 4 + P * vs + n * 8
-    if kind == "ohu":
-        return n * nh * ts + n * nw * 4 + n * 8 + nsplit * P * ts
-    return nsplit * P * ts + 2 * P * vs
+    t_bytes, spins = n * nh * ts, n * nw * 4
+    if kind == "ov":          # w = O v: T, spins and v in, w out
+        return t_bytes + spins + P * vs + n * 8
+    if kind == "ohu":         # O^H u: T, spins and u in, one P-vector out
+        return t_bytes + spins + n * 8 + P * vs
+    return 3 * P * vs         # split reduction: the P-vector out, p in, Ap out
+
+
+def fp32_peak_tflops(clk):
+    """Nominal FP32 FMA issue rate of the B200 (148 SMs x 128 lanes x 2 flops) at the median SM clock
+    sampled during the timed steps (max clock when no sample)."""
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def issue_rooflines(cfg, nqs, form, clk):
+    """Sampler and local energy, bound by FP32 issue (their working sets live in shared memory and L2):
+    achieved = algorithmic flops / phase time, against the nominal FP32 rate at the sampled clock.
+    Work units (restated from the kernels' arithmetic): one ratio factor per hidden unit and
+    proposal in the sampler (complex: (C + g t S) products, 14 flops; real: 3 flops), plus the
+    accepted-move cache update it amortises; one (move, hidden unit) term per sample in the local
+    energy (complex: one complex FMA and one complex multiply, 14 flops; real: 3 flops)."""
+    net = nqs.net
+    n = cfg["chains"] * cfg["samples"]
+    f_unit = 14 if net.is_complex else 3
+    proposals = cfg["chains"] * cfg["samples"] * cfg["sweep"]
+    n_moves = nqs._dev_ham.n_moves
+    peak = fp32_peak_tflops(clk)
+    out = {}
+    for phase, units, what in (("sample", proposals * net.nh, "proposal x hidden-unit ratio factors"),
+                               ("local_energy", n * n_moves * net.nh, "sample x move x hidden-unit terms")):
+        ms = float(np.mean(form["phase_ms"][phase]))
+        tf = units * f_unit / (ms / 1e3) / 1e12
+        out[phase] = {"kernel": "sampler_kernel" if phase == "sample" else "eloc_moves_kernel",
+                      "bound": "fp32_issue", "work_units_per_launch": int(units), "unit_definition": what,
+                      "flops_per_unit": f_unit, "avg_launch_us": ms * 1e3, "achieved": tf, "peak": peak,
+                      "unit": "TFLOP/s", "frac": tf / peak,
+                      "peak_source": "nominal FP32 FMA rate at the sampled SM clock (not a measured peak)"}
+    return out
 
 
 def roofline(cfg, nqs, form):
-    """Roofline of the kernel with the largest share of the timed steps (live CUDA-event times)."""
+    """Roofline of the kernel with the largest share of the profiled steps (live CUDA-event times on the
+    launching stream; the profiled CG checks convergence after every iteration, so every bracketed
+    launch did work)."""
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -592,7 +623,8 @@ def roofline(cfg, nqs, form):
     tc = _lib.sr_uses_tensor_cores(dv.dtype_code(net.flat), net.ns, net.nh, cfg["chains"] * cfg["samples"])
     names = {"ov": "tc_ov_kernel (O v, tcgen05)" if tc else "ov_kernel (O v, CUDA cores)",
              "ohu": "tc_ohu_kernel (O^H u, tcgen05)" if tc else "ohu_kernel (O^H u, CUDA cores)",
-             "reduce": "reduce_splits_kernel", "sample": "sampler_kernel", "local_energy": "eloc_moves_kernel",
+             "reduce": "reduce_splits_kernel / cg_fused_kernel", "sample": "sampler_kernel",
+             "local_energy": "eloc_moves_kernel",
              "forward": "theta_tc_kernel (tcgen05)" if dv.forward_uses_tensor_cores(
                  net.flat, net.ns, net.nh, cfg["chains"] * cfg["samples"]) else "rbm_forward_kernel"}
     out = {"kernel": names.get(dom, dom), "launches_timed": cnt, "avg_launch_us": avg_s * 1e6,
@@ -600,15 +632,13 @@ def roofline(cfg, nqs, form):
            "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src}
     if dom in ("ov", "ohu", "reduce"):
         b = kernel_bytes(cfg, nqs, dom, tc=tc)
-        ach = b / avg_s / 1e9
         tr = traffic_db.get(cfg.get("name", ""), {}).get(dom)
-        out.update({"achieved": ach, "frac": ach / hbm, "algorithmic_bytes_per_launch": b, "traffic": tr})
     else:
-        net = nqs.net
         n = cfg["chains"] * cfg["samples"]
         b = n * net.nh * (8 if net.is_complex else 4) + n * ((net.ns + 31) // 32) * 4
-        ach = b / avg_s / 1e9
-        out.update({"achieved": ach, "frac": ach / hbm, "algorithmic_bytes_per_launch": b, "traffic": None})
+        tr = None
+    ach = b / avg_s / 1e9
+    out.update({"achieved": ach, "frac": ach / hbm, "algorithmic_bytes_per_launch": int(b), "traffic": tr})
     return out
 
 

@@ -327,6 +327,12 @@ int qes_set_cg_graphs(int enable);
  * parameter vectors up to a few thousand entries, where launch latency
  * dominates), 0 = never (three kernels).                                   */
 int qes_set_cg_fused(int mode);
+/* Test hook of the fused CG kernel's grid barriers (no reference
+ * counterpart): (1, polls) makes every barrier wait for one arrival that
+ * never comes and give up after `polls` polls, so a solve returns
+ * QES_ERR_TIMEOUT at its next status check; (0, 0) restores the normal
+ * barriers.  Process-wide; meant for tests of the time-out path only.      */
+int qes_sr_set_barrier_test(unsigned int extra_arrivals, unsigned int poll_limit);
 
 /* RBM forward on the tensor cores: theta = Sigma W + b with W split into
  * three BF16 terms (exact for float32 W) and float32 accumulation; outputs

@@ -91,6 +91,9 @@ class MetropolisSampler:
         self.step = 0
         self.proposed = np.zeros(n_chains, dtype=np.int64)
         self.accepted = np.zeros(n_chains, dtype=np.int64)
+        # smallest |log u - log_acc| met by each chain's decisions: a float32 implementation can take
+        # the other branch only where this margin is within its rounding of Delta log psi
+        self.min_margin = np.full(n_chains, np.inf)
         self.needs_therm = True
 
     def _propose(self, r0, r1):
@@ -123,7 +126,9 @@ class MetropolisSampler:
                 lp_new[moved] = rbm_mod.log_psi(params, new[moved])
             delta = np.real(lp_new - lp)
             log_acc = np.minimum(self.beta * self.mu * delta, 0.0)
-            keep = np.log(philox.uniform_open(r2)) < log_acc
+            logu = np.log(philox.uniform_open(r2))
+            keep = logu < log_acc
+            self.min_margin = np.minimum(self.min_margin, np.abs(logu - log_acc))
             self.states = np.where(keep[:, None], new, self.states)
             lp = np.where(keep, lp_new, lp)
             self.proposed += 1
@@ -176,6 +181,7 @@ class ParallelTemperingSampler:
         self.betas = np.repeat(self.pt_betas[:, None], self.C, axis=1)
         self.round = 0
         self.swaps = np.zeros(max(self.R - 1, 1), dtype=np.int64)
+        self.swap_margin = np.full(self.C, np.inf)     # as MetropolisSampler.min_margin, for the swaps
 
     def _round(self, params):
         b = self.base
@@ -192,11 +198,17 @@ class ParallelTemperingSampler:
             log_acc = (bi - bj) * b.mu * (np.real(lp[r + 1]) - np.real(lp[r]))
             u = philox.uniform_open(philox.philox4x32_10(cols, self.round, r, philox.STREAM_PT_SWAP, k0, k1)[0])
             acc = np.log(u) < np.minimum(log_acc, 0.0)
+            self.swap_margin = np.minimum(self.swap_margin, np.abs(np.log(u) - np.minimum(log_acc, 0.0)))
             self.betas[r] = np.where(acc, bj, bi)
             self.betas[r + 1] = np.where(acc, bi, bj)
             self.swaps[r] += int(acc.sum())
         self.round += 1
         return lp
+
+    @property
+    def min_margin(self):
+        """Per chain column: the smallest decision margin of its R slots' Metropolis steps and swaps."""
+        return np.minimum(self.base.min_margin.reshape(self.R, self.C).min(axis=0), self.swap_margin)
 
     def sample(self, params, num_samples):
         b = self.base

@@ -111,3 +111,66 @@ def solve_sr(e_loc, O, *, shift=1e-3, probs=None, method="dense", rtol=1e-8,
         if nrm > grad_clip:
             x = x * (grad_clip / (nrm + 1e-12))
     return x, info
+
+
+# --------------------------------------------------------------------------------------
+# Large shapes: O built chunk by chunk from the RBM (never whole), same normalisation
+# --------------------------------------------------------------------------------------
+
+def _o_chunks(params, sigma, chunk):
+    from . import rbm as rbm_mod
+    for r0 in range(0, sigma.shape[0], chunk):
+        yield r0, rbm_mod.log_derivatives(params, sigma[r0:r0 + chunk])
+
+
+def matvec_chunked(params, sigma, v, shift=0.0, chunk=64, probs=None):
+    """(S + shift) v with S = O_c^H diag(w) O_c / Ns, O rebuilt per sample chunk (two passes)."""
+    sigma = np.asarray(sigma, dtype=np.float64)
+    ns = sigma.shape[0]
+    w = np.ones(ns) if probs is None else np.asarray(probs, dtype=np.float64)
+    Ov = np.concatenate([O @ v for _, O in _o_chunks(params, sigma, chunk)])
+    u = w * (Ov - np.sum(w * Ov) / ns) / ns
+    y = shift * np.asarray(v, dtype=np.result_type(v, Ov))
+    for r0, O in _o_chunks(params, sigma, chunk):
+        y = y + np.conj(O).T @ u[r0:r0 + O.shape[0]]
+    return y
+
+
+def solve_sr_chunked(params, sigma, e_loc, shift, rhs_prefactor=-1.0, chunk=64):
+    """Parameter-space SR solution through the sample-space identity
+    (O_c^H O_c / Ns + shift)^-1 O_c^H E_c / Ns = O_c^H (O_c O_c^H / Ns + shift)^-1 E_c / Ns,
+    with the Ns x Ns Gram matrix accumulated from O chunks; returns (x * rhs_prefactor, F)."""
+    sigma = np.asarray(sigma, dtype=np.float64)
+    ns = sigma.shape[0]
+    e = np.asarray(e_loc)
+    ec = e - e.mean()
+    chunks = list(range(0, ns, chunk))
+    om = None
+    for _, O in _o_chunks(params, sigma, chunk):
+        om = O.sum(axis=0) if om is None else om + O.sum(axis=0)
+    om = om / ns
+    G = np.zeros((ns, ns), dtype=np.complex128 if np.iscomplexobj(om) else np.float64)
+    F = np.zeros_like(om)
+    for a in chunks:
+        Oa = _o_chunks_one(params, sigma, a, chunk) - om[None, :]
+        F = F + np.conj(Oa).T @ ec[a:a + Oa.shape[0]]
+        for b in chunks:
+            if b < a:
+                continue
+            Ob = Oa if b == a else _o_chunks_one(params, sigma, b, chunk) - om[None, :]
+            blk = Oa @ np.conj(Ob).T
+            G[a:a + Oa.shape[0], b:b + Ob.shape[0]] = blk
+            if b != a:
+                G[b:b + Ob.shape[0], a:a + Oa.shape[0]] = np.conj(blk).T
+    F = F / ns
+    y = np.linalg.solve(G / ns + shift * np.eye(ns), ec / ns)
+    x = np.zeros_like(om)
+    for a in chunks:
+        Oa = _o_chunks_one(params, sigma, a, chunk) - om[None, :]
+        x = x + np.conj(Oa).T @ y[a:a + Oa.shape[0]]
+    return rhs_prefactor * x, F
+
+
+def _o_chunks_one(params, sigma, r0, chunk):
+    from . import rbm as rbm_mod
+    return rbm_mod.log_derivatives(params, sigma[r0:r0 + chunk])

@@ -42,17 +42,50 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in SOURCES + HEADERS)
 
 
+OBJ_DIR = os.path.join(HERE, "_build")
+
+
+def _obj(src: str) -> str:
+    return os.path.join(OBJ_DIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel (objects older than their source or any header
+    are rebuilt), then link the shared library."""
     if not force and not needs_build():
         return LIB_PATH
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    newest_header = max(os.path.getmtime(h) for h in HEADERS + glob.glob(os.path.join(HERE, "csrc", "*.h")))
+    todo = [s for s in SOURCES if force or not os.path.exists(_obj(s)) or
+            os.path.getmtime(_obj(s)) < max(os.path.getmtime(s), newest_header)]
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"] + ["-c"]
+
+    def compile_one(src):
+        cmd = [_nvcc()] + compile_flags + ["-o", _obj(src) + ".tmp", src]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode == 0:
+            os.replace(_obj(src) + ".tmp", _obj(src))
+        return src, res
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, todo))
+    failed = [(s, r) for s, r in results if r.returncode != 0]
+    for s, r in failed:
+        sys.stderr.write(r.stdout + r.stderr)
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(os.path.basename(s) for s, _ in failed))
     tmp = LIB_PATH + ".tmp"
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + SOURCES
+    cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC", "-o", tmp] + \
+        [_obj(s) for s in SOURCES]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building " + LIB_NAME)
+        raise RuntimeError("nvcc failed linking " + LIB_NAME)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 

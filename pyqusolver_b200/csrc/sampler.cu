@@ -42,7 +42,9 @@ QES_D float log_abs<float2>(float2 v) { return 0.5f * logf(v.x * v.x + v.y * v.y
 QES_D float tanh_cache(float x) { return 1.f - __fdividef(2.f, __expf(2.f * x) + 1.f); }
 // Complex: the pole-safe form of tanhx, tanh(x+iy) = [sign(x)(1 - q^2) + i 4 q sin y cos y] /
 // [(1 - q)^2 + 4 q cos^2 y] with q = e^{-2|x|} in (0, 1], so no term cancels except near the poles
-// (x = 0, cos y = 0) where t is large in any evaluation.  y is first reduced to [-pi, pi] by
+// (x = 0, cos y = 0) where t is large in any evaluation; at an exact pole (den = 0 in float32) the
+// divisor is clamped to 1e-30 so that the cache holds a finite value instead of 0/0 = NaN (a NaN
+// would silently decide every later acceptance of the chain).  y is first reduced to [-pi, pi] by
 // Cody-Waite reduction (2 pi split into a float head and tail) because the hardware sine/cosine
 // is accurate (abs error ~4e-7) only on that interval.
 QES_D float2 tanh_cache(float2 z) {
@@ -53,7 +55,7 @@ QES_D float2 tanh_cache(float2 z) {
   y = fmaf(-k, -1.7484555314695172e-7f, y);                      // 2 pi - float(2 pi)
   float sy, cy;
   __sincosf(y, &sy, &cy);
-  const float den = em * em + 4.f * q * cy * cy;
+  const float den = fmaxf(em * em + 4.f * q * cy * cy, 1e-30f);
   const float re = __fdividef(copysignf(-em * (2.f + em), z.x), den);
   const float im = __fdividef(4.f * q * sy * cy, den);
   return make_float2(re, im);

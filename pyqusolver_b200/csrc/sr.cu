@@ -591,7 +591,13 @@ constexpr uint32_t kGridBarLimit = 1u << 24;     // polls (with a short sleep) b
 
 // count and gen live in different 128-byte lines; waiters poll gen with plain volatile loads so
 // that the arrivals (atomics on count) do not queue behind polling atomics
-__device__ __forceinline__ void grid_barrier(unsigned int* count, unsigned int* gen, unsigned int nb, int* err) {
+// Test hook: `extra` arrivals that never come and a short poll limit make every barrier wait run out
+// (set by qes_sr_set_barrier_test; zero / kGridBarLimit in normal use).
+struct BarCfg { unsigned int extra; unsigned int limit; };
+
+__device__ __forceinline__ void grid_barrier(unsigned int* count, unsigned int* gen, unsigned int nb, int* err,
+                                             BarCfg bc) {
+  nb += bc.extra;
   __syncthreads();
   if (threadIdx.x == 0 && threadIdx.y == 0) {
     volatile unsigned int* vgen = gen;
@@ -604,7 +610,7 @@ __device__ __forceinline__ void grid_barrier(unsigned int* count, unsigned int* 
     } else {
       uint32_t it = 0;
       while (*vgen == g) {
-        if (++it > kGridBarLimit) { atomicExch(err, 1); break; }
+        if (++it > bc.limit) { atomicExch(err, 1); break; }
         __nanosleep(20);
       }
     }
@@ -622,9 +628,10 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
                                                                  V* __restrict__ p, V* __restrict__ Ap,
                                                                  double* __restrict__ scal, double* __restrict__ part,
                                                                  unsigned int* __restrict__ bar, int* __restrict__ err,
-                                                                 TcDims td, uint16_t* __restrict__ vp) {
+                                                                 TcDims td, uint16_t* __restrict__ vp, BarCfg bc) {
   const double rr = scal[0], thresh = scal[3];
   if (scal[4] != 0.0) return;                      // converged: every CTA leaves (scal only changes below)
+  if (*(volatile int*)err != 0) return;            // an earlier barrier wait gave up: the solve is abandoned
   constexpr int NT = CF_TX * CF_TY;
   constexpr int E = VEC ? (int)(16 / sizeof(T)) : 1;      // columns per vector
   const int tid = threadIdx.y * CF_TX + threadIdx.x;
@@ -695,7 +702,7 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
   };
   d = block_sum(d);
   if (tid == 0) part[blockIdx.x] = d;
-  grid_barrier(bar, bar + 32, nb, err);
+  grid_barrier(bar, bar + 32, nb, err, bc);
   // every CTA sums the nb partials with the whole block (same fixed order in every CTA)
   auto sum_parts = [&](const double* src) -> double {
     double v = 0.0;
@@ -715,7 +722,7 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
   }
   e = block_sum(e);
   if (tid == 0) part[nb + blockIdx.x] = e;
-  grid_barrier(bar, bar + 32, nb, err);
+  grid_barrier(bar, bar + 32, nb, err, bc);
   const double rr_new = sum_parts(part + nb);
   const double beta = (rr > 0.0) ? rr_new / rr : 0.0;
   const bool conv = rr_new <= thresh;
@@ -885,7 +892,7 @@ extern "C" int qes_sr_uses_tensor_cores(int dtype, int ns, int nh, int64_t n_sam
 
 static int sr_prepare(int dtype, int64_t n_samples, const uint32_t* bits, const void* tt, const SRWork& L,
                       cudaStream_t st);
-static int sr_check_status(const SRWork& L, cudaStream_t st);
+static int sr_check_status(const SRWork& L, cudaStream_t st, bool cg_words = false);
 
 extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
                             const void* tanh_theta, const void* eloc, void* force_out, void* workspace,
@@ -938,13 +945,19 @@ static int sr_prepare(int dtype, int64_t n_samples, const uint32_t* bits, const 
   return tc_prepare_step(dtype, L.td, n_samples, bits, tt, L.tw, st);
 }
 
-static int sr_check_status(const SRWork& L, cudaStream_t st) {
-  if (!L.tc) return QES_OK;
-  int h = 0;
-  QES_CUDA_CHECK(cudaMemcpyAsync(&h, L.tw.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+// Reads the tensor-core status word and, inside a CG solve (cg_words: counter[4] was zeroed at the
+// start of the solve), the grid-barrier error word of the fused CG kernel; synchronises the stream.
+static int sr_check_status(const SRWork& L, cudaStream_t st, bool cg_words) {
+  int h[2] = {0, 0};
+  if (L.tc) QES_CUDA_CHECK(cudaMemcpyAsync(&h[0], L.tw.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (cg_words) QES_CUDA_CHECK(cudaMemcpyAsync(&h[1], L.counter + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaStreamSynchronize(st));
-  if (h != 0) {
+  if (h[0] != 0) {
     qes_set_last_message("SR tensor-core matvec: a bounded device wait gave up");
+    return QES_ERR_TIMEOUT;
+  }
+  if (h[1] != 0) {
+    qes_set_last_message("SR CG: a bounded grid-barrier wait gave up");
     return QES_ERR_TIMEOUT;
   }
   return QES_OK;
@@ -983,7 +996,7 @@ namespace {
 struct CgGraphKey {
   const void* bits; const void* tt; const void* ws; int64_t n; int ns, nh, dtype, chunk, tc, l2;
   int big, kc, nsplit, nnc, nc, spc, cl;  // tiling of the captured kernels
-  int pad;                                 // keeps the struct free of padding bytes (memcmp)
+  int bartest;                             // grid-barrier test hook armed (also keeps the struct free of padding)
   double shift;
   bool operator==(const CgGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
@@ -1008,6 +1021,8 @@ CgGraphSlot g_graph[kMaxGraphDevices];
 std::atomic<int> g_use_graphs{1};
 std::atomic<int> g_l2_persist{0};
 std::atomic<int> g_cg_fused{1};            // automatic
+std::atomic<unsigned int> g_bar_extra{0};   // test hook of the fused kernel's grid barrier
+std::atomic<unsigned int> g_bar_limit{kGridBarLimit};
 std::atomic<int> g_cg_loop{1};             // device-side loop over the CG chunks
 
 // L2 persistence of the tensor-core operands across the CG iterations: an access-policy window
@@ -1050,15 +1065,25 @@ void l2_window(cudaStream_t st, int dev, const void* base, size_t bytes) {
 __global__ void cg_loop_reset_kernel(unsigned int* count) { *count = 0u; }
 __global__ void cg_loop_cond_kernel(cudaGraphConditionalHandle h, const double* __restrict__ scal,
                                     unsigned int* __restrict__ count, unsigned int max_chunks,
-                                    const int* __restrict__ status) {
+                                    const int* __restrict__ status, const int* __restrict__ bar_err) {
   const unsigned int c = *count + 1u;
   *count = c;
-  const bool more = scal[4] == 0.0 && c < max_chunks && (status == nullptr || *status == 0);
+  const bool more = scal[4] == 0.0 && c < max_chunks && (status == nullptr || *status == 0) && *bar_err == 0;
   cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 extern "C" int qes_set_cg_device_loop(int enable) {
   g_cg_loop.store(enable ? 1 : 0);
+  return QES_OK;
+}
+
+extern "C" int qes_sr_set_barrier_test(unsigned int extra_arrivals, unsigned int poll_limit) {
+  if (extra_arrivals > 1u || (extra_arrivals == 0u) != (poll_limit == 0u)) {
+    qes_set_last_message("qes_sr_set_barrier_test: (0, 0) restores normal barriers; (1, polls) arms the test");
+    return QES_ERR_ARG;
+  }
+  g_bar_extra.store(extra_arrivals);
+  g_bar_limit.store(extra_arrivals ? std::min(poll_limit, kGridBarLimit) : kGridBarLimit);
   return QES_OK;
 }
 
@@ -1156,6 +1181,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     // 22.7 us, 6x6 J1-J2 (158 CTAs) 44.6 vs 45.7 us, 10x10 Heisenberg (290 CTAs) 46.3 vs 45.5 us)
     if (fused_mode == 1 && fused_grid > 160) fused = false;
   }
+  const BarCfg bcfg{g_bar_extra.load(), g_bar_limit.load()};
   auto run_direct = [&](int nrun, int it0) -> int {
     for (int q = 0; q < nrun; ++q) {
       if (fused) {
@@ -1190,12 +1216,12 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
           QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, true>, P, L.nsplit, fused_cv,
                                             (const T*)L.partial, opt->shift, x, r, p, Ap, L.scal, L.parts,
                                             L.counter + 32, (int*)(L.counter + 4), L.td,
-                                            L.tc ? L.tw.vp : (uint16_t*)nullptr));
+                                            L.tc ? L.tw.vp : (uint16_t*)nullptr, bcfg));
         else
           QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, false>, P, L.nsplit, fused_cv,
                                             (const T*)L.partial, opt->shift, x, r, p, Ap, L.scal, L.parts,
                                             L.counter + 32, (int*)(L.counter + 4), L.td,
-                                            L.tc ? L.tw.vp : (uint16_t*)nullptr));
+                                            L.tc ? L.tw.vp : (uint16_t*)nullptr, bcfg));
         qes_prof_end(pfr, st);
         QES_LAUNCH_CHECK();
         continue;
@@ -1242,7 +1268,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       }
       const CgGraphKey key{bits, tt, L.w, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
                            L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0), L.td.big ? 1 : 0, L.td.KC, L.nsplit,
-                           L.td.nnc, L.td.NC, L.td.SPC, L.td.cl, 0, opt->shift};
+                           L.td.nnc, L.td.NC, L.td.SPC, L.td.cl, (int)bcfg.extra, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {
           cudaGraphExecDestroy(gs.exec);
@@ -1314,7 +1340,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
               st = gs.cs;
               int rcap = run_direct(check, 1);
               if (!rcap) {
-                cg_loop_cond_kernel<<<1, 1, 0, gs.cs>>>(hnd, L.scal, lcount, lmax, L.tc ? L.tw.status : nullptr);
+                cg_loop_cond_kernel<<<1, 1, 0, gs.cs>>>(hnd, L.scal, lcount, lmax, L.tc ? L.tw.status : nullptr,
+                                                         (const int*)(L.counter + 4));
                 if (cudaPeekAtLastError() != cudaSuccess) rcap = QES_ERR_CUDA;
                 else qes_count_launches(1);
               }
@@ -1366,7 +1393,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       unsigned int chunks = 0;
       QES_CUDA_CHECK(cudaMemcpyAsync(&chunks, loop_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
       QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      rc = sr_check_status(L, st);            // synchronises the stream
+      rc = sr_check_status(L, st, true);            // synchronises the stream
       if (rc) return rc;
       if (chunks < 1 || chunks > loop_max) {
         qes_set_last_message("SR CG: the device loop ran an impossible number of chunks");
@@ -1379,7 +1406,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     }
     it += nrun;
     QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    rc = sr_check_status(L, st);          // synchronises the stream
+    rc = sr_check_status(L, st, true);          // synchronises the stream
     if (rc) return rc;
     done = hs[4] != 0.0;
   }
@@ -1388,16 +1415,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     if (graphs && g_graph[dev].init) l2_window(g_graph[dev].cs, dev, nullptr, 0);
   }
   // a bounded wait of the force pass must surface even when CG needed no iteration
-  if ((rc = sr_check_status(L, st))) return rc;
-  if (fused) {
-    int berr = 0;
-    QES_CUDA_CHECK(cudaMemcpyAsync(&berr, L.counter + 4, sizeof(int), cudaMemcpyDeviceToHost, st));
-    QES_CUDA_CHECK(cudaStreamSynchronize(st));
-    if (berr) {
-      qes_set_last_message("SR CG: a bounded grid-barrier wait gave up");
-      return QES_ERR_TIMEOUT;
-    }
-  }
+  if ((rc = sr_check_status(L, st, true))) return rc;
   // x_out = rhs_prefactor * x
   QES_CUDA_CHECK(cudaMemcpyAsync(x_out, x, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
   if (opt->rhs_prefactor != 1.0) {

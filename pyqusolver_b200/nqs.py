@@ -187,7 +187,8 @@ class NQS:
 
     # ------------------------------------------------------------------ checkpoints
     def save_checkpoint(self, directory, step, metadata=None, stats: Optional["NQSTrainStats"] = None):
-        """Flat float64/complex128 parameters + metadata (``NQSCheckpointManager`` layout of this package)."""
+        """The float64 / complex128 parameter tree and metadata in the reference's checkpoint layout
+        (``checkpoint_<step>.npz`` with "/"-flattened keys, JSON metadata beside it)."""
         from .checkpoint import NQSCheckpointManager
         meta = {"model": type(self._model).__name__, "ns": self._net.ns, "nh": self._net.nh,
                 "dtype": str(self._net.dtype), "seed": self._seed,
@@ -197,15 +198,21 @@ class NQS:
             meta["history"] = [complex(h) for h in stats.history]
             meta["history_std"] = list(stats.history_std)
         meta.update(metadata or {})
-        params = {k: v.detach().cpu().numpy() for k, v in self._net.get_params().items()}
-        return NQSCheckpointManager(directory).save(step, params, meta)
+        return NQSCheckpointManager(directory).save(step, self._net.get_params(), meta)
 
-    def load_checkpoint(self, directory, step=None):
+    def load_checkpoint(self, directory, step=None, filename=None):
+        """Load a checkpoint written by this package or by the reference (its npz layout); returns its
+        metadata."""
         from .checkpoint import NQSCheckpointManager
         mgr = NQSCheckpointManager(directory)
-        flat = mgr.load(step)
-        self._net.set_params(flat)
-        return mgr.load_metadata(step)
+        if step is None and filename is None:
+            step = mgr.latest_step
+        tree = mgr.load(step, filename=filename)
+        if set(tree) == {"params"}:
+            self._net.set_params(tree["params"])
+        else:
+            self._net.set_params(tree)
+        return mgr.load_metadata(step, filename=filename)
 
     # ------------------------------------------------------------------ evaluation
     def ansatz(self, states):
@@ -272,13 +279,51 @@ class NQS:
                                    params_cpx=net.params_cpx)
 
     # ------------------------------------------------------------------ training
-    def train(self, n_epochs=300, checkpoint_every=50, load_checkpoint=False, *, lin_solver="scipy_cg", n_batch=128,
-              num_samples=None, num_chains=None, num_thermal=None, num_sweep=None, lr=1e-2, use_sr=True,
-              use_minsr=False, rhs_prefactor=-1.0, diag_shift=1e-3, exact_predictions=None, upd_fun=None,
-              sr_tol=1e-8, sr_maxiter=1000, grad_clip=None, reset_stats=True, use_pbar=False, callback=None,
-              pt_betas=None, **kwargs) -> NQSTrainStats:
+    def train(self, n_epochs=300, checkpoint_every=50, load_checkpoint=False, *, checkpoint_step=None,
+              reset_weights=False, override=True, background=False, lin_solver="scipy_cg", pre_solver=None,
+              ode_solver="Euler", tdvp=None, grad_clip=None, n_batch=128, n_update=None, num_samples=None,
+              num_chains=None, num_thermal=None, num_sweep=None, pt_betas=None, phases=None, timing_mode="basic",
+              early_stopper=None, optimizer="sgd", lower_states=None, lr_scheduler=None, reg_scheduler=None,
+              diag_scheduler=None, lr=1e-2, reg=None, lin_sigma=None, lin_is_gram=True, lin_force_mat=False,
+              use_sr=True, use_minsr=False, rhs_prefactor=-1.0, diag_shift=1e-3, save_path=None, reset_stats=True,
+              use_pbar=True, exact_predictions=None, exact_method=None, upd_fun=None, update_kwargs=None,
+              symmetrize=None, sr_tol=1e-8, sr_maxiter=1000, callback=None, **kwargs) -> NQSTrainStats:
+        """The training loop of ``NQSTrainer.train`` (``QES/NQS/src/nqs_train.py:1460-1619``) with the
+        signature of ``NQS.train`` (``QES/NQS/nqs.py:3002-3062``).
+
+        Implemented: SR / MinSR / plain gradient with Euler (SGD) updates, the sampler overrides,
+        parallel-tempering betas, gradient clipping, learning-rate and diagonal-shift schedules given
+        as callables ``f(epoch)`` or ``f(epoch, last_loss)``, checkpoints every ``checkpoint_every``
+        epochs under ``save_path`` (and ``load_checkpoint`` / ``checkpoint_step`` to resume from one),
+        ``reset_weights``.  ``n_batch`` only chunks the reference's evaluation, which does not change
+        its results (the reference's chunking-invariance test); the kernels here need no chunking.
+        Every option whose effect is not implemented raises (no silent drop): other ODE integrators or
+        optimisers, phase and named schedulers, early stopping, excited states (``lower_states``),
+        regularisation, symmetrisation, preconditioners, other linear solvers, a formed S matrix."""
+        unsupported = {
+            "ode_solver": ode_solver not in ("Euler", "euler", None),
+            "optimizer": optimizer not in ("sgd", "SGD", None),
+            "phases": phases is not None, "early_stopper": early_stopper is not None,
+            "lower_states": bool(lower_states), "reg_scheduler": reg_scheduler is not None,
+            "reg": bool(reg), "lin_sigma": lin_sigma is not None, "lin_force_mat": bool(lin_force_mat),
+            "symmetrize": bool(symmetrize), "update_kwargs": bool(update_kwargs), "n_update": n_update is not None,
+            "background": bool(background), "exact_method": exact_method is not None,
+            "pre_solver": pre_solver not in (None, "identity", "none"),
+            "lr_scheduler": lr_scheduler is not None and not callable(lr_scheduler),
+            "diag_scheduler": diag_scheduler is not None and not callable(diag_scheduler),
+        }
+        bad = [k for k, v in unsupported.items() if v] + sorted(kwargs)
+        if bad:
+            raise NotImplementedError(f"NQS.train: options not implemented on the GPU path: {', '.join(bad)}")
         if upd_fun is not None and str(upd_fun).upper() != self._sampler._upd_rule_name:
             raise ValueError("change the update rule at construction (s_upd_fun)")
+        if reset_weights:
+            self._net.set_params(RBM((self._net.ns,), n_hidden=self._net.nh, dtype=self._net.dtype, seed=self._net.seed,
+                                     init_scale=self._net.init_scale, device=self._net.device).get_params(unravel=True))
+        if load_checkpoint:
+            if save_path is None:
+                raise ValueError("load_checkpoint needs save_path (the checkpoint directory)")
+            self.load_checkpoint(save_path, step=checkpoint_step)
         if num_chains is not None:
             self._sampler.set_numchains(num_chains)
         if num_sweep is not None:
@@ -287,35 +332,52 @@ class NQS:
             self._sampler._therm_steps = int(num_thermal)
         if pt_betas is not None:
             self._sampler.set_pt_betas(pt_betas)
-        self._tdvp = TDVP(use_sr=use_sr, use_minsr=use_minsr, rhs_prefactor=rhs_prefactor, sr_lin_solver=lin_solver,
-                          sr_diag_shift=diag_shift, sr_tol=sr_tol, sr_maxiter=sr_maxiter, grad_clip=grad_clip)
+        if tdvp is not None:
+            self._tdvp = tdvp
+        else:
+            self._tdvp = TDVP(use_sr=use_sr, use_minsr=use_minsr, rhs_prefactor=rhs_prefactor, sr_lin_solver=lin_solver,
+                              sr_diag_shift=diag_shift, sr_tol=sr_tol, sr_maxiter=sr_maxiter, grad_clip=grad_clip,
+                              sr_lin_solver_t="gram" if lin_is_gram else "matvec")
         stats = NQSTrainStats(seed=self._seed)
         if exact_predictions is not None:
             stats.exact_predictions = np.atleast_1d(np.asarray(exact_predictions))
             stats.exact = float(np.min(np.real(stats.exact_predictions)))
             self.exact = stats.exact
+
+        def sched(f, epoch, default):
+            if f is None:
+                return default
+            try:
+                return float(f(epoch, stats.history[-1] if stats.history else None))
+            except TypeError:
+                return float(f(epoch))
         for epoch in range(int(n_epochs)):
+            lr_e = sched(lr_scheduler, epoch, lr)
+            shift_e = sched(diag_scheduler, epoch, diag_shift)
+            self._tdvp.set_diag_shift(shift_e)
             t0 = time.perf_counter()
-            info = self.train_step(num_samples=num_samples, lr=lr)
+            info = self.train_step(num_samples=num_samples, lr=lr_e)
             torch.cuda.synchronize()
             stats.timings.append(time.perf_counter() - t0)
             stats.history.append(info["mean"])
             stats.history_std.append(info["std"])
-            stats.lr_history.append(float(lr))
-            stats.diag_history.append(float(diag_shift))
+            stats.lr_history.append(float(lr_e))
+            stats.diag_history.append(float(shift_e))
             stats.sigma2_history.append(info["sigma2"])
             stats.rhat_history.append(info["r_hat"])
             stats.acceptance.append(info["acceptance"])
             stats.cg_iterations.append(info["cg_iterations"])
             if callback is not None:
                 callback(epoch, info)
+            if save_path is not None and checkpoint_every and (epoch + 1) % int(checkpoint_every) == 0:
+                self.save_checkpoint(save_path, epoch + 1, stats=stats)
             if not np.isfinite(np.real(info["mean"])):
                 break
         return stats
 
     def train_step(self, num_samples=None, lr=1e-2, tdvp: Optional[TDVP] = None):
         """One VMC epoch on the GPU; returns host-side statistics of this epoch."""
-        tdvp = tdvp or self._tdvp or TDVP()
+        tdvp = tdvp or self._tdvp or TDVP(rhs_prefactor=-1.0, sr_maxiter=1000)
         net = self._net
         bits, _ = self._sampler.sample_bits(num_samples)
         _, tn, _ = dv.rbm_forward_step(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)

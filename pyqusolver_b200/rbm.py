@@ -57,18 +57,18 @@ class RBM:
         self.version = getattr(self, "version", 0) + 1
 
     def get_params(self, unravel=False):
+        """The parameter tree in the reference RBM's layout, ``{"visible_bias": a, "VisibleToHidden":
+        {"kernel": W, "bias": b}}`` (``Python/tests/nqs/test_nqs_entropy_exact_sum.py:51-57``), or the
+        flat [a, b, W] vector with ``unravel``."""
         if unravel:
             return self.master.clone()
         a, b, W = dv.split_params(self.master, self.ns, self.nh)
-        return {"visible_bias": a.clone(), "hidden_bias": b.clone(), "W": W.clone()}
+        return {"visible_bias": a.clone(), "VisibleToHidden": {"kernel": W.clone(), "bias": b.clone()}}
 
     def set_params(self, params):
         if isinstance(params, dict):
-            a = torch.as_tensor(params["visible_bias"]).reshape(-1)
-            b = torch.as_tensor(params["hidden_bias"]).reshape(-1)
-            W = torch.as_tensor(params["W"]).reshape(-1)
-            flat = torch.cat([a.to(self.master_dtype).cpu(), b.to(self.master_dtype).cpu(),
-                              W.to(self.master_dtype).cpu()])
+            a, b, W = rbm_leaves(params)
+            flat = torch.cat([torch.as_tensor(x).reshape(-1).to(self.master_dtype).cpu() for x in (a, b, W)])
         else:
             flat = torch.as_tensor(params).reshape(-1)
         if flat.numel() != self.n_params:
@@ -143,6 +143,32 @@ class RBM:
         """log psi as a differentiable function of the flat parameter tensor."""
         p = self.flat.detach().requires_grad_(True) if params is None else params
         return RBMLogPsi.apply(p, self.bits(states), self), p
+
+
+def rbm_leaves(params):
+    """(a, b, W) of an RBM parameter tree: the reference's nested layout (``visible_bias``,
+    ``VisibleToHidden/kernel``, ``VisibleToHidden/bias``), its flattened npz form with keys joined
+    by "/", or the names ``visible_bias`` / ``hidden_bias`` / ``W``; a leading ``params/`` level is
+    accepted.  Raises KeyError when a leaf is missing."""
+    flat = {}
+
+    def walk(d, prefix):
+        for k, v in d.items():
+            key = f"{prefix}/{k}" if prefix else str(k)
+            if isinstance(v, dict):
+                walk(v, key)
+            else:
+                flat[key] = v
+    walk(params, "")
+    flat = {(k[len("params/"):] if k.startswith("params/") else k): v for k, v in flat.items()}
+
+    def pick(*names):
+        for n in names:
+            if n in flat:
+                return flat[n]
+        raise KeyError(f"RBM parameter tree has none of {names}; keys: {sorted(flat)}")
+    return (pick("visible_bias"), pick("VisibleToHidden/bias", "hidden_bias"),
+            pick("VisibleToHidden/kernel", "W"))
 
 
 def _is_complex(dt):

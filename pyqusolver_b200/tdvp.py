@@ -35,17 +35,39 @@ class TDVPStepInfo:
     residual: float
 
 
+_SOLVERS_CG = ("scipy_cg", "cg")
+
+
 class TDVP:
-    def __init__(self, use_sr=True, use_minsr=False, rhs_prefactor=-1.0, sr_lin_solver="scipy_cg",
-                 sr_diag_shift=1e-3, sr_tol=1e-8, sr_atol=0.0, sr_maxiter=1000, grad_clip=None,
-                 check_every=16, sr_lin_x0=None, use_old_result=False, **kwargs):
-        solver = str(sr_lin_solver).lower()
-        if solver not in ("scipy_cg", "cg"):
-            raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG")
+    """Keyword arguments mirror ``TDVP.__init__`` (``tdvp.py:322-350``), defaults included
+    (``rhs_prefactor=1.0``, ``sr_maxiter=100``; ``NQS.train`` passes the trainer's -1.0 / 1000).
+    Options whose effect this path does not implement raise instead of being ignored; options that
+    only tune solvers or features this path does not offer (the pseudo-inverse and SNR tolerances,
+    backend, logger, timing) are accepted because they cannot change a CG result.  ``sr_tol`` /
+    ``sr_atol`` (SciPy's rtol / atol), ``check_every`` and ``use_old_result`` are this package's
+    additions."""
+
+    def __init__(self, use_sr=True, use_minsr=False, rhs_prefactor=1.0, *, regularization=0.0,
+                 sr_lin_solver=None, sr_precond=None, sr_snr_tol=1e-3, sr_pinv_tol=1e-14, sr_pinv_cutoff=1e-8,
+                 sr_diag_shift=1e-3, sr_lin_solver_t="gram", sr_lin_x0=None, sr_maxiter=100, sr_form_matrix=False,
+                 backend="default", logger=None, use_timing=False, dtype=None, grad_clip=None, verbose=False,
+                 sr_tol=1e-8, sr_atol=0.0, check_every=16, use_old_result=False):
+        solver = "scipy_cg" if sr_lin_solver is None else str(getattr(sr_lin_solver, "name", sr_lin_solver)).lower()
+        if solver not in _SOLVERS_CG:
+            raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG (scipy_cg)")
+        if sr_precond not in (None, "identity", "none"):
+            raise NotImplementedError(f"preconditioner {sr_precond!r} is not implemented on the GPU path")
+        if str(sr_lin_solver_t).lower() not in ("gram", "matvec", "matrix_free"):
+            raise NotImplementedError(f"solver form {sr_lin_solver_t!r}: the GPU path applies S matrix-free")
+        if sr_form_matrix:
+            raise NotImplementedError("sr_form_matrix=True is not implemented on the GPU path")
+        if regularization:
+            raise NotImplementedError("regularization != 0 is not implemented on the GPU path")
         self.use_sr = bool(use_sr)
         self.use_minsr = bool(use_minsr)
         self._minsr_ws = None
         self.rhs_prefactor = float(rhs_prefactor)
+        self.sr_lin_solver = solver
         self.sr_diag_shift = float(sr_diag_shift)
         self.sr_tol = float(sr_tol)
         self.sr_atol = float(sr_atol)

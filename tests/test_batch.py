@@ -111,7 +111,7 @@ def test_batch_training_step_updates_each_problem_like_single():
         for b, m in enumerate(models):
             q = single(m, seeds[b], "float32", 32, 4, 2)
             assert torch.equal(q.net.master, before[b])
-            i1 = q.train_step(lr=0.02, tdvp=TDVP(sr_diag_shift=1e-3))
+            i1 = q.train_step(lr=0.02, tdvp=TDVP(rhs_prefactor=-1.0, sr_diag_shift=1e-3))
             assert info["mean"][b] == pytest.approx(i1["mean"], rel=1e-12)
             d_batch = B.params(b) - before[b]
             d_single = q.net.master - before[b]

@@ -47,6 +47,27 @@ def rel_err(a, b):
     return np.max(np.abs(a - b)) / max(1e-30, np.max(np.abs(b)))
 
 
+# A float32 Delta log psi (with the sampler's hardware-approximation tanh cache) can decide a
+# Metropolis step the other way only where the float64 oracle's |log u - log_acc| is within its
+# rounding; chains whose decisions all kept a larger margin must follow the oracle exactly.
+TIE = 1e-3
+
+
+def assert_same_trajectories(got, cfg, ref, n_chains, accepted=None):
+    """Rows are sample-major (row = sample * n_chains + chain).  Chains that never met a near-tie
+    decision in the oracle must match row for row (and in their acceptance counts); the near-tie
+    chains are a small minority."""
+    tie = ref.min_margin <= TIE
+    chain_of_row = np.arange(got.shape[0]) % n_chains
+    strict = ~tie[chain_of_row]
+    bad = np.flatnonzero(strict & np.any(got != cfg, axis=1))
+    assert bad.size == 0, (bad[:10], ref.min_margin[chain_of_row[bad[:10]]])
+    assert np.mean(tie) <= 0.05, np.mean(tie)
+    if accepted is not None:
+        assert np.array_equal(accepted[~tie], ref.accepted[~tie])
+    return strict
+
+
 # ------------------------------------------------------------------------- chains
 @pytest.mark.parametrize("ns", [16, 36, 100, 400])
 def test_init_chains_match_oracle(ns):
@@ -282,10 +303,8 @@ def test_sampler_local_trajectory_matches_oracle(cplx, nh):
     got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
     ref = osm.MetropolisSampler(ns, 64, rule="LOCAL", seed=77, therm_steps=2, sweep_steps=5)
     cfg, lp_ref, _ = ref.sample(oracle_params(net), 6)
-    mism = np.mean(np.any(got != cfg, axis=1))
-    assert mism <= 0.02, mism          # float32 vs float64 ties may flip a rare decision
-    same = np.all(got == cfg, axis=1)
-    wrap_close(lp.cpu().numpy()[same], lp_ref[same])
+    strict = assert_same_trajectories(got, cfg, ref, 64, accepted=smp.accepted.cpu().numpy())
+    wrap_close(lp.cpu().numpy()[strict], lp_ref[strict])
     assert np.array_equal(smp.proposed.cpu().numpy(), ref.proposed)
 
 
@@ -301,9 +320,7 @@ def test_sampler_exchange_trajectory_matches_oracle(cplx):
                                 therm_steps=1, sweep_steps=7, init="RND_FIXED", n_up=8)
     cfg, _, _ = ref.sample(oracle_params(net), 5)
     assert np.all((got > 0).sum(1) == 8)
-    assert np.mean(np.any(got != cfg, axis=1)) <= 0.02
-    acc_g = smp.accepted.cpu().numpy()
-    assert np.mean(acc_g != ref.accepted) <= 0.05
+    assert_same_trajectories(got, cfg, ref, 64, accepted=smp.accepted.cpu().numpy())
 
 
 @pytest.mark.parametrize("rule,cplx,nh", [("LOCAL", False, 64), ("EXCHANGE", True, 200), ("EXCHANGE", False, 20)])
@@ -330,7 +347,7 @@ def test_capped_sampler_kernel_is_bit_identical(rule, cplx, nh):
     ref = osm.MetropolisSampler(ns, 256, rule=rule, seed=23, therm_steps=2, sweep_steps=6, **okw)
     cfg, _, _ = ref.sample(oracle_params(net), 4)
     got = dv.unpack_states(torch.as_tensor(out[1][0]).cuda(), ns, 1.0).cpu().numpy()
-    assert np.mean(np.any(got != cfg, axis=1)) <= 0.02
+    assert_same_trajectories(got, cfg, ref, 256, accepted=out[1][2])
 
 
 def test_sampler_tanh_cache_error_bound():
@@ -349,11 +366,17 @@ def test_sampler_tanh_cache_error_bound():
     n = 200000
     z = (rng.uniform(-6, 6, n) + 1j * rng.uniform(-40, 40, n)).astype(np.complex64)
     z[:1000] = (rng.normal(scale=1e-3, size=1000) + 1j * rng.uniform(-3, 3, 1000)).astype(np.complex64)
-    zt = torch.as_tensor(z).cuda()
+    # the poles x = 0, y = pi/2 + k pi (in float32): the cache must stay finite there
+    poles = np.float32(np.pi / 2) + np.float32(np.pi) * np.arange(-8, 8, dtype=np.float32)
+    zt = torch.as_tensor(np.concatenate([z, 1j * poles.astype(np.complex64), 1j * np.nextafter(poles, np.float32(9))
+                                         .astype(np.complex64)])).cuda()
     yt = torch.empty_like(zt)
     torch.cuda.synchronize()
-    _lib.call("qes_sampler_tanh_cache", _lib.DTYPE_C64, n, _lib.ptr(zt), _lib.ptr(yt), _lib.stream_ptr())
+    _lib.call("qes_sampler_tanh_cache", _lib.DTYPE_C64, int(zt.numel()), _lib.ptr(zt), _lib.ptr(yt),
+              _lib.stream_ptr())
     got = yt.cpu().numpy().astype(np.complex128)
+    assert np.all(np.isfinite(got))
+    got = got[:n]
     ref = np.tanh(z.astype(np.complex128))
     err = np.abs(got - ref) / (1.0 + np.abs(ref) ** 2)
     assert np.max(err) < 1e-6, np.max(err)
@@ -388,8 +411,7 @@ def test_sampler_exchange_process_matches_oracle_histogram():
     ref = osm.MetropolisSampler(ns, 512, rule="EXCHANGE", neighbor_table=olat.neighbor_table(OL), seed=3,
                                 therm_steps=4, sweep_steps=10, init="RND_FIXED", n_up=5)
     cfg, _, _ = ref.sample(oracle_params(net), 20)
-    frac = np.mean(np.any(got != cfg, axis=1))
-    assert frac <= 0.02, frac
+    assert_same_trajectories(got, cfg, ref, 512, accepted=smp.accepted.cpu().numpy())
 
 
 def test_sampler_continues_chains_without_rethermalising():
@@ -724,9 +746,10 @@ def test_parallel_tempering_matches_oracle(rule):
     ref = osm.ParallelTemperingSampler(ns, C, betas, rule=rule, neighbor_table=olat.neighbor_table(OL), seed=9,
                                        therm_steps=1, sweep_steps=5, init=init or "RND", n_up=n_up)
     cfg, lp_ref, _ = ref.sample(oracle_params(net), 4)
-    assert np.mean(np.any(got != cfg, axis=1)) <= 0.03
+    assert_same_trajectories(got, cfg, ref, C)
     gb = smp.chain_betas.cpu().numpy().astype(np.float64)
-    assert np.mean(np.any(gb != ref.betas, axis=0)) <= 0.05
+    strict = ref.min_margin > TIE
+    assert np.array_equal(gb[:, strict], ref.betas[:, strict])
     assert smp._pt_round == ref.round
 
 

@@ -165,19 +165,54 @@ def test_torch_ops_are_registered():
 
 def test_checkpoint_manager_roundtrip(tmp_path):
     from pyqusolver_b200.checkpoint import NQSCheckpointManager
+    from pyqusolver_b200.rbm import rbm_leaves
     mgr = NQSCheckpointManager(tmp_path, max_to_keep=2)
     rng = np.random.default_rng(0)
-    params = {"visible_bias": rng.normal(size=4) + 1j, "hidden_bias": rng.normal(size=8) + 0j,
-              "W": rng.normal(size=(4, 8)) - 2j}
+    params = {"visible_bias": rng.normal(size=4) + 1j,
+              "VisibleToHidden": {"kernel": rng.normal(size=(4, 8)) - 2j, "bias": rng.normal(size=8) + 0j}}
     for step in (1, 2, 3):
         mgr.save(step, params, {"energy": complex(-1.5, 0.0), "lr": 0.01})
     assert mgr.list_checkpoints() == [2, 3]                 # max_to_keep prunes the oldest
-    assert mgr.latest_step() == 3
-    flat = mgr.load()
-    ref = np.concatenate([params["visible_bias"], params["hidden_bias"], params["W"].reshape(-1)])
-    assert flat.dtype == np.complex128 and np.array_equal(flat, ref)
+    assert mgr.latest_step == 3
+    assert not (tmp_path / "metadata_1.json").exists() and not (tmp_path / "checkpoint_1.json").exists()
+    tree = mgr.load()
+    assert sorted(tree) == ["VisibleToHidden/bias", "VisibleToHidden/kernel", "visible_bias"]
+    a, b, W = rbm_leaves(tree)
+    assert np.array_equal(a, params["visible_bias"]) and np.array_equal(W, params["VisibleToHidden"]["kernel"])
+    assert np.array_equal(b, params["VisibleToHidden"]["bias"])
     meta = mgr.load_metadata(3)
-    assert meta["step"] == 3 and meta["lr"] == 0.01 and meta["energy"] == {"re": -1.5, "im": 0.0}
+    assert meta["step"] == 3 and meta["lr"] == 0.01
+    assert meta["energy"] == {"__complex__": True, "real": -1.5, "imag": 0.0}
+    # a custom file name keeps its metadata beside it
+    p = mgr.save("x", params, {"lr": 0.5}, filename="custom.h5")
+    assert p.name == "custom.npz" and (tmp_path / "custom.json").exists()
+    assert mgr.load_metadata(filename="custom.h5")["lr"] == 0.5
+    assert sorted(mgr.load(filename="custom.h5")) == sorted(tree)
+
+
+def test_checkpoint_reads_files_in_the_reference_layout(tmp_path):
+    """Files as the reference's HDF5-less path writes them (QES/NQS/src/nqs_checkpoint_manager.py:
+    np.savez of the "/"-flattened tree, metadata_<step>.json with the complex encoding of
+    _make_json_serializable), read back by this package's manager and RBM tree reader."""
+    import json
+    from pyqusolver_b200.checkpoint import NQSCheckpointManager
+    from pyqusolver_b200.rbm import rbm_leaves
+    rng = np.random.default_rng(3)
+    a = rng.normal(size=6) + 1j * rng.normal(size=6)
+    W = rng.normal(size=(6, 12)) + 1j * rng.normal(size=(6, 12))
+    b = rng.normal(size=12) + 1j * rng.normal(size=12)
+    np.savez(tmp_path / "checkpoint_7.npz", **{"visible_bias": a, "VisibleToHidden/kernel": W,
+                                               "VisibleToHidden/bias": b})
+    (tmp_path / "metadata_7.json").write_text(json.dumps(
+        {"step": 7, "E": {"__complex__": True, "real": -3.25, "imag": 0.5}}, indent=2))
+    mgr = NQSCheckpointManager(tmp_path)
+    assert mgr.list_checkpoints() == [7] and mgr.latest_step == 7
+    ga, gb, gW = rbm_leaves(mgr.load(7))
+    assert np.array_equal(ga, a) and np.array_equal(gb, b) and np.array_equal(gW, W)
+    assert mgr.load_metadata(7)["E"]["real"] == -3.25
+    # the names of the older flat layout are read as well
+    ga, gb, gW = rbm_leaves({"params": {"visible_bias": a, "hidden_bias": b, "W": W}})
+    assert np.array_equal(gW, W) and np.array_equal(gb, b)
 
 
 def test_tdvp_initial_guess_selection():

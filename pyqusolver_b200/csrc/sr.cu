@@ -67,79 +67,6 @@ QES_D float from_c(float2 v, float) { return v.x; }
 QES_D float2 from_c(float2 v, float2) { return v; }
 
 // ----------------------------------------------------------------------------
-// (O v)_s : theta-like pass with V in place of W, fused with the dot with t_s
-// ----------------------------------------------------------------------------
-constexpr int OV_SB = 16;
-constexpr int OV_THREADS = 256;
-
-// samples [s0, s0 + OV_SB) of one problem; smw holds OV_SB * n_words(ns) words
-template <class T, class V>
-QES_D void ov_block(int64_t s0, uint32_t* smw, int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits,
-                    const T* __restrict__ tanh_theta, const V* __restrict__ v, float2* __restrict__ w_out) {
-  const int nw = n_words(ns);
-  const int nsb = (int)min((int64_t)OV_SB, n_samples - s0);
-  for (int q = threadIdx.x; q < OV_SB * nw; q += blockDim.x) {
-    const int sl = q / nw;
-    smw[q] = (sl < nsb) ? bits[(s0 + sl) * nw + (q % nw)] : 0u;
-  }
-  __syncthreads();
-  const V* va = v;
-  const V* vb = v + ns;
-  const V* vW = v + ns + nh;
-  T part[OV_SB];
-#pragma unroll
-  for (int q = 0; q < OV_SB; ++q) part[q] = ScalarTraits<T>::zero();
-  for (int m = threadIdx.x; m < nh; m += blockDim.x) {
-    const T bm = to_f(vb[m]);
-    T z[OV_SB];
-#pragma unroll
-    for (int q = 0; q < OV_SB; ++q) z[q] = bm;
-    for (int i = 0; i < ns; ++i) {
-      const T x = to_f(vW[(int64_t)i * nh + m]);
-#pragma unroll
-      for (int q = 0; q < OV_SB; ++q) {
-        const uint32_t bit = (smw[q * nw + (i >> 5)] >> (i & 31)) & 1u;
-        z[q] = addx(z[q], bit ? x : scal(-1.f, x));
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < OV_SB; ++q)
-      if (q < nsb) part[q] = addx(part[q], mulx(tanh_theta[(s0 + q) * nh + m], z[q]));
-  }
-  for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-    const T x = to_f(va[i]);
-#pragma unroll
-    for (int q = 0; q < OV_SB; ++q) {
-      const uint32_t bit = (smw[q * nw + (i >> 5)] >> (i & 31)) & 1u;
-      part[q] = addx(part[q], bit ? x : scal(-1.f, x));
-    }
-  }
-  __shared__ T red[OV_THREADS / 32][OV_SB];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < OV_SB; ++q) {
-    T s = warp_sum(part[q]);
-    if (lane == 0) red[warp][q] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x < nsb) {
-    T s = ScalarTraits<T>::zero();
-    for (int w = 0; w < OV_THREADS / 32; ++w) s = addx(s, red[w][threadIdx.x]);
-    w_out[s0 + threadIdx.x] = to_c(s);
-  }
-}
-
-template <class T, class V>
-__global__ void __launch_bounds__(OV_THREADS) ov_kernel(int ns, int nh, int64_t n_samples,
-                                                        const uint32_t* __restrict__ bits,
-                                                        const T* __restrict__ tanh_theta, const V* __restrict__ v,
-                                                        float2* __restrict__ w_out, const double* __restrict__ cg_done) {
-  extern __shared__ uint32_t smw[];
-  if (cg_done && *cg_done != 0.0) return;                  // converged CG (stream order: exact)
-  ov_block<T, V>((int64_t)blockIdx.x * OV_SB, smw, ns, nh, n_samples, bits, tanh_theta, v, w_out);
-}
-
-// ----------------------------------------------------------------------------
 // mean of a complex float32 vector in float64 -> out[0..1]  (one block)
 // ----------------------------------------------------------------------------
 constexpr int MEAN_THREADS = 1024;
@@ -161,109 +88,218 @@ __global__ void __launch_bounds__(MEAN_THREADS) mean_c_kernel(int64_t n, const f
 }
 
 // ----------------------------------------------------------------------------
-// O^H u with u_s = (w_s - mean) * scale.   Block: 64 hidden units (tx) x
-// 4 rows of 4 sites (ty) over one split of the samples; 32-sample sub-chunks
-// of Q_sm = conj(t_sm) u_s and of the spin words are staged in shared memory.
+// Plain-FP32 form: register-tiled CUDA-core contractions.  The spins are staged in shared memory
+// as +-1 floats, so every sign x value product is one FMA.  Block 32 x 8 threads; a thread owns R
+// rows x PT_C columns of the output tile, columns interleaved by 32 (conflict-free shared-memory
+// loads), rows interleaved by 8 (all lanes of a warp read the same spin: a broadcast).
 // ----------------------------------------------------------------------------
-constexpr int OHU_TM = 64;
-constexpr int OHU_TY = 4;
-constexpr int OHU_SPT = 4;                       // sites per thread
-constexpr int OHU_TI = OHU_TY * OHU_SPT;         // 16 sites per block
-constexpr int OHU_SC = 32;                       // samples per staged sub-chunk
-constexpr int OHU_SPLIT_SAMPLES = 256;           // samples per split
+constexpr int PT_TX = 32, PT_TY = 8, PT_C = 4;
+constexpr int PT_THREADS = PT_TX * PT_TY;
+constexpr int PT_U = PT_TX * PT_C;            // columns (hidden units) per block
+constexpr int PT_K = 32;                      // contraction slice staged per pass
+constexpr int PT_SPLIT = 512;                 // samples per O^H u split (one partial P-vector each)
 
-// tile (bx: 64 hidden units, by: 16 sites, bz: one split of samples) of one problem
-template <class T>
-QES_D void ohu_block(int bx, int by, int bz, int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits,
-                     const T* __restrict__ tanh_theta, const float2* __restrict__ w,
-                     const double* __restrict__ wmean, double scale, T* __restrict__ partial) {
-  __shared__ T Q[OHU_SC][OHU_TM];
-  __shared__ T U[OHU_SC];
-  __shared__ uint32_t SW[OHU_SC][2];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * OHU_TM + tx;
-  const int m0 = bx * OHU_TM, i0 = by * OHU_TI;
-  const int m = m0 + tx;
-  const int64_t sbeg = (int64_t)bz * OHU_SPLIT_SAMPLES;
-  const int64_t send = min(n_samples, sbeg + OHU_SPLIT_SAMPLES);
+QES_D float fma_s(float s, float v, float a) { return fmaf(s, v, a); }
+QES_D float2 fma_s(float s, float2 v, float2 a) { return make_float2(fmaf(s, v.x, a.x), fmaf(s, v.y, a.y)); }
+
+// wpart[ub][s] = sum over the hidden units j of block ub of t_sj (v_b,j + sum_i sigma_si V_ij),
+// plus sigma_s . v_a in unit block 0: z = Sigma V is accumulated in registers over 32-site slices
+// (one spin word per sample and slice), then folded with t and summed over the warp's lanes.
+template <class T, class V, int R>
+__global__ void __launch_bounds__(PT_THREADS) ov_tile_kernel(int ns, int nh, int64_t n_samples,
+                                                             const uint32_t* __restrict__ bits,
+                                                             const T* __restrict__ tanh_theta,
+                                                             const V* __restrict__ v, float2* __restrict__ wpart,
+                                                             const double* __restrict__ cg_done) {
+  constexpr int S = PT_TY * R;                   // samples per block
+  __shared__ float sg[PT_K][S];
+  __shared__ T vs[PT_K][PT_U];
+  if (cg_done && *cg_done != 0.0) return;        // converged CG (stream order: exact)
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PT_TX + tx;
+  const int64_t s0 = (int64_t)blockIdx.x * S;
+  const int j0 = blockIdx.y * PT_U;
   const int nw = n_words(ns);
-  const int wlo = i0 >> 5;
-  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  const V* va = v;
+  const V* vb = v + ns;
+  const V* vW = v + ns + nh;
+  T z[R][PT_C];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int c = 0; c < PT_C; ++c) z[r][c] = ScalarTraits<T>::zero();
+  for (int i0 = 0; i0 < ns; i0 += PT_K) {
+    __syncthreads();                             // the previous slice is consumed
+    for (int e = tid; e < PT_K * S; e += PT_THREADS) {
+      const int sl = e % S, il = e / S;
+      const int64_t s = s0 + sl;
+      float x = 0.f;
+      if (s < n_samples && i0 + il < ns) x = ((__ldg(bits + s * nw + (i0 >> 5)) >> il) & 1u) ? 1.f : -1.f;
+      sg[il][sl] = x;
+    }
+    for (int e = tid; e < PT_K * PT_U; e += PT_THREADS) {
+      const int il = e / PT_U, jl = e % PT_U;
+      const int i = i0 + il, j = j0 + jl;
+      vs[il][jl] = (i < ns && j < nh) ? to_f(vW[(int64_t)i * nh + j]) : ScalarTraits<T>::zero();
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int il = 0; il < PT_K; ++il) {
+      float sv[R];
+      T q[PT_C];
+#pragma unroll
+      for (int r = 0; r < R; ++r) sv[r] = sg[il][r * PT_TY + ty];
+#pragma unroll
+      for (int c = 0; c < PT_C; ++c) q[c] = vs[il][c * PT_TX + tx];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int c = 0; c < PT_C; ++c) z[r][c] = fma_s(sv[r], q[c], z[r][c]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t s = s0 + r * PT_TY + ty;
+    T acc = ScalarTraits<T>::zero();
+    if (s < n_samples) {
+#pragma unroll
+      for (int c = 0; c < PT_C; ++c) {
+        const int j = j0 + c * PT_TX + tx;
+        if (j < nh) acc = addx(acc, mulx(tanh_theta[s * nh + j], addx(z[r][c], to_f(vb[j]))));
+      }
+      if (blockIdx.y == 0) {                     // sigma_s . v_a, lanes over the sites
+        for (int i = tx; i < ns; i += PT_TX) {
+          const bool up = (__ldg(bits + s * nw + (i >> 5)) >> (i & 31)) & 1u;
+          acc = addx(acc, up ? to_f(va[i]) : scal(-1.f, to_f(va[i])));
+        }
+      }
+    }
+    acc = warp_sum(acc);
+    if (tx == 0 && s < n_samples) wpart[(int64_t)blockIdx.y * n_samples + s] = to_c(acc);
+  }
+}
+
+// w = sum of the unit-block partials (fixed order); mean of w in float64 when wmean is given
+__global__ void __launch_bounds__(1024) wsum_kernel(int64_t n, int nub, const float2* __restrict__ wpart,
+                                                     float2* __restrict__ w, double* __restrict__ wmean,
+                                                     const double* __restrict__ cg_done) {
+  if (cg_done && *cg_done != 0.0) return;
+  double sr = 0, si = 0;
+  for (int64_t k = threadIdx.x; k < n; k += blockDim.x) {
+    float2 a = wpart[k];
+    for (int b = 1; b < nub; ++b) a = a + wpart[(int64_t)b * n + k];
+    w[k] = a;
+    sr += a.x;
+    si += a.y;
+  }
+  if (!wmean) return;
+  __shared__ double rr[32], ri[32];
+  sr = warp_sum(sr);
+  si = warp_sum(si);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) { rr[warp] = sr; ri[warp] = si; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { a += rr[q]; b += ri[q]; }
+    wmean[0] = a / (double)n;
+    wmean[1] = b / (double)n;
+  }
+}
+
+// partial[split] = Sigma~^T Q~ over PT_SPLIT samples: rows are the sites plus a ones row at site
+// ns (-> g_b), columns the hidden units plus a virtual unit at nh carrying u itself (-> g_a);
+// Q_sj = conj(t_sj) u_s with u_s = (w_s - mean) * scale, staged 32 samples at a time.
+template <class T, int R>
+__global__ void __launch_bounds__(PT_THREADS) ohu_tile_kernel(int ns, int nh, int64_t n_samples,
+                                                              const uint32_t* __restrict__ bits,
+                                                              const T* __restrict__ tanh_theta,
+                                                              const float2* __restrict__ w,
+                                                              const double* __restrict__ wmean, double scale,
+                                                              T* __restrict__ partial,
+                                                              const double* __restrict__ cg_done) {
+  constexpr int IB = PT_TY * R;                  // sites per block
+  __shared__ float sg[PT_K][IB];
+  __shared__ T qs[PT_K][PT_U];
+  __shared__ T us[PT_K];
+  if (cg_done && *cg_done != 0.0) return;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PT_TX + tx;
+  const int j0 = blockIdx.x * PT_U, i0 = blockIdx.y * IB;
+  const int64_t sbeg = (int64_t)blockIdx.z * PT_SPLIT;
+  const int64_t send = min(n_samples, sbeg + PT_SPLIT);
+  const int nw = n_words(ns);
   const float mr = wmean ? (float)wmean[0] : 0.f, mi = wmean ? (float)wmean[1] : 0.f;
   const float fs = (float)scale;
-
-  T acc[OHU_SPT], accb = ScalarTraits<T>::zero(), acca[OHU_SPT];
+  T acc[R][PT_C];
 #pragma unroll
-  for (int k = 0; k < OHU_SPT; ++k) { acc[k] = ScalarTraits<T>::zero(); acca[k] = ScalarTraits<T>::zero(); }
-
-  for (int64_t c0 = sbeg; c0 < send; c0 += OHU_SC) {
-    const int nc = (int)min((int64_t)OHU_SC, send - c0);
-    if (tid < OHU_SC) {
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int c = 0; c < PT_C; ++c) acc[r][c] = ScalarTraits<T>::zero();
+  for (int64_t c0 = sbeg; c0 < send; c0 += PT_K) {
+    const int nc = (int)min((int64_t)PT_K, send - c0);
+    __syncthreads();                             // the previous sub-chunk is consumed
+    if (tid < PT_K) {
       T u = ScalarTraits<T>::zero();
       if (tid < nc) {
         const float2 wv = w[c0 + tid];
         u = from_c(make_float2((wv.x - mr) * fs, (wv.y - mi) * fs), T());
       }
-      U[tid] = u;
-      SW[tid][0] = (tid < nc) ? bits[(c0 + tid) * nw + wlo] : 0u;
-      SW[tid][1] = (tid < nc && wlo + 1 < nw) ? bits[(c0 + tid) * nw + wlo + 1] : 0u;
+      us[tid] = u;
     }
-    __syncthreads();
-    for (int e = tid; e < OHU_SC * OHU_TM; e += OHU_TM * OHU_TY) {
-      const int sl = e / OHU_TM, ml = e % OHU_TM;
+    for (int e = tid; e < PT_K * IB; e += PT_THREADS) {
+      const int sl = e / IB, il = e % IB, i = i0 + il;
+      float x = 0.f;
+      if (sl < nc) {
+        if (i < ns) x = ((__ldg(bits + (c0 + sl) * nw + (i >> 5)) >> (i & 31)) & 1u) ? 1.f : -1.f;
+        else if (i == ns) x = 1.f;
+      }
+      sg[sl][il] = x;
+    }
+    __syncthreads();                             // us
+    for (int e = tid; e < PT_K * PT_U; e += PT_THREADS) {
+      const int sl = e / PT_U, jl = e % PT_U, j = j0 + jl;
       T q = ScalarTraits<T>::zero();
-      if (sl < nc && m0 + ml < nh) q = mulx(conjx(tanh_theta[(c0 + sl) * nh + m0 + ml]), U[sl]);
-      Q[sl][ml] = q;
+      if (sl < nc) {
+        if (j < nh) q = mulx(conjx(tanh_theta[(c0 + sl) * nh + j]), us[sl]);
+        else if (j == nh) q = us[sl];
+      }
+      qs[sl][jl] = q;
     }
     __syncthreads();
-    for (int sl = 0; sl < nc; ++sl) {
-      const T q = Q[sl][tx];
-      const uint64_t wd = ((uint64_t)SW[sl][1] << 32) | SW[sl][0];
+#pragma unroll 8
+    for (int sl = 0; sl < PT_K; ++sl) {
+      float sv[R];
+      T q[PT_C];
 #pragma unroll
-      for (int k = 0; k < OHU_SPT; ++k) {
-        const int il = ty * OHU_SPT + k + (i0 & 31);
-        const bool up = (wd >> il) & 1ull;
-        acc[k] = addx(acc[k], up ? q : scal(-1.f, q));
-      }
-      if (by == 0 && ty == 0) accb = addx(accb, q);
-      if (bx == 0 && tx == 0) {
-        const T u = U[sl];
+      for (int r = 0; r < R; ++r) sv[r] = sg[sl][r * PT_TY + ty];
 #pragma unroll
-        for (int k = 0; k < OHU_SPT; ++k) {
-          const int il = ty * OHU_SPT + k + (i0 & 31);
-          const bool up = (wd >> il) & 1ull;
-          acca[k] = addx(acca[k], up ? u : scal(-1.f, u));
-        }
-      }
+      for (int c = 0; c < PT_C; ++c) q[c] = qs[sl][c * PT_TX + tx];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int c = 0; c < PT_C; ++c) acc[r][c] = fma_s(sv[r], q[c], acc[r][c]);
     }
-    __syncthreads();
   }
-  T* out = partial + (int64_t)bz * P;
-  if (m < nh) {
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  T* out = partial + (int64_t)blockIdx.z * P;
 #pragma unroll
-    for (int k = 0; k < OHU_SPT; ++k) {
-      const int i = i0 + ty * OHU_SPT + k;
-      if (i < ns) out[ns + nh + (int64_t)i * nh + m] = acc[k];
-    }
-    if (by == 0 && ty == 0) out[ns + m] = accb;
-  }
-  if (bx == 0 && tx == 0) {
+  for (int r = 0; r < R; ++r) {
+    const int i = i0 + r * PT_TY + ty;
 #pragma unroll
-    for (int k = 0; k < OHU_SPT; ++k) {
-      const int i = i0 + ty * OHU_SPT + k;
-      if (i < ns) out[i] = acca[k];
+    for (int c = 0; c < PT_C; ++c) {
+      const int j = j0 + c * PT_TX + tx;
+      if (i < ns && j < nh) out[ns + nh + (int64_t)i * nh + j] = acc[r][c];
+      else if (i == ns && j < nh) out[ns + j] = acc[r][c];
+      else if (i < ns && j == nh) out[i] = acc[r][c];
     }
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(OHU_TM * OHU_TY) ohu_kernel(
-    int ns, int nh, int64_t n_samples, const uint32_t* __restrict__ bits, const T* __restrict__ tanh_theta,
-    const float2* __restrict__ w, const double* __restrict__ wmean, double scale, T* __restrict__ partial,
-    const double* __restrict__ cg_done) {
-  if (cg_done && *cg_done != 0.0) return;                  // converged CG (stream order: exact)
-  ohu_block<T>(blockIdx.x, blockIdx.y, blockIdx.z, ns, nh, n_samples, bits, tanh_theta, w, wmean, scale, partial);
-}
+// row-tile heights: 8 rows per thread where the sites or samples are many (fewer re-reads of
+// the column operand), 4 otherwise
+static int pt_rows_ov(int64_t n_samples) { return n_samples >= 64 * 148 ? 8 : 4; }
+static int pt_rows_ohu(int ns) { return ns + 1 > 64 ? 8 : 4; }
+
+constexpr int OHU_SPLIT_SAMPLES = 256;           // samples per split of the batched O^H u
 
 // sum the split partials in float64; optional  y = G + shift * p  and  dot partials of p^H y.
 // A block covers cv column vectors (16 bytes: 2 complex / 4 real columns when VEC, else one
@@ -751,6 +787,7 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
 // ----------------------------------------------------------------------------
 struct SRWork {
   float2* w;          // [Ns]
+  float2* wpart;      // [ceil(nh / PT_U)][Ns] unit-block partials of w (plain form)
   double* wmean;      // [2] (+ pad)
   void* partial;      // [nsplit][P] of T
   void* x; void* r; void* p; void* Ap; void* b;   // [P] of V each
@@ -770,7 +807,7 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   const size_t ts = (dtype == QES_DTYPE_C64) ? sizeof(float2) : sizeof(float);
   const size_t vs = (dtype == QES_DTYPE_C64) ? sizeof(double2) : sizeof(double);
-  const int64_t nsplit_simt = (n_samples + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES;
+  const int64_t nsplit_simt = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
   SRWork L;
   L.td = TcDims{};
   const bool tc_ok = tc_plan(dtype, ns, nh, n_samples, &L.td);
@@ -781,6 +818,7 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   size_t off = 0;
   auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off += align256(bytes); return p; };
   L.w = (float2*)take((size_t)n_samples * sizeof(float2));
+  L.wpart = (float2*)take((size_t)((nh + PT_U - 1) / PT_U) * n_samples * sizeof(float2));
   L.wmean = (double*)take(4 * sizeof(double));
   L.partial = take((size_t)std::max<int64_t>(nsplit_max, 1) * P * ts);
   L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
@@ -799,20 +837,36 @@ extern "C" int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_sampl
   return QES_OK;
 }
 
+// split partials of O^H ((w - mean(w)) * scale) on the CUDA cores (register tiles)
+template <class T>
+static int launch_ohu_plain(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
+                            const double* wmean, double scale, T* partial, cudaStream_t st,
+                            const double* cg_done = nullptr) {
+  const int64_t nsplit = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
+  QES_ARG_CHECK(nsplit <= 65535, "SR: too many samples");
+  const int R = pt_rows_ohu(ns);
+  dim3 grid((nh + 1 + PT_U - 1) / PT_U, (ns + 1 + PT_TY * R - 1) / (PT_TY * R), (unsigned)nsplit);
+  const int pf = qes_prof_begin(QES_PROF_OHU, st);
+  if (R == 8)
+    ohu_tile_kernel<T, 8><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, partial,
+                                                              cg_done);
+  else
+    ohu_tile_kernel<T, 4><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, partial,
+                                                              cg_done);
+  QES_LAUNCH_CHECK();
+  qes_prof_end(pf, st);
+  return QES_OK;
+}
+
 // g = O^H ((w - mean(w)) * scale)   [+ shift * p, dot partials]   into y
 template <class T, class V>
 static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
                      const double* wmean, double scale, const SRWork& L, double shift, const V* p, V* y,
                      double* dot_part, cudaStream_t st, const double* cg_done = nullptr) {
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-  const int64_t nsplit = (n_samples + OHU_SPLIT_SAMPLES - 1) / OHU_SPLIT_SAMPLES;
-  QES_ARG_CHECK(nsplit <= 65535, "SR: too many samples");
-  dim3 grid((nh + OHU_TM - 1) / OHU_TM, (ns + OHU_TI - 1) / OHU_TI, (unsigned)nsplit);
-  dim3 block(OHU_TM, OHU_TY);
-  const int pf = qes_prof_begin(QES_PROF_OHU, st);
-  ohu_kernel<T><<<grid, block, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial, cg_done);
-  QES_LAUNCH_CHECK();
-  qes_prof_end(pf, st);
+  const int64_t nsplit = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
+  if (int rc = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial, st, cg_done))
+    return rc;
   const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
   if (int rc_ = launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
       dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
@@ -821,18 +875,23 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
   return QES_OK;
 }
 
+// w = O v on the CUDA cores (register tiles; unit-block partials summed in a fixed order), and
+// its float64 mean when wmean is given
 template <class T, class V>
 static int apply_ov(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const V* v, float2* w,
-                    double* wmean, cudaStream_t st, const double* cg_done = nullptr) {
-  const int nw = n_words(ns);
-  const size_t sm = (size_t)OV_SB * nw * sizeof(uint32_t);
-  QES_ARG_CHECK(sm <= 48 * 1024, "SR: ns too large");
+                    double* wmean, const SRWork& L, cudaStream_t st, const double* cg_done = nullptr) {
+  const int nub = (nh + PT_U - 1) / PT_U;
+  const int R = pt_rows_ov(n_samples);
+  dim3 grid((unsigned)((n_samples + PT_TY * R - 1) / (PT_TY * R)), (unsigned)nub);
+  QES_ARG_CHECK(nub <= 65535, "SR: nh too large");
   const int pf = qes_prof_begin(QES_PROF_OV, st);
-  ov_kernel<T, V><<<(unsigned)((n_samples + OV_SB - 1) / OV_SB), OV_THREADS, sm, st>>>(ns, nh, n_samples, bits, tt,
-                                                                                     v, w, cg_done);
+  if (R == 8)
+    ov_tile_kernel<T, V, 8><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, v, L.wpart, cg_done);
+  else
+    ov_tile_kernel<T, V, 4><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, v, L.wpart, cg_done);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
-  mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, w, wmean);
+  wsum_kernel<<<1, 1024, 0, st>>>(n_samples, nub, L.wpart, w, wmean, cg_done);
   QES_LAUNCH_CHECK();
   return QES_OK;
 }
@@ -932,7 +991,7 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
     qes_prof_end(pfr, st);
     return QES_OK;
   }
-  int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, st, cg_done);
+  int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, L, st, cg_done);
   if (rc) return rc;
   return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples, L, shift, v, y,
                          dot_part, st, cg_done);
@@ -1192,14 +1251,11 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
                              L.scal + 4);
           if (r2) return r2;
         } else {
-          int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, st, L.scal + 4);
+          int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, L, st, L.scal + 4);
           if (r2) return r2;
-          dim3 grid((nh + OHU_TM - 1) / OHU_TM, (ns + OHU_TI - 1) / OHU_TI, (unsigned)L.nsplit);
-          const int pf = qes_prof_begin(QES_PROF_OHU, st);
-          ohu_kernel<T><<<grid, dim3(OHU_TM, OHU_TY), 0, st>>>(ns, nh, n_samples, bits, tt, L.w, L.wmean,
-                                                             1.0 / (double)n_samples, (T*)L.partial, L.scal + 4);
-          QES_LAUNCH_CHECK();
-          qes_prof_end(pf, st);
+          r2 = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples,
+                                   (T*)L.partial, st, L.scal + 4);
+          if (r2) return r2;
         }
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(fused_grid);
@@ -1628,10 +1684,7 @@ static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* 
       if (L.tc) {                                                                     // w = O g
         if ((rc = tc_ov(dtype, L.td, n, bits, g, L.w, L.tw, st))) return rc;
       } else {
-        const int nw = n_words(ns);
-        ov_kernel<T, V><<<(unsigned)((n + OV_SB - 1) / OV_SB), OV_THREADS, (size_t)OV_SB * nw * sizeof(uint32_t), st>>>(
-            ns, nh, n, bits, tt, g, L.w, nullptr);
-        QES_LAUNCH_CHECK();
+        if ((rc = apply_ov<T, V>(ns, nh, n, bits, tt, g, L.w, nullptr, L, st))) return rc;
       }
       mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n, L.w, L.wmean);
       minsr_ap_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(n, L.w, L.wmean, opt->shift, p, Ap, L.parts, L.scal,

@@ -49,8 +49,9 @@ def rel_err(a, b):
 
 # A float32 Delta log psi (with the sampler's hardware-approximation tanh cache) can decide a
 # Metropolis step the other way only where the float64 oracle's |log u - log_acc| is within its
-# rounding; chains whose decisions all kept a larger margin must follow the oracle exactly.
-TIE = 1e-3
+# rounding; chains whose decisions all kept a larger margin must follow the oracle exactly.  The
+# bound covers a few hundred float32 ratio factors (relative error ~1e-7 each) in Delta.
+TIE = 1e-4
 
 
 def assert_same_trajectories(got, cfg, ref, n_chains, accepted=None):
@@ -60,9 +61,11 @@ def assert_same_trajectories(got, cfg, ref, n_chains, accepted=None):
     tie = ref.min_margin <= TIE
     chain_of_row = np.arange(got.shape[0]) % n_chains
     strict = ~tie[chain_of_row]
-    bad = np.flatnonzero(strict & np.any(got != cfg, axis=1))
+    mism = np.any(got != cfg, axis=1)
+    bad = np.flatnonzero(strict & mism)
     assert bad.size == 0, (bad[:10], ref.min_margin[chain_of_row[bad[:10]]])
-    assert np.mean(tie) <= 0.05, np.mean(tie)
+    # near-tie chains (each decision has a ~TIE chance of one): a minority, most of them still exact
+    assert np.mean(tie) <= 0.15, np.mean(tie)
     if accepted is not None:
         assert np.array_equal(accepted[~tie], ref.accepted[~tie])
     return strict

@@ -148,9 +148,9 @@ def test_nqs_sample_and_step_through_public_api(mu):
     cfg_ref, lp_ref, probs_ref = ref.sample(p, S)
     got = cfg.cpu().numpy()
     assert got.shape == (C * S, 16) and set(np.unique(got)) <= {-0.5, 0.5}
-    tie = ref.min_margin <= 1e-3
+    tie = ref.min_margin <= 1e-4
     strict = ~tie[np.arange(C * S) % C]
-    assert np.mean(tie) <= 0.05
+    assert np.mean(tie) <= 0.15
     assert np.array_equal(got[strict], cfg_ref[strict] * 0.5)
     # log psi of the returned rows is log psi of those configurations
     lp_of_rows = orbm.log_psi(p, orbm.to_sigma(got))

@@ -283,10 +283,15 @@ typedef struct {
 
 typedef struct {
     int iterations;
-    int converged;
-    double residual;
+    int converged;             /* SciPy's rule met by CG's recursive residual */
+    double residual;           /* recursive residual norm at exit */
     double rhs_norm;
     double e_mean_re, e_mean_im;
+    double true_residual;      /* ||F - (S + shift) x|| / ||F|| recomputed with one more
+                                  matvec after the solve (-1: not computed).  With float32
+                                  or BF16-split contractions it levels off near their
+                                  rounding (~1e-6-1e-5) while the recursive residual keeps
+                                  falling; no counterpart in the reference (float64 SR). */
 } qes_sr_result;
 
 int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
@@ -372,6 +377,26 @@ int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples,
                     const uint32_t* bits, const void* tanh_theta, const void* eloc,
                     const qes_sr_options* opt, void* x_out, qes_sr_result* result,
                     void* workspace, size_t workspace_bytes, void* stream);
+/* The same three with per-sample weights `probs` (float32, normalised to sum
+ * Ns, as VMCSampler returns them when 1/logprob_fact != mu beta;
+ * QES/Solver/MonteCarlo/vmc.py:1173-1184): means are weighted,
+ * <X> = sum_s p_s X_s / Ns, and every sample sum carries p_s:
+ *   F = O^H (p (E - <E>)) / Ns,  S v = O^H (p (O v - <O v>)) / Ns,
+ * which is O_c^H diag(p) O_c / Ns with O_c centred by the weighted mean.
+ * The weighting of the SR sums is this library's reading of the reference
+ * (its SR module is not in the snapshot; its sampler produces the weights
+ * and its estimator takes them).  probs = NULL is the unweighted call.      */
+int qes_sr_force_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                          const void* tanh_theta, const void* eloc, const float* probs,
+                          void* force_out, void* workspace, size_t workspace_bytes, void* stream);
+int qes_sr_matvec_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                           const void* tanh_theta, const float* probs, double shift, const void* v,
+                           void* y_out, void* workspace, size_t workspace_bytes, void* stream);
+int qes_sr_solve_cg_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                             const void* tanh_theta, const void* eloc, const float* probs,
+                             const qes_sr_options* opt, const void* x0, void* x_out,
+                             qes_sr_result* result, void* workspace, size_t workspace_bytes,
+                             void* stream);
 /* As qes_sr_solve_cg with an initial guess x0 (device, P float64 / complex128)
  * of the unscaled system (S + shift) x = F, i.e. a previous x_out divided by
  * rhs_prefactor; r0 = F - (S + shift) x0 costs one extra matvec and the stop

@@ -80,7 +80,7 @@ class SROptions(C.Structure):
 class SRResult(C.Structure):
     _fields_ = [
         ("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double), ("rhs_norm", C.c_double),
-        ("e_mean_re", C.c_double), ("e_mean_im", C.c_double),
+        ("e_mean_re", C.c_double), ("e_mean_im", C.c_double), ("true_residual", C.c_double),
     ]
 
 
@@ -132,6 +132,11 @@ SIGNATURES = {
                         C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_sr_solve_cg_x0": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp, _vp,
                            C.POINTER(SRResult), _vp, _sz, _vp],
+    "qes_sr_force_weighted": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
+    "qes_sr_matvec_weighted": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.c_double, _vp, _vp, _vp, _sz,
+                               _vp],
+    "qes_sr_solve_cg_weighted": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
+                                 _vp, C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_sr_minsr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
     "qes_sr_solve_minsr": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
                            C.POINTER(SRResult), _vp, _sz, _vp],

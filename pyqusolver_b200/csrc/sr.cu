@@ -71,9 +71,14 @@ QES_D float2 from_c(float2 v, float2) { return v; }
 // ----------------------------------------------------------------------------
 constexpr int MEAN_THREADS = 1024;
 __global__ void __launch_bounds__(MEAN_THREADS) mean_c_kernel(int64_t n, const float2* __restrict__ w,
-                                                              double* __restrict__ out) {
+                                                              double* __restrict__ out,
+                                                              const float* __restrict__ wts = nullptr) {
   double sr = 0, si = 0;
-  for (int64_t k = threadIdx.x; k < n; k += blockDim.x) { sr += w[k].x; si += w[k].y; }
+  for (int64_t k = threadIdx.x; k < n; k += blockDim.x) {
+    const double f = wts ? (double)wts[k] : 1.0;           // sum wts w / Ns: the weighted mean
+    sr += f * w[k].x;
+    si += f * w[k].y;
+  }
   __shared__ double rr[MEAN_THREADS / 32], ri[MEAN_THREADS / 32];
   sr = warp_sum(sr); si = warp_sum(si);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -178,18 +183,21 @@ __global__ void __launch_bounds__(PT_THREADS) ov_tile_kernel(int ns, int nh, int
   }
 }
 
-// w = sum of the unit-block partials (fixed order); mean of w in float64 when wmean is given
+// w = sum of the unit-block partials (fixed order); mean of w in float64 (weighted by wts, which sum
+// to Ns, when given) when wmean is given
 __global__ void __launch_bounds__(1024) wsum_kernel(int64_t n, int nub, const float2* __restrict__ wpart,
                                                      float2* __restrict__ w, double* __restrict__ wmean,
-                                                     const double* __restrict__ cg_done) {
+                                                     const double* __restrict__ cg_done,
+                                                     const float* __restrict__ wts) {
   if (cg_done && *cg_done != 0.0) return;
   double sr = 0, si = 0;
   for (int64_t k = threadIdx.x; k < n; k += blockDim.x) {
     float2 a = wpart[k];
     for (int b = 1; b < nub; ++b) a = a + wpart[(int64_t)b * n + k];
     w[k] = a;
-    sr += a.x;
-    si += a.y;
+    const double f = wts ? (double)wts[k] : 1.0;
+    sr += f * a.x;
+    si += f * a.y;
   }
   if (!wmean) return;
   __shared__ double rr[32], ri[32];
@@ -208,7 +216,8 @@ __global__ void __launch_bounds__(1024) wsum_kernel(int64_t n, int nub, const fl
 
 // partial[split] = Sigma~^T Q~ over PT_SPLIT samples: rows are the sites plus a ones row at site
 // ns (-> g_b), columns the hidden units plus a virtual unit at nh carrying u itself (-> g_a);
-// Q_sj = conj(t_sj) u_s with u_s = (w_s - mean) * scale, staged 32 samples at a time.
+// Q_sj = conj(t_sj) u_s with u_s = wts_s (w_s - mean) * scale (wts_s = 1 without weights), staged
+// 32 samples at a time.
 template <class T, int R>
 __global__ void __launch_bounds__(PT_THREADS) ohu_tile_kernel(int ns, int nh, int64_t n_samples,
                                                               const uint32_t* __restrict__ bits,
@@ -216,7 +225,8 @@ __global__ void __launch_bounds__(PT_THREADS) ohu_tile_kernel(int ns, int nh, in
                                                               const float2* __restrict__ w,
                                                               const double* __restrict__ wmean, double scale,
                                                               T* __restrict__ partial,
-                                                              const double* __restrict__ cg_done) {
+                                                              const double* __restrict__ cg_done,
+                                                              const float* __restrict__ wts) {
   constexpr int IB = PT_TY * R;                  // sites per block
   __shared__ float sg[PT_K][IB];
   __shared__ T qs[PT_K][PT_U];
@@ -241,7 +251,8 @@ __global__ void __launch_bounds__(PT_THREADS) ohu_tile_kernel(int ns, int nh, in
       T u = ScalarTraits<T>::zero();
       if (tid < nc) {
         const float2 wv = w[c0 + tid];
-        u = from_c(make_float2((wv.x - mr) * fs, (wv.y - mi) * fs), T());
+        const float f = wts ? fs * wts[c0 + tid] : fs;
+        u = from_c(make_float2((wv.x - mr) * f, (wv.y - mi) * f), T());
       }
       us[tid] = u;
     }
@@ -609,6 +620,31 @@ __global__ void __launch_bounds__(RED_THREADS) norm2_kernel(int64_t P, const V* 
   }
 }
 
+// ||b - y||^2: per-block partial sums, then one block adds them into *out
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) diff_norm2_kernel(int64_t P, const V* __restrict__ b,
+                                                                 const V* __restrict__ y, double* __restrict__ part) {
+  double d = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V e = vadd(b[k], vscale(-1.0, y[k]));
+    d += vdotc(e, e);
+  }
+  __shared__ double red[RED_THREADS / 32];
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) t += red[q];
+    part[blockIdx.x] = t;
+  }
+}
+__global__ void __launch_bounds__(SC_THREADS) sum_parts_kernel(int n, const double* __restrict__ parts,
+                                                               double* __restrict__ out) {
+  const double t = block_sum_parts(n, parts);
+  if (threadIdx.x == 0) *out = t;
+}
+
 template <class V>
 __global__ void scale_vec_kernel(int64_t P, double s, V* __restrict__ x) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x)
@@ -788,6 +824,7 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
 struct SRWork {
   float2* w;          // [Ns]
   float2* wpart;      // [ceil(nh / PT_U)][Ns] unit-block partials of w (plain form)
+  const float* wts;   // per-sample weights normalised to sum Ns, or nullptr (uniform); set per call
   double* wmean;      // [2] (+ pad)
   void* partial;      // [nsplit][P] of T
   void* x; void* r; void* p; void* Ap; void* b;   // [P] of V each
@@ -827,6 +864,7 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   L.counter = (unsigned int*)take(128 * sizeof(unsigned int));     // tickets, barrier words (own lines)
   char* tcb = tc_ok ? take(tc_workspace_bytes(L.td)) : nullptr;
   L.tw = (tc_ok && base) ? tc_layout(L.td, tcb) : TcWork{};
+  L.wts = nullptr;
   L.total = off;
   return L;
 }
@@ -841,7 +879,7 @@ extern "C" int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_sampl
 template <class T>
 static int launch_ohu_plain(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
                             const double* wmean, double scale, T* partial, cudaStream_t st,
-                            const double* cg_done = nullptr) {
+                            const double* cg_done = nullptr, const float* wts = nullptr) {
   const int64_t nsplit = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
   QES_ARG_CHECK(nsplit <= 65535, "SR: too many samples");
   const int R = pt_rows_ohu(ns);
@@ -849,10 +887,10 @@ static int launch_ohu_plain(int ns, int nh, int64_t n_samples, const uint32_t* b
   const int pf = qes_prof_begin(QES_PROF_OHU, st);
   if (R == 8)
     ohu_tile_kernel<T, 8><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, partial,
-                                                              cg_done);
+                                                              cg_done, wts);
   else
     ohu_tile_kernel<T, 4><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, partial,
-                                                              cg_done);
+                                                              cg_done, wts);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;
@@ -865,7 +903,8 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
                      double* dot_part, cudaStream_t st, const double* cg_done = nullptr) {
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   const int64_t nsplit = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
-  if (int rc = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial, st, cg_done))
+  if (int rc = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial, st, cg_done,
+                                   L.wts))
     return rc;
   const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
   if (int rc_ = launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
@@ -891,7 +930,7 @@ static int apply_ov(int ns, int nh, int64_t n_samples, const uint32_t* bits, con
     ov_tile_kernel<T, V, 4><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, v, L.wpart, cg_done);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
-  wsum_kernel<<<1, 1024, 0, st>>>(n_samples, nub, L.wpart, w, wmean, cg_done);
+  wsum_kernel<<<1, 1024, 0, st>>>(n_samples, nub, L.wpart, w, wmean, cg_done, L.wts);
   QES_LAUNCH_CHECK();
   return QES_OK;
 }
@@ -900,7 +939,7 @@ template <class T>
 static int sr_force_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* eloc,
                       typename VecT<T>::type* F, const SRWork& L, cudaStream_t st) {
   using V = typename VecT<T>::type;
-  mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, eloc, L.wmean);
+  mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n_samples, eloc, L.wmean, L.wts);
   QES_LAUNCH_CHECK();
   if (L.tc) {
     const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
@@ -953,14 +992,15 @@ static int sr_prepare(int dtype, int64_t n_samples, const uint32_t* bits, const 
                       cudaStream_t st);
 static int sr_check_status(const SRWork& L, cudaStream_t st, bool cg_words = false);
 
-extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
-                            const void* tanh_theta, const void* eloc, void* force_out, void* workspace,
-                            size_t workspace_bytes, void* stream) {
+extern "C" int qes_sr_force_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                     const void* tanh_theta, const void* eloc, const float* probs, void* force_out,
+                                     void* workspace, size_t workspace_bytes, void* stream) {
   QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && eloc && force_out, "qes_sr_force: bad args");
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_force: bad dtype");
   SRWork L;
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
+  L.wts = L.tw.wts = probs;
   cudaStream_t st = (cudaStream_t)stream;
   rc = sr_prepare(dtype, n_samples, bits, tanh_theta, L, st);
   if (rc) return rc;
@@ -972,6 +1012,13 @@ extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const 
                             (double2*)force_out, L, st);
   if (rc) return rc;
   return sr_check_status(L, st);
+}
+
+extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                            const void* tanh_theta, const void* eloc, void* force_out, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  return qes_sr_force_weighted(dtype, ns, nh, n_samples, bits, tanh_theta, eloc, nullptr, force_out, workspace,
+                               workspace_bytes, stream);
 }
 
 template <class T>
@@ -1022,14 +1069,15 @@ static int sr_check_status(const SRWork& L, cudaStream_t st, bool cg_words) {
   return QES_OK;
 }
 
-extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
-                             const void* tanh_theta, double shift, const void* v, void* y_out, void* workspace,
-                             size_t workspace_bytes, void* stream) {
+extern "C" int qes_sr_matvec_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                      const void* tanh_theta, const float* probs, double shift, const void* v,
+                                      void* y_out, void* workspace, size_t workspace_bytes, void* stream) {
   QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && v && y_out, "qes_sr_matvec: bad args");
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_matvec: bad dtype");
   SRWork L;
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
+  L.wts = L.tw.wts = probs;
   cudaStream_t st = (cudaStream_t)stream;
   rc = sr_prepare(dtype, n_samples, bits, tanh_theta, L, st);
   if (rc) return rc;
@@ -1043,6 +1091,13 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
   return sr_check_status(L, st);
 }
 
+extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                             const void* tanh_theta, double shift, const void* v, void* y_out, void* workspace,
+                             size_t workspace_bytes, void* stream) {
+  return qes_sr_matvec_weighted(dtype, ns, nh, n_samples, bits, tanh_theta, nullptr, shift, v, y_out, workspace,
+                                workspace_bytes, stream);
+}
+
 // ----------------------------------------------------------------------------
 // CUDA graph of one chunk of CG iterations (matvec + x/r update + direction
 // update, `check_every` times), captured on a private stream and replayed
@@ -1053,13 +1108,13 @@ extern "C" int qes_sr_matvec(int dtype, int ns, int nh, int64_t n_samples, const
 
 namespace {
 struct CgGraphKey {
-  const void* bits; const void* tt; const void* ws; int64_t n; int ns, nh, dtype, chunk, tc, l2;
+  const void* bits; const void* tt; const void* ws; const void* wts; int64_t n; int ns, nh, dtype, chunk, tc, l2;
   int big, kc, nsplit, nnc, nc, spc, cl;  // tiling of the captured kernels
   int bartest;                             // grid-barrier test hook armed (also keeps the struct free of padding)
   double shift;
   bool operator==(const CgGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
 };
-static_assert(sizeof(CgGraphKey) == 3 * sizeof(void*) + 8 + 14 * 4 + 8, "CgGraphKey has padding bytes (memcmp key)");
+static_assert(sizeof(CgGraphKey) == 4 * sizeof(void*) + 8 + 14 * 4 + 8, "CgGraphKey has padding bytes (memcmp key)");
 struct CgGraphSlot {
   bool init = false;
   cudaStream_t cs = nullptr;
@@ -1254,7 +1309,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
           int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, L, st, L.scal + 4);
           if (r2) return r2;
           r2 = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples,
-                                   (T*)L.partial, st, L.scal + 4);
+                                   (T*)L.partial, st, L.scal + 4, L.wts);
           if (r2) return r2;
         }
         cudaLaunchConfig_t lc = {};
@@ -1322,7 +1377,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         gs.init = true;
         if (l2) l2_window(gs.cs, dev, L.tw.t_rows, l2_bytes);
       }
-      const CgGraphKey key{bits, tt, L.w, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
+      const CgGraphKey key{bits, tt, L.w, L.wts, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
                            L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0), L.td.big ? 1 : 0, L.td.KC, L.nsplit,
                            L.td.nnc, L.td.NC, L.td.SPC, L.td.cl, (int)bcfg.extra, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
@@ -1472,6 +1527,18 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   }
   // a bounded wait of the force pass must surface even when CG needed no iteration
   if ((rc = sr_check_status(L, st, true))) return rc;
+  // true residual of the solution, ||F - (S + shift) x|| / ||F||, with one more matvec: CG's recursive
+  // residual drifts from it once the rounding of the float32 / BF16-split contractions dominates
+  double true_rr = -1.0;
+  if (opt->maxiter > 0) {
+    rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, x, Ap, nullptr, L, st, false);
+    if (rc) return rc;
+    diff_norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, Ap, L.parts);
+    sum_parts_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, L.scal + 10);
+    QES_LAUNCH_CHECK_N(2);
+    QES_CUDA_CHECK(cudaMemcpyAsync(&true_rr, L.scal + 10, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if ((rc = sr_check_status(L, st))) return rc;        // synchronises the stream
+  }
   // x_out = rhs_prefactor * x
   QES_CUDA_CHECK(cudaMemcpyAsync(x_out, x, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
   if (opt->rhs_prefactor != 1.0) {
@@ -1485,14 +1552,16 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     res->rhs_norm = sqrt(hs[6]);
     res->e_mean_re = emean[0];
     res->e_mean_im = emean[1];
+    res->true_residual = true_rr < 0.0 ? -1.0 : (hs[6] > 0.0 ? sqrt(true_rr / hs[6]) : 0.0);
   }
   return done ? QES_OK : QES_ERR_NOT_CONVERGED;
 }
 
-extern "C" int qes_sr_solve_cg_x0(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
-                                  const void* tanh_theta, const void* eloc, const qes_sr_options* opt,
-                                  const void* x0, void* x_out, qes_sr_result* result, void* workspace,
-                                  size_t workspace_bytes, void* stream) {
+extern "C" int qes_sr_solve_cg_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                        const void* tanh_theta, const void* eloc, const float* probs,
+                                        const qes_sr_options* opt, const void* x0, void* x_out,
+                                        qes_sr_result* result, void* workspace, size_t workspace_bytes,
+                                        void* stream) {
   QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && eloc && opt && x_out,
                 "qes_sr_solve_cg: bad args");
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_solve_cg: bad dtype");
@@ -1500,12 +1569,21 @@ extern "C" int qes_sr_solve_cg_x0(int dtype, int ns, int nh, int64_t n_samples, 
   SRWork L;
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
+  L.wts = L.tw.wts = probs;
   cudaStream_t st = (cudaStream_t)stream;
   if (dtype == QES_DTYPE_F32)
     return sr_cg_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc, opt,
                           (double*)x_out, result, L, st, (const double*)x0);
   return sr_cg_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc, opt,
                          (double2*)x_out, result, L, st, (const double2*)x0);
+}
+
+extern "C" int qes_sr_solve_cg_x0(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                  const void* tanh_theta, const void* eloc, const qes_sr_options* opt,
+                                  const void* x0, void* x_out, qes_sr_result* result, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  return qes_sr_solve_cg_weighted(dtype, ns, nh, n_samples, bits, tanh_theta, eloc, nullptr, opt, x0, x_out, result,
+                                  workspace, workspace_bytes, stream);
 }
 
 extern "C" int qes_sr_solve_cg(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
@@ -1712,6 +1790,7 @@ static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* 
     res->rhs_norm = sqrt(hs[6]);
     res->e_mean_re = emean[0];
     res->e_mean_im = emean[1];
+    res->true_residual = -1.0;                          // not computed for the sample-space solve
   }
   return done ? QES_OK : QES_ERR_NOT_CONVERGED;
 }

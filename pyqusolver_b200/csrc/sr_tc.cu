@@ -258,7 +258,8 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
                                                          const V* __restrict__ v, const uint16_t* __restrict__ t_rows,
                                                          const uint16_t* __restrict__ vp, float2* __restrict__ w_out,
                                                          double2* __restrict__ wsum_part, int* __restrict__ status,
-                                                         const double* __restrict__ cg_done) {
+                                                         const double* __restrict__ cg_done,
+                                                         const float* __restrict__ wts) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   const int ns = d.ns, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
@@ -426,7 +427,8 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
     for (int g = 1; g < kColGroups; ++g) wv = wv + s_part[g][row];
     if (!sval) wv = make_float2(0.f, 0.f);
     if (sval) w_out[s] = wv;
-    double2 ps = make_double2(wv.x, wv.y);
+    const double wt = (wts && sval) ? (double)wts[s] : 1.0;          // weighted sum for the weighted mean
+    double2 ps = make_double2(wt * wv.x, wt * wv.y);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       ps.x += __shfl_xor_sync(0xffffffffu, ps.x, o);
@@ -454,7 +456,8 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
                                                           const double2* __restrict__ wsum_part, int wsum_n,
                                                           double scale, const uint16_t* __restrict__ sig_cols,
                                                           const uint16_t* __restrict__ t_cols, T* __restrict__ partial,
-                                                          int* __restrict__ status, const double* __restrict__ cg_done) {
+                                                          int* __restrict__ status, const double* __restrict__ cg_done,
+                                                          const float* __restrict__ wts) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   const int ns = d.ns, nh = d.nh, Mp = d.Mp, Np = d.Np, KC = d.KC;
@@ -536,8 +539,9 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     T u = ScalarTraits<T>::zero();
     if (s < n_samples) {
       const float2 wv = w[s];
-      if constexpr (CPLX) u = make_float2((wv.x - mr) * fs, (wv.y - mi) * fs);
-      else u = (wv.x - mr) * fs;
+      const float f = wts ? fs * wts[s] : fs;
+      if constexpr (CPLX) u = make_float2((wv.x - mr) * f, (wv.y - mi) * f);
+      else u = (wv.x - mr) * f;
     }
     s_u[k] = u;
   }
@@ -834,7 +838,8 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_big_kernel(TcDims d, int64_t 
                                                               double scale, const uint16_t* __restrict__ sig_cols,
                                                               const uint16_t* __restrict__ t_cols,
                                                               T* __restrict__ partial, int* __restrict__ status,
-                                                              const double* __restrict__ cg_done) {
+                                                              const double* __restrict__ cg_done,
+                                                              const float* __restrict__ wts) {
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   constexpr int H = CPLX ? 2 : 1;
@@ -925,8 +930,9 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_big_kernel(TcDims d, int64_t 
       T u = ScalarTraits<T>::zero();
       if (s < n_samples) {
         const float2 wv = w[s];
-        if constexpr (CPLX) u = make_float2((wv.x - mr) * fs, (wv.y - mi) * fs);
-        else u = (wv.x - mr) * fs;
+        const float f = wts ? fs * wts[s] : fs;
+        if constexpr (CPLX) u = make_float2((wv.x - mr) * f, (wv.y - mi) * f);
+        else u = (wv.x - mr) * f;
       }
       u_b[k] = u;
     }
@@ -1237,11 +1243,11 @@ static int launch_tc_ohu(const TcDims& d, int64_t n_samples, const float2* g, co
     cfg.numAttrs = qes_pdl_on() ? 2 : 1;
     QES_CUDA_CHECK(cudaLaunchKernelEx(&cfg, tc_ohu_kernel<T, 2>, d, n_samples, g, gsum_part, gsum_n, scale,
                                       (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status,
-                                      cg_done));
+                                      cg_done, w.wts));
   } else {
     QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_kernel<T, 1>, dim3(d.n_chunks), dim3(kThreads), (size_t)d.ohu_smem, st, d,
                                   n_samples, g, gsum_part, gsum_n, scale, (const uint16_t*)w.sig_cols,
-                                  (const uint16_t*)w.t_cols, partial, w.status, cg_done));
+                                  (const uint16_t*)w.t_cols, partial, w.status, cg_done, w.wts));
   }
   return QES_OK;
 }
@@ -1286,7 +1292,7 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
   int pf = qes_prof_begin(QES_PROF_OV, st);
   QES_CUDA_CHECK(qes_launch_pdl(tc_ov_kernel<T, V>, dim3(d.n_tiles), dim3(kThreads), (size_t)d.ov_smem, st, d,
                                 n_samples, bits, v, (const uint16_t*)w.t_rows, (const uint16_t*)w.vp, w_out, w.wsum,
-                                w.status, cg_done));
+                                w.status, cg_done, w.wts));
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   pf = qes_prof_begin(QES_PROF_OHU, st);
@@ -1295,7 +1301,7 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
     QES_CUDA_CHECK(qes_launch_pdl(tc_ohu_big_kernel<T>, dim3(d.nnc, d.nsplit), dim3(kThreads), (size_t)d.ohu_smem, st,
                                   d, n_samples, (const float2*)w_out, (const double2*)w.wsum, d.n_tiles, inv_n,
                                   (const uint16_t*)w.sig_cols, (const uint16_t*)w.t_cols, partial, w.status,
-                                  cg_done));
+                                  cg_done, w.wts));
   else if (int rc = launch_tc_ohu<T>(d, n_samples, w_out, w.wsum, d.n_tiles, inv_n, w, partial, st, cg_done))
     return rc;
   QES_LAUNCH_CHECK();
@@ -1312,7 +1318,7 @@ static int tc_ov_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, con
   QES_LAUNCH_CHECK();
   const int pf = qes_prof_begin(QES_PROF_OV, st);
   tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
-                                                           w.status, nullptr);
+                                                           w.status, nullptr, w.wts);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;
@@ -1338,10 +1344,10 @@ int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const
   if (d.big) {
     if (dtype == QES_DTYPE_C64)
       tc_ohu_big_kernel<float2><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
-          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float2*)partial, w.status, nullptr);
+          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float2*)partial, w.status, nullptr, w.wts);
     else
       tc_ohu_big_kernel<float><<<dim3(d.nnc, d.nsplit), kThreads, d.ohu_smem, st>>>(
-          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float*)partial, w.status, nullptr);
+          d, n_samples, g, gsum_part, gsum_n, scale, w.sig_cols, w.t_cols, (float*)partial, w.status, nullptr, w.wts);
   } else if (dtype == QES_DTYPE_C64) {
     if (int rc = launch_tc_ohu<float2>(d, n_samples, g, gsum_part, gsum_n, scale, w, (float2*)partial, st)) return rc;
   } else {

@@ -34,8 +34,9 @@ struct TcWork {
   uint16_t* t_cols;     // ohu B before scaling: per sample chunk, hi/lo BF16 tiles of T^T
   uint16_t* sig_cols;   // ohu A: per sample chunk, Sigma^T (128 x KC) BF16
   uint16_t* vp;         // ov B: V' hi/lo BF16 tiles (per CG iteration)
-  double2* wsum;        // n_tiles partial sums of w = O v
+  double2* wsum;        // n_tiles partial sums of w = O v (weighted by wts when given)
   int* status;          // first error code of a bounded wait
+  const float* wts;     // per-sample weights normalised to sum Ns (nullptr: uniform); set per call
 };
 
 constexpr size_t kTcSmemLimit = 220 * 1024;
@@ -46,15 +47,15 @@ TcWork tc_layout(const TcDims& d, char* base);
 // once per VMC step: BF16 tiles of T, T^T and Sigma^T
 int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
                     const TcWork& w, cudaStream_t st);
-// w_out = O v, partial[chunk] = O^H ((w - mean w) / Ns); cg_done (optional): a CG solve's converged
-// flag, on which the kernels skip their work
+// w_out = O v, partial[chunk] = O^H (wts (w - mean w) / Ns) with mean w = sum wts w / Ns (wts = 1 when
+// w.wts is null); cg_done (optional): a CG solve's converged flag, on which the kernels skip their work
 int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
               void* partial, const TcWork& w, cudaStream_t st, bool build_vp = true,
               const double* cg_done = nullptr);
 // w_out = O v only (builds the V' operand from v first)
 int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
           const TcWork& w, cudaStream_t st);
-// partial[chunk] = O^H ((g - mean) * scale): gsum_n > 0 -> gsum_part holds gsum_n partial sums
+// partial[chunk] = O^H (wts (g - mean) * scale): gsum_n > 0 -> gsum_part holds gsum_n partial sums
 // (mean = sum / Ns); gsum_n < 0 -> gsum_part[0] is the mean; gsum_part == nullptr -> no centring
 int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
            double scale, void* partial, const TcWork& w, cudaStream_t st);

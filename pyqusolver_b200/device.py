@@ -232,31 +232,44 @@ def sr_workspace(dtype_c, ns, nh, n, device):
     return torch.empty((int(nb.value),), dtype=torch.uint8, device=device)
 
 
-def sr_force(flat_params, ns, nh, bits, tanh_theta, eloc, workspace=None):
+def sample_weights(probs, n, device):
+    """float32 device weights normalised to sum n (the reference's probs), or None for uniform sampling."""
+    if probs is None:
+        return None
+    p = torch.as_tensor(probs, device=device).reshape(-1).to(torch.float64)
+    if p.numel() != n:
+        raise ValueError(f"probs has {p.numel()} entries for {n} samples")
+    return (p * (n / p.sum())).to(torch.float32).contiguous()
+
+
+def sr_force(flat_params, ns, nh, bits, tanh_theta, eloc, workspace=None, probs=None):
     dc = dtype_code(flat_params)
     n = int(bits.shape[0])
     ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
     F = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
-    call("qes_sr_force", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), ptr(F), ptr(ws), int(ws.numel()),
-         stream_ptr())
+    w = sample_weights(probs, n, bits.device)
+    call("qes_sr_force_weighted", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), ptr(w), ptr(F), ptr(ws),
+         int(ws.numel()), stream_ptr())
     return F
 
 
-def sr_matvec(flat_params, ns, nh, bits, tanh_theta, v, shift=0.0, workspace=None):
+def sr_matvec(flat_params, ns, nh, bits, tanh_theta, v, shift=0.0, workspace=None, probs=None):
     dc = dtype_code(flat_params)
     n = int(bits.shape[0])
     ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
     v = v.to(vec_dtype(flat_params.dtype)).contiguous()
     y = torch.empty_like(v)
-    call("qes_sr_matvec", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), float(shift), ptr(v), ptr(y), ptr(ws),
-         int(ws.numel()), stream_ptr())
+    w = sample_weights(probs, n, bits.device)
+    call("qes_sr_matvec_weighted", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(w), float(shift), ptr(v), ptr(y),
+         ptr(ws), int(ws.numel()), stream_ptr())
     return y
 
 
 def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
-                check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True, x0=None):
+                check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True, x0=None, probs=None):
     """x0: initial guess of the unscaled system (S + shift) x = F (a previous solution divided by
-    rhs_prefactor), float64 / complex128 of length P on the device; None starts from zero."""
+    rhs_prefactor), float64 / complex128 of length P on the device; None starts from zero.
+    probs: per-sample weights (any positive scale; normalised to sum Ns here), None = uniform."""
     dc = dtype_code(flat_params)
     n = int(bits.shape[0])
     ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
@@ -268,10 +281,12 @@ def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8
     opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor))
     res = _lib.SRResult()
     allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_converged else ()
-    call("qes_sr_solve_cg_x0", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), C.byref(opt), ptr(x0), ptr(x),
-         C.byref(res), ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
+    w = sample_weights(probs, n, bits.device)
+    call("qes_sr_solve_cg_weighted", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), ptr(w), C.byref(opt),
+         ptr(x0), ptr(x), C.byref(res), ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
     info = {"iterations": res.iterations, "converged": bool(res.converged), "residual": res.residual,
-            "rhs_norm": res.rhs_norm, "e_mean": complex(res.e_mean_re, res.e_mean_im)}
+            "rhs_norm": res.rhs_norm, "e_mean": complex(res.e_mean_re, res.e_mean_im),
+            "true_residual": res.true_residual}
     return x, info
 
 

@@ -379,12 +379,13 @@ class NQS:
         """One VMC epoch on the GPU; returns host-side statistics of this epoch."""
         tdvp = tdvp or self._tdvp or TDVP(rhs_prefactor=-1.0, sr_maxiter=1000)
         net = self._net
-        bits, _ = self._sampler.sample_bits(num_samples)
+        bits, lp = self._sampler.sample_bits(num_samples)
+        probs = self._sampler.sample_probs(lp)                  # None when the sampler draws |psi|^2
         _, tn, _ = dv.rbm_forward_step(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
         eloc = self.local_energy_bits(bits, tn)
-        st = dv.loss_stats(eloc)
+        st = dv.loss_stats(eloc, probs)
         rh = dv.loss_rhat(eloc, self._sampler.numchains)
-        x = tdvp.solve(net, bits, tn, eloc)
+        x = tdvp.solve(net, bits, tn, eloc, probs=probs)
         dv.param_update(net.flat, net.master, x, lr)
         net.bump()
         s = st.cpu().numpy()

@@ -273,6 +273,16 @@ class VMCSampler:
     def has_uniform_weights(self):
         return (1.0 / self._logprob_fact - self._mu * self._phys_beta) == 0.0
 
+    def sample_probs(self, logpsi):
+        """Reweighting factors of a batch (``vmc.py:1173-1184``): exp((1/logprob_fact - mu beta) Re log psi)
+        normalised to sum Ns, or None when the sampler draws |psi|^2 itself (uniform weights)."""
+        if self.has_uniform_weights:
+            return None
+        exponent = 1.0 / self._logprob_fact - self._mu * self._phys_beta
+        lu = exponent * logpsi.real.to(torch.float64)
+        pr = torch.exp(lu - lu.max())
+        return (pr / torch.clamp(pr.sum(), min=1e-10) * logpsi.shape[0]).to(torch.float32)
+
     def set_numchains(self, n):
         if int(n) != self._numchains:
             self._numchains = int(n)
@@ -316,12 +326,7 @@ class VMCSampler:
             self.set_numchains(num_chains)
         bits, lp = self.sample_bits(num_samples, num_therm)
         states = dv.unpack_states(bits, self._net.ns)
-        probs = None
-        if not self.has_uniform_weights:
-            exponent = 1.0 / self._logprob_fact - self._mu * self._phys_beta
-            lu = exponent * lp.real.to(torch.float64)
-            pr = torch.exp(lu - lu.max())
-            probs = (pr / torch.clamp(pr.sum(), min=1e-10) * lp.shape[0]).to(torch.float32)
+        probs = self.sample_probs(lp)
         last_states = dv.unpack_states(self._states, self._net.ns)
         if self.is_pt:
             last_states = last_states.view(self._n_replicas, self._numchains, self._net.ns)

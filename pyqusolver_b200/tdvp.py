@@ -5,7 +5,7 @@ Mirrors ``QES/NQS/src/tdvp.py`` for the RBM path:
 * centring and float64 promotion (``get_tdvp_standard`` ``:1056-1132``);
 * force F = O_c^H E_c / Ns, standard SR (O_c^H O_c / Ns + shift) x = F in the
   GRAM / MATVEC form (``_solve_prepare_matvec`` ``:1138-1197``);
-* x <- rhs_prefactor * x (default -1), optional global-norm clip
+* x <- rhs_prefactor * x (default 1, as the reference's TDVP; NQS.train passes -1), optional global-norm clip
   (``_finalize_solution`` ``:1410-1422``, ``_apply_grad_clip`` ``:882-907``);
 * ``use_sr=False`` returns x = -rhs_prefactor * F ... i.e. the reference's
   ``-final_b`` branch (``solve`` ``:1561-1569``);
@@ -13,8 +13,10 @@ Mirrors ``QES/NQS/src/tdvp.py`` for the RBM path:
   and returns O_c^H y (``_solve_prepare_s_and_loss`` ``:1199-1226``, ``_project_minsr_result``
   ``:1393-1408``), matrix-free on the same kernels.
 
-The solve runs on the GPU (``qes_sr_solve_cg``): the RBM's O is applied in
-structured form and never materialised, CG vectors and dots are float64.
+The solve runs on the GPU (``qes_sr_solve_cg_weighted``): the RBM's O is applied in
+structured form and never materialised, CG vectors and dots are float64.  With the
+sampler's reweighting factors (``probs``, when mu * beta != 1 / logprob_fact) the means
+and sample sums of F and S are weighted (``vmc.py:1173-1184``).
 """
 
 from __future__ import annotations
@@ -106,13 +108,17 @@ class TDVP:
             return None
         return torch.as_tensor(x0)
 
-    def solve(self, net, bits, tanh_theta, eloc, use_old_result=None):
-        """Parameter direction x (float64 / complex128, length P), already scaled by rhs_prefactor."""
+    def solve(self, net, bits, tanh_theta, eloc, use_old_result=None, probs=None):
+        """Parameter direction x (float64 / complex128, length P), already scaled by rhs_prefactor.
+        probs: the sampler's reweighting factors (None when it samples |psi|^2): weighted means and
+        sample sums in F and S (``qes_sr_solve_cg_weighted``)."""
         n = int(bits.shape[0])
         ws = self._ws(net, n)
         use_old = self.use_old_result if use_old_result is None else bool(use_old_result)
+        if probs is not None and self.use_sr and self.use_minsr:
+            raise NotImplementedError("MinSR with non-uniform sample weights is not implemented on the GPU path")
         if not self.use_sr:
-            F = dv.sr_force(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, workspace=ws)
+            F = dv.sr_force(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, workspace=ws, probs=probs)
             x = -(F * self.rhs_prefactor) if self.rhs_prefactor != 1.0 else -F
             self.last_info = {"iterations": 0, "converged": True, "residual": 0.0}
         elif self.use_minsr:
@@ -126,7 +132,7 @@ class TDVP:
             x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
                                      rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,
                                      check_every=self.check_every, rhs_prefactor=self.rhs_prefactor, workspace=ws,
-                                     x0=x0)
+                                     x0=x0, probs=probs)
             self.last_info = info
             self._solution = x.detach().clone()
         if self.grad_clip is not None and self.grad_clip > 0:

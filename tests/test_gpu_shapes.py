@@ -7,9 +7,19 @@
   N chunks, sample chunks folded in TMEM).
 
 Forward, E_loc and O are held to 1e-5 relative against the float64 oracle (the plain-FP32 bar);
-the SR force, matvec and CG solution to 1e-4 / 1e-4 / 1e-3 against the oracle's SR, whose O is
-rebuilt chunk by chunk from the oracle RBM (never whole).  The SR checks run on the tensor cores
-(impl 2, the mixed form) and on the CUDA cores (impl 1, the plain form).
+the SR force and matvec to 1e-4 against the oracle's SR, whose O is rebuilt chunk by chunk from
+the oracle RBM (never whole).  The SR checks run on the tensor cores (impl 2, the mixed form) and
+on the CUDA cores (impl 1, the plain form).
+
+The CG solution is held to backward-error bars, not to an entrywise bar: at these shapes
+(P >> Ns, shift 1e-3 / 1e-4) S + shift has condition numbers of 1e5-1e7, and a float32 or
+BF16-split contraction (relative error ~1e-6-1e-5) limits the true residual of any Krylov solve to
+about that level; the solution components along the near-null directions of S (eigenvalue ~ shift)
+then differ from the float64 solve by up to residual / shift, while everything the update does to
+the energy agrees.  Measured (GPU vs the oracle's exact solve): true residual 1e-5 (mixed and
+plain, 10x10) and 4e-7 / 6e-6 (plain / mixed, 20x20); F^H x to 1e-6 or better.  Asserted: the
+relative true residual in the oracle's float64 operator below 1e-4, F^H x within 1e-5, and the
+error in the (S + shift)-norm (the norm CG minimises) below 1e-2 of the solution's.
 """
 
 import numpy as np
@@ -126,7 +136,17 @@ def test_sr_force_matvec_and_solution_at_bench_shape(sr_impl, shape, impl):
     assert rel_err(F, F_ref) < 1e-4
     x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=1e-8, maxiter=3000)
     assert info["converged"]
-    assert rel_err(x.cpu().numpy(), x_ref) < 1e-3
+    xg = x.cpu().numpy()
+    A = lambda u: osr.matvec_chunked(p, sig, u, shift=shift, chunk=chunk)
+    resid = np.linalg.norm(A(-xg) - F_ref) / np.linalg.norm(F_ref)          # x carries rhs_prefactor -1
+    assert resid < 1e-4, resid
+    fx = lambda u: np.vdot(F_ref, u)
+    assert abs(fx(xg) - fx(x_ref)) <= 1e-5 * abs(fx(x_ref))
+    err = xg - x_ref
+    a_err = np.sqrt(abs(np.vdot(err, A(err)))) / np.sqrt(abs(np.vdot(x_ref, A(x_ref))))
+    assert a_err < 1e-2, a_err
+    # the library's own post-solve check of the true residual agrees with the oracle's
+    assert info["true_residual"] == pytest.approx(resid, rel=0.5, abs=1e-6)
 
 
 # ------------------------------------------------------------------------- public API: NQS.sample / NQS.step

@@ -55,3 +55,103 @@ def test_fused_cg_barrier_timeout_is_reported_and_solver_recovers(impl, device_l
         _lib.call("qes_set_cg_fused", 1)
         _lib.call("qes_set_cg_device_loop", 1)
         _lib.set_sr_impl(0)
+
+
+# ------------------------------------------------------------------------- sample weights
+from oracle import rbm as orbm, sr as osr
+
+
+def _oracle_params(net):
+    flat = net.flat.detach().cpu().numpy().astype(np.complex128 if net.is_complex else np.float64)
+    return orbm.RBMParams.from_flat(flat, net.ns, net.nh)
+
+
+def rel_err(a, b):
+    return np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(1e-30, np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("cplx,impl,big", [(True, 2, False), (True, 1, False), (False, 2, False), (False, 1, False),
+                                           (False, 2, True)])
+def test_weighted_sr_matches_oracle(cplx, impl, big):
+    """probs-weighted force, matvec and CG solution (qes_sr_*_weighted) against the oracle's weighted
+    centring F = O_c^H diag(p) E_c / Ns, S = O_c^H diag(p) O_c / Ns with means sum p X / Ns; the
+    weights are the sampler's reweighting factors exp(c Re log psi), normalised to sum Ns.  `big`
+    runs the M/N-tiled tensor-core O^H u (144 sites)."""
+    if big:
+        ns, nh, n = 144, 144, 512
+        model = qb.TransverseFieldIsing(qb.SquareLattice(2, 12, 12), j=1.0, hx=1.5)
+    else:
+        ns, nh, n = 9, 18, 700
+        model = qb.XXZ(qb.SquareLattice(2, 3, 3), jxy=-1.0, jz=-1.0, hx=0.4)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=6, init_scale=0.2 if not big else 0.05)
+    rng = np.random.default_rng(6)
+    st = np.where(rng.random((n, ns)) < 0.5, 0.5, -0.5)
+    bits = dv.pack_states(st)
+    _, tn, lp = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=True)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    # reweighting factors as VMCSampler returns them (exponent 1: samples drawn from |psi|^1)
+    lu = lp.real.double().cpu().numpy()
+    pr = np.exp(lu - lu.max())
+    probs = pr / pr.sum() * n
+    probs_t = torch.as_tensor(probs.astype(np.float32)).cuda()
+    w = probs_t.double().cpu().numpy()
+    w = w / w.sum() * n                                        # the library renormalises the same way
+    e = eloc.cpu().numpy().astype(np.complex128)
+    if not cplx:
+        e = e.real
+    O = orbm.log_derivatives(_oracle_params(net), orbm.to_sigma(st))
+    ec, Oc, w_, _, _ = osr.prepare(e, O, w)
+    F = osr.force(Oc, ec, w_)
+    S = osr.s_matrix(Oc, w_)
+    _lib.set_sr_impl(impl)
+    try:
+        if impl == 2:
+            assert _lib.sr_uses_tensor_cores(dv.dtype_code(net.flat), ns, nh, n)
+        Fg = dv.sr_force(net.flat, ns, nh, bits, tn, eloc, probs=probs_t).cpu().numpy()
+        assert rel_err(Fg, F) < 1e-4
+        v = rng.normal(size=O.shape[1]) + (1j * rng.normal(size=O.shape[1]) if cplx else 0)
+        y = dv.sr_matvec(net.flat, ns, nh, bits, tn, torch.as_tensor(v).cuda(), shift=1e-3, probs=probs_t)
+        assert rel_err(y.cpu().numpy(), S @ v + 1e-3 * v) < 1e-4
+        x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-10, maxiter=3000,
+                                 probs=probs_t)
+        A = S + 1e-2 * np.eye(S.shape[0])
+        xr = -np.linalg.solve(A, F)
+        assert info["converged"]
+        resid = np.linalg.norm(A @ (-x.cpu().numpy()) - F) / np.linalg.norm(F)
+        assert resid < 1e-4 and info["true_residual"] == pytest.approx(resid, rel=0.5, abs=1e-6)
+        assert rel_err(x.cpu().numpy(), xr) < 1e-2
+        # unit weights reproduce the unweighted entry points exactly
+        ones = torch.ones(n, dtype=torch.float32, device="cuda")
+        assert torch.equal(dv.sr_force(net.flat, ns, nh, bits, tn, eloc, probs=ones),
+                           dv.sr_force(net.flat, ns, nh, bits, tn, eloc))
+    finally:
+        _lib.set_sr_impl(0)
+
+
+def test_train_step_uses_the_sampler_weights():
+    """NQS with s_mu = 1 (samples from |psi|^1): train_step's energy is the weighted mean and its
+    SR direction the weighted solve of the same batch."""
+    L = qb.SquareLattice(1, 10)
+    model = qb.TransverseFieldIsing(L, j=1.0, hx=0.7)
+    kw = dict(alpha=1, dtype="float32", seed=4, s_numchains=256, s_numsamples=2, s_therm_steps=4, s_sweep_steps=4,
+              init_scale=0.2)
+    nqs = qb.NQS("rbm", model, s_mu=1.0, **kw)
+    assert not nqs.sampler.has_uniform_weights
+    from pyqusolver_b200.tdvp import TDVP
+    td = TDVP(rhs_prefactor=-1.0, sr_diag_shift=1e-2, sr_maxiter=2000, sr_tol=1e-10)
+    flat0 = nqs.net.master.clone()
+    # the same batch the step will draw: a twin NQS in the same state
+    twin = qb.NQS("rbm", model, s_mu=1.0, **kw)
+    bits, lp = twin.sampler.sample_bits()
+    probs = twin.sampler.sample_probs(lp)
+    _, tn, _ = dv.rbm_forward_step(twin.net.flat, 10, 10, bits, tanh=True, logpsi=False)
+    eloc = twin.local_energy_bits(bits, tn)
+    st = dv.loss_stats(eloc, probs).cpu().numpy()
+    x_ref, _ = dv.sr_solve_cg(twin.net.flat, 10, 10, bits, tn, eloc, shift=1e-2, rtol=1e-10, maxiter=2000,
+                              probs=probs)
+    info = nqs.train_step(lr=0.1, tdvp=td)
+    assert info["mean"] == pytest.approx(complex(st[0], st[1]), rel=1e-12)
+    step = (nqs.net.master - flat0) / 0.1
+    assert torch.allclose(step, x_ref, rtol=1e-9, atol=1e-12)

@@ -109,7 +109,7 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------- our arm
-def build_nqs(cfg, seed):
+def build_nqs(cfg, seed, sampler_seed=None):
     import pyqusolver_b200 as qb
     L = qb.SquareLattice(cfg["dim"], cfg["lx"], cfg["ly"], bc="pbc")
     if cfg["model"] == "xxz":
@@ -120,8 +120,8 @@ def build_nqs(cfg, seed):
         model = qb.TransverseFieldIsing(L, **cfg["kw"])
     nqs = qb.NQS("rbm", model, alpha=cfg["alpha"], dtype=cfg["dtype"], seed=seed, s_upd_fun=cfg["rule"],
                  s_initstate=cfg["init"], nparticles=L.ns // 2, s_numchains=cfg["chains"],
-                 s_numsamples=cfg["samples"], s_therm_steps=1, s_sweep_steps=cfg["sweep"], s_seed=seed,
-                 init_scale=0.01)
+                 s_numsamples=cfg["samples"], s_therm_steps=1, s_sweep_steps=cfg["sweep"],
+                 s_seed=seed if sampler_seed is None else sampler_seed, init_scale=0.01)
     from pyqusolver_b200.tdvp import TDVP
     tdvp = TDVP(rhs_prefactor=-1.0, sr_diag_shift=cfg["shift"], sr_tol=cfg["rtol"], sr_maxiter=cfg["maxiter"], check_every=32)
     return nqs, tdvp
@@ -205,6 +205,59 @@ def accuracy_check(epochs, name="tfim16"):
     _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
     out["e_exact"] = e_exact
     out["equal_dE_1e-4"] = bool(out["mixed"]["rel_err"] <= 1e-4 and out["plain_fp32"]["rel_err"] <= 1e-4)
+    return out
+
+
+def energy_estimate(nqs, batches):
+    """Variational energy of the current parameters: the mean of `batches` sampling-only batches of
+    E_loc (the chains continue between batches), with the standard error of the batch means."""
+    import torch
+    from pyqusolver_b200 import device as dv
+    net = nqs.net
+    means = []
+    for _ in range(int(batches)):
+        bits, _ = nqs.sampler.sample_bits()
+        _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, tanh=True, logpsi=False)
+        st = dv.loss_stats(nqs.local_energy_bits(bits, tn))
+        means.append(st[0])
+    m = torch.stack(means).cpu().numpy()
+    return float(m.mean()), float(m.std(ddof=1) / np.sqrt(len(m)))
+
+
+def matched_energy_check(epochs, eval_batches, name="heis10x10"):
+    """Equal-Delta-E on the benchmarked workload, where no ED exists: the same VMC run (same initial
+    parameters and chains) in the float64 form (SR contractions in float64 on CUDA cores, the
+    reference's SR precision), the mixed form and the plain-FP32 form, then each form's final
+    parameters evaluated with `eval_batches` sampling-only batches.  A second float64 run with other
+    sampler seeds measures the run-to-run spread of the final energy (the noise floor of the check:
+    the trajectories of independent Markov chains decorrelate after a few epochs in any precision)."""
+    import torch
+    from pyqusolver_b200 import _lib
+    cfg = CONFIGS[name]
+    out = {"workload": name, "epochs": int(epochs), "lr": cfg["lr"], "shift": cfg["shift"],
+           "eval_samples": int(eval_batches) * cfg["chains"] * cfg["samples"],
+           "reference": "float64 form (impl 3): the same step with float64 SR contractions of the float32 T"}
+    runs = (("fp64", _lib.SR_IMPL_FP64, None), ("fp64_other_chains", _lib.SR_IMPL_FP64, 777),
+            ("mixed", _lib.SR_IMPL_AUTO, None), ("plain_fp32", _lib.SR_IMPL_CUDA_CORES, None))
+    for form, impl, sseed in runs:
+        _lib.set_sr_impl(impl)
+        nqs, tdvp = build_nqs(cfg, seed=1, sampler_seed=sseed)
+        t0 = time.perf_counter()
+        for _ in range(int(epochs)):
+            nqs.train_step(lr=cfg["lr"], tdvp=tdvp)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        e, se = energy_estimate(nqs, eval_batches)
+        out[form] = {"energy": e, "stderr": se, "train_seconds": t_train,
+                     "ms_per_step": 1e3 * t_train / max(1, int(epochs))}
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+    e_ref = out["fp64"]["energy"]
+    for form in ("fp64_other_chains", "mixed", "plain_fp32"):
+        out[form]["rel_diff_vs_fp64"] = abs(out[form]["energy"] - e_ref) / abs(e_ref)
+        out[form]["rel_stderr"] = float(np.hypot(out[form]["stderr"], out["fp64"]["stderr"]) / abs(e_ref))
+    out["noise_floor_rel"] = out["fp64_other_chains"]["rel_diff_vs_fp64"]
+    out["equal_dE_1e-4"] = bool(out["mixed"]["rel_diff_vs_fp64"] <= 1e-4 and
+                                out["plain_fp32"]["rel_diff_vs_fp64"] <= 1e-4)
     return out
 
 
@@ -485,6 +538,15 @@ def run_ours(args, cfg, rank, world, local_rank):
     }
     if rank == 0 and args.accuracy_epochs > 0:
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
+    if rank == 0 and args.matched_epochs > 0 and args.config == "heis10x10":
+        line["accuracy_matched_fp64"] = matched_energy_check(args.matched_epochs, args.matched_eval)
+    if rank == 0 and world == 1 and not args.no_other_configs:
+        oc = {}
+        for name in ("tfim16", "j1j2_6x6", "tfim20x20"):
+            if name != args.config:
+                oc[name] = config_summary(name, args.other_steps, 3, flush)
+        oc["tfim_batch64"] = batch_summary(args.other_steps, 3, flush)
+        line["other_configs"] = oc
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
     if dist is not None:
@@ -492,6 +554,81 @@ def run_ours(args, cfg, rank, world, local_rank):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def config_summary(name, steps, warmup, flush):
+    """Both forms of another single-problem workload (fewer steps than the headline), with the live
+    roofline of its dominant kernel from separately profiled steps."""
+    import torch
+    from pyqusolver_b200 import _lib
+    cfg = CONFIGS[name]
+    forms = {}
+    for form, impl in (("plain_fp32", _lib.SR_IMPL_CUDA_CORES), ("mixed", _lib.SR_IMPL_AUTO)):
+        _lib.set_sr_impl(impl)
+        nqs, tdvp = build_nqs(cfg, seed=1234)
+        for _ in range(warmup):
+            timed_step(nqs, tdvp, cfg, [torch.cuda.Event(enable_timing=True) for _ in range(7)])
+        torch.cuda.synchronize()
+        step_ms, phase_ms, cg_iters, launches, _ = timed_loop(nqs, tdvp, cfg, steps, flush, profile=False)
+        f = {"nqs": nqs, "total_ms": float(np.sum(step_ms)), "phase_ms": phase_ms, "cg_iters": cg_iters,
+             "launches": launches, "prof": None}
+        if form == "mixed":
+            ce = tdvp.check_every
+            tdvp.check_every = 1
+            _, f["prof_phase_ms"], f["prof_cg_iters"], _, f["prof"] = timed_loop(nqs, tdvp, cfg, min(steps, 3), flush,
+                                                                                profile=True)
+            tdvp.check_every = ce
+        forms[form] = f
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+    n = cfg["chains"] * cfg["samples"]
+    out = {"workload": name, "steps": steps, "warmup": warmup, "samples_per_step": n,
+           "n_params": forms["mixed"]["nqs"].net.n_params}
+    for form, f in forms.items():
+        ms = f["total_ms"] / steps
+        out[form] = {"ms_per_step": ms, "vmc_steps_per_s": 1e3 / ms, "samples_per_s": n * 1e3 / ms,
+                     "phase_ms": {p: float(np.mean(v)) for p, v in f["phase_ms"].items()},
+                     "cg_iterations_mean": float(np.mean(f["cg_iters"])), "gpu_launches": int(f["launches"])}
+    out["mixed_over_plain_steps_per_s"] = forms["plain_fp32"]["total_ms"] / forms["mixed"]["total_ms"]
+    out["roofline"] = roofline(cfg, forms["mixed"]["nqs"], forms["mixed"])
+    out["issue_rooflines"] = issue_rooflines(cfg, forms["mixed"]["nqs"], forms["mixed"], None)
+    return out
+
+
+def batch_summary(steps, warmup, flush):
+    """The batched uneven workload (64 TFIM problems, one form): steps/s and the phase split."""
+    import torch
+    from pyqusolver_b200 import _lib
+    cfg = CONFIGS["tfim_batch64"]
+    B, Ls, hx = build_batch(cfg, seed=1)
+    kw = dict(shift=cfg["shift"], rtol=cfg["rtol"], maxiter=cfg["maxiter"], check_every=32)
+    mk = lambda: [torch.cuda.Event(enable_timing=True) for _ in range(7)]
+
+    def step(ev):
+        ev[0].record(); B.sample()
+        ev[1].record(); B.forward()
+        ev[2].record(); B.local_energy()
+        ev[3].record(); B.loss_stats()
+        ev[4].record(); B.sr_solve(**kw)
+        ev[5].record(); B.update(cfg["lr"])
+        ev[6].record()
+    for _ in range(warmup):
+        step(mk())
+    torch.cuda.synchronize()
+    _lib.launch_count(reset=True)
+    tot, ph = [], {p: [] for p in BATCH_PHASES}
+    for _ in range(steps):
+        flush.fill_(1.0)
+        ev = mk()
+        step(ev)
+        torch.cuda.synchronize()
+        tot.append(ev[0].elapsed_time(ev[6]))
+        for k, p in enumerate(BATCH_PHASES):
+            ph[p].append(ev[k].elapsed_time(ev[k + 1]))
+    ms = float(np.mean(tot))
+    return {"workload": "tfim_batch64", "steps": steps, "warmup": warmup, "problems": int(B.n_inst),
+            "samples_per_step": int(B.n_samples_total), "ms_per_step": ms, "vmc_steps_per_s": 1e3 / ms,
+            "samples_per_s": B.n_samples_total * 1e3 / ms, "phase_ms": {p: float(np.mean(v)) for p, v in ph.items()},
+            "gpu_launches": int(_lib.launch_count(reset=True))}
 
 
 def nqs_energy(info):
@@ -765,6 +902,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--accuracy-epochs", type=int, default=300,
                     help="epochs of the ED-checked mixed vs plain comparison on tfim16 (0 = skip)")
+    ap.add_argument("--matched-epochs", type=int, default=200,
+                    help="epochs of the float64 / mixed / plain comparison on heis10x10 (0 = skip)")
+    ap.add_argument("--matched-eval", type=int, default=200,
+                    help="sampling-only batches (16,384 samples each) that evaluate each final energy")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the per-workload summaries of tfim16, j1j2_6x6, tfim20x20 and tfim_batch64")
+    ap.add_argument("--other-steps", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local_rank = env_rank()

@@ -297,10 +297,13 @@ typedef struct {
 int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
 
 /* Matvec implementation of the SR calls in this process: 0 = 5th-generation
- * tensor cores (tcgen05, BF16 hi/lo split, FP32 accumulate) when ns <= 127,
- * nh <= 256 and the operands fit shared memory, CUDA cores otherwise
- * (default); 1 = CUDA cores only; 2 = tensor cores required (QES_ERR_SIZE
- * when the shapes do not allow them).  No counterpart in the reference
+ * tensor cores (tcgen05, BF16 hi/lo split, FP32 accumulate) when the tiling
+ * fits (ns <= 511, V' <= 512 rows, shared memory), CUDA cores otherwise
+ * (default); 1 = CUDA cores only (float32); 2 = tensor cores required
+ * (QES_ERR_SIZE when the shapes do not allow them); 3 = CUDA cores with
+ * float64 contractions of the same float32 T (the reference's SR precision:
+ * it promotes O to float64, tdvp.py:827-858), a slow reference form for
+ * accuracy checks (not MinSR).  No counterpart in the reference
  * (its SR runs on XLA).  qes_sr_force / qes_sr_matvec synchronise the stream
  * when the tensor-core path ran, to report bounded-wait time-outs.          */
 int qes_set_sr_impl(int impl);

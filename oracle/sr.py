@@ -117,26 +117,44 @@ def solve_sr(e_loc, O, *, shift=1e-3, probs=None, method="dense", rtol=1e-8,
 # Large shapes: O built chunk by chunk from the RBM (never whole), same normalisation
 # --------------------------------------------------------------------------------------
 
-def _o_chunks(params, sigma, chunk):
+def o_rows(params, sigma, tanh=None):
+    """O rows [sigma, t, sigma (x) t] in float64 / complex128.  tanh=None evaluates t = tanh(theta)
+    from the parameters in float64; given, t is the network's own (float32) output promoted, which
+    is what the reference's SR receives (it promotes the network's O to float64,
+    ``tdvp.py:827-858``)."""
     from . import rbm as rbm_mod
+    if tanh is None:
+        return rbm_mod.log_derivatives(params, sigma)
+    t = np.asarray(tanh)
+    t = t.astype(np.complex128 if np.iscomplexobj(t) else np.float64)
+    sigma = np.atleast_2d(np.asarray(sigma, dtype=np.float64))
+    ow = (sigma[:, :, None] * t[:, None, :]).reshape(sigma.shape[0], -1)
+    return np.concatenate([sigma.astype(t.dtype), t, ow.astype(t.dtype)], axis=1)
+
+
+def _o_chunks(params, sigma, chunk, tanh=None):
     for r0 in range(0, sigma.shape[0], chunk):
-        yield r0, rbm_mod.log_derivatives(params, sigma[r0:r0 + chunk])
+        yield r0, _o_chunks_one(params, sigma, r0, chunk, tanh)
 
 
-def matvec_chunked(params, sigma, v, shift=0.0, chunk=64, probs=None):
+def _o_chunks_one(params, sigma, r0, chunk, tanh=None):
+    return o_rows(params, sigma[r0:r0 + chunk], None if tanh is None else tanh[r0:r0 + chunk])
+
+
+def matvec_chunked(params, sigma, v, shift=0.0, chunk=64, probs=None, tanh=None):
     """(S + shift) v with S = O_c^H diag(w) O_c / Ns, O rebuilt per sample chunk (two passes)."""
     sigma = np.asarray(sigma, dtype=np.float64)
     ns = sigma.shape[0]
     w = np.ones(ns) if probs is None else np.asarray(probs, dtype=np.float64)
-    Ov = np.concatenate([O @ v for _, O in _o_chunks(params, sigma, chunk)])
+    Ov = np.concatenate([O @ v for _, O in _o_chunks(params, sigma, chunk, tanh)])
     u = w * (Ov - np.sum(w * Ov) / ns) / ns
     y = shift * np.asarray(v, dtype=np.result_type(v, Ov))
-    for r0, O in _o_chunks(params, sigma, chunk):
+    for r0, O in _o_chunks(params, sigma, chunk, tanh):
         y = y + np.conj(O).T @ u[r0:r0 + O.shape[0]]
     return y
 
 
-def solve_sr_chunked(params, sigma, e_loc, shift, rhs_prefactor=-1.0, chunk=64):
+def solve_sr_chunked(params, sigma, e_loc, shift, rhs_prefactor=-1.0, chunk=64, tanh=None):
     """Parameter-space SR solution through the sample-space identity
     (O_c^H O_c / Ns + shift)^-1 O_c^H E_c / Ns = O_c^H (O_c O_c^H / Ns + shift)^-1 E_c / Ns,
     with the Ns x Ns Gram matrix accumulated from O chunks; returns (x * rhs_prefactor, F)."""
@@ -146,18 +164,18 @@ def solve_sr_chunked(params, sigma, e_loc, shift, rhs_prefactor=-1.0, chunk=64):
     ec = e - e.mean()
     chunks = list(range(0, ns, chunk))
     om = None
-    for _, O in _o_chunks(params, sigma, chunk):
+    for _, O in _o_chunks(params, sigma, chunk, tanh):
         om = O.sum(axis=0) if om is None else om + O.sum(axis=0)
     om = om / ns
     G = np.zeros((ns, ns), dtype=np.complex128 if np.iscomplexobj(om) else np.float64)
     F = np.zeros_like(om)
     for a in chunks:
-        Oa = _o_chunks_one(params, sigma, a, chunk) - om[None, :]
+        Oa = _o_chunks_one(params, sigma, a, chunk, tanh) - om[None, :]
         F = F + np.conj(Oa).T @ ec[a:a + Oa.shape[0]]
         for b in chunks:
             if b < a:
                 continue
-            Ob = Oa if b == a else _o_chunks_one(params, sigma, b, chunk) - om[None, :]
+            Ob = Oa if b == a else _o_chunks_one(params, sigma, b, chunk, tanh) - om[None, :]
             blk = Oa @ np.conj(Ob).T
             G[a:a + Oa.shape[0], b:b + Ob.shape[0]] = blk
             if b != a:
@@ -166,11 +184,6 @@ def solve_sr_chunked(params, sigma, e_loc, shift, rhs_prefactor=-1.0, chunk=64):
     y = np.linalg.solve(G / ns + shift * np.eye(ns), ec / ns)
     x = np.zeros_like(om)
     for a in chunks:
-        Oa = _o_chunks_one(params, sigma, a, chunk) - om[None, :]
+        Oa = _o_chunks_one(params, sigma, a, chunk, tanh) - om[None, :]
         x = x + np.conj(Oa).T @ y[a:a + Oa.shape[0]]
     return rhs_prefactor * x, F
-
-
-def _o_chunks_one(params, sigma, r0, chunk):
-    from . import rbm as rbm_mod
-    return rbm_mod.log_derivatives(params, sigma[r0:r0 + chunk])

@@ -193,7 +193,7 @@ def call(name, *args, allow=()):
     return rc
 
 
-SR_IMPL_AUTO, SR_IMPL_CUDA_CORES, SR_IMPL_TENSOR_CORES = 0, 1, 2
+SR_IMPL_AUTO, SR_IMPL_CUDA_CORES, SR_IMPL_TENSOR_CORES, SR_IMPL_FP64 = 0, 1, 2, 3
 
 
 _SR_IMPL = [0]
@@ -201,7 +201,8 @@ _SR_IMPL = [0]
 
 def set_sr_impl(impl: int):
     """0 = tensor cores where the shapes allow (mixed form), 1 = CUDA cores only (plain FP32 form), 2 = tensor
-    cores required.  Also selects the forward (theta) path used by the training step."""
+    cores required, 3 = CUDA cores with float64 contractions (the float64 reference form).  Also selects the
+    forward (theta) path used by the training step (tensor cores only in forms 0 and 2)."""
     call("qes_set_sr_impl", int(impl))
     _SR_IMPL[0] = int(impl)
 

@@ -19,11 +19,12 @@
 #include <atomic>
 #include <vector>
 
-// 0 = tensor cores when the shapes allow it, 1 = CUDA cores only, 2 = tensor cores required
+// 0 = tensor cores when the shapes allow it, 1 = CUDA cores only (float32), 2 = tensor cores required,
+// 3 = CUDA cores with float64 contractions (the reference's SR precision, for accuracy checks)
 static std::atomic<int> g_sr_impl{0};
 extern "C" int qes_set_sr_impl(int impl) {
-  if (impl < 0 || impl > 2) {
-    qes_set_last_message("qes_set_sr_impl: impl must be 0 (auto), 1 (cuda cores) or 2 (tensor cores)");
+  if (impl < 0 || impl > 3) {
+    qes_set_last_message("qes_set_sr_impl: impl must be 0 (auto), 1 (cuda cores), 2 (tensor cores) or 3 (float64)");
     return QES_ERR_ARG;
   }
   g_sr_impl.store(impl);
@@ -55,6 +56,11 @@ QES_D float to_f(double v) { return (float)v; }
 QES_D float2 to_f(double2 v) { return make_float2((float)v.x, (float)v.y); }
 QES_D double to_d(float v) { return (double)v; }
 QES_D double2 to_d(float2 v) { return make_double2(v.x, v.y); }
+QES_D double to_d(double v) { return v; }
+QES_D double2 to_d(double2 v) { return v; }
+template <class T> struct IsF64 { static constexpr bool value = false; };
+template <> struct IsF64<double> { static constexpr bool value = true; };
+template <> struct IsF64<double2> { static constexpr bool value = true; };
 QES_D double vadd(double a, double b) { return a + b; }
 QES_D double2 vadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 QES_D double vscale(double s, double a) { return s * a; }
@@ -93,32 +99,87 @@ __global__ void __launch_bounds__(MEAN_THREADS) mean_c_kernel(int64_t n, const f
 }
 
 // ----------------------------------------------------------------------------
-// Plain-FP32 form: register-tiled CUDA-core contractions.  The spins are staged in shared memory
-// as +-1 floats, so every sign x value product is one FMA.  Block 32 x 8 threads; a thread owns R
-// rows x PT_C columns of the output tile, columns interleaved by 32 (conflict-free shared-memory
-// loads), rows interleaved by 8 (all lanes of a warp read the same spin: a broadcast).
+// CUDA-core forms: register-tiled contractions.  The spins are staged in shared memory as +-1
+// reals, so every sign x value product is one FMA.  Block 32 x 8 threads; a thread owns R rows x
+// PT_C columns of the output tile, columns interleaved by 32 (conflict-free shared-memory loads),
+// rows interleaved by 8 (all lanes of a warp read the same spin: a broadcast).  The accumulator
+// type A is float / float2 in the plain-FP32 form and double / double2 in the float64 form (the
+// same float32 T promoted, the reference's SR precision); K is the contraction slice per pass.
 // ----------------------------------------------------------------------------
 constexpr int PT_TX = 32, PT_TY = 8, PT_C = 4;
 constexpr int PT_THREADS = PT_TX * PT_TY;
 constexpr int PT_U = PT_TX * PT_C;            // columns (hidden units) per block
-constexpr int PT_K = 32;                      // contraction slice staged per pass
+constexpr int PT_K = 32;                      // contraction slice staged per pass (float32 accumulators)
+constexpr int PT_K64 = 16;                    // ... (float64 accumulators)
 constexpr int PT_SPLIT = 512;                 // samples per O^H u split (one partial P-vector each)
 
+// accumulator traits: RA = real type, W = complex type of the per-sample vectors w / u
+template <class A> struct Acc;
+template <> struct Acc<float> { using RA = float; using W = float2; };
+template <> struct Acc<float2> { using RA = float; using W = float2; };
+template <> struct Acc<double> { using RA = double; using W = double2; };
+template <> struct Acc<double2> { using RA = double; using W = double2; };
+
+QES_D float acc_cv(float x, float) { return x; }
+QES_D float acc_cv(double x, float) { return (float)x; }
+QES_D float2 acc_cv(float2 x, float2) { return x; }
+QES_D float2 acc_cv(double2 x, float2) { return make_float2((float)x.x, (float)x.y); }
+QES_D double acc_cv(float x, double) { return (double)x; }
+QES_D double acc_cv(double x, double) { return x; }
+QES_D double2 acc_cv(float2 x, double2) { return make_double2(x.x, x.y); }
+QES_D double2 acc_cv(double2 x, double2) { return x; }
+QES_D float2 acc_to_w(float x) { return make_float2(x, 0.f); }
+QES_D float2 acc_to_w(float2 x) { return x; }
+QES_D double2 acc_to_w(double x) { return make_double2(x, 0.0); }
+QES_D double2 acc_to_w(double2 x) { return x; }
+QES_D float acc_from_w(float2 w, float) { return w.x; }
+QES_D float2 acc_from_w(float2 w, float2) { return w; }
+QES_D double acc_from_w(float2 w, double) { return (double)w.x; }
+QES_D double2 acc_from_w(float2 w, double2) { return make_double2(w.x, w.y); }
+QES_D double acc_from_w(double2 w, double) { return w.x; }
+QES_D double2 acc_from_w(double2 w, double2) { return w; }
 QES_D float fma_s(float s, float v, float a) { return fmaf(s, v, a); }
 QES_D float2 fma_s(float s, float2 v, float2 a) { return make_float2(fmaf(s, v.x, a.x), fmaf(s, v.y, a.y)); }
+QES_D double fma_s(double s, double v, double a) { return fma(s, v, a); }
+QES_D double2 fma_s(double s, double2 v, double2 a) { return make_double2(fma(s, v.x, a.x), fma(s, v.y, a.y)); }
+QES_D float amul(float a, float b) { return a * b; }
+QES_D float2 amul(float2 a, float2 b) { return a * b; }
+QES_D double amul(double a, double b) { return a * b; }
+QES_D double2 amul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+QES_D float aadd(float a, float b) { return a + b; }
+QES_D float2 aadd(float2 a, float2 b) { return a + b; }
+QES_D double aadd(double a, double b) { return a + b; }
+QES_D double2 aadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+QES_D float aconj(float a) { return a; }
+QES_D float2 aconj(float2 a) { return conjf2(a); }
+QES_D double aconj(double a) { return a; }
+QES_D double2 aconj(double2 a) { return make_double2(a.x, -a.y); }
+template <class A> QES_D A azero() { return acc_cv(0.f, A()); }
+template <> QES_D float2 azero<float2>() { return make_float2(0.f, 0.f); }
+template <> QES_D double2 azero<double2>() { return make_double2(0.0, 0.0); }
+QES_D double2 warp_sum(double2 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
 
 // wpart[ub][s] = sum over the hidden units j of block ub of t_sj (v_b,j + sum_i sigma_si V_ij),
-// plus sigma_s . v_a in unit block 0: z = Sigma V is accumulated in registers over 32-site slices
-// (one spin word per sample and slice), then folded with t and summed over the warp's lanes.
-template <class T, class V, int R>
+// plus sigma_s . v_a in unit block 0: z = Sigma V is accumulated in registers over K-site slices
+// (spins from one word per sample and slice), then folded with t and summed over the warp's lanes.
+template <class T, class A, class V, int R, int K>
 __global__ void __launch_bounds__(PT_THREADS) ov_tile_kernel(int ns, int nh, int64_t n_samples,
                                                              const uint32_t* __restrict__ bits,
                                                              const T* __restrict__ tanh_theta,
-                                                             const V* __restrict__ v, float2* __restrict__ wpart,
+                                                             const V* __restrict__ v,
+                                                             typename Acc<A>::W* __restrict__ wpart,
                                                              const double* __restrict__ cg_done) {
+  using RA = typename Acc<A>::RA;
   constexpr int S = PT_TY * R;                   // samples per block
-  __shared__ float sg[PT_K][S];
-  __shared__ T vs[PT_K][PT_U];
+  __shared__ RA sg[K][S];
+  __shared__ A vs[K][PT_U];
   if (cg_done && *cg_done != 0.0) return;        // converged CG (stream order: exact)
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PT_TX + tx;
   const int64_t s0 = (int64_t)blockIdx.x * S;
@@ -127,30 +188,31 @@ __global__ void __launch_bounds__(PT_THREADS) ov_tile_kernel(int ns, int nh, int
   const V* va = v;
   const V* vb = v + ns;
   const V* vW = v + ns + nh;
-  T z[R][PT_C];
+  A z[R][PT_C];
 #pragma unroll
   for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int c = 0; c < PT_C; ++c) z[r][c] = ScalarTraits<T>::zero();
-  for (int i0 = 0; i0 < ns; i0 += PT_K) {
+    for (int c = 0; c < PT_C; ++c) z[r][c] = azero<A>();
+  for (int i0 = 0; i0 < ns; i0 += K) {           // K divides 32: a slice lies in one spin word
     __syncthreads();                             // the previous slice is consumed
-    for (int e = tid; e < PT_K * S; e += PT_THREADS) {
+    for (int e = tid; e < K * S; e += PT_THREADS) {
       const int sl = e % S, il = e / S;
       const int64_t s = s0 + sl;
-      float x = 0.f;
-      if (s < n_samples && i0 + il < ns) x = ((__ldg(bits + s * nw + (i0 >> 5)) >> il) & 1u) ? 1.f : -1.f;
+      const int i = i0 + il;
+      RA x = (RA)0;
+      if (s < n_samples && i < ns) x = ((__ldg(bits + s * nw + (i >> 5)) >> (i & 31)) & 1u) ? (RA)1 : (RA)-1;
       sg[il][sl] = x;
     }
-    for (int e = tid; e < PT_K * PT_U; e += PT_THREADS) {
+    for (int e = tid; e < K * PT_U; e += PT_THREADS) {
       const int il = e / PT_U, jl = e % PT_U;
       const int i = i0 + il, j = j0 + jl;
-      vs[il][jl] = (i < ns && j < nh) ? to_f(vW[(int64_t)i * nh + j]) : ScalarTraits<T>::zero();
+      vs[il][jl] = (i < ns && j < nh) ? acc_cv(vW[(int64_t)i * nh + j], A()) : azero<A>();
     }
     __syncthreads();
 #pragma unroll 8
-    for (int il = 0; il < PT_K; ++il) {
-      float sv[R];
-      T q[PT_C];
+    for (int il = 0; il < K; ++il) {
+      RA sv[R];
+      A q[PT_C];
 #pragma unroll
       for (int r = 0; r < R; ++r) sv[r] = sg[il][r * PT_TY + ty];
 #pragma unroll
@@ -164,36 +226,38 @@ __global__ void __launch_bounds__(PT_THREADS) ov_tile_kernel(int ns, int nh, int
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int64_t s = s0 + r * PT_TY + ty;
-    T acc = ScalarTraits<T>::zero();
+    A acc = azero<A>();
     if (s < n_samples) {
 #pragma unroll
       for (int c = 0; c < PT_C; ++c) {
         const int j = j0 + c * PT_TX + tx;
-        if (j < nh) acc = addx(acc, mulx(tanh_theta[s * nh + j], addx(z[r][c], to_f(vb[j]))));
+        if (j < nh)
+          acc = aadd(acc, amul(acc_cv(tanh_theta[s * nh + j], A()), aadd(z[r][c], acc_cv(vb[j], A()))));
       }
       if (blockIdx.y == 0) {                     // sigma_s . v_a, lanes over the sites
         for (int i = tx; i < ns; i += PT_TX) {
           const bool up = (__ldg(bits + s * nw + (i >> 5)) >> (i & 31)) & 1u;
-          acc = addx(acc, up ? to_f(va[i]) : scal(-1.f, to_f(va[i])));
+          acc = fma_s(up ? (RA)1 : (RA)-1, acc_cv(va[i], A()), acc);
         }
       }
     }
     acc = warp_sum(acc);
-    if (tx == 0 && s < n_samples) wpart[(int64_t)blockIdx.y * n_samples + s] = to_c(acc);
+    if (tx == 0 && s < n_samples) wpart[(int64_t)blockIdx.y * n_samples + s] = acc_to_w(acc);
   }
 }
 
 // w = sum of the unit-block partials (fixed order); mean of w in float64 (weighted by wts, which sum
 // to Ns, when given) when wmean is given
-__global__ void __launch_bounds__(1024) wsum_kernel(int64_t n, int nub, const float2* __restrict__ wpart,
-                                                     float2* __restrict__ w, double* __restrict__ wmean,
+template <class W>
+__global__ void __launch_bounds__(1024) wsum_kernel(int64_t n, int nub, const W* __restrict__ wpart,
+                                                     W* __restrict__ w, double* __restrict__ wmean,
                                                      const double* __restrict__ cg_done,
                                                      const float* __restrict__ wts) {
   if (cg_done && *cg_done != 0.0) return;
   double sr = 0, si = 0;
   for (int64_t k = threadIdx.x; k < n; k += blockDim.x) {
-    float2 a = wpart[k];
-    for (int b = 1; b < nub; ++b) a = a + wpart[(int64_t)b * n + k];
+    W a = wpart[k];
+    for (int b = 1; b < nub; ++b) a = aadd(a, wpart[(int64_t)b * n + k]);
     w[k] = a;
     const double f = wts ? (double)wts[k] : 1.0;
     sr += f * a.x;
@@ -217,69 +281,73 @@ __global__ void __launch_bounds__(1024) wsum_kernel(int64_t n, int nub, const fl
 // partial[split] = Sigma~^T Q~ over PT_SPLIT samples: rows are the sites plus a ones row at site
 // ns (-> g_b), columns the hidden units plus a virtual unit at nh carrying u itself (-> g_a);
 // Q_sj = conj(t_sj) u_s with u_s = wts_s (w_s - mean) * scale (wts_s = 1 without weights), staged
-// 32 samples at a time.
-template <class T, int R>
+// K samples at a time.  WI: the type of the per-sample input w (complex64 E_loc or O v of the form).
+template <class T, class A, class WI, int R, int K>
 __global__ void __launch_bounds__(PT_THREADS) ohu_tile_kernel(int ns, int nh, int64_t n_samples,
                                                               const uint32_t* __restrict__ bits,
                                                               const T* __restrict__ tanh_theta,
-                                                              const float2* __restrict__ w,
+                                                              const WI* __restrict__ w,
                                                               const double* __restrict__ wmean, double scale,
-                                                              T* __restrict__ partial,
+                                                              A* __restrict__ partial,
                                                               const double* __restrict__ cg_done,
                                                               const float* __restrict__ wts) {
+  using RA = typename Acc<A>::RA;
   constexpr int IB = PT_TY * R;                  // sites per block
-  __shared__ float sg[PT_K][IB];
-  __shared__ T qs[PT_K][PT_U];
-  __shared__ T us[PT_K];
+  __shared__ RA sg[K][IB];
+  __shared__ A qs[K][PT_U];
+  __shared__ A us[K];
   if (cg_done && *cg_done != 0.0) return;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PT_TX + tx;
   const int j0 = blockIdx.x * PT_U, i0 = blockIdx.y * IB;
   const int64_t sbeg = (int64_t)blockIdx.z * PT_SPLIT;
   const int64_t send = min(n_samples, sbeg + PT_SPLIT);
   const int nw = n_words(ns);
-  const float mr = wmean ? (float)wmean[0] : 0.f, mi = wmean ? (float)wmean[1] : 0.f;
-  const float fs = (float)scale;
-  T acc[R][PT_C];
+  const double mr = wmean ? wmean[0] : 0.0, mi = wmean ? wmean[1] : 0.0;
+  A acc[R][PT_C];
 #pragma unroll
   for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int c = 0; c < PT_C; ++c) acc[r][c] = ScalarTraits<T>::zero();
-  for (int64_t c0 = sbeg; c0 < send; c0 += PT_K) {
-    const int nc = (int)min((int64_t)PT_K, send - c0);
+    for (int c = 0; c < PT_C; ++c) acc[r][c] = azero<A>();
+  for (int64_t c0 = sbeg; c0 < send; c0 += K) {
+    const int nc = (int)min((int64_t)K, send - c0);
     __syncthreads();                             // the previous sub-chunk is consumed
-    if (tid < PT_K) {
-      T u = ScalarTraits<T>::zero();
+    if (tid < K) {
+      A u = azero<A>();
       if (tid < nc) {
-        const float2 wv = w[c0 + tid];
-        const float f = wts ? fs * wts[c0 + tid] : fs;
-        u = from_c(make_float2((wv.x - mr) * f, (wv.y - mi) * f), T());
+        const WI wv = w[c0 + tid];
+        const double f = wts ? scale * (double)wts[c0 + tid] : scale;
+        // float32 forms: (w - mean) * scale in float32, as before; float64 form: all in float64
+        if constexpr (sizeof(RA) == 4)
+          u = acc_from_w(make_float2(((float)wv.x - (float)mr) * (float)f, ((float)wv.y - (float)mi) * (float)f), A());
+        else
+          u = acc_from_w(make_double2(((double)wv.x - mr) * f, ((double)wv.y - mi) * f), A());
       }
       us[tid] = u;
     }
-    for (int e = tid; e < PT_K * IB; e += PT_THREADS) {
+    for (int e = tid; e < K * IB; e += PT_THREADS) {
       const int sl = e / IB, il = e % IB, i = i0 + il;
-      float x = 0.f;
+      RA x = (RA)0;
       if (sl < nc) {
-        if (i < ns) x = ((__ldg(bits + (c0 + sl) * nw + (i >> 5)) >> (i & 31)) & 1u) ? 1.f : -1.f;
-        else if (i == ns) x = 1.f;
+        if (i < ns) x = ((__ldg(bits + (c0 + sl) * nw + (i >> 5)) >> (i & 31)) & 1u) ? (RA)1 : (RA)-1;
+        else if (i == ns) x = (RA)1;
       }
       sg[sl][il] = x;
     }
     __syncthreads();                             // us
-    for (int e = tid; e < PT_K * PT_U; e += PT_THREADS) {
+    for (int e = tid; e < K * PT_U; e += PT_THREADS) {
       const int sl = e / PT_U, jl = e % PT_U, j = j0 + jl;
-      T q = ScalarTraits<T>::zero();
+      A q = azero<A>();
       if (sl < nc) {
-        if (j < nh) q = mulx(conjx(tanh_theta[(c0 + sl) * nh + j]), us[sl]);
+        if (j < nh) q = amul(aconj(acc_cv(tanh_theta[(c0 + sl) * nh + j], A())), us[sl]);
         else if (j == nh) q = us[sl];
       }
       qs[sl][jl] = q;
     }
     __syncthreads();
 #pragma unroll 8
-    for (int sl = 0; sl < PT_K; ++sl) {
-      float sv[R];
-      T q[PT_C];
+    for (int sl = 0; sl < K; ++sl) {
+      RA sv[R];
+      A q[PT_C];
 #pragma unroll
       for (int r = 0; r < R; ++r) sv[r] = sg[sl][r * PT_TY + ty];
 #pragma unroll
@@ -291,7 +359,7 @@ __global__ void __launch_bounds__(PT_THREADS) ohu_tile_kernel(int ns, int nh, in
     }
   }
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
-  T* out = partial + (int64_t)blockIdx.z * P;
+  A* out = partial + (int64_t)blockIdx.z * P;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = i0 + r * PT_TY + ty;
@@ -434,7 +502,7 @@ static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, doub
                                 double* dot_part, double* scal, unsigned int* counter, cudaStream_t st,
                                 const double* cg_done = nullptr) {
   constexpr int EV = (int)(16 / sizeof(T));
-  const bool vec = (P % EV == 0) && ((reinterpret_cast<uintptr_t>(partial) & 15) == 0);
+  const bool vec = !IsF64<T>::value && (P % EV == 0) && ((reinterpret_cast<uintptr_t>(partial) & 15) == 0);
   const int64_t nvec = vec ? P / EV : P;
   const int target = 2 * qes_sm_count();                   // two resident blocks per SM
   int64_t cv = (nvec + target - 1) / target;
@@ -443,10 +511,13 @@ static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, doub
   cv = std::min<int64_t>(cv, std::max<int64_t>(RS_THREADS / std::max<int64_t>(need, 1), 1));
   cv = std::max<int64_t>(1, std::min<int64_t>(cv, 128));
   const int grid = (int)std::min<int64_t>((nvec + cv - 1) / cv, RS_MAX_BLOCKS);
-  if (vec)
-    QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, true>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
-                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done));
-  else
+  if constexpr (!IsF64<T>::value) {
+    if (vec) {
+      QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, true>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
+                                    (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done));
+      return QES_OK;
+    }
+  }
     QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
                                   (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done));
   return QES_OK;
@@ -825,6 +896,8 @@ struct SRWork {
   float2* w;          // [Ns]
   float2* wpart;      // [ceil(nh / PT_U)][Ns] unit-block partials of w (plain form)
   const float* wts;   // per-sample weights normalised to sum Ns, or nullptr (uniform); set per call
+  bool fp64;          // float64 contractions on CUDA cores (impl 3): partials, wpart and w64 in float64
+  double2* w64;       // [Ns] O v of the float64 form
   double* wmean;      // [2] (+ pad)
   void* partial;      // [nsplit][P] of T
   void* x; void* r; void* p; void* Ap; void* b;   // [P] of V each
@@ -849,15 +922,17 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   L.td = TcDims{};
   const bool tc_ok = tc_plan(dtype, ns, nh, n_samples, &L.td);
   const int impl = g_sr_impl.load();
-  L.tc = tc_ok && impl != 1;
+  L.fp64 = impl == 3;
+  L.tc = tc_ok && impl != 1 && !L.fp64;
   const int64_t nsplit_max = std::max<int64_t>(nsplit_simt, tc_ok ? L.td.nsplit : 1);
   L.nsplit = (int)(L.tc ? L.td.nsplit : nsplit_simt);
   size_t off = 0;
   auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off += align256(bytes); return p; };
   L.w = (float2*)take((size_t)n_samples * sizeof(float2));
-  L.wpart = (float2*)take((size_t)((nh + PT_U - 1) / PT_U) * n_samples * sizeof(float2));
+  L.wpart = (float2*)take((size_t)((nh + PT_U - 1) / PT_U) * n_samples * (L.fp64 ? sizeof(double2) : sizeof(float2)));
+  L.w64 = L.fp64 ? (double2*)take((size_t)n_samples * sizeof(double2)) : nullptr;
   L.wmean = (double*)take(4 * sizeof(double));
-  L.partial = take((size_t)std::max<int64_t>(nsplit_max, 1) * P * ts);
+  L.partial = take((size_t)std::max<int64_t>(nsplit_max, 1) * P * (L.fp64 ? vs : ts));
   L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
   L.parts = (double*)take(std::max(RED_BLOCKS, RS_MAX_BLOCKS) * sizeof(double));
   L.scal = (double*)take(16 * sizeof(double));
@@ -875,62 +950,87 @@ extern "C" int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_sampl
   return QES_OK;
 }
 
-// split partials of O^H ((w - mean(w)) * scale) on the CUDA cores (register tiles)
+// split partials of O^H (wts (w - mean(w)) * scale) on the CUDA cores (register tiles); the float64
+// form (fp64) accumulates in double, from w64 when it is the form's own O v (float64), else from w
 template <class T>
 static int launch_ohu_plain(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
-                            const double* wmean, double scale, T* partial, cudaStream_t st,
-                            const double* cg_done = nullptr, const float* wts = nullptr) {
+                            const double* wmean, double scale, void* partial, cudaStream_t st,
+                            const double* cg_done = nullptr, const float* wts = nullptr, bool fp64 = false,
+                            const double2* w64 = nullptr) {
+  using V = typename VecT<T>::type;
   const int64_t nsplit = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
   QES_ARG_CHECK(nsplit <= 65535, "SR: too many samples");
-  const int R = pt_rows_ohu(ns);
+  const int R = fp64 ? 4 : pt_rows_ohu(ns);
   dim3 grid((nh + 1 + PT_U - 1) / PT_U, (ns + 1 + PT_TY * R - 1) / (PT_TY * R), (unsigned)nsplit);
+  const dim3 blk(PT_TX, PT_TY);
   const int pf = qes_prof_begin(QES_PROF_OHU, st);
-  if (R == 8)
-    ohu_tile_kernel<T, 8><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, partial,
-                                                              cg_done, wts);
-  else
-    ohu_tile_kernel<T, 4><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale, partial,
-                                                              cg_done, wts);
+  if (fp64) {
+    if (w64)
+      ohu_tile_kernel<T, V, double2, 4, PT_K64><<<grid, blk, 0, st>>>(ns, nh, n_samples, bits, tt, w64, wmean, scale,
+                                                                      (V*)partial, cg_done, wts);
+    else
+      ohu_tile_kernel<T, V, float2, 4, PT_K64><<<grid, blk, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale,
+                                                                     (V*)partial, cg_done, wts);
+  } else if (R == 8) {
+    ohu_tile_kernel<T, T, float2, 8, PT_K><<<grid, blk, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale,
+                                                                 (T*)partial, cg_done, wts);
+  } else {
+    ohu_tile_kernel<T, T, float2, 4, PT_K><<<grid, blk, 0, st>>>(ns, nh, n_samples, bits, tt, w, wmean, scale,
+                                                                 (T*)partial, cg_done, wts);
+  }
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;
 }
 
-// g = O^H ((w - mean(w)) * scale)   [+ shift * p, dot partials]   into y
+// g = O^H (wts (w - mean(w)) * scale)   [+ shift * p, dot partials]   into y
 template <class T, class V>
 static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
                      const double* wmean, double scale, const SRWork& L, double shift, const V* p, V* y,
                      double* dot_part, cudaStream_t st, const double* cg_done = nullptr) {
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   const int64_t nsplit = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
-  if (int rc = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, w, wmean, scale, (T*)L.partial, st, cg_done,
-                                   L.wts))
+  const double2* w64 = (L.fp64 && w == L.w) ? L.w64 : nullptr;     // the form's own O v
+  if (int rc = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, w, wmean, scale, L.partial, st, cg_done, L.wts,
+                                   L.fp64, w64))
     return rc;
   const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
-  if (int rc_ = launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
-      dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
+  if (L.fp64) {
+    if (int rc_ = launch_reduce_splits<V, V>(P, (int)nsplit, L.partial, shift, p, y,
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
+  } else {
+    if (int rc_ = launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
+  }
   QES_LAUNCH_CHECK();
   qes_prof_end(pfr, st);
   return QES_OK;
 }
 
 // w = O v on the CUDA cores (register tiles; unit-block partials summed in a fixed order), and
-// its float64 mean when wmean is given
+// its float64 mean when wmean is given; the float64 form writes L.w64 instead of w
 template <class T, class V>
 static int apply_ov(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const V* v, float2* w,
                     double* wmean, const SRWork& L, cudaStream_t st, const double* cg_done = nullptr) {
   const int nub = (nh + PT_U - 1) / PT_U;
-  const int R = pt_rows_ov(n_samples);
+  const int R = L.fp64 ? 4 : pt_rows_ov(n_samples);
   dim3 grid((unsigned)((n_samples + PT_TY * R - 1) / (PT_TY * R)), (unsigned)nub);
   QES_ARG_CHECK(nub <= 65535, "SR: nh too large");
+  const dim3 blk(PT_TX, PT_TY);
   const int pf = qes_prof_begin(QES_PROF_OV, st);
-  if (R == 8)
-    ov_tile_kernel<T, V, 8><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, v, L.wpart, cg_done);
+  if (L.fp64)
+    ov_tile_kernel<T, V, V, 4, PT_K64><<<grid, blk, 0, st>>>(ns, nh, n_samples, bits, tt, v, (double2*)L.wpart,
+                                                             cg_done);
+  else if (R == 8)
+    ov_tile_kernel<T, T, V, 8, PT_K><<<grid, blk, 0, st>>>(ns, nh, n_samples, bits, tt, v, L.wpart, cg_done);
   else
-    ov_tile_kernel<T, V, 4><<<grid, dim3(PT_TX, PT_TY), 0, st>>>(ns, nh, n_samples, bits, tt, v, L.wpart, cg_done);
+    ov_tile_kernel<T, T, V, 4, PT_K><<<grid, blk, 0, st>>>(ns, nh, n_samples, bits, tt, v, L.wpart, cg_done);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
-  wsum_kernel<<<1, 1024, 0, st>>>(n_samples, nub, L.wpart, w, wmean, cg_done, L.wts);
+  if (L.fp64)
+    wsum_kernel<double2><<<1, 1024, 0, st>>>(n_samples, nub, (const double2*)L.wpart, L.w64, wmean, cg_done, L.wts);
+  else
+    wsum_kernel<float2><<<1, 1024, 0, st>>>(n_samples, nub, L.wpart, w, wmean, cg_done, L.wts);
   QES_LAUNCH_CHECK();
   return QES_OK;
 }
@@ -1266,7 +1366,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   // fused vector kernel (split reduction, x/r and direction updates with two grid barriers):
   // always (2), never (0), or automatically (1) for grids of up to 160 CTAs
   const int fused_mode = g_cg_fused.load();
-  bool fused = fused_mode != 0;
+  bool fused = fused_mode != 0 && !L.fp64;         // the fused kernel reads float32 split partials
   int fused_grid = 0, fused_cv = 1;
   constexpr int FEV = (int)(16 / sizeof(T));
   const bool fused_vec = (P % FEV == 0) && ((reinterpret_cast<uintptr_t>(L.partial) & 15) == 0);
@@ -1309,7 +1409,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
           int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, L, st, L.scal + 4);
           if (r2) return r2;
           r2 = launch_ohu_plain<T>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples,
-                                   (T*)L.partial, st, L.scal + 4, L.wts);
+                                   L.partial, st, L.scal + 4, L.wts);
           if (r2) return r2;
         }
         cudaLaunchConfig_t lc = {};
@@ -1737,6 +1837,7 @@ static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* 
   const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   V* y = (V*)M.y; V* r = (V*)M.r; V* p = (V*)M.p; V* Ap = (V*)M.Ap; V* b = (V*)M.b; V* g = (V*)M.g;
+  QES_ARG_CHECK(!L.fp64, "qes_sr_solve_minsr: the float64 form (impl 3) is not implemented for MinSR");
   int rc = sr_prepare(dtype, n, bits, tt, L, st);
   if (rc) return rc;
   mean_c_kernel<<<1, MEAN_THREADS, 0, st>>>(n, eloc, L.wmean);

@@ -121,7 +121,7 @@ def rbm_forward(flat_params, ns, nh, bits, theta=False, tanh=True, logpsi=True, 
 def forward_uses_tensor_cores(flat_params, ns, nh, n) -> bool:
     """The training step's forward runs on the tensor cores in the mixed form (SR impl 0 or 2) when the
     shapes fit the tensor-core forward."""
-    if _lib.sr_impl() == _lib.SR_IMPL_CUDA_CORES or n <= 0:
+    if _lib.sr_impl() in (_lib.SR_IMPL_CUDA_CORES, _lib.SR_IMPL_FP64) or n <= 0:
         return False
     nb = C.c_size_t(0)
     rc = call("qes_rbm_forward_tc_workspace_bytes", dtype_code(flat_params), ns, nh, int(n), C.byref(nb),

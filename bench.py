@@ -208,56 +208,75 @@ def accuracy_check(epochs, name="tfim16"):
     return out
 
 
-def energy_estimate(nqs, batches):
-    """Variational energy of the current parameters: the mean of `batches` sampling-only batches of
-    E_loc (the chains continue between batches), with the standard error of the batch means."""
+def matched_energy_check(epochs, every, name="heis10x10"):
+    """Equal-Delta-E on the benchmarked workload, where no ED exists.  Independent VMC runs cannot
+    resolve 1e-4 here: the Markov chains of two runs decorrelate within a few epochs in any
+    precision, and the final energies of two float64 runs that differ only in their sampler seeds
+    differ by ~1e-2 after a few hundred epochs.  So the forms are compared on the same batches: the
+    mixed form drives the training run, and every `every` epochs the batch it has just drawn is also
+    solved by the float64 form (SR contractions in float64 on CUDA cores, the reference's SR
+    precision) and by the plain-FP32 form.  Per checked epoch: the first-order energy change of the
+    update, dE = 2 lr Re(F^H x) (the SR step minimises it), for each form against the float64 one,
+    the error of x in the (S + shift)-norm of the float64 operator, and each solve's true residual."""
     import torch
-    from pyqusolver_b200 import device as dv
+    from pyqusolver_b200 import _lib, device as dv
+    from pyqusolver_b200.tdvp import TDVP
+    cfg = CONFIGS[name]
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+    nqs, tdvp = build_nqs(cfg, seed=1)
     net = nqs.net
-    means = []
-    for _ in range(int(batches)):
+    forms = {"fp64": _lib.SR_IMPL_FP64, "mixed": _lib.SR_IMPL_AUTO, "plain_fp32": _lib.SR_IMPL_CUDA_CORES}
+    rows, energies = [], []
+    t0 = time.perf_counter()
+    for ep in range(int(epochs)):
+        info = nqs.train_step(lr=cfg["lr"], tdvp=tdvp)
+        energies.append(info["mean"].real)
+        if (ep + 1) % int(every):
+            continue
+        # the next batch, solved by every form (then used by the mixed form's training step)
         bits, _ = nqs.sampler.sample_bits()
         _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, tanh=True, logpsi=False)
-        st = dv.loss_stats(nqs.local_energy_bits(bits, tn))
-        means.append(st[0])
-    m = torch.stack(means).cpu().numpy()
-    return float(m.mean()), float(m.std(ddof=1) / np.sqrt(len(m)))
-
-
-def matched_energy_check(epochs, eval_batches, name="heis10x10"):
-    """Equal-Delta-E on the benchmarked workload, where no ED exists: the same VMC run (same initial
-    parameters and chains) in the float64 form (SR contractions in float64 on CUDA cores, the
-    reference's SR precision), the mixed form and the plain-FP32 form, then each form's final
-    parameters evaluated with `eval_batches` sampling-only batches.  A second float64 run with other
-    sampler seeds measures the run-to-run spread of the final energy (the noise floor of the check:
-    the trajectories of independent Markov chains decorrelate after a few epochs in any precision)."""
-    import torch
-    from pyqusolver_b200 import _lib
-    cfg = CONFIGS[name]
-    out = {"workload": name, "epochs": int(epochs), "lr": cfg["lr"], "shift": cfg["shift"],
-           "eval_samples": int(eval_batches) * cfg["chains"] * cfg["samples"],
-           "reference": "float64 form (impl 3): the same step with float64 SR contractions of the float32 T"}
-    runs = (("fp64", _lib.SR_IMPL_FP64, None), ("fp64_other_chains", _lib.SR_IMPL_FP64, 777),
-            ("mixed", _lib.SR_IMPL_AUTO, None), ("plain_fp32", _lib.SR_IMPL_CUDA_CORES, None))
-    for form, impl, sseed in runs:
-        _lib.set_sr_impl(impl)
-        nqs, tdvp = build_nqs(cfg, seed=1, sampler_seed=sseed)
-        t0 = time.perf_counter()
-        for _ in range(int(epochs)):
-            nqs.train_step(lr=cfg["lr"], tdvp=tdvp)
-        torch.cuda.synchronize()
-        t_train = time.perf_counter() - t0
-        e, se = energy_estimate(nqs, eval_batches)
-        out[form] = {"energy": e, "stderr": se, "train_seconds": t_train,
-                     "ms_per_step": 1e3 * t_train / max(1, int(epochs))}
-    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
-    e_ref = out["fp64"]["energy"]
-    for form in ("fp64_other_chains", "mixed", "plain_fp32"):
-        out[form]["rel_diff_vs_fp64"] = abs(out[form]["energy"] - e_ref) / abs(e_ref)
-        out[form]["rel_stderr"] = float(np.hypot(out[form]["stderr"], out["fp64"]["stderr"]) / abs(e_ref))
-    out["noise_floor_rel"] = out["fp64_other_chains"]["rel_diff_vs_fp64"]
-    out["equal_dE_1e-4"] = bool(out["mixed"]["rel_diff_vs_fp64"] <= 1e-4 and
-                                out["plain_fp32"]["rel_diff_vs_fp64"] <= 1e-4)
+        eloc = nqs.local_energy_bits(bits, tn)
+        xs, res = {}, {}
+        for form, impl in forms.items():
+            _lib.set_sr_impl(impl)
+            x, inf = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tn, eloc, shift=cfg["shift"], rtol=cfg["rtol"],
+                                    maxiter=4 * cfg["maxiter"], check_every=32)
+            xs[form], res[form] = x, inf
+        _lib.set_sr_impl(_lib.SR_IMPL_FP64)
+        F = dv.sr_force(net.flat, net.ns, net.nh, bits, tn, eloc)
+        Ax = lambda v: dv.sr_matvec(net.flat, net.ns, net.nh, bits, tn, v, shift=cfg["shift"])
+        _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+        x64 = xs["fp64"]
+        dE64 = 2 * cfg["lr"] * torch.vdot(F, x64).real.item()
+        nA64 = torch.vdot(x64, Ax(x64)).real.item()
+        row = {"epoch": ep + 1, "dE_fp64": dE64, "cg_iterations": {f: res[f]["iterations"] for f in forms},
+               "true_residual": {f: res[f]["true_residual"] for f in forms}}
+        for form in ("mixed", "plain_fp32"):
+            dE = 2 * cfg["lr"] * torch.vdot(F, xs[form]).real.item()
+            e = xs[form] - x64
+            row[form] = {"dE_rel_diff": abs(dE - dE64) / abs(dE64),
+                         "x_err_A_norm": float(np.sqrt(max(torch.vdot(e, Ax(e)).real.item(), 0.0) / nA64))}
+        rows.append(row)
+        # the mixed form's step on this batch (the same update the training run would make)
+        x = tdvp.solve(net, bits, tn, eloc)
+        dv.param_update(net.flat, net.master, x, cfg["lr"])
+        net.bump()
+    torch.cuda.synchronize()
+    E = np.array(energies)
+    out = {"workload": name, "epochs": int(epochs), "checked_every": int(every), "checked_epochs": len(rows),
+           "lr": cfg["lr"], "shift": cfg["shift"], "driver_form": "mixed", "seconds": time.perf_counter() - t0,
+           "reference": "float64 form (impl 3): float64 SR contractions of the float32 T",
+           "energy_first": float(E[0]), "energy_last10_mean": float(E[-10:].mean())}
+    for form in ("mixed", "plain_fp32"):
+        d = np.array([r[form]["dE_rel_diff"] for r in rows])
+        a = np.array([r[form]["x_err_A_norm"] for r in rows])
+        out[form] = {"dE_rel_diff_max": float(d.max()), "dE_rel_diff_median": float(np.median(d)),
+                     "x_err_A_norm_max": float(a.max()), "x_err_A_norm_median": float(np.median(a)),
+                     "true_residual_max": float(max(r["true_residual"][form] for r in rows))}
+    out["fp64_true_residual_max"] = float(max(r["true_residual"]["fp64"] for r in rows))
+    out["equal_dE_1e-4"] = bool(out["mixed"]["dE_rel_diff_max"] <= 1e-4 and out["plain_fp32"]["dE_rel_diff_max"] <= 1e-4)
+    out["per_epoch"] = rows
     return out
 
 
@@ -539,7 +558,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     if rank == 0 and args.accuracy_epochs > 0:
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
     if rank == 0 and args.matched_epochs > 0 and args.config == "heis10x10":
-        line["accuracy_matched_fp64"] = matched_energy_check(args.matched_epochs, args.matched_eval)
+        line["accuracy_matched_fp64"] = matched_energy_check(args.matched_epochs, args.matched_every)
     if rank == 0 and world == 1 and not args.no_other_configs:
         oc = {}
         for name in ("tfim16", "j1j2_6x6", "tfim20x20"):
@@ -547,6 +566,8 @@ def run_ours(args, cfg, rank, world, local_rank):
                 oc[name] = config_summary(name, args.other_steps, 3, flush)
         oc["tfim_batch64"] = batch_summary(args.other_steps, 3, flush)
         line["other_configs"] = oc
+    if rank == 0 and world == 1 and not args.no_dense:
+        line["dense_sr"] = dense_summary(flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
     if dist is not None:
@@ -591,6 +612,72 @@ def config_summary(name, steps, warmup, flush):
     out["mixed_over_plain_steps_per_s"] = forms["plain_fp32"]["total_ms"] / forms["mixed"]["total_ms"]
     out["roofline"] = roofline(cfg, forms["mixed"]["nqs"], forms["mixed"])
     out["issue_rooflines"] = issue_rooflines(cfg, forms["mixed"]["nqs"], forms["mixed"], None)
+    return out
+
+
+def dense_summary(flush, names=("tfim16", "j1j2_6x6", "heis10x10"), steps=3):
+    """The formed-S path (TDVP sr_form_matrix=True): tensor-core Gram + float64 Cholesky.  Per workload,
+    after a few matrix-free warm-up epochs: one profiled dense solve (Gram and Cholesky times from CUDA
+    events on the launch stream, Gram TFLOP/s against the measured sustained BF16 peak) and, where a
+    step takes under a second, the VMC steps/s of the dense form next to the matrix-free one."""
+    import torch
+    from pyqusolver_b200 import _lib, device as dv
+    from pyqusolver_b200.tdvp import TDVP
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("bf16_tflops_sustained", 1400.0)
+    out = {}
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+    for name in names:
+        cfg = CONFIGS[name]
+        nqs, tdvp = build_nqs(cfg, seed=1234)
+        for _ in range(3):
+            nqs.train_step(lr=cfg["lr"], tdvp=tdvp)
+        net = nqs.net
+        bits, _ = nqs.sampler.sample_bits()
+        _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, tanh=True, logpsi=False)
+        eloc = nqs.local_energy_bits(bits, tn)
+        n, P = int(bits.shape[0]), net.n_params
+        ws = dv.sr_dense_workspace(dv.dtype_code(net.flat), net.ns, net.nh, n, bits.device)
+        dv.sr_solve_dense(net.flat, net.ns, net.nh, bits, tn, eloc, shift=cfg["shift"], workspace=ws)   # warm-up
+        flush.fill_(1.0)
+        _lib.profile_read(reset=True)
+        _lib.profile_enable(True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        x, info, _ = dv.sr_solve_dense(net.flat, net.ns, net.nh, bits, tn, eloc, shift=cfg["shift"], workspace=ws)
+        ev[1].record()
+        torch.cuda.synchronize()
+        prof = _lib.profile_read(reset=True)
+        _lib.profile_enable(False)
+        gram_ms, chol_ms = prof["gram"][0], prof["cholesky"][0]
+        flops = (4.0 if net.is_complex else 1.0) * n * P * P          # Hermitian half of the Gram
+        r = {"n_params": P, "samples": n, "solve_ms": ev[0].elapsed_time(ev[1]), "gram_ms": gram_ms,
+             "cholesky_ms": chol_ms, "gram_algorithmic_flop": flops,
+             "gram_tflops": flops / (gram_ms / 1e3) / 1e12 if gram_ms > 0 else None,
+             "gram_frac_of_bf16_sustained": (flops / (gram_ms / 1e3) / 1e12) / peak if gram_ms > 0 else None,
+             "peak_bf16_tflops_sustained": peak, "true_residual": info["true_residual"],
+             "workspace_gb": ws.numel() / 1e9}
+        if r["solve_ms"] < 1000.0:
+            td = TDVP(rhs_prefactor=-1.0, sr_diag_shift=cfg["shift"], sr_form_matrix=True)
+            for _ in range(2):
+                nqs.train_step(lr=cfg["lr"], tdvp=td)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                nqs.train_step(lr=cfg["lr"], tdvp=td)
+            torch.cuda.synchronize()
+            r["dense_vmc_steps_per_s"] = steps / (time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                nqs.train_step(lr=cfg["lr"], tdvp=tdvp)
+            torch.cuda.synchronize()
+            r["matrix_free_vmc_steps_per_s"] = steps / (time.perf_counter() - t0)
+        del ws
+        out[name] = r
     return out
 
 
@@ -770,6 +857,11 @@ def roofline(cfg, nqs, form):
     if dom in ("ov", "ohu", "reduce"):
         b = kernel_bytes(cfg, nqs, dom, tc=tc)
         tr = traffic_db.get(cfg.get("name", ""), {}).get(dom)
+    elif dom in ("sample", "local_energy"):
+        # working sets in shared memory and L2: bound by FP32 issue, not by HBM
+        ir = issue_rooflines(cfg, nqs, {"phase_ms": phases}, None)[dom]
+        ir["share_of_timed_region"] = out["share_of_timed_region"]
+        return ir
     else:
         n = cfg["chains"] * cfg["samples"]
         b = n * net.nh * (8 if net.is_complex else 4) + n * ((net.ns + 31) // 32) * 4
@@ -902,13 +994,14 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--accuracy-epochs", type=int, default=300,
                     help="epochs of the ED-checked mixed vs plain comparison on tfim16 (0 = skip)")
-    ap.add_argument("--matched-epochs", type=int, default=200,
+    ap.add_argument("--matched-epochs", type=int, default=300,
                     help="epochs of the float64 / mixed / plain comparison on heis10x10 (0 = skip)")
-    ap.add_argument("--matched-eval", type=int, default=200,
-                    help="sampling-only batches (16,384 samples each) that evaluate each final energy")
+    ap.add_argument("--matched-every", type=int, default=15,
+                    help="solve the batch of every n-th epoch in all three forms")
     ap.add_argument("--no-other-configs", action="store_true",
                     help="skip the per-workload summaries of tfim16, j1j2_6x6, tfim20x20 and tfim_batch64")
     ap.add_argument("--other-steps", type=int, default=8)
+    ap.add_argument("--no-dense", action="store_true", help="skip the formed-S (Gram + Cholesky) summary")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local_rank = env_rank()

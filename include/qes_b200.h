@@ -361,7 +361,8 @@ int qes_set_l2_persist(int enable);
 
 /* Per-kernel CUDA-event timing of the SR matvec halves, for measurement:
  * while enabled, every launch of class k (0: O v, 1: O^H u, 2: split
- * reduction) is bracketed by two events on its launch stream and CG graphs
+ * reduction, 3: dense Gram, 4: dense Cholesky, the whole factorisation)
+ * is bracketed by two events on its launch stream and CG graphs
  * are bypassed.  qes_profile_read synchronises the device and returns the
  * accumulated milliseconds and launch counts (reset != 0 zeroes them).
  * No counterpart in the reference (it has no per-kernel timing).          */
@@ -411,6 +412,30 @@ int qes_sr_solve_cg_x0(int dtype, int ns, int nh, int64_t n_samples,
                        const qes_sr_options* opt, const void* x0, void* x_out,
                        qes_sr_result* result, void* workspace, size_t workspace_bytes,
                        void* stream);
+
+/* Formed SR matrix (TDVP sr_form_matrix=True; QES/NQS/src/tdvp.py:340,455
+ * and the covariance of get_tdvp_standard :1113-1117) and its direct solve.
+ * S = O_c^H diag(p) O_c / Ns (p = probs normalised to sum Ns, NULL =
+ * uniform; O_c centred by the weighted mean) is formed on the tensor cores:
+ * the centred O as BF16 hi/lo tiles, hi*hi + hi*lo + lo*hi tcgen05 MMAs with
+ * FP32 accumulation in TMEM over the samples, combined into float64.
+ * qes_sr_gram writes S (P x P row-major, full Hermitian, float64 /
+ * complex128) to s_out.  qes_sr_solve_dense factorises S + shift = L L^H in
+ * float64 (blocked Cholesky) and solves for x = rhs_prefactor (S + shift)^-1 F;
+ * result: iterations 0, converged 0 and QES_ERR_NOT_CONVERGED when S + shift
+ * is not positive definite in float64, true_residual = ||F - (S + shift) x||
+ * / ||F|| with the formed S.  Memory grows as P^2: QES_ERR_SIZE when the
+ * workspace would exceed 100 GB (use the matrix-free qes_sr_solve_cg).
+ * Workspace from qes_sr_dense_workspace_bytes (gram_only != 0: the smaller
+ * workspace of qes_sr_gram).                                               */
+int qes_sr_dense_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, int gram_only, size_t* bytes);
+int qes_sr_gram(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                const void* tanh_theta, const float* probs, void* s_out, void* workspace,
+                size_t workspace_bytes, void* stream);
+int qes_sr_solve_dense(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                       const void* tanh_theta, const void* eloc, const float* probs,
+                       const qes_sr_options* opt, void* x_out, qes_sr_result* result,
+                       void* workspace, size_t workspace_bytes, void* stream);
 
 /* Vector-Jacobian product of log psi for the hand-written backward:
  * grad = O^H g  (g: complex64 per sample; real part used for a real RBM),

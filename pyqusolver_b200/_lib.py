@@ -137,6 +137,10 @@ SIGNATURES = {
                                _vp],
     "qes_sr_solve_cg_weighted": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
                                  _vp, C.POINTER(SRResult), _vp, _sz, _vp],
+    "qes_sr_dense_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.c_int, C.POINTER(_sz)],
+    "qes_sr_gram": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
+    "qes_sr_solve_dense": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
+                           C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_sr_minsr_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
     "qes_sr_solve_minsr": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
                            C.POINTER(SRResult), _vp, _sz, _vp],
@@ -228,7 +232,7 @@ def sr_uses_tensor_cores(dtype_code: int, ns: int, nh: int, n_samples: int) -> b
     return bool(u.value)
 
 
-PROFILE_CLASSES = ("ov", "ohu", "reduce")
+PROFILE_CLASSES = ("ov", "ohu", "reduce", "gram", "cholesky")
 
 
 def profile_enable(on: bool):

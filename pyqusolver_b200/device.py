@@ -350,3 +350,51 @@ def sampler_run(flat_params, ns, nh, cfg: _lib.SamplerConfig, flip_tables, exch,
     call("qes_sampler_run", dtype_code(flat_params), C.byref(cfg), ptr(a), ptr(b), ptr(W), ptr(fC), ptr(fS),
          ptr(nbr), ptr(nbr_pair), ptr(pi), ptr(pj), npairs, ptr(pC), ptr(pS), ptr(chain_bits), ptr(chain_step),
          ptr(proposed), ptr(accepted), ptr(sample_bits), ptr(sample_logpsi), ptr(last_logpsi), stream_ptr())
+
+
+# --------------------------------------------------------------------------------------
+# formed SR matrix (tensor-core Gram) and its float64 Cholesky solve
+# --------------------------------------------------------------------------------------
+
+def sr_dense_workspace(dtype_c, ns, nh, n, device, gram_only=False):
+    nb = C.c_size_t(0)
+    call("qes_sr_dense_workspace_bytes", dtype_c, ns, nh, n, 1 if gram_only else 0, C.byref(nb))
+    return torch.empty((int(nb.value),), dtype=torch.uint8, device=device)
+
+
+def sr_gram(flat_params, ns, nh, bits, tanh_theta, probs=None, workspace=None):
+    """S = O_c^H diag(p) O_c / Ns as a (P, P) float64 / complex128 device tensor (full Hermitian)."""
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    P = n_params(ns, nh)
+    ws = workspace if workspace is not None else sr_dense_workspace(dc, ns, nh, n, bits.device, gram_only=True)
+    S = torch.empty((P, P), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    w = sample_weights(probs, n, bits.device)
+    call("qes_sr_gram", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(w), ptr(S), ptr(ws), int(ws.numel()),
+         stream_ptr())
+    return S
+
+
+def sr_solve_dense(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rhs_prefactor=-1.0, probs=None,
+                   workspace=None, allow_not_pd=True):
+    """x = rhs_prefactor (S + shift)^-1 F with S formed on the tensor cores and a float64 Cholesky solve."""
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    ws = workspace if workspace is not None else sr_dense_workspace(dc, ns, nh, n, bits.device)
+    x = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    opt = _lib.SROptions(float(shift), 0.0, 0.0, 0, 0, float(rhs_prefactor))
+    res = _lib.SRResult()
+    w = sample_weights(probs, n, bits.device)
+    allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_pd else ()
+    call("qes_sr_solve_dense", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), ptr(w), C.byref(opt), ptr(x),
+         C.byref(res), ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
+    info = {"iterations": 0, "converged": bool(res.converged), "residual": res.residual, "rhs_norm": res.rhs_norm,
+            "e_mean": complex(res.e_mean_re, res.e_mean_im), "true_residual": res.true_residual}
+    return x, info, ws
+
+
+def sr_dense_workspace_bytes(flat_params, ns, nh, n, gram_only=False):
+    nb = C.c_size_t(0)
+    call("qes_sr_dense_workspace_bytes", dtype_code(flat_params), ns, nh, int(n), 1 if gram_only else 0,
+         C.byref(nb))
+    return int(nb.value)

@@ -299,13 +299,14 @@ class NQS:
         its results (the reference's chunking-invariance test); the kernels here need no chunking.
         Every option whose effect is not implemented raises (no silent drop): other ODE integrators or
         optimisers, phase and named schedulers, early stopping, excited states (``lower_states``),
-        regularisation, symmetrisation, preconditioners, other linear solvers, a formed S matrix."""
+        regularisation, symmetrisation, preconditioners, other linear solvers.  ``lin_force_mat=True``
+        forms S on the tensor cores and solves it by a float64 Cholesky factorisation."""
         unsupported = {
             "ode_solver": ode_solver not in ("Euler", "euler", None),
             "optimizer": optimizer not in ("sgd", "SGD", None),
             "phases": phases is not None, "early_stopper": early_stopper is not None,
             "lower_states": bool(lower_states), "reg_scheduler": reg_scheduler is not None,
-            "reg": bool(reg), "lin_sigma": lin_sigma is not None, "lin_force_mat": bool(lin_force_mat),
+            "reg": bool(reg), "lin_sigma": lin_sigma is not None,
             "symmetrize": bool(symmetrize), "update_kwargs": bool(update_kwargs), "n_update": n_update is not None,
             "background": bool(background), "exact_method": exact_method is not None,
             "pre_solver": pre_solver not in (None, "identity", "none"),
@@ -337,7 +338,8 @@ class NQS:
         else:
             self._tdvp = TDVP(use_sr=use_sr, use_minsr=use_minsr, rhs_prefactor=rhs_prefactor, sr_lin_solver=lin_solver,
                               sr_diag_shift=diag_shift, sr_tol=sr_tol, sr_maxiter=sr_maxiter, grad_clip=grad_clip,
-                              sr_lin_solver_t="gram" if lin_is_gram else "matvec")
+                              sr_lin_solver_t="gram" if lin_is_gram else "matvec",
+                              sr_form_matrix=bool(lin_force_mat))
         stats = NQSTrainStats(seed=self._seed)
         if exact_predictions is not None:
             stats.exact_predictions = np.atleast_1d(np.asarray(exact_predictions))

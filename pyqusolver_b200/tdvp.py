@@ -38,6 +38,7 @@ class TDVPStepInfo:
 
 
 _SOLVERS_CG = ("scipy_cg", "cg")
+_SOLVERS_DIRECT = ("cholesky", "direct", "scipy_direct", "solve")
 
 
 class TDVP:
@@ -55,14 +56,21 @@ class TDVP:
                  backend="default", logger=None, use_timing=False, dtype=None, grad_clip=None, verbose=False,
                  sr_tol=1e-8, sr_atol=0.0, check_every=16, use_old_result=False):
         solver = "scipy_cg" if sr_lin_solver is None else str(getattr(sr_lin_solver, "name", sr_lin_solver)).lower()
-        if solver not in _SOLVERS_CG:
-            raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG (scipy_cg)")
+        if solver not in _SOLVERS_CG + _SOLVERS_DIRECT:
+            raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG (scipy_cg) "
+                                      f"and, on the formed matrix, a Cholesky solve")
         if sr_precond not in (None, "identity", "none"):
             raise NotImplementedError(f"preconditioner {sr_precond!r} is not implemented on the GPU path")
         if str(sr_lin_solver_t).lower() not in ("gram", "matvec", "matrix_free"):
             raise NotImplementedError(f"solver form {sr_lin_solver_t!r}: the GPU path applies S matrix-free")
-        if sr_form_matrix:
-            raise NotImplementedError("sr_form_matrix=True is not implemented on the GPU path")
+        if solver in _SOLVERS_DIRECT and not sr_form_matrix:
+            raise ValueError(f"linear solver {sr_lin_solver!r} needs the formed matrix (sr_form_matrix=True)")
+        if sr_form_matrix and use_minsr:
+            raise NotImplementedError("sr_form_matrix with MinSR (the Ns x Ns matrix) is not implemented")
+        # formed matrix: S on the tensor cores, solved by a float64 Cholesky factorisation (the CG
+        # solution it stands for is the same solution to within the CG tolerance)
+        self.form_matrix = bool(sr_form_matrix)
+        self._dense_ws = None
         if regularization:
             raise NotImplementedError("regularization != 0 is not implemented on the GPU path")
         self.use_sr = bool(use_sr)
@@ -121,6 +129,14 @@ class TDVP:
             F = dv.sr_force(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, workspace=ws, probs=probs)
             x = -(F * self.rhs_prefactor) if self.rhs_prefactor != 1.0 else -F
             self.last_info = {"iterations": 0, "converged": True, "residual": 0.0}
+        elif self.form_matrix:
+            x, info, self._dense_ws = dv.sr_solve_dense(
+                net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
+                rhs_prefactor=self.rhs_prefactor, probs=probs,
+                workspace=self._dense_ws if self._dense_ws is not None and self._dense_ws.numel() >=
+                dv.sr_dense_workspace_bytes(net.flat, net.ns, net.nh, n) else None)
+            self.last_info = info
+            self._solution = x.detach().clone()
         elif self.use_minsr:
             x, info, self._minsr_ws = dv.sr_solve_minsr(
                 net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift, rtol=self.sr_tol,

@@ -257,14 +257,14 @@ __global__ void __launch_bounds__(G_THREADS, 1) dense_gram_kernel(int n_rb, int 
 }
 
 // g vectors of one solve (one block): gw_s = p_s / Ns (-> conj(O-bar)), ge_s = p_s (E_s - <E>) / Ns
-// (-> F), with <E> = sum p E / Ns written to emean[0..1]
+// (-> F), with <E> = sum p E / Ns written to emean[0..1]; eloc == nullptr (the Gram-only call): gw only
 __global__ void __launch_bounds__(1024) dense_g_kernel(int64_t n, const float2* __restrict__ eloc,
                                                         const float* __restrict__ wts, double2* __restrict__ gw,
                                                         double2* __restrict__ ge, double* __restrict__ emean) {
   __shared__ double rr[32], ri[32];
   __shared__ double m[2];
   double sr = 0.0, si = 0.0;
-  for (int64_t s = threadIdx.x; s < n; s += blockDim.x) {
+  for (int64_t s = threadIdx.x; eloc && s < n; s += blockDim.x) {      // no E_loc in the Gram-only call
     const double f = wts ? (double)wts[s] : 1.0;
     sr += f * eloc[s].x;
     si += f * eloc[s].y;

@@ -484,6 +484,19 @@ int qes_ed_matvec(int ns, const qes_hamiltonian* ham, const double* x, double* y
 int qes_ed_lanczos(int ns, const qes_hamiltonian* ham, int max_iter, double tol, uint64_t seed,
                    double* e0_out, int* iterations_out, void* workspace, size_t workspace_bytes,
                    void* stream);
+/* Lanczos in one S^z sector (n_up up spins) of an S^z-conserving Hamiltonian (anti-parallel pair
+ * moves only), optionally restricted further to one spin-flip parity (+1 / -1; needs ns = 2 n_up
+ * and no z field): the basis is indexed by the colex rank of the bit-packed state (the lower
+ * ns - 1 sites with parity, a state and its flip sharing one basis vector), so no index table is
+ * stored and the vectors hold C(ns, n_up) (or C(ns - 1, n_up)) float64 entries.  ns <= 62,
+ * n_up <= 32.  Workspace from qes_ed_sector_workspace_bytes; qes_ed_sector_dim gives the
+ * dimension.  Replaces model.diagonalize(method='lanczos') on a symmetry sector
+ * (QES/Algebra/hamil.py:1809+, QES/Algebra/Hamil/hamil_diag_engine.py:176-305).              */
+int qes_ed_sector_dim(int ns, int n_up, int parity, uint64_t* dim);
+int qes_ed_sector_workspace_bytes(int ns, int n_up, int parity, size_t* bytes);
+int qes_ed_lanczos_sector(int ns, int n_up, int parity, const qes_hamiltonian* ham, int max_iter,
+                          double tol, uint64_t seed, double* e0_out, int* iterations_out,
+                          void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Batched independent problems.  Many (RBM, Hamiltonian, chain set) triples

@@ -10,9 +10,10 @@ first call raises.
 
 from .lattice import SquareLattice, get_neighbor_table
 from .hilbert import HilbertSpace
-from .hamiltonian import TransverseFieldIsing, XXZ, J1J2Model, SpinHamiltonian
+from .hamiltonian import TransverseFieldIsing, XXZ, J1J2Model, SpinHamiltonian, SpinOperator
 
 __all__ = [
+    "SpinOperator",
     "SquareLattice", "get_neighbor_table", "HilbertSpace", "TransverseFieldIsing", "XXZ", "J1J2Model",
     "SpinHamiltonian", "RBM", "VMCSampler", "TDVP", "NQS", "NQSSingleStepResult", "NQSTrainStats", "NQSBatch",
 ]

@@ -148,6 +148,10 @@ SIGNATURES = {
     "qes_param_update": [C.c_int, _i64, C.c_double, _vp, _vp, _vp, _vp],
     "qes_swap_region": [_i64, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp],
     "qes_ed_workspace_bytes": [C.c_int, C.POINTER(_sz)],
+    "qes_ed_sector_dim": [C.c_int, C.c_int, C.c_int, C.POINTER(_u64)],
+    "qes_ed_sector_workspace_bytes": [C.c_int, C.c_int, C.c_int, C.POINTER(_sz)],
+    "qes_ed_lanczos_sector": [C.c_int, C.c_int, C.c_int, C.POINTER(Hamiltonian), C.c_int, C.c_double, _u64,
+                              C.POINTER(C.c_double), C.POINTER(C.c_int), _vp, _sz, _vp],
     "qes_ed_matvec": [C.c_int, C.POINTER(Hamiltonian), _vp, _vp, _vp],
     "qes_ed_lanczos": [C.c_int, C.POINTER(Hamiltonian), C.c_int, C.c_double, _u64, C.POINTER(C.c_double),
                        C.POINTER(C.c_int), _vp, _sz, _vp],

@@ -289,3 +289,217 @@ extern "C" int qes_ed_lanczos(int ns, const qes_hamiltonian* ham, int max_iter, 
   if (iterations_out) *iterations_out = it;
   return conv ? QES_OK : QES_ERR_NOT_CONVERGED;
 }
+
+// ================================================================================================
+// S^z sector (and spin-flip parity) Lanczos
+// ================================================================================================
+// Basis: the states of ns sites with n_up up spins, indexed by their colex rank
+//   rank(s) = sum_k C(p_k, k + 1),  p_0 < p_1 < ... the positions of the set bits,
+// so that a state is found from its bits and back in O(n_up) with a binomial table (no lookup
+// array).  With spin-flip parity (ns = 2 n_up, no z field) a state and its flip ~s are one
+// basis vector; the representative is the one whose top site (ns - 1) is down, i.e. the
+// n_up-subsets of the lower ns - 1 sites, and psi(~s) = parity * psi(s).  The Hamiltonian must
+// conserve S^z: pair moves of anti-parallel spins only (no single flips, no pair flips of parallel
+// spins, which the lowering drops for the isotropic models).
+constexpr int ED_BINOM_N = 65, ED_BINOM_K = 33;
+
+struct EdSector {
+  int ns, n_up, bits;        // bits: ns, or ns - 1 with spin-flip parity (the representatives' range)
+  int parity;                // 0: none, +1 / -1: spin-flip parity
+};
+
+__device__ __forceinline__ uint64_t ed_rank(uint64_t s, int n_up, const uint64_t* __restrict__ C) {
+  uint64_t r = 0;
+  for (int k = 0; k < n_up; ++k) {
+    const int p = __ffsll((long long)s) - 1;
+    r += C[p * ED_BINOM_K + k + 1];
+    s &= s - 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint64_t ed_unrank(uint64_t r, int n_up, int bits, const uint64_t* __restrict__ C) {
+  uint64_t s = 0;
+  int p = bits - 1;
+  for (int k = n_up; k >= 1; --k) {
+    while (C[p * ED_BINOM_K + k] > r) --p;           // largest p with C(p, k) <= r
+    r -= C[p * ED_BINOM_K + k];
+    s |= 1ull << p;
+    --p;
+  }
+  return s;
+}
+
+__global__ void __launch_bounds__(ED_THREADS) ed_sector_matvec_kernel(
+    EdSector sec, uint64_t dim, EdTerms nt, const int32_t* __restrict__ mi, const int32_t* __restrict__ mj,
+    const float4* __restrict__ mcoef, const int32_t* __restrict__ zf_site, const float* __restrict__ zf_h,
+    const int32_t* __restrict__ zz_i, const int32_t* __restrict__ zz_j, const float* __restrict__ zz_J,
+    const uint64_t* __restrict__ binom, const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ uint64_t C[ED_BINOM_N * ED_BINOM_K];
+  __shared__ uint64_t s_mask[ED_MAX_TERMS];
+  __shared__ int2 s_ij[ED_MAX_TERMS];
+  __shared__ float s_c[ED_MAX_TERMS];
+  __shared__ int2 s_zz[ED_MAX_TERMS];
+  __shared__ float s_zzJ[ED_MAX_TERMS];
+  __shared__ int s_zf[ED_MAX_TERMS];
+  __shared__ float s_zfh[ED_MAX_TERMS];
+  for (int t = threadIdx.x; t < ED_BINOM_N * ED_BINOM_K; t += blockDim.x) C[t] = binom[t];
+  for (int k = threadIdx.x; k < nt.n_moves; k += blockDim.x) {
+    const int i = mi[k], j = mj[k];
+    s_mask[k] = (1ull << i) | (1ull << j);
+    s_ij[k] = make_int2(i, j);
+    s_c[k] = mcoef[k].x;
+  }
+  for (int t = threadIdx.x; t < nt.n_zz; t += blockDim.x) { s_zz[t] = make_int2(zz_i[t], zz_j[t]); s_zzJ[t] = zz_J[t]; }
+  for (int t = threadIdx.x; t < nt.n_zf; t += blockDim.x) { s_zf[t] = zf_site[t]; s_zfh[t] = zf_h[t]; }
+  __syncthreads();
+  const uint64_t full = (sec.ns == 64) ? ~0ull : ((1ull << sec.ns) - 1ull);
+  const uint64_t top = 1ull << (sec.ns - 1);
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < dim; r += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = ed_unrank(r, sec.n_up, sec.bits, C);
+    double d = 0.0;
+    for (int t = 0; t < nt.n_zf; ++t) d += (double)s_zfh[t] * (((s >> s_zf[t]) & 1ull) ? 1.0 : -1.0);
+    for (int t = 0; t < nt.n_zz; ++t) {
+      const int2 p = s_zz[t];
+      d += (double)s_zzJ[t] * ((((s >> p.x) ^ (s >> p.y)) & 1ull) ? -1.0 : 1.0);
+    }
+    double acc = d * x[r];
+    for (int k = 0; k < nt.n_moves; ++k) {
+      const int2 p = s_ij[k];
+      if (((s >> p.x) ^ (s >> p.y)) & 1ull) {           // anti-parallel: the exchange is allowed
+        uint64_t t2 = s ^ s_mask[k];
+        double f = (double)s_c[k];
+        if (sec.parity != 0 && (t2 & top)) {             // back to the representative of {t2, ~t2}
+          t2 = ~t2 & full;
+          f *= (double)sec.parity;
+        }
+        acc += f * x[ed_rank(t2, sec.n_up, C)];
+      }
+    }
+    y[r] = acc;
+  }
+}
+
+namespace {
+void ed_binomials(std::vector<uint64_t>& C) {
+  C.assign((size_t)ED_BINOM_N * ED_BINOM_K, 0ull);
+  for (int n = 0; n < ED_BINOM_N; ++n) {
+    C[(size_t)n * ED_BINOM_K] = 1ull;
+    for (int k = 1; k < ED_BINOM_K && k <= n; ++k)
+      C[(size_t)n * ED_BINOM_K + k] = C[(size_t)(n - 1) * ED_BINOM_K + k - 1] +
+                                       (k <= n - 1 ? C[(size_t)(n - 1) * ED_BINOM_K + k] : 0ull);
+  }
+}
+
+int ed_sector_dims(int ns, int n_up, int parity, uint64_t* dim, EdSector* sec) {
+  QES_ARG_CHECK(ns > 0 && ns <= 62 && n_up >= 0 && n_up <= ns && n_up < ED_BINOM_K,
+                "qes_ed_sector: need 0 < ns <= 62 and n_up <= 32");
+  QES_ARG_CHECK(parity == 0 || ((parity == 1 || parity == -1) && 2 * n_up == ns),
+                "qes_ed_sector: spin-flip parity needs ns = 2 n_up");
+  std::vector<uint64_t> C;
+  ed_binomials(C);
+  const int bits = parity ? ns - 1 : ns;
+  *dim = C[(size_t)bits * ED_BINOM_K + n_up];
+  if (sec) *sec = EdSector{ns, n_up, bits, parity};
+  return QES_OK;
+}
+}  // namespace
+
+extern "C" int qes_ed_sector_dim(int ns, int n_up, int parity, uint64_t* dim) {
+  QES_ARG_CHECK(dim, "qes_ed_sector_dim: null output");
+  return ed_sector_dims(ns, n_up, parity, dim, nullptr);
+}
+
+extern "C" int qes_ed_sector_workspace_bytes(int ns, int n_up, int parity, size_t* bytes) {
+  QES_ARG_CHECK(bytes, "qes_ed_sector_workspace_bytes: null output");
+  uint64_t dim = 0;
+  int rc = ed_sector_dims(ns, n_up, parity, &dim, nullptr);
+  if (rc) return rc;
+  *bytes = 3 * (size_t)dim * sizeof(double) + ED_BLOCKS * sizeof(double) +
+           (size_t)ED_BINOM_N * ED_BINOM_K * sizeof(uint64_t) + 256;
+  return QES_OK;
+}
+
+extern "C" int qes_ed_lanczos_sector(int ns, int n_up, int parity, const qes_hamiltonian* ham, int max_iter,
+                                     double tol, uint64_t seed, double* e0_out, int* iterations_out,
+                                     void* workspace, size_t workspace_bytes, void* stream) {
+  QES_ARG_CHECK(ham && e0_out && max_iter >= 2 && tol > 0.0, "qes_ed_lanczos_sector: bad args");
+  QES_ARG_CHECK(ham->n_moves >= 0 && ham->n_moves <= ED_MAX_TERMS && ham->n_zz <= ED_MAX_TERMS &&
+                    ham->n_zfield <= ED_MAX_TERMS,
+                "qes_ed_lanczos_sector: too many terms");
+  uint64_t dim = 0;
+  EdSector sec{};
+  int rc = ed_sector_dims(ns, n_up, parity, &dim, &sec);
+  if (rc) return rc;
+  QES_ARG_CHECK(dim >= 1, "qes_ed_lanczos_sector: empty sector");
+  QES_ARG_CHECK(!(parity != 0 && ham->n_zfield > 0), "qes_ed_lanczos_sector: a z field breaks the spin-flip parity");
+  size_t need = 0;
+  qes_ed_sector_workspace_bytes(ns, n_up, parity, &need);
+  if (!workspace || workspace_bytes < need) {
+    qes_set_last_message("qes_ed_lanczos_sector: workspace too small");
+    return QES_ERR_WORKSPACE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  // S^z conservation and real matrix elements: anti-parallel pair moves only, real coefficients
+  if (ham->n_moves > 0) {
+    std::vector<float> c((size_t)ham->n_moves * 4);
+    std::vector<int32_t> kind(ham->n_moves);
+    QES_CUDA_CHECK(cudaMemcpyAsync(c.data(), ham->move_coef, c.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    QES_CUDA_CHECK(cudaMemcpyAsync(kind.data(), ham->move_kind, kind.size() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                   st));
+    QES_CUDA_CHECK(cudaStreamSynchronize(st));
+    for (int k = 0; k < ham->n_moves; ++k) {
+      QES_ARG_CHECK(kind[k] == QES_MOVE_PAIR_ANTI, "qes_ed_lanczos_sector: the Hamiltonian does not conserve S^z");
+      QES_ARG_CHECK(c[4 * k + 1] == 0.f && c[4 * k + 2] == 0.f && c[4 * k + 3] == 0.f,
+                    "qes_ed_lanczos_sector: complex matrix elements");
+    }
+  }
+  double* v = (double*)workspace;
+  double* vp = v + dim;
+  double* w = vp + dim;
+  double* part = w + dim;
+  uint64_t* binom = reinterpret_cast<uint64_t*>(part + ED_BLOCKS);
+  std::vector<uint64_t> C;
+  ed_binomials(C);
+  QES_CUDA_CHECK(cudaMemcpyAsync(binom, C.data(), C.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  std::vector<double> hpart(ED_BLOCKS), alpha, beta;
+  ed_init_kernel<<<ED_BLOCKS, ED_THREADS, 0, st>>>(dim, (uint32_t)seed, (uint32_t)(seed >> 32), v, vp, part);
+  QES_LAUNCH_CHECK();
+  double nrm2 = 0.0;
+  if ((rc = ed_sum(part, hpart.data(), st, &nrm2))) return rc;
+  ed_scale_kernel<<<ED_BLOCKS, ED_THREADS, 0, st>>>(dim, 1.0 / sqrt(nrm2), v);
+  QES_LAUNCH_CHECK();
+  const EdTerms nt{ham->n_moves, ham->n_zz, ham->n_zfield};
+  double e_prev = 0.0, e = 0.0, b_prev = 0.0;
+  int it = 0;
+  bool conv = false;
+  for (; it < max_iter; ++it) {
+    ed_sector_matvec_kernel<<<ED_BLOCKS, ED_THREADS, 0, st>>>(sec, dim, nt, ham->move_i, ham->move_j,
+                                                              (const float4*)ham->move_coef, ham->zf_site, ham->zf_h,
+                                                              ham->zz_i, ham->zz_j, ham->zz_J, binom, v, w);
+    ed_dot_kernel<<<ED_BLOCKS, ED_THREADS, 0, st>>>(dim, v, w, part);
+    QES_LAUNCH_CHECK_N(2);
+    double a = 0.0;
+    if ((rc = ed_sum(part, hpart.data(), st, &a))) return rc;
+    alpha.push_back(a);
+    ed_axpy_norm_kernel<<<ED_BLOCKS, ED_THREADS, 0, st>>>(dim, a, b_prev, v, vp, w, part);
+    QES_LAUNCH_CHECK();
+    double b2 = 0.0;
+    if ((rc = ed_sum(part, hpart.data(), st, &b2))) return rc;
+    const double b = sqrt(b2);
+    e = tridiag_lowest(alpha, beta);
+    if ((it >= 8 && fabs(e - e_prev) <= tol * std::max(1.0, fabs(e))) || b <= 1e-12 * std::max(1.0, fabs(e))) {
+      conv = true;
+      ++it;
+      break;
+    }
+    e_prev = e;
+    beta.push_back(b);
+    ed_shift_kernel<<<ED_BLOCKS, ED_THREADS, 0, st>>>(dim, 1.0 / b, vp, v, w);
+    QES_LAUNCH_CHECK();
+    b_prev = b;
+  }
+  *e0_out = e;
+  if (iterations_out) *iterations_out = it;
+  return conv ? QES_OK : QES_ERR_NOT_CONVERGED;
+}

@@ -294,13 +294,12 @@ __global__ void __launch_bounds__(1024) dense_g_kernel(int64_t n, const float2* 
 
 // A = S + shift I with S from the Gram tiles (float64, full Hermitian, row-major P x P):
 // complex S_pq = (G[p][q] + G[P+p][P+q] + i (G[p][P+q] - G[P+p][q])) / Ns, real S_pq = G[p][q] / Ns.
-// Only the tiles (I <= J) of G were formed; an element below them is read from its mirror.
+// Only the tiles (I <= J) of G were formed; every element is read from the upper triangle
+// (a <= b; the mirror below it), so S comes out exactly Hermitian.
 template <class V>
 __global__ void dense_combine_kernel(int64_t P, int64_t ldg, const float* __restrict__ G, double inv_n,
                                      double shift, V* __restrict__ A) {
-  auto g = [&](int64_t a, int64_t b) -> double {
-    return (double)((a / GR <= b / GR) ? G[a * ldg + b] : G[b * ldg + a]);
-  };
+  auto g = [&](int64_t a, int64_t b) -> double { return (double)((a <= b) ? G[a * ldg + b] : G[b * ldg + a]); };
   const int64_t total = P * P;
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
        idx += (int64_t)gridDim.x * blockDim.x) {

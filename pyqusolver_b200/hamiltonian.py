@@ -133,8 +133,10 @@ class SpinHamiltonian:
 
     # -- exact ground energy -------------------------------------------------------------
     def diagonalize(self, method: str = "lanczos", k: int = 1, tol: float = 1e-12, maxiter: int = 600,
-                    seed: int = 7, **kwargs):
-        """Ground energy by Lanczos on the GPU over the full 2^ns basis (``qes_ed_lanczos``).
+                    seed: int = 7, n_up=None, spin_flip=None, **kwargs):
+        """Ground energy by Lanczos on the GPU (``qes_ed_lanczos``: the full 2^ns basis; with ``n_up``,
+        ``qes_ed_lanczos_sector``: the S^z sector of n_up up spins, and with ``spin_flip`` = +1 / -1
+        also one spin-flip parity, for S^z-conserving models without a field).
 
         Mirrors ``model.diagonalize(method='lanczos')`` (``QES/Algebra/hamil.py:1809``) for the
         lowest eigenvalue: the result is stored in ``eig_val`` (ascending, length 1).
@@ -147,6 +149,20 @@ class SpinHamiltonian:
         import torch
         from . import _lib, device as dv
         dh = dv.DeviceHamiltonian(self.lower())
+        if n_up is not None or spin_flip is not None:
+            n_up = self.ns // 2 if n_up is None else int(n_up)
+            parity = 0 if spin_flip in (None, 0) else (1 if int(spin_flip) > 0 else -1)
+            nb = C.c_size_t(0)
+            _lib.call("qes_ed_sector_workspace_bytes", self.ns, n_up, parity, C.byref(nb))
+            ws = torch.empty((int(nb.value),), dtype=torch.uint8, device="cuda")
+            e0, its = C.c_double(0.0), C.c_int(0)
+            _lib.call("qes_ed_lanczos_sector", self.ns, n_up, parity, C.byref(dh.struct), int(maxiter), float(tol),
+                      C.c_uint64(int(seed)), C.byref(e0), C.byref(its), _lib.ptr(ws), int(ws.numel()),
+                      _lib.stream_ptr())
+            del ws
+            self._eig_val = np.array([e0.value])
+            self.lanczos_iterations = its.value
+            return self._eig_val
         nb = C.c_size_t(0)
         _lib.call("qes_ed_workspace_bytes", self.ns, C.byref(nb))
         ws = torch.empty((int(nb.value),), dtype=torch.uint8, device="cuda")
@@ -336,3 +352,43 @@ class J1J2Model(SpinHamiltonian):
                         continue
                     phase = lattice.boundary_phase_from_winding(*lattice.bond_winding(i, j))
                     exch(-phase * self._j2[i], i, int(j))
+
+
+class SpinOperator(SpinHamiltonian):
+    """A spin-1/2 operator on a lattice as an ordered term list, evaluated by the same lowering and
+    ratio kernel as the models (observables of ``NQS.compute_observable`` / ``NQS.measure``).
+
+    Terms use the reference's operator conventions (X flips with 0.5**k, Y flips with prod(i 0.5 sigma)
+    on the state before the flip, Z keeps the state with prod(0.5 sigma);
+    ``QES/Algebra/Operator/impl/jax/operators_spin.py:131-143,220-248,353-370``); z terms act on one or
+    two sites, x / y terms flip one or two sites.  The constructors below build the common ones."""
+
+    def __init__(self, lattice, terms=(), name="O", **kwargs):
+        super().__init__(lattice, **kwargs)
+        self.name = name
+        for op, mult, sites in terms:
+            self.add(op, mult, sites)
+
+    @classmethod
+    def sigma(cls, lattice, op, site, mult=1.0):
+        """S^op on one site (op in x, y, z)."""
+        return cls(lattice, [(op, mult, (site,))], name=f"S{op}_{site}")
+
+    @classmethod
+    def magnetization(cls, lattice, op="z"):
+        """(1 / N) sum_i S^op_i."""
+        return cls(lattice, [(op, 1.0 / lattice.ns, (i,)) for i in range(lattice.ns)], name=f"M{op}")
+
+    @classmethod
+    def correlation(cls, lattice, i, j, op="z"):
+        """S^op_i S^op_j (i != j)."""
+        if i == j:
+            raise ValueError("correlation needs two distinct sites")
+        return cls(lattice, [(op, 1.0, (i, j))], name=f"S{op}{op}_{i}_{j}")
+
+    @classmethod
+    def exchange(cls, lattice, i, j):
+        """S_i . S_j = SxSx + SySy + SzSz on two distinct sites."""
+        if i == j:
+            raise ValueError("exchange needs two distinct sites")
+        return cls(lattice, [("x", 1.0, (i, j)), ("y", 1.0, (i, j)), ("z", 1.0, (i, j))], name=f"SS_{i}_{j}")

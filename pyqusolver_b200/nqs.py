@@ -62,6 +62,28 @@ class NQSTrainStats:
         return self.history[-1] if self.history else None
 
 
+@dataclass
+class NQSObservable:
+    """Local values and statistics of one observable (the fields of the reference's ``NQSObservable``,
+    ``QES/NQS/src/nqs_engine.py:231-300``)."""
+    values: Any
+    mean: Any = None
+    std: Optional[float] = None
+    variance: Optional[float] = None
+    error_of_mean: Optional[float] = None
+    min_val: Optional[float] = None
+    max_val: Optional[float] = None
+    n_samples: int = 0
+    observable_name: str = ""
+    backend_used: str = "cuda"
+    has_stats: bool = True
+
+    def summary(self):
+        return {"name": self.observable_name, "expectation": self.mean, "std": self.std, "min": self.min_val,
+                "max": self.max_val, "variance": self.variance, "error_of_mean": self.error_of_mean,
+                "n_samples": self.n_samples}
+
+
 class NQS:
     def __init__(self, logansatz="rbm", model: SpinHamiltonian = None, hilbert=None, *, sampler="vmc",
                  batch_size=None, backend="cuda", dtype=np.complex64, param_dtype=None, seed=0, alpha=1.0,
@@ -184,6 +206,87 @@ class NQS:
             return (tr, err) if return_error else tr
         s2 = -np.log(max(tr, min_swap_value))
         return (s2, err / max(tr, min_swap_value)) if return_error else s2
+
+    # ------------------------------------------------------------------ observables
+    def _observable_device(self, op):
+        cache = self.__dict__.setdefault("_obs_cache", {})
+        ent = cache.get(id(op))
+        if ent is None or ent[0] is not op:
+            ent = (op, dv.DeviceHamiltonian(op.lower(), self._net.device))
+            cache[id(op)] = ent
+        return ent[1]
+
+    def local_values(self, op, bits, tanh_theta=None):
+        """Local values O_loc(s) = sum_s' conj(<s'|O|s>) psi(s') / psi(s) of a lowered spin operator (the
+        local-energy kernel with the operator's own move tables), complex64 per sample."""
+        if not isinstance(op, SpinHamiltonian):
+            raise TypeError("observables on the GPU path are SpinOperator / model instances (a Python callable "
+                            "of the reference's form has no device evaluation here)")
+        if op.ns != self._net.ns:
+            raise ValueError("observable acts on a different number of sites")
+        net = self._net
+        if tanh_theta is None:
+            _, tanh_theta, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+        h = self._observable_device(op)
+        tables = dv.move_tables(net.flat, net.ns, net.nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+        return dv.local_energy(net.flat, net.ns, net.nh, bits, tanh_theta, h, tables)
+
+    def compute_observable(self, states=None, ansatze=None, functions=None, names=None, *, params=None,
+                           probabilities=None, batch_size=None, num_samples=None, num_chains=None, return_stats=True,
+                           return_values=False, args=None, **kwargs):
+        """Observables on sampled (or given) configurations (``QES/NQS/nqs.py:1565-1600`` ->
+        ``nqs_engine.py:543-660``): local values O_loc(s) on states drawn from |psi|^2 (the NQS sampler
+        when ``states`` is None), mean and std weighted by ``probabilities`` when given.  ``functions``
+        is one operator or a list (SpinOperator or a model); returns one NQSObservable, a list of them,
+        or the value arrays with ``return_values``."""
+        if args is not None:
+            raise NotImplementedError("observable arguments: build one SpinOperator per argument instead")
+        if functions is None or (isinstance(functions, (list, tuple)) and len(functions) == 0):
+            raise ValueError("At least one observable function must be provided")
+        if params is not None:
+            self.set_params(params)
+        single = not isinstance(functions, (list, tuple))
+        ops = [functions] if single else list(functions)
+        net = self._net
+        if states is None:
+            if num_chains is not None:
+                self._sampler.set_numchains(num_chains)
+            bits, lp = self._sampler.sample_bits(num_samples)
+            if probabilities is None:
+                probabilities = self._sampler.sample_probs(lp)
+        else:
+            bits = net.bits(states)
+        _, tn, _ = dv.rbm_forward(net.flat, net.ns, net.nh, bits, theta=False, tanh=True, logpsi=False)
+        w = None if probabilities is None else dv.sample_weights(probabilities, int(bits.shape[0]), bits.device)
+        out, vals = [], []
+        for k, op in enumerate(ops):
+            v = self.local_values(op, bits, tn)
+            vals.append(v)
+            if return_values:
+                continue
+            st = dv.loss_stats(v, w).cpu().numpy()
+            n = int(v.shape[0])
+            vr = v.real
+            name = names[k] if isinstance(names, (list, tuple)) else (names if isinstance(names, str) else
+                                                                     getattr(op, "name", f"O_{k}"))
+            out.append(NQSObservable(values=v, mean=complex(st[0], st[1]), std=float(st[3]),
+                                     variance=float(st[2]), error_of_mean=float(st[3]) / np.sqrt(max(n, 1)),
+                                     min_val=float(vr.min()), max_val=float(vr.max()), n_samples=n,
+                                     observable_name=name, has_stats=bool(return_stats)))
+        if return_values:
+            return vals[0] if single else vals
+        return out[0] if single else out
+
+    expectation = compute_observable
+
+    def measure(self, observables, **kwargs):
+        """One operator, a list, or a mapping name -> operator (then a dict of results keyed by name);
+        ``QES/NQS/nqs.py:1602-1660``."""
+        if isinstance(observables, dict):
+            names = list(observables.keys())
+            res = self.compute_observable(functions=list(observables.values()), names=names, **kwargs)
+            return {n: r for n, r in zip(names, res)}
+        return self.compute_observable(functions=observables, **kwargs)
 
     # ------------------------------------------------------------------ checkpoints
     def save_checkpoint(self, directory, step, metadata=None, stats: Optional["NQSTrainStats"] = None):

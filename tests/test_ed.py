@@ -64,3 +64,38 @@ def test_ed_rejects_large_or_bad_input():
     model = qb.TransverseFieldIsing(qb.SquareLattice(1, 40, 1, bc="pbc"), j=1.0, hx=1.0, hz=0.0)
     with pytest.raises(_lib.QESError):
         model.diagonalize()
+
+
+# ------------------------------------------------------------------------- S^z sectors and spin-flip parity
+@pytest.mark.gpu
+def test_sector_lanczos_matches_oracle_and_full_basis():
+    """S^z-sector Lanczos (colex-ranked basis) against the oracle's sector ED, and the spin-flip
+    parities against the sector: min over parities = the sector's ground energy."""
+    L, OL = qb.SquareLattice(2, 4, 4), olat.SquareLattice(2, 4, 4)
+    model = qb.J1J2Model(L, J1=-1.0, J2=-0.5)
+    terms = oH.j1j2_terms(OL, -1.0, -0.5)
+    e8 = float(model.diagonalize(n_up=8)[0])
+    assert e8 == pytest.approx(oed.ground_energy(terms, 16, n_up=8), rel=1e-8)
+    e7 = float(model.diagonalize(n_up=7)[0])
+    assert e7 == pytest.approx(oed.ground_energy(terms, 16, n_up=7), rel=1e-8)
+    ep = float(model.diagonalize(n_up=8, spin_flip=+1)[0])
+    em = float(model.diagonalize(n_up=8, spin_flip=-1)[0])
+    assert min(ep, em) == pytest.approx(e8, rel=1e-8) and max(ep, em) >= e8 - 1e-9
+    full = float(model.diagonalize()[0])
+    assert min(e8, e7) == pytest.approx(full, rel=1e-8) or full < min(e8, e7)
+
+
+@pytest.mark.gpu
+def test_sector_lanczos_xxz_chain_all_sectors():
+    L, OL = qb.SquareLattice(1, 12), olat.SquareLattice(1, 12)
+    model = qb.XXZ(L, jxy=-1.0, jz=-0.6, hz=0.3)
+    terms = oH.xxz_terms(OL, -1.0, -0.6, hz=0.3)
+    es = [float(model.diagonalize(n_up=u)[0]) for u in range(13)]
+    for u in (0, 3, 6, 11):
+        assert es[u] == pytest.approx(oed.ground_energy(terms, 12, n_up=u), rel=1e-8, abs=1e-10)
+    assert min(es) == pytest.approx(float(model.diagonalize()[0]), rel=1e-8)
+    with pytest.raises(_lib.QESError):
+        model.diagonalize(n_up=6, spin_flip=1)             # a z field breaks the spin-flip parity
+    tfim = qb.TransverseFieldIsing(L, j=1.0, hx=0.5, hz=0.0)
+    with pytest.raises(_lib.QESError):
+        tfim.diagonalize(n_up=6)                           # single flips do not conserve S^z

@@ -567,7 +567,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         oc["tfim_batch64"] = batch_summary(args.other_steps, 3, flush)
         line["other_configs"] = oc
     if rank == 0 and world == 1 and not args.no_dense:
-        line["dense_sr"] = dense_summary(flush)
+        line["dense_sr"] = dense_summary(flush, names=[n.strip() for n in args.dense_configs.split(",") if n.strip()])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
     if dist is not None:
@@ -1002,6 +1002,8 @@ def main():
                     help="skip the per-workload summaries of tfim16, j1j2_6x6, tfim20x20 and tfim_batch64")
     ap.add_argument("--other-steps", type=int, default=8)
     ap.add_argument("--no-dense", action="store_true", help="skip the formed-S (Gram + Cholesky) summary")
+    ap.add_argument("--dense-configs", default="tfim16,j1j2_6x6,heis10x10",
+                    help="workloads of the formed-S summary")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local_rank = env_rank()

@@ -481,6 +481,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         return float(t.item())
 
     forms = {}
+    tuned = None
     # plain FP32 form: every SR contraction on CUDA cores in float32 (float64 CG vectors)
     # mixed form: SR contractions on tcgen05 tensor cores (BF16 hi/lo split, FP32 accumulate)
     wanted = [f.strip() for f in args.forms.split(",") if f.strip()]
@@ -492,6 +493,17 @@ def run_ours(args, cfg, rank, world, local_rank):
         for _ in range(args.warmup):                        # the first call thermalises the chains
             timed_step(nqs, tdvp, cfg, [torch.cuda.Event(enable_timing=True) for _ in range(7)])
         torch.cuda.synchronize()
+        if form == "mixed" and args.autotune:
+            # tensor-core SR tiling picked by timing the candidates on the current batch (autotune.py)
+            from pyqusolver_b200.autotune import tune_sr_tiling
+            from pyqusolver_b200 import device as dv
+            net = nqs.net
+            bits, _ = nqs.sampler.sample_bits()
+            _, tn, _ = dv.rbm_forward_step(net.flat, net.ns, net.nh, bits, tanh=True, logpsi=False)
+            tuned = tune_sr_tiling(net, bits, tn)
+            for _ in range(2):
+                timed_step(nqs, tdvp, cfg, [torch.cuda.Event(enable_timing=True) for _ in range(7)])
+            torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         clocks = ClockSampler(local_rank) if form == "mixed" else None
@@ -554,7 +566,13 @@ def run_ours(args, cfg, rank, world, local_rank):
         "e2e": e2e,
         "roofline": roof,
         "issue_rooflines": issue_rooflines(cfg, nqs, mixed, mixed["clocks"]),
+        "sr_tiling": ({"choice (mode, nc, ctas, pairs, fused_sv)": tuned["choice"], "matvec_ms": tuned["ms"],
+                       "candidates_ms": tuned["timings"], "cached": tuned["cached"]} if tuned else "automatic"),
     }
+    if tuned:
+        # the tuned tiling is process-wide: the other workloads below run the automatic one
+        from pyqusolver_b200.autotune import apply_tiling
+        apply_tiling(0, 0, 0, 0, 1)
     if rank == 0 and args.accuracy_epochs > 0:
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
     if rank == 0 and args.matched_epochs > 0 and args.config == "heis10x10":
@@ -779,6 +797,8 @@ def kernel_bytes(cfg, nqs, kind, tc):
         return t_bytes + spins + P * vs + n * 8
     if kind == "ohu":         # O^H u: T, spins and u in, one P-vector out
         return t_bytes + spins + n * 8 + P * vs
+    if kind == "sv":          # fused S v: T and spins once, v in, one P-vector out
+        return t_bytes + spins + 2 * P * vs
     return 3 * P * vs         # split reduction: the P-vector out, p in, Ap out
 
 
@@ -848,13 +868,14 @@ def roofline(cfg, nqs, form):
     names = {"ov": "tc_ov_kernel (O v, tcgen05)" if tc else "ov_kernel (O v, CUDA cores)",
              "ohu": "tc_ohu_kernel (O^H u, tcgen05)" if tc else "ohu_kernel (O^H u, CUDA cores)",
              "reduce": "reduce_splits_kernel / cg_fused_kernel", "sample": "sampler_kernel",
+             "sv": "tc_sv_kernel (S v: O v and O^H u fused, tcgen05)",
              "local_energy": "eloc_moves_kernel",
              "forward": "theta_tc_kernel (tcgen05)" if dv.forward_uses_tensor_cores(
                  net.flat, net.ns, net.nh, cfg["chains"] * cfg["samples"]) else "rbm_forward_kernel"}
     out = {"kernel": names.get(dom, dom), "launches_timed": cnt, "avg_launch_us": avg_s * 1e6,
            "share_of_timed_region": total_ms / float(np.sum([np.sum(v) for v in phases.values()])),
            "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src}
-    if dom in ("ov", "ohu", "reduce"):
+    if dom in ("ov", "ohu", "reduce", "sv"):
         b = kernel_bytes(cfg, nqs, dom, tc=tc)
         tr = traffic_db.get(cfg.get("name", ""), {}).get(dom)
     elif dom in ("sample", "local_energy"):
@@ -1001,6 +1022,8 @@ def main():
     ap.add_argument("--no-other-configs", action="store_true",
                     help="skip the per-workload summaries of tfim16, j1j2_6x6, tfim20x20 and tfim_batch64")
     ap.add_argument("--other-steps", type=int, default=8)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the automatic tensor-core SR tiling instead of timing the candidates")
     ap.add_argument("--no-dense", action="store_true", help="skip the formed-S (Gram + Cholesky) summary")
     ap.add_argument("--dense-configs", default="tfim16,j1j2_6x6,heis10x10",
                     help="workloads of the formed-S summary")

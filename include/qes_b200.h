@@ -279,7 +279,17 @@ typedef struct {
     int maxiter;
     int check_every;           /* host convergence check period (iterations) */
     double rhs_prefactor;
+    int precond;               /* QES_PRECOND_NONE, or QES_PRECOND_JACOBI: CG with
+                                  M = 1 / diag(S + shift), diag(S)_k = mean|O_k|^2 -
+                                  |mean O_k|^2 (weighted), SciPy's cg(M=...) semantics
+                                  (the stopping rule stays on ||r||).  The CG solve only;
+                                  MinSR and the batched CG take QES_PRECOND_NONE.
+                                  Replaces the 'jacobi' pre_solver / sr_precond of
+                                  QES/NQS/src/tdvp.py:332,686-710.                    */
 } qes_sr_options;
+
+#define QES_PRECOND_NONE 0
+#define QES_PRECOND_JACOBI 1
 
 typedef struct {
     int iterations;
@@ -312,8 +322,9 @@ int qes_set_sr_impl(int impl);
 int qes_sr_uses_tensor_cores(int dtype, int ns, int nh, int64_t n_samples, int* uses);
 /* Tiling of the tensor-core path for these shapes (for roofline accounting):
  * out = [uses, big, KC, n_chunks, nsplit, n_tiles, Kd, NB, Np, MT, NC, NR,
- * nnc, SPC, ov_stages, cl] (first n_out entries); cl = 2 when the O^H u CTAs
- * run as pairs that add their partials on chip.                            */
+ * nnc, SPC, ov_stages, cl, sv, sv_grid] (first n_out entries); cl = 2 when
+ * the O^H u CTAs run as pairs that add their partials on chip; sv = 1 when
+ * the matvec runs as the fused S v kernel of sv_grid CTAs (one partial each). */
 int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int32_t* out, int n_out);
 /* Tiling of the tensor-core O^H u in this process: mode 0 = automatic (the
  * single-M-tile kernel when the shapes allow it), 1 = single-M-tile kernel
@@ -326,6 +337,13 @@ int qes_sr_set_tiling(int mode, int nc, int ctas);
  * per CTA (0, the default: the pairs measured slower on B200).  Same sums in a
  * fixed order either way.                                                  */
 int qes_sr_set_ohu_pairs(int on);
+/* The tensor-core S v of single-M-tile problems as one cooperative launch (1,
+ * the default): each CTA computes O v for its 128-sample tiles, a grid
+ * barrier gives every CTA the weighted mean of O v, and the same CTA then
+ * accumulates O^H u of its tiles in TMEM (Q = conj(t) u built from the
+ * float32 T) and writes one partial P-vector; or as the two kernels O v and
+ * O^H u (0).  Same operator, different float32 summation order.           */
+int qes_sr_set_fused_sv(int on);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);
@@ -361,7 +379,8 @@ int qes_set_l2_persist(int enable);
 
 /* Per-kernel CUDA-event timing of the SR matvec halves, for measurement:
  * while enabled, every launch of class k (0: O v, 1: O^H u, 2: split
- * reduction, 3: dense Gram, 4: dense Cholesky, the whole factorisation)
+ * reduction, 3: dense Gram, 4: dense Cholesky, the whole factorisation,
+ * 5: the fused S v kernel)
  * is bracketed by two events on its launch stream and CG graphs
  * are bypassed.  qes_profile_read synchronises the device and returns the
  * accumulated milliseconds and launch counts (reset != 0 zeroes them).

@@ -55,28 +55,44 @@ def s_matrix(O_c, w=None):
     return np.conj(O_c).T @ (w[:, None] * O_c) / ns
 
 
-def cg(matvec, b, *, rtol=1e-8, atol=0.0, maxiter=1000, x0=None):
-    """Conjugate gradients in float64/complex128.  Returns (x, iterations, residual_norm, converged)."""
+def cg(matvec, b, *, rtol=1e-8, atol=0.0, maxiter=1000, x0=None, minv=None):
+    """Conjugate gradients in float64/complex128.  Returns (x, iterations, residual_norm, converged).
+    minv: the diagonal of a preconditioner M ~ A^-1 (SciPy's ``cg(M=...)``: z = M r, rho = r^H z);
+    the stopping rule stays ||r|| <= max(rtol ||b||, atol)."""
     b = np.asarray(b)
     x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=b.dtype)
     r = b - matvec(x) if x0 is not None else b.copy()
-    p = r.copy()
-    rr = np.vdot(r, r).real
+    z = r if minv is None else minv * r
+    p = z.copy()
+    rho = np.vdot(r, z).real
     bnorm = np.linalg.norm(b)
     thresh = max(rtol * bnorm, atol)
-    if np.sqrt(rr) <= thresh:
-        return x, 0, np.sqrt(rr), True
+    if np.linalg.norm(r) <= thresh:
+        return x, 0, np.linalg.norm(r), True
     for it in range(1, maxiter + 1):
         Ap = matvec(p)
-        alpha = rr / np.vdot(p, Ap)
+        alpha = rho / np.vdot(p, Ap)
         x = x + alpha * p
         r = r - alpha * Ap
-        rr_new = np.vdot(r, r).real
-        if np.sqrt(rr_new) <= thresh:
-            return x, it, np.sqrt(rr_new), True
-        p = r + (rr_new / rr) * p
-        rr = rr_new
-    return x, maxiter, np.sqrt(rr), False
+        rn = np.linalg.norm(r)
+        if rn <= thresh:
+            return x, it, rn, True
+        z = r if minv is None else minv * r
+        rho_new = np.vdot(r, z).real
+        p = z + (rho_new / rho) * p
+        rho = rho_new
+    return x, maxiter, np.linalg.norm(r), False
+
+
+def jacobi_minv(O_c, w=None, shift=0.0):
+    """Inverse diagonal of S + shift, diag(S)_k = sum_s w_s |O_c,sk|^2 / Ns: the Jacobi preconditioner
+    named 'jacobi' by the reference's solver options (``QES/NQS/__init__.py:405-407``,
+    ``tdvp.py:686-710``; its implementation lives in the absent ``general_python`` submodule, so this
+    is the textbook diagonal of the same S)."""
+    n = O_c.shape[0]
+    w = np.ones(n) if w is None else np.asarray(w, dtype=np.float64)
+    d = (w[:, None] * np.abs(O_c) ** 2).sum(axis=0) / n + shift
+    return 1.0 / d
 
 
 def solve_sr(e_loc, O, *, shift=1e-3, probs=None, method="dense", rtol=1e-8,

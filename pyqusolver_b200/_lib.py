@@ -73,8 +73,11 @@ class Hamiltonian(C.Structure):
 class SROptions(C.Structure):
     _fields_ = [
         ("shift", C.c_double), ("rtol", C.c_double), ("atol", C.c_double), ("maxiter", C.c_int),
-        ("check_every", C.c_int), ("rhs_prefactor", C.c_double),
+        ("check_every", C.c_int), ("rhs_prefactor", C.c_double), ("precond", C.c_int),
     ]
+
+
+PRECOND_NONE, PRECOND_JACOBI = 0, 1
 
 
 class SRResult(C.Structure):
@@ -118,6 +121,7 @@ SIGNATURES = {
     "qes_sr_tc_plan": [C.c_int, C.c_int, C.c_int, _i64, _vp, C.c_int],
     "qes_sr_set_tiling": [C.c_int, C.c_int, C.c_int],
     "qes_sr_set_ohu_pairs": [C.c_int],
+    "qes_sr_set_fused_sv": [C.c_int],
     "qes_set_cg_graphs": [C.c_int],
     "qes_set_cg_fused": [C.c_int],
     "qes_sr_set_barrier_test": [C.c_uint, C.c_uint],
@@ -220,7 +224,7 @@ def sr_impl() -> int:
 
 
 TC_PLAN_FIELDS = ("uses", "big", "KC", "n_chunks", "nsplit", "n_tiles", "Kd", "NB", "Np", "MT", "NC", "NR", "nnc",
-                  "SPC", "ov_stages", "cl")
+                  "SPC", "ov_stages", "cl", "sv", "sv_grid")
 
 
 def sr_tc_plan(dtype_code: int, ns: int, nh: int, n_samples: int) -> dict:
@@ -236,7 +240,7 @@ def sr_uses_tensor_cores(dtype_code: int, ns: int, nh: int, n_samples: int) -> b
     return bool(u.value)
 
 
-PROFILE_CLASSES = ("ov", "ohu", "reduce", "gram", "cholesky")
+PROFILE_CLASSES = ("ov", "ohu", "reduce", "gram", "cholesky", "sv")
 
 
 def profile_enable(on: bool):

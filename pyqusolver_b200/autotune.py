@@ -3,7 +3,9 @@
 The tcgen05 O^H u has two tilings (``qes_sr_tc_plan``): one 128-row M tile per sample chunk (small
 problems) or an M/N-tiled kernel whose CTAs fold several sample chunks into TMEM (N chunks of NC
 hidden units, a target CTA count); ``qes_sr_set_ohu_pairs`` runs the single-tile kernel as pairs
-of CTAs that add their split-K partials through distributed shared memory.  ``tune_sr_tiling`` times
+of CTAs that add their split-K partials through distributed shared memory, and
+``qes_sr_set_fused_sv`` runs the single-tile matvec as one cooperative S v kernel (O v, the mean of
+O v over a grid barrier and O^H u in the same CTAs).  ``tune_sr_tiling`` times
 the SR matvec (``qes_sr_matvec``: O v, O^H u and the split reduction, the body of one CG iteration)
 of a given batch for every candidate with CUDA events on the current stream, keeps the fastest,
 applies it process-wide and persists it in a JSON cache keyed by device, dtype and shape
@@ -29,23 +31,25 @@ def _cache_path(cache=None):
 
 
 def _candidates(ns, nh, cplx):
-    out = [(0, 0, 0, 0), (0, 0, 0, 1)]                     # automatic, automatic with CTA pairs
+    # (mode, nc, ctas, pairs, fused S v): automatic with the fused kernel, the kernel pair, the pair
+    # with O^H u in CTA pairs, then the M/N-tiled O^H u
+    out = [(0, 0, 0, 0, 1), (0, 0, 0, 0, 0), (0, 0, 0, 1, 0)]
     for nc in (256, 208, 128, 96, 64, 32):
         if nc > ((nh + 15) // 16) * 16:
             continue
         for ctas in (148, 296, 592):
-            out.append((2, nc, ctas, 0))
+            out.append((2, nc, ctas, 0, 0))
     return out
 
 
 def tune_sr_tiling(net, bits, tanh_theta, *, repeats=5, cache=None, candidates=None):
-    """Time the SR matvec of (net, bits, tanh_theta) under each tiling candidate (mode, nc, ctas, pairs);
+    """Time the SR matvec of (net, bits, tanh_theta) under each tiling candidate (mode, nc, ctas, pairs, sv);
     apply and return the fastest as a dict with the timings.  A cached choice for the same device and
     shapes is applied without timing."""
     dc = dv.dtype_code(net.flat)
     n = int(bits.shape[0])
     dev = torch.cuda.get_device_name(bits.device)
-    key = f"sr_tiling|{dev}|{dc}|{net.ns}|{net.nh}|{n}"
+    key = f"sr_tiling5|{dev}|{dc}|{net.ns}|{net.nh}|{n}"
     path = _cache_path(cache)
     table = {}
     try:
@@ -87,9 +91,9 @@ def tune_sr_tiling(net, bits, tanh_theta, *, repeats=5, cache=None, candidates=N
             if t < best_t:
                 best, best_t = cand, t
     finally:
-        apply_tiling(*(best or (0, 0, 0, 0)))
+        apply_tiling(*(best or (0, 0, 0, 0, 1)))
     if best is None:
-        return {"choice": (0, 0, 0, 0), "ms": None, "timings": timings, "cached": False}
+        return {"choice": (0, 0, 0, 0, 1), "ms": None, "timings": timings, "cached": False}
     entry = {"choice": list(best), "ms": best_t, "timings": timings}
     table[key] = entry
     try:
@@ -103,6 +107,7 @@ def tune_sr_tiling(net, bits, tanh_theta, *, repeats=5, cache=None, candidates=N
     return dict(entry, cached=False)
 
 
-def apply_tiling(mode, nc, ctas, pairs):
+def apply_tiling(mode, nc, ctas, pairs, sv=1):
     _lib.call("qes_sr_set_tiling", int(mode), int(nc), int(ctas))
     _lib.call("qes_sr_set_ohu_pairs", int(pairs))
+    _lib.call("qes_sr_set_fused_sv", int(sv))

@@ -38,7 +38,7 @@ void qes_count_launches(int n);
 // Per-kernel-class CUDA-event timing (enabled by qes_profile_enable): a launch site
 // brackets its kernel with qes_prof_begin / qes_prof_end on the launch stream.
 enum { QES_PROF_OV = 0, QES_PROF_OHU = 1, QES_PROF_REDUCE = 2, QES_PROF_GRAM = 3, QES_PROF_CHOL = 4,
-       QES_PROF_CLASSES = 5 };
+       QES_PROF_SV = 5, QES_PROF_CLASSES = 6 };
 bool qes_prof_on();
 int qes_prof_begin(int cls, cudaStream_t st);        // returns a slot or -1
 void qes_prof_end(int slot, cudaStream_t st);

@@ -525,7 +525,8 @@ static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, doub
 
 // ----------------------------------------------------------------------------
 // CG state on the device (float64):
-//   scal[0] rr   scal[1] pAp   scal[2] rr_new   scal[3] threshold^2   scal[4] done
+//   scal[0] rho (r^H r, or r^H D^-1 r with the Jacobi preconditioner)   scal[1] pAp
+//   scal[2] rr_new = ||r||^2   scal[3] threshold^2   scal[4] done
 //   scal[5] iterations   scal[6] ||b||^2   scal[7] alpha   scal[8] beta
 // Partial sums are reduced by one block of 1024 threads in a fixed order.
 // ----------------------------------------------------------------------------
@@ -544,31 +545,45 @@ __device__ __forceinline__ double block_sum_parts(int n, const double* __restric
   return t;                                // valid in thread 0
 }
 
+// dinv (optional): the Jacobi preconditioner D^-1 = 1 / diag(S + shift); the block also sums
+// rho = r^H D^-1 r into rz_part (PCG's alpha / beta numerator; plain CG uses rho = r^H r)
 template <class V>
 __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* __restrict__ p, const V* __restrict__ Ap,
                                                             V* __restrict__ x, V* __restrict__ r,
                                                             double* __restrict__ scal, double* __restrict__ rr_part,
-                                                            unsigned int* __restrict__ counter) {
+                                                            unsigned int* __restrict__ counter,
+                                                            const double* __restrict__ dinv = nullptr,
+                                                            double* __restrict__ rz_part = nullptr) {
   pdl_trigger();
   pdl_wait();                                              // Ap and alpha: previous kernel
   if (scal[4] != 0.0) return;                              // converged: x and r are final (every block)
   const double alpha = scal[7];
-  double d = 0.0;
+  double d = 0.0, dz = 0.0;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
     V rk = r[k];
     x[k] = vadd(x[k], vscale(alpha, p[k]));
     rk = vadd(rk, vscale(-alpha, Ap[k]));
     r[k] = rk;
-    d += vdotc(rk, rk);
+    const double q = vdotc(rk, rk);
+    d += q;
+    if (dinv) dz += q * dinv[k];
   }
-  __shared__ double red[RED_THREADS / 32];
+  __shared__ double red[RED_THREADS / 32], redz[RED_THREADS / 32];
   d = warp_sum(d);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+  dz = warp_sum(dz);
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = d;
+    redz[threadIdx.x >> 5] = dz;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0;
-    for (int q = 0; q < RED_THREADS / 32; ++q) s += red[q];
+    double s = 0, sz = 0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) {
+      s += red[q];
+      sz += redz[q];
+    }
     rr_part[blockIdx.x] = s;
+    if (dinv) rz_part[blockIdx.x] = sz;
   }
   // the last block to finish: rr_new, convergence, beta = rr_new / rr, rr <- rr_new
   __shared__ bool last;
@@ -579,20 +594,31 @@ __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* 
   __syncthreads();
   if (!last) return;
   __threadfence();
-  double v = 0.0;
-  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) v += ((volatile double*)rr_part)[q];
+  double v = 0.0, vz = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) {
+    v += ((volatile double*)rr_part)[q];
+    if (dinv) vz += ((volatile double*)rz_part)[q];
+  }
   v = warp_sum(v);
+  vz = warp_sum(vz);
   __syncthreads();
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = v;
+    redz[threadIdx.x >> 5] = vz;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double rr_new = 0.0;
-    for (int q = 0; q < RED_THREADS / 32; ++q) rr_new += red[q];
+    double rr_new = 0.0, rz_new = 0.0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) {
+      rr_new += red[q];
+      rz_new += redz[q];
+    }
+    const double rho_new = dinv ? rz_new : rr_new;
     if (scal[4] == 0.0) {
       scal[2] = rr_new;
       scal[5] += 1.0;
-      scal[8] = (scal[0] > 0.0) ? rr_new / scal[0] : 0.0;
-      scal[0] = rr_new;
+      scal[8] = (scal[0] > 0.0) ? rho_new / scal[0] : 0.0;
+      scal[0] = rho_new;
       if (rr_new <= scal[3]) scal[4] = 1.0;
     }
     *counter = 0u;
@@ -603,14 +629,16 @@ __global__ void __launch_bounds__(RED_THREADS) cg_xr_kernel(int64_t P, const V* 
 template <class V>
 __global__ void __launch_bounds__(RED_THREADS) cg_p_kernel(int64_t P, const V* __restrict__ r, V* __restrict__ p,
                                                            const double* __restrict__ scal, TcDims td,
-                                                           uint16_t* __restrict__ vp) {
+                                                           uint16_t* __restrict__ vp,
+                                                           const double* __restrict__ dinv = nullptr) {
   pdl_trigger();
   pdl_wait();                                              // r and beta: previous kernel
   if (scal[4] != 0.0) return;
   const double beta = scal[8];
   const int ns = td.ns, nh = td.nh;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
-    const V pk = vadd(r[k], vscale(beta, p[k]));
+    const V zk = dinv ? vscale(dinv[k], r[k]) : r[k];     // z = D^-1 r (PCG) or r
+    const V pk = vadd(zk, vscale(beta, p[k]));
     p[k] = pk;
     if (vp && k >= ns) {
       const int64_t q = k - ns;
@@ -631,39 +659,117 @@ static int vec_blocks(int64_t n) {
 }
 
 // r = p = b - A x0 (x already holds x0, Ap holds A x0)
+// (p = D^-1 r with the Jacobi preconditioner dinv)
 template <class V>
 __global__ void cg_init_x0_kernel(int64_t P, const V* __restrict__ b, const V* __restrict__ Ax0, V* __restrict__ r,
-                                  V* __restrict__ p) {
+                                  V* __restrict__ p, const double* __restrict__ dinv = nullptr) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
     const V rk = vadd(b[k], vscale(-1.0, Ax0[k]));
     r[k] = rk;
-    p[k] = rk;
+    p[k] = dinv ? vscale(dinv[k], rk) : rk;
   }
 }
 
-// x = 0, r = p = b
+// x = 0, r = b, p = b (or D^-1 b)
 template <class V>
 __global__ void cg_init_kernel(int64_t P, const V* __restrict__ b, V* __restrict__ x, V* __restrict__ r,
-                               V* __restrict__ p) {
+                               V* __restrict__ p, const double* __restrict__ dinv = nullptr) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
     x[k] = vzero(V());
     r[k] = b[k];
-    p[k] = b[k];
+    p[k] = dinv ? vscale(dinv[k], b[k]) : b[k];
   }
 }
 
+// per-block partial sums of r^H D^-1 r
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) wnorm2_kernel(int64_t P, const V* __restrict__ r,
+                                                             const double* __restrict__ dinv,
+                                                             double* __restrict__ part) {
+  double d = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x)
+    d += vdotc(r[k], r[k]) * dinv[k];
+  __shared__ double red[RED_THREADS / 32];
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) t += red[q];
+    part[blockIdx.x] = t;
+  }
+}
+
+// Jacobi preconditioner of S + shift: diag(S)_k = sum_s p_s |O_sk - Obar_k|^2 / Ns = mean|O_k|^2 - |Obar_k|^2
+// with mean|O_k|^2 = 1 for the visible biases (sigma^2 = 1) and mean|t_m|^2 for b_m and W_im.
+// Partial column sums of p_s |t_sm|^2 over sample splits (grid.y), then their fixed-order sum.
+constexpr int TSQ_SPLITS = 128;
+template <class T>
+__global__ void tsq_part_kernel(int nh, int64_t n, const T* __restrict__ tt, const float* __restrict__ wts,
+                                double* __restrict__ part) {
+  const int m = blockIdx.x * 32 + threadIdx.x;
+  const int64_t s0 = (int64_t)blockIdx.y * n / gridDim.y, s1 = (int64_t)(blockIdx.y + 1) * n / gridDim.y;
+  double acc = 0.0;
+  if (m < nh)
+    for (int64_t s = s0 + threadIdx.y; s < s1; s += blockDim.y) {
+      const T t = tt[s * nh + m];
+      double a;
+      if constexpr (ScalarTraits<T>::is_complex) a = (double)t.x * t.x + (double)t.y * t.y;
+      else a = (double)t * t;
+      acc += wts ? (double)wts[s] * a : a;
+    }
+  __shared__ double red[8][32];
+  red[threadIdx.y][threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.y == 0 && m < nh) {
+    double t = 0.0;
+    for (int q = 0; q < (int)blockDim.y; ++q) t += red[q][threadIdx.x];
+    part[(int64_t)blockIdx.y * nh + m] = t;
+  }
+}
+__global__ void tsq_sum_kernel(int nh, int nsplit, double inv_n, const double* __restrict__ part,
+                               double* __restrict__ tsq) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < nh; m += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int z = 0; z < nsplit; ++z) t += part[(int64_t)z * nh + m];
+    tsq[m] = t * inv_n;
+  }
+}
+// obar_h = O^H p / Ns (the conjugated weighted mean of the O rows); dinv = 1 / (max(diag S, 0) + shift)
+template <class V>
+__global__ void jacobi_dinv_kernel(int ns, int nh, int64_t P, const double* __restrict__ tsq,
+                                   const V* __restrict__ obar_h, double shift, double* __restrict__ dinv) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    double msq = 1.0;
+    if (k >= ns) msq = tsq[(k < ns + nh) ? (int)(k - ns) : (int)((k - ns - nh) % nh)];
+    const double d = fmax(msq - vdotc(obar_h[k], obar_h[k]), 0.0) + shift;
+    dinv[k] = d > 0.0 ? 1.0 / d : 1.0;
+  }
+}
+__global__ void fill_ones_kernel(int64_t n, float2* __restrict__ g) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    g[k] = make_float2(1.f, 0.f);
+}
+
 // parts_r: dot partials of ||r0||^2 for a start x0 != 0 (nullptr: r0 = b)
+// parts_z: dot partials of r0^H D^-1 r0 (Jacobi PCG: rho0; nullptr: rho0 = ||r0||^2)
 __global__ void __launch_bounds__(SC_THREADS) cg_setup_kernel(int n, const double* __restrict__ parts, double rtol,
                                                               double atol, double* __restrict__ scal,
-                                                              const double* __restrict__ parts_r = nullptr) {
+                                                              const double* __restrict__ parts_r = nullptr,
+                                                              const double* __restrict__ parts_z = nullptr) {
   const double s = block_sum_parts(n, parts);
   double rr0 = s;
   if (parts_r) {
     __syncthreads();                                      // block_sum_parts reuses its shared buffer
     rr0 = block_sum_parts(n, parts_r);
   }
+  double rho0 = rr0;
+  if (parts_z) {
+    __syncthreads();
+    rho0 = block_sum_parts(n, parts_z);
+  }
   if (threadIdx.x != 0) return;
-  scal[0] = rr0;                    // rr = ||r0||^2
+  scal[0] = rho0;                   // rho = ||r0||^2 (CG) or r0^H D^-1 r0 (PCG)
   scal[6] = s;                      // ||b||^2
   const double th = fmax(rtol * sqrt(s), atol);
   scal[3] = th * th;
@@ -730,13 +836,10 @@ __global__ void scale_vec_kernel(int64_t P, double s, V* __restrict__ x) {
 // each barrier wait is bounded and records a time-out in *err.
 // ----------------------------------------------------------------------------
 constexpr int CF_TX = 32, CF_TY = 16;            // 512 threads: 32 columns x 16 split groups
-constexpr uint32_t kGridBarLimit = 1u << 24;     // polls (with a short sleep) before giving up
 
 // count and gen live in different 128-byte lines; waiters poll gen with plain volatile loads so
-// that the arrivals (atomics on count) do not queue behind polling atomics
-// Test hook: `extra` arrivals that never come and a short poll limit make every barrier wait run out
-// (set by qes_sr_set_barrier_test; zero / kGridBarLimit in normal use).
-struct BarCfg { unsigned int extra; unsigned int limit; };
+// that the arrivals (atomics on count) do not queue behind polling atomics.  BarCfg (sr_tc.h) is the
+// test hook set by qes_sr_set_barrier_test.
 
 __device__ __forceinline__ void grid_barrier(unsigned int* count, unsigned int* gen, unsigned int nb, int* err,
                                              BarCfg bc) {
@@ -771,8 +874,9 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
                                                                  V* __restrict__ p, V* __restrict__ Ap,
                                                                  double* __restrict__ scal, double* __restrict__ part,
                                                                  unsigned int* __restrict__ bar, int* __restrict__ err,
-                                                                 TcDims td, uint16_t* __restrict__ vp, BarCfg bc) {
-  const double rr = scal[0], thresh = scal[3];
+                                                                 TcDims td, uint16_t* __restrict__ vp, BarCfg bc,
+                                                                 const double* __restrict__ dinv) {
+  const double rr = scal[0], thresh = scal[3];     // rr: rho (r^H D^-1 r with the preconditioner)
   if (scal[4] != 0.0) return;                      // converged: every CTA leaves (scal only changes below)
   if (*(volatile int*)err != 0) return;            // an earlier barrier wait gave up: the solve is abandoned
   constexpr int NT = CF_TX * CF_TY;
@@ -854,26 +958,34 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
   };
   const double pap = sum_parts(part);
   const double alpha = (pap > 0.0) ? rr / pap : 0.0;
-  // phase 2: x, r and r^H r
-  double e = 0.0;
+  // phase 2: x, r, r^H r (and r^H D^-1 r)
+  double e = 0.0, ez = 0.0;
   const int64_t stride = (int64_t)nb * NT;
   for (int64_t k = (int64_t)blockIdx.x * NT + tid; k < P; k += stride) {
     x[k] = vadd(x[k], vscale(alpha, p[k]));
     const V rk = vadd(r[k], vscale(-alpha, Ap[k]));
     r[k] = rk;
-    e += vdotc(rk, rk);
+    const double q = vdotc(rk, rk);
+    e += q;
+    if (dinv) ez += q * dinv[k];
   }
   e = block_sum(e);
   if (tid == 0) part[nb + blockIdx.x] = e;
+  if (dinv) {
+    ez = block_sum(ez);
+    if (tid == 0) part[2 * nb + blockIdx.x] = ez;
+  }
   grid_barrier(bar, bar + 32, nb, err, bc);
   const double rr_new = sum_parts(part + nb);
-  const double beta = (rr > 0.0) ? rr_new / rr : 0.0;
+  const double rho_new = dinv ? sum_parts(part + 2 * nb) : rr_new;
+  const double beta = (rr > 0.0) ? rho_new / rr : 0.0;
   const bool conv = rr_new <= thresh;
   // phase 3: direction update (same index map as phase 2: each thread updates what it wrote)
   if (!conv) {
     const int ns = td.ns, nh = td.nh;
     for (int64_t k = (int64_t)blockIdx.x * NT + tid; k < P; k += stride) {
-      const V pk = vadd(r[k], vscale(beta, p[k]));
+      const V zk = dinv ? vscale(dinv[k], r[k]) : r[k];
+      const V pk = vadd(zk, vscale(beta, p[k]));
       p[k] = pk;
       if (vp && k >= ns) {
         const int64_t q = k - ns;
@@ -883,7 +995,7 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
     }
   }
   if (blockIdx.x == 0 && tid == 0) {
-    scal[1] = pap; scal[7] = alpha; scal[2] = rr_new; scal[8] = beta; scal[0] = rr_new;
+    scal[1] = pap; scal[7] = alpha; scal[2] = rr_new; scal[8] = beta; scal[0] = rho_new;
     scal[5] += 1.0;
     if (conv) scal[4] = 1.0;
   }
@@ -903,11 +1015,14 @@ struct SRWork {
   void* x; void* r; void* p; void* Ap; void* b;   // [P] of V each
   double* parts;      // [RED_BLOCKS]
   double* scal;       // [16]
+  double* dinv;       // [P] Jacobi preconditioner 1 / diag(S + shift)
+  double* tsq;        // [nh] weighted mean of |t_m|^2, then [TSQ_SPLITS][nh] partial sums
   unsigned int* counter;  // [2] last-block tickets (reduce, x/r update)
   bool tc;            // tensor-core matvec in use
   TcDims td;
   TcWork tw;
   int nsplit;         // partial P-vectors written by the O^H u stage
+  int mv_nsplit;      // partial P-vectors written by the matvec (tc_matvec_nsplit on the tensor-core path)
   size_t total;
 };
 
@@ -924,8 +1039,9 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   const int impl = g_sr_impl.load();
   L.fp64 = impl == 3;
   L.tc = tc_ok && impl != 1 && !L.fp64;
-  const int64_t nsplit_max = std::max<int64_t>(nsplit_simt, tc_ok ? L.td.nsplit : 1);
+  const int64_t nsplit_max = std::max<int64_t>(nsplit_simt, tc_ok ? std::max(L.td.nsplit, tc_matvec_nsplit(L.td)) : 1);
   L.nsplit = (int)(L.tc ? L.td.nsplit : nsplit_simt);
+  L.mv_nsplit = (int)(L.tc ? tc_matvec_nsplit(L.td) : nsplit_simt);
   size_t off = 0;
   auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off += align256(bytes); return p; };
   L.w = (float2*)take((size_t)n_samples * sizeof(float2));
@@ -936,6 +1052,8 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
   L.parts = (double*)take(std::max(RED_BLOCKS, RS_MAX_BLOCKS) * sizeof(double));
   L.scal = (double*)take(16 * sizeof(double));
+  L.dinv = (double*)take(P * sizeof(double));
+  L.tsq = (double*)take((size_t)(TSQ_SPLITS + 1) * nh * sizeof(double));
   L.counter = (unsigned int*)take(128 * sizeof(unsigned int));     // tickets, barrier words (own lines)
   char* tcb = tc_ok ? take(tc_workspace_bytes(L.td)) : nullptr;
   L.tw = (tc_ok && base) ? tc_layout(L.td, tcb) : TcWork{};
@@ -1075,9 +1193,9 @@ extern "C" int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int3
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_tc_plan: bad dtype");
   const SRWork L = sr_layout(dtype, ns, nh, n_samples, nullptr);
   const TcDims& d = L.td;
-  const int32_t f[16] = {L.tc ? 1 : 0, d.big ? 1 : 0, d.KC, d.n_chunks, d.nsplit, d.n_tiles, d.Kd, d.NB, d.Np,
-                         d.MT, d.NC, d.NR, d.nnc, d.SPC, d.ov_stages, d.cl};
-  for (int k = 0; k < n_out; ++k) out[k] = k < 16 ? f[k] : 0;
+  const int32_t f[18] = {L.tc ? 1 : 0, d.big ? 1 : 0, d.KC, d.n_chunks, d.nsplit, d.n_tiles, d.Kd, d.NB, d.Np,
+                         d.MT, d.NC, d.NR, d.nnc, d.SPC, d.ov_stages, d.cl, d.sv ? 1 : 0, d.sv ? d.sv_grid : 0};
+  for (int k = 0; k < n_out; ++k) out[k] = k < 18 ? f[k] : 0;
   return QES_OK;
 }
 
@@ -1121,6 +1239,10 @@ extern "C" int qes_sr_force(int dtype, int ns, int nh, int64_t n_samples, const 
                                workspace_bytes, stream);
 }
 
+// grid-barrier test hook of the fused kernels (qes_sr_set_barrier_test)
+static std::atomic<unsigned int> g_bar_extra{0};
+static std::atomic<unsigned int> g_bar_limit{kGridBarLimit};
+
 template <class T>
 static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, double shift,
                        const typename VecT<T>::type* v, typename VecT<T>::type* y, double* dot_part, const SRWork& L,
@@ -1128,11 +1250,12 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
   using V = typename VecT<T>::type;
   if (L.tc) {
     const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
-    int rc = tc_matvec(dtype, L.td, n_samples, bits, v, L.w, L.partial, L.tw, st, !vp_ready, cg_done);
+    int rc = tc_matvec(dtype, L.td, n_samples, bits, tt, v, L.w, L.partial, L.tw, st, !vp_ready, cg_done,
+                       BarCfg{g_bar_extra.load(), g_bar_limit.load()});
     if (rc) return rc;
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
     const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
-    if (int rc_ = launch_reduce_splits<T, V>(P, L.nsplit, L.partial, shift, v, y,
+    if (int rc_ = launch_reduce_splits<T, V>(P, L.mv_nsplit, L.partial, shift, v, y,
         dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
     QES_LAUNCH_CHECK();
     qes_prof_end(pfr, st);
@@ -1235,8 +1358,6 @@ CgGraphSlot g_graph[kMaxGraphDevices];
 std::atomic<int> g_use_graphs{1};
 std::atomic<int> g_l2_persist{0};
 std::atomic<int> g_cg_fused{1};            // automatic
-std::atomic<unsigned int> g_bar_extra{0};   // test hook of the fused kernel's grid barrier
-std::atomic<unsigned int> g_bar_limit{kGridBarLimit};
 std::atomic<int> g_cg_loop{1};             // device-side loop over the CG chunks
 
 // L2 persistence of the tensor-core operands across the CG iterations: an access-policy window
@@ -1323,6 +1444,39 @@ extern "C" int qes_set_cg_graphs(int enable) {
   return QES_OK;
 }
 
+// Jacobi preconditioner D^-1 = 1 / diag(S + shift) into L.dinv: Obar^H = O^H p / Ns by the O^H pass
+// (g = 1, no centring; into L.Ap, free before the iterations), the weighted column means of |t|^2,
+// then diag(S)_k = mean|O_k|^2 - |Obar_k|^2 (clamped at 0)
+template <class T>
+static int sr_jacobi_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, double shift,
+                       const SRWork& L, cudaStream_t st) {
+  using V = typename VecT<T>::type;
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  float2* ones = (float2*)L.wpart;                       // scratch of at least Ns float2
+  fill_ones_kernel<<<RED_BLOCKS, RED_THREADS, 0, st>>>(n_samples, ones);
+  QES_LAUNCH_CHECK();
+  V* obar_h = (V*)L.Ap;
+  const double inv_n = 1.0 / (double)n_samples;
+  if (L.tc) {
+    const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
+    int rc = tc_ohu(dtype, L.td, n_samples, ones, nullptr, 0, inv_n, L.partial, L.tw, st);
+    if (rc) return rc;
+    if ((rc = launch_reduce_splits<T, V>(P, L.nsplit, L.partial, 0.0, nullptr, obar_h, nullptr, nullptr, nullptr,
+                                         st)))
+      return rc;
+    QES_LAUNCH_CHECK();
+  } else if (int rc = apply_ohu<T, V>(ns, nh, n_samples, bits, tt, ones, nullptr, inv_n, L, 0.0, nullptr, obar_h,
+                                      nullptr, st)) {
+    return rc;
+  }
+  double* part = L.tsq + nh;
+  tsq_part_kernel<T><<<dim3((nh + 31) / 32, TSQ_SPLITS), dim3(32, 8), 0, st>>>(nh, n_samples, tt, L.wts, part);
+  tsq_sum_kernel<<<(nh + 255) / 256, 256, 0, st>>>(nh, TSQ_SPLITS, inv_n, part, L.tsq);
+  jacobi_dinv_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(ns, nh, P, L.tsq, obar_h, shift, L.dinv);
+  QES_LAUNCH_CHECK_N(3);
+  return QES_OK;
+}
+
 // x0: start of the iteration for the unscaled system (nullptr: zero)
 template <class T>
 static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* eloc,
@@ -1340,21 +1494,40 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   double emean[2] = {0, 0};
   QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 128 * sizeof(unsigned int), st));
+  // preconditioned CG (SciPy's cg with M = D^-1): z = D^-1 r in the direction update, rho = r^H z
+  const double* dinv = nullptr;
+  if (opt->precond == QES_PRECOND_JACOBI) {
+    rc = sr_jacobi_t<T>(ns, nh, n_samples, bits, tt, opt->shift, L, st);
+    if (rc) return rc;
+    dinv = L.dinv;
+  }
+  double* parts_z = dinv ? L.parts + 2 * RED_BLOCKS : nullptr;
   if (x0) {
-    // warm start: x = x0, r = p = b - (S + shift) x0; the threshold stays rtol * ||b||
+    // warm start: x = x0, r = b - (S + shift) x0, p = D^-1 r; the threshold stays rtol * ||b||
     QES_CUDA_CHECK(cudaMemcpyAsync(x, x0, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
     rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, x, Ap, nullptr, L, st, false);
     if (rc) return rc;
-    cg_init_x0_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, Ap, r, p);
+    cg_init_x0_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, Ap, r, p, dinv);
     norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
     norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, L.parts + RED_BLOCKS);
-    cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal, L.parts + RED_BLOCKS);
-    QES_LAUNCH_CHECK_N(4);
-  } else {
-    cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p);
-    norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
-    cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal);
     QES_LAUNCH_CHECK_N(3);
+    if (dinv) {
+      wnorm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, dinv, parts_z);
+      QES_LAUNCH_CHECK();
+    }
+    cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal, L.parts + RED_BLOCKS,
+                                              parts_z);
+    QES_LAUNCH_CHECK();
+  } else {
+    cg_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, x, r, p, dinv);
+    norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
+    QES_LAUNCH_CHECK_N(2);
+    if (dinv) {
+      wnorm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, dinv, parts_z);
+      QES_LAUNCH_CHECK();
+    }
+    cg_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, opt->rtol, opt->atol, L.scal, nullptr, parts_z);
+    QES_LAUNCH_CHECK();
   }
   const int check = opt->check_every > 0 ? opt->check_every : 8;
   double hs[8] = {0};
@@ -1385,8 +1558,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     const int64_t nvec = fused_vec ? P / FEV : P;
     int64_t cv = (nvec + cap - 1) / cap;
     const int nthr = CF_TX * CF_TY;
-    cv = std::max<int64_t>(cv, nthr / std::max(L.nsplit, 1));
-    const int64_t need = (L.nsplit + RS_BATCH - 1) / RS_BATCH;
+    cv = std::max<int64_t>(cv, nthr / std::max(L.mv_nsplit, 1));
+    const int64_t need = (L.mv_nsplit + RS_BATCH - 1) / RS_BATCH;
     cv = std::min<int64_t>(cv, std::max<int64_t>(nthr / std::max<int64_t>(need, 1), 1));
     cv = std::max<int64_t>(1, std::min<int64_t>(cv, 128));
     fused_cv = (int)cv;
@@ -1402,8 +1575,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         // O v and O^H u (split partials), then the fused vector kernel
         if (L.tc) {
           const int dtype_ = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
-          int r2 = tc_matvec(dtype_, L.td, n_samples, bits, p, L.w, L.partial, L.tw, st, it0 + q == 0,
-                             L.scal + 4);
+          int r2 = tc_matvec(dtype_, L.td, n_samples, bits, tt, p, L.w, L.partial, L.tw, st, it0 + q == 0,
+                             L.scal + 4, bcfg);
           if (r2) return r2;
         } else {
           int r2 = apply_ov<T, V>(ns, nh, n_samples, bits, tt, p, L.w, L.wmean, L, st, L.scal + 4);
@@ -1424,15 +1597,15 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         lc.numAttrs = 1;
         const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
         if (fused_vec)
-          QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, true>, P, L.nsplit, fused_cv,
+          QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, true>, P, L.mv_nsplit, fused_cv,
                                             (const T*)L.partial, opt->shift, x, r, p, Ap, L.scal, L.parts,
                                             L.counter + 32, (int*)(L.counter + 4), L.td,
-                                            L.tc ? L.tw.vp : (uint16_t*)nullptr, bcfg));
+                                            L.tc ? L.tw.vp : (uint16_t*)nullptr, bcfg, dinv));
         else
-          QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, false>, P, L.nsplit, fused_cv,
+          QES_CUDA_CHECK(cudaLaunchKernelEx(&lc, cg_fused_kernel<T, V, false>, P, L.mv_nsplit, fused_cv,
                                             (const T*)L.partial, opt->shift, x, r, p, Ap, L.scal, L.parts,
                                             L.counter + 32, (int*)(L.counter + 4), L.td,
-                                            L.tc ? L.tw.vp : (uint16_t*)nullptr, bcfg));
+                                            L.tc ? L.tw.vp : (uint16_t*)nullptr, bcfg, dinv));
         qes_prof_end(pfr, st);
         QES_LAUNCH_CHECK();
         continue;
@@ -1442,9 +1615,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       if (r2) return r2;
       // (alpha is computed by the last block of the matvec's split reduction)
       QES_CUDA_CHECK(qes_launch_pdl(cg_xr_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P, (const V*)p,
-                                    (const V*)Ap, x, r, L.scal, L.parts, L.counter + 1));
+                                    (const V*)Ap, x, r, L.scal, L.parts, L.counter + 1, dinv,
+                                    dinv ? L.parts + RED_BLOCKS : (double*)nullptr));
       QES_CUDA_CHECK(qes_launch_pdl(cg_p_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P, (const V*)r, p,
-                                    (const double*)L.scal, L.td, L.tc ? L.tw.vp : (uint16_t*)nullptr));
+                                    (const double*)L.scal, L.td, L.tc ? L.tw.vp : (uint16_t*)nullptr, dinv));
       QES_LAUNCH_CHECK_N(2);
     }
     return QES_OK;
@@ -1478,8 +1652,9 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         if (l2) l2_window(gs.cs, dev, L.tw.t_rows, l2_bytes);
       }
       const CgGraphKey key{bits, tt, L.w, L.wts, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
-                           L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0), L.td.big ? 1 : 0, L.td.KC, L.nsplit,
-                           L.td.nnc, L.td.NC, L.td.SPC, L.td.cl, (int)bcfg.extra, opt->shift};
+                           L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0) | (dinv ? 4 : 0), L.td.big ? 1 : 0,
+                           L.td.KC, L.mv_nsplit,
+                           L.td.nnc, L.td.NC, L.td.SPC, L.td.cl | (L.td.sv ? 4 : 0), (int)bcfg.extra, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {
           cudaGraphExecDestroy(gs.exec);
@@ -1666,6 +1841,8 @@ extern "C" int qes_sr_solve_cg_weighted(int dtype, int ns, int nh, int64_t n_sam
                 "qes_sr_solve_cg: bad args");
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_solve_cg: bad dtype");
   QES_ARG_CHECK(opt->maxiter >= 0 && opt->shift >= 0.0, "qes_sr_solve_cg: bad options");
+  QES_ARG_CHECK(opt->precond == QES_PRECOND_NONE || opt->precond == QES_PRECOND_JACOBI,
+                "qes_sr_solve_cg: precond must be QES_PRECOND_NONE or QES_PRECOND_JACOBI");
   SRWork L;
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
@@ -1903,6 +2080,7 @@ extern "C" int qes_sr_solve_minsr(int dtype, int ns, int nh, int64_t n_samples, 
                 "qes_sr_solve_minsr: bad args");
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_solve_minsr: bad dtype");
   QES_ARG_CHECK(opt->maxiter >= 0 && opt->shift >= 0.0, "qes_sr_solve_minsr: bad options");
+  QES_ARG_CHECK(opt->precond == QES_PRECOND_NONE, "qes_sr_solve_minsr: no preconditioner on the MinSR system");
   SRWork L;
   int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
   if (rc) return rc;
@@ -2556,6 +2734,7 @@ extern "C" int qes_batch_sr_solve_cg(int dtype, int n_inst, const qes_batch_inst
   QES_ARG_CHECK(inst && ov_items && ohu_items && sample_bits && tanh_theta && eloc && opts && x_out,
                 "qes_batch_sr_solve_cg: null pointer");
   QES_ARG_CHECK(opts->maxiter >= 0 && opts->shift >= 0.0, "qes_batch_sr_solve_cg: bad options");
+  QES_ARG_CHECK(opts->precond == QES_PRECOND_NONE, "qes_batch_sr_solve_cg: no preconditioner on the batched CG");
   const size_t need = batch_sr_layout(dtype, n_inst, n_params_total, n_samples_total, sr_part_total, nullptr, nullptr);
   if (!workspace || workspace_bytes < need) {
     qes_set_last_message("qes_batch_sr_solve_cg: workspace too small");

@@ -1070,6 +1070,496 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_big_kernel(TcDims d, int64_t 
 }
 
 // ================================================================================================
+// sv: the whole tensor-core S v in one cooperative launch (single-M-tile problems)
+// ================================================================================================
+// CTA b takes the 128-sample tiles b, b + G, b + 2G, ... of the G CTAs, all resident (at most one
+// per SM).  Phase 1, per tile: w = O v as in tc_ov_kernel (T and V' streamed through a sv_stages-deep
+// pipeline, hi*hi + hi*lo + lo*hi MMAs, the spin signs folded in the epilogue); w -> w_out and the
+// tile's weighted sum -> wsum_part.  A bounded grid barrier; then every CTA forms the same weighted
+// mean of w from the tile sums, in the same order.  Phase 2, per tile: u = wts (w - mean) scale;
+// A = Sigma^T (128 sites x 128 samples, +-1, the ones row 127 yields g_b) is written into shared
+// memory from the spin words; B = Q^T with Q = conj(t) u is built from the float32 T in chunks of
+// SV_QROWS operand rows (BF16 hi/lo), double-buffered, so that the MMAs of one chunk run while the
+// next is built.  The MMAs accumulate in TMEM over all of the CTA's tiles and the CTA writes one
+// partial P-vector.  A bounded wait that runs out records QES_ERR_TIMEOUT in *status; launches
+// that find *status set return at once (the host reports the error after the solve).
+constexpr int SV_QROWS = 128;                              // Q^T operand rows per chunk
+constexpr uint32_t SV_SIG_BYTES = 128u * 128u * 2u;        // Sigma^T tile: 128 sites x 128 samples
+constexpr uint32_t SV_QTERM = SV_QROWS * 128u * 2u;        // one BF16 term of a Q^T chunk
+constexpr uint32_t SV_QBUF = 2u * SV_QTERM;                // hi + lo
+
+// count and gen on separate 128-byte lines; waiters poll gen with volatile loads (a sense-reversal
+// barrier: the last arrival resets count and advances gen); every wait is bounded
+__device__ __forceinline__ void sv_grid_barrier(unsigned int* count, unsigned int* gen, unsigned int nb,
+                                                int* status, BarCfg bc) {
+  nb += bc.extra;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* vgen = gen;
+    const unsigned int g = *vgen;
+    __threadfence();
+    if (atomicAdd(count, 1u) == nb - 1) {
+      *count = 0u;
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      uint32_t it = 0;
+      while (*vgen == g) {
+        if (++it > bc.limit) {
+          record_error(status, QES_ERR_TIMEOUT);
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(kThreads, 1) tc_sv_kernel(TcDims d, int64_t n_samples, const uint32_t* __restrict__ bits,
+                                                            const V* __restrict__ v, const T* __restrict__ tt,
+                                                            const uint16_t* __restrict__ t_rows,
+                                                            const uint16_t* __restrict__ vp, float2* __restrict__ w_out,
+                                                            double2* __restrict__ wsum_part, T* __restrict__ partial,
+                                                            int* __restrict__ status, const double* __restrict__ cg_done,
+                                                            const float* __restrict__ wts, double scale,
+                                                            unsigned int* __restrict__ bar, BarCfg bc) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  constexpr bool CPLX = ScalarTraits<T>::is_complex;
+  constexpr int NQ = CPLX ? SV_QROWS / 2 : SV_QROWS;       // hidden units per Q^T chunk
+  const int ns = d.ns, nh = d.nh, KCH = d.KCH, NB = d.NB, Sp = d.Sp, Mp = d.Mp;
+  const int nK = d.Kd / KCH, S = d.sv_stages;
+  const uint32_t a_term = 128u * KCH * 2u, b_term = (uint32_t)NB * KCH * 2u;
+  const uint32_t stage_bytes = 2u * (a_term + b_term);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + d.sv_region);
+  uint64_t* empty = full + S;
+  uint64_t* done = empty + S;                              // the O v MMAs of one tile
+  uint64_t* qbar = done + 1;                               // [2]: the MMAs that read Q^T buffer b
+  uint64_t* fin = qbar + 2;                                // every O^H u MMA of the CTA
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+  const int nsp = (ns + 1) & ~1;
+  T* s_va = reinterpret_cast<T*>(tslot + 4);
+  T* s_ga = s_va + nsp;                                    // g_a, summed over the CTA's tiles
+  T* s_u = s_ga + nsp;                                     // u of the current tile
+  uint32_t* s_bits = reinterpret_cast<uint32_t*>(s_u + 128);   // spin words, [word][row]
+  __shared__ double2 red[kWarps];
+  __shared__ float2 s_part[kColGroups][128];
+  __shared__ double2 s_mean;
+  __shared__ int s_err;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int G = gridDim.x;
+  const int nw = n_words(ns);
+  pdl_trigger();
+  if (cg_block_done(cg_done)) return;                      // converged CG: nothing to do
+  if (tid == 0) s_err = *reinterpret_cast<volatile int*>(status);
+  __syncthreads();
+  if (s_err != 0) return;                                  // an earlier wait of this solve gave up
+  if (tid == 0) {
+    for (int q = 0; q < S; ++q) {
+      umma::mbar_init(&full[q], 1);
+      umma::mbar_init(&empty[q], 1);
+    }
+    umma::mbar_init(done, 1);
+    umma::mbar_init(&qbar[0], 1);
+    umma::mbar_init(&qbar[1], 1);
+    umma::mbar_init(fin, 1);
+    umma::fence_mbar_init();
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, d.tmem_cols);
+    umma::tmem_relinquish();
+  }
+  for (int i = tid; i < ns; i += kThreads) {
+    if constexpr (CPLX) s_va[i] = make_float2(vre(v, i), vim(v, i));
+    else s_va[i] = vre(v, i);
+    s_ga[i] = ScalarTraits<T>::zero();
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tbase = *tslot;
+  const uint8_t* gbv = reinterpret_cast<const uint8_t*>(vp);
+
+  // ---------------------------------------------------------------- phase 1: w = O v per tile
+  int j = 0;
+  for (int tile = blockIdx.x; tile < d.n_tiles; tile += G, ++j) {
+    const uint8_t* ga = reinterpret_cast<const uint8_t*>(t_rows) + (size_t)tile * nK * 2 * a_term;
+    const int g0 = j * nK;                                 // pipeline chunks issued before this tile
+    const int64_t r0 = (int64_t)tile * 128;
+    const int rows = (n_samples - r0 < 128) ? (int)(n_samples - r0) : 128;
+    if (warp >= 2) {
+      // while the pipeline runs: the tile's spin words (epilogue input)
+      const int t2 = tid - 64, n2 = kThreads - 64;
+      for (int q = t2; q < 128 * nw; q += n2) {
+        const int r = q / nw, wd = q - r * nw;
+        s_bits[wd * 128 + r] = (r < rows) ? bits[r0 * nw + q] : 0u;
+      }
+    } else if (warp == 0 && lane == 0) {
+      // producer: stage s is refilled once the MMAs that read it have completed
+      for (int c = 0; c < nK; ++c) {
+        const int g = g0 + c, s = g % S;
+        if (g >= S && !umma::mbar_wait(&empty[s], ((g / S) - 1) & 1, kWaitLimit)) {
+          record_error(status, QES_ERR_TIMEOUT);
+          break;
+        }
+        uint8_t* stp = smem + s * stage_bytes;
+        umma::mbar_arrive_expect_tx(&full[s], stage_bytes);
+        umma::bulk_g2s(stp, ga + (size_t)c * 2 * a_term, 2 * a_term, &full[s]);
+        umma::bulk_g2s(stp + 2 * a_term, gbv + (size_t)c * 2 * b_term, 2 * b_term, &full[s]);
+      }
+    } else if (warp == 1 && lane == 0) {
+      // MMA issuer: D (128 x NB) += A_hi B_hi + A_hi B_lo + A_lo B_hi over every 16-wide k-step
+      const uint32_t idesc = umma::idesc_bf16_f32(128, (uint32_t)NB);
+      for (int c = 0; c < nK; ++c) {
+        const int g = g0 + c, s = g % S;
+        if (!umma::mbar_wait(&full[s], (g / S) & 1, kWaitLimit)) {
+          record_error(status, QES_ERR_TIMEOUT);
+          break;
+        }
+        umma::tc_fence_after();
+        const uint32_t sa = umma::smem_u32(smem + s * stage_bytes);
+        const uint32_t ahi = sa, alo = sa + a_term, bhi = sa + 2 * a_term, blo = bhi + b_term;
+        for (int kk = 0; kk < KCH / 16; ++kk) {
+          const uint32_t ko_a = 2u * kk * 128u * 16u, ko_b = 2u * kk * NB * 16u;
+          const uint64_t dah = umma::smem_desc(ahi + ko_a, 128u * 16u, 128u);
+          const uint64_t dal = umma::smem_desc(alo + ko_a, 128u * 16u, 128u);
+          const uint64_t dbh = umma::smem_desc(bhi + ko_b, NB * 16u, 128u);
+          const uint64_t dbl = umma::smem_desc(blo + ko_b, NB * 16u, 128u);
+          umma::mma_bf16(tbase, dah, dbh, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+          umma::mma_bf16(tbase, dah, dbl, idesc, 1u);
+          umma::mma_bf16(tbase, dal, dbh, idesc, 1u);
+        }
+        umma::mma_commit(&empty[s]);
+      }
+      umma::mma_commit(done);                              // every MMA of this tile has completed
+    }
+    __syncthreads();
+    if (!umma::mbar_wait(done, j & 1, kWaitLimit)) record_error(status, QES_ERR_TIMEOUT);
+    umma::tc_fence_after();
+    // epilogue: warp w reads lane quarter w % 4 (sample rows) and column group w / 4
+    {
+      const int quarter = warp & 3, cg = warp >> 2;
+      const int row = 32 * quarter + lane;
+      const bool sval = row < rows;
+      const uint32_t* wrd = s_bits + row;                  // word w of this row at wrd[128 w]
+      float2 acc = make_float2(0.f, 0.f);
+      const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+      int c = cg;
+      for (; c + kColGroups < NB / 16; c += 2 * kColGroups) {
+        float y0[16], y1[16];
+        umma::tmem_ld16x2(lane_addr + 16 * c, lane_addr + 16 * (c + kColGroups), y0, y1);
+        ov_fold16<CPLX>(16 * c, y0, ns, Sp, wrd, nw, acc);
+        ov_fold16<CPLX>(16 * (c + kColGroups), y1, ns, Sp, wrd, nw, acc);
+      }
+      if (c < NB / 16) {
+        float y[16];
+        umma::tmem_ld16(lane_addr + 16 * c, y);
+        ov_fold16<CPLX>(16 * c, y, ns, Sp, wrd, nw, acc);
+      }
+      // + sigma_s . v_a: column group cg takes the sites of spin words cg, cg + 4, ...
+      for (int wd = cg; wd < nw; wd += kColGroups) {
+        const uint32_t word = wrd[128 * wd];
+        const int i1 = (32 * wd + 32 < ns) ? 32 * wd + 32 : ns;
+        float sre = 0.f, sim = 0.f;
+        for (int i = 32 * wd; i < i1; ++i) {
+          const int sgn = (int)((~word >> (i & 31)) & 1u) << 31;
+          const T va = s_va[i];
+          if constexpr (CPLX) {
+            sre += __int_as_float(__float_as_int(va.x) ^ sgn);
+            sim += __int_as_float(__float_as_int(va.y) ^ sgn);
+          } else {
+            sre += __int_as_float(__float_as_int(va) ^ sgn);
+          }
+        }
+        acc.x += sre;
+        acc.y += sim;
+      }
+      s_part[cg][row] = acc;
+      umma::tc_fence_before();
+      __syncthreads();
+      if (cg == 0) {
+        float2 wv = s_part[0][row];
+#pragma unroll
+        for (int g = 1; g < kColGroups; ++g) wv = wv + s_part[g][row];
+        if (!sval) wv = make_float2(0.f, 0.f);
+        if (sval) w_out[r0 + row] = wv;
+        const double wt = (wts && sval) ? (double)wts[r0 + row] : 1.0;
+        double2 ps = make_double2(wt * wv.x, wt * wv.y);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          ps.x += __shfl_xor_sync(0xffffffffu, ps.x, o);
+          ps.y += __shfl_xor_sync(0xffffffffu, ps.y, o);
+        }
+        if (lane == 0) red[quarter] = ps;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int q = 0; q < 4; ++q) { t.x += red[q].x; t.y += red[q].y; }
+        wsum_part[tile] = t;
+      }
+    }
+    umma::tc_fence_before();
+    __syncthreads();                                       // TMEM read before the next tile's MMAs
+  }
+
+  // ---------------------------------------------------------------- the weighted mean of w
+  sv_grid_barrier(bar, bar + 32, (unsigned int)G, status, bc);
+  {
+    double2 t = make_double2(0.0, 0.0);
+    for (int q = tid; q < d.n_tiles; q += kThreads) {
+      const double2 x = __ldcg(wsum_part + q);
+      t.x += x.x;
+      t.y += x.y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+    }
+    if (lane == 0) red[warp] = t;
+    __syncthreads();
+    if (tid == 0) {
+      double2 m = make_double2(0.0, 0.0);
+      for (int q = 0; q < kWarps; ++q) { m.x += red[q].x; m.y += red[q].y; }
+      s_mean = make_double2(m.x / (double)n_samples, m.y / (double)n_samples);
+    }
+    __syncthreads();
+  }
+
+  // ---------------------------------------------------------------- phase 2: O^H u per tile
+  const float mr = (float)s_mean.x, mi = (float)s_mean.y, fs = (float)scale;
+  uint8_t* sA = smem;
+  uint8_t* sQ = smem + SV_SIG_BYTES;
+  const uint32_t a_addr = umma::smem_u32(sA), q_addr = umma::smem_u32(sQ);
+  const int nq = (Mp + NQ - 1) / NQ;
+  int gq = 0;                                              // Q^T chunks issued by this CTA
+  j = 0;
+  for (int tile = blockIdx.x; tile < d.n_tiles; tile += G, ++j) {
+    const int64_t r0 = (int64_t)tile * 128;
+    const int rows = (n_samples - r0 < 128) ? (int)(n_samples - r0) : 128;
+    if (j > 0) {
+      // the previous tile's MMAs read Sigma^T: wait for its last chunk (and so for all of them)
+      if (tid == 0 && !umma::mbar_wait(&qbar[(gq - 1) & 1], ((gq - 1) >> 1) & 1, kWaitLimit))
+        record_error(status, QES_ERR_TIMEOUT);
+      __syncthreads();
+    }
+    for (int q = tid; q < 128 * nw; q += kThreads) {
+      const int r = q / nw, wd = q - r * nw;
+      s_bits[wd * 128 + r] = (r < rows) ? bits[r0 * nw + q] : 0u;
+    }
+    for (int k = tid; k < 128; k += kThreads) {
+      T u = ScalarTraits<T>::zero();
+      if (k < rows) {
+        const float2 wv = w_out[r0 + k];
+        const float f = wts ? fs * wts[r0 + k] : fs;
+        if constexpr (CPLX) u = make_float2((wv.x - mr) * f, (wv.y - mi) * f);
+        else u = (wv.x - mr) * f;
+      }
+      s_u[k] = u;
+    }
+    __syncthreads();
+    // Sigma^T: item (site r, samples 8 k8 .. 8 k8 + 7), consecutive threads -> consecutive 16-byte rows
+    for (int it = tid; it < 128 * 16; it += kThreads) {
+      const int r = it & 127, k8 = it >> 7;
+      uint16_t vv[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int k = 8 * k8 + q;
+        uint16_t x = 0;
+        if (k < rows) {
+          if (r < ns) x = ((s_bits[(r >> 5) * 128 + k] >> (r & 31)) & 1u) ? 0x3F80u : 0xBF80u;
+          else if (r == 127) x = 0x3F80u;                  // ones row: D[127] = sum_s Q_s = g_b
+        }
+        vv[q] = x;
+      }
+      *reinterpret_cast<uint4*>(sA + umma::kmajor_offset(r, 8 * k8, 128)) = pack8(vv);
+    }
+    // g_a[i] += sum_s sigma_si u_s (four threads per site, uniform trip count for the shuffles)
+    for (int base = 0; base < ns * 4; base += kThreads) {
+      const int it = base + tid;
+      const bool act = it < ns * 4;
+      const int i = act ? (it >> 2) : 0, grp = it & 3;
+      T ga = ScalarTraits<T>::zero();
+      for (int k = grp; act && k < rows; k += 4) {
+        const float sg = ((s_bits[(i >> 5) * 128 + k] >> (i & 31)) & 1u) ? 1.f : -1.f;
+        ga = addx(ga, scal(sg, s_u[k]));
+      }
+      if constexpr (CPLX) {
+        ga.x += __shfl_xor_sync(0xffffffffu, ga.x, 1);
+        ga.y += __shfl_xor_sync(0xffffffffu, ga.y, 1);
+        ga.x += __shfl_xor_sync(0xffffffffu, ga.x, 2);
+        ga.y += __shfl_xor_sync(0xffffffffu, ga.y, 2);
+      } else {
+        ga += __shfl_xor_sync(0xffffffffu, ga, 1);
+        ga += __shfl_xor_sync(0xffffffffu, ga, 2);
+      }
+      if (act && grp == 0) s_ga[i] = addx(s_ga[i], ga);
+    }
+    for (int h = 0; h < nq; ++h, ++gq) {
+      const int b = gq & 1;
+      const int m0 = h * NQ, nqu = (Mp - m0 < NQ) ? Mp - m0 : NQ;
+      if (gq >= 2) {                                       // buffer b: the MMAs of chunk gq - 2 are done
+        if (tid == 0 && !umma::mbar_wait(&qbar[b], ((gq - 2) >> 1) & 1, kWaitLimit))
+          record_error(status, QES_ERR_TIMEOUT);
+        __syncthreads();
+      }
+      uint8_t* qb = sQ + b * SV_QBUF;
+      // item (unit n, samples 8 k8 .. 8 k8 + 7): consecutive threads take consecutive units, so the
+      // loads of T (one sample row at a time) are coalesced and the 16-byte stores conflict-free
+      for (int it = tid; it < nqu * 16; it += kThreads) {
+        const int n = it % nqu, k8 = it / nqu;
+        const int m = m0 + n;
+        float qr[8], qi[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int k = 8 * k8 + q;
+          float tr_ = 0.f, ti_ = 0.f;
+          if (m < nh && k < rows) {
+            const int64_t e = (r0 + k) * (int64_t)nh + m;
+            tr_ = tre(tt, e);
+            ti_ = tim(tt, e);
+          }
+          const T u = s_u[k];
+          if constexpr (CPLX) {
+            qr[q] = tr_ * u.x + ti_ * u.y;                 // conj(t) u
+            qi[q] = tr_ * u.y - ti_ * u.x;
+          } else {
+            qr[q] = tr_ * u;
+            qi[q] = 0.f;
+          }
+        }
+        uint32_t rh[4], rl[4];
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) split2_bf16(qr[2 * q2], qr[2 * q2 + 1], rh[q2], rl[q2]);
+        const uint32_t offr = umma::kmajor_offset(n, 8 * k8, SV_QROWS);
+        *reinterpret_cast<uint4*>(qb + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        *reinterpret_cast<uint4*>(qb + SV_QTERM + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+        if constexpr (CPLX) {
+          uint32_t ih[4], il[4];
+#pragma unroll
+          for (int q2 = 0; q2 < 4; ++q2) split2_bf16(qi[2 * q2], qi[2 * q2 + 1], ih[q2], il[q2]);
+          const uint32_t offi = umma::kmajor_offset(NQ + n, 8 * k8, SV_QROWS);
+          *reinterpret_cast<uint4*>(qb + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+          *reinterpret_cast<uint4*>(qb + SV_QTERM + offi) = make_uint4(il[0], il[1], il[2], il[3]);
+        }
+      }
+      umma::fence_proxy_async_smem();                     // generic-proxy stores -> tensor core
+      __syncthreads();
+      if (tid == kThreads - 1) {
+        // D_re[:, m0 ..) (+ D_im[:, im_off + m0 ..)) += Sigma^T Q^T_hi + Sigma^T Q^T_lo over K = 128
+        umma::tc_fence_after();
+        const uint32_t idesc = umma::idesc_bf16_f32(128, (uint32_t)nqu);
+        const uint32_t qa = q_addr + (uint32_t)b * SV_QBUF;
+        for (int kk = 0; kk < 8; ++kk) {
+          const uint64_t ad = umma::smem_desc(a_addr + 2u * kk * 128u * 16u, 128u * 16u, 128u);
+          for (int term = 0; term < 2; ++term) {
+            for (int half = 0; half < (CPLX ? 2 : 1); ++half) {
+              const uint64_t bd = umma::smem_desc(qa + (uint32_t)term * SV_QTERM + (uint32_t)half * (NQ / 8) * 128u +
+                                                      2u * kk * SV_QROWS * 16u,
+                                                  SV_QROWS * 16u, 128u);
+              umma::mma_bf16(tbase + (uint32_t)(half * d.im_off + m0), ad, bd, idesc,
+                             (j > 0 || kk > 0 || term > 0) ? 1u : 0u);
+            }
+          }
+        }
+        umma::mma_commit(&qbar[b]);
+      }
+    }
+  }
+  if (tid == kThreads - 1) umma::mma_commit(fin);          // arrives once every MMA above is done
+  __syncthreads();
+  if (!umma::mbar_wait(fin, 0, kWaitLimit)) record_error(status, QES_ERR_TIMEOUT);
+  umma::tc_fence_after();
+
+  // ---------------------------------------------------------------- the CTA's partial P-vector
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  T* out = partial + (int64_t)blockIdx.x * P;
+  const int quarter = warp & 3, cg = warp >> 2;
+  const int i = 32 * quarter + lane;                       // site row of the accumulator
+  const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+  // the W block is staged row by row (16-byte row starts, an odd number of 16-byte units) in the
+  // freed operand buffers and written out by whole warps along each row
+  constexpr int EV = 16 / (int)sizeof(T);
+  int ldm = (nh + EV - 1) / EV * EV;
+  if (((ldm / EV) & 1) == 0) ldm += EV;
+  const bool staged = (size_t)ns * ldm * sizeof(T) <= (size_t)d.sv_region;
+  T* stage = reinterpret_cast<T*>(smem);
+  for (int c = cg; c < Mp / 16; c += kColGroups) {
+    const int c0 = 16 * c;
+    float gr[16], gi[16];
+    if constexpr (CPLX) umma::tmem_ld16x2(lane_addr + c0, lane_addr + d.im_off + c0, gr, gi);
+    else umma::tmem_ld16(lane_addr + c0, gr);
+    if (staged && i < ns) {
+      T* rw = stage + (size_t)i * ldm;
+      if (c0 + 16 <= ldm) {
+        float4* dst = reinterpret_cast<float4*>(rw + c0);
+        if constexpr (CPLX) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) dst[q] = make_float4(gr[2 * q], gi[2 * q], gr[2 * q + 1], gi[2 * q + 1]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) dst[q] = make_float4(gr[4 * q], gr[4 * q + 1], gr[4 * q + 2], gr[4 * q + 3]);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int m = c0 + q;
+          if (m < nh) {
+            if constexpr (CPLX) rw[m] = make_float2(gr[q], gi[q]);
+            else rw[m] = gr[q];
+          }
+        }
+      }
+    } else if (i < ns || i == 127) {
+      T* rowp = (i == 127) ? out + ns : out + ns + nh + (int64_t)i * nh;   // row 127 = g_b
+      const bool vec = (c0 + 16 <= nh) && ((reinterpret_cast<uintptr_t>(rowp + c0) & 15) == 0);
+      if (vec) {
+        float4* dst = reinterpret_cast<float4*>(rowp + c0);
+        if constexpr (CPLX) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) dst[q] = make_float4(gr[2 * q], gi[2 * q], gr[2 * q + 1], gi[2 * q + 1]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) dst[q] = make_float4(gr[4 * q], gr[4 * q + 1], gr[4 * q + 2], gr[4 * q + 3]);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int m = c0 + q;
+          if (m < nh) {
+            if constexpr (CPLX) rowp[m] = make_float2(gr[q], gi[q]);
+            else rowp[m] = gr[q];
+          }
+        }
+      }
+    }
+  }
+  for (int e = tid; e < ns; e += kThreads) out[e] = s_ga[e];
+  if (staged) {
+    __syncthreads();
+    T* dstW = out + ns + nh;
+    const bool vec = ((reinterpret_cast<uintptr_t>(dstW) & 15) == 0) && (nh % EV == 0);
+    for (int r = warp; r < ns; r += kWarps) {
+      const T* src = stage + (size_t)r * ldm;
+      T* dst = dstW + (int64_t)r * nh;
+      if (vec) {
+        for (int q = lane; q < nh / EV; q += 32)
+          reinterpret_cast<float4*>(dst)[q] = reinterpret_cast<const float4*>(src)[q];
+      } else {
+        for (int q = lane; q < nh; q += 32) dst[q] = src[q];
+      }
+    }
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tbase, d.tmem_cols);
+}
+
+// ================================================================================================
 // host side
 // ================================================================================================
 static int pow2_at_least(int x) {
@@ -1082,9 +1572,27 @@ static int pow2_at_least(int x) {
 // hidden units per N chunk and target CTA count of the M/N-tiled O^H u (0 = automatic)
 static std::atomic<int> g_tile_mode{0}, g_tile_nc{0}, g_tile_ctas{0};
 static std::atomic<int> g_ohu_pairs{0};      // measured slower on B200 (heis 10x10: 49.5 vs 46.2 us per CG iteration)
+static std::atomic<int> g_sv{1};             // fused S v kernel where the tiling admits it
 extern "C" int qes_sr_set_ohu_pairs(int on) {
   g_ohu_pairs.store(on ? 1 : 0);
   return QES_OK;
+}
+extern "C" int qes_sr_set_fused_sv(int on) {
+  g_sv.store(on ? 1 : 0);
+  return QES_OK;
+}
+
+// SM count of the current device (cached per device; 148 when it cannot be read)
+static int tc_sm_count() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
 }
 extern "C" int qes_sr_set_tiling(int mode, int nc, int ctas) {
   if (mode < 0 || mode > 2 || nc < 0 || (nc % 16) != 0 || ctas < 0) {
@@ -1145,6 +1653,22 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
     t.cl = (g_ohu_pairs.load() && fits && t.n_chunks >= 2) ? 2 : 1;
     t.nsplit = (t.n_chunks + t.cl - 1) / t.cl;
     t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh + ns) * tsz + 64);
+    // fused S v: the shared region holds the O v pipeline, later Sigma^T and two Q^T buffers; one CTA
+    // per SM at most (launch bounds cap the registers at 128 per thread), so sv_grid CTAs are resident
+    if (g_sv.load() != 0) {
+      const int nsp = (ns + 1) & ~1, nw = (ns + 31) / 32;
+      for (int S2 = 4; S2 >= 2 && !t.sv; --S2) {
+        const size_t region = std::max<size_t>((size_t)S2 * stage, SV_SIG_BYTES + 2u * SV_QBUF);
+        const size_t extra = 8u * (2 * S2 + 4) + 16 + (size_t)(2 * nsp + 128) * tsz + 512u * nw + 16;
+        if (region + extra <= kTcSmemLimit) {
+          t.sv = true;
+          t.sv_stages = S2;
+          t.sv_region = (int)region;
+          t.sv_smem = (int)(region + extra);
+        }
+      }
+      t.sv_grid = (int)std::min<int64_t>(t.n_tiles, tc_sm_count());
+    }
     *dout = t;
     return true;
   }
@@ -1192,7 +1716,7 @@ static size_t sz_vp(const TcDims& d) { return (size_t)d.NB * d.Kd * 2 * 2; }
 
 size_t tc_workspace_bytes(const TcDims& d) {
   return al256(sz_t_rows(d)) + al256(sz_t_cols(d)) + al256(sz_sig_cols(d)) + al256(sz_vp(d)) +
-         al256((size_t)d.n_tiles * sizeof(double2)) + al256(sizeof(int) * 4);
+         al256((size_t)d.n_tiles * sizeof(double2)) + al256(sizeof(int) * 4) + al256(sizeof(unsigned int) * 64);
 }
 
 TcWork tc_layout(const TcDims& d, char* base) {
@@ -1204,6 +1728,7 @@ TcWork tc_layout(const TcDims& d, char* base) {
   w.vp = (uint16_t*)(base + off); off += al256(sz_vp(d));
   w.wsum = (double2*)(base + off); off += al256((size_t)d.n_tiles * sizeof(double2));
   w.status = (int*)(base + off); off += al256(sizeof(int) * 4);
+  w.bar = (unsigned int*)(base + off); off += al256(sizeof(unsigned int) * 64);
   return w;
 }
 
@@ -1216,6 +1741,8 @@ static int tc_set_attrs() {
   QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
   QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_big_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemLimit));
+  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_sv_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
   return QES_OK;
 }
@@ -1257,6 +1784,7 @@ int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_
   int rc = (dtype == QES_DTYPE_C64) ? tc_set_attrs<float2, double2>() : tc_set_attrs<float, double>();
   if (rc) return rc;
   QES_CUDA_CHECK(cudaMemsetAsync(w.status, 0, sizeof(int), st));
+  QES_CUDA_CHECK(cudaMemsetAsync(w.bar, 0, sizeof(unsigned int) * 64, st));
   if (d.big)
     tc_sigma_cols_big_kernel<<<1184, 256, 0, st>>>(d.ns, d.MT * 128, d.KC, n_samples, d.n_chunks, bits, w.sig_cols);
   else
@@ -1277,9 +1805,36 @@ int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_
 }
 
 template <class T, class V>
-static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const V* v, float2* w_out,
-                       T* partial, const TcWork& w, cudaStream_t st, bool build_vp, const double* cg_done) {
+static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const T* tt, const V* v,
+                       float2* w_out, T* partial, const TcWork& w, cudaStream_t st, bool build_vp,
+                       const double* cg_done, BarCfg bc) {
   const bool cplx = ScalarTraits<T>::is_complex;
+  if (d.sv) {
+    // one cooperative launch (every CTA resident: the mean of w is a grid barrier), after an
+    // ordinary launch that builds V' on the first iteration
+    if (build_vp) {
+      const int items = d.NB * (d.Kd / 8);
+      tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
+      QES_LAUNCH_CHECK();
+    }
+    const int pf = qes_prof_begin(QES_PROF_SV, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)d.sv_grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = (size_t)d.sv_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    QES_CUDA_CHECK(cudaLaunchKernelEx(&cfg, tc_sv_kernel<T, V>, d, n_samples, bits, v, tt,
+                                      (const uint16_t*)w.t_rows, (const uint16_t*)w.vp, w_out, w.wsum, partial,
+                                      w.status, cg_done, w.wts, 1.0 / (double)n_samples, w.bar, bc));
+    QES_LAUNCH_CHECK();
+    qes_prof_end(pf, st);
+    return QES_OK;
+  }
   // the CG iteration's kernels form a programmatic-dependent-launch chain (qes_launch_pdl)
   if (build_vp) {
     // first iteration: an ordinary launch, so that everything before it (the setup that clears the
@@ -1330,13 +1885,14 @@ int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, c
   return tc_ov_t<float, double>(d, n_samples, bits, (const double*)v, w_out, w, st);
 }
 
-int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
-              void* partial, const TcWork& w, cudaStream_t st, bool build_vp, const double* cg_done) {
+int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
+              const void* v, float2* w_out, void* partial, const TcWork& w, cudaStream_t st, bool build_vp,
+              const double* cg_done, BarCfg bc) {
   if (dtype == QES_DTYPE_C64)
-    return tc_matvec_t<float2, double2>(d, n_samples, bits, (const double2*)v, w_out, (float2*)partial, w, st,
-                                        build_vp, cg_done);
-  return tc_matvec_t<float, double>(d, n_samples, bits, (const double*)v, w_out, (float*)partial, w, st, build_vp,
-                                    cg_done);
+    return tc_matvec_t<float2, double2>(d, n_samples, bits, (const float2*)tanh_theta, (const double2*)v, w_out,
+                                        (float2*)partial, w, st, build_vp, cg_done, bc);
+  return tc_matvec_t<float, double>(d, n_samples, bits, (const float*)tanh_theta, (const double*)v, w_out,
+                                    (float*)partial, w, st, build_vp, cg_done, bc);
 }
 
 int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,

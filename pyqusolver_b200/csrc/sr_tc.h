@@ -27,7 +27,17 @@ struct TcDims {
   // NR = NC (real) or 2 NC (complex) operand rows), and one CTA folds SPC sample chunks into TMEM
   bool big;
   int MT, NC, NR, nnc, SPC;
+  // fused S v (tc_sv_kernel, single-M-tile problems): one cooperative launch of sv_grid CTAs, each
+  // taking every sv_grid-th 128-sample tile and writing one partial P-vector; sv_region bytes of
+  // shared memory hold the O v pipeline (sv_stages stages), then Sigma^T and two Q^T chunk buffers
+  bool sv;
+  int sv_grid, sv_stages, sv_region, sv_smem;
 };
+
+// Configuration of a bounded grid barrier: `extra` arrivals that never come and a short poll limit
+// make every wait run out (a test hook); zero / kGridBarLimit in normal use.
+struct BarCfg { unsigned int extra; unsigned int limit; };
+constexpr unsigned int kGridBarLimit = 1u << 24;     // polls (with a short sleep) before giving up
 
 struct TcWork {
   uint16_t* t_rows;     // ov A: per tile and K chunk, hi/lo BF16 tiles of T
@@ -36,6 +46,7 @@ struct TcWork {
   uint16_t* vp;         // ov B: V' hi/lo BF16 tiles (per CG iteration)
   double2* wsum;        // n_tiles partial sums of w = O v (weighted by wts when given)
   int* status;          // first error code of a bounded wait
+  unsigned int* bar;    // grid barrier of tc_sv_kernel: count at [0], generation at [32]
   const float* wts;     // per-sample weights normalised to sum Ns (nullptr: uniform); set per call
 };
 
@@ -47,11 +58,14 @@ TcWork tc_layout(const TcDims& d, char* base);
 // once per VMC step: BF16 tiles of T, T^T and Sigma^T
 int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
                     const TcWork& w, cudaStream_t st);
-// w_out = O v, partial[chunk] = O^H (wts (w - mean w) / Ns) with mean w = sum wts w / Ns (wts = 1 when
-// w.wts is null); cg_done (optional): a CG solve's converged flag, on which the kernels skip their work
-int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
-              void* partial, const TcWork& w, cudaStream_t st, bool build_vp = true,
-              const double* cg_done = nullptr);
+// w_out = O v, partial[split] = O^H (wts (w - mean w) / Ns) with mean w = sum wts w / Ns (wts = 1 when
+// w.wts is null), split over tc_matvec_nsplit(d) partial P-vectors; tanh_theta is T itself (float32 /
+// complex64, Ns x nh), read by the fused kernel; cg_done (optional): a CG solve's converged flag, on
+// which the kernels skip their work
+int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,
+              const void* v, float2* w_out, void* partial, const TcWork& w, cudaStream_t st, bool build_vp = true,
+              const double* cg_done = nullptr, BarCfg bc = BarCfg{0u, kGridBarLimit});
+inline int tc_matvec_nsplit(const TcDims& d) { return d.sv ? d.sv_grid : d.nsplit; }
 // w_out = O v only (builds the V' operand from v first)
 int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
           const TcWork& w, cudaStream_t st);

@@ -402,8 +402,9 @@ class NQS:
         its results (the reference's chunking-invariance test); the kernels here need no chunking.
         Every option whose effect is not implemented raises (no silent drop): other ODE integrators or
         optimisers, phase and named schedulers, early stopping, excited states (``lower_states``),
-        regularisation, symmetrisation, preconditioners, other linear solvers.  ``lin_force_mat=True``
-        forms S on the tensor cores and solves it by a float64 Cholesky factorisation."""
+        regularisation, symmetrisation, preconditioners other than ``"jacobi"``, other linear solvers.
+        ``pre_solver="jacobi"`` preconditions the CG by 1 / diag(S + shift); ``lin_force_mat=True`` forms S
+        on the tensor cores and solves it by a float64 Cholesky factorisation."""
         unsupported = {
             "ode_solver": ode_solver not in ("Euler", "euler", None),
             "optimizer": optimizer not in ("sgd", "SGD", None),
@@ -412,7 +413,8 @@ class NQS:
             "reg": bool(reg), "lin_sigma": lin_sigma is not None,
             "symmetrize": bool(symmetrize), "update_kwargs": bool(update_kwargs), "n_update": n_update is not None,
             "background": bool(background), "exact_method": exact_method is not None,
-            "pre_solver": pre_solver not in (None, "identity", "none"),
+            "pre_solver": pre_solver is not None and str(getattr(pre_solver, "name", pre_solver)).lower() not in (
+                "identity", "none", "jacobi"),
             "lr_scheduler": lr_scheduler is not None and not callable(lr_scheduler),
             "diag_scheduler": diag_scheduler is not None and not callable(diag_scheduler),
         }
@@ -442,7 +444,7 @@ class NQS:
             self._tdvp = TDVP(use_sr=use_sr, use_minsr=use_minsr, rhs_prefactor=rhs_prefactor, sr_lin_solver=lin_solver,
                               sr_diag_shift=diag_shift, sr_tol=sr_tol, sr_maxiter=sr_maxiter, grad_clip=grad_clip,
                               sr_lin_solver_t="gram" if lin_is_gram else "matvec",
-                              sr_form_matrix=bool(lin_force_mat))
+                              sr_form_matrix=bool(lin_force_mat), sr_precond=pre_solver)
         stats = NQSTrainStats(seed=self._seed)
         if exact_predictions is not None:
             stats.exact_predictions = np.atleast_1d(np.asarray(exact_predictions))

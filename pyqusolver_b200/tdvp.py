@@ -59,8 +59,14 @@ class TDVP:
         if solver not in _SOLVERS_CG + _SOLVERS_DIRECT:
             raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG (scipy_cg) "
                                       f"and, on the formed matrix, a Cholesky solve")
-        if sr_precond not in (None, "identity", "none"):
-            raise NotImplementedError(f"preconditioner {sr_precond!r} is not implemented on the GPU path")
+        precond = None if sr_precond is None else str(getattr(sr_precond, "name", sr_precond)).lower()
+        if precond in ("identity", "none"):
+            precond = None
+        if precond not in (None, "jacobi"):
+            raise NotImplementedError(f"preconditioner {sr_precond!r}: the GPU path implements 'jacobi' "
+                                      f"(1 / diag(S + shift)) and none")
+        if precond is not None and use_minsr:
+            raise NotImplementedError("a preconditioner on the MinSR (sample-space) system is not implemented")
         if str(sr_lin_solver_t).lower() not in ("gram", "matvec", "matrix_free"):
             raise NotImplementedError(f"solver form {sr_lin_solver_t!r}: the GPU path applies S matrix-free")
         if solver in _SOLVERS_DIRECT and not sr_form_matrix:
@@ -70,6 +76,9 @@ class TDVP:
         # formed matrix: S on the tensor cores, solved by a float64 Cholesky factorisation (the CG
         # solution it stands for is the same solution to within the CG tolerance)
         self.form_matrix = bool(sr_form_matrix)
+        # Jacobi: CG on S + shift preconditioned by 1 / diag(S + shift) (a direct solve of the formed
+        # matrix gives the same solution with or without it)
+        self.sr_precond = precond
         self._dense_ws = None
         if regularization:
             raise NotImplementedError("regularization != 0 is not implemented on the GPU path")
@@ -148,7 +157,7 @@ class TDVP:
             x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
                                      rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,
                                      check_every=self.check_every, rhs_prefactor=self.rhs_prefactor, workspace=ws,
-                                     x0=x0, probs=probs)
+                                     x0=x0, probs=probs, precond=self.sr_precond)
             self.last_info = info
             self._solution = x.detach().clone()
         if self.grad_clip is not None and self.grad_clip > 0:

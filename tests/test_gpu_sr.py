@@ -158,3 +158,116 @@ def test_train_step_uses_the_sampler_weights():
     assert info["mean"] == pytest.approx(complex(st[0], st[1]), rel=1e-12)
     step = (nqs.net.master - flat0) / 0.1
     assert torch.allclose(step, x_ref, rtol=1e-9, atol=1e-12)
+
+
+# ------------------------------------------------------------------------- fused S v kernel
+@pytest.mark.parametrize("cplx", [True, False])
+@pytest.mark.parametrize("n", [700, 19244])
+def test_fused_sv_matches_kernel_pair_and_oracle(cplx, n):
+    """The cooperative S v kernel (qes_sr_set_fused_sv(1), the default) against the O v + O^H u kernel
+    pair (0) on the same weighted batch, and both against the oracle's weighted S v.  n = 19244 is
+    151 sample tiles (the last one 44 samples): more tiles than CTAs, so some CTAs fold two tiles
+    into their TMEM accumulators."""
+    ns, nh = 9, 18
+    model = qb.XXZ(qb.SquareLattice(2, 3, 3), jxy=-1.0, jz=-1.0, hx=0.4)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=8, init_scale=0.2)
+    rng = np.random.default_rng(8)
+    st = np.where(rng.random((n, ns)) < 0.5, 0.5, -0.5)
+    bits = dv.pack_states(st)
+    _, tn, lp = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=True)
+    lu = lp.real.double().cpu().numpy()
+    pr = np.exp(lu - lu.max())
+    probs_t = torch.as_tensor((pr / pr.sum() * n).astype(np.float32)).cuda()
+    w = probs_t.double().cpu().numpy()
+    w = w / w.sum() * n
+    O = osr.o_rows(None, orbm.to_sigma(st), tanh=tn.cpu().numpy())
+    _, Oc, w_, _, _ = osr.prepare(np.zeros(n), O, w)
+    S = osr.s_matrix(Oc, w_)
+    v = rng.normal(size=O.shape[1]) + (1j * rng.normal(size=O.shape[1]) if cplx else 0)
+    vt = torch.as_tensor(v).cuda()
+    ys = {}
+    _lib.set_sr_impl(2)
+    try:
+        for fused in (1, 0):
+            _lib.call("qes_sr_set_fused_sv", fused)
+            assert _lib.sr_uses_tensor_cores(dv.dtype_code(net.flat), ns, nh, n)
+            ys[fused] = dv.sr_matvec(net.flat, ns, nh, bits, tn, vt, shift=1e-3, probs=probs_t).cpu().numpy()
+            again = dv.sr_matvec(net.flat, ns, nh, bits, tn, vt, shift=1e-3, probs=probs_t).cpu().numpy()
+            assert np.array_equal(ys[fused], again)              # fixed summation order: repeatable
+    finally:
+        _lib.call("qes_sr_set_fused_sv", 1)
+        _lib.set_sr_impl(0)
+    ref = S @ v + 1e-3 * v
+    assert rel_err(ys[1], ref) < 1e-4
+    assert rel_err(ys[0], ref) < 1e-4
+    assert rel_err(ys[1], ys[0]) < 2e-5
+
+
+# ------------------------------------------------------------------------- Jacobi-preconditioned CG
+@pytest.mark.parametrize("cplx,impl,fused", [(True, 0, 0), (True, 0, 2), (True, 1, 0), (False, 0, 0),
+                                             (False, 1, 2)])
+def test_jacobi_pcg_matches_oracle(cplx, impl, fused):
+    """qes_sr_solve_cg with QES_PRECOND_JACOBI (TDVP(sr_precond="jacobi")): the solution of the weighted
+    SR system against a dense float64 solve (backward error, A-norm error), and the iteration count
+    against the oracle's preconditioned CG on the same float64 system; the diagonal is the weighted
+    diag(S) + shift.  fused = 2 runs the vector updates in the cooperative CG kernel."""
+    ns, nh, n = 9, 18, 700
+    model = qb.XXZ(qb.SquareLattice(2, 3, 3), jxy=-1.0, jz=-1.0, hx=0.4)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=5, init_scale=0.3)
+    rng = np.random.default_rng(5)
+    st = np.where(rng.random((n, ns)) < 0.5, 0.5, -0.5)
+    bits = dv.pack_states(st)
+    _, tn, lp = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=True)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    lu = lp.real.double().cpu().numpy()
+    pr = np.exp(0.5 * (lu - lu.max()))
+    probs_t = torch.as_tensor((pr / pr.sum() * n).astype(np.float32)).cuda()
+    w = probs_t.double().cpu().numpy()
+    w = w / w.sum() * n
+    e = eloc.cpu().numpy().astype(np.complex128)
+    if not cplx:
+        e = e.real
+    O = osr.o_rows(None, orbm.to_sigma(st), tanh=tn.cpu().numpy())
+    ec, Oc, w_, _, _ = osr.prepare(e, O, w)
+    F = osr.force(Oc, ec, w_)
+    shift = 1e-2
+    A = osr.s_matrix(Oc, w_) + shift * np.eye(O.shape[1])
+    minv = osr.jacobi_minv(Oc, w_, shift)
+    assert np.allclose(1.0 / minv, np.real(np.diag(A)), rtol=1e-12)
+    _, it_ref, _, conv_ref = osr.cg(lambda v: A @ v, F, rtol=1e-8, maxiter=3000, minv=minv)
+    _, it_plain, _, _ = osr.cg(lambda v: A @ v, F, rtol=1e-8, maxiter=3000)
+    assert conv_ref
+    _lib.set_sr_impl(impl)
+    _lib.call("qes_set_cg_fused", fused)
+    try:
+        x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=1e-8, maxiter=3000,
+                                 probs=probs_t, precond="jacobi", check_every=4)
+    finally:
+        _lib.call("qes_set_cg_fused", 1)
+        _lib.set_sr_impl(0)
+    assert info["converged"]
+    xg = -x.cpu().numpy()
+    assert np.linalg.norm(A @ xg - F) / np.linalg.norm(F) < 1e-4
+    xr = np.linalg.solve(A, F)
+    err = xg - xr
+    assert np.sqrt(abs(np.vdot(err, A @ err)) / abs(np.vdot(xr, A @ xr))) < 1e-3
+    # float32 operator vs float64: the iteration counts agree to a few percent
+    assert abs(info["iterations"] - it_ref) <= max(3, 0.05 * it_ref), (info["iterations"], it_ref, it_plain)
+
+
+def test_tdvp_jacobi_option_reaches_the_solver():
+    """TDVP(sr_precond="jacobi") and NQS.train(pre_solver="jacobi") run the preconditioned CG (the
+    iteration count differs from the plain CG on the same batch); unknown preconditioners raise."""
+    from pyqusolver_b200.tdvp import TDVP
+    net, bits, tn, eloc = _small_problem(cplx=True)
+    plain = TDVP(rhs_prefactor=-1.0, sr_diag_shift=1e-2, sr_maxiter=2000)
+    jac = TDVP(rhs_prefactor=-1.0, sr_diag_shift=1e-2, sr_maxiter=2000, sr_precond="jacobi")
+    x0 = plain.solve(net, bits, tn, eloc)
+    x1 = jac.solve(net, bits, tn, eloc)
+    assert plain.last_info["converged"] and jac.last_info["converged"]
+    assert plain.last_info["iterations"] != jac.last_info["iterations"]
+    assert torch.allclose(x0, x1, rtol=1e-3, atol=1e-5 * float(x0.abs().max()))
+    with pytest.raises(NotImplementedError):
+        TDVP(sr_precond="ilu")

@@ -231,3 +231,30 @@ def test_tdvp_initial_guess_selection():
     td2 = TDVP(rhs_prefactor=-1.0, sr_lin_x0=torch.ones(4, dtype=torch.float64))
     assert torch.equal(td2._solve_handle_x0(4, False), torch.ones(4, dtype=torch.float64))
     assert td2._solve_handle_x0(3, False) is None
+
+
+def test_oracle_pcg_matches_scipy_cg_with_jacobi_preconditioner():
+    """The oracle's preconditioned CG (z = M r, stopping rule on ||r||) reproduces SciPy's cg(M=...)
+    iterate for iterate on a weighted SR system."""
+    import numpy as np
+    import scipy.sparse.linalg as sla
+    from oracle import sr as osr
+    rng = np.random.default_rng(3)
+    O = rng.normal(size=(300, 40)) + 1j * rng.normal(size=(300, 40))
+    O[:, :5] *= 10.0                                       # badly scaled columns: Jacobi matters
+    e = rng.normal(size=300) + 1j * rng.normal(size=300)
+    w = rng.random(300) + 0.5
+    ec, Oc, w_, _, _ = osr.prepare(e, O, w)
+    A = osr.s_matrix(Oc, w_) + 1e-3 * np.eye(40)
+    F = osr.force(Oc, ec, w_)
+    minv = osr.jacobi_minv(Oc, w_, 1e-3)
+    x, it, res, conv = osr.cg(lambda v: A @ v, F, rtol=1e-10, maxiter=500, minv=minv)
+    count = [0]
+    xs, info = sla.cg(A, F, rtol=1e-10, atol=0.0, maxiter=500, M=sla.LinearOperator(A.shape, matvec=lambda r: minv * r,
+                                                                                     dtype=A.dtype),
+                      callback=lambda xk: count.__setitem__(0, count[0] + 1))
+    assert conv and info == 0
+    assert it == count[0]
+    assert np.allclose(x, xs, rtol=1e-9, atol=1e-12 * np.abs(xs).max())
+    _, it_plain, _, _ = osr.cg(lambda v: A @ v, F, rtol=1e-10, maxiter=500)
+    assert it < it_plain

@@ -302,6 +302,9 @@ typedef struct {
                                   or BF16-split contractions it levels off near their
                                   rounding (~1e-6-1e-5) while the recursive residual keeps
                                   falling; no counterpart in the reference (float64 SR). */
+    double acond;              /* MINRES: max / min of the rotated diagonal (gamma_k), the
+                                  estimate of cond(S + shift) that MINRES-QLP compares
+                                  with its switch threshold; -1 for the other solvers.   */
 } qes_sr_result;
 
 int qes_sr_workspace_bytes(int dtype, int ns, int nh, int64_t n_samples, size_t* bytes);
@@ -420,6 +423,19 @@ int qes_sr_solve_cg_weighted(int dtype, int ns, int nh, int64_t n_samples, const
                              const qes_sr_options* opt, const void* x0, void* x_out,
                              qes_sr_result* result, void* workspace, size_t workspace_bytes,
                              void* stream);
+/* The same system solved by MINRES (Paige-Saunders recurrences as in SciPy's
+ * minres, no preconditioner): same force, matvec, workspace, x0 and
+ * rhs_prefactor handling as the CG; it stops when the recurrence's residual
+ * norm phibar <= max(rtol ||F||, atol) (the CG's rule) and reports the
+ * condition estimate in result->acond.  Replaces the 'minres' / 'minres_qlp'
+ * lin_solver of QES/NQS/__init__.py:406 and tdvp.py:322-350 (MINRES-QLP
+ * follows MINRES until the condition estimate passes its switch threshold,
+ * ~1e7 in the published algorithm; the caller can compare result->acond). */
+int qes_sr_solve_minres_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                 const void* tanh_theta, const void* eloc, const float* probs,
+                                 const qes_sr_options* opt, const void* x0, void* x_out,
+                                 qes_sr_result* result, void* workspace, size_t workspace_bytes,
+                                 void* stream);
 /* As qes_sr_solve_cg with an initial guess x0 (device, P float64 / complex128)
  * of the unscaled system (S + shift) x = F, i.e. a previous x_out divided by
  * rhs_prefactor; r0 = F - (S + shift) x0 costs one extra matvec and the stop

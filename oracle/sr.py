@@ -84,6 +84,53 @@ def cg(matvec, b, *, rtol=1e-8, atol=0.0, maxiter=1000, x0=None, minv=None):
     return x, maxiter, np.linalg.norm(r), False
 
 
+def minres(matvec, b, *, rtol=1e-8, atol=0.0, maxiter=1000, x0=None):
+    """MINRES for a Hermitian operator (Paige & Saunders 1975; the recurrences of SciPy's ``minres``
+    without a preconditioner), stopping when the recurrence's residual norm phibar <=
+    max(rtol ||b||, atol), the rule of ``cg``.  The reference selects it with lin_solver 'minres' /
+    'minres_qlp' (``QES/NQS/__init__.py:406``; the solvers live in the absent ``general_python``
+    submodule).  Returns (x, iterations, phibar, converged, acond)."""
+    b = np.asarray(b)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=b.dtype)
+    r1 = b - matvec(x) if x0 is not None else b.copy()
+    y = r1.copy()
+    beta1 = np.sqrt(np.vdot(r1, y).real)
+    thresh = max(rtol * np.linalg.norm(b), atol)
+    if beta1 <= thresh:
+        return x, 0, beta1, True, -1.0
+    oldb, beta, dbar, epsln, phibar = 0.0, beta1, 0.0, 0.0, beta1
+    cs, sn = -1.0, 0.0
+    w = np.zeros_like(b)
+    w2 = np.zeros_like(b)
+    r2 = r1.copy()
+    gmax, gmin = 0.0, np.inf
+    for it in range(1, maxiter + 1):
+        v = y / beta
+        y = matvec(v)
+        if it >= 2:
+            y = y - (beta / oldb) * r1
+        alfa = np.vdot(v, y).real
+        y = y - (alfa / beta) * r2
+        r1, r2 = r2, y
+        oldb, beta = beta, np.sqrt(np.vdot(r2, r2).real)
+        oldeps = epsln
+        delta = cs * dbar + sn * alfa
+        gbar = sn * dbar - cs * alfa
+        epsln = sn * beta
+        dbar = -cs * beta
+        gamma = max(np.hypot(gbar, beta), np.finfo(float).tiny)
+        cs, sn = gbar / gamma, beta / gamma
+        phi, phibar = cs * phibar, sn * phibar
+        w1, w2 = w2, w
+        w = (v - oldeps * w1 - delta * w2) / gamma
+        x = x + phi * w
+        gmax, gmin = max(gmax, gamma), min(gmin, gamma)
+        y = r2
+        if phibar <= thresh or beta == 0.0:
+            return x, it, phibar, True, gmax / gmin
+    return x, maxiter, phibar, False, gmax / gmin
+
+
 def jacobi_minv(O_c, w=None, shift=0.0):
     """Inverse diagonal of S + shift, diag(S)_k = sum_s w_s |O_c,sk|^2 / Ns: the Jacobi preconditioner
     named 'jacobi' by the reference's solver options (``QES/NQS/__init__.py:405-407``,

@@ -84,6 +84,7 @@ class SRResult(C.Structure):
     _fields_ = [
         ("iterations", C.c_int), ("converged", C.c_int), ("residual", C.c_double), ("rhs_norm", C.c_double),
         ("e_mean_re", C.c_double), ("e_mean_im", C.c_double), ("true_residual", C.c_double),
+        ("acond", C.c_double),
     ]
 
 
@@ -141,6 +142,8 @@ SIGNATURES = {
                                _vp],
     "qes_sr_solve_cg_weighted": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
                                  _vp, C.POINTER(SRResult), _vp, _sz, _vp],
+    "qes_sr_solve_minres_weighted": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, C.POINTER(SROptions), _vp,
+                                     _vp, C.POINTER(SRResult), _vp, _sz, _vp],
     "qes_sr_dense_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.c_int, C.POINTER(_sz)],
     "qes_sr_gram": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
     "qes_sr_solve_dense": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, C.POINTER(SROptions), _vp,

@@ -1002,6 +1002,181 @@ __global__ void __launch_bounds__(CF_TX * CF_TY) cg_fused_kernel(int64_t P, int 
 }
 
 // ----------------------------------------------------------------------------
+// MINRES (Paige & Saunders 1975, the recurrences of SciPy's minres without a
+// preconditioner) on the Hermitian S + shift.  The Lanczos vector v is the
+// matvec input (the CG's p buffer, V' tiles on the tensor-core path), y = A v
+// comes out of the split reduction with alpha = v^H A v (its dot partials, the
+// last block's pAp = scal[1]).  State scalars in ms[]:
+//   0 beta   1 oldb   2 dbar   3 epsln   4 phibar   5 cs   6 sn   7 phi
+//   8 delta  9 denom 10 oldeps 11 converged 12 gmax 13 gmin
+// and the shared flags of the CG: scal[2] = phibar^2 (the residual estimate),
+// scal[3] threshold^2, scal[4] done, scal[5] iterations, scal[6] ||b||^2.
+// ----------------------------------------------------------------------------
+// r2 = r1 = b - A x0 (x0 given: Ax0 in y) or b; partial sums of ||r2||^2
+template <class V>
+__global__ void minres_init_kernel(int64_t P, const V* __restrict__ b, const V* __restrict__ Ax0, V* __restrict__ x,
+                                   V* __restrict__ r1, V* __restrict__ r2, V* __restrict__ w1, V* __restrict__ w2,
+                                   bool has_x0) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V rk = has_x0 ? vadd(b[k], vscale(-1.0, Ax0[k])) : b[k];
+    if (!has_x0) x[k] = vzero(V());
+    r1[k] = rk;
+    r2[k] = rk;
+    w1[k] = vzero(V());
+    w2[k] = vzero(V());
+  }
+}
+// parts: ||b||^2 partials, parts_r: ||r0||^2 partials
+__global__ void __launch_bounds__(SC_THREADS) minres_setup_kernel(int n, const double* __restrict__ parts,
+                                                                  const double* __restrict__ parts_r, double rtol,
+                                                                  double atol, double* __restrict__ scal,
+                                                                  double* __restrict__ ms) {
+  const double bb = block_sum_parts(n, parts);
+  __syncthreads();
+  const double rr0 = block_sum_parts(n, parts_r);
+  if (threadIdx.x != 0) return;
+  const double beta1 = sqrt(rr0);
+  scal[6] = bb;
+  const double th = fmax(rtol * sqrt(bb), atol);
+  scal[3] = th * th;
+  scal[2] = rr0;
+  scal[5] = 0.0;
+  scal[4] = (rr0 <= scal[3]) ? 1.0 : 0.0;
+  for (int q = 0; q < 32; ++q) ms[q] = 0.0;
+  ms[0] = beta1;                  // beta
+  ms[4] = beta1;                  // phibar
+  ms[5] = -1.0;                   // cs
+  ms[12] = 0.0;                   // gmax
+  ms[13] = 1e308;                 // gmin
+}
+// v = r2 / beta (the first Lanczos vector; later ones come from minres_update_kernel)
+template <class V>
+__global__ void minres_v_kernel(int64_t P, const V* __restrict__ r2, V* __restrict__ v, const double* __restrict__ ms,
+                                TcDims td, uint16_t* __restrict__ vp) {
+  const double s = ms[0] > 0.0 ? 1.0 / ms[0] : 0.0;
+  const int ns = td.ns, nh = td.nh;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V vk = vscale(s, r2[k]);
+    v[k] = vk;
+    if (vp && k >= ns) {
+      const int64_t q = k - ns;
+      if (q < nh) tc_put_vp_elem(td, vp, ns, (int)q, vk);
+      else tc_put_vp_elem(td, vp, (int)((q - nh) / nh), (int)((q - nh) % nh), vk);
+    }
+  }
+}
+// y = A v - (beta / oldb) r1 - (alpha / beta) r2;  r1 <- r2;  r2 <- y;  ||y||^2.  The last block runs the
+// scalar recurrences: beta_new = ||y||, the Givens rotation that updates the QR factor of the Lanczos
+// tridiagonal, phi / phibar (phibar = the residual norm of the iterate), the convergence test.
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) minres_lanczos_kernel(int64_t P, const V* __restrict__ Av,
+                                                                     V* __restrict__ r1, V* __restrict__ r2,
+                                                                     double* __restrict__ scal, double* __restrict__ ms,
+                                                                     double* __restrict__ part,
+                                                                     unsigned int* __restrict__ counter) {
+  pdl_trigger();
+  pdl_wait();                                              // A v and alpha: previous kernel
+  if (scal[4] != 0.0) return;
+  const double beta = ms[0], oldb = ms[1], alpha = scal[1];
+  const double c1 = oldb > 0.0 ? beta / oldb : 0.0, c2 = beta > 0.0 ? alpha / beta : 0.0;
+  double d = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V r2k = r2[k];
+    const V y = vadd(vadd(Av[k], vscale(-c1, r1[k])), vscale(-c2, r2k));
+    r1[k] = r2k;
+    r2[k] = y;
+    d += vdotc(y, y);
+  }
+  __shared__ double red[RED_THREADS / 32];
+  __shared__ bool last;
+  d = warp_sum(d);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) t += red[q];
+    part[blockIdx.x] = t;
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) v += ((volatile double*)part)[q];
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double yy = 0.0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) yy += red[q];
+    const double bnew = sqrt(yy);
+    const double cs = ms[5], sn = ms[6], dbar = ms[2];
+    const double oldeps = ms[3];
+    const double delta = cs * dbar + sn * alpha;
+    const double gbar = sn * dbar - cs * alpha;
+    const double epsln = sn * bnew;
+    const double dbar_new = -cs * bnew;
+    const double gamma = fmax(hypot(gbar, bnew), 1e-300);
+    const double cs_new = gbar / gamma, sn_new = bnew / gamma;
+    const double phi = cs_new * ms[4];
+    const double phibar = sn_new * ms[4];
+    ms[1] = beta;  ms[0] = bnew;  ms[2] = dbar_new;  ms[3] = epsln;  ms[4] = phibar;
+    ms[5] = cs_new;  ms[6] = sn_new;  ms[7] = phi;  ms[8] = delta;  ms[9] = 1.0 / gamma;  ms[10] = oldeps;
+    ms[12] = fmax(ms[12], gamma);
+    ms[13] = fmin(ms[13], gamma);
+    scal[2] = phibar * phibar;
+    ms[11] = (phibar * phibar <= scal[3] || bnew == 0.0) ? 1.0 : 0.0;
+    *counter = 0u;
+  }
+}
+// w = (v - oldeps w_(k-2) - delta w_(k-1)) / gamma;  x += phi w;  v <- r2 / beta_new (+ its V' tiles); the
+// last block counts the iteration and publishes the convergence found by the Lanczos step
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) minres_update_kernel(int64_t P, V* __restrict__ v, V* __restrict__ w1,
+                                                                    V* __restrict__ w2, V* __restrict__ x,
+                                                                    const V* __restrict__ r2, double* __restrict__ scal,
+                                                                    const double* __restrict__ ms,
+                                                                    unsigned int* __restrict__ counter, TcDims td,
+                                                                    uint16_t* __restrict__ vp) {
+  pdl_trigger();
+  pdl_wait();
+  if (scal[4] != 0.0) return;
+  const double oldeps = ms[10], delta = ms[8], denom = ms[9], phi = ms[7];
+  const double s = ms[0] > 0.0 ? 1.0 / ms[0] : 0.0;
+  const bool conv = ms[11] != 0.0;
+  const int ns = td.ns, nh = td.nh;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V wk = vscale(denom, vadd(vadd(v[k], vscale(-oldeps, w1[k])), vscale(-delta, w2[k])));
+    w1[k] = w2[k];
+    w2[k] = wk;
+    x[k] = vadd(x[k], vscale(phi, wk));
+    if (!conv) {
+      const V vk = vscale(s, r2[k]);
+      v[k] = vk;
+      if (vp && k >= ns) {
+        const int64_t q = k - ns;
+        if (q < nh) tc_put_vp_elem(td, vp, ns, (int)q, vk);
+        else tc_put_vp_elem(td, vp, (int)((q - nh) / nh), (int)((q - nh) % nh), vk);
+      }
+    }
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  scal[5] += 1.0;
+  if (conv) scal[4] = 1.0;
+  *counter = 0u;
+}
+
+// ----------------------------------------------------------------------------
 // workspace layout
 // ----------------------------------------------------------------------------
 struct SRWork {
@@ -1016,6 +1191,8 @@ struct SRWork {
   double* parts;      // [RED_BLOCKS]
   double* scal;       // [16]
   double* dinv;       // [P] Jacobi preconditioner 1 / diag(S + shift)
+  void* mr2; void* mw1; void* mw2;   // [P] of V each: MINRES r2, w_(k-2), w_(k-1)
+  double* mscal;      // [32] MINRES recurrence scalars
   double* tsq;        // [nh] weighted mean of |t_m|^2, then [TSQ_SPLITS][nh] partial sums
   unsigned int* counter;  // [2] last-block tickets (reduce, x/r update)
   bool tc;            // tensor-core matvec in use
@@ -1053,6 +1230,8 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   L.parts = (double*)take(std::max(RED_BLOCKS, RS_MAX_BLOCKS) * sizeof(double));
   L.scal = (double*)take(16 * sizeof(double));
   L.dinv = (double*)take(P * sizeof(double));
+  L.mr2 = take(P * vs); L.mw1 = take(P * vs); L.mw2 = take(P * vs);
+  L.mscal = (double*)take(32 * sizeof(double));
   L.tsq = (double*)take((size_t)(TSQ_SPLITS + 1) * nh * sizeof(double));
   L.counter = (unsigned int*)take(128 * sizeof(unsigned int));     // tickets, barrier words (own lines)
   char* tcb = tc_ok ? take(tc_workspace_bytes(L.td)) : nullptr;
@@ -1823,11 +2002,12 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   if (res) {
     res->iterations = (int)hs[5];
     res->converged = done ? 1 : 0;
-    res->residual = sqrt(hs[4] != 0.0 ? hs[2] : hs[0]);
+    res->residual = sqrt(hs[2]);                         // ||r|| (scal[0] holds rho = r^H D^-1 r with PCG)
     res->rhs_norm = sqrt(hs[6]);
     res->e_mean_re = emean[0];
     res->e_mean_im = emean[1];
     res->true_residual = true_rr < 0.0 ? -1.0 : (hs[6] > 0.0 ? sqrt(true_rr / hs[6]) : 0.0);
+    res->acond = -1.0;
   }
   return done ? QES_OK : QES_ERR_NOT_CONVERGED;
 }
@@ -1853,6 +2033,114 @@ extern "C" int qes_sr_solve_cg_weighted(int dtype, int ns, int nh, int64_t n_sam
                           (double*)x_out, result, L, st, (const double*)x0);
   return sr_cg_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc, opt,
                          (double2*)x_out, result, L, st, (const double2*)x0);
+}
+
+// MINRES on (S + shift) x = F with the same force, matvec kernels and stopping rule as the CG
+// (||r|| <= max(rtol ||b||, atol), ||r|| = phibar of the recurrences); chunks of check_every
+// iterations launched directly, one host check per chunk
+template <class T>
+static int sr_minres_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* eloc,
+                       const qes_sr_options* opt, typename VecT<T>::type* x_out, qes_sr_result* res, const SRWork& L,
+                       cudaStream_t st, const typename VecT<T>::type* x0) {
+  using V = typename VecT<T>::type;
+  const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
+  V* x = (V*)L.x; V* r1 = (V*)L.r; V* v = (V*)L.p; V* y = (V*)L.Ap; V* b = (V*)L.b;
+  V* r2 = (V*)L.mr2; V* w1 = (V*)L.mw1; V* w2 = (V*)L.mw2;
+  int rc = sr_prepare(ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32, n_samples, bits, tt, L, st);
+  if (rc) return rc;
+  rc = sr_force_t<T>(ns, nh, n_samples, bits, tt, eloc, b, L, st);
+  if (rc) return rc;
+  double emean[2] = {0, 0};
+  QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 128 * sizeof(unsigned int), st));
+  if (x0) {
+    QES_CUDA_CHECK(cudaMemcpyAsync(x, x0, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
+    rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, x, y, nullptr, L, st, false);
+    if (rc) return rc;
+  }
+  minres_init_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, y, x, r1, r2, w1, w2, x0 != nullptr);
+  norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, L.parts);
+  norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r2, L.parts + RED_BLOCKS);
+  minres_setup_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, L.parts + RED_BLOCKS, opt->rtol, opt->atol, L.scal,
+                                               L.mscal);
+  minres_v_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r2, v, L.mscal, L.td, (uint16_t*)nullptr);
+  QES_LAUNCH_CHECK_N(5);
+  const int check = opt->check_every > 0 ? opt->check_every : 8;
+  double hs[8] = {0};
+  QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  QES_CUDA_CHECK(cudaStreamSynchronize(st));
+  bool done = hs[4] != 0.0;
+  int it = 0;
+  while (!done && it < opt->maxiter) {
+    const int nrun = std::min(check, opt->maxiter - it);
+    for (int q = 0; q < nrun; ++q) {
+      // y = (S + shift) v and alpha = v^H y (the split reduction's last block: scal[1])
+      rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, v, y, L.parts, L, st, /*vp_ready=*/it + q > 0,
+                          L.scal + 4);
+      if (rc) return rc;
+      QES_CUDA_CHECK(qes_launch_pdl(minres_lanczos_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P,
+                                    (const V*)y, r1, r2, L.scal, L.mscal, L.parts, L.counter + 1));
+      QES_CUDA_CHECK(qes_launch_pdl(minres_update_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P, v, w1,
+                                    w2, x, (const V*)r2, L.scal, (const double*)L.mscal, L.counter + 2, L.td,
+                                    L.tc ? L.tw.vp : (uint16_t*)nullptr));
+      QES_LAUNCH_CHECK_N(2);
+    }
+    it += nrun;
+    QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if ((rc = sr_check_status(L, st, true))) return rc;     // synchronises the stream
+    done = hs[4] != 0.0;
+  }
+  if ((rc = sr_check_status(L, st, true))) return rc;
+  double ms[16] = {0};
+  QES_CUDA_CHECK(cudaMemcpyAsync(ms, L.mscal, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  double true_rr = -1.0;
+  if (opt->maxiter > 0) {
+    rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, x, y, nullptr, L, st, false);
+    if (rc) return rc;
+    diff_norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, y, L.parts);
+    sum_parts_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, L.scal + 10);
+    QES_LAUNCH_CHECK_N(2);
+    QES_CUDA_CHECK(cudaMemcpyAsync(&true_rr, L.scal + 10, sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  if ((rc = sr_check_status(L, st))) return rc;            // synchronises the stream
+  QES_CUDA_CHECK(cudaMemcpyAsync(x_out, x, P * sizeof(V), cudaMemcpyDeviceToDevice, st));
+  if (opt->rhs_prefactor != 1.0) {
+    scale_vec_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, opt->rhs_prefactor, x_out);
+    QES_LAUNCH_CHECK();
+  }
+  if (res) {
+    res->iterations = (int)hs[5];
+    res->converged = done ? 1 : 0;
+    res->residual = sqrt(hs[2]);
+    res->rhs_norm = sqrt(hs[6]);
+    res->e_mean_re = emean[0];
+    res->e_mean_im = emean[1];
+    res->true_residual = true_rr < 0.0 ? -1.0 : (hs[6] > 0.0 ? sqrt(true_rr / hs[6]) : 0.0);
+    res->acond = (ms[13] > 0.0 && ms[13] < 1e300) ? ms[12] / ms[13] : -1.0;
+  }
+  return done ? QES_OK : QES_ERR_NOT_CONVERGED;
+}
+
+extern "C" int qes_sr_solve_minres_weighted(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
+                                            const void* tanh_theta, const void* eloc, const float* probs,
+                                            const qes_sr_options* opt, const void* x0, void* x_out,
+                                            qes_sr_result* result, void* workspace, size_t workspace_bytes,
+                                            void* stream) {
+  QES_ARG_CHECK(ns > 0 && nh > 0 && n_samples > 0 && bits && tanh_theta && eloc && opt && x_out,
+                "qes_sr_solve_minres: bad args");
+  QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_solve_minres: bad dtype");
+  QES_ARG_CHECK(opt->maxiter >= 0 && opt->shift >= 0.0, "qes_sr_solve_minres: bad options");
+  QES_ARG_CHECK(opt->precond == QES_PRECOND_NONE, "qes_sr_solve_minres: no preconditioner on the MINRES path");
+  SRWork L;
+  int rc = check_ws(dtype, ns, nh, n_samples, workspace, workspace_bytes, &L);
+  if (rc) return rc;
+  L.wts = L.tw.wts = probs;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype == QES_DTYPE_F32)
+    return sr_minres_t<float>(ns, nh, n_samples, bits, (const float*)tanh_theta, (const float2*)eloc, opt,
+                              (double*)x_out, result, L, st, (const double*)x0);
+  return sr_minres_t<float2>(ns, nh, n_samples, bits, (const float2*)tanh_theta, (const float2*)eloc, opt,
+                             (double2*)x_out, result, L, st, (const double2*)x0);
 }
 
 extern "C" int qes_sr_solve_cg_x0(int dtype, int ns, int nh, int64_t n_samples, const uint32_t* bits,
@@ -2069,6 +2357,7 @@ static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* 
     res->e_mean_re = emean[0];
     res->e_mean_im = emean[1];
     res->true_residual = -1.0;                          // not computed for the sample-space solve
+    res->acond = -1.0;
   }
   return done ? QES_OK : QES_ERR_NOT_CONVERGED;
 }

@@ -690,6 +690,7 @@ int dense_solve_t(int ns, int nh, int64_t n, const uint32_t* bits, const typenam
     res->e_mean_re = em[0];
     res->e_mean_im = em[1];
     res->true_residual = sc[1] > 0.0 ? sqrt(sc[0] / sc[1]) : 0.0;
+    res->acond = -1.0;
   }
   if (info != 0) {
     qes_set_last_message("dense SR: S + shift is not positive definite in float64 (Cholesky pivot <= 0)");

@@ -297,6 +297,31 @@ def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8
     return x, info
 
 
+def sr_solve_minres(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
+                    check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True, x0=None,
+                    probs=None):
+    """The SR system solved by MINRES (``qes_sr_solve_minres_weighted``): arguments and stopping rule as
+    sr_solve_cg; info["acond"] is the recurrence's condition estimate of S + shift."""
+    dc = dtype_code(flat_params)
+    n = int(bits.shape[0])
+    ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
+    x = torch.empty((n_params(ns, nh),), dtype=vec_dtype(flat_params.dtype), device=bits.device)
+    if x0 is not None:
+        x0 = x0.to(device=bits.device, dtype=x.dtype).contiguous()
+        if x0.numel() != x.numel():
+            raise ValueError(f"x0 has {x0.numel()} entries, the parameter vector {x.numel()}")
+    opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor))
+    res = _lib.SRResult()
+    allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_converged else ()
+    w = sample_weights(probs, n, bits.device)
+    call("qes_sr_solve_minres_weighted", dc, ns, nh, n, ptr(bits), ptr(tanh_theta), ptr(eloc), ptr(w), C.byref(opt),
+         ptr(x0), ptr(x), C.byref(res), ptr(ws), int(ws.numel()), stream_ptr(), allow=allow)
+    info = {"iterations": res.iterations, "converged": bool(res.converged), "residual": res.residual,
+            "rhs_norm": res.rhs_norm, "e_mean": complex(res.e_mean_re, res.e_mean_im),
+            "true_residual": res.true_residual, "acond": res.acond}
+    return x, info
+
+
 def sr_solve_minsr(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
                    check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True):
     """MinSR: x = rhs_prefactor * O_c^H y with (O_c O_c^H / Ns + shift) y = E_c / Ns (sample-space CG)."""

@@ -402,7 +402,8 @@ class NQS:
         its results (the reference's chunking-invariance test); the kernels here need no chunking.
         Every option whose effect is not implemented raises (no silent drop): other ODE integrators or
         optimisers, phase and named schedulers, early stopping, excited states (``lower_states``),
-        regularisation, symmetrisation, preconditioners other than ``"jacobi"``, other linear solvers.
+        regularisation, symmetrisation, preconditioners other than ``"jacobi"``, linear solvers other than
+        CG, MINRES (``"minres"``, ``"minres_qlp"``) and the formed-matrix Cholesky.
         ``pre_solver="jacobi"`` preconditions the CG by 1 / diag(S + shift); ``lin_force_mat=True`` forms S
         on the tensor cores and solves it by a float64 Cholesky factorisation."""
         unsupported = {

@@ -38,6 +38,7 @@ class TDVPStepInfo:
 
 
 _SOLVERS_CG = ("scipy_cg", "cg")
+_SOLVERS_MINRES = ("minres", "scipy_minres", "minres_qlp")
 _SOLVERS_DIRECT = ("cholesky", "direct", "scipy_direct", "solve")
 
 
@@ -56,9 +57,9 @@ class TDVP:
                  backend="default", logger=None, use_timing=False, dtype=None, grad_clip=None, verbose=False,
                  sr_tol=1e-8, sr_atol=0.0, check_every=16, use_old_result=False):
         solver = "scipy_cg" if sr_lin_solver is None else str(getattr(sr_lin_solver, "name", sr_lin_solver)).lower()
-        if solver not in _SOLVERS_CG + _SOLVERS_DIRECT:
-            raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG (scipy_cg) "
-                                      f"and, on the formed matrix, a Cholesky solve")
+        if solver not in _SOLVERS_CG + _SOLVERS_MINRES + _SOLVERS_DIRECT:
+            raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG (scipy_cg), "
+                                      f"MINRES (minres, minres_qlp) and, on the formed matrix, a Cholesky solve")
         precond = None if sr_precond is None else str(getattr(sr_precond, "name", sr_precond)).lower()
         if precond in ("identity", "none"):
             precond = None
@@ -67,6 +68,10 @@ class TDVP:
                                       f"(1 / diag(S + shift)) and none")
         if precond is not None and use_minsr:
             raise NotImplementedError("a preconditioner on the MinSR (sample-space) system is not implemented")
+        if precond is not None and solver in _SOLVERS_MINRES:
+            raise NotImplementedError("a preconditioner on the MINRES path is not implemented (CG takes 'jacobi')")
+        if solver in _SOLVERS_MINRES and (use_minsr or sr_form_matrix):
+            raise NotImplementedError("MINRES runs on the matrix-free S v of the parameter-space SR system")
         if str(sr_lin_solver_t).lower() not in ("gram", "matvec", "matrix_free"):
             raise NotImplementedError(f"solver form {sr_lin_solver_t!r}: the GPU path applies S matrix-free")
         if solver in _SOLVERS_DIRECT and not sr_form_matrix:
@@ -154,10 +159,18 @@ class TDVP:
             self.last_info = info
         else:
             x0 = self._solve_handle_x0(dv.n_params(net.ns, net.nh), use_old)
-            x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
-                                     rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,
-                                     check_every=self.check_every, rhs_prefactor=self.rhs_prefactor, workspace=ws,
-                                     x0=x0, probs=probs, precond=self.sr_precond)
+            if self.sr_lin_solver in _SOLVERS_MINRES:
+                # minres_qlp: MINRES iterates until the condition estimate (info["acond"]) passes
+                # MINRES-QLP's switch threshold, which a positive shift keeps S + shift far from
+                x, info = dv.sr_solve_minres(net.flat, net.ns, net.nh, bits, tanh_theta, eloc,
+                                             shift=self.sr_diag_shift, rtol=self.sr_tol, atol=self.sr_atol,
+                                             maxiter=self.sr_maxiter, check_every=self.check_every,
+                                             rhs_prefactor=self.rhs_prefactor, workspace=ws, x0=x0, probs=probs)
+            else:
+                x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
+                                         rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,
+                                         check_every=self.check_every, rhs_prefactor=self.rhs_prefactor,
+                                         workspace=ws, x0=x0, probs=probs, precond=self.sr_precond)
             self.last_info = info
             self._solution = x.detach().clone()
         if self.grad_clip is not None and self.grad_clip > 0:

@@ -271,3 +271,64 @@ def test_tdvp_jacobi_option_reaches_the_solver():
     assert torch.allclose(x0, x1, rtol=1e-3, atol=1e-5 * float(x0.abs().max()))
     with pytest.raises(NotImplementedError):
         TDVP(sr_precond="ilu")
+
+
+# ------------------------------------------------------------------------- MINRES
+@pytest.mark.parametrize("cplx,impl", [(True, 0), (True, 1), (False, 0), (False, 1)])
+def test_minres_matches_oracle(cplx, impl):
+    """qes_sr_solve_minres_weighted (TDVP(sr_lin_solver="minres" / "minres_qlp")): solution against a dense
+    float64 solve, iteration count and condition estimate against the oracle's MINRES on the same float64
+    weighted system."""
+    ns, nh, n = 9, 18, 700
+    model = qb.XXZ(qb.SquareLattice(2, 3, 3), jxy=-1.0, jz=-1.0, hx=0.4)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=9, init_scale=0.3)
+    rng = np.random.default_rng(9)
+    st = np.where(rng.random((n, ns)) < 0.5, 0.5, -0.5)
+    bits = dv.pack_states(st)
+    _, tn, lp = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=True)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    lu = lp.real.double().cpu().numpy()
+    pr = np.exp(0.5 * (lu - lu.max()))
+    probs_t = torch.as_tensor((pr / pr.sum() * n).astype(np.float32)).cuda()
+    w = probs_t.double().cpu().numpy()
+    w = w / w.sum() * n
+    e = eloc.cpu().numpy().astype(np.complex128)
+    if not cplx:
+        e = e.real
+    O = osr.o_rows(None, orbm.to_sigma(st), tanh=tn.cpu().numpy())
+    ec, Oc, w_, _, _ = osr.prepare(e, O, w)
+    F = osr.force(Oc, ec, w_)
+    shift = 1e-2
+    A = osr.s_matrix(Oc, w_) + shift * np.eye(O.shape[1])
+    _, it_ref, _, conv_ref, acond_ref = osr.minres(lambda v: A @ v, F, rtol=1e-8, maxiter=3000)
+    assert conv_ref
+    _lib.set_sr_impl(impl)
+    try:
+        x, info = dv.sr_solve_minres(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=1e-8, maxiter=3000,
+                                     probs=probs_t, check_every=8)
+    finally:
+        _lib.set_sr_impl(0)
+    assert info["converged"]
+    xg = -x.cpu().numpy()
+    assert np.linalg.norm(A @ xg - F) / np.linalg.norm(F) < 1e-4
+    assert 0.0 <= info["true_residual"] < 1e-4
+    xr = np.linalg.solve(A, F)
+    err = xg - xr
+    assert np.sqrt(abs(np.vdot(err, A @ err)) / abs(np.vdot(xr, A @ xr))) < 1e-3
+    assert abs(info["iterations"] - it_ref) <= max(3, 0.05 * it_ref), (info["iterations"], it_ref)
+    assert info["acond"] == pytest.approx(acond_ref, rel=0.05)
+
+
+def test_tdvp_minres_qlp_option():
+    from pyqusolver_b200.tdvp import TDVP
+    net, bits, tn, eloc = _small_problem(cplx=True)
+    cg = TDVP(rhs_prefactor=-1.0, sr_diag_shift=1e-2, sr_maxiter=2000, sr_tol=1e-10)
+    mr = TDVP(rhs_prefactor=-1.0, sr_diag_shift=1e-2, sr_maxiter=2000, sr_tol=1e-10, sr_lin_solver="minres_qlp")
+    x0 = cg.solve(net, bits, tn, eloc)
+    x1 = mr.solve(net, bits, tn, eloc)
+    assert mr.last_info["converged"] and mr.last_info["acond"] > 1.0
+    assert torch.allclose(x0, x1, rtol=1e-4, atol=1e-6 * float(x0.abs().max()))
+    with pytest.raises(NotImplementedError):
+        TDVP(sr_lin_solver="minres", sr_precond="jacobi")

@@ -258,3 +258,24 @@ def test_oracle_pcg_matches_scipy_cg_with_jacobi_preconditioner():
     assert np.allclose(x, xs, rtol=1e-9, atol=1e-12 * np.abs(xs).max())
     _, it_plain, _, _ = osr.cg(lambda v: A @ v, F, rtol=1e-10, maxiter=500)
     assert it < it_plain
+
+
+def test_oracle_minres_matches_scipy_minres():
+    """The oracle's MINRES restatement follows SciPy's minres iterates on a Hermitian positive-definite
+    SR system (same solution; its residual recurrence equals the true residual norm)."""
+    import numpy as np
+    import scipy.sparse.linalg as sla
+    from oracle import sr as osr
+    rng = np.random.default_rng(4)
+    O = rng.normal(size=(200, 30)) + 1j * rng.normal(size=(200, 30))
+    e = rng.normal(size=200) + 1j * rng.normal(size=200)
+    ec, Oc, w_, _, _ = osr.prepare(e, O, None)
+    A = osr.s_matrix(Oc, w_) + 1e-2 * np.eye(30)
+    F = osr.force(Oc, ec, w_)
+    x, it, phibar, conv, acond = osr.minres(lambda v: A @ v, F, rtol=1e-10, maxiter=300)
+    assert conv
+    assert abs(phibar - np.linalg.norm(A @ x - F)) <= 1e-6 * np.linalg.norm(F)
+    xs, info = sla.minres(A, F, rtol=1e-12, maxiter=300)
+    assert np.allclose(x, xs, rtol=1e-7, atol=1e-9 * np.abs(xs).max())
+    ev = np.linalg.eigvalsh(A)
+    assert 0.1 * ev[-1] / ev[0] <= acond <= 10 * ev[-1] / ev[0]

@@ -577,6 +577,16 @@ def run_ours(args, cfg, rank, world, local_rank):
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
     if rank == 0 and args.matched_epochs > 0 and args.config == "heis10x10":
         line["accuracy_matched_fp64"] = matched_energy_check(args.matched_epochs, args.matched_every)
+    if rank == 0 and world == 1 and args.matched_other_epochs > 0:
+        # the same common-batch float64 comparison on the other single-problem workloads (C1, C3, C5)
+        mo = {}
+        for name in [n.strip() for n in args.matched_configs.split(",") if n.strip()]:
+            if name == args.config or name not in CONFIGS or CONFIGS[name].get("batch"):
+                continue
+            r = matched_energy_check(args.matched_other_epochs, max(1, args.matched_other_epochs // 5), name=name)
+            r.pop("per_epoch", None)
+            mo[name] = r
+        line["accuracy_matched_fp64_other"] = mo
     if rank == 0 and world == 1 and not args.no_other_configs:
         oc = {}
         for name in ("tfim16", "j1j2_6x6", "tfim20x20"):
@@ -928,8 +938,22 @@ def batch_problem_cfgs(cfg):
             for b, (L, h) in enumerate(zip(Ls, hx))]
 
 
+CPU_CHAINS = 64      # chains per timed CPU step (per-sample throughput is flat beyond a few dozen)
+
+
+def cpu_port_threads():
+    """Compile the oracle's multi-core log-cosh kernel (oracle/fast.py) before any timing; returns the
+    host threads the port runs on (Numba's pool and OpenBLAS's, both sized to the host) and a label."""
+    from oracle import fast
+    on = fast.enable()
+    if on:
+        return max(fast.threads(), 1), "float64 NumPy/OpenBLAS + Numba prange (log cosh of the local energy)"
+    return os.cpu_count() or 1, "float64 NumPy/OpenBLAS"
+
+
 def cpu_baseline(cfg, budget_s=20.0):
     """The oracle (float64 NumPy restatement of the reference's algorithm) on the host cores."""
+    threads, how = cpu_port_threads()
     if cfg.get("batch"):
         # bounded sample: one VMC step of 16 chains on successive problems until the budget is used
         t0 = time.perf_counter()
@@ -942,24 +966,24 @@ def cpu_baseline(cfg, budget_s=20.0):
             if time.perf_counter() - t0 > budget_s:
                 break
         dt = time.perf_counter() - t0
-        return {"value": samples / dt, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
+        return {"value": samples / dt, "unit": "samples/s", "cores": threads, "kind": "port",
                 "sample": f"one VMC step of 16 chains x {cfg['samples']} samples on each of the first {done} "
-                          f"problems (float64 NumPy oracle, problems one after another)"}
-    n_chains = 16
+                          f"problems ({how}, problems one after another)"}
+    n_chains = CPU_CHAINS
     p, terms, smp = oracle_setup(cfg, n_chains)
     t0 = time.perf_counter()
     steps = 0
     while True:
         p, _ = cpu_step(cfg, p, terms, smp)
         steps += 1
-        if time.perf_counter() - t0 > budget_s or steps >= 3:
+        if time.perf_counter() - t0 > budget_s or steps >= 8:
             break
     dt = time.perf_counter() - t0
     samples = steps * n_chains * cfg["samples"]
-    return {"value": samples / dt, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{steps} VMC step(s) of {n_chains} chains x {cfg['samples']} samples (same per-sample "
-                      f"algorithm as the reference: full RBM re-evaluation per connected state and per exchange "
-                      f"proposal, float64 NumPy/OpenBLAS)"}
+    return {"value": samples / dt, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} steady-state VMC step(s) of {n_chains} chains x {cfg['samples']} samples (same "
+                      f"per-sample algorithm as the reference: full RBM re-evaluation per connected state and per "
+                      f"exchange proposal; {how}; thermalisation not timed)"}
 
 
 def run_reference(args, cfg, rank, world):
@@ -980,7 +1004,8 @@ def run_reference(args, cfg, rank, world):
                 "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
-    n_chains = 16
+    threads, how = cpu_port_threads()
+    n_chains = CPU_CHAINS
     p, terms, smp = oracle_setup(cfg, n_chains)
     for _ in range(args.warmup):
         p, _ = cpu_step(cfg, p, terms, smp)
@@ -991,13 +1016,13 @@ def run_reference(args, cfg, rank, world):
     samples = args.steps * n_chains * cfg["samples"]
     v = samples / dt
     sample_desc = (f"each step {n_chains} chains x {cfg['samples']} samples of the {args.config} workload "
-                   f"(bounded sample), oracle port of the reference algorithm on {os.cpu_count()} host threads")
+                   f"(bounded sample), oracle port of the reference algorithm ({how}) on {threads} host threads")
     line = {"metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": args.config, "samples_per_step": n_chains * cfg["samples"]},
             "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": os.cpu_count(), "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port",
                              "sample": sample_desc},
             "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -1017,6 +1042,10 @@ def main():
                     help="epochs of the ED-checked mixed vs plain comparison on tfim16 (0 = skip)")
     ap.add_argument("--matched-epochs", type=int, default=300,
                     help="epochs of the float64 / mixed / plain comparison on heis10x10 (0 = skip)")
+    ap.add_argument("--matched-configs", default="tfim16,j1j2_6x6,tfim20x20",
+                    help="other workloads given the common-batch float64 comparison (summary only)")
+    ap.add_argument("--matched-other-epochs", type=int, default=60,
+                    help="training epochs of each of those comparisons (5 checked batches; 0 = skip)")
     ap.add_argument("--matched-every", type=int, default=15,
                     help="solve the batch of every n-th epoch in all three forms")
     ap.add_argument("--no-other-configs", action="store_true",

@@ -85,9 +85,16 @@ def theta(p: RBMParams, sigma):
     return np.asarray(sigma, dtype=np.float64) @ p.W + p.b
 
 
+# set by oracle.fast.enable() (the timed CPU baseline): a multi-core row sum of log cosh, same formula,
+# for the large row blocks of the local energy (thread start-up outweighs it on a few chains' rows)
+_ROWSUM_LOGCOSH = None
+
+
 def log_psi(p: RBMParams, sigma):
     sigma = np.asarray(sigma, dtype=np.float64)
     th = theta(p, sigma)
+    if _ROWSUM_LOGCOSH is not None and th.ndim == 2 and th.shape[0] >= 4096:
+        return sigma @ p.a + _ROWSUM_LOGCOSH(th)
     return sigma @ p.a + np.sum(log_cosh(th), axis=-1)
 
 

@@ -236,14 +236,18 @@ def test_jacobi_pcg_matches_oracle(cplx, impl, fused):
     A = osr.s_matrix(Oc, w_) + shift * np.eye(O.shape[1])
     minv = osr.jacobi_minv(Oc, w_, shift)
     assert np.allclose(1.0 / minv, np.real(np.diag(A)), rtol=1e-12)
-    _, it_ref, _, conv_ref = osr.cg(lambda v: A @ v, F, rtol=1e-8, maxiter=3000, minv=minv)
-    _, it_plain, _, _ = osr.cg(lambda v: A @ v, F, rtol=1e-8, maxiter=3000)
+    # iteration counts are compared at rtol 1e-5, above the float32 operator's rounding (~1e-6): closer to
+    # it, lost orthogonality adds iterations in any float32-operator Krylov solve
+    _, it_ref, _, conv_ref = osr.cg(lambda v: A @ v, F, rtol=1e-5, maxiter=3000, minv=minv)
+    _, it_plain, _, _ = osr.cg(lambda v: A @ v, F, rtol=1e-5, maxiter=3000)
     assert conv_ref
     _lib.set_sr_impl(impl)
     _lib.call("qes_set_cg_fused", fused)
     try:
         x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=1e-8, maxiter=3000,
                                  probs=probs_t, precond="jacobi", check_every=4)
+        _, info5 = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=1e-5, maxiter=3000,
+                                  probs=probs_t, precond="jacobi", check_every=1)
     finally:
         _lib.call("qes_set_cg_fused", 1)
         _lib.set_sr_impl(0)
@@ -253,8 +257,7 @@ def test_jacobi_pcg_matches_oracle(cplx, impl, fused):
     xr = np.linalg.solve(A, F)
     err = xg - xr
     assert np.sqrt(abs(np.vdot(err, A @ err)) / abs(np.vdot(xr, A @ xr))) < 1e-3
-    # float32 operator vs float64: the iteration counts agree to a few percent
-    assert abs(info["iterations"] - it_ref) <= max(3, 0.05 * it_ref), (info["iterations"], it_ref, it_plain)
+    assert abs(info5["iterations"] - it_ref) <= max(3, 0.05 * it_ref), (info5["iterations"], it_ref, it_plain)
 
 
 def test_tdvp_jacobi_option_reaches_the_solver():
@@ -302,12 +305,14 @@ def test_minres_matches_oracle(cplx, impl):
     F = osr.force(Oc, ec, w_)
     shift = 1e-2
     A = osr.s_matrix(Oc, w_) + shift * np.eye(O.shape[1])
-    _, it_ref, _, conv_ref, acond_ref = osr.minres(lambda v: A @ v, F, rtol=1e-8, maxiter=3000)
+    _, it_ref, _, conv_ref, acond_ref = osr.minres(lambda v: A @ v, F, rtol=1e-5, maxiter=3000)
     assert conv_ref
     _lib.set_sr_impl(impl)
     try:
         x, info = dv.sr_solve_minres(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=1e-8, maxiter=3000,
                                      probs=probs_t, check_every=8)
+        _, info5 = dv.sr_solve_minres(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=1e-5, maxiter=3000,
+                                      probs=probs_t, check_every=1)
     finally:
         _lib.set_sr_impl(0)
     assert info["converged"]
@@ -317,8 +322,9 @@ def test_minres_matches_oracle(cplx, impl):
     xr = np.linalg.solve(A, F)
     err = xg - xr
     assert np.sqrt(abs(np.vdot(err, A @ err)) / abs(np.vdot(xr, A @ xr))) < 1e-3
-    assert abs(info["iterations"] - it_ref) <= max(3, 0.05 * it_ref), (info["iterations"], it_ref)
-    assert info["acond"] == pytest.approx(acond_ref, rel=0.05)
+    # counts at rtol 1e-5 (above the float32 operator's rounding), as in the PCG test
+    assert abs(info5["iterations"] - it_ref) <= max(3, 0.05 * it_ref), (info5["iterations"], it_ref)
+    assert info5["acond"] == pytest.approx(acond_ref, rel=0.05)
 
 
 def test_tdvp_minres_qlp_option():

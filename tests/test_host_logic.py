@@ -279,3 +279,21 @@ def test_oracle_minres_matches_scipy_minres():
     assert np.allclose(x, xs, rtol=1e-7, atol=1e-9 * np.abs(xs).max())
     ev = np.linalg.eigvalsh(A)
     assert 0.1 * ev[-1] / ev[0] <= acond <= 10 * ev[-1] / ev[0]
+
+
+def test_oracle_fast_log_psi_matches_numpy_path():
+    """oracle.fast (the CPU baseline's multi-core log cosh sum) gives the NumPy oracle's log psi."""
+    import numpy as np
+    import pytest
+    from oracle import fast, rbm
+    for cplx in (True, False):
+        p = rbm.random_params(30, 60, complex_=cplx, scale=0.8, seed=2)
+        sig = np.where(np.random.default_rng(1).random((5000, 30)) < 0.5, 1.0, -1.0)
+        ref = rbm.log_psi(p, sig)
+        if not fast.enable():
+            pytest.skip("numba not available")
+        try:
+            got = rbm.log_psi(p, sig)
+        finally:
+            fast.disable()
+        assert np.allclose(got, ref, rtol=0, atol=1e-11)

@@ -566,13 +566,13 @@ def run_ours(args, cfg, rank, world, local_rank):
         "e2e": e2e,
         "roofline": roof,
         "issue_rooflines": issue_rooflines(cfg, nqs, mixed, mixed["clocks"]),
-        "sr_tiling": ({"choice (mode, nc, ctas, pairs, fused_sv)": tuned["choice"], "matvec_ms": tuned["ms"],
+        "sr_tiling": ({"choice (mode, nc, ctas, pairs, fused_sv)": tuned["choice"], "cg_iteration_ms": tuned["ms"],
                        "candidates_ms": tuned["timings"], "cached": tuned["cached"]} if tuned else "automatic"),
     }
     if tuned:
         # the tuned tiling is process-wide: the other workloads below run the automatic one
         from pyqusolver_b200.autotune import apply_tiling
-        apply_tiling(0, 0, 0, 0, 1)
+        apply_tiling(0, 0, 0, 0, 0)
     if rank == 0 and args.accuracy_epochs > 0:
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
     if rank == 0 and args.matched_epochs > 0 and args.config == "heis10x10":
@@ -1056,10 +1056,16 @@ def main():
     ap.add_argument("--no-dense", action="store_true", help="skip the formed-S (Gram + Cholesky) summary")
     ap.add_argument("--dense-configs", default="tfim16,j1j2_6x6,heis10x10",
                     help="workloads of the formed-S summary")
+    ap.add_argument("--chains", type=int, default=0,
+                    help="override the workload's chain count (smaller cases for profiler captures; the "
+                         "bench line of a workload uses its own count)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local_rank = env_rank()
     cfg = CONFIGS[args.config]
+    if args.chains > 0:
+        cfg = dict(cfg, chains=int(args.chains))
+        CONFIGS[args.config] = cfg
     if args.impl == "reference":
         run_reference(args, cfg, rank, world)
     elif cfg.get("batch"):

@@ -340,12 +340,13 @@ int qes_sr_set_tiling(int mode, int nc, int ctas);
  * per CTA (0, the default: the pairs measured slower on B200).  Same sums in a
  * fixed order either way.                                                  */
 int qes_sr_set_ohu_pairs(int on);
-/* The tensor-core S v of single-M-tile problems as one cooperative launch (1,
- * the default): each CTA computes O v for its 128-sample tiles, a grid
- * barrier gives every CTA the weighted mean of O v, and the same CTA then
- * accumulates O^H u of its tiles in TMEM (Q = conj(t) u built from the
- * float32 T) and writes one partial P-vector; or as the two kernels O v and
- * O^H u (0).  Same operator, different float32 summation order.           */
+/* The tensor-core S v of single-M-tile problems as one cooperative launch
+ * (1): each CTA computes O v for its 128-sample tiles, a grid barrier gives
+ * every CTA the weighted mean of O v, and the same CTA then accumulates
+ * O^H u of its tiles in TMEM (Q = conj(t) u built from the float32 T) and
+ * writes one partial P-vector; or as the two kernels O v and O^H u (0, the
+ * default: measured faster on B200).  Same operator, different float32
+ * summation order.                                                        */
 int qes_sr_set_fused_sv(int on);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */

@@ -6,12 +6,13 @@ hidden units, a target CTA count); ``qes_sr_set_ohu_pairs`` runs the single-tile
 of CTAs that add their split-K partials through distributed shared memory, and
 ``qes_sr_set_fused_sv`` runs the single-tile matvec as one cooperative S v kernel (O v, the mean of
 O v over a grid barrier and O^H u in the same CTAs).  ``tune_sr_tiling`` times
-the SR matvec (``qes_sr_matvec``: O v, O^H u and the split reduction, the body of one CG iteration)
-of a given batch for every candidate with CUDA events on the current stream, keeps the fastest,
-applies it process-wide and persists it in a JSON cache keyed by device, dtype and shape
-(``$QES_B200_AUTOTUNE`` or ``~/.cache/pyqusolver_b200/autotune.json``).  Candidates that the shapes
-do not admit (QES_ERR_SIZE / QES_ERR_ARG) are skipped.  Every candidate computes the same matvec; the
-choice changes only the order of the float32 partial sums.
+CG iterations on a given batch for every candidate (``qes_sr_solve_cg`` with the tolerance at zero, so
+that it runs exactly the iterations asked for; the time of K iterations subtracted from that of 2K
+removes the once-per-solve work: operand preparation, force, set-up), keeps the fastest, applies it
+process-wide and persists it in a JSON cache keyed by device, dtype and shape (``$QES_B200_AUTOTUNE``
+or ``~/.cache/pyqusolver_b200/autotune.json``).  Candidates that the shapes do not admit
+(QES_ERR_SIZE / QES_ERR_ARG) are skipped.  Every candidate computes the same operator; the choice
+changes only the order of the float32 partial sums.
 """
 
 from __future__ import annotations
@@ -31,9 +32,9 @@ def _cache_path(cache=None):
 
 
 def _candidates(ns, nh, cplx):
-    # (mode, nc, ctas, pairs, fused S v): automatic with the fused kernel, the kernel pair, the pair
-    # with O^H u in CTA pairs, then the M/N-tiled O^H u
-    out = [(0, 0, 0, 0, 1), (0, 0, 0, 0, 0), (0, 0, 0, 1, 0)]
+    # (mode, nc, ctas, pairs, fused S v): automatic (the kernel pair), the fused kernel, the pair with
+    # O^H u in CTA pairs, then the M/N-tiled O^H u
+    out = [(0, 0, 0, 0, 0), (0, 0, 0, 0, 1), (0, 0, 0, 1, 0)]
     for nc in (256, 208, 128, 96, 64, 32):
         if nc > ((nh + 15) // 16) * 16:
             continue
@@ -42,14 +43,14 @@ def _candidates(ns, nh, cplx):
     return out
 
 
-def tune_sr_tiling(net, bits, tanh_theta, *, repeats=5, cache=None, candidates=None):
-    """Time the SR matvec of (net, bits, tanh_theta) under each tiling candidate (mode, nc, ctas, pairs, sv);
-    apply and return the fastest as a dict with the timings.  A cached choice for the same device and
-    shapes is applied without timing."""
+def tune_sr_tiling(net, bits, tanh_theta, *, repeats=3, iters=24, cache=None, candidates=None):
+    """Time a CG iteration on (net, bits, tanh_theta) under each tiling candidate (mode, nc, ctas, pairs,
+    sv); apply and return the fastest as a dict with the per-iteration times in ms.  A cached choice for
+    the same device and shapes is applied without timing."""
     dc = dv.dtype_code(net.flat)
     n = int(bits.shape[0])
     dev = torch.cuda.get_device_name(bits.device)
-    key = f"sr_tiling5|{dev}|{dc}|{net.ns}|{net.nh}|{n}"
+    key = f"sr_cg_iter|{dev}|{dc}|{net.ns}|{net.nh}|{n}"
     path = _cache_path(cache)
     table = {}
     try:
@@ -61,11 +62,25 @@ def tune_sr_tiling(net, bits, tanh_theta, *, repeats=5, cache=None, candidates=N
         apply_tiling(*table[key]["choice"])
         return dict(table[key], cached=True)
     cands = candidates or _candidates(net.ns, net.nh, net.is_complex)
-    P = dv.n_params(net.ns, net.nh)
-    v = torch.randn(P, dtype=dv.vec_dtype(net.flat.dtype), device=bits.device)
+    eloc = torch.randn(n, dtype=torch.complex64, device=bits.device)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     timings = {}
     best, best_t = None, float("inf")
+
+    def solve(ws, k):
+        dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=1e-3, rtol=0.0, atol=0.0,
+                       maxiter=k, check_every=k, workspace=ws, allow_not_converged=True)
+
+    def timed(ws, k):
+        ts = []
+        for _ in range(repeats):
+            ev0.record()
+            solve(ws, k)
+            ev1.record()
+            torch.cuda.synchronize()
+            ts.append(ev0.elapsed_time(ev1))
+        return sorted(ts)[len(ts) // 2]
+
     try:
         for cand in cands:
             apply_tiling(*cand)
@@ -73,27 +88,21 @@ def tune_sr_tiling(net, bits, tanh_theta, *, repeats=5, cache=None, candidates=N
                 continue
             try:
                 ws = dv.sr_workspace(dc, net.ns, net.nh, n, bits.device)
-                dv.sr_matvec(net.flat, net.ns, net.nh, bits, tanh_theta, v, workspace=ws)   # warm-up
+                solve(ws, iters)                                        # warm-up, graph capture
+                solve(ws, 2 * iters)
                 torch.cuda.synchronize()
-                ts = []
-                for _ in range(repeats):
-                    ev0.record()
-                    dv.sr_matvec(net.flat, net.ns, net.nh, bits, tanh_theta, v, workspace=ws)
-                    ev1.record()
-                    torch.cuda.synchronize()
-                    ts.append(ev0.elapsed_time(ev1))
+                t = (timed(ws, 2 * iters) - timed(ws, iters)) / iters
             except _lib.QESError as e:
                 if e.code not in (_lib.QES_ERR_SIZE, _lib.QES_ERR_ARG):
                     raise
                 continue
-            t = sorted(ts)[len(ts) // 2]
             timings[str(cand)] = t
             if t < best_t:
                 best, best_t = cand, t
     finally:
-        apply_tiling(*(best or (0, 0, 0, 0, 1)))
+        apply_tiling(*(best or (0, 0, 0, 0, 0)))
     if best is None:
-        return {"choice": (0, 0, 0, 0, 1), "ms": None, "timings": timings, "cached": False}
+        return {"choice": (0, 0, 0, 0, 0), "ms": None, "timings": timings, "cached": False}
     entry = {"choice": list(best), "ms": best_t, "timings": timings}
     table[key] = entry
     try:
@@ -107,7 +116,7 @@ def tune_sr_tiling(net, bits, tanh_theta, *, repeats=5, cache=None, candidates=N
     return dict(entry, cached=False)
 
 
-def apply_tiling(mode, nc, ctas, pairs, sv=1):
+def apply_tiling(mode, nc, ctas, pairs, sv=0):
     _lib.call("qes_sr_set_tiling", int(mode), int(nc), int(ctas))
     _lib.call("qes_sr_set_ohu_pairs", int(pairs))
     _lib.call("qes_sr_set_fused_sv", int(sv))

@@ -1572,7 +1572,9 @@ static int pow2_at_least(int x) {
 // hidden units per N chunk and target CTA count of the M/N-tiled O^H u (0 = automatic)
 static std::atomic<int> g_tile_mode{0}, g_tile_nc{0}, g_tile_ctas{0};
 static std::atomic<int> g_ohu_pairs{0};      // measured slower on B200 (heis 10x10: 49.5 vs 46.2 us per CG iteration)
-static std::atomic<int> g_sv{1};             // fused S v kernel where the tiling admits it
+// fused S v kernel where the tiling admits it: off by default (heis10x10 CG iteration 54.6 us with it,
+// 44.2 us with the O v / O^H u pair: its per-tile phases run one after another behind block barriers)
+static std::atomic<int> g_sv{0};
 extern "C" int qes_sr_set_ohu_pairs(int on) {
   g_ohu_pairs.store(on ? 1 : 0);
   return QES_OK;

@@ -839,10 +839,16 @@ def test_tilings_agree_and_graphs_follow_tiling_changes(sr_impl):
             xs.append(x.cpu().numpy())
     finally:
         _lib.call("qes_sr_set_tiling", 0, 0, 0)
-    # float32 products summed in a different order; CG carries that through the conditioning of S
+    # float32 products summed in a different order; CG carries that through the conditioning of S: with
+    # P > Ns, S + shift has many eigenvalues equal to the shift, so the solutions are compared in the
+    # (S + shift)-norm, the error norm CG minimises, not entry by entry
     assert rel_err(xs[-1], xs[0]) < 1e-12          # same tiling again (graph replay): identical
+    x0 = torch.as_tensor(xs[0]).cuda()
+    a0 = torch.vdot(x0, dv.sr_matvec(net.flat, ns, nh, bits, tn, x0, shift=1e-2)).real.item()
     for x in xs[1:-1]:
-        assert rel_err(x, xs[0]) < 1e-3
+        e = torch.as_tensor(x).cuda() - x0
+        ae = torch.vdot(e, dv.sr_matvec(net.flat, ns, nh, bits, tn, e, shift=1e-2)).real.item()
+        assert np.sqrt(max(ae, 0.0) / a0) < 1e-3
 
 
 @pytest.mark.parametrize("cplx,ns,nh,n", [(False, 16, 16, 300), (True, 100, 200, 1000), (True, 36, 144, 700),

@@ -161,6 +161,16 @@ int qes_set_cg_device_loop(int enable);
  * needs fewer waves of resident chains and spills no more (default);
  * 2 = the capped kernel always.  Samples are the same in every mode.        */
 int qes_sampler_set_capped(int mode);
+/* Hidden layers wider than one warp's register cache (nh > 512 real, > 256
+ * complex), process-wide: 1 (default) runs each chain on a block of 2, 4 or
+ * 8 warps, every thread holding 16 (real) / 8 (complex) units of the chain's
+ * theta cache in registers, so a proposal's whole table row is fetched in
+ * one round trip and the log-ratio is summed over the warps in order
+ * (nh up to 4096 real / 2048 complex); 0 runs one warp per chain with the
+ * cache in shared memory (nh up to 2048 real / 512 complex).  The two modes
+ * draw the same random numbers and differ only in float32 summation order.
+ * No counterpart in the reference (its sampler re-evaluates the network).  */
+int qes_sampler_set_wide(int on);
 
 /* The sampler's tanh of its acceptance cache applied elementwise (y = tanh x,
  * n elements of dtype): hardware exponential / sine / cosine / reciprocal

@@ -108,6 +108,7 @@ SIGNATURES = {
     "qes_set_pdl": [C.c_int],
     "qes_set_cg_device_loop": [C.c_int],
     "qes_sampler_set_capped": [C.c_int],
+    "qes_sampler_set_wide": [C.c_int],
     "qes_sampler_tanh_cache": [C.c_int, _i64, _vp, _vp, _vp],
     "qes_pt_swap": [C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_float, _u64, _i64, _vp, _vp],
     "qes_pt_collect": [C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_float, _vp, _vp, _vp, _vp, _vp],

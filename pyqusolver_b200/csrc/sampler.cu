@@ -88,10 +88,13 @@ struct ThetaCache<T, MPL, true> {
   QES_D T& tn(int r) { return tn_[32 * r]; }
 };
 
-template <class T, class Cache>
+// lane: the thread's index within its chain (warp lane, or warp-in-chain * 32 + lane when KW warps
+// share a chain); unit m = lane + 32 KW r
+template <class T, class Cache, int KW = 1>
 QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ b,
                       const T* __restrict__ W, Cache& c) {
   constexpr int MPL = Cache::kMPL;
+  constexpr int STRIDE = 32 * KW;
   // accumulate CH units per lane in registers, then store (CH = MPL for register caches)
   constexpr int CH = Cache::kSmem ? 16 : MPL;
 #pragma unroll
@@ -99,7 +102,7 @@ QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __
     T acc[CH];
 #pragma unroll
     for (int r = 0; r < CH; ++r) {
-      const int m = lane + 32 * (c0 + r);
+      const int m = lane + STRIDE * (c0 + r);
       acc[r] = (m < nh) ? b[m] : ScalarTraits<T>::zero();
     }
     auto site = [&](int i) {
@@ -107,7 +110,7 @@ QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __
       const T* wr = W + (int64_t)i * nh;
 #pragma unroll
       for (int r = 0; r < CH; ++r) {
-        const int m = lane + 32 * (c0 + r);
+        const int m = lane + STRIDE * (c0 + r);
         if (m < nh) acc[r] = addx(acc[r], scal(sg, wr[m]));
       }
     };
@@ -127,20 +130,38 @@ QES_D void full_theta(int ns, int nh, int lane, const uint32_t* cfg, const T* __
   }
 }
 
-template <class T, class Cache>
-QES_D T chain_logpsi(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ a, Cache& c) {
+// red (KW > 1): KW shared slots for the sum over the chain's warps (block-wide barriers)
+template <class T, class Cache, int KW = 1>
+QES_D T chain_logpsi(int ns, int nh, int lane, const uint32_t* cfg, const T* __restrict__ a, Cache& c,
+                     T* red = nullptr) {
   constexpr int MPL = Cache::kMPL;
+  constexpr int STRIDE = 32 * KW;
   T s = ScalarTraits<T>::zero();
 #pragma unroll
   for (int r = 0; r < MPL; ++r) {
-    const int m = lane + 32 * r;
+    const int m = lane + STRIDE * r;
     if (m < nh) s = addx(s, log_cosh(c.th(r)));
   }
-  for (int i = lane; i < ns; i += 32) {
+  for (int i = lane; i < ns; i += STRIDE) {
     const float sg = ((cfg[i >> 5] >> (i & 31)) & 1u) ? 1.f : -1.f;
     s = addx(s, scal(sg, a[i]));
   }
-  return warp_sum(s);
+  s = warp_sum(s);
+  if constexpr (KW > 1) {
+    if ((lane & 31) == 0) red[lane >> 5] = s;
+    __syncthreads();
+    s = red[0];
+    for (int w = 1; w < KW; ++w) s = addx(s, red[w]);
+    __syncthreads();                                  // the slots are reused by the next call
+  }
+  return s;
+}
+
+// barrier over the threads of one chain: its warp, or its block when KW warps share the chain
+template <int KW>
+QES_D void chain_sync() {
+  if constexpr (KW == 1) __syncwarp();
+  else __syncthreads();
 }
 
 // Everything one chain needs; pointers are already offset to the chain's problem.
@@ -157,18 +178,26 @@ struct ChainCtx {
 
 // Runs proposals for chain `chain` (index within its problem) with the
 // problem's packed spins staged in `cw` (shared memory, one warp).
-template <class T, int MPL, int RULE, bool SMEM = false>
+// KW > 1: the chain runs on a whole block of KW warps (register caches only); thread gl = threadIdx.x
+// owns units gl + 32 KW r, every thread draws the same Philox numbers and takes the same decision,
+// and the log-ratio is summed over the warps through `red_la` (two sets of KW slots, used
+// alternately) and `red_lp` (KW slots) in shared memory, in warp order.
+template <class T, int MPL, int RULE, bool SMEM = false, int KW = 1>
 QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_slice, uint32_t* __restrict__ chain_bits,
                      uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed,
                      int32_t* __restrict__ accepted, uint32_t* __restrict__ sample_bits,
-                     T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi) {
-  const int lane = threadIdx.x & 31;
+                     T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi, float* red_la = nullptr,
+                     T* red_lp = nullptr) {
+  static_assert(KW == 1 || !SMEM, "chains shared by several warps keep their caches in registers");
+  constexpr int STRIDE = 32 * KW;
+  const int lane = KW == 1 ? (int)(threadIdx.x & 31) : (int)threadIdx.x;   // index within the chain
   const int ns = P.ns, nh = P.nh, nw = n_words(ns);
   const T* __restrict__ a = P.a;
   const T* __restrict__ b = P.b;
   const T* __restrict__ W = P.W;
-  for (int q = lane; q < nw; q += 32) cw[q] = chain_bits[(int64_t)chain * nw + q];
-  __syncwarp();
+  for (int q = lane; q < nw; q += STRIDE) cw[q] = chain_bits[(int64_t)chain * nw + q];
+  chain_sync<KW>();
+  int red_par = 0;
 
   const uint32_t cid = (uint32_t)P.chain_id;
   uint64_t step = chain_step[chain];
@@ -178,7 +207,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
 
   ThetaCache<T, MPL, SMEM> cache;
   cache.bind(theta_slice, lane, (nh + 31) >> 5);
-  full_theta<T>(ns, nh, lane, cw, b, W, cache);
+  full_theta<T, ThetaCache<T, MPL, SMEM>, KW>(ns, nh, lane, cw, b, W, cache);
   int since = 0;
 
   const int64_t total = P.therm_steps_total + (int64_t)P.num_samples * P.sweep_steps;
@@ -228,7 +257,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
         T cb[2][PF], sb[2][PF];
 #pragma unroll
         for (int q = 0; q < PF; ++q) {
-          const int m = lane + 32 * q;
+          const int m = lane + STRIDE * q;
           cb[0][q] = (m < nh) ? Crow[m] : ScalarTraits<T>::one();
           sb[0][q] = (m < nh) ? Srow[m] : ScalarTraits<T>::zero();
         }
@@ -238,7 +267,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
           if (c0 + PF < MPL) {
 #pragma unroll
             for (int q = 0; q < PF; ++q) {
-              const int m = lane + 32 * (c0 + PF + q);
+              const int m = lane + STRIDE * (c0 + PF + q);
               cb[cur ^ 1][q] = (m < nh) ? Crow[m] : ScalarTraits<T>::one();
               sb[cur ^ 1][q] = (m < nh) ? Srow[m] : ScalarTraits<T>::zero();
             }
@@ -246,7 +275,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
 #pragma unroll
           for (int q = 0; q < PF; ++q) {
             const int rr = c0 + q;
-            const T t = (!SMEM || 32 * rr < nh) ? cache.tn(rr) : ScalarTraits<T>::zero();
+            const T t = (!SMEM || STRIDE * rr < nh) ? cache.tn(rr) : ScalarTraits<T>::zero();
             prod = mulx(prod, ratio_factor(cb[cur][q], g, t, sb[cur][q]));
             if ((rr & 7) == 7) renorm(prod, ex);
           }
@@ -254,13 +283,23 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
       } else {
 #pragma unroll
         for (int rr = 0; rr < MPL; ++rr) {
-          const int m = lane + 32 * rr;
+          const int m = lane + STRIDE * rr;
           if (m < nh) prod = mulx(prod, ratio_factor(Crow[m], g, cache.tn(rr), Srow[m]));
           if ((rr & 7) == 7) renorm(prod, ex);
         }
       }
       float la = log_abs<T>(prod) + 0.69314718055994531f * (float)ex;
       la = warp_sum(la);
+      if constexpr (KW > 1) {
+        // every reduction is separated from the one two before it by the barrier of the one between,
+        // so alternating slot sets cannot be overwritten while a warp still reads them
+        float* slots = red_la + red_par * KW;
+        if ((lane & 31) == 0) slots[lane >> 5] = la;
+        __syncthreads();
+        la = slots[0];
+        for (int w = 1; w < KW; ++w) la += slots[w];
+        red_par ^= 1;
+      }
       T av = a[i0];
       if (j0 >= 0) av = addx(av, scal(-1.f, a[j0]));
       re_delta = la + 2.f * g * to_re(av);
@@ -277,14 +316,14 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
           T d[PU];
 #pragma unroll
           for (int q = 0; q < PU; ++q) {          // all loads of the chunk first
-            const int m = lane + 32 * (c0 + q);
+            const int m = lane + STRIDE * (c0 + q);
             d[q] = (m < nh) ? wi[m] : ScalarTraits<T>::zero();
             if (j0 >= 0) d[q] = addx(d[q], scal(-1.f, (m < nh) ? wj[m] : ScalarTraits<T>::zero()));
           }
 #pragma unroll
           for (int q = 0; q < PU; ++q) {
             const int rr = c0 + q;
-            if (lane + 32 * rr < nh) {
+            if (lane + STRIDE * rr < nh) {
               const T t2 = addx(cache.th(rr), scal(2.f * g, d[q]));
               cache.th(rr) = t2;
               cache.tn(rr) = tanh_cache(t2);
@@ -294,7 +333,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
       } else {
 #pragma unroll
         for (int rr = 0; rr < MPL; ++rr) {
-          const int m = lane + 32 * rr;
+          const int m = lane + STRIDE * rr;
           if (m < nh) {
             T d = wi[m];
             if (j0 >= 0) d = addx(d, scal(-1.f, wj[m]));
@@ -304,38 +343,38 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
           }
         }
       }
-      __syncwarp();
+      chain_sync<KW>();
       if (lane == 0) {
         cw[i0 >> 5] ^= 1u << (i0 & 31);
         if (j0 >= 0) cw[j0 >> 5] ^= 1u << (j0 & 31);
       }
-      __syncwarp();
+      chain_sync<KW>();
     }
     n_prop += 1;
     n_acc += keep ? 1 : 0;
     ++step;
     if (++since >= recompute) {
-      full_theta<T>(ns, nh, lane, cw, b, W, cache);
+      full_theta<T, ThetaCache<T, MPL, SMEM>, KW>(ns, nh, lane, cw, b, W, cache);
       since = 0;
     }
     if (it + 1 == next_record) {
       const int64_t row = rec * P.n_chains + chain;
-      for (int q = lane; q < nw; q += 32) sample_bits[row * nw + q] = cw[q];
-      const T lp = chain_logpsi<T>(ns, nh, lane, cw, a, cache);
+      for (int q = lane; q < nw; q += STRIDE) sample_bits[row * nw + q] = cw[q];
+      const T lp = chain_logpsi<T, ThetaCache<T, MPL, SMEM>, KW>(ns, nh, lane, cw, a, cache, red_lp);
       if (lane == 0 && sample_logpsi) sample_logpsi[row] = lp;
       ++rec;
       next_record += P.sweep_steps;
     }
   }
-  for (int q = lane; q < nw; q += 32) chain_bits[(int64_t)chain * nw + q] = cw[q];
-  const T lp = chain_logpsi<T>(ns, nh, lane, cw, a, cache);
+  for (int q = lane; q < nw; q += STRIDE) chain_bits[(int64_t)chain * nw + q] = cw[q];
+  const T lp = chain_logpsi<T, ThetaCache<T, MPL, SMEM>, KW>(ns, nh, lane, cw, a, cache, red_lp);
   if (lane == 0) {
     chain_step[chain] = step;
     proposed[chain] = n_prop;
     accepted[chain] = n_acc;
     if (last_logpsi) last_logpsi[chain] = lp;
   }
-  __syncwarp();
+  chain_sync<KW>();
 }
 
 // Wide theta caches (SMEM = true) live in dynamic shared memory, 2 * 32 * MPL elements per warp.
@@ -368,9 +407,67 @@ __global__ void __launch_bounds__(32 * SMP_WARPS, MINB) sampler_kernel(
                                 sample_bits, sample_logpsi, last_logpsi);
 }
 
+// Wide hidden layers, one chain per block of KW warps: every thread holds MPL units of the chain's
+// theta / tanh cache in registers, so one proposal's table row is in flight at once (one L2 round
+// trip) instead of being walked one chunk per round trip by a single warp, and no shared-memory cache
+// caps the resident chains.  Same arithmetic per unit as the one-warp kernels; the log-ratio is summed
+// per warp and then over the warps in order.
+template <class T, int MPL, int RULE, int KW>
+__global__ void __launch_bounds__(32 * KW) sampler_wide_kernel(
+    qes_sampler_config cfg, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ W,
+    const T* __restrict__ flipC, const T* __restrict__ flipS, const int32_t* __restrict__ nbr,
+    const int32_t* __restrict__ nbr_pair, const int32_t* __restrict__ pair_i, const int32_t* __restrict__ pair_j,
+    const T* __restrict__ pairC, const T* __restrict__ pairS, uint32_t* __restrict__ chain_bits,
+    uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed, int32_t* __restrict__ accepted,
+    uint32_t* __restrict__ sample_bits, T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi,
+    const float* __restrict__ chain_beta) {
+  __shared__ uint32_t cw[SMP_MAX_WORDS];
+  __shared__ float red_la[2 * KW];
+  __shared__ T red_lp[KW];
+  const int chain = blockIdx.x;                 // the grid is exactly n_chains blocks
+  ChainCtx<T> P;
+  P.ns = cfg.ns; P.nh = cfg.nh; P.n_chains = cfg.n_chains; P.deg = cfg.deg; P.sweep_steps = cfg.sweep_steps;
+  P.recompute_every = cfg.recompute_every; P.num_samples = cfg.num_samples;
+  P.therm_steps_total = cfg.therm_steps_total;
+  P.beta_mu = (chain_beta ? chain_beta[chain] : cfg.beta) * cfg.mu;
+  P.k0 = (uint32_t)(cfg.seed & 0xffffffffu); P.k1 = (uint32_t)(cfg.seed >> 32);
+  P.chain_id = cfg.chain_offset + chain;
+  P.a = a; P.b = b; P.W = W; P.flipC = flipC; P.flipS = flipS; P.pairC = pairC; P.pairS = pairS;
+  P.nbr = nbr; P.nbr_pair = nbr_pair; P.pair_i = pair_i; P.pair_j = pair_j;
+  run_chain<T, MPL, RULE, false, KW>(P, chain, cw, nullptr, chain_bits, chain_step, proposed, accepted, sample_bits,
+                                     sample_logpsi, last_logpsi, red_la, red_lp);
+}
+
 // register caches up to 16 units per lane (real) / 8 (complex); wider ones in shared memory
 template <class T, int MPL>
 constexpr bool sampler_smem_cache() { return MPL > (ScalarTraits<T>::is_complex ? 8 : 16); }
+
+// wide layers: chains of KW warps (1), or one warp per chain with a shared-memory cache (0)
+static std::atomic<int> g_smp_wide{1};
+extern "C" int qes_sampler_set_wide(int on) {
+  g_smp_wide.store(on ? 1 : 0);
+  return QES_OK;
+}
+
+template <class T, int MPL, int KW>
+static int launch_sampler_wide(const qes_sampler_config* cfg, const void* a, const void* b, const void* W,
+                               const void* flipC, const void* flipS, const int32_t* nbr, const int32_t* nbr_pair,
+                               const int32_t* pi, const int32_t* pj, const void* pairC, const void* pairS,
+                               uint32_t* chain_bits, uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
+                               uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi, const float* chain_beta,
+                               cudaStream_t st) {
+#define QES_SMPW_ARGS                                                                                             \
+  *cfg, (const T*)a, (const T*)b, (const T*)W, (const T*)flipC, (const T*)flipS, nbr, nbr_pair, pi, pj,            \
+      (const T*)pairC, (const T*)pairS, chain_bits, chain_step, proposed, accepted, sample_bits, (T*)sample_logpsi, \
+      (T*)last_logpsi, chain_beta
+  if (cfg->rule == QES_RULE_LOCAL)
+    sampler_wide_kernel<T, MPL, QES_RULE_LOCAL, KW><<<(unsigned)cfg->n_chains, 32 * KW, 0, st>>>(QES_SMPW_ARGS);
+  else
+    sampler_wide_kernel<T, MPL, QES_RULE_EXCHANGE, KW><<<(unsigned)cfg->n_chains, 32 * KW, 0, st>>>(QES_SMPW_ARGS);
+#undef QES_SMPW_ARGS
+  QES_LAUNCH_CHECK();
+  return QES_OK;
+}
 
 template <class T, int MPL, int RULE, bool SM, int MINB>
 static int launch_sampler_kernel(unsigned grid, size_t smem, const qes_sampler_config* cfg, const void* a,
@@ -491,6 +588,30 @@ static int launch_sampler(int mpl_needed, int mpl_max, const qes_sampler_config*
   return QES_ERR_SIZE;
 }
 
+// Chains of several warps for hidden layers beyond one warp's register cache: KW = 2, 4 or 8 warps
+// of MPL = 16 (real) / 8 (complex) units per thread.  Returns QES_ERR_SIZE when none fits.
+template <class T>
+static int launch_sampler_multiwarp(int mpl_needed, const qes_sampler_config* cfg, const void* a, const void* b,
+                                    const void* W, const void* flipC, const void* flipS, const int32_t* nbr,
+                                    const int32_t* nbr_pair, const int32_t* pi, const int32_t* pj,
+                                    const void* pairC, const void* pairS, uint32_t* chain_bits,
+                                    uint64_t* chain_step, int32_t* proposed, int32_t* accepted,
+                                    uint32_t* sample_bits, void* sample_logpsi, void* last_logpsi,
+                                    const float* chain_beta, cudaStream_t st) {
+  constexpr int M = ScalarTraits<T>::is_complex ? 8 : 16;
+#define QES_SMPW_CASE(K)                                                                                        \
+  if (mpl_needed <= K * M)                                                                                      \
+    return launch_sampler_wide<T, M, K>(cfg, a, b, W, flipC, flipS, nbr, nbr_pair, pi, pj, pairC, pairS,        \
+                                        chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi, \
+                                        last_logpsi, chain_beta, st);
+  QES_SMPW_CASE(2)
+  QES_SMPW_CASE(4)
+  QES_SMPW_CASE(8)
+#undef QES_SMPW_CASE
+  qes_set_last_message("qes_sampler_run: too many hidden units for the multi-warp chains");
+  return QES_ERR_SIZE;
+}
+
 static int sampler_run_impl(int dtype, const qes_sampler_config* cfg, const float* chain_beta, const void* a,
                             const void* b, const void* W, const void* flipCt, const void* flipSt,
                             const int32_t* nbr_table, const int32_t* nbr_pair, const int32_t* pair_i,
@@ -515,6 +636,19 @@ static int sampler_run_impl(int dtype, const qes_sampler_config* cfg, const floa
   if (cfg->n_chains == 0) return QES_OK;
   const int mpl = (cfg->nh + 31) / 32;
   cudaStream_t st = (cudaStream_t)stream;
+  // hidden layers wider than one warp's register cache: chains of several warps (default), or one warp
+  // per chain with the cache in shared memory (qes_sampler_set_wide(0))
+  const int reg_max = dtype == QES_DTYPE_F32 ? 16 : 8;
+  if (mpl > reg_max && g_smp_wide.load(std::memory_order_relaxed) != 0) {
+    QES_ARG_CHECK(cfg->n_chains <= 0x7fffffff, "qes_sampler_run: too many chains");
+    if (dtype == QES_DTYPE_F32)
+      return launch_sampler_multiwarp<float>(mpl, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j,
+                                             pairCt, pairSt, chain_bits, chain_step, proposed, accepted, sample_bits,
+                                             sample_logpsi, last_logpsi, chain_beta, st);
+    return launch_sampler_multiwarp<float2>(mpl, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j,
+                                            pairCt, pairSt, chain_bits, chain_step, proposed, accepted, sample_bits,
+                                            sample_logpsi, last_logpsi, chain_beta, st);
+  }
   if (dtype == QES_DTYPE_F32)
     return launch_sampler<float>(mpl, 64, cfg, a, b, W, flipCt, flipSt, nbr_table, nbr_pair, pair_i, pair_j, pairCt,
                                  pairSt, chain_bits, chain_step, proposed, accepted, sample_bits, sample_logpsi,

@@ -295,14 +295,21 @@ def _gpu_sampler(net, rule, ns, chains, seed, therm, sweep, lattice=None, init=N
                       numsamples=1, lattice=lattice, initstate=init, n_particles=n_up)
 
 
-@pytest.mark.parametrize("cplx,nh", [(False, 20), (True, 20), (False, 600), (True, 300)])
-def test_sampler_local_trajectory_matches_oracle(cplx, nh):
-    """nh = 600 (real) / 300 (complex) run the shared-memory theta cache of the sampler."""
+@pytest.mark.parametrize("cplx,nh,wide", [(False, 20, 1), (True, 20, 1), (False, 600, 1), (True, 300, 1),
+                                          (False, 600, 0), (True, 300, 0), (False, 1600, 1), (True, 1000, 1)])
+def test_sampler_local_trajectory_matches_oracle(cplx, nh, wide):
+    """Hidden layers wider than one warp's register cache (nh > 512 real / 256 complex) run chains of
+    2-8 warps (wide = 1, the default: nh = 600 / 300 on two warps, 1600 / 1000 on four) or one warp per
+    chain with the theta cache in shared memory (wide = 0)."""
     ns = 10
     net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=8,
               init_scale=0.3 if nh <= 32 else 0.05)
-    smp = _gpu_sampler(net, "LOCAL", ns, 64, seed=77, therm=2, sweep=5)
-    bits, lp = smp.sample_bits(num_samples=6)
+    _lib.call("qes_sampler_set_wide", wide)
+    try:
+        smp = _gpu_sampler(net, "LOCAL", ns, 64, seed=77, therm=2, sweep=5)
+        bits, lp = smp.sample_bits(num_samples=6)
+    finally:
+        _lib.call("qes_sampler_set_wide", 1)
     got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()
     ref = osm.MetropolisSampler(ns, 64, rule="LOCAL", seed=77, therm_steps=2, sweep_steps=5)
     cfg, lp_ref, _ = ref.sample(oracle_params(net), 6)
@@ -311,11 +318,13 @@ def test_sampler_local_trajectory_matches_oracle(cplx, nh):
     assert np.array_equal(smp.proposed.cpu().numpy(), ref.proposed)
 
 
-@pytest.mark.parametrize("cplx", [False, True])
-def test_sampler_exchange_trajectory_matches_oracle(cplx):
+@pytest.mark.parametrize("cplx,nh", [(False, 32), (True, 32), (True, 400), (False, 800)])
+def test_sampler_exchange_trajectory_matches_oracle(cplx, nh):
+    """nh = 400 (complex) / 800 (real): exchange moves on multi-warp chains."""
     L, OL = qb.SquareLattice(2, 4, 4), olat.SquareLattice(2, 4, 4)
     ns = 16
-    net = RBM((ns,), n_hidden=32, dtype="complex64" if cplx else "float32", seed=9, init_scale=0.3)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=9,
+              init_scale=0.3 if nh <= 32 else 0.05)
     smp = _gpu_sampler(net, "EXCHANGE", ns, 64, seed=5, therm=1, sweep=7, lattice=L, init="RND_FIXED", n_up=8)
     bits, _ = smp.sample_bits(num_samples=5)
     got = dv.unpack_states(bits, ns, 1.0).cpu().numpy()

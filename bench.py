@@ -566,13 +566,13 @@ def run_ours(args, cfg, rank, world, local_rank):
         "e2e": e2e,
         "roofline": roof,
         "issue_rooflines": issue_rooflines(cfg, nqs, mixed, mixed["clocks"]),
-        "sr_tiling": ({"choice (mode, nc, ctas, pairs, fused_sv)": tuned["choice"], "cg_iteration_ms": tuned["ms"],
+        "sr_tiling": ({"choice (mode, nc, ctas, pairs, fused_sv, ov_split)": tuned["choice"], "cg_iteration_ms": tuned["ms"],
                        "candidates_ms": tuned["timings"], "cached": tuned["cached"]} if tuned else "automatic"),
     }
     if tuned:
         # the tuned tiling is process-wide: the other workloads below run the automatic one
         from pyqusolver_b200.autotune import apply_tiling
-        apply_tiling(0, 0, 0, 0, 0)
+        apply_tiling(0, 0, 0, 0, 0, 0)
     if rank == 0 and args.accuracy_epochs > 0:
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
     if rank == 0 and args.matched_epochs > 0 and args.config == "heis10x10":
@@ -884,7 +884,11 @@ def roofline(cfg, nqs, form):
                  net.flat, net.ns, net.nh, cfg["chains"] * cfg["samples"]) else "rbm_forward_kernel"}
     out = {"kernel": names.get(dom, dom), "launches_timed": cnt, "avg_launch_us": avg_s * 1e6,
            "share_of_timed_region": total_ms / float(np.sum([np.sum(v) for v in phases.values()])),
-           "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src}
+           "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": src,
+           # every profiled SR kernel class: launches and mean CUDA-event duration (the bracketing events
+           # serialise the chain, so these are upper bounds of the live per-launch times)
+           "sr_classes_us": {k: {"launches": int(c), "avg_us": float(ms) / c * 1e3}
+                             for k, (ms, c) in (form["prof"] or {}).items() if c}}
     if dom in ("ov", "ohu", "reduce", "sv"):
         b = kernel_bytes(cfg, nqs, dom, tc=tc)
         tr = traffic_db.get(cfg.get("name", ""), {}).get(dom)

@@ -358,6 +358,16 @@ int qes_sr_set_ohu_pairs(int on);
  * default: measured faster on B200).  Same operator, different float32
  * summation order.                                                        */
 int qes_sr_set_fused_sv(int on);
+/* Complex O v on the tensor cores when 2 (sites + 1) <= 256 (1):
+ * two products T_re V''^T and T_im V''^T into two TMEM accumulators, V'' =
+ * [Re v ; Im v] over the hidden units, combined in the epilogue (Re Y =
+ * D1_re - D2_im, Im Y = D1_im + D2_re); every O v CTA then reads half the
+ * direction-operand bytes of the single product over K = [Re t | Im t]
+ * against [Re v | -Im v ; Im v | Re v] (0, the default: measured as fast,
+ * O v is bound by its MMAs).  Same products, different
+ * float32 summation order.  Takes the fused S v kernel out of the plan
+ * (it reads the single-product operand).                                  */
+int qes_sr_set_ov_split(int on);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);

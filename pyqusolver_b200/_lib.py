@@ -124,6 +124,7 @@ SIGNATURES = {
     "qes_sr_set_tiling": [C.c_int, C.c_int, C.c_int],
     "qes_sr_set_ohu_pairs": [C.c_int],
     "qes_sr_set_fused_sv": [C.c_int],
+    "qes_sr_set_ov_split": [C.c_int],
     "qes_set_cg_graphs": [C.c_int],
     "qes_set_cg_fused": [C.c_int],
     "qes_sr_set_barrier_test": [C.c_uint, C.c_uint],

@@ -184,11 +184,12 @@ template <class V>
 __global__ void tc_build_vp_kernel(TcDims d, bool cplx, const V* __restrict__ v, uint16_t* __restrict__ out) {
   pdl_trigger();
   pdl_wait();                                             // v comes from the previous kernel
-  const int ns = d.ns, nh = d.nh, Mp = d.Mp, Kd = d.Kd, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
+  const int ns = d.ns, nh = d.nh, Mp = d.Mp, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
+  const bool spl = d.splitc;                               // V'': K = hidden units, rows Re v then Im v
   const V* vb = v + ns;
   const V* vW = v + ns + nh;
   const size_t term_bytes = (size_t)NB * KCH * 2;
-  const int items = NB * (Kd / 8);
+  const int items = NB * (d.VK / 8);
   for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
     const int n = it % NB, k8 = it / NB;
     const bool yim = cplx && n >= Sp;                     // row produces Im Y
@@ -197,14 +198,15 @@ __global__ void tc_build_vp_kernel(TcDims d, bool cplx, const V* __restrict__ v,
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int k = 8 * k8 + q;
-      const bool kim = cplx && k >= Mp;                    // K column holds Im t
+      const bool kim = !spl && cplx && k >= Mp;            // K column holds Im t
       const int m = kim ? k - Mp : k;
       float x = 0.f;
       if (m < nh && i <= ns) {
         const float vr = (i < ns) ? vre(vW, (int64_t)i * nh + m) : vre(vb, m);
         const float vi = (i < ns) ? vim(vW, (int64_t)i * nh + m) : vim(vb, m);
         // Re Y = Re t Re v - Im t Im v ;  Im Y = Re t Im v + Im t Re v
-        if (!yim) x = kim ? -vi : vr;
+        if (spl) x = yim ? vi : vr;
+        else if (!yim) x = kim ? -vi : vr;
         else x = kim ? vr : vi;
       }
       split_bf16(x, h[q], l[q]);
@@ -263,9 +265,15 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
   extern __shared__ __align__(128) uint8_t smem[];
   constexpr bool CPLX = ScalarTraits<T>::is_complex;
   const int ns = d.ns, KCH = d.KCH, NB = d.NB, Sp = d.Sp;
-  const int nK = d.Kd / KCH;
+  const int nK = d.Kd / KCH;                               // K chunks of a T tile
+  // split-complex: a stage holds the Re t and Im t chunks of the same hidden units and one V'' chunk;
+  // nKh = chunks per half (the Im chunks of a tile start there); the pipeline runs over nKh stages
+  const bool spl = d.splitc;
+  const int nKh = d.VK / KCH;
+  const int nP = spl ? nKh : nK;
   const uint32_t a_term = 128u * KCH * 2u, b_term = (uint32_t)NB * KCH * 2u;
-  const uint32_t stage_bytes = 2u * (a_term + b_term);
+  const uint32_t a_bytes = (spl ? 4u : 2u) * a_term;       // A part of a stage (hi, lo[, Im hi, Im lo])
+  const uint32_t stage_bytes = a_bytes + 2u * b_term;
   const int S = d.ov_stages;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * stage_bytes);
   uint64_t* empty = full + S;
@@ -297,15 +305,18 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
     umma::fence_mbar_init();
     // the first S stages go out before the TMEM allocation and the block-wide setup; the T tiles
     // (per-step operands) even before the previous kernel, which writes V', has completed
-    for (int c = 0; c < S && c < nK; ++c) {
+    for (int c = 0; c < S && c < nP; ++c) {
       umma::mbar_arrive_expect_tx(&full[c], stage_bytes);
       umma::bulk_g2s(smem + c * stage_bytes, ga + (size_t)c * 2 * a_term, 2 * a_term, &full[c]);
+      if (spl)
+        umma::bulk_g2s(smem + c * stage_bytes + 2 * a_term, ga + (size_t)(nKh + c) * 2 * a_term, 2 * a_term,
+                       &full[c]);
     }
   }
   pdl_wait();
   if (tid == 0) {
-    for (int c = 0; c < S && c < nK; ++c)
-      umma::bulk_g2s(smem + c * stage_bytes + 2 * a_term, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[c]);
+    for (int c = 0; c < S && c < nP; ++c)
+      umma::bulk_g2s(smem + c * stage_bytes + a_bytes, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[c]);
   }
   if (warp == 0) {
     umma::tmem_alloc(tslot, d.tmem_cols);
@@ -331,7 +342,7 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
     }
   } else if (warp == 0 && lane == 0) {
     // producer: stage s is refilled once the MMAs that read it have completed
-    for (int c = S; c < nK; ++c) {
+    for (int c = S; c < nP; ++c) {
       const int s = c % S;
       if (!umma::mbar_wait(&empty[s], ((c / S) - 1) & 1, kWaitLimit)) {
         record_error(status, QES_ERR_TIMEOUT);
@@ -340,14 +351,16 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
       uint8_t* st = smem + s * stage_bytes;
       umma::mbar_arrive_expect_tx(&full[s], stage_bytes);
       umma::bulk_g2s(st, ga + (size_t)c * 2 * a_term, 2 * a_term, &full[s]);
-      umma::bulk_g2s(st + 2 * a_term, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[s]);
+      if (spl) umma::bulk_g2s(st + 2 * a_term, ga + (size_t)(nKh + c) * 2 * a_term, 2 * a_term, &full[s]);
+      umma::bulk_g2s(st + a_bytes, gb + (size_t)c * 2 * b_term, 2 * b_term, &full[s]);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer: D (128 x NB) += A_hi B_hi + A_hi B_lo + A_lo B_hi over every 16-wide k-step;
     // NB > 256 is issued as two N parts (rows [0, 256) and [256, NB) of V') into adjacent TMEM columns
+    // split-complex: D1 (columns 0..) += T_re V''^T, D2 (columns 256..) += T_im V''^T, three terms each
     const int n_parts = NB > 256 ? 2 : 1;
     const uint32_t np0 = NB > 256 ? 256u : (uint32_t)NB;
-    for (int c = 0; c < nK; ++c) {
+    for (int c = 0; c < nP; ++c) {
       const int s = c % S;
       if (!umma::mbar_wait(&full[s], (c / S) & 1, kWaitLimit)) {
         record_error(status, QES_ERR_TIMEOUT);
@@ -355,11 +368,26 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
       }
       umma::tc_fence_after();
       const uint32_t sa = umma::smem_u32(smem + s * stage_bytes);
-      const uint32_t ahi = sa, alo = sa + a_term, bhi = sa + 2 * a_term, blo = bhi + b_term;
+      const uint32_t ahi = sa, alo = sa + a_term, bhi = sa + a_bytes, blo = bhi + b_term;
       for (int kk = 0; kk < KCH / 16; ++kk) {
         const uint32_t ko_a = 2u * kk * 128u * 16u, ko_b = 2u * kk * NB * 16u;
         const uint64_t dah = umma::smem_desc(ahi + ko_a, 128u * 16u, 128u);
         const uint64_t dal = umma::smem_desc(alo + ko_a, 128u * 16u, 128u);
+        if (spl) {
+          const uint32_t idesc = umma::idesc_bf16_f32(128, (uint32_t)NB);
+          const uint64_t dih = umma::smem_desc(ahi + 2 * a_term + ko_a, 128u * 16u, 128u);
+          const uint64_t dil = umma::smem_desc(ahi + 3 * a_term + ko_a, 128u * 16u, 128u);
+          const uint64_t dbh = umma::smem_desc(bhi + ko_b, NB * 16u, 128u);
+          const uint64_t dbl = umma::smem_desc(blo + ko_b, NB * 16u, 128u);
+          const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+          umma::mma_bf16(tbase, dah, dbh, idesc, acc);
+          umma::mma_bf16(tbase, dah, dbl, idesc, 1u);
+          umma::mma_bf16(tbase, dal, dbh, idesc, 1u);
+          umma::mma_bf16(tbase + 256u, dih, dbh, idesc, acc);
+          umma::mma_bf16(tbase + 256u, dih, dbl, idesc, 1u);
+          umma::mma_bf16(tbase + 256u, dil, dbh, idesc, 1u);
+          continue;
+        }
         for (int pt = 0; pt < n_parts; ++pt) {
           const uint32_t n0 = pt ? np0 : 0u, nn = pt ? (uint32_t)NB - np0 : np0;
           const uint32_t idesc = umma::idesc_bf16_f32(128, nn);
@@ -399,6 +427,18 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
     float y[16];
     umma::tmem_ld16(lane_addr + 16 * c, y);
     ov_fold16<CPLX>(16 * c, y, ns, Sp, wrd, nw, acc);
+  }
+  if (spl) {
+    // D2 = T_im V''^T: column n < Sp is Im t . Re v_n (-> Im Y_n), column Sp + n is Im t . Im v_n
+    // (-> -Re Y_n); folded with the same spin signs, then rotated into acc
+    float2 acc2 = make_float2(0.f, 0.f);
+    for (int c2 = cg; c2 < NB / 16; c2 += kColGroups) {
+      float y[16];
+      umma::tmem_ld16(lane_addr + 256u + 16 * c2, y);
+      ov_fold16<CPLX>(16 * c2, y, ns, Sp, wrd, nw, acc2);
+    }
+    acc.x -= acc2.y;
+    acc.y += acc2.x;
   }
   // + sigma_s . v_a: column group cg takes the sites of spin words cg, cg + 4, ...
   for (int w = cg; w < nw; w += kColGroups) {
@@ -1571,6 +1611,13 @@ static int pow2_at_least(int x) {
 // tiling overrides (qes_sr_set_tiling): 0 = automatic, 1 = single-M-tile kernel, 2 = M/N-tiled kernel;
 // hidden units per N chunk and target CTA count of the M/N-tiled O^H u (0 = automatic)
 static std::atomic<int> g_tile_mode{0}, g_tile_nc{0}, g_tile_ctas{0};
+// split-complex O v (V'' operand) where NB <= 256: off by default (heis10x10 CG iteration 45.0 us with
+// it, 44.9 us without: O v is bound by its MMAs, not by the direction operand it halves)
+static std::atomic<int> g_ov_split{0};
+extern "C" int qes_sr_set_ov_split(int on) {
+  g_ov_split.store(on ? 1 : 0);
+  return QES_OK;
+}
 static std::atomic<int> g_ohu_pairs{0};      // measured slower on B200 (heis 10x10: 49.5 vs 46.2 us per CG iteration)
 // fused S v kernel where the tiling admits it: off by default (heis10x10 CG iteration 54.6 us with it,
 // 44.2 us with the O v / O^H u pair: its per-tile phases run one after another behind block barriers)
@@ -1613,18 +1660,24 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   TcDims t{};
   t.ns = ns;
   t.nh = nh;
-  t.KCH = 32;
   t.Mp = (nh + 15) / 16 * 16;
   t.Np = cplx ? 2 * t.Mp : t.Mp;
-  t.Kd = cplx ? 2 * t.Mp : (nh + 31) / 32 * 32;               // multiple of KCH
   t.Sp = cplx ? (ns + 1 + 7) / 8 * 8 : (ns + 1 + 15) / 16 * 16;  // sites + the v_b row
   t.NB = cplx ? 2 * t.Sp : t.Sp;
-  if (n_samples < 1 || t.Kd % t.KCH != 0 || t.NB > 512) return false;
+  // complex O v as two products against V'' (two accumulators of NB <= 256 columns), K chunks of 16
+  // so that the Re t and Im t chunks of the same hidden units pair up
+  t.splitc = cplx && t.NB <= 256 && g_ov_split.load() != 0;
+  t.KCH = t.splitc ? 16 : 32;
+  t.Kd = cplx ? 2 * t.Mp : (nh + 31) / 32 * 32;               // multiple of KCH
+  t.VK = t.splitc ? t.Mp : t.Kd;
+  if (n_samples < 1 || t.Kd % t.KCH != 0 || t.VK % t.KCH != 0 || t.NB > 512) return false;
   const size_t tsz = cplx ? 8 : 4;
-  // ov: as many pipeline stages (2..4) as shared memory holds
-  const size_t stage = 2u * (128u * t.KCH * 2 + (size_t)t.NB * t.KCH * 2);
-  const size_t ov_extra = 8 * (2 * 4 + 1) + 16 + ((size_t)ns * tsz + 15) / 16 * 16 + 128u * 4u * ((ns + 31) / 32) + 64;
-  const int S = (int)std::min<size_t>(4, (kTcSmemLimit - ov_extra) / stage);
+  // ov: as many pipeline stages (2..4, 2..6 split) as shared memory holds
+  const size_t a_term = 128u * t.KCH * 2, b_term = (size_t)t.NB * t.KCH * 2;
+  const size_t stage = t.splitc ? 4u * a_term + 2u * b_term : 2u * (a_term + b_term);
+  const int smax = t.splitc ? 6 : 4;
+  const size_t ov_extra = 8 * (2 * smax + 1) + 16 + ((size_t)ns * tsz + 15) / 16 * 16 + 128u * 4u * ((ns + 31) / 32) + 64;
+  const int S = (int)std::min<size_t>(smax, (kTcSmemLimit - ov_extra) / stage);
   if (S < 2) return false;
   t.ov_stages = S;
   t.ov_smem = (int)(S * stage + ov_extra);
@@ -1635,7 +1688,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   if (mode == 1 && t.big) return false;
   if (!t.big) {
     t.im_off = pow2_at_least(t.Mp);
-    t.tmem_cols = pow2_at_least(std::max(cplx ? 2 * t.im_off : t.im_off, t.NB));
+    t.tmem_cols = pow2_at_least(std::max(cplx ? 2 * t.im_off : t.im_off, t.splitc ? 256 + t.NB : t.NB));
     if (t.tmem_cols > 512) return false;
     int kc = 256;
     while (kc >= 16) {
@@ -1657,7 +1710,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
     t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh + ns) * tsz + 64);
     // fused S v: the shared region holds the O v pipeline, later Sigma^T and two Q^T buffers; one CTA
     // per SM at most (launch bounds cap the registers at 128 per thread), so sv_grid CTAs are resident
-    if (g_sv.load() != 0) {
+    if (g_sv.load() != 0 && !t.splitc) {          // the fused kernel reads the [Re | -Im ; Im | Re] V'
       const int nsp = (ns + 1) & ~1, nw = (ns + 31) / 32;
       for (int S2 = 4; S2 >= 2 && !t.sv; --S2) {
         const size_t region = std::max<size_t>((size_t)S2 * stage, SV_SIG_BYTES + 2u * SV_QBUF);
@@ -1702,7 +1755,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   t.ohu_smem = (int)(2u * (R * kc * 2 + 2u * t.NR * kc * 2) + 2u * kc * tsz + 16 + 8 * 4 + 16 + 64);
   t.im_off = 0;
   t.cl = 1;
-  t.tmem_cols = pow2_at_least(std::max(t.MT * H * t.NC, t.NB));
+  t.tmem_cols = pow2_at_least(std::max(t.MT * H * t.NC, t.splitc ? 256 + t.NB : t.NB));
   if (t.tmem_cols > 512) return false;
   *dout = t;
   return true;
@@ -1714,7 +1767,7 @@ static size_t sz_t_cols(const TcDims& d) {
   return d.big ? (size_t)d.n_chunks * d.nnc * d.NR * d.KC * 2 * 2 : (size_t)d.n_chunks * d.Np * d.KC * 2 * 2;
 }
 static size_t sz_sig_cols(const TcDims& d) { return (size_t)d.n_chunks * (d.big ? d.MT * 128 : 128) * d.KC * 2; }
-static size_t sz_vp(const TcDims& d) { return (size_t)d.NB * d.Kd * 2 * 2; }
+static size_t sz_vp(const TcDims& d) { return (size_t)d.NB * d.VK * 2 * 2; }
 
 size_t tc_workspace_bytes(const TcDims& d) {
   return al256(sz_t_rows(d)) + al256(sz_t_cols(d)) + al256(sz_sig_cols(d)) + al256(sz_vp(d)) +
@@ -1815,7 +1868,7 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
     // one cooperative launch (every CTA resident: the mean of w is a grid barrier), after an
     // ordinary launch that builds V' on the first iteration
     if (build_vp) {
-      const int items = d.NB * (d.Kd / 8);
+      const int items = d.NB * (d.VK / 8);
       tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
       QES_LAUNCH_CHECK();
     }
@@ -1842,7 +1895,7 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
     // first iteration: an ordinary launch, so that everything before it (the setup that clears the
     // converged flag of the previous solve) has completed before the PDL chain begins; the flag is
     // read by tc_ov / tc_ohu before they wait on their predecessor
-    const int items = d.NB * (d.Kd / 8);
+    const int items = d.NB * (d.VK / 8);
     tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
     QES_LAUNCH_CHECK();
   }
@@ -1870,7 +1923,7 @@ template <class T, class V>
 static int tc_ov_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const V* v, float2* w_out,
                    const TcWork& w, cudaStream_t st) {
   const bool cplx = ScalarTraits<T>::is_complex;
-  const int items = d.NB * (d.Kd / 8);
+  const int items = d.NB * (d.VK / 8);
   tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
   QES_LAUNCH_CHECK();
   const int pf = qes_prof_begin(QES_PROF_OV, st);

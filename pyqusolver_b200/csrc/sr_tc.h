@@ -11,6 +11,11 @@ struct TcDims {
   int Np;            // ohu B rows: 2*Mp (complex) or Mp (real)
   int Kd;            // ov K: 2*Mp (complex: [Re t | Im t]) or nh padded to KCH (real)
   int KCH;           // ov K chunk per pipeline stage
+  // complex O v with NB <= 256 (splitc): two products T_re V''^T and T_im V''^T into two TMEM
+  // accumulators (columns 0 and 256), V'' = [Re v rows ; Im v rows] over K = the hidden units (VK =
+  // Mp): half the bytes of the [Re | -Im ; Im | Re] operand that every O v CTA reads; otherwise VK = Kd
+  bool splitc;
+  int VK;
   int Sp;            // sites + the v_b row, padded (rows of one Y half)
   int NB;            // ov N: 2*Sp (complex) or Sp (real)
   int KC;            // samples per ohu chunk (K of the ohu GEMM, multiple of 16)
@@ -94,6 +99,11 @@ __device__ __forceinline__ void tc_put_vp_elem(const TcDims& d, uint16_t* vp, in
 }
 __device__ __forceinline__ void tc_put_vp_elem(const TcDims& d, uint16_t* vp, int i, int m, double2 v) {
   const float vr = (float)v.x, vi = (float)v.y;
+  if (d.splitc) {                                            // V'' rows: Re v, then Im v
+    tc_put_vp(d, vp, i, m, vr);
+    tc_put_vp(d, vp, d.Sp + i, m, vi);
+    return;
+  }
   tc_put_vp(d, vp, i, m, vr);                                // Re Y row: [Re v | -Im v]
   tc_put_vp(d, vp, i, d.Mp + m, -vi);
   tc_put_vp(d, vp, d.Sp + i, m, vi);                         // Im Y row: [Im v | Re v]

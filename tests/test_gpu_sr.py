@@ -164,8 +164,9 @@ def test_train_step_uses_the_sampler_weights():
 @pytest.mark.parametrize("cplx", [True, False])
 @pytest.mark.parametrize("n", [700, 19244])
 def test_fused_sv_matches_kernel_pair_and_oracle(cplx, n):
-    """The cooperative S v kernel (qes_sr_set_fused_sv(1), the default) against the O v + O^H u kernel
-    pair (0) on the same weighted batch, and both against the oracle's weighted S v.  n = 19244 is
+    """The cooperative S v kernel (qes_sr_set_fused_sv(1)) against the O v + O^H u kernel pair (0, the
+    default), with the single-product and the split-complex O v (qes_sr_set_ov_split), on the same
+    weighted batch, and all against the oracle's weighted S v.  n = 19244 is
     151 sample tiles (the last one 44 samples): more tiles than CTAs, so some CTAs fold two tiles
     into their TMEM accumulators."""
     ns, nh = 9, 18
@@ -188,19 +189,24 @@ def test_fused_sv_matches_kernel_pair_and_oracle(cplx, n):
     ys = {}
     _lib.set_sr_impl(2)
     try:
-        for fused in (1, 0):
+        # (fused S v, split-complex O v): the fused kernel reads the single-product operand
+        for fused, split in ((1, 0), (0, 0), (0, 1)):
             _lib.call("qes_sr_set_fused_sv", fused)
+            _lib.call("qes_sr_set_ov_split", split)
             assert _lib.sr_uses_tensor_cores(dv.dtype_code(net.flat), ns, nh, n)
-            ys[fused] = dv.sr_matvec(net.flat, ns, nh, bits, tn, vt, shift=1e-3, probs=probs_t).cpu().numpy()
+            plan = _lib.sr_tc_plan(dv.dtype_code(net.flat), ns, nh, n)
+            assert plan["sv"] == fused
+            ys[fused, split] = dv.sr_matvec(net.flat, ns, nh, bits, tn, vt, shift=1e-3, probs=probs_t).cpu().numpy()
             again = dv.sr_matvec(net.flat, ns, nh, bits, tn, vt, shift=1e-3, probs=probs_t).cpu().numpy()
-            assert np.array_equal(ys[fused], again)              # fixed summation order: repeatable
+            assert np.array_equal(ys[fused, split], again)      # fixed summation order: repeatable
     finally:
         _lib.call("qes_sr_set_fused_sv", 0)
+        _lib.call("qes_sr_set_ov_split", 0)
         _lib.set_sr_impl(0)
     ref = S @ v + 1e-3 * v
-    assert rel_err(ys[1], ref) < 1e-4
-    assert rel_err(ys[0], ref) < 1e-4
-    assert rel_err(ys[1], ys[0]) < 2e-5
+    for key, y in ys.items():
+        assert rel_err(y, ref) < 1e-4, key
+        assert rel_err(y, ys[0, 0]) < 2e-5, key
 
 
 # ------------------------------------------------------------------------- Jacobi-preconditioned CG

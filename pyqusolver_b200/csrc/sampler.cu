@@ -214,8 +214,34 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
   int64_t rec = 0;
   int64_t next_record = P.therm_steps_total + P.sweep_steps;
 
+  // One-warp chains: the Philox draws of 32 consecutive proposals are computed at once, lane q
+  // taking step + q, and handed out by shuffles (one counter-mode call per 32 proposals instead of
+  // one per proposal; the same numbers, so the same chain; heis10x10 sampling 1.47 -> 1.28 ms).
+  // Multi-warp chains draw per proposal: the three live registers pushed their kernel past its
+  // register cap (20x20 TFIM 28 -> 30 ms).
+  uint32_t pb_x = 0, pb_y = 0;
+  float pb_lu = 0.f;
+  int pb_k = 32;
   for (int64_t it = 0; it < total; ++it) {
-    const Philox4 r = philox4x32_10(cid, (uint32_t)step, (uint32_t)(step >> 32), QES_STREAM_PROPOSAL, P.k0, P.k1);
+    Philox4 r;
+    float log_u;
+    if constexpr (KW == 1) {
+      if (pb_k == 32) {
+        const uint64_t sb = step + (uint64_t)(threadIdx.x & 31);
+        const Philox4 rb = philox4x32_10(cid, (uint32_t)sb, (uint32_t)(sb >> 32), QES_STREAM_PROPOSAL, P.k0, P.k1);
+        pb_x = rb.x;
+        pb_y = rb.y;
+        pb_lu = logf(uniform_open(rb.z));
+        pb_k = 0;
+      }
+      r.x = __shfl_sync(0xffffffffu, pb_x, pb_k);
+      r.y = __shfl_sync(0xffffffffu, pb_y, pb_k);
+      log_u = __shfl_sync(0xffffffffu, pb_lu, pb_k);
+      ++pb_k;
+    } else {
+      r = philox4x32_10(cid, (uint32_t)step, (uint32_t)(step >> 32), QES_STREAM_PROPOSAL, P.k0, P.k1);
+      log_u = logf(uniform_open(r.z));
+    }
     const int i = (int)bounded_u32(r.x, (uint32_t)ns);
     bool moved;
     int i0 = i, j0 = -1;        // sites flipped (j0 = -1 for a single flip)
@@ -305,7 +331,7 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
       re_delta = la + 2.f * g * to_re(av);
     }
     const float log_acc = fminf(bm * re_delta, 0.f);
-    const bool keep = logf(uniform_open(r.z)) < log_acc;
+    const bool keep = log_u < log_acc;
     if (keep && moved) {
       const T* wi = W + (int64_t)i0 * nh;
       const T* wj = W + (int64_t)(j0 >= 0 ? j0 : i0) * nh;

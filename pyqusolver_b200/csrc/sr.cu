@@ -2914,6 +2914,26 @@ static int launch_batch_ohu(int n_ohu, int threads, int SC, int qstride, int sst
   return QES_OK;
 }
 
+struct BatchGraphKey {
+  const void* inst; const void* ov_items; const void* ohu_items; const void* bits; const void* tt; const void* x;
+  const void* bscal;
+  int n_inst, n_ov, n_ohu, chunk, cplx, ov_threads, ohu_threads, ohu_sc, ohu_qstride, ohu_sstride, pad0, pad1;
+  int64_t ov_smem, ohu_smem;
+  double shift;
+  bool operator==(const BatchGraphKey& o) const { return std::memcmp(this, &o, sizeof(*this)) == 0; }
+};
+static_assert(sizeof(BatchGraphKey) == 7 * sizeof(void*) + 12 * 4 + 2 * 8 + 8, "BatchGraphKey has padding bytes");
+struct BatchGraphSlot {
+  bool init = false;
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  BatchGraphKey key{};
+  long long nodes = 0;
+};
+static std::mutex g_bgraph_mu;
+static BatchGraphSlot g_bgraph[kMaxGraphDevices];
+
 template <class T>
 static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, const int4* ov_items, int n_ohu,
                          const int4* ohu_items, int64_t n_params_total, const uint32_t* bits, const T* tt,
@@ -2974,17 +2994,69 @@ static int batch_sr_cg_t(int n_inst, const qes_batch_instance* inst, int n_ov, c
   QES_CUDA_CHECK(cudaMemcpyAsync(&done, L.n_done, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
   QES_CUDA_CHECK(cudaStreamSynchronize(st));
   int it = 0;
-  while ((int)done < n_inst && it < opt->maxiter) {
-    const int nrun = std::min(check, opt->maxiter - it);
+  auto run_chunk = [&](int nrun) -> int {
     for (int q = 0; q < nrun; ++q) {
-      if ((rc = ov(p))) return rc;
+      int r2;
+      if ((r2 = ov(p))) return r2;
       batch_mean_kernel<<<n_inst, BCG_THREADS, 0, st>>>(inst, L.w, L.bscal, 9, 1);
-      if ((rc = ohu(L.w, 1))) return rc;
+      if ((r2 = ohu(L.w, 1))) return r2;
       const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
       batch_cg_update_kernel<T, V><<<n_inst, BCG_THREADS, 0, st>>>(inst, partial, opt->shift, x, r, p, Ap, L.bscal,
                                                                    L.n_done);
       qes_prof_end(pfr, st);
       QES_LAUNCH_CHECK_N(4);
+    }
+    return QES_OK;
+  };
+  // Full chunks run as one CUDA graph on a private stream (captured once per launch configuration
+  // and set of buffers, then replayed): four launches per lockstep iteration otherwise
+  int dev = 0;
+  QES_CUDA_CHECK(cudaGetDevice(&dev));
+  const bool graphs = g_use_graphs.load() != 0 && !qes_prof_on() && dev >= 0 && dev < kMaxGraphDevices;
+  while ((int)done < n_inst && it < opt->maxiter) {
+    const int nrun = std::min(check, opt->maxiter - it);
+    if (!graphs || nrun != check) {
+      if ((rc = run_chunk(nrun))) return rc;
+    } else {
+      std::lock_guard<std::mutex> lock(g_bgraph_mu);
+      BatchGraphSlot& gs = g_bgraph[dev];
+      if (!gs.init) {
+        QES_CUDA_CHECK(cudaStreamCreateWithFlags(&gs.cs, cudaStreamNonBlocking));
+        QES_CUDA_CHECK(cudaEventCreateWithFlags(&gs.ev_in, cudaEventDisableTiming));
+        QES_CUDA_CHECK(cudaEventCreateWithFlags(&gs.ev_out, cudaEventDisableTiming));
+        gs.init = true;
+      }
+      const BatchGraphKey key{inst, ov_items, ohu_items, bits, tt, x, L.bscal, n_inst, n_ov, n_ohu, nrun,
+                              CPLX ? 1 : 0, ov_threads, ohu_threads, ohu_sc, ohu_qstride, ohu_sstride, 0, 0,
+                              (int64_t)ov_smem, (int64_t)ohu_smem, opt->shift};
+      if (gs.exec == nullptr || !(gs.key == key)) {
+        if (gs.exec) {
+          cudaGraphExecDestroy(gs.exec);
+          gs.exec = nullptr;
+        }
+        const long long before = qes_launch_count(0);
+        QES_CUDA_CHECK(cudaStreamBeginCapture(gs.cs, cudaStreamCaptureModeThreadLocal));
+        cudaStream_t saved = st;
+        st = gs.cs;
+        const int rcap = run_chunk(nrun);
+        st = saved;
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(gs.cs, &g);
+        if (rcap) return rcap;
+        if (ec != cudaSuccess) { qes_set_last_error(ec, "cudaStreamEndCapture"); return QES_ERR_CUDA; }
+        const cudaError_t ei = cudaGraphInstantiate(&gs.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) { gs.exec = nullptr; qes_set_last_error(ei, "cudaGraphInstantiate"); return QES_ERR_CUDA; }
+        gs.nodes = qes_launch_count(0) - before;
+        qes_count_launches((int)-gs.nodes);     // captured, not run
+        gs.key = key;
+      }
+      QES_CUDA_CHECK(cudaEventRecord(gs.ev_in, st));
+      QES_CUDA_CHECK(cudaStreamWaitEvent(gs.cs, gs.ev_in, 0));
+      QES_CUDA_CHECK(cudaGraphLaunch(gs.exec, gs.cs));
+      QES_CUDA_CHECK(cudaEventRecord(gs.ev_out, gs.cs));
+      QES_CUDA_CHECK(cudaStreamWaitEvent(st, gs.ev_out, 0));
+      qes_count_launches((int)gs.nodes);
     }
     it += nrun;
     QES_CUDA_CHECK(cudaMemcpyAsync(&done, L.n_done, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));

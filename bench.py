@@ -208,6 +208,34 @@ def accuracy_check(epochs, name="tfim16"):
     return out
 
 
+def ed_energy_check(epochs, name="j1j2_6x6"):
+    """Energy against ED on the 6x6 J1-J2 workload: train it (mixed form) and compare the mean
+    energy of the last 50 epochs with the exact ground energy of the committed fixture
+    ``tests/golden/ed_j1j2_6x6.json`` (GPU Lanczos in the k = 0, even-flip sector,
+    ``qes_ed_lanczos_symm``; regenerate with ``python tests/golden/make_ed_j1j2_6x6.py``)."""
+    import torch
+    from pyqusolver_b200 import _lib
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "ed_j1j2_6x6.json")) as f:
+        e_exact = float(json.load(f)["e0_j2_0.5"])
+    cfg = CONFIGS[name]
+    _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
+    nqs, tdvp = build_nqs(cfg, seed=1)
+    hist = []
+    t0 = time.perf_counter()
+    for _ in range(int(epochs)):
+        info = nqs.train_step(lr=cfg["lr"], tdvp=tdvp)
+        hist.append(info["mean"].real)
+    torch.cuda.synchronize()
+    tail = np.array(hist[-50:])
+    e = float(tail.mean())
+    return {"workload": name, "epochs": int(epochs), "lr": cfg["lr"], "shift": cfg["shift"],
+            "exact_method": "GPU Lanczos, 6x6 k=0 even-flip sector (qes_ed_lanczos_symm), committed fixture",
+            "e_exact": e_exact, "energy": e, "stderr": float(tail.std() / np.sqrt(len(tail))),
+            "rel_err": abs(e - e_exact) / abs(e_exact), "energy_by_100_epochs": [float(np.mean(hist[i:i + 100]))
+                                                                                 for i in range(0, len(hist), 100)],
+            "seconds": time.perf_counter() - t0}
+
+
 def matched_energy_check(epochs, every, name="heis10x10"):
     """Equal-Delta-E on the benchmarked workload, where no ED exists.  Independent VMC runs cannot
     resolve 1e-4 here: the Markov chains of two runs decorrelate within a few epochs in any
@@ -575,6 +603,8 @@ def run_ours(args, cfg, rank, world, local_rank):
         apply_tiling(0, 0, 0, 0, 0, 0)
     if rank == 0 and args.accuracy_epochs > 0:
         line["accuracy"] = accuracy_check(args.accuracy_epochs)
+    if rank == 0 and world == 1 and args.ed_epochs > 0:
+        line["accuracy_ed_j1j2_6x6"] = ed_energy_check(args.ed_epochs)
     if rank == 0 and args.matched_epochs > 0 and args.config == "heis10x10":
         line["accuracy_matched_fp64"] = matched_energy_check(args.matched_epochs, args.matched_every)
     if rank == 0 and world == 1 and args.matched_other_epochs > 0:
@@ -1042,6 +1072,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="plain_fp32,mixed", help="comma list of plain_fp32, mixed (mixed is required)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--ed-epochs", type=int, default=1500,
+                    help="epochs of the 6x6 J1-J2 training compared with its exact energy (0: skip)")
     ap.add_argument("--accuracy-epochs", type=int, default=300,
                     help="epochs of the ED-checked mixed vs plain comparison on tfim16 (0 = skip)")
     ap.add_argument("--matched-epochs", type=int, default=300,

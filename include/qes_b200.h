@@ -553,6 +553,27 @@ int qes_ed_sector_workspace_bytes(int ns, int n_up, int parity, size_t* bytes);
 int qes_ed_lanczos_sector(int ns, int n_up, int parity, const qes_hamiltonian* ham, int max_iter,
                           double tol, uint64_t seed, double* e0_out, int* iterations_out,
                           void* workspace, size_t workspace_bytes, void* stream);
+/* Lanczos in a momentum sector of a translation-invariant S^z-conserving Hamiltonian on an
+ * lx x ly periodic lattice (site x + lx*y; a chain is ly = 1, lx*ly <= 62): the states with n_up
+ * up spins reduced by the lx*ly translations and, with parity = +1 / -1 (ns = 2 n_up, no z field),
+ * the spin flip; momentum 0 (kx/ky = 0) or pi (= 1, even side) per axis, the real characters of
+ * QES/Algebra/Symmetries/translation.py:470-519 (sector index 0 or L/2).  Basis: the orbit
+ * minima, listed on the device by two enumeration passes over the C(ns, n_up) (C(ns - 1, n_up)
+ * with the flip; at most 2^37) colex ranks.  Call qes_ed_symm_dim (workspace from
+ * qes_ed_symm_workspace_bytes with dim = 0) for the dimension, then qes_ed_symm_workspace_bytes
+ * with it (≈ 32 (dim + 1) + C/8 bytes for C ranks) for qes_ed_lanczos_symm.  The Hamiltonian is
+ * checked on the host: anti-parallel pair moves with real coefficients, bonds and fields that map
+ * onto themselves under T(1, 0) and T(0, 1) (else QES_ERR_ARG).  dim_out (optional) receives
+ * the sector dimension.  Replaces model.diagonalize(method='lanczos') in a symmetry sector of a
+ * HilbertSpace with translation and parity symmetries (QES/Algebra/hamil.py:1809+,
+ * QES/Algebra/Symmetries/momentum_sectors.py).                                               */
+int qes_ed_symm_workspace_bytes(int lx, int ly, int n_up, int parity, int kx, int ky, uint64_t dim,
+                                size_t* bytes);
+int qes_ed_symm_dim(int lx, int ly, int n_up, int parity, int kx, int ky, uint64_t* dim,
+                    void* workspace, size_t workspace_bytes, void* stream);
+int qes_ed_lanczos_symm(int lx, int ly, int n_up, int parity, int kx, int ky, const qes_hamiltonian* ham,
+                        int max_iter, double tol, uint64_t seed, double* e0_out, int* iterations_out,
+                        uint64_t* dim_out, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Batched independent problems.  Many (RBM, Hamiltonian, chain set) triples

@@ -161,6 +161,11 @@ SIGNATURES = {
     "qes_ed_sector_workspace_bytes": [C.c_int, C.c_int, C.c_int, C.POINTER(_sz)],
     "qes_ed_lanczos_sector": [C.c_int, C.c_int, C.c_int, C.POINTER(Hamiltonian), C.c_int, C.c_double, _u64,
                               C.POINTER(C.c_double), C.POINTER(C.c_int), _vp, _sz, _vp],
+    "qes_ed_symm_workspace_bytes": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _u64, C.POINTER(_sz)],
+    "qes_ed_symm_dim": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_u64), _vp, _sz, _vp],
+    "qes_ed_lanczos_symm": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(Hamiltonian), C.c_int,
+                            C.c_double, _u64, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(_u64), _vp, _sz,
+                            _vp],
     "qes_ed_matvec": [C.c_int, C.POINTER(Hamiltonian), _vp, _vp, _vp],
     "qes_ed_lanczos": [C.c_int, C.POINTER(Hamiltonian), C.c_int, C.c_double, _u64, C.POINTER(C.c_double),
                        C.POINTER(C.c_int), _vp, _sz, _vp],

@@ -133,10 +133,14 @@ class SpinHamiltonian:
 
     # -- exact ground energy -------------------------------------------------------------
     def diagonalize(self, method: str = "lanczos", k: int = 1, tol: float = 1e-12, maxiter: int = 600,
-                    seed: int = 7, n_up=None, spin_flip=None, **kwargs):
+                    seed: int = 7, n_up=None, spin_flip=None, momentum=None, **kwargs):
         """Ground energy by Lanczos on the GPU (``qes_ed_lanczos``: the full 2^ns basis; with ``n_up``,
         ``qes_ed_lanczos_sector``: the S^z sector of n_up up spins, and with ``spin_flip`` = +1 / -1
-        also one spin-flip parity, for S^z-conserving models without a field).
+        also one spin-flip parity, for S^z-conserving models without a field).  With ``momentum``
+        (the translation sector index per axis, ``n`` or ``(nx, ny)``, each 0 or L/2 as in
+        ``QES/Algebra/Symmetries/translation.py:196-262``; periodic lattices only),
+        ``qes_ed_lanczos_symm``: the sector reduced by the lattice translations as well; the sector
+        dimension is stored in ``sector_dim``.
 
         Mirrors ``model.diagonalize(method='lanczos')`` (``QES/Algebra/hamil.py:1809``) for the
         lowest eigenvalue: the result is stored in ``eig_val`` (ascending, length 1).
@@ -149,6 +153,8 @@ class SpinHamiltonian:
         import torch
         from . import _lib, device as dv
         dh = dv.DeviceHamiltonian(self.lower())
+        if momentum is not None:
+            return self._diagonalize_symm(dh, n_up, spin_flip, momentum, maxiter, tol, seed)
         if n_up is not None or spin_flip is not None:
             n_up = self.ns // 2 if n_up is None else int(n_up)
             parity = 0 if spin_flip in (None, 0) else (1 if int(spin_flip) > 0 else -1)
@@ -172,6 +178,48 @@ class SpinHamiltonian:
                   _lib.stream_ptr())
         self._eig_val = np.array([e0.value])
         self.lanczos_iterations = its.value
+        return self._eig_val
+
+    def _diagonalize_symm(self, dh, n_up, spin_flip, momentum, maxiter, tol, seed):
+        import ctypes as C
+        import torch
+        from . import _lib
+        lat = self.lattice
+        lx, ly = int(getattr(lat, "lx", self.ns)), int(getattr(lat, "ly", 1))
+        if lx * ly != self.ns or str(getattr(lat, "bc", "pbc")).lower() != "pbc":
+            raise ValueError("diagonalize(momentum=...): needs a periodic lx x ly lattice")
+        mom = (momentum,) if np.isscalar(momentum) else tuple(momentum)
+        mom = tuple(int(m) for m in mom) + (0,) * (2 - len(mom))
+        k = []
+        for n, size in zip(mom, (lx, ly)):
+            n %= size
+            if n == 0:
+                k.append(0)
+            elif 2 * n == size:
+                k.append(1)
+            else:
+                raise NotImplementedError("diagonalize(momentum=...): sector index 0 or L/2 per axis "
+                                          "(the real characters)")
+        n_up = self.ns // 2 if n_up is None else int(n_up)
+        parity = 0 if spin_flip in (None, 0) else (1 if int(spin_flip) > 0 else -1)
+        args = (lx, ly, n_up, parity, k[0], k[1])
+        nb = C.c_size_t(0)
+        _lib.call("qes_ed_symm_workspace_bytes", *args, C.c_uint64(0), C.byref(nb))
+        ws = torch.empty((int(nb.value),), dtype=torch.uint8, device="cuda")
+        dim = C.c_uint64(0)
+        _lib.call("qes_ed_symm_dim", *args, C.byref(dim), _lib.ptr(ws), int(ws.numel()), _lib.stream_ptr())
+        if dim.value == 0:
+            raise ValueError(f"diagonalize: the sector {dict(n_up=n_up, spin_flip=parity, momentum=mom)} is empty")
+        _lib.call("qes_ed_symm_workspace_bytes", *args, C.c_uint64(dim.value), C.byref(nb))
+        del ws
+        ws = torch.empty((int(nb.value),), dtype=torch.uint8, device="cuda")
+        e0, its, d2 = C.c_double(0.0), C.c_int(0), C.c_uint64(0)
+        _lib.call("qes_ed_lanczos_symm", *args, C.byref(dh.struct), int(maxiter), float(tol), C.c_uint64(int(seed)),
+                  C.byref(e0), C.byref(its), C.byref(d2), _lib.ptr(ws), int(ws.numel()), _lib.stream_ptr())
+        del ws
+        self._eig_val = np.array([e0.value])
+        self.lanczos_iterations = its.value
+        self.sector_dim = int(d2.value)
         return self._eig_val
 
     @property

@@ -179,15 +179,15 @@ struct ChainCtx {
 // Runs proposals for chain `chain` (index within its problem) with the
 // problem's packed spins staged in `cw` (shared memory, one warp).
 // KW > 1: the chain runs on a whole block of KW warps (register caches only); thread gl = threadIdx.x
-// owns units gl + 32 KW r, every thread draws the same Philox numbers and takes the same decision,
-// and the log-ratio is summed over the warps through `red_la` (two sets of KW slots, used
+// owns units gl + 32 KW r, the block draws the Philox numbers of 32 KW proposals at once into `rng`
+// (shared memory), every thread takes the same decision, and the log-ratio is summed over the warps through `red_la` (two sets of KW slots, used
 // alternately) and `red_lp` (KW slots) in shared memory, in warp order.
 template <class T, int MPL, int RULE, bool SMEM = false, int KW = 1>
 QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_slice, uint32_t* __restrict__ chain_bits,
                      uint64_t* __restrict__ chain_step, int32_t* __restrict__ proposed,
                      int32_t* __restrict__ accepted, uint32_t* __restrict__ sample_bits,
                      T* __restrict__ sample_logpsi, T* __restrict__ last_logpsi, float* red_la = nullptr,
-                     T* red_lp = nullptr) {
+                     T* red_lp = nullptr, uint4* rng = nullptr) {
   static_assert(KW == 1 || !SMEM, "chains shared by several warps keep their caches in registers");
   constexpr int STRIDE = 32 * KW;
   const int lane = KW == 1 ? (int)(threadIdx.x & 31) : (int)threadIdx.x;   // index within the chain
@@ -214,14 +214,14 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
   int64_t rec = 0;
   int64_t next_record = P.therm_steps_total + P.sweep_steps;
 
-  // One-warp chains: the Philox draws of 32 consecutive proposals are computed at once, lane q
-  // taking step + q, and handed out by shuffles (one counter-mode call per 32 proposals instead of
-  // one per proposal; the same numbers, so the same chain; heis10x10 sampling 1.47 -> 1.28 ms).
-  // Multi-warp chains draw per proposal: the three live registers pushed their kernel past its
-  // register cap (20x20 TFIM 28 -> 30 ms).
+  // The Philox draws of STRIDE consecutive proposals are computed at once, thread q taking step + q
+  // (one counter-mode call per STRIDE proposals instead of one per proposal in every thread; the same
+  // numbers, so the same chain): one-warp chains hand them out by shuffles (heis10x10 sampling
+  // 1.47 -> 1.28 ms), multi-warp chains through `rng` in shared memory (three more live registers
+  // per thread pushed their kernel past its register cap).
   uint32_t pb_x = 0, pb_y = 0;
   float pb_lu = 0.f;
-  int pb_k = 32;
+  int pb_k = STRIDE;
   for (int64_t it = 0; it < total; ++it) {
     Philox4 r;
     float log_u;
@@ -239,8 +239,18 @@ QES_D void run_chain(const ChainCtx<T>& P, int chain, uint32_t* cw, T* theta_sli
       log_u = __shfl_sync(0xffffffffu, pb_lu, pb_k);
       ++pb_k;
     } else {
-      r = philox4x32_10(cid, (uint32_t)step, (uint32_t)(step >> 32), QES_STREAM_PROPOSAL, P.k0, P.k1);
-      log_u = logf(uniform_open(r.z));
+      if (pb_k == STRIDE) {
+        chain_sync<KW>();                     // every thread has read the previous batch
+        const uint64_t sb = step + (uint64_t)lane;
+        const Philox4 rb = philox4x32_10(cid, (uint32_t)sb, (uint32_t)(sb >> 32), QES_STREAM_PROPOSAL, P.k0, P.k1);
+        rng[lane] = make_uint4(rb.x, rb.y, __float_as_uint(logf(uniform_open(rb.z))), 0u);
+        chain_sync<KW>();
+        pb_k = 0;
+      }
+      const uint4 q = rng[pb_k++];
+      r.x = q.x;
+      r.y = q.y;
+      log_u = __uint_as_float(q.z);
     }
     const int i = (int)bounded_u32(r.x, (uint32_t)ns);
     bool moved;
@@ -437,9 +447,12 @@ __global__ void __launch_bounds__(32 * SMP_WARPS, MINB) sampler_kernel(
 // theta / tanh cache in registers, so one proposal's table row is in flight at once (one L2 round
 // trip) instead of being walked one chunk per round trip by a single warp, and no shared-memory cache
 // caps the resident chains.  Same arithmetic per unit as the one-warp kernels; the log-ratio is summed
-// per warp and then over the warps in order.
+// per warp and then over the warps in order.  Four-warp chains are held to 72 registers (seven
+// chains per SM): with the Philox draws batched the compiler took 96 (five chains per SM) and the
+// 20x20 TFIM sampling ran 30.2 ms, capped 25.8 ms (28.7 ms before the batching; caps of 8 and 9
+// chains per SM ran 29.0 and 27.0 ms).
 template <class T, int MPL, int RULE, int KW>
-__global__ void __launch_bounds__(32 * KW) sampler_wide_kernel(
+__global__ void __launch_bounds__(32 * KW, KW == 4 ? 7 : 1) sampler_wide_kernel(
     qes_sampler_config cfg, const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ W,
     const T* __restrict__ flipC, const T* __restrict__ flipS, const int32_t* __restrict__ nbr,
     const int32_t* __restrict__ nbr_pair, const int32_t* __restrict__ pair_i, const int32_t* __restrict__ pair_j,
@@ -450,6 +463,7 @@ __global__ void __launch_bounds__(32 * KW) sampler_wide_kernel(
   __shared__ uint32_t cw[SMP_MAX_WORDS];
   __shared__ float red_la[2 * KW];
   __shared__ T red_lp[KW];
+  __shared__ uint4 rng[32 * KW];
   const int chain = blockIdx.x;                 // the grid is exactly n_chains blocks
   ChainCtx<T> P;
   P.ns = cfg.ns; P.nh = cfg.nh; P.n_chains = cfg.n_chains; P.deg = cfg.deg; P.sweep_steps = cfg.sweep_steps;
@@ -461,7 +475,7 @@ __global__ void __launch_bounds__(32 * KW) sampler_wide_kernel(
   P.a = a; P.b = b; P.W = W; P.flipC = flipC; P.flipS = flipS; P.pairC = pairC; P.pairS = pairS;
   P.nbr = nbr; P.nbr_pair = nbr_pair; P.pair_i = pair_i; P.pair_j = pair_j;
   run_chain<T, MPL, RULE, false, KW>(P, chain, cw, nullptr, chain_bits, chain_step, proposed, accepted, sample_bits,
-                                     sample_logpsi, last_logpsi, red_la, red_lp);
+                                     sample_logpsi, last_logpsi, red_la, red_lp, rng);
 }
 
 // register caches up to 16 units per lane (real) / 8 (complex); wider ones in shared memory

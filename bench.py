@@ -58,7 +58,8 @@ CONFIGS = {
 
 
 def env_rank():
-    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+    from pyqusolver_b200.replicas import rank_env
+    return rank_env()
 
 
 # ---------------------------------------------------------------------------------------- clocks
@@ -328,13 +329,10 @@ def run_batch(args, cfg, rank, world, local_rank):
     """Batched uneven problems (one launch per phase over all problems); one form (float32 CUDA cores)."""
     import torch
     from pyqusolver_b200 import _lib
+    from pyqusolver_b200 import replicas
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    B, Ls, hx = build_batch(cfg, seed=1 + rank)
+    dist = replicas.init_group(world)
+    B, Ls, hx = build_batch(cfg, seed=replicas.replica_seed(1, rank))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     kw = dict(shift=cfg["shift"], rtol=cfg["rtol"], maxiter=cfg["maxiter"], check_every=32)
 
@@ -381,13 +379,9 @@ def run_batch(args, cfg, rank, world, local_rank):
         prof_total += ev[0].elapsed_time(ev[6])
     prof = _lib.profile_read(reset=True)
     _lib.profile_enable(False)
-    total = float(np.sum(step_ms))
-    if dist is not None:
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = replicas.max_over_ranks(float(np.sum(step_ms)), dist)
     n_step = B.n_samples_total
-    value = world * n_step * args.steps / (total / 1e3)
+    value = replicas.job_throughput(n_step, args.steps, total, world)
     ms = total / args.steps
 
     # end to end: the same training run once more through the public API (a fresh batch built like
@@ -464,9 +458,7 @@ def run_batch(args, cfg, rank, world, local_rank):
         line["accuracy"] = batch_accuracy(B, cfg, args.accuracy_epochs, Ls)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
     if rank == 0:
         print(json.dumps(line))
 
@@ -492,21 +484,14 @@ def batch_accuracy(B, cfg, epochs, Ls):
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     from pyqusolver_b200 import _lib
+    from pyqusolver_b200 import replicas
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = replicas.init_group(world)
     ns_per_step = cfg["chains"] * cfg["samples"]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist)
 
     forms = {}
     tuned = None
@@ -517,7 +502,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         if form not in wanted:
             continue
         _lib.set_sr_impl(impl)
-        nqs, tdvp = build_nqs(cfg, seed=1234 + rank)
+        nqs, tdvp = build_nqs(cfg, seed=replicas.replica_seed(1234, rank))
         for _ in range(args.warmup):                        # the first call thermalises the chains
             timed_step(nqs, tdvp, cfg, [torch.cuda.Event(enable_timing=True) for _ in range(7)])
         torch.cuda.synchronize()
@@ -554,12 +539,12 @@ def run_ours(args, cfg, rank, world, local_rank):
     _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
     mixed = forms["mixed"]
     plain = forms.get("plain_fp32")
-    value = world * ns_per_step * args.steps / (mixed["total_ms"] / 1e3)
+    value = replicas.job_throughput(ns_per_step, args.steps, mixed["total_ms"], world)
     ms_step = mixed["total_ms"] / args.steps
     nqs, tdvp = mixed["nqs"], mixed["tdvp"]
 
     # --- end to end through the public API with host buffers (params in, stats + params out)
-    e2e = run_e2e(cfg, args, dist, world, seed=1234 + rank)
+    e2e = run_e2e(cfg, args, dist, world, seed=replicas.replica_seed(1234, rank))
 
     # --- roofline of the dominant kernel (measured live over the timed steps)
     roof = roofline(cfg, nqs, mixed)
@@ -594,7 +579,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         "e2e": e2e,
         "roofline": roof,
         "issue_rooflines": issue_rooflines(cfg, nqs, mixed, mixed["clocks"]),
-        "sr_tiling": ({"choice (mode, nc, ctas, pairs, fused_sv, ov_split)": tuned["choice"], "cg_iteration_ms": tuned["ms"],
+        "sr_tiling": ({"choice (mode, nc, ctas, pairs, fused_sv, ov_split, ovz)": tuned["choice"], "cg_iteration_ms": tuned["ms"],
                        "candidates_ms": tuned["timings"], "cached": tuned["cached"]} if tuned else "automatic"),
     }
     if tuned:
@@ -628,9 +613,7 @@ def run_ours(args, cfg, rank, world, local_rank):
         line["dense_sr"] = dense_summary(flush, names=[n.strip() for n in args.dense_configs.split(",") if n.strip()])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, budget_s=args.cpu_budget)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
     if rank == 0:
         print(json.dumps(line))
 
@@ -809,13 +792,11 @@ def run_e2e(cfg, args, dist, world, seed):
         if k >= args.warmup:
             times.append(s.elapsed_time(e))
         host_in, host_out = host_out, host_in                  # the next step starts from them
-    total = float(np.sum(times))
-    if dist is not None:
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    from pyqusolver_b200 import replicas
+    total = replicas.max_over_ranks(float(np.sum(times)), dist)
     nbytes = host_in.numel() * host_in.element_size()
-    return {"value": world * cfg["chains"] * cfg["samples"] * args.steps / (total / 1e3), "unit": "samples/s",
+    return {"value": replicas.job_throughput(cfg["chains"] * cfg["samples"], args.steps, total, world),
+            "unit": "samples/s",
             "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes + 32),
             "ms_per_step": total / args.steps}
 

@@ -296,6 +296,10 @@ typedef struct {
                                   MinSR and the batched CG take QES_PRECOND_NONE.
                                   Replaces the 'jacobi' pre_solver / sr_precond of
                                   QES/NQS/src/tdvp.py:332,686-710.                    */
+    int skip_true_residual;    /* nonzero: the CG / MINRES solve does not recompute
+                                  ||F - (S + shift) x|| / ||F|| after it ends (one
+                                  matvec and a host read fewer; result->true_residual
+                                  = -1).  0 (a zero-initialised struct): computed.   */
 } qes_sr_options;
 
 #define QES_PRECOND_NONE 0
@@ -335,9 +339,10 @@ int qes_set_sr_impl(int impl);
 int qes_sr_uses_tensor_cores(int dtype, int ns, int nh, int64_t n_samples, int* uses);
 /* Tiling of the tensor-core path for these shapes (for roofline accounting):
  * out = [uses, big, KC, n_chunks, nsplit, n_tiles, Kd, NB, Np, MT, NC, NR,
- * nnc, SPC, ov_stages, cl, sv, sv_grid] (first n_out entries); cl = 2 when
- * the O^H u CTAs run as pairs that add their partials on chip; sv = 1 when
- * the matvec runs as the fused S v kernel of sv_grid CTAs (one partial each). */
+ * nnc, SPC, ov_stages, cl, sv, sv_grid, ovz] (first n_out entries); cl = 2
+ * when the O^H u CTAs run as pairs that add their partials on chip; sv = 1
+ * when the matvec runs as the fused S v kernel of sv_grid CTAs (one partial
+ * each); ovz = 1 when O v runs through z = Sigma V (qes_sr_set_ovz).       */
 int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int32_t* out, int n_out);
 /* Tiling of the tensor-core O^H u in this process: mode 0 = automatic (the
  * single-M-tile kernel when the shapes allow it), 1 = single-M-tile kernel
@@ -368,6 +373,17 @@ int qes_sr_set_fused_sv(int on);
  * float32 summation order.  Takes the fused S v kernel out of the plan
  * (it reads the single-product operand).                                  */
 int qes_sr_set_ov_split(int on);
+/* O v through z = Sigma V (1, the default where the operands fit: NZ = 2 Mp
+ * (complex) or Mp (real) hidden-unit rows <= 512 and 128 x Kz spins plus the
+ * whole NZ x Kz direction operand within shared memory, Kz = sites + 1 padded
+ * to 16): A = the +-1 spins and a ones column (exact in BF16), B = the
+ * direction's W block and v_b (BF16 hi + lo), so the MMAs yield
+ * z_s = sigma_s^T V + v_b for every hidden unit; the epilogue forms
+ * (O v)_s = sum_m t_sm z_sm + sigma_s . v_a with t in float32 read from
+ * tanh_theta itself.  0: the product over the hidden axis (T as A in hi/lo
+ * against V').  Same operator; the hi/lo split touches v only.  Takes the
+ * fused S v kernel and the split-complex product out of the plan.          */
+int qes_sr_set_ovz(int on);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);
@@ -377,6 +393,26 @@ int qes_set_cg_graphs(int enable);
  * parameter vectors up to a few thousand entries, where launch latency
  * dominates), 0 = never (three kernels).                                   */
 int qes_set_cg_fused(int mode);
+/* CG steps in the Chronopoulos-Gear form on the kernel-chain path (1; for
+ * the unpreconditioned CG): the matvec is applied to r_k, its
+ * split reduction also sums |r_k|^2 with r_k^H A r_k, and its last block
+ * forms beta_k = |r_k|^2 / |r_{k-1}|^2, alpha_k = |r_k|^2 / (r_k^H A r_k -
+ * beta_k |r_k|^2 / alpha_{k-1}) and the convergence test on |r_k|^2; one
+ * kernel then updates p, s = A p (by recurrence), x and r: one grid-wide
+ * reduction and one kernel per step fewer than the standard form (0, the
+ * default: the matvec of p, then the x/r update with its |r|^2 reduction,
+ * then the p update).  The same Krylov iterates in exact arithmetic and the
+ * same stopping rule on the residual vector's norm (Chronopoulos and Gear,
+ * J. Comput. Appl. Math. 25 (1989)); p^H A p is formed from the vectors
+ * (bilinear in the recurrences), not from orthogonality.  Measured on B200:
+ * 10x10 Heisenberg CG iteration 43.3 -> 40.3 us at the same iteration count,
+ * but the recurrence of s carries the float32 / BF16-split operator's
+ * rounding forward, and a strongly rank-deficient system (20x20 TFIM, 256
+ * samples, 642,000 parameters) did not converge where the standard form
+ * does, so it is off by default.  With the Jacobi preconditioner and in the
+ * fused cooperative vector kernel (qes_set_cg_fused) the standard form
+ * runs.                                                                    */
+int qes_set_cg_single_reduction(int on);
 /* Test hook of the fused CG kernel's grid barriers (no reference
  * counterpart): (1, polls) makes every barrier wait for one arrival that
  * never comes and give up after `polls` polls, so a solve returns

@@ -74,6 +74,7 @@ class SROptions(C.Structure):
     _fields_ = [
         ("shift", C.c_double), ("rtol", C.c_double), ("atol", C.c_double), ("maxiter", C.c_int),
         ("check_every", C.c_int), ("rhs_prefactor", C.c_double), ("precond", C.c_int),
+        ("skip_true_residual", C.c_int),
     ]
 
 
@@ -125,8 +126,10 @@ SIGNATURES = {
     "qes_sr_set_ohu_pairs": [C.c_int],
     "qes_sr_set_fused_sv": [C.c_int],
     "qes_sr_set_ov_split": [C.c_int],
+    "qes_sr_set_ovz": [C.c_int],
     "qes_set_cg_graphs": [C.c_int],
     "qes_set_cg_fused": [C.c_int],
+    "qes_set_cg_single_reduction": [C.c_int],
     "qes_sr_set_barrier_test": [C.c_uint, C.c_uint],
     "qes_rbm_forward_tc_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],
     "qes_rbm_forward_tc": [C.c_int, C.c_int, C.c_int, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp],
@@ -234,7 +237,7 @@ def sr_impl() -> int:
 
 
 TC_PLAN_FIELDS = ("uses", "big", "KC", "n_chunks", "nsplit", "n_tiles", "Kd", "NB", "Np", "MT", "NC", "NR", "nnc",
-                  "SPC", "ov_stages", "cl", "sv", "sv_grid")
+                  "SPC", "ov_stages", "cl", "sv", "sv_grid", "ovz")
 
 
 def sr_tc_plan(dtype_code: int, ns: int, nh: int, n_samples: int) -> dict:

@@ -32,27 +32,29 @@ def _cache_path(cache=None):
 
 
 def _candidates(ns, nh, cplx):
-    # (mode, nc, ctas, pairs, fused S v, split-complex O v): automatic (the kernel pair), the pair with
-    # the split-complex O v, the fused kernel (single product), O^H u in CTA pairs, then the M/N-tiled
-    # O^H u; the split flag matters for complex networks only
+    # (mode, nc, ctas, pairs, fused S v, split-complex O v, O v through z = Sigma V): automatic with
+    # the z-form O v, the same with O^H u in CTA pairs, the product over the hidden axis (T as A), its
+    # split-complex variant, the fused kernel, then the M/N-tiled O^H u with the z-form O v; the
+    # split flag matters for complex networks only
     splits = (0, 1) if cplx else (0,)
-    out = [(0, 0, 0, 0, 0, sp) for sp in splits] + [(0, 0, 0, 0, 1, 0), (0, 0, 0, 1, 0, 0)]
+    out = [(0, 0, 0, 0, 0, 0, 1), (0, 0, 0, 1, 0, 0, 1)]
+    out += [(0, 0, 0, 0, 0, sp, 0) for sp in splits] + [(0, 0, 0, 0, 1, 0, 0)]
     for nc in (256, 208, 128, 96, 64, 32):
         if nc > ((nh + 15) // 16) * 16:
             continue
         for ctas in (148, 296, 592):
-            out.append((2, nc, ctas, 0, 0, 0))
+            out.append((2, nc, ctas, 0, 0, 0, 1))
     return out
 
 
 def tune_sr_tiling(net, bits, tanh_theta, *, repeats=3, iters=24, cache=None, candidates=None):
     """Time a CG iteration on (net, bits, tanh_theta) under each tiling candidate (mode, nc, ctas, pairs,
-    sv, split); apply and return the fastest as a dict with the per-iteration times in ms.  A cached choice for
+    sv, split, ovz); apply and return the fastest as a dict with the per-iteration times in ms.  A cached choice for
     the same device and shapes is applied without timing."""
     dc = dv.dtype_code(net.flat)
     n = int(bits.shape[0])
     dev = torch.cuda.get_device_name(bits.device)
-    key = f"sr_cg_iter6|{dev}|{dc}|{net.ns}|{net.nh}|{n}"
+    key = f"sr_cg_iter7|{dev}|{dc}|{net.ns}|{net.nh}|{n}"
     path = _cache_path(cache)
     table = {}
     try:
@@ -102,9 +104,9 @@ def tune_sr_tiling(net, bits, tanh_theta, *, repeats=3, iters=24, cache=None, ca
             if t < best_t:
                 best, best_t = cand, t
     finally:
-        apply_tiling(*(best or (0, 0, 0, 0, 0, 0)))
+        apply_tiling(*(best or DEFAULT_TILING))
     if best is None:
-        return {"choice": (0, 0, 0, 0, 0, 0), "ms": None, "timings": timings, "cached": False}
+        return {"choice": DEFAULT_TILING, "ms": None, "timings": timings, "cached": False}
     entry = {"choice": list(best), "ms": best_t, "timings": timings}
     table[key] = entry
     try:
@@ -118,8 +120,12 @@ def tune_sr_tiling(net, bits, tanh_theta, *, repeats=3, iters=24, cache=None, ca
     return dict(entry, cached=False)
 
 
-def apply_tiling(mode, nc, ctas, pairs, sv=0, split=0):
+DEFAULT_TILING = (0, 0, 0, 0, 0, 0, 1)
+
+
+def apply_tiling(mode, nc, ctas, pairs, sv=0, split=0, ovz=1):
     _lib.call("qes_sr_set_tiling", int(mode), int(nc), int(ctas))
     _lib.call("qes_sr_set_ohu_pairs", int(pairs))
     _lib.call("qes_sr_set_fused_sv", int(sv))
     _lib.call("qes_sr_set_ov_split", int(split))
+    _lib.call("qes_sr_set_ovz", int(ovz))

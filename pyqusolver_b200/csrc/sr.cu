@@ -401,7 +401,9 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
                                                                       double* __restrict__ dot_part,
                                                                       double* __restrict__ scal,
                                                                       unsigned int* __restrict__ counter,
-                                                                      const double* __restrict__ cg_done) {
+                                                                      const double* __restrict__ cg_done,
+                                                                      const V* __restrict__ pold,
+                                                                      const V* __restrict__ sold) {
   constexpr int E = VEC ? (int)(16 / sizeof(T)) : 1;      // columns per vector
   __shared__ V red[RS_THREADS * E];                        // [split group][column vector][E]
   pdl_trigger();
@@ -410,7 +412,11 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
   const int tid = threadIdx.x;
   const int groups = RS_THREADS / cv, c = tid % cv, sg = tid / cv;
   const int64_t nvec = P / E;                              // P % E == 0 when VEC
-  double d = 0.0;
+  // dd[0] = Re v^H y; with pold / sold (a Chronopoulos-Gear CG step: v = r_k, y = A r_k, the previous
+  // direction p_{k-1} and s_{k-1} = A p_{k-1}): dd[1] = |v|^2, dd[2] = Re v^H s_{k-1},
+  // dd[3] = Re p_{k-1}^H y, dd[4] = Re p_{k-1}^H s_{k-1}
+  const bool cgmode = pold != nullptr;
+  double dd[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t v0 = (int64_t)blockIdx.x * cv; v0 < nvec; v0 += (int64_t)gridDim.x * cv) {
     const int64_t vi = v0 + c;
     V g[E];
@@ -453,7 +459,14 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
         if (p) {
           const V pk = p[kk];
           t = vadd(t, vscale(shift, pk));
-          d += vdotc(pk, t);
+          dd[0] += vdotc(pk, t);
+          if (cgmode) {
+            const V po = pold[kk], so = sold[kk];
+            dd[1] += vdotc(pk, pk);
+            dd[2] += vdotc(pk, so);
+            dd[3] += vdotc(po, t);
+            dd[4] += vdotc(po, so);
+          }
         }
         y[kk] = t;
       }
@@ -461,15 +474,21 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
     __syncthreads();
   }
   if (!dot_part) return;
-  __shared__ double sred[RS_THREADS / 32];
+  // dot partials: dd[q] of block b at dot_part[q * RS_MAX_BLOCKS + b]
+  const int nd = cgmode ? 5 : 1;
+  __shared__ double sred[5][RS_THREADS / 32];
   __shared__ bool last;
-  d = warp_sum(d);
-  if ((tid & 31) == 0) sred[tid >> 5] = d;
+  for (int q = 0; q < nd; ++q) {
+    const double v = warp_sum(dd[q]);
+    if ((tid & 31) == 0) sred[q][tid >> 5] = v;
+  }
   __syncthreads();
   if (tid == 0) {
-    double s = 0.0;
-    for (int q = 0; q < RS_THREADS / 32; ++q) s += sred[q];
-    dot_part[blockIdx.x] = s;
+    for (int q = 0; q < nd; ++q) {
+      double s = 0.0;
+      for (int w = 0; w < RS_THREADS / 32; ++w) s += sred[q][w];
+      dot_part[q * RS_MAX_BLOCKS + blockIdx.x] = s;
+    }
     // the last block to finish sums the dot partials: pAp and alpha = rr / pAp
     if (scal) {
       __threadfence();
@@ -480,17 +499,44 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
   __syncthreads();
   if (!last) return;
   __threadfence();
-  double v = 0.0;
-  for (int q = tid; q < (int)gridDim.x; q += RS_THREADS) v += ((volatile double*)dot_part)[q];
-  v = warp_sum(v);
-  __syncthreads();
-  if ((tid & 31) == 0) sred[tid >> 5] = v;
+  for (int q = 0; q < nd; ++q) {
+    double v = 0.0;
+    for (int b = tid; b < (int)gridDim.x; b += RS_THREADS) v += ((volatile double*)dot_part)[q * RS_MAX_BLOCKS + b];
+    v = warp_sum(v);
+    __syncthreads();
+    if ((tid & 31) == 0) sred[q][tid >> 5] = v;
+  }
   __syncthreads();
   if (tid == 0) {
-    double pap = 0.0;
-    for (int q = 0; q < RS_THREADS / 32; ++q) pap += sred[q];
-    scal[1] = pap;
-    scal[7] = (scal[4] == 0.0 && pap > 0.0) ? scal[0] / pap : 0.0;
+    double tot[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int q = 0; q < nd; ++q)
+      for (int w = 0; w < RS_THREADS / 32; ++w) tot[q] += sred[q][w];
+    if (!cgmode) {
+      const double pap = tot[0];
+      scal[1] = pap;
+      scal[7] = (scal[4] == 0.0 && pap > 0.0) ? scal[0] / pap : 0.0;
+    } else if (scal[4] == 0.0) {
+      // Chronopoulos-Gear step k on r_k (v = r_k, y = A r_k): rr = |r_k|^2 from the vector itself,
+      // the convergence test on it (x_k is final: this step's update is skipped), else
+      // beta_k = rr / rr_{k-1} and alpha_k = rr / p_k^H A p_k with p_k^H A p_k expanded bilinearly
+      // in p_k = r_k + beta p_{k-1}, s_k = A r_k + beta s_{k-1} (the update kernel's recurrences):
+      // r^H A r + beta (Re r^H s_{k-1} + Re p_{k-1}^H A r) + beta^2 Re p_{k-1}^H s_{k-1}, from the
+      // vectors themselves rather than from the orthogonality relations of exact arithmetic
+      const double rw = tot[0], rr = tot[1];
+      scal[2] = rr;
+      if (rr <= scal[3]) {
+        scal[4] = 1.0;
+      } else {
+        const bool first = scal[5] == 0.0;
+        const double beta = (first || scal[0] <= 0.0) ? 0.0 : rr / scal[0];
+        const double den = first ? rw : rw + beta * (tot[2] + tot[3]) + beta * beta * tot[4];
+        scal[1] = den;                                   // p_k^H A p_k
+        scal[7] = den > 0.0 ? rr / den : 0.0;
+        scal[8] = beta;
+        scal[0] = rr;
+        scal[5] += 1.0;
+      }
+    }
     *counter = 0u;
   }
 }
@@ -500,7 +546,8 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
 template <class T, class V>
 static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, double shift, const V* p, V* y,
                                 double* dot_part, double* scal, unsigned int* counter, cudaStream_t st,
-                                const double* cg_done = nullptr) {
+                                const double* cg_done = nullptr, const V* pold = nullptr,
+                                const V* sold = nullptr) {
   constexpr int EV = (int)(16 / sizeof(T));
   const bool vec = !IsF64<T>::value && (P % EV == 0) && ((reinterpret_cast<uintptr_t>(partial) & 15) == 0);
   const int64_t nvec = vec ? P / EV : P;
@@ -514,12 +561,14 @@ static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, doub
   if constexpr (!IsF64<T>::value) {
     if (vec) {
       QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, true>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
-                                    (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done));
+                                    (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done,
+                                    pold, sold));
       return QES_OK;
     }
   }
     QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
-                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done));
+                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done,
+                                  pold, sold));
   return QES_OK;
 }
 
@@ -652,6 +701,44 @@ __global__ void __launch_bounds__(RED_THREADS) cg_p_kernel(int64_t P, const V* _
   }
 }
 
+// Chronopoulos-Gear CG step k, second half (one reduction per step: the split reduction of A r_k
+// also sums |r_k|^2 and its last block forms alpha_k, beta_k and the convergence test):
+//   p_k = r_k + beta_k p_{k-1},  s_k = A r_k + beta_k s_{k-1}  (= A p_k),
+//   x_{k+1} = x_k + alpha_k p_k,  r_{k+1} = r_k - alpha_k s_k,
+// and the tensor-core operand tiles of r_{k+1}, the next matvec input (Chronopoulos and Gear,
+// J. Comput. Appl. Math. 25 (1989) 153-168).  beta_0 = 0: p_0 = r_0 and s_0 = A r_0 exactly.
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) cg_cgstep_kernel(int64_t P, const V* __restrict__ Ar,
+                                                                V* __restrict__ x, V* __restrict__ r,
+                                                                V* __restrict__ p, V* __restrict__ sv,
+                                                                const double* __restrict__ scal, TcDims td,
+                                                                uint16_t* __restrict__ vp) {
+  pdl_trigger();
+  pdl_wait();                                              // A r_k, alpha_k, beta_k: previous kernel
+  if (scal[4] != 0.0) return;                              // converged: x is final
+  const double alpha = scal[7], beta = scal[8];
+  const int ns = td.ns, nh = td.nh;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < P; k += (int64_t)gridDim.x * blockDim.x) {
+    const V rk = r[k], wk = Ar[k];
+    const V pk = beta != 0.0 ? vadd(rk, vscale(beta, p[k])) : rk;
+    const V sk = beta != 0.0 ? vadd(wk, vscale(beta, sv[k])) : wk;
+    p[k] = pk;
+    sv[k] = sk;
+    x[k] = vadd(x[k], vscale(alpha, pk));
+    const V rn = vadd(rk, vscale(-alpha, sk));
+    r[k] = rn;
+    if (vp && k >= ns) {
+      const int64_t q = k - ns;
+      if (q < nh) {
+        tc_put_vp_elem(td, vp, ns, (int)q, rn);                          // v_b row
+      } else {
+        const uint32_t qw = (uint32_t)(q - nh);                          // ns * nh < 2^32 on this path
+        tc_put_vp_elem(td, vp, (int)(qw / (uint32_t)nh), (int)(qw % (uint32_t)nh), rn);
+      }
+    }
+  }
+}
+
 // grid of the per-iteration vector kernels: one element per thread up to RED_BLOCKS blocks (fewer
 // blocks, fewer tickets on the last-block counter for small parameter vectors)
 static int vec_blocks(int64_t n) {
@@ -779,6 +866,7 @@ __global__ void __launch_bounds__(SC_THREADS) cg_setup_kernel(int n, const doubl
   scal[2] = rr0;
   scal[7] = 0.0;
   scal[8] = 0.0;
+  scal[9] = 0.0;
 }
 
 template <class V>
@@ -1227,7 +1315,7 @@ static SRWork sr_layout(int dtype, int ns, int nh, int64_t n_samples, char* base
   L.wmean = (double*)take(4 * sizeof(double));
   L.partial = take((size_t)std::max<int64_t>(nsplit_max, 1) * P * (L.fp64 ? vs : ts));
   L.x = take(P * vs); L.r = take(P * vs); L.p = take(P * vs); L.Ap = take(P * vs); L.b = take(P * vs);
-  L.parts = (double*)take(std::max(RED_BLOCKS, RS_MAX_BLOCKS) * sizeof(double));
+  L.parts = (double*)take(5 * std::max(RED_BLOCKS, RS_MAX_BLOCKS) * sizeof(double));
   L.scal = (double*)take(16 * sizeof(double));
   L.dinv = (double*)take(P * sizeof(double));
   L.mr2 = take(P * vs); L.mw1 = take(P * vs); L.mw2 = take(P * vs);
@@ -1284,7 +1372,8 @@ static int launch_ohu_plain(int ns, int nh, int64_t n_samples, const uint32_t* b
 template <class T, class V>
 static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, const float2* w,
                      const double* wmean, double scale, const SRWork& L, double shift, const V* p, V* y,
-                     double* dot_part, cudaStream_t st, const double* cg_done = nullptr) {
+                     double* dot_part, cudaStream_t st, const double* cg_done = nullptr, const V* pold = nullptr,
+                     const V* sold = nullptr) {
   const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
   const int64_t nsplit = (n_samples + PT_SPLIT - 1) / PT_SPLIT;
   const double2* w64 = (L.fp64 && w == L.w) ? L.w64 : nullptr;     // the form's own O v
@@ -1294,10 +1383,10 @@ static int apply_ohu(int ns, int nh, int64_t n_samples, const uint32_t* bits, co
   const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
   if (L.fp64) {
     if (int rc_ = launch_reduce_splits<V, V>(P, (int)nsplit, L.partial, shift, p, y,
-        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done, pold, sold)) return rc_;
   } else {
     if (int rc_ = launch_reduce_splits<T, V>(P, (int)nsplit, L.partial, shift, p, y,
-        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done, pold, sold)) return rc_;
   }
   QES_LAUNCH_CHECK();
   qes_prof_end(pfr, st);
@@ -1372,9 +1461,10 @@ extern "C" int qes_sr_tc_plan(int dtype, int ns, int nh, int64_t n_samples, int3
   QES_ARG_CHECK(dtype == QES_DTYPE_F32 || dtype == QES_DTYPE_C64, "qes_sr_tc_plan: bad dtype");
   const SRWork L = sr_layout(dtype, ns, nh, n_samples, nullptr);
   const TcDims& d = L.td;
-  const int32_t f[18] = {L.tc ? 1 : 0, d.big ? 1 : 0, d.KC, d.n_chunks, d.nsplit, d.n_tiles, d.Kd, d.NB, d.Np,
-                         d.MT, d.NC, d.NR, d.nnc, d.SPC, d.ov_stages, d.cl, d.sv ? 1 : 0, d.sv ? d.sv_grid : 0};
-  for (int k = 0; k < n_out; ++k) out[k] = k < 18 ? f[k] : 0;
+  const int32_t f[19] = {L.tc ? 1 : 0, d.big ? 1 : 0, d.KC, d.n_chunks, d.nsplit, d.n_tiles, d.Kd, d.NB, d.Np,
+                         d.MT, d.NC, d.NR, d.nnc, d.SPC, d.ov_stages, d.cl, d.sv ? 1 : 0, d.sv ? d.sv_grid : 0,
+                         d.ovz ? 1 : 0};
+  for (int k = 0; k < n_out; ++k) out[k] = k < 19 ? f[k] : 0;
   return QES_OK;
 }
 
@@ -1425,7 +1515,8 @@ static std::atomic<unsigned int> g_bar_limit{kGridBarLimit};
 template <class T>
 static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, const T* tt, double shift,
                        const typename VecT<T>::type* v, typename VecT<T>::type* y, double* dot_part, const SRWork& L,
-                       cudaStream_t st, bool vp_ready = false, const double* cg_done = nullptr) {
+                       cudaStream_t st, bool vp_ready = false, const double* cg_done = nullptr,
+                       const typename VecT<T>::type* pold = nullptr, const typename VecT<T>::type* sold = nullptr) {
   using V = typename VecT<T>::type;
   if (L.tc) {
     const int dtype = ScalarTraits<T>::is_complex ? QES_DTYPE_C64 : QES_DTYPE_F32;
@@ -1435,7 +1526,7 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
     const int64_t P = (int64_t)ns + nh + (int64_t)ns * nh;
     const int pfr = qes_prof_begin(QES_PROF_REDUCE, st);
     if (int rc_ = launch_reduce_splits<T, V>(P, L.mv_nsplit, L.partial, shift, v, y,
-        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done)) return rc_;
+        dot_part, dot_part ? L.scal : nullptr, L.counter, st, cg_done, pold, sold)) return rc_;
     QES_LAUNCH_CHECK();
     qes_prof_end(pfr, st);
     return QES_OK;
@@ -1443,7 +1534,7 @@ static int sr_matvec_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
   int rc = apply_ov<T, V>(ns, nh, n_samples, bits, tt, v, L.w, L.wmean, L, st, cg_done);
   if (rc) return rc;
   return apply_ohu<T, V>(ns, nh, n_samples, bits, tt, L.w, L.wmean, 1.0 / (double)n_samples, L, shift, v, y,
-                         dot_part, st, cg_done);
+                         dot_part, st, cg_done, pold, sold);
 }
 
 // per-step operands of the tensor-core path (spins as BF16 tiles) and the status word
@@ -1576,7 +1667,13 @@ void l2_window(cudaStream_t st, int dev, const void* base, size_t bytes) {
 // The loop condition of the device-driven CG: one more chunk while the solve has not converged,
 // no bounded wait has given up, and fewer than max_chunks chunks have run.  The counter makes the
 // loop finite whatever the other kernels do.
-__global__ void cg_loop_reset_kernel(unsigned int* count) { *count = 0u; }
+// entry of the device loop: no chunk when the solve has already converged (or a wait gave up)
+__global__ void cg_loop_reset_kernel(unsigned int* count, cudaGraphConditionalHandle h, const double* __restrict__ scal,
+                                     const int* __restrict__ status, const int* __restrict__ bar_err) {
+  *count = 0u;
+  const bool run = scal[4] == 0.0 && (status == nullptr || *status == 0) && *bar_err == 0;
+  cudaGraphSetConditional(h, run ? 1u : 0u);
+}
 __global__ void cg_loop_cond_kernel(cudaGraphConditionalHandle h, const double* __restrict__ scal,
                                     unsigned int* __restrict__ count, unsigned int max_chunks,
                                     const int* __restrict__ status, const int* __restrict__ bar_err) {
@@ -1601,6 +1698,17 @@ extern "C" int qes_sr_set_barrier_test(unsigned int extra_arrivals, unsigned int
   return QES_OK;
 }
 
+// Chronopoulos-Gear CG steps (the matvec of r, one reduction, one update kernel) on the kernel-chain
+// path: off by default -- one kernel and one grid-wide reduction fewer per step (heis10x10 CG
+// iteration 43.3 -> 40.3 us, the same 136 iterations), but the s = A p recurrence does not damp the
+// rounding of a float32 / BF16-split operator, and on strongly rank-deficient systems (20x20 TFIM,
+// 256 samples, P = 642,000, shift 1e-4) it failed to converge within 3,000 steps where the
+// standard form converges
+static std::atomic<int> g_cg_single{0};
+extern "C" int qes_set_cg_single_reduction(int on) {
+  g_cg_single.store(on ? 1 : 0);
+  return QES_OK;
+}
 extern "C" int qes_set_cg_fused(int mode) {
   if (mode < 0 || mode > 2) {
     qes_set_last_message("qes_set_cg_fused: mode 0 (off), 1 (automatic) or 2 (always)");
@@ -1670,8 +1778,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   // b = F
   rc = sr_force_t<T>(ns, nh, n_samples, bits, tt, eloc, b, L, st);
   if (rc) return rc;
-  double emean[2] = {0, 0};
-  QES_CUDA_CHECK(cudaMemcpyAsync(emean, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  // the energy mean stays on the device (scal[12..13]) until the final read of the solver state
+  QES_CUDA_CHECK(cudaMemcpyAsync(L.scal + 12, L.wmean, 2 * sizeof(double), cudaMemcpyDeviceToDevice, st));
   QES_CUDA_CHECK(cudaMemsetAsync(L.counter, 0, 128 * sizeof(unsigned int), st));
   // preconditioned CG (SciPy's cg with M = D^-1): z = D^-1 r in the direction update, rho = r^H z
   const double* dinv = nullptr;
@@ -1709,12 +1817,11 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     QES_LAUNCH_CHECK();
   }
   const int check = opt->check_every > 0 ? opt->check_every : 8;
-  double hs[8] = {0};
+  // No host read before the first chunk: a system that needs no iteration (||F|| <= atol) has its
+  // converged flag set by cg_setup_kernel, and every CG kernel then returns at once.
+  double hs[16] = {0};
   int it = 0;
   bool done = false;
-  QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
-  QES_CUDA_CHECK(cudaStreamSynchronize(st));
-  done = hs[4] != 0.0;
   // fused vector kernel (split reduction, x/r and direction updates with two grid barriers):
   // always (2), never (0), or automatically (1) for grids of up to 160 CTAs
   const int fused_mode = g_cg_fused.load();
@@ -1748,6 +1855,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     if (fused_mode == 1 && fused_grid > 160) fused = false;
   }
   const BarCfg bcfg{g_bar_extra.load(), g_bar_limit.load()};
+  const bool single = !fused && dinv == nullptr && g_cg_single.load() != 0;
   auto run_direct = [&](int nrun, int it0) -> int {
     for (int q = 0; q < nrun; ++q) {
       if (fused) {
@@ -1789,6 +1897,18 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
         QES_LAUNCH_CHECK();
         continue;
       }
+      if (single) {
+        // Chronopoulos-Gear step: the matvec of r, one reduction (r^H A r, |r|^2, alpha, beta,
+        // the convergence test), one update kernel
+        int r2 = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, r, Ap, L.parts, L, st,
+                                /*vp_ready=*/it0 + q > 0, L.scal + 4, (const V*)p, (const V*)L.mw1);
+        if (r2) return r2;
+        QES_CUDA_CHECK(qes_launch_pdl(cg_cgstep_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P,
+                                      (const V*)Ap, x, r, p, (V*)L.mw1, (const double*)L.scal, L.td,
+                                      L.tc ? L.tw.vp : (uint16_t*)nullptr));
+        QES_LAUNCH_CHECK();
+        continue;
+      }
       int r2 = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, p, Ap, L.parts, L, st,
                               /*vp_ready=*/it0 + q > 0, L.scal + 4);
       if (r2) return r2;
@@ -1820,6 +1940,12 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     if (!graphs || it == 0 || nrun != check) {
       rc = run_direct(nrun, it);
       if (rc) return rc;
+      // the first chunk goes on to the device loop without a host read: the loop checks the
+      // converged flag before its first chunk
+      if (it == 0 && graphs && g_cg_loop.load() != 0 && nrun == check && (opt->maxiter - nrun) / check >= 2) {
+        it += nrun;
+        continue;
+      }
     } else {
       std::lock_guard<std::mutex> lock(g_graph_mu);
       CgGraphSlot& gs = g_graph[dev];
@@ -1833,7 +1959,9 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       const CgGraphKey key{bits, tt, L.w, L.wts, n_samples, ns, nh, ScalarTraits<T>::is_complex ? 1 : 0, nrun,
                            L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0) | (dinv ? 4 : 0), L.td.big ? 1 : 0,
                            L.td.KC, L.mv_nsplit,
-                           L.td.nnc, L.td.NC, L.td.SPC, L.td.cl | (L.td.sv ? 4 : 0), (int)bcfg.extra, opt->shift};
+                           L.td.nnc, L.td.NC, L.td.SPC,
+                           L.td.cl | (L.td.sv ? 4 : 0) | (L.td.ovz ? 8 : 0) | (L.td.splitc ? 16 : 0) | (single ? 32 : 0),
+                           (int)bcfg.extra, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {
           cudaGraphExecDestroy(gs.exec);
@@ -1875,15 +2003,18 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
           bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
           cudaGraphNode_t n0 = nullptr, n1 = nullptr;
           cudaGraphConditionalHandle hnd = 0;
+          if (ok) ok = cudaGraphConditionalHandleCreate(&hnd, g, 0u, cudaGraphCondAssignDefault) == cudaSuccess;
           if (ok) {
-            void* kargs[] = {(void*)&lcount};
+            const double* scal_arg = L.scal;
+            const int* status_arg = L.tc ? L.tw.status : nullptr;
+            const int* barerr_arg = (const int*)(L.counter + 4);
+            void* kargs[] = {(void*)&lcount, (void*)&hnd, (void*)&scal_arg, (void*)&status_arg, (void*)&barerr_arg};
             cudaKernelNodeParams kp = {};
             kp.func = (void*)cg_loop_reset_kernel;
             kp.gridDim = dim3(1);
             kp.blockDim = dim3(1);
             kp.kernelParams = kargs;
-            ok = cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp) == cudaSuccess &&
-                 cudaGraphConditionalHandleCreate(&hnd, g, 1u, cudaGraphCondAssignDefault) == cudaSuccess;
+            ok = cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp) == cudaSuccess;
           }
           cudaGraph_t body = nullptr;
           if (ok) {
@@ -1957,10 +2088,10 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     if (loop_count) {
       unsigned int chunks = 0;
       QES_CUDA_CHECK(cudaMemcpyAsync(&chunks, loop_count, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
-      QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
       rc = sr_check_status(L, st, true);            // synchronises the stream
       if (rc) return rc;
-      if (chunks < 1 || chunks > loop_max) {
+      if (chunks > loop_max) {
         qes_set_last_message("SR CG: the device loop ran an impossible number of chunks");
         return QES_ERR_CUDA;
       }
@@ -1970,7 +2101,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       continue;
     }
     it += nrun;
-    QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
     rc = sr_check_status(L, st, true);          // synchronises the stream
     if (rc) return rc;
     done = hs[4] != 0.0;
@@ -1979,12 +2110,22 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     l2_window(st, dev, nullptr, 0);
     if (graphs && g_graph[dev].init) l2_window(g_graph[dev].cs, dev, nullptr, 0);
   }
-  // a bounded wait of the force pass must surface even when CG needed no iteration
+  // Chronopoulos-Gear steps test |r|^2 at the start of the next step: the residual of the last
+  // step before maxiter is tested here (|r|^2 into scal[2]; r does not change after convergence)
+  if (single) {
+    norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, r, L.parts);
+    sum_parts_kernel<<<1, SC_THREADS, 0, st>>>(RED_BLOCKS, L.parts, L.scal + 2);
+    QES_LAUNCH_CHECK_N(2);
+  }
+  // the final solver state (also when CG ran no chunk); a bounded wait of the force pass must
+  // surface even when CG needed no iteration
+  QES_CUDA_CHECK(cudaMemcpyAsync(hs, L.scal, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
   if ((rc = sr_check_status(L, st, true))) return rc;
+  done = hs[4] != 0.0 || (single && hs[2] <= hs[3]);
   // true residual of the solution, ||F - (S + shift) x|| / ||F||, with one more matvec: CG's recursive
   // residual drifts from it once the rounding of the float32 / BF16-split contractions dominates
   double true_rr = -1.0;
-  if (opt->maxiter > 0) {
+  if (opt->maxiter > 0 && !opt->skip_true_residual) {
     rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, x, Ap, nullptr, L, st, false);
     if (rc) return rc;
     diff_norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, Ap, L.parts);
@@ -2004,8 +2145,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
     res->converged = done ? 1 : 0;
     res->residual = sqrt(hs[2]);                         // ||r|| (scal[0] holds rho = r^H D^-1 r with PCG)
     res->rhs_norm = sqrt(hs[6]);
-    res->e_mean_re = emean[0];
-    res->e_mean_im = emean[1];
+    res->e_mean_re = hs[12];
+    res->e_mean_im = hs[13];
     res->true_residual = true_rr < 0.0 ? -1.0 : (hs[6] > 0.0 ? sqrt(true_rr / hs[6]) : 0.0);
     res->acond = -1.0;
   }
@@ -2094,7 +2235,7 @@ static int sr_minres_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, 
   double ms[16] = {0};
   QES_CUDA_CHECK(cudaMemcpyAsync(ms, L.mscal, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
   double true_rr = -1.0;
-  if (opt->maxiter > 0) {
+  if (opt->maxiter > 0 && !opt->skip_true_residual) {
     rc = sr_matvec_t<T>(ns, nh, n_samples, bits, tt, opt->shift, x, y, nullptr, L, st, false);
     if (rc) return rc;
     diff_norm2_kernel<V><<<RED_BLOCKS, RED_THREADS, 0, st>>>(P, b, y, L.parts);
@@ -2326,7 +2467,7 @@ static int sr_minsr_t(int ns, int nh, int64_t n, const uint32_t* bits, const T* 
     for (int q = 0; q < nrun; ++q) {
       if ((rc = minsr_ohu<T>(ns, nh, n, bits, tt, p, g, L, M, st))) return rc;       // g = O_c^H p
       if (L.tc) {                                                                     // w = O g
-        if ((rc = tc_ov(dtype, L.td, n, bits, g, L.w, L.tw, st))) return rc;
+        if ((rc = tc_ov(dtype, L.td, n, bits, tt, g, L.w, L.tw, st))) return rc;
       } else {
         if ((rc = apply_ov<T, V>(ns, nh, n, bits, tt, g, L.w, nullptr, L, st))) return rc;
       }

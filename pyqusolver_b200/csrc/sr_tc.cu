@@ -486,6 +486,286 @@ __global__ void __launch_bounds__(kThreads) tc_ov_kernel(TcDims d, int64_t n_sam
 }
 
 // ================================================================================================
+// ovz: O v through z = Sigma V.  A = [sigma_s | 1] (128 samples x Kz: sites, the ones column at
+// K index ns, zeros beyond), built by the CTA from the spin words, exact in BF16; B = Bz (hi/lo),
+// NZ rows x Kz, copied whole into shared memory with one mbarrier per 16-wide k-step.  The MMAs
+// give z_s = sigma_s^T V + v_b for every hidden unit (columns m: Re, Mp + m: Im) in TMEM, and the
+// epilogue forms (O v)_s = sum_m t_sm z_sm + sigma_s . v_a with t in float32, read from T transposed
+// per 128-sample tile once per step (t_tiles[tile][m][row]: the 32 rows of a warp are 32 consecutive
+// elements).  Against tc_ov_kernel: K is the sites (Kz = 112 for 100 sites) instead of the hidden
+// axis (2 Mp = 416 complex), and only B is split, so a tile takes two MMAs per k-step instead of
+// three per K column pair.
+// ================================================================================================
+// T per 128-sample tile, transposed: out[tile][m][r] = T[tile * 128 + r][m] (rows beyond Ns: 0).
+// Block (32 x 8) moves a 32 x 32 (rows x units) square through shared memory.
+template <class T>
+__global__ void tc_t_tiles_kernel(int nh, int64_t n_samples, int n_tiles, const T* __restrict__ tt,
+                                  T* __restrict__ out) {
+  __shared__ T sq[32][33];
+  const int mb = (nh + 31) / 32;
+  const int64_t squares = (int64_t)n_tiles * 4 * mb;
+  for (int64_t q = blockIdx.x; q < squares; q += gridDim.x) {
+    const int m0 = 32 * (int)(q % mb);
+    const int64_t rq = q / mb;                             // 32-row block of the whole sample range
+    const int64_t r0 = 32 * rq;
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += 8) {
+      const int64_t s = r0 + i;
+      const int m = m0 + threadIdx.x;
+      sq[i][threadIdx.x] = (s < n_samples && m < nh) ? tt[s * nh + m] : ScalarTraits<T>::zero();
+    }
+    __syncthreads();
+    const int64_t tile = rq >> 2;
+    const int rr = (int)(rq & 3) * 32 + threadIdx.x;      // row within the tile
+    for (int j = threadIdx.y; j < 32; j += 8) {
+      const int m = m0 + j;
+      if (m < nh) out[((size_t)tile * nh + m) * 128 + rr] = sq[threadIdx.x][j];
+    }
+  }
+}
+
+// Bz operand from the direction vector v (v_a, v_b, W row-major [site][hidden unit]):
+// item (n, k8) writes the 8 K entries [8 k8, 8 k8 + 8) of row n, hi and lo
+template <class V>
+__global__ void tc_build_vz_kernel(TcDims d, bool cplx, const V* __restrict__ v, uint16_t* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();                                             // v comes from the previous kernel
+  const int ns = d.ns, nh = d.nh, Mp = d.Mp, NZ = d.NZ;
+  const V* vb = v + ns;
+  const V* vW = v + ns + nh;
+  const size_t tile_bytes = (size_t)NZ * 32;
+  const int items = NZ * (d.Kz / 8);
+  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
+    const int n = it % NZ, k8 = it / NZ;
+    const bool im = cplx && n >= Mp;
+    const int m = im ? n - Mp : n;
+    uint16_t h[8], l[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int k = 8 * k8 + q;                           // site (k == ns: v_b)
+      float x = 0.f;
+      if (m < nh && k <= ns) {
+        if (k < ns) x = im ? vim(vW, (int64_t)k * nh + m) : vre(vW, (int64_t)k * nh + m);
+        else x = im ? vim(vb, m) : vre(vb, m);
+      }
+      split_bf16(x, h[q], l[q]);
+    }
+    uint8_t* base = reinterpret_cast<uint8_t*>(out) + (size_t)(k8 >> 1) * 2 * tile_bytes;
+    const uint32_t off = umma::kmajor_offset(n, 8 * (k8 & 1), NZ);
+    *reinterpret_cast<uint4*>(base + off) = pack8(h);
+    *reinterpret_cast<uint4*>(base + tile_bytes + off) = pack8(l);
+  }
+}
+
+// t of 16 hidden units [m0, m0 + 16) of one sample row from the tile-transposed T (element (m, r)
+// at tcol[m * 128]: a warp's 32 rows read 32 consecutive elements), zero beyond nh
+template <class T>
+__device__ __forceinline__ void ovz_load16(const T* __restrict__ tcol, int m0, int nh, T (&t)[16]) {
+#pragma unroll
+  for (int q = 0; q < 16; ++q) t[q] = (m0 + q < nh) ? __ldg(tcol + (size_t)(m0 + q) * 128) : ScalarTraits<T>::zero();
+}
+__device__ __forceinline__ void ovz_dot16(const float2 (&t)[16], const float (&zr)[16], const float (&zi)[16],
+                                          float2& acc) {
+  float ar = 0.f, ai = 0.f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    ar = fmaf(t[q].x, zr[q], fmaf(-t[q].y, zi[q], ar));
+    ai = fmaf(t[q].x, zi[q], fmaf(t[q].y, zr[q], ai));
+  }
+  acc.x += ar;
+  acc.y += ai;
+}
+__device__ __forceinline__ void ovz_dot16(const float (&t)[16], const float (&zr)[16], const float (&)[16],
+                                          float2& acc) {
+  float a = 0.f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) a = fmaf(t[q], zr[q], a);
+  acc.x += a;
+}
+
+template <class T, class V>
+__global__ void __launch_bounds__(kThreads) tc_ovz_kernel(TcDims d, int64_t n_samples, const uint32_t* __restrict__ bits,
+                                                          const V* __restrict__ v, const T* __restrict__ t_tiles,
+                                                          const uint16_t* __restrict__ vz, float2* __restrict__ w_out,
+                                                          double2* __restrict__ wsum_part, int* __restrict__ status,
+                                                          const double* __restrict__ cg_done,
+                                                          const float* __restrict__ wts) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  constexpr bool CPLX = ScalarTraits<T>::is_complex;
+  const int ns = d.ns, nh = d.nh, Kz = d.Kz, NZ = d.NZ, Mp = d.Mp;
+  const int nks = Kz / 16;
+  const uint32_t a_bytes = 128u * Kz * 2u;
+  const uint32_t ks_bytes = 2u * NZ * 32u;                 // one k-step of Bz: hi and lo tiles
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + a_bytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sB + (size_t)nks * ks_bytes);
+  uint64_t* done = full + nks;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  T* s_va = reinterpret_cast<T*>(tslot + 4);
+  const int nw = n_words(ns);
+  // spin words of the tile, word-major ([word][row]) so that a warp reads consecutive rows
+  uint32_t* s_bits = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(s_va) +
+                                                 (((size_t)ns * sizeof(T) + 15) & ~(size_t)15));
+  __shared__ double2 red[4];
+  __shared__ float2 s_part[kColGroups][128];
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tile = blockIdx.x;
+  pdl_trigger();
+  if (cg_block_done(cg_done)) {         // converged CG: nothing issued yet, nothing to drain
+    pdl_wait();
+    return;
+  }
+  if (tid == 0) {
+    for (int c = 0; c < nks; ++c) umma::mbar_init(&full[c], 1);
+    umma::mbar_init(done, 1);
+    umma::fence_mbar_init();
+  }
+  // per-step inputs (older than the previous kernel): the tile's spin words, then A
+  const int64_t r0 = (int64_t)tile * 128;
+  const int rows = (n_samples - r0 < 128) ? (int)(n_samples - r0) : 128;
+  for (int q = tid; q < 128 * nw; q += kThreads) {
+    const int r = q / nw, w = q - r * nw;
+    s_bits[w * 128 + r] = (r < rows) ? bits[r0 * nw + q] : 0u;
+  }
+  __syncthreads();
+  for (int it = tid; it < 128 * (Kz / 8); it += kThreads) {
+    const int r = it & 127, k8 = it >> 7;
+    uint16_t a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int k = 8 * k8 + q;
+      uint16_t x = 0;
+      if (r < rows) {
+        if (k < ns) x = ((s_bits[(k >> 5) * 128 + r] >> (k & 31)) & 1u) ? 0x3F80u : 0xBF80u;
+        else if (k == ns) x = 0x3F80u;                    // the v_b column
+      }
+      a[q] = x;
+    }
+    *reinterpret_cast<uint4*>(sA + umma::kmajor_offset(r, 8 * k8, 128)) = pack8(a);
+  }
+  umma::fence_proxy_async_smem();       // A (generic-proxy stores) -> visible to the tensor core
+  pdl_wait();                           // Bz and v_a: written by the previous kernel
+  if (tid == 0) {
+    for (int c = 0; c < nks; ++c) {
+      umma::mbar_arrive_expect_tx(&full[c], ks_bytes);
+      umma::bulk_g2s(sB + (size_t)c * ks_bytes, reinterpret_cast<const uint8_t*>(vz) + (size_t)c * ks_bytes, ks_bytes,
+                     &full[c]);
+    }
+  }
+  for (int i = tid; i < ns; i += kThreads) {
+    if constexpr (CPLX) s_va[i] = make_float2(vre(v, i), vim(v, i));
+    else s_va[i] = vre(v, i);
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, d.ovz_tmem);
+    umma::tmem_relinquish();
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tbase = *tslot;
+
+  // epilogue rows: warp w reads lane quarter w % 4 (sample rows) and column group w / 4
+  const int quarter = warp & 3, cg = warp >> 2;
+  const int row = 32 * quarter + lane;
+  const int64_t s = r0 + row;
+  const bool sval = s < n_samples;
+  const T* tcol = t_tiles + (size_t)tile * nh * 128 + row;
+  const uint32_t* wrd = s_bits + row;                     // word w of this row at wrd[128 w]
+  float2 acc = make_float2(0.f, 0.f);
+  // sigma_s . v_a first (column group cg takes spin words cg, cg + 4, ...), while Bz is in flight
+  for (int w = cg; w < nw; w += kColGroups) {
+    const uint32_t word = wrd[128 * w];
+    const int i1 = (32 * w + 32 < ns) ? 32 * w + 32 : ns;
+    float sre = 0.f, sim = 0.f;
+    for (int i = 32 * w; i < i1; ++i) {
+      const int sgn = (int)((~word >> (i & 31)) & 1u) << 31;
+      const T va = s_va[i];
+      if constexpr (CPLX) {
+        sre += __int_as_float(__float_as_int(va.x) ^ sgn);
+        sim += __int_as_float(__float_as_int(va.y) ^ sgn);
+      } else {
+        sre += __int_as_float(__float_as_int(va) ^ sgn);
+      }
+    }
+    acc.x += sre;
+    acc.y += sim;
+  }
+  if (warp == 1) {
+    if (lane == 0) {
+      // D (128 x NZ) = A Bz_hi^T + A Bz_lo^T; NZ > 256 is issued as two N parts
+      const int n_parts = NZ > 256 ? 2 : 1;
+      const uint32_t np0 = NZ > 256 ? 256u : (uint32_t)NZ;
+      const uint32_t sa = umma::smem_u32(sA), sb = umma::smem_u32(sB);
+      for (int c = 0; c < nks; ++c) {
+        if (!umma::mbar_wait(&full[c], 0, kWaitLimit)) {
+          record_error(status, QES_ERR_TIMEOUT);
+          break;
+        }
+        umma::tc_fence_after();
+        const uint64_t ad = umma::smem_desc(sa + (uint32_t)c * 2u * 128u * 16u, 128u * 16u, 128u);
+        for (int pt = 0; pt < n_parts; ++pt) {
+          const uint32_t n0 = pt ? np0 : 0u, nn = pt ? (uint32_t)NZ - np0 : np0;
+          const uint32_t idesc = umma::idesc_bf16_f32(128, nn);
+          const uint32_t bh = sb + (uint32_t)c * ks_bytes + (n0 / 8u) * 128u;
+          const uint64_t dbh = umma::smem_desc(bh, (uint32_t)NZ * 16u, 128u);
+          const uint64_t dbl = umma::smem_desc(bh + (uint32_t)NZ * 32u, (uint32_t)NZ * 16u, 128u);
+          umma::mma_bf16(tbase + n0, ad, dbh, idesc, c > 0 ? 1u : 0u);
+          umma::mma_bf16(tbase + n0, ad, dbl, idesc, 1u);
+        }
+      }
+      umma::mma_commit(done);               // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+  }
+  // t of the first 16-unit chunk is loaded before the MMAs complete; each pass loads the next
+  const uint32_t lane_addr = tbase + ((uint32_t)(32 * quarter) << 16);
+  const int nch = (nh + 15) / 16;
+  T tcur[16];
+  if (cg < nch) ovz_load16(tcol, 16 * cg, nh, tcur);
+  if (!umma::mbar_wait(done, 0, kWaitLimit)) record_error(status, QES_ERR_TIMEOUT);
+  umma::tc_fence_after();
+  for (int c = cg; c < nch; c += kColGroups) {
+    T tnext[16];
+    if (c + kColGroups < nch) ovz_load16(tcol, 16 * (c + kColGroups), nh, tnext);
+    float zr[16], zi[16];
+    if constexpr (CPLX) umma::tmem_ld16x2(lane_addr + 16 * c, lane_addr + Mp + 16 * c, zr, zi);
+    else umma::tmem_ld16(lane_addr + 16 * c, zr);
+    ovz_dot16(tcur, zr, zi, acc);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) tcur[q] = tnext[q];
+  }
+  s_part[cg][row] = acc;
+  umma::tc_fence_before();
+  __syncthreads();
+  if (cg == 0) {
+    float2 wv = s_part[0][row];
+#pragma unroll
+    for (int g = 1; g < kColGroups; ++g) wv = wv + s_part[g][row];
+    if (!sval) wv = make_float2(0.f, 0.f);
+    if (sval) w_out[s] = wv;
+    const double wt = (wts && sval) ? (double)wts[s] : 1.0;          // weighted sum for the weighted mean
+    double2 ps = make_double2(wt * wv.x, wt * wv.y);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      ps.x += __shfl_xor_sync(0xffffffffu, ps.x, o);
+      ps.y += __shfl_xor_sync(0xffffffffu, ps.y, o);
+    }
+    if (lane == 0) red[quarter] = ps;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double2 t = make_double2(0.0, 0.0);
+    for (int q = 0; q < 4; ++q) { t.x += red[q].x; t.y += red[q].y; }
+    wsum_part[tile] = t;
+    // a k-step whose wait gave up may still be in flight: drain every copy (bounded) before exit
+    for (int c = 0; c < nks; ++c) umma::mbar_wait(&full[c], 0, kWaitLimit);
+  }
+  if (warp == 0) umma::tmem_dealloc(tbase, d.ovz_tmem);
+}
+
+// ================================================================================================
 // ohu: one CTA per KC-sample chunk; writes one P-vector of partial sums
 // ================================================================================================
 // CL = 2: the CTAs run in clusters of two (chunks 2c, 2c + 1); after staging, each adds its half
@@ -1618,6 +1898,12 @@ extern "C" int qes_sr_set_ov_split(int on) {
   g_ov_split.store(on ? 1 : 0);
   return QES_OK;
 }
+// O v through z = Sigma V (tc_ovz_kernel) where its operands fit: on by default
+static std::atomic<int> g_ovz{1};
+extern "C" int qes_sr_set_ovz(int on) {
+  g_ovz.store(on ? 1 : 0);
+  return QES_OK;
+}
 static std::atomic<int> g_ohu_pairs{0};      // measured slower on B200 (heis 10x10: 49.5 vs 46.2 us per CG iteration)
 // fused S v kernel where the tiling admits it: off by default (heis10x10 CG iteration 54.6 us with it,
 // 44.2 us with the O v / O^H u pair: its per-tile phases run one after another behind block barriers)
@@ -1681,6 +1967,17 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
   if (S < 2) return false;
   t.ov_stages = S;
   t.ov_smem = (int)(S * stage + ov_extra);
+  // ovz operands: A (128 x Kz) and the whole Bz (NZ x Kz, hi/lo) in shared memory, NZ TMEM columns
+  t.Kz = (ns + 1 + 15) / 16 * 16;
+  t.NZ = cplx ? 2 * t.Mp : t.Mp;
+  {
+    const size_t zsm = 128u * t.Kz * 2 + (size_t)t.Kz * t.NZ * 4 + 8u * (t.Kz / 16 + 1) + 16 +
+                       ((size_t)ns * tsz + 15) / 16 * 16 + 128u * 4u * ((ns + 31) / 32) + 64;
+    // an explicit request for the split-complex product or the fused S v kernel (both read V') wins
+    t.ovz = g_ovz.load() != 0 && !t.splitc && g_sv.load() == 0 && t.NZ <= 512 && zsm <= kTcSmemLimit;
+    t.ovz_smem = (int)zsm;
+    t.ovz_tmem = pow2_at_least(std::max(t.NZ, 32));
+  }
   t.n_tiles = (int)((n_samples + 127) / 128);
   t.big = ns > 127 || t.Mp > 256 || t.NB > 256;
   const int mode = g_tile_mode.load();
@@ -1710,7 +2007,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
     t.ohu_smem = (int)(128u * kc * 2 + 2u * t.Np * kc * 2 + (size_t)(kc + nh + ns) * tsz + 64);
     // fused S v: the shared region holds the O v pipeline, later Sigma^T and two Q^T buffers; one CTA
     // per SM at most (launch bounds cap the registers at 128 per thread), so sv_grid CTAs are resident
-    if (g_sv.load() != 0 && !t.splitc) {          // the fused kernel reads the [Re | -Im ; Im | Re] V'
+    if (g_sv.load() != 0 && !t.splitc && !t.ovz) {          // the fused kernel reads the [Re | -Im ; Im | Re] V'
       const int nsp = (ns + 1) & ~1, nw = (ns + 31) / 32;
       for (int S2 = 4; S2 >= 2 && !t.sv; --S2) {
         const size_t region = std::max<size_t>((size_t)S2 * stage, SV_SIG_BYTES + 2u * SV_QBUF);
@@ -1767,7 +2064,9 @@ static size_t sz_t_cols(const TcDims& d) {
   return d.big ? (size_t)d.n_chunks * d.nnc * d.NR * d.KC * 2 * 2 : (size_t)d.n_chunks * d.Np * d.KC * 2 * 2;
 }
 static size_t sz_sig_cols(const TcDims& d) { return (size_t)d.n_chunks * (d.big ? d.MT * 128 : 128) * d.KC * 2; }
-static size_t sz_vp(const TcDims& d) { return (size_t)d.NB * d.VK * 2 * 2; }
+// the direction-vector operand buffer holds V' or Bz (sized for both, so that switching forms
+// between calls needs no new workspace)
+static size_t sz_vp(const TcDims& d) { return std::max((size_t)d.NB * d.VK * 2 * 2, (size_t)d.Kz * d.NZ * 4); }
 
 size_t tc_workspace_bytes(const TcDims& d) {
   return al256(sz_t_rows(d)) + al256(sz_t_cols(d)) + al256(sz_sig_cols(d)) + al256(sz_vp(d)) +
@@ -1798,6 +2097,8 @@ static int tc_set_attrs() {
   QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ohu_big_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
   QES_CUDA_CHECK(cudaFuncSetAttribute(tc_sv_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTcSmemLimit));
+  QES_CUDA_CHECK(cudaFuncSetAttribute(tc_ovz_kernel<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kTcSmemLimit));
   return QES_OK;
 }
@@ -1845,17 +2146,45 @@ int tc_prepare_step(int dtype, const TcDims& d, int64_t n_samples, const uint32_
   else
     tc_sigma_cols_kernel<<<1184, 256, 0, st>>>(d.ns, d.KC, n_samples, d.n_chunks, bits, w.sig_cols);
   QES_LAUNCH_CHECK();
+  // tc_ovz_kernel reads T transposed per tile (in the t_rows buffer, which holds it: 128 x 2 Mp x 4
+  // bytes per tile >= 128 x nh x 8 complex, 128 x Kd x 4 >= 128 x nh x 4 real)
+  const bool rows = !d.ovz || d.sv;
+  if (!rows) {
+    const int64_t squares = (int64_t)d.n_tiles * 4 * ((d.nh + 31) / 32);
+    const int grid = (int)std::min<int64_t>(squares, 4096);
+    if (dtype == QES_DTYPE_C64)
+      tc_t_tiles_kernel<float2><<<grid, dim3(32, 8), 0, st>>>(d.nh, n_samples, d.n_tiles, (const float2*)tanh_theta,
+                                                              reinterpret_cast<float2*>(w.t_rows));
+    else
+      tc_t_tiles_kernel<float><<<grid, dim3(32, 8), 0, st>>>(d.nh, n_samples, d.n_tiles, (const float*)tanh_theta,
+                                                             reinterpret_cast<float*>(w.t_rows));
+    QES_LAUNCH_CHECK();
+  }
   if (dtype == QES_DTYPE_C64) {
-    tc_t_rows_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_rows);
+    if (rows) tc_t_rows_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_rows);
     if (d.big) tc_t_cols_big_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_cols);
     else tc_t_cols_kernel<float2><<<1184, 256, 0, st>>>(d, n_samples, (const float2*)tanh_theta, w.t_cols);
     QES_LAUNCH_CHECK_N(2);
   } else {
-    tc_t_rows_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_rows);
+    if (rows) tc_t_rows_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_rows);
     if (d.big) tc_t_cols_big_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_cols);
     else tc_t_cols_kernel<float><<<1184, 256, 0, st>>>(d, n_samples, (const float*)tanh_theta, w.t_cols);
     QES_LAUNCH_CHECK_N(2);
   }
+  return QES_OK;
+}
+
+// the direction-vector operand of the O v kernel in use (V' or Bz), built from v
+template <class V>
+static int tc_build_operand(const TcDims& d, bool cplx, const V* v, const TcWork& w, cudaStream_t st) {
+  if (d.ovz) {
+    const int items = d.NZ * (d.Kz / 8);
+    tc_build_vz_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
+  } else {
+    const int items = d.NB * (d.VK / 8);
+    tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
+  }
+  QES_LAUNCH_CHECK();
   return QES_OK;
 }
 
@@ -1895,14 +2224,17 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
     // first iteration: an ordinary launch, so that everything before it (the setup that clears the
     // converged flag of the previous solve) has completed before the PDL chain begins; the flag is
     // read by tc_ov / tc_ohu before they wait on their predecessor
-    const int items = d.NB * (d.VK / 8);
-    tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
-    QES_LAUNCH_CHECK();
+    if (int rc = tc_build_operand<V>(d, cplx, v, w, st)) return rc;
   }
   int pf = qes_prof_begin(QES_PROF_OV, st);
-  QES_CUDA_CHECK(qes_launch_pdl(tc_ov_kernel<T, V>, dim3(d.n_tiles), dim3(kThreads), (size_t)d.ov_smem, st, d,
-                                n_samples, bits, v, (const uint16_t*)w.t_rows, (const uint16_t*)w.vp, w_out, w.wsum,
-                                w.status, cg_done, w.wts));
+  if (d.ovz)
+    QES_CUDA_CHECK(qes_launch_pdl(tc_ovz_kernel<T, V>, dim3(d.n_tiles), dim3(kThreads), (size_t)d.ovz_smem, st, d,
+                                  n_samples, bits, v, reinterpret_cast<const T*>(w.t_rows), (const uint16_t*)w.vp,
+                                  w_out, w.wsum, w.status, cg_done, w.wts));
+  else
+    QES_CUDA_CHECK(qes_launch_pdl(tc_ov_kernel<T, V>, dim3(d.n_tiles), dim3(kThreads), (size_t)d.ov_smem, st, d,
+                                  n_samples, bits, v, (const uint16_t*)w.t_rows, (const uint16_t*)w.vp, w_out, w.wsum,
+                                  w.status, cg_done, w.wts));
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   pf = qes_prof_begin(QES_PROF_OHU, st);
@@ -1920,24 +2252,28 @@ static int tc_matvec_t(const TcDims& d, int64_t n_samples, const uint32_t* bits,
 }
 
 template <class T, class V>
-static int tc_ov_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const V* v, float2* w_out,
+static int tc_ov_t(const TcDims& d, int64_t n_samples, const uint32_t* bits, const T* tt, const V* v, float2* w_out,
                    const TcWork& w, cudaStream_t st) {
   const bool cplx = ScalarTraits<T>::is_complex;
-  const int items = d.NB * (d.VK / 8);
-  tc_build_vp_kernel<V><<<(items + 255) / 256, 256, 0, st>>>(d, cplx, v, w.vp);
-  QES_LAUNCH_CHECK();
+  if (int rc = tc_build_operand<V>(d, cplx, v, w, st)) return rc;
   const int pf = qes_prof_begin(QES_PROF_OV, st);
-  tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
-                                                           w.status, nullptr, w.wts);
+  if (d.ovz)
+    tc_ovz_kernel<T, V><<<d.n_tiles, kThreads, d.ovz_smem, st>>>(d, n_samples, bits, v,
+                                                               reinterpret_cast<const T*>(w.t_rows), w.vp, w_out,
+                                                               w.wsum, w.status, nullptr, w.wts);
+  else
+    tc_ov_kernel<T, V><<<d.n_tiles, kThreads, d.ov_smem, st>>>(d, n_samples, bits, v, w.t_rows, w.vp, w_out, w.wsum,
+                                                             w.status, nullptr, w.wts);
   QES_LAUNCH_CHECK();
   qes_prof_end(pf, st);
   return QES_OK;
 }
 
-int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
-          const TcWork& w, cudaStream_t st) {
-  if (dtype == QES_DTYPE_C64) return tc_ov_t<float2, double2>(d, n_samples, bits, (const double2*)v, w_out, w, st);
-  return tc_ov_t<float, double>(d, n_samples, bits, (const double*)v, w_out, w, st);
+int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta, const void* v,
+          float2* w_out, const TcWork& w, cudaStream_t st) {
+  if (dtype == QES_DTYPE_C64)
+    return tc_ov_t<float2, double2>(d, n_samples, bits, (const float2*)tanh_theta, (const double2*)v, w_out, w, st);
+  return tc_ov_t<float, double>(d, n_samples, bits, (const float*)tanh_theta, (const double*)v, w_out, w, st);
 }
 
 int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta,

@@ -37,6 +37,12 @@ struct TcDims {
   // shared memory hold the O v pipeline (sv_stages stages), then Sigma^T and two Q^T chunk buffers
   bool sv;
   int sv_grid, sv_stages, sv_region, sv_smem;
+  // O v through z = Sigma V (tc_ovz_kernel): A = the spins and a ones column (128 samples x Kz,
+  // Kz = sites + 1 padded to 16, exact in BF16), B = Bz (NZ rows x Kz, hi/lo): row m is Re V_{.,m},
+  // row Mp + m (complex) is Im V_{.,m}, K index ns holds v_b; (O v)_s = sum_m t_sm z_sm + sigma_s . v_a
+  // with t in float32.  Bz replaces V' in the direction-vector buffer when ovz is set.
+  bool ovz;
+  int Kz, NZ, ovz_smem, ovz_tmem;
 };
 
 // Configuration of a bounded grid barrier: `extra` arrivals that never come and a short poll limit
@@ -72,8 +78,8 @@ int tc_matvec(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bit
               const double* cg_done = nullptr, BarCfg bc = BarCfg{0u, kGridBarLimit});
 inline int tc_matvec_nsplit(const TcDims& d) { return d.sv ? d.sv_grid : d.nsplit; }
 // w_out = O v only (builds the V' operand from v first)
-int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* v, float2* w_out,
-          const TcWork& w, cudaStream_t st);
+int tc_ov(int dtype, const TcDims& d, int64_t n_samples, const uint32_t* bits, const void* tanh_theta, const void* v,
+          float2* w_out, const TcWork& w, cudaStream_t st);
 // partial[chunk] = O^H (wts (g - mean) * scale): gsum_n > 0 -> gsum_part holds gsum_n partial sums
 // (mean = sum / Ns); gsum_n < 0 -> gsum_part[0] is the mean; gsum_part == nullptr -> no centring
 int tc_ohu(int dtype, const TcDims& d, int64_t n_samples, const float2* g, const double2* gsum_part, int gsum_n,
@@ -94,11 +100,30 @@ __device__ __forceinline__ void tc_put_vp(const TcDims& d, uint16_t* vp, int n, 
   *reinterpret_cast<uint16_t*>(base + off) = hi;
   *reinterpret_cast<uint16_t*>(base + term_bytes + off) = lo;
 }
+// Bz entry (row n, K index k): k-step k / 16 holds [hi tile | lo tile] of NZ rows x 16
+__device__ __forceinline__ void tc_put_vz(const TcDims& d, uint16_t* vz, int n, int k, float x) {
+  const uint16_t hi = __bfloat16_as_ushort(__float2bfloat16_rn(x));
+  const uint16_t lo = __bfloat16_as_ushort(__float2bfloat16_rn(x - __bfloat162float(__ushort_as_bfloat16(hi))));
+  const size_t tile_bytes = (size_t)d.NZ * 32;
+  uint8_t* base = reinterpret_cast<uint8_t*>(vz) + (size_t)(k >> 4) * 2 * tile_bytes;
+  const uint32_t off = umma::kmajor_offset((uint32_t)n, (uint32_t)(k & 15), (uint32_t)d.NZ);
+  *reinterpret_cast<uint16_t*>(base + off) = hi;
+  *reinterpret_cast<uint16_t*>(base + tile_bytes + off) = lo;
+}
 __device__ __forceinline__ void tc_put_vp_elem(const TcDims& d, uint16_t* vp, int i, int m, double vr) {
+  if (d.ovz) {                                               // Bz: row m, K index i
+    tc_put_vz(d, vp, m, i, (float)vr);
+    return;
+  }
   tc_put_vp(d, vp, i, m, (float)vr);                         // real RBM: row i, column m
 }
 __device__ __forceinline__ void tc_put_vp_elem(const TcDims& d, uint16_t* vp, int i, int m, double2 v) {
   const float vr = (float)v.x, vi = (float)v.y;
+  if (d.ovz) {                                               // Bz: rows m (Re) and Mp + m (Im), K index i
+    tc_put_vz(d, vp, m, i, vr);
+    tc_put_vz(d, vp, d.Mp + m, i, vi);
+    return;
+  }
   if (d.splitc) {                                            // V'' rows: Re v, then Im v
     tc_put_vp(d, vp, i, m, vr);
     tc_put_vp(d, vp, d.Sp + i, m, vi);

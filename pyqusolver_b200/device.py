@@ -267,11 +267,13 @@ def sr_matvec(flat_params, ns, nh, bits, tanh_theta, v, shift=0.0, workspace=Non
 
 def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
                 check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True, x0=None, probs=None,
-                precond=None):
+                precond=None, true_residual=True):
     """x0: initial guess of the unscaled system (S + shift) x = F (a previous solution divided by
     rhs_prefactor), float64 / complex128 of length P on the device; None starts from zero.
     probs: per-sample weights (any positive scale; normalised to sum Ns here), None = uniform.
-    precond: None or "jacobi" (CG preconditioned by 1 / diag(S + shift), SciPy's cg(M=...))."""
+    precond: None or "jacobi" (CG preconditioned by 1 / diag(S + shift), SciPy's cg(M=...)).
+    true_residual: recompute ||F - (S + shift) x|| / ||F|| after the solve (one more matvec);
+    info["true_residual"] is -1 when False."""
     dc = dtype_code(flat_params)
     n = int(bits.shape[0])
     ws = workspace if workspace is not None else sr_workspace(dc, ns, nh, n, bits.device)
@@ -285,7 +287,7 @@ def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8
     if pc is None:
         raise ValueError(f"preconditioner {precond!r}: None or 'jacobi'")
     opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor),
-                         pc)
+                         pc, 0 if true_residual else 1)
     res = _lib.SRResult()
     allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_converged else ()
     w = sample_weights(probs, n, bits.device)
@@ -299,7 +301,7 @@ def sr_solve_cg(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8
 
 def sr_solve_minres(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=1e-8, atol=0.0, maxiter=1000,
                     check_every=16, rhs_prefactor=-1.0, workspace=None, allow_not_converged=True, x0=None,
-                    probs=None):
+                    probs=None, true_residual=True):
     """The SR system solved by MINRES (``qes_sr_solve_minres_weighted``): arguments and stopping rule as
     sr_solve_cg; info["acond"] is the recurrence's condition estimate of S + shift."""
     dc = dtype_code(flat_params)
@@ -310,7 +312,8 @@ def sr_solve_minres(flat_params, ns, nh, bits, tanh_theta, eloc, *, shift, rtol=
         x0 = x0.to(device=bits.device, dtype=x.dtype).contiguous()
         if x0.numel() != x.numel():
             raise ValueError(f"x0 has {x0.numel()} entries, the parameter vector {x.numel()}")
-    opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor))
+    opt = _lib.SROptions(float(shift), float(rtol), float(atol), int(maxiter), int(check_every), float(rhs_prefactor),
+                         _lib.PRECOND_NONE, 0 if true_residual else 1)
     res = _lib.SRResult()
     allow = (_lib.QES_ERR_NOT_CONVERGED,) if allow_not_converged else ()
     w = sample_weights(probs, n, bits.device)

@@ -48,14 +48,16 @@ class TDVP:
     Options whose effect this path does not implement raise instead of being ignored; options that
     only tune solvers or features this path does not offer (the pseudo-inverse and SNR tolerances,
     backend, logger, timing) are accepted because they cannot change a CG result.  ``sr_tol`` /
-    ``sr_atol`` (SciPy's rtol / atol), ``check_every`` and ``use_old_result`` are this package's
-    additions."""
+    ``sr_atol`` (SciPy's rtol / atol), ``check_every``, ``use_old_result`` and ``true_residual`` are
+    this package's additions; ``true_residual=True`` has every CG / MINRES solve recompute
+    ||F - (S + shift) x|| / ||F|| with one more matvec (``last_info["true_residual"]``, -1 when off,
+    the default: the reference computes no such diagnostic)."""
 
     def __init__(self, use_sr=True, use_minsr=False, rhs_prefactor=1.0, *, regularization=0.0,
                  sr_lin_solver=None, sr_precond=None, sr_snr_tol=1e-3, sr_pinv_tol=1e-14, sr_pinv_cutoff=1e-8,
                  sr_diag_shift=1e-3, sr_lin_solver_t="gram", sr_lin_x0=None, sr_maxiter=100, sr_form_matrix=False,
                  backend="default", logger=None, use_timing=False, dtype=None, grad_clip=None, verbose=False,
-                 sr_tol=1e-8, sr_atol=0.0, check_every=16, use_old_result=False):
+                 sr_tol=1e-8, sr_atol=0.0, check_every=16, use_old_result=False, true_residual=False):
         solver = "scipy_cg" if sr_lin_solver is None else str(getattr(sr_lin_solver, "name", sr_lin_solver)).lower()
         if solver not in _SOLVERS_CG + _SOLVERS_MINRES + _SOLVERS_DIRECT:
             raise NotImplementedError(f"linear solver {sr_lin_solver!r}: the GPU path implements CG (scipy_cg), "
@@ -98,6 +100,7 @@ class TDVP:
         self.sr_maxiter = int(sr_maxiter)
         self.grad_clip = grad_clip
         self.check_every = int(check_every)
+        self.true_residual = bool(true_residual)
         self._workspace = None
         self.last_info = None
         # initial guess of the CG (QES/NQS/src/tdvp.py:1346-1380): a fixed vector sr_lin_x0, or with
@@ -165,12 +168,14 @@ class TDVP:
                 x, info = dv.sr_solve_minres(net.flat, net.ns, net.nh, bits, tanh_theta, eloc,
                                              shift=self.sr_diag_shift, rtol=self.sr_tol, atol=self.sr_atol,
                                              maxiter=self.sr_maxiter, check_every=self.check_every,
-                                             rhs_prefactor=self.rhs_prefactor, workspace=ws, x0=x0, probs=probs)
+                                             rhs_prefactor=self.rhs_prefactor, workspace=ws, x0=x0, probs=probs,
+                                             true_residual=self.true_residual)
             else:
                 x, info = dv.sr_solve_cg(net.flat, net.ns, net.nh, bits, tanh_theta, eloc, shift=self.sr_diag_shift,
                                          rtol=self.sr_tol, atol=self.sr_atol, maxiter=self.sr_maxiter,
                                          check_every=self.check_every, rhs_prefactor=self.rhs_prefactor,
-                                         workspace=ws, x0=x0, probs=probs, precond=self.sr_precond)
+                                         workspace=ws, x0=x0, probs=probs, precond=self.sr_precond,
+                                         true_residual=self.true_residual)
             self.last_info = info
             self._solution = x.detach().clone()
         if self.grad_clip is not None and self.grad_clip > 0:

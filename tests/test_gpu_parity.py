@@ -455,10 +455,25 @@ def sr_impl():
     _lib.set_sr_impl(_lib.SR_IMPL_AUTO)
 
 
+@pytest.fixture
+def ovz_switch():
+    yield lambda on: _lib.call("qes_sr_set_ovz", int(on))
+    _lib.call("qes_sr_set_ovz", 1)
+
+
 @pytest.mark.parametrize("cplx,ns,nh,n", [(False, 16, 16, 300), (True, 9, 18, 700), (True, 36, 144, 1000),
                                            (False, 20, 40, 513), (True, 100, 200, 300),
-                                           (False, 150, 300, 700), (True, 130, 100, 500)])
-def test_sr_matvec_tensor_cores_match_oracle(sr_impl, cplx, ns, nh, n):
+                                           (False, 150, 300, 700), (True, 130, 100, 500),
+                                           (True, 12, 21, 333), (False, 15, 30, 257), (True, 31, 255, 129)])
+@pytest.mark.parametrize("ovz", [1, 0])
+def test_sr_matvec_tensor_cores_match_oracle(sr_impl, ovz_switch, cplx, ns, nh, n, ovz):
+    """The tensor-core S v against the float64 oracle, with O v through z = Sigma V (ovz = 1, where its
+    operands fit: the default) and as the product over the hidden axis (ovz = 0).  Shapes include odd
+    hidden-unit counts (T read element by element), sites + 1 on a 16 boundary, partial sample tiles
+    and the M/N-tiled O^H u."""
+    ovz_switch(ovz)
+    if (ns, nh) in ((100, 200), (36, 144), (12, 21), (15, 30), (31, 255)):
+        assert _lib.sr_tc_plan(_lib.DTYPE_C64 if cplx else _lib.DTYPE_F32, ns, nh, n)["ovz"] == ovz
     net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=21, init_scale=0.1)
     st = rand_states(n, ns, seed=22)
     bits = dv.pack_states(st)

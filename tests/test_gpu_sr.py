@@ -364,3 +364,67 @@ def test_tdvp_minres_qlp_option():
     assert torch.allclose(x0, x1, rtol=1e-4, atol=1e-6 * float(x0.abs().max()))
     with pytest.raises(NotImplementedError):
         TDVP(sr_lin_solver="minres", sr_precond="jacobi")
+
+
+# ------------------------------------------------------------------------- Chronopoulos-Gear CG steps
+@pytest.mark.parametrize("impl", [0, 1, 3])
+@pytest.mark.parametrize("rtol", [1e-8, 1e-10])
+def test_cg_single_reduction_matches_two_reduction_form(impl, rtol):
+    """qes_set_cg_single_reduction(1) (Chronopoulos-Gear steps, the matvec of r with |r|^2 summed by
+    its split reduction, one update kernel) against the standard steps (0, the default: matvec of
+    p, x/r update with its |r|^2 reduction, p update) on the same weighted system, down to tight
+    tolerances (the convergence test runs on the residual vector's norm in both): both converge;
+    the standard form meets the dense solve's backward-error bar of 1e-4, the Chronopoulos-Gear
+    form 1e-4 in float64 and 1e-3 in the float32 forms (its s = A p recurrence carries the
+    operator's rounding forward, a wider residual gap); in the float64 form (impl 3) the iteration
+    counts agree to within 3% and the solutions to 1e-6, in the float32 forms (0 = tensor cores,
+    1 = CUDA cores, whose operator rounding makes late iterations sensitive to any change) the
+    iteration counts to within 25%."""
+    ns, nh, n = 10, 20, 700                      # P = 230: the vector form of the split reduction
+    model = qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.4)
+    net = RBM((ns,), n_hidden=nh, dtype="complex64", seed=15, init_scale=0.3)
+    rng = np.random.default_rng(15)
+    st = np.where(rng.random((n, ns)) < 0.5, 0.5, -0.5)
+    bits = dv.pack_states(st)
+    _, tn, lp = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=True)
+    h = dv.DeviceHamiltonian(model.lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    lu = lp.real.double().cpu().numpy()
+    pr = np.exp(0.5 * (lu - lu.max()))
+    probs_t = torch.as_tensor((pr / pr.sum() * n).astype(np.float32)).cuda()
+    w = probs_t.double().cpu().numpy()
+    w = w / w.sum() * n
+    e = eloc.cpu().numpy().astype(np.complex128)
+    O = osr.o_rows(None, orbm.to_sigma(st), tanh=tn.cpu().numpy())
+    ec, Oc, w_, _, _ = osr.prepare(e, O, w)
+    F = osr.force(Oc, ec, w_)
+    shift = 1e-2
+    A = osr.s_matrix(Oc, w_) + shift * np.eye(O.shape[1])
+    out = {}
+    _lib.set_sr_impl(impl)
+    _lib.call("qes_set_cg_fused", 0)
+    try:
+        for single in (1, 0):
+            _lib.call("qes_set_cg_single_reduction", single)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=shift, rtol=rtol, maxiter=3000,
+                                     probs=probs_t, check_every=8)
+            out[single] = (-x.cpu().numpy(), info)
+    finally:
+        _lib.call("qes_set_cg_single_reduction", 0)
+        _lib.call("qes_set_cg_fused", 1)
+        _lib.set_sr_impl(0)
+    (x1, i1), (x0, i0) = out[1], out[0]
+    assert i1["converged"] and i0["converged"]
+    assert i1["residual"] <= rtol * i1["rhs_norm"] * (1 + 1e-12)
+    assert np.linalg.norm(A @ x0 - F) / np.linalg.norm(F) < 1e-4
+    # the s = A p recurrence carries the float32 operator's rounding forward: a larger gap between
+    # the recursive and the true residual in the float32 forms
+    bar1 = 1e-4 if impl == 3 else 1e-3
+    assert np.linalg.norm(A @ x1 - F) / np.linalg.norm(F) < bar1
+    if impl == 3:
+        assert abs(i1["iterations"] - i0["iterations"]) <= max(1, 0.03 * i0["iterations"]), (i1["iterations"],
+                                                                                            i0["iterations"])
+        assert np.max(np.abs(x1 - x0)) / np.max(np.abs(x0)) < 1e-6
+    else:
+        assert abs(i1["iterations"] - i0["iterations"]) <= max(2, 0.25 * i0["iterations"])

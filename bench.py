@@ -886,7 +886,9 @@ def roofline(cfg, nqs, form):
     from pyqusolver_b200 import _lib, device as dv
     net = nqs.net
     tc = _lib.sr_uses_tensor_cores(dv.dtype_code(net.flat), net.ns, net.nh, cfg["chains"] * cfg["samples"])
-    names = {"ov": "tc_ov_kernel (O v, tcgen05)" if tc else "ov_kernel (O v, CUDA cores)",
+    ovz = tc and _lib.sr_tc_plan(dv.dtype_code(net.flat), net.ns, net.nh, cfg["chains"] * cfg["samples"])["ovz"]
+    names = {"ov": ("tc_ovz_kernel (O v through z = Sigma V, tcgen05)" if ovz else "tc_ov_kernel (O v, tcgen05)")
+             if tc else "ov_kernel (O v, CUDA cores)",
              "ohu": "tc_ohu_kernel (O^H u, tcgen05)" if tc else "ohu_kernel (O^H u, CUDA cores)",
              "reduce": "reduce_splits_kernel / cg_fused_kernel", "sample": "sampler_kernel",
              "sv": "tc_sv_kernel (S v: O v and O^H u fused, tcgen05)",

@@ -413,6 +413,15 @@ int qes_set_cg_fused(int mode);
  * fused cooperative vector kernel (qes_set_cg_fused) the standard form
  * runs.                                                                    */
 int qes_set_cg_single_reduction(int on);
+/* The split reduction of the SR matvec (the sum of the split-K partial
+ * P-vectors that the O^H u kernels write, + shift p and the CG dot products)
+ * with each block's column slices of every partial moved into shared memory
+ * by bulk copies under one mbarrier (1, where the slices fit 88 KB: two
+ * blocks per SM), or loaded by the threads in batches of 16-byte loads (0,
+ * the default: measured faster on B200, 12.8 against 16.8 us per launch on
+ * the 10x10 workload, where the bulk form issues 147 small copies per
+ * block).  Same sums in the same order: bit-identical results.            */
+int qes_set_reduce_bulk(int on);
 /* Test hook of the fused CG kernel's grid barriers (no reference
  * counterpart): (1, polls) makes every barrier wait for one arrival that
  * never comes and give up after `polls` polls, so a solve returns

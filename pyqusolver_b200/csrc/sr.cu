@@ -394,7 +394,88 @@ constexpr int RS_MAX_BLOCKS = 1184;      // upper bound of dot partials written 
 QES_D void acc4(double* g, float4 q) { g[0] += q.x; g[1] += q.y; g[2] += q.z; g[3] += q.w; }
 QES_D void acc4(double2* g, float4 q) { g[0].x += q.x; g[0].y += q.y; g[1].x += q.z; g[1].y += q.w; }
 
-template <class T, class V, bool VEC>
+// Dot partials of a split-reduction block and, in the last block to finish, the CG scalars:
+// alpha (standard steps) or the Chronopoulos-Gear step's scalars (cgmode).
+template <bool CG>
+QES_D void reduce_splits_tail(const double (&dd)[5], double* __restrict__ dot_part,
+                              double* __restrict__ scal, unsigned int* __restrict__ counter) {
+  if (!dot_part) return;
+  const int tid = threadIdx.x;
+  // dot partials: dd[q] of block b at dot_part[q * RS_MAX_BLOCKS + b]
+  constexpr bool cgmode = CG;
+  constexpr int nd = CG ? 5 : 1;
+  __shared__ double sred[5][RS_THREADS / 32];
+  __shared__ bool last;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q >= nd) break;
+    const double v = warp_sum(dd[q]);
+    if ((tid & 31) == 0) sred[q][tid >> 5] = v;
+  }
+  __syncthreads();
+  if (tid == 0) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      if (q >= nd) break;
+      double s = 0.0;
+      for (int w = 0; w < RS_THREADS / 32; ++w) s += sred[q][w];
+      dot_part[q * RS_MAX_BLOCKS + blockIdx.x] = s;
+    }
+    // the last block to finish sums the dot partials: pAp and alpha = rr / pAp
+    if (scal) {
+      __threadfence();
+      last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+  }
+  if (!scal) return;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (q >= nd) break;
+    double v = 0.0;
+    for (int b = tid; b < (int)gridDim.x; b += RS_THREADS) v += ((volatile double*)dot_part)[q * RS_MAX_BLOCKS + b];
+    v = warp_sum(v);
+    __syncthreads();
+    if ((tid & 31) == 0) sred[q][tid >> 5] = v;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double tot[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int q = 0; q < nd; ++q)
+      for (int w = 0; w < RS_THREADS / 32; ++w) tot[q] += sred[q][w];
+    if (!cgmode) {
+      const double pap = tot[0];
+      scal[1] = pap;
+      scal[7] = (scal[4] == 0.0 && pap > 0.0) ? scal[0] / pap : 0.0;
+    } else if (scal[4] == 0.0) {
+      // Chronopoulos-Gear step k on r_k (v = r_k, y = A r_k): rr = |r_k|^2 from the vector itself,
+      // the convergence test on it (x_k is final: this step's update is skipped), else
+      // beta_k = rr / rr_{k-1} and alpha_k = rr / p_k^H A p_k with p_k^H A p_k expanded bilinearly
+      // in p_k = r_k + beta p_{k-1}, s_k = A r_k + beta s_{k-1} (the update kernel's recurrences):
+      // r^H A r + beta (Re r^H s_{k-1} + Re p_{k-1}^H A r) + beta^2 Re p_{k-1}^H s_{k-1}, from the
+      // vectors themselves rather than from the orthogonality relations of exact arithmetic
+      const double rw = tot[0], rr = tot[1];
+      scal[2] = rr;
+      if (rr <= scal[3]) {
+        scal[4] = 1.0;
+      } else {
+        const bool first = scal[5] == 0.0;
+        const double beta = (first || scal[0] <= 0.0) ? 0.0 : rr / scal[0];
+        const double den = first ? rw : rw + beta * (tot[2] + tot[3]) + beta * beta * tot[4];
+        scal[1] = den;                                   // p_k^H A p_k
+        scal[7] = den > 0.0 ? rr / den : 0.0;
+        scal[8] = beta;
+        scal[0] = rr;
+        scal[5] += 1.0;
+      }
+    }
+    *counter = 0u;
+  }
+}
+
+template <class T, class V, bool VEC, bool CG>
 __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P, int nsplit, int cv,
                                                                       const T* __restrict__ partial, double shift,
                                                                       const V* __restrict__ p, V* __restrict__ y,
@@ -415,7 +496,7 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
   // dd[0] = Re v^H y; with pold / sold (a Chronopoulos-Gear CG step: v = r_k, y = A r_k, the previous
   // direction p_{k-1} and s_{k-1} = A p_{k-1}): dd[1] = |v|^2, dd[2] = Re v^H s_{k-1},
   // dd[3] = Re p_{k-1}^H y, dd[4] = Re p_{k-1}^H s_{k-1}
-  const bool cgmode = pold != nullptr;
+  constexpr bool cgmode = CG;
   double dd[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t v0 = (int64_t)blockIdx.x * cv; v0 < nvec; v0 += (int64_t)gridDim.x * cv) {
     const int64_t vi = v0 + c;
@@ -460,7 +541,7 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
           const V pk = p[kk];
           t = vadd(t, vscale(shift, pk));
           dd[0] += vdotc(pk, t);
-          if (cgmode) {
+          if constexpr (cgmode) {
             const V po = pold[kk], so = sold[kk];
             dd[1] += vdotc(pk, pk);
             dd[2] += vdotc(pk, so);
@@ -473,72 +554,104 @@ __global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_kernel(int64_t P,
     }
     __syncthreads();
   }
-  if (!dot_part) return;
-  // dot partials: dd[q] of block b at dot_part[q * RS_MAX_BLOCKS + b]
-  const int nd = cgmode ? 5 : 1;
-  __shared__ double sred[5][RS_THREADS / 32];
-  __shared__ bool last;
-  for (int q = 0; q < nd; ++q) {
-    const double v = warp_sum(dd[q]);
-    if ((tid & 31) == 0) sred[q][tid >> 5] = v;
-  }
-  __syncthreads();
+  reduce_splits_tail<CG>(dd, dot_part, scal, counter);
+}
+
+// The same split reduction with the partials moved by bulk copies: a block's column slice of every
+// split (cv 16-byte vectors each) lands in shared memory through one mbarrier, so the loads do
+// not wait in the threads' scoreboards (the register-load form is bound by load latency: 24 MB of
+// partials at about 2 TB/s on the 10x10 workload).  Same sums in the same fixed order as
+// reduce_splits_kernel<VEC = true>, so the results are bit-identical.  A bounded wait that runs
+// out records QES_ERR_TIMEOUT in *err and the block goes on with what it has.
+template <class T, class V, bool CG>
+__global__ void __launch_bounds__(RS_THREADS, 2) reduce_splits_bulk_kernel(int64_t P, int nsplit, int cv,
+                                                                          const T* __restrict__ partial,
+                                                                          double shift, const V* __restrict__ p,
+                                                                          V* __restrict__ y,
+                                                                          double* __restrict__ dot_part,
+                                                                          double* __restrict__ scal,
+                                                                          unsigned int* __restrict__ counter,
+                                                                          const double* __restrict__ cg_done,
+                                                                          const V* __restrict__ pold,
+                                                                          const V* __restrict__ sold,
+                                                                          int* __restrict__ err) {
+  constexpr int E = (int)(16 / sizeof(T));
+  extern __shared__ __align__(128) uint8_t rs_smem[];
+  float4* sbuf = reinterpret_cast<float4*>(rs_smem);      // [split][cv]
+  __shared__ V red[RS_THREADS * E];
+  __shared__ __align__(8) uint64_t bar;
+  pdl_trigger();
+  pdl_wait();                                              // the partials: previous kernel
+  if (cg_done && *cg_done != 0.0) return;
+  const int tid = threadIdx.x;
+  const int groups = RS_THREADS / cv, c = tid % cv, sg = tid / cv;
+  const int64_t nvec = P / E;
   if (tid == 0) {
-    for (int q = 0; q < nd; ++q) {
-      double s = 0.0;
-      for (int w = 0; w < RS_THREADS / 32; ++w) s += sred[q][w];
-      dot_part[q * RS_MAX_BLOCKS + blockIdx.x] = s;
-    }
-    // the last block to finish sums the dot partials: pAp and alpha = rr / pAp
-    if (scal) {
-      __threadfence();
-      last = (atomicAdd(counter, 1u) == gridDim.x - 1);
-    }
+    umma::mbar_init(&bar, 1);
+    umma::fence_mbar_init();
   }
-  if (!scal) return;
   __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int q = 0; q < nd; ++q) {
-    double v = 0.0;
-    for (int b = tid; b < (int)gridDim.x; b += RS_THREADS) v += ((volatile double*)dot_part)[q * RS_MAX_BLOCKS + b];
-    v = warp_sum(v);
+  constexpr bool cgmode = CG;
+  double dd[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  uint32_t phase = 0;
+  for (int64_t v0 = (int64_t)blockIdx.x * cv; v0 < nvec; v0 += (int64_t)gridDim.x * cv) {
+    const int cvv = (int)((nvec - v0 < cv) ? (nvec - v0) : cv);
+    if (tid == 0) {
+      umma::fence_proxy_async_smem();                      // earlier reads of sbuf before the new copies
+      umma::mbar_arrive_expect_tx(&bar, (uint32_t)(nsplit * cvv * 16));
+      const float4* src = reinterpret_cast<const float4*>(partial) + v0;
+      for (int z = 0; z < nsplit; ++z)
+        umma::bulk_g2s(sbuf + (size_t)z * cv, src + (int64_t)z * nvec, (uint32_t)(cvv * 16), &bar);
+    }
+    if (!umma::mbar_wait(&bar, phase, 1u << 22) && tid == 0 && err) atomicCAS(err, 0, QES_ERR_TIMEOUT);
+    phase ^= 1u;
+    V g[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) g[e] = vzero(V());
+    if (sg < groups && c < cvv) {
+      // the same split order as the register-load form (z = sg, sg + groups, ...)
+#pragma unroll 4
+      for (int z = sg; z < nsplit; z += groups) acc4(g, sbuf[(size_t)z * cv + c]);
+    }
+    if (sg < groups) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) red[(sg * cv + c) * E + e] = g[e];
+    }
     __syncthreads();
-    if ((tid & 31) == 0) sred[q][tid >> 5] = v;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    double tot[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int q = 0; q < nd; ++q)
-      for (int w = 0; w < RS_THREADS / 32; ++w) tot[q] += sred[q][w];
-    if (!cgmode) {
-      const double pap = tot[0];
-      scal[1] = pap;
-      scal[7] = (scal[4] == 0.0 && pap > 0.0) ? scal[0] / pap : 0.0;
-    } else if (scal[4] == 0.0) {
-      // Chronopoulos-Gear step k on r_k (v = r_k, y = A r_k): rr = |r_k|^2 from the vector itself,
-      // the convergence test on it (x_k is final: this step's update is skipped), else
-      // beta_k = rr / rr_{k-1} and alpha_k = rr / p_k^H A p_k with p_k^H A p_k expanded bilinearly
-      // in p_k = r_k + beta p_{k-1}, s_k = A r_k + beta s_{k-1} (the update kernel's recurrences):
-      // r^H A r + beta (Re r^H s_{k-1} + Re p_{k-1}^H A r) + beta^2 Re p_{k-1}^H s_{k-1}, from the
-      // vectors themselves rather than from the orthogonality relations of exact arithmetic
-      const double rw = tot[0], rr = tot[1];
-      scal[2] = rr;
-      if (rr <= scal[3]) {
-        scal[4] = 1.0;
-      } else {
-        const bool first = scal[5] == 0.0;
-        const double beta = (first || scal[0] <= 0.0) ? 0.0 : rr / scal[0];
-        const double den = first ? rw : rw + beta * (tot[2] + tot[3]) + beta * beta * tot[4];
-        scal[1] = den;                                   // p_k^H A p_k
-        scal[7] = den > 0.0 ? rr / den : 0.0;
-        scal[8] = beta;
-        scal[0] = rr;
-        scal[5] += 1.0;
+    if (tid < cv * E) {
+      const int64_t kk = v0 * E + tid;
+      if (kk < P) {
+        V t = red[tid];
+        for (int q = 1; q < groups; ++q) t = vadd(t, red[q * cv * E + tid]);
+        if (p) {
+          const V pk = p[kk];
+          t = vadd(t, vscale(shift, pk));
+          dd[0] += vdotc(pk, t);
+          if constexpr (cgmode) {
+            const V po = pold[kk], so = sold[kk];
+            dd[1] += vdotc(pk, pk);
+            dd[2] += vdotc(pk, so);
+            dd[3] += vdotc(po, t);
+            dd[4] += vdotc(po, so);
+          }
+        }
+        y[kk] = t;
       }
     }
-    *counter = 0u;
+    __syncthreads();
   }
+  reduce_splits_tail<CG>(dd, dot_part, scal, counter);
+}
+
+// the bulk-copy split reduction (qes_set_reduce_bulk) where a block's slices fit 88 KB of shared
+// memory (two blocks per SM): off by default -- one thread issuing a small bulk copy per split
+// (147 x 560 B per block on the 10x10 workload) made the reduction slower, 16.8 against 12.8 us
+// per launch (CG iteration 43.4 against 42.2 us; 6x6 J1-J2 30.2 against 28.7 us)
+static std::atomic<int> g_reduce_bulk{0};
+constexpr size_t kReduceBulkSmem = 88 * 1024;
+extern "C" int qes_set_reduce_bulk(int on) {
+  g_reduce_bulk.store(on ? 1 : 0);
+  return QES_OK;
 }
 
 // y = sum of the nsplit partial P-vectors (+ shift * p, dot partials, alpha): the vector form
@@ -558,15 +671,32 @@ static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, doub
   cv = std::min<int64_t>(cv, std::max<int64_t>(RS_THREADS / std::max<int64_t>(need, 1), 1));
   cv = std::max<int64_t>(1, std::min<int64_t>(cv, 128));
   const int grid = (int)std::min<int64_t>((nvec + cv - 1) / cv, RS_MAX_BLOCKS);
+  const bool cg = pold != nullptr;
   if constexpr (!IsF64<T>::value) {
+    const size_t bulk_smem = (size_t)nsplit * (size_t)cv * 16;
+    if (vec && g_reduce_bulk.load() != 0 && bulk_smem <= kReduceBulkSmem) {
+      static bool attr_set = false;                        // per process (the attribute is per function)
+      if (!attr_set) {
+        QES_CUDA_CHECK(cudaFuncSetAttribute(reduce_splits_bulk_kernel<T, V, false>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReduceBulkSmem));
+        QES_CUDA_CHECK(cudaFuncSetAttribute(reduce_splits_bulk_kernel<T, V, true>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReduceBulkSmem));
+        attr_set = true;
+      }
+      QES_CUDA_CHECK(qes_launch_pdl(cg ? reduce_splits_bulk_kernel<T, V, true> : reduce_splits_bulk_kernel<T, V, false>,
+                                    dim3(grid), dim3(RS_THREADS), bulk_smem, st, P,
+                                    nsplit, (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter,
+                                    cg_done, pold, sold, counter ? (int*)(counter + 4) : (int*)nullptr));
+      return QES_OK;
+    }
     if (vec) {
-      QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, true>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
+      QES_CUDA_CHECK(qes_launch_pdl(cg ? reduce_splits_kernel<T, V, true, true> : reduce_splits_kernel<T, V, true, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
                                     (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done,
                                     pold, sold));
       return QES_OK;
     }
   }
-    QES_CUDA_CHECK(qes_launch_pdl(reduce_splits_kernel<T, V, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
+    QES_CUDA_CHECK(qes_launch_pdl(cg ? reduce_splits_kernel<T, V, false, true> : reduce_splits_kernel<T, V, false, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
                                   (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done,
                                   pold, sold));
   return QES_OK;

@@ -891,3 +891,35 @@ def test_forward_tensor_cores_match_cuda_cores_and_oracle(cplx, ns, nh, n):
     wrap_close(lp1.cpu().numpy(), lp0.cpu().numpy())
     p = oracle_params(net)
     wrap_close(lp1.cpu().numpy(), orbm.log_psi(p, orbm.to_sigma(st)))
+
+
+# ------------------------------------------------------------------------- bulk-copy split reduction
+@pytest.mark.parametrize("cplx,ns,nh,n", [(True, 100, 200, 4000), (False, 36, 144, 3000), (True, 24, 48, 777)])
+def test_bulk_split_reduction_is_bit_identical(sr_impl, cplx, ns, nh, n):
+    """qes_set_reduce_bulk(1) (the split-K partials moved into shared memory by bulk copies) against
+    the register-load reduction (0, the default): the same sums in the same order, so the S v of
+    the tensor-core and CUDA-core forms and a CG solve agree bit for bit."""
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=31, init_scale=0.1)
+    st = rand_states(n, ns, seed=32)
+    bits = dv.pack_states(st)
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    rng = np.random.default_rng(33)
+    P = dv.n_params(ns, nh)
+    v = torch.as_tensor(rng.normal(size=P) + (1j * rng.normal(size=P) if cplx else 0)).cuda()
+    eloc = torch.as_tensor((rng.normal(size=n) + 1j * rng.normal(size=n)).astype(np.complex64)).cuda()
+    out = {}
+    try:
+        for impl in (_lib.SR_IMPL_TENSOR_CORES, _lib.SR_IMPL_CUDA_CORES):
+            sr_impl(impl)
+            for bulk in (1, 0):
+                _lib.call("qes_set_reduce_bulk", bulk)
+                y = dv.sr_matvec(net.flat, ns, nh, bits, tn, v, shift=1e-3).cpu().numpy()
+                x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-8, maxiter=500,
+                                         check_every=16)
+                out[impl, bulk] = (y, x.cpu().numpy(), info["iterations"])
+    finally:
+        _lib.call("qes_set_reduce_bulk", 0)
+    for impl in (_lib.SR_IMPL_TENSOR_CORES, _lib.SR_IMPL_CUDA_CORES):
+        (y1, x1, i1), (y0, x0, i0) = out[impl, 1], out[impl, 0]
+        assert np.array_equal(y1, y0), impl
+        assert np.array_equal(x1, x0) and i1 == i0, impl

@@ -391,7 +391,8 @@ int qes_set_cg_graphs(int enable);
  * direction updates) as one cooperative kernel with two bounded grid
  * barriers: 2 = always, 1 = when its grid is at most 160 CTAs (the default:
  * parameter vectors up to a few thousand entries, where launch latency
- * dominates), 0 = never (three kernels).                                   */
+ * dominates), 3 = always with one CTA per SM (fewer grid-barrier arrivals),
+ * 0 = never (three kernels).                                               */
 int qes_set_cg_fused(int mode);
 /* CG steps in the Chronopoulos-Gear form on the kernel-chain path (1; for
  * the unpreconditioned CG): the matvec is applied to r_k, its

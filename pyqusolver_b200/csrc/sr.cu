@@ -1840,8 +1840,8 @@ extern "C" int qes_set_cg_single_reduction(int on) {
   return QES_OK;
 }
 extern "C" int qes_set_cg_fused(int mode) {
-  if (mode < 0 || mode > 2) {
-    qes_set_last_message("qes_set_cg_fused: mode 0 (off), 1 (automatic) or 2 (always)");
+  if (mode < 0 || mode > 3) {
+    qes_set_last_message("qes_set_cg_fused: mode 0 (off), 1 (automatic), 2 (always) or 3 (always, one CTA per SM)");
     return QES_ERR_ARG;
   }
   g_cg_fused.store(mode);
@@ -1970,7 +1970,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
       QES_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_fused_kernel<T, V, false>,
                                                                    CF_TX * CF_TY, 0));
     // column vectors per block pass as in the standalone split reduction, the grid within residency
-    const int64_t cap = std::min<int64_t>((int64_t)nsm * std::max(per_sm, 1), RED_BLOCKS);
+    // mode 3: one CTA per SM (the grid barriers then wait for fewer arrivals)
+    const int64_t cap = std::min<int64_t>((int64_t)nsm * (fused_mode == 3 ? 1 : std::max(per_sm, 1)), RED_BLOCKS);
     const int64_t nvec = fused_vec ? P / FEV : P;
     int64_t cv = (nvec + cap - 1) / cap;
     const int nthr = CF_TX * CF_TY;

@@ -5,7 +5,8 @@ problems) or an M/N-tiled kernel whose CTAs fold several sample chunks into TMEM
 hidden units, a target CTA count); ``qes_sr_set_ohu_pairs`` runs the single-tile kernel as pairs
 of CTAs that add their split-K partials through distributed shared memory, and
 ``qes_sr_set_fused_sv`` runs the single-tile matvec as one cooperative S v kernel (O v, the mean of
-O v over a grid barrier and O^H u in the same CTAs).  ``tune_sr_tiling`` times
+O v over a grid barrier and O^H u in the same CTAs); ``qes_sr_set_ov_split`` and ``qes_sr_set_ovz`` choose
+the O v product (split-complex over the hidden axis, or through z = Sigma V).  ``tune_sr_tiling`` times
 CG iterations on a given batch for every candidate (``qes_sr_solve_cg`` with the tolerance at zero, so
 that it runs exactly the iterations asked for; the time of K iterations subtracted from that of 2K
 removes the once-per-solve work: operand preparation, force, set-up), keeps the fastest, applies it

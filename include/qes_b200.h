@@ -423,6 +423,15 @@ int qes_set_cg_single_reduction(int on);
  * the 10x10 workload, where the bulk form issues 147 small copies per
  * block).  Same sums in the same order: bit-identical results.            */
 int qes_set_reduce_bulk(int on);
+/* The x/r update and the direction update of a standard CG step in one
+ * launch (1, the default on the kernel-chain path): phase 1 updates x and r
+ * and sums |r|^2 per block, a bounded grid barrier, then every CTA sums the
+ * partials in the same order as the two-kernel form and updates its slice
+ * of p and the tensor-core operand tiles (0: cg_xr then cg_p).  Bit-
+ * identical results; one launch boundary and one last-block step fewer.
+ * The fused cooperative vector kernel (qes_set_cg_fused) and the
+ * Chronopoulos-Gear steps take precedence where they are selected.         */
+int qes_set_cg_xrp(int on);
 /* Test hook of the fused CG kernel's grid barriers (no reference
  * counterpart): (1, polls) makes every barrier wait for one arrival that
  * never comes and give up after `polls` polls, so a solve returns

@@ -1083,6 +1083,91 @@ __device__ __forceinline__ void grid_barrier(unsigned int* count, unsigned int* 
   __syncthreads();
 }
 
+// x/r update and direction update of a CG step in one launch (qes_set_cg_xrp): phase 1 as
+// cg_xr_kernel (x += alpha p, r -= alpha Ap, per-block |r|^2 and r^H D^-1 r partials), a bounded
+// grid barrier, then every CTA sums the grid's partials in the same fixed order as cg_xr_kernel's
+// last block (so the scalars are bit-identical to the two-kernel form) and updates its own slice of
+// p and the operand tiles.  One launch boundary and one last-block step fewer per iteration.  The
+// grid (<= 296 blocks of 256 threads) is co-resident once every CTA has executed the programmatic
+// trigger, which is what lets the next kernel launch, so the barrier cannot wait on a CTA that a
+// dependent kernel keeps off the SMs; a barrier wait that runs out sets *err (the solve reports
+// QES_ERR_TIMEOUT).
+template <class V>
+__global__ void __launch_bounds__(RED_THREADS) cg_xrp_kernel(int64_t P, const V* __restrict__ Ap, V* __restrict__ x,
+                                                             V* __restrict__ r, V* __restrict__ p,
+                                                             double* __restrict__ scal, double* __restrict__ part,
+                                                             unsigned int* __restrict__ bar, int* __restrict__ err,
+                                                             TcDims td, uint16_t* __restrict__ vp, BarCfg bc,
+                                                             const double* __restrict__ dinv) {
+  pdl_trigger();
+  pdl_wait();                                              // Ap and alpha: previous kernel
+  // every CTA reads the scalars before any CTA can pass the barrier (CTA 0 rewrites them after it)
+  const double rho = scal[0], thresh = scal[3], alpha = scal[7];
+  if (scal[4] != 0.0) return;                              // converged at an earlier step
+  const unsigned int nb = gridDim.x;
+  const int tid = threadIdx.x;
+  __shared__ double sred[RED_THREADS / 32];
+  auto block_sum = [&](double v) -> double {
+    v = warp_sum(v);
+    if ((tid & 31) == 0) sred[tid >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int q = 0; q < RED_THREADS / 32; ++q) t += sred[q];
+    __syncthreads();
+    return t;
+  };
+  double e = 0.0, ez = 0.0;
+  const int64_t stride = (int64_t)nb * RED_THREADS;
+  for (int64_t k = (int64_t)blockIdx.x * RED_THREADS + tid; k < P; k += stride) {
+    x[k] = vadd(x[k], vscale(alpha, p[k]));
+    const V rk = vadd(r[k], vscale(-alpha, Ap[k]));
+    r[k] = rk;
+    const double q = vdotc(rk, rk);
+    e += q;
+    if (dinv) ez += q * dinv[k];
+  }
+  e = block_sum(e);
+  if (tid == 0) part[blockIdx.x] = e;
+  if (dinv) {
+    ez = block_sum(ez);
+    if (tid == 0) part[nb + blockIdx.x] = ez;
+  }
+  grid_barrier(bar, bar + 32, nb, err, bc);
+  auto sum_parts = [&](const double* src) -> double {
+    double v = 0.0;
+    for (unsigned int b = tid; b < nb; b += RED_THREADS) v += __ldcg(src + b);
+    return block_sum(v);
+  };
+  const double rr_new = sum_parts(part);
+  const double rho_new = dinv ? sum_parts(part + nb) : rr_new;
+  const double beta = (rho > 0.0) ? rho_new / rho : 0.0;
+  const bool conv = rr_new <= thresh;
+  if (!conv) {
+    const int ns = td.ns, nh = td.nh;
+    for (int64_t k = (int64_t)blockIdx.x * RED_THREADS + tid; k < P; k += stride) {
+      const V zk = dinv ? vscale(dinv[k], r[k]) : r[k];
+      const V pk = vadd(zk, vscale(beta, p[k]));
+      p[k] = pk;
+      if (vp && k >= ns) {
+        const int64_t q = k - ns;
+        if (q < nh) {
+          tc_put_vp_elem(td, vp, ns, (int)q, pk);                        // v_b row
+        } else {
+          const uint32_t qw = (uint32_t)(q - nh);                        // ns * nh < 2^32 on this path
+          tc_put_vp_elem(td, vp, (int)(qw / (uint32_t)nh), (int)(qw % (uint32_t)nh), pk);
+        }
+      }
+    }
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    scal[2] = rr_new;
+    scal[5] += 1.0;
+    scal[8] = beta;
+    scal[0] = rho_new;
+    if (conv) scal[4] = 1.0;
+  }
+}
+
 // cv: column vectors per block pass (16-byte vectors when VEC), chosen by the host like the
 // standalone split reduction (every thread issues its split loads in one batch)
 template <class T, class V, bool VEC>
@@ -1828,6 +1913,13 @@ extern "C" int qes_sr_set_barrier_test(unsigned int extra_arrivals, unsigned int
   return QES_OK;
 }
 
+// x/r and direction updates of the standard CG step in one launch with a grid barrier
+// (cg_xrp_kernel): on by default
+static std::atomic<int> g_cg_xrp{1};
+extern "C" int qes_set_cg_xrp(int on) {
+  g_cg_xrp.store(on ? 1 : 0);
+  return QES_OK;
+}
 // Chronopoulos-Gear CG steps (the matvec of r, one reduction, one update kernel) on the kernel-chain
 // path: off by default -- one kernel and one grid-wide reduction fewer per step (heis10x10 CG
 // iteration 43.3 -> 40.3 us, the same 136 iterations), but the s = A p recurrence does not damp the
@@ -1987,6 +2079,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
   }
   const BarCfg bcfg{g_bar_extra.load(), g_bar_limit.load()};
   const bool single = !fused && dinv == nullptr && g_cg_single.load() != 0;
+  const bool xrp = !fused && !single && g_cg_xrp.load() != 0;
   auto run_direct = [&](int nrun, int it0) -> int {
     for (int q = 0; q < nrun; ++q) {
       if (fused) {
@@ -2044,6 +2137,13 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
                               /*vp_ready=*/it0 + q > 0, L.scal + 4);
       if (r2) return r2;
       // (alpha is computed by the last block of the matvec's split reduction)
+      if (xrp) {
+        QES_CUDA_CHECK(qes_launch_pdl(cg_xrp_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P,
+                                      (const V*)Ap, x, r, p, L.scal, L.parts, L.counter + 32, (int*)(L.counter + 4),
+                                      L.td, L.tc ? L.tw.vp : (uint16_t*)nullptr, bcfg, dinv));
+        QES_LAUNCH_CHECK();
+        continue;
+      }
       QES_CUDA_CHECK(qes_launch_pdl(cg_xr_kernel<V>, dim3(vec_blocks(P)), dim3(RED_THREADS), 0, st, P, (const V*)p,
                                     (const V*)Ap, x, r, L.scal, L.parts, L.counter + 1, dinv,
                                     dinv ? L.parts + RED_BLOCKS : (double*)nullptr));
@@ -2091,7 +2191,8 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
                            L.tc ? 1 : 0, (l2 ? 1 : 0) | (fused ? 2 : 0) | (dinv ? 4 : 0), L.td.big ? 1 : 0,
                            L.td.KC, L.mv_nsplit,
                            L.td.nnc, L.td.NC, L.td.SPC,
-                           L.td.cl | (L.td.sv ? 4 : 0) | (L.td.ovz ? 8 : 0) | (L.td.splitc ? 16 : 0) | (single ? 32 : 0),
+                           L.td.cl | (L.td.sv ? 4 : 0) | (L.td.ovz ? 8 : 0) | (L.td.splitc ? 16 : 0) | (single ? 32 : 0) |
+                               (xrp ? 64 : 0),
                            (int)bcfg.extra, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {

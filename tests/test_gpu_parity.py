@@ -923,3 +923,33 @@ def test_bulk_split_reduction_is_bit_identical(sr_impl, cplx, ns, nh, n):
         (y1, x1, i1), (y0, x0, i0) = out[impl, 1], out[impl, 0]
         assert np.array_equal(y1, y0), impl
         assert np.array_equal(x1, x0) and i1 == i0, impl
+
+
+@pytest.mark.parametrize("impl", [_lib.SR_IMPL_TENSOR_CORES, _lib.SR_IMPL_CUDA_CORES])
+@pytest.mark.parametrize("cplx,precond", [(True, None), (True, "jacobi"), (False, None)])
+def test_cg_xrp_kernel_is_bit_identical(sr_impl, impl, cplx, precond):
+    """qes_set_cg_xrp(1) (the default: the x/r and direction updates in one launch with a grid
+    barrier) against cg_xr + cg_p (0): the same per-block partials summed in the same order, so the
+    solutions, iteration counts and residuals agree bit for bit, through the device loop's graph."""
+    ns, nh, n = 30, 60, 3000                     # P = 1,890: a multi-block vector grid
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=41, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=42))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    sr_impl(impl)
+    out = {}
+    try:
+        _lib.call("qes_set_cg_fused", 0)
+        for on in (1, 0):
+            _lib.call("qes_set_cg_xrp", on)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-9, maxiter=2000,
+                                     check_every=8, precond=precond)
+            out[on] = (x.cpu().numpy(), info["iterations"], info["residual"], info["converged"])
+    finally:
+        _lib.call("qes_set_cg_xrp", 1)
+        _lib.call("qes_set_cg_fused", 1)
+    assert out[1][3] and out[0][3] and out[1][1] > 16
+    assert out[1][1] == out[0][1] and out[1][2] == out[0][2]
+    assert np.array_equal(out[1][0], out[0][0])

@@ -384,6 +384,12 @@ int qes_sr_set_ov_split(int on);
  * against V').  Same operator; the hi/lo split touches v only.  Takes the
  * fused S v kernel and the split-complex product out of the plan.          */
 int qes_sr_set_ovz(int on);
+/* tc_ovz_kernel's CTAs pull their 128-sample tile of the transposed T into
+ * L2 (cp.async.bulk.prefetch.L2) before they wait on the previous kernel
+ * of the CG chain (1), or not (0, the default: measured the same, 42.1 vs
+ * 42.3 us per 10x10 CG iteration, T already stays in L2).  A hint: results
+ * are the same either way.                                                 */
+int qes_sr_set_prefetch(int on);
 /* CG iteration chunks replayed as CUDA graphs on a private stream (1, the
  * default) or launched one by one on the caller's stream (0).              */
 int qes_set_cg_graphs(int enable);

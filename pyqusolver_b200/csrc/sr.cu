@@ -2192,7 +2192,7 @@ static int sr_cg_t(int ns, int nh, int64_t n_samples, const uint32_t* bits, cons
                            L.td.KC, L.mv_nsplit,
                            L.td.nnc, L.td.NC, L.td.SPC,
                            L.td.cl | (L.td.sv ? 4 : 0) | (L.td.ovz ? 8 : 0) | (L.td.splitc ? 16 : 0) | (single ? 32 : 0) |
-                               (xrp ? 64 : 0),
+                               (xrp ? 64 : 0) | (L.td.prefetch ? 128 : 0),
                            (int)bcfg.extra, opt->shift};
       if (gs.exec == nullptr || !(gs.key == key)) {
         if (gs.exec) {

@@ -620,6 +620,14 @@ __global__ void __launch_bounds__(kThreads) tc_ovz_kernel(TcDims d, int64_t n_sa
     for (int c = 0; c < nks; ++c) umma::mbar_init(&full[c], 1);
     umma::mbar_init(done, 1);
     umma::fence_mbar_init();
+    // the tile's transposed T (per-step data, read in the epilogue) is pulled into L2 while this
+    // CTA waits on its predecessor
+    const size_t tbytes = (size_t)nh * 128 * sizeof(T);
+    if (d.prefetch && ((reinterpret_cast<uintptr_t>(t_tiles) | tbytes) & 15) == 0) {
+      const uint8_t* tb = reinterpret_cast<const uint8_t*>(t_tiles) + (size_t)tile * tbytes;
+      for (size_t o = 0; o < tbytes; o += 65536)
+        umma::bulk_prefetch_l2(tb + o, (uint32_t)((tbytes - o < 65536) ? (tbytes - o) : 65536));
+    }
   }
   // per-step inputs (older than the previous kernel): the tile's spin words, then A
   const int64_t r0 = (int64_t)tile * 128;
@@ -1900,6 +1908,14 @@ extern "C" int qes_sr_set_ov_split(int on) {
 }
 // O v through z = Sigma V (tc_ovz_kernel) where its operands fit: on by default
 static std::atomic<int> g_ovz{1};
+// L2 prefetch of tc_ovz_kernel's T tile before it waits on its predecessor: off by default
+// (heis10x10 CG iteration 42.3 us with it, 42.1 us without; 6x6 J1-J2 28.8 both: T already stays
+// in L2 between iterations)
+static std::atomic<int> g_prefetch{0};
+extern "C" int qes_sr_set_prefetch(int on) {
+  g_prefetch.store(on ? 1 : 0);
+  return QES_OK;
+}
 extern "C" int qes_sr_set_ovz(int on) {
   g_ovz.store(on ? 1 : 0);
   return QES_OK;
@@ -1977,6 +1993,7 @@ bool tc_plan(int dtype, int ns, int nh, int64_t n_samples, TcDims* dout) {
     t.ovz = g_ovz.load() != 0 && !t.splitc && g_sv.load() == 0 && t.NZ <= 512 && zsm <= kTcSmemLimit;
     t.ovz_smem = (int)zsm;
     t.ovz_tmem = pow2_at_least(std::max(t.NZ, 32));
+    t.prefetch = g_prefetch.load() != 0;
   }
   t.n_tiles = (int)((n_samples + 127) / 128);
   t.big = ns > 127 || t.Mp > 256 || t.NB > 256;

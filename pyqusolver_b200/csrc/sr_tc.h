@@ -43,6 +43,7 @@ struct TcDims {
   // with t in float32.  Bz replaces V' in the direction-vector buffer when ovz is set.
   bool ovz;
   int Kz, NZ, ovz_smem, ovz_tmem;
+  bool prefetch;     // tc_ovz_kernel pulls its T tile into L2 before waiting on its predecessor
 };
 
 // Configuration of a bounded grid barrier: `extra` arrivals that never come and a short poll limit

@@ -829,6 +829,15 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
     }
   }
   pdl_wait();                                             // w and its partial sums: previous kernel
+  // this thread's sample of w (and weight) is requested before the mean's block reduction, so the
+  // two global round trips overlap (KC <= 256 < kThreads, tc_plan: one sample per thread)
+  static_assert(kThreads >= 256, "one sample of the O^H u chunk per thread");
+  float2 w_pre = make_float2(0.f, 0.f);
+  float wt_pre = 1.f;
+  if (tid < KC && s0 + tid < n_samples) {
+    w_pre = w[s0 + tid];
+    if (wts) wt_pre = wts[s0 + tid];
+  }
   // mean of w: the per-tile partial sums are reduced by the whole block (fixed order)
   {
     double2 t = make_double2(0.0, 0.0);
@@ -862,16 +871,14 @@ __global__ void __launch_bounds__(kThreads) tc_ohu_kernel(TcDims d, int64_t n_sa
   umma::tc_fence_after();
   const uint32_t tbase = *tslot;
   const float mr = (float)s_mean.x, mi = (float)s_mean.y, fs = (float)scale;
-  for (int k = tid; k < KC; k += kThreads) {
-    const int64_t s = s0 + k;
+  if (tid < KC) {
     T u = ScalarTraits<T>::zero();
-    if (s < n_samples) {
-      const float2 wv = w[s];
-      const float f = wts ? fs * wts[s] : fs;
-      if constexpr (CPLX) u = make_float2((wv.x - mr) * f, (wv.y - mi) * f);
-      else u = (wv.x - mr) * f;
+    if (s0 + tid < n_samples) {
+      const float f = wts ? fs * wt_pre : fs;
+      if constexpr (CPLX) u = make_float2((w_pre.x - mr) * f, (w_pre.y - mi) * f);
+      else u = (w_pre.x - mr) * f;
     }
-    s_u[k] = u;
+    s_u[tid] = u;
   }
   __syncthreads();
   const bool loaded = valid && umma::mbar_wait(&bars[0], 0, kWaitLimit);

@@ -953,3 +953,30 @@ def test_cg_xrp_kernel_is_bit_identical(sr_impl, impl, cplx, precond):
     assert out[1][3] and out[0][3] and out[1][1] > 16
     assert out[1][1] == out[0][1] and out[1][2] == out[0][2]
     assert np.array_equal(out[1][0], out[0][0])
+
+
+def test_ovz_l2_prefetch_changes_nothing(sr_impl):
+    """qes_sr_set_prefetch(1) only adds an L2 prefetch of the z-form O v kernel's T tile: S v and a CG
+    solve through the device loop are bit-identical with and without it."""
+    ns, nh, n = 100, 200, 2000
+    net = RBM((ns,), n_hidden=nh, dtype="complex64", seed=51, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=52))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    assert _lib.sr_tc_plan(_lib.DTYPE_C64, ns, nh, n)["ovz"] == 1
+    rng = np.random.default_rng(53)
+    P = dv.n_params(ns, nh)
+    v = torch.as_tensor(rng.normal(size=P) + 1j * rng.normal(size=P)).cuda()
+    eloc = torch.as_tensor((rng.normal(size=n) + 1j * rng.normal(size=n)).astype(np.complex64)).cuda()
+    sr_impl(_lib.SR_IMPL_TENSOR_CORES)
+    out = {}
+    try:
+        for on in (1, 0):
+            _lib.call("qes_sr_set_prefetch", on)
+            y = dv.sr_matvec(net.flat, ns, nh, bits, tn, v, shift=1e-3).cpu().numpy()
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-8, maxiter=300,
+                                     check_every=8)
+            out[on] = (y, x.cpu().numpy(), info["iterations"])
+    finally:
+        _lib.call("qes_sr_set_prefetch", 0)
+    assert np.array_equal(out[1][0], out[0][0])
+    assert np.array_equal(out[1][1], out[0][1]) and out[1][2] == out[0][2]

@@ -683,22 +683,22 @@ static int launch_reduce_splits(int64_t P, int nsplit, const void* partial, doub
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kReduceBulkSmem));
         attr_set = true;
       }
-      QES_CUDA_CHECK(qes_launch_pdl(cg ? reduce_splits_bulk_kernel<T, V, true> : reduce_splits_bulk_kernel<T, V, false>,
-                                    dim3(grid), dim3(RS_THREADS), bulk_smem, st, P,
-                                    nsplit, (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter,
-                                    cg_done, pold, sold, counter ? (int*)(counter + 4) : (int*)nullptr));
+      auto kern = cg ? reduce_splits_bulk_kernel<T, V, true> : reduce_splits_bulk_kernel<T, V, false>;
+      QES_CUDA_CHECK(qes_launch_pdl(kern, dim3(grid), dim3(RS_THREADS), bulk_smem, st, P, nsplit, (int)cv,
+                                    (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done, pold, sold,
+                                    counter ? (int*)(counter + 4) : (int*)nullptr));
       return QES_OK;
     }
     if (vec) {
-      QES_CUDA_CHECK(qes_launch_pdl(cg ? reduce_splits_kernel<T, V, true, true> : reduce_splits_kernel<T, V, true, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
-                                    (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done,
-                                    pold, sold));
+      auto kern = cg ? reduce_splits_kernel<T, V, true, true> : reduce_splits_kernel<T, V, true, false>;
+      QES_CUDA_CHECK(qes_launch_pdl(kern, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit, (int)cv, (const T*)partial,
+                                    shift, p, y, dot_part, scal, counter, cg_done, pold, sold));
       return QES_OK;
     }
   }
-    QES_CUDA_CHECK(qes_launch_pdl(cg ? reduce_splits_kernel<T, V, false, true> : reduce_splits_kernel<T, V, false, false>, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit,
-                                  (int)cv, (const T*)partial, shift, p, y, dot_part, scal, counter, cg_done,
-                                  pold, sold));
+  auto kern = cg ? reduce_splits_kernel<T, V, false, true> : reduce_splits_kernel<T, V, false, false>;
+  QES_CUDA_CHECK(qes_launch_pdl(kern, dim3(grid), dim3(RS_THREADS), 0, st, P, nsplit, (int)cv, (const T*)partial, shift,
+                                p, y, dot_part, scal, counter, cg_done, pold, sold));
   return QES_OK;
 }
 

@@ -438,6 +438,13 @@ int qes_set_reduce_bulk(int on);
  * The fused cooperative vector kernel (qes_set_cg_fused) and the
  * Chronopoulos-Gear steps take precedence where they are selected.         */
 int qes_set_cg_xrp(int on);
+/* The fused cooperative vector kernel (qes_set_cg_fused) launched by
+ * programmatic dependent launch (1, the default) instead of as a cooperative
+ * launch (0): its grid, sized within residency, is co-resident once every
+ * CTA has run the trigger at its entry, and its prologue overlaps the O^H u
+ * kernel's tail (TFIM-16 CG iteration 18.8 -> 18.3 us).  Same kernel, same
+ * sums: bit-identical results.                                            */
+int qes_set_cg_fused_pdl(int on);
 /* Test hook of the fused CG kernel's grid barriers (no reference
  * counterpart): (1, polls) makes every barrier wait for one arrival that
  * never comes and give up after `polls` polls, so a solve returns

@@ -132,6 +132,7 @@ SIGNATURES = {
     "qes_set_cg_single_reduction": [C.c_int],
     "qes_set_reduce_bulk": [C.c_int],
     "qes_set_cg_xrp": [C.c_int],
+    "qes_set_cg_fused_pdl": [C.c_int],
     "qes_sr_set_prefetch": [C.c_int],
     "qes_sr_set_barrier_test": [C.c_uint, C.c_uint],
     "qes_rbm_forward_tc_workspace_bytes": [C.c_int, C.c_int, C.c_int, _i64, C.POINTER(_sz)],

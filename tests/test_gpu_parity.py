@@ -980,3 +980,32 @@ def test_ovz_l2_prefetch_changes_nothing(sr_impl):
         _lib.call("qes_sr_set_prefetch", 0)
     assert np.array_equal(out[1][0], out[0][0])
     assert np.array_equal(out[1][1], out[0][1]) and out[1][2] == out[0][2]
+
+
+@pytest.mark.parametrize("cplx", [True, False])
+def test_fused_vector_kernel_pdl_launch_is_bit_identical(sr_impl, cplx):
+    """qes_set_cg_fused_pdl(1) (the default: the fused vector kernel launched by programmatic dependent
+    launch) against the cooperative launch (0): the same kernel and sums, so the CG solutions,
+    iteration counts and residuals agree bit for bit."""
+    ns, nh, n = 16, 32, 2048
+    net = RBM((ns,), n_hidden=nh, dtype="complex64" if cplx else "float32", seed=61, init_scale=0.1)
+    bits = dv.pack_states(rand_states(n, ns, seed=62))
+    _, tn, _ = dv.rbm_forward(net.flat, ns, nh, bits, tanh=True, logpsi=False)
+    h = dv.DeviceHamiltonian(qb.XXZ(qb.SquareLattice(1, ns), jxy=-1.0, jz=-1.0, hx=0.3).lower())
+    tables = dv.move_tables(net.flat, ns, nh, h.move_i, h.move_j, h.move_kind, move_major=False)
+    eloc = dv.local_energy(net.flat, ns, nh, bits, tn, h, tables)
+    sr_impl(_lib.SR_IMPL_TENSOR_CORES)
+    out = {}
+    try:
+        _lib.call("qes_set_cg_fused", 2)
+        for on in (1, 0):
+            _lib.call("qes_set_cg_fused_pdl", on)
+            x, info = dv.sr_solve_cg(net.flat, ns, nh, bits, tn, eloc, shift=1e-2, rtol=1e-9, maxiter=2000,
+                                     check_every=8)
+            out[on] = (x.cpu().numpy(), info["iterations"], info["residual"], info["converged"])
+    finally:
+        _lib.call("qes_set_cg_fused_pdl", 1)
+        _lib.call("qes_set_cg_fused", 1)
+    assert out[1][3] and out[0][3]
+    assert out[1][1] == out[0][1] and out[1][2] == out[0][2]
+    assert np.array_equal(out[1][0], out[0][0])
